@@ -1,0 +1,239 @@
+/*
+ * mz_b200.h -- C ABI of the B200 evaluator for the spline EAM/MEAM fitting
+ * objective.
+ *
+ * The reference program evaluates its objective through the polymorphic C++
+ * class Potential (src/potential.h:35-109).  Every optimizer (Powell,
+ * simulated annealing, genetic algorithm) calls
+ *     double Potential::compute(const Comm&, ErrorVec* = nullptr)   potential.h:67
+ * which, for the spline styles, runs PotMEAMSpline::fast_compute<Spline3Eq>
+ * (src/pots/pot_meam_spline/pot_meam_spline.cpp:102-283) or
+ * PotEAMSpline::fast_compute<Spline3Eq>
+ * (src/pots/pot_eam_spline/pot_eam_spline.cpp:100-223).
+ *
+ * This header is the drop-in boundary for that call.  It carries plain
+ * pointers and sizes only.  No C++ exception crosses it: every function
+ * returns an mz_status (0 = success) and mz_last_error() returns the message
+ * of the last failure on the calling thread.  Host buffers are owned by the
+ * caller; the evaluator context owns its device memory, stream and graphs.
+ * One context may be used by one host thread at a time.
+ *
+ * File formats are the reference's own (potential file pot_list.cpp:101-142
+ * and spline3eq.cpp:54-106, configuration file cell.cpp:39-136), and the
+ * parameter vector layout is the reference's Potential::coeff order
+ * (potential.cpp:192-206 -> pot_fns.cpp:209-218 -> spline.cpp:105-114 ->
+ * spline3eq.cpp:376-382): for each function group in file order, for each
+ * alloy spline, the free knot values in ascending knot order, then the free
+ * end slopes (left, right).
+ */
+#ifndef MZ_B200_H
+#define MZ_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int mz_status;
+
+enum {
+  MZ_OK = 0,
+  MZ_ERR_ARG = 1,          /* bad argument (null pointer, size mismatch)          */
+  MZ_ERR_IO = 2,           /* file cannot be opened                              */
+  MZ_ERR_FORMAT = 3,       /* malformed potential / configuration file           */
+  MZ_ERR_RANGE = 4,        /* pair closer than a spline's first knot, cell too    */
+                           /* small, or a neighbour row beyond the kernel limit   */
+  MZ_ERR_UNSUPPORTED = 5,  /* potential style / basis not implemented            */
+  MZ_ERR_CUDA = 6,         /* CUDA runtime error (message has the CUDA text)      */
+  MZ_ERR_NOMEM = 7,        /* host or device allocation failed                   */
+  MZ_ERR_TIMEOUT = 8       /* a bounded device wait gave up                      */
+};
+
+/* arithmetic of an evaluation */
+enum {
+  MZ_FP64 = 0,   /* everything in FP64 (reference parity path)                    */
+  MZ_MIXED = 1   /* FP32 spline and triplet arithmetic, FP64 per-atom densities,  */
+                 /* energies, virials, residuals and gradient sums                */
+};
+
+/* potential styles (the #T string of the potential file) */
+enum { MZ_STYLE_EAM_SPLINE = 0, MZ_STYLE_MEAM_SPLINE = 1 };
+
+typedef struct mz_pot mz_pot;  /* a potential: splines + parameter layout        */
+typedef struct mz_db mz_db;    /* configuration database + neighbour lists       */
+typedef struct mz_ctx mz_ctx;  /* device-resident evaluator                      */
+
+/* Message of the last failed call on this thread ("" if none). */
+const char *mz_last_error(void);
+
+/* ---------------------------------------------------------------- potential */
+
+/* Read a potential file (first #P block).  Replaces PotList::init
+ * (src/pot_list.cpp:84-177) + Potential::read_pot (potential.cpp:153-161)
+ * for the eam/spline and meam/spline styles with spline3eq bases. */
+mz_status mz_pot_read(const char *path, mz_pot **out);
+/* Same from the file's text held in memory. */
+mz_status mz_pot_parse(const char *text, mz_pot **out);
+void mz_pot_free(mz_pot *pot);
+/* Style (MZ_STYLE_*), number of atom types, number of splines. */
+mz_status mz_pot_info(const mz_pot *pot, int *style, int *ntypes, int *nsplines);
+/* Number of adjustable coefficients: Potential::get_ncoeff (potential.h:59). */
+mz_status mz_pot_ncoeff(const mz_pot *pot, int *ncoeff);
+/* Read / write all coefficients in Potential::coeff(i) order (potential.h:60). */
+mz_status mz_pot_get_coeffs(const mz_pot *pot, double *coeffs);
+mz_status mz_pot_set_coeffs(mz_pot *pot, const double *coeffs);
+/* Write the potential in the reference format (Potential::write_pot,
+ * potential.cpp:299-319; Spline3Eq::write_basis_fn, spline3eq.cpp:248-273). */
+mz_status mz_pot_write(const mz_pot *pot, const char *path);
+/* Evaluate spline s of the potential at x: value and slope.  Mirrors
+ * Spline3Eq::splint_comb(double, double*) (spline3eq.h:204-236), linear
+ * extrapolation outside the knots.  Host-side, for tests and tools. */
+mz_status mz_pot_spline_eval(const mz_pot *pot, int spline, double x, double *val, double *grad);
+
+/* ----------------------------------------------------------------- database */
+
+/* Cells given as arrays (all host memory, copied).  Atoms are in cell order.
+ * Replaces the parsed result of Cell::read_cell (src/cell.cpp:39-136). */
+typedef struct {
+  int ncells;
+  int natoms;
+  const int *cell_natoms;      /* [ncells]                                   */
+  const double *cell_lattice;  /* [ncells][3][3] rows = #X #Y #Z vectors    */
+  const double *cell_energy0;  /* [ncells] target energy per atom (#E)      */
+  const double *cell_stress0;  /* [ncells][6] xx yy zz xy yz zx (#S)        */
+  const double *cell_weight;   /* [ncells] (#W, default 1)  nullable        */
+  const double *cell_eweight;  /* [ncells] (#EW, default 1) nullable        */
+  const double *cell_sweight;  /* [ncells] (#SW, default 1) nullable        */
+  const int *atom_type;        /* [natoms]                                   */
+  const double *atom_pos;      /* [natoms][3]                                */
+  const double *atom_force0;   /* [natoms][3] target forces                  */
+} mz_cells_desc;
+
+/* Build the database and its neighbour lists for a potential.  Replaces
+ * Config::init (config.cpp:46-119): Cell::find_scale (cell.cpp:158-170),
+ * Config::find_pairs (config.cpp:143-234, full double-counted list), the
+ * per-pair knot/shift set-up of check_pair (pair_meam_spline.cpp:50-99,
+ * pair_eam_spline.cpp:50-86) and, for MEAM, find_triplets
+ * (config.cpp:240-285) whose triplets are enumerated implicitly as the j<k
+ * pairs of each atom's row.  Fails with MZ_ERR_RANGE where the reference
+ * throws (pair shorter than a spline's first knot). */
+mz_status mz_db_build(const mz_cells_desc *cells, const mz_pot *pot, mz_db **out);
+/* Read a configuration file (#N/#X/#Y/#Z/#E/#S/#W/#EW/#SW/#F) and build. */
+mz_status mz_db_read(const char *config_path, const mz_pot *pot, mz_db **out);
+void mz_db_free(mz_db *db);
+
+typedef struct {
+  int ncells;
+  int natoms;
+  int64_t npairs;       /* entries of the full neighbour list             */
+  int64_t ntriplets;    /* j<k pairs of every row (= reference triplets)  */
+  int max_row;          /* longest neighbour row                          */
+  int esize;            /* residual entries of the cells: 8 ncells + 3    */
+                        /* natoms (the style penalties add 1 for MEAM,    */
+                        /* ntypes for EAM)                                */
+} mz_db_stats;
+mz_status mz_db_info(const mz_db *db, mz_db_stats *stats);
+
+/* Read-only view of the built database (pointers into the mz_db, valid
+ * until mz_db_free).  Pair data of atom i occupy slots
+ * [pair_off[i], pair_off[i+1]) in the reference's pair order; pair_knot and
+ * pair_shift hold (phi, rho, f) per slot, knot -1 where the reference's is
+ * -1 (f unused for EAM).  in_off/in_slot list, per atom, the slots whose
+ * neighbour it is. */
+typedef struct {
+  int ncells, natoms;
+  int64_t npairs;
+  const int *cell_atom0;  /* [ncells+1] */
+  const double *cell_vol, *cell_weight, *cell_eweight, *cell_sweight, *cell_energy0;
+  const double *cell_stress0;  /* [ncells][6] */
+  const double *cell_lattice;  /* [ncells][9] */
+  const int *atom_type, *atom_cell;
+  const double *atom_pos, *atom_force0;  /* [natoms][3] */
+  const int64_t *pair_off;               /* [natoms+1] */
+  const int *pair_nbr;
+  const double *pair_r, *pair_u;         /* u: [npairs][3] */
+  const int8_t *pair_knot;               /* [npairs][3] */
+  const double *pair_shift;              /* [npairs][3] */
+  const int64_t *in_off, *in_slot;
+} mz_db_view;
+mz_status mz_db_get_view(const mz_db *db, mz_db_view *view);
+
+/* One spline of a potential as read (group-major order: phi..., rho...,
+ * U..., f..., g...).  Pointers valid until the potential changes. */
+typedef struct {
+  int group, alloy, nknots;
+  double left, right;
+  int nat[2];         /* natural end (bc -1)       */
+  int grad_fixed[2];  /* end slope fixed (bc 1)    */
+  double grad[2];
+  const int *y_fixed;
+  const double *y;
+} mz_spline_view;
+mz_status mz_pot_get_spline(const mz_pot *pot, int spline, mz_spline_view *view);
+
+/* Replace the targets (energy per atom, stress, forces) of every cell. */
+mz_status mz_db_set_targets(mz_db *db, const double *energy0, const double *stress0,
+                            const double *force0);
+
+/* ---------------------------------------------------------------- evaluator */
+
+typedef struct {
+  double energy_weight;   /* param key energy_weight (config.cpp:50), default 0 */
+  double stress_weight;   /* param key stress_weight (config.cpp:51), default 0 */
+  int embed_extrap;       /* param key embed_extrap (pot_eam.cpp:71), default 0 */
+  int device;             /* CUDA device ordinal                               */
+  int max_candidates;     /* largest ncand per call (sizes device buffers)     */
+} mz_settings;
+
+/* Copy the database and the potential's fixed structure to the device. */
+mz_status mz_create(const mz_db *db, const mz_pot *pot, const mz_settings *settings, mz_ctx **out);
+void mz_destroy(mz_ctx *ctx);
+
+/* Objective of ncand parameter vectors (params[ncand][ncoeff], host).
+ * obj[ncand] receives the weighted sum of squares that Potential::compute
+ * returns.  Optional outputs (nullable, host):
+ *   errvec [ncand][esize]     the ErrorVec, layout of accumulate_error
+ *                             (potential.cpp:415-491) + the style penalty
+ *                             entries (pot_meam_spline.cpp:274-278 or
+ *                             pot_eam_spline.cpp:211-218)
+ *   forces [ncand][natoms][3] per-atom forces in configuration order
+ *   energy [ncand][ncells]    energy per atom of each cell
+ *   stress [ncand][ncells][6] stress of each cell (xx yy zz xy yz zx)
+ * precision is MZ_FP64 or MZ_MIXED. */
+mz_status mz_objective(mz_ctx *ctx, int ncand, const double *params, int precision, double *obj,
+                       double *errvec, double *forces, double *energy, double *stress);
+
+/* Objective and its gradient with respect to every coefficient
+ * (grad[ncand][ncoeff]), by a hand-written adjoint pass.  The reference has
+ * no gradient; its optimizers take forward differences of compute()
+ * (opt_powell.cpp:348-389). */
+mz_status mz_objective_grad(mz_ctx *ctx, int ncand, const double *params, int precision,
+                            double *obj, double *grad);
+
+/* Embedding densities of every atom for one parameter vector (dens[natoms],
+ * configuration order).  Mirrors fast_compute_densities
+ * (pot_meam_spline.cpp:289-349, pot_eam_spline.cpp:229-268). */
+mz_status mz_densities(mz_ctx *ctx, const double *params, double *dens);
+
+/* Same as mz_objective with device pointers (params, obj, errvec, forces on
+ * the device; any output may be null) enqueued on the context's stream; the
+ * call returns before the work completes.  mz_sync waits for it. */
+mz_status mz_objective_device(mz_ctx *ctx, int ncand, const double *d_params, int precision,
+                              double *d_obj, double *d_errvec, double *d_forces);
+mz_status mz_objective_grad_device(mz_ctx *ctx, int ncand, const double *d_params, int precision,
+                                   double *d_obj, double *d_grad);
+mz_status mz_sync(mz_ctx *ctx);
+/* The context's CUDA stream (a cudaStream_t), for callers that time or order
+ * work against it. */
+void *mz_stream(mz_ctx *ctx);
+
+/* Counters since mz_create: kernel launches issued by this context. */
+mz_status mz_launch_count(const mz_ctx *ctx, int64_t *launches);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MZ_B200_H */

@@ -1,0 +1,56 @@
+// Device-side data layout and shared helpers of the evaluator.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace mzb {
+
+constexpr int MAX_SPLINES = 64;     // splines in one potential (8 types MEAM: 36+8+8+36+8)
+constexpr int BLOCK_SLOTS = 256;    // pair slots (threads) of one atom block
+constexpr int BLOCK_ATOMS = 64;     // atoms of one atom block
+
+// Geometry of one spline, shared by every candidate (knot positions never
+// change: Potential::check_if_similar, pot_list.cpp:165-174).
+struct SplineGeom {
+  double x0, xN, step, invstep;
+  double cut;   // xN * (1 + 1e-8): knot == -1 beyond it (spline.cpp:79)
+  int n;        // knots
+  int toff;     // offset of this spline in a candidate's table
+};
+
+// A candidate's table, per spline at toff: y[n], ypp[n], grad[2]
+// (total tab_stride doubles per candidate).
+
+struct DevDb {
+  int ncells, natoms, nblocks;
+  int64_t npairs;
+  // cells
+  const int *cell_atom0;          // [ncells+1]
+  const double *cell_vol, *cell_w, *cell_ew, *cell_sw, *cell_e0, *cell_s0;
+  // atoms
+  const int *atom_type, *atom_cell;
+  const double *force0;           // [3N]
+  const int *pair_off;            // [N+1]
+  const int *in_off, *in_slot;    // incoming lists
+  // pairs
+  const int *pair_nbr;
+  const double *pair_r, *pair_ux, *pair_uy, *pair_uz;
+  const double *pair_shift;       // [3][Np] phi, rho, f
+  const int *pair_knot;           // packed: (phi+1) | (rho+1) << 8 | (f+1) << 16
+  const float *pair_rf, *pair_uxf, *pair_uyf, *pair_uzf, *pair_shiftf;  // FP32 copies
+  // atom blocks
+  const int *blk_atom0;           // [nblocks+1]
+};
+
+struct DevPot {
+  int style;          // MZ_STYLE_*
+  int ntypes;
+  int nsplines;
+  int tab_stride;     // doubles per candidate table
+  int s_phi, s_rho, s_U, s_f, s_g;  // first spline of each group
+  int embed_extrap;
+  double energy_weight, stress_weight;
+};
+
+}  // namespace mzb

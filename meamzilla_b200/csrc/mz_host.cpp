@@ -1,0 +1,787 @@
+// Host side of the evaluator: potential files, parameter layout, spline
+// arithmetic shared with the device tables, configuration files and the
+// periodic neighbour-list builder.  Built with -ffp-contract=off (see
+// mz_host.hpp).
+#include "mz_host.hpp"
+
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <fstream>
+#include <sstream>
+#include <stdexcept>
+#include <thread>
+
+namespace mzb {
+
+static thread_local std::string g_last_error;
+
+void set_error(const std::string &msg) { g_last_error = msg; }
+
+[[noreturn]] static void fail(int status, const std::string &msg) { throw Failure{status, msg}; }
+
+// ------------------------------------------------------------------ Spline3
+
+void Spline3::set_grid() {
+  // Spline3Eq::set_spline (spline3eq.cpp:354-370)
+  step = (right - left) / (nknots - 1);
+  invstep = 1. / step;
+  x.assign(nknots, 0.0);
+  x[0] = left;
+  x[nknots - 1] = right;
+  for (int i = 1; i < nknots - 1; ++i) x[i] = left + step * i;
+}
+
+int Spline3::ncoeff() const {
+  int n = 0;
+  for (int k = 0; k < nknots; ++k) n += y_fixed[k] ? 0 : 1;
+  for (int i = 0; i < 2; ++i) n += (!grad_fixed[i] && !nat[i]) ? 1 : 0;
+  return n;
+}
+
+int Spline3::knotshift(double r, double *shift) const {
+  // Spline::get_knotshift (spline.cpp:74-99)
+  int knot = -1;
+  if (r < x.back() * (1. + 1.e-8)) {
+    int klo = 0, khi = nknots - 1;
+    while (khi - klo > 1) {
+      int k = (khi + klo) >> 1;
+      if (x[k] > r) khi = k;
+      else klo = k;
+    }
+    knot = klo;
+    double h = x[khi] - x[klo];
+    *shift = (r - x[klo]) / h;
+  }
+  return knot;
+}
+
+void Spline3::refresh(std::vector<double> &ypp) const {
+  // Tridiagonal solve of Spline3Eq::refresh_basis (spline3eq.cpp:192-225):
+  // clamped ends use the end slope, natural ends a zero second derivative.
+  const int n = nknots;
+  std::vector<double> u(n, 0.0);
+  ypp.assign(n, 0.0);
+  if (nat[0]) {
+    ypp[0] = 0;
+  } else {
+    ypp[0] = -0.5;
+    u[0] = (3.0 * invstep) * ((y[1] - y[0]) * invstep - grad[0]);
+  }
+  for (int i = 1; i < n - 1; ++i) {
+    double p = 0.5 * ypp[i - 1] + 2.0;
+    ypp[i] = (-0.5) / p;
+    u[i] = (y[i + 1] - y[i]) * invstep - (y[i] - y[i - 1]) * invstep;
+    u[i] = (6.0 * u[i] * 0.5 * invstep - 0.5 * u[i - 1]) / p;
+  }
+  double qn, un;
+  if (nat[1]) {
+    qn = un = 0.0;
+  } else {
+    qn = 0.5;
+    un = (3.0 * invstep) * (grad[1] - (y[n - 1] - y[n - 2]) * invstep);
+  }
+  ypp[n - 1] = (un - qn * u[n - 2]) / (qn * ypp[n - 2] + 1.0);
+  for (int k = n - 2; k >= 0; --k) ypp[k] = ypp[k] * ypp[k + 1] + u[k];
+}
+
+double Spline3::eval(const std::vector<double> &ypp, double r, double *g) const {
+  // Spline3Eq::splint_comb(double, double*) (spline3eq.h:204-236)
+  if (r < x[0]) {
+    *g = grad[0];
+    return y[0] + grad[0] * (r - x[0]);
+  } else if (r > x[nknots - 1]) {
+    *g = grad[1];
+    return y[nknots - 1] + grad[1] * (r - x[nknots - 1]);
+  }
+  double dr = r - x[0];
+  int k = (dr < 0) ? 0 : int(dr * invstep);
+  if (k >= nknots - 1) k = nknots - 2;
+  double b = (dr - k * step) * invstep, a = 1.0 - b;
+  double p1 = y[k], d21 = ypp[k], p2 = y[k + 1], d22 = ypp[k + 1];
+  *g = (p2 - p1) * invstep + ((3 * (b * b) - 1) * d22 - (3 * (a * a) - 1) * d21) * step / 6.0;
+  return a * p1 + b * p2 + ((a * a * a - a) * d21 + (b * b * b - b) * d22) * (step * step) / 6.0;
+}
+
+// ---------------------------------------------------------------------- Pot
+
+int Pot::nsplines() const {
+  int n = 0;
+  for (auto &g : groups) n += (int)g.size();
+  return n;
+}
+int Pot::spline_index(int group, int alloy) const {
+  int s = 0;
+  for (int g = 0; g < group; ++g) s += (int)groups[g].size();
+  return s + alloy;
+}
+const Spline3 &Pot::spline(int s) const {
+  for (auto &g : groups) {
+    if (s < (int)g.size()) return g[s];
+    s -= (int)g.size();
+  }
+  fail(MZ_ERR_ARG, "spline index out of range");
+}
+Spline3 &Pot::spline(int s) { return const_cast<Spline3 &>(static_cast<const Pot *>(this)->spline(s)); }
+
+int Pot::ncoeff() const {
+  int n = 0;
+  for (auto &g : groups)
+    for (auto &s : g) n += s.ncoeff();
+  return n;
+}
+
+// Coefficient order: Potential::coeff -> PotFns::coeff -> Spline::coeff ->
+// Spline3Eq::bc_coeff (potential.cpp:192-206, pot_fns.cpp:209-218,
+// spline.cpp:105-114, spline3eq.cpp:376-382).
+void Pot::get_coeffs(double *out) const {
+  int i = 0;
+  for (auto &g : groups)
+    for (auto &s : g) {
+      for (int k = 0; k < s.nknots; ++k)
+        if (!s.y_fixed[k]) out[i++] = s.y[k];
+      for (int e = 0; e < 2; ++e)
+        if (!s.grad_fixed[e] && !s.nat[e]) out[i++] = s.grad[e];
+    }
+}
+void Pot::set_coeffs(const double *in) {
+  int i = 0;
+  for (auto &g : groups)
+    for (auto &s : g) {
+      for (int k = 0; k < s.nknots; ++k)
+        if (!s.y_fixed[k]) s.y[k] = in[i++];
+      for (int e = 0; e < 2; ++e)
+        if (!s.grad_fixed[e] && !s.nat[e]) s.grad[e] = in[i++];
+    }
+}
+
+double Pot::max_rcut() const {
+  // radial groups: phi, rho and (MEAM) f
+  double m = 0.0;
+  for (int gi = 0; gi < (int)groups.size(); ++gi) {
+    if (gi == G_U || gi == G_G) continue;
+    for (auto &s : groups[gi]) m = std::max(m, s.x.back());
+  }
+  return m;
+}
+
+static std::vector<std::string> split_lines(const std::string &text) {
+  // Universe::read_file (universe.cpp:145-165): strip CR, drop blank lines.
+  std::vector<std::string> out;
+  std::istringstream is(text);
+  std::string line;
+  while (std::getline(is, line)) {
+    size_t cr = line.find('\r');
+    if (cr != std::string::npos) line.erase(cr, 1);
+    for (char c : line)
+      if (!std::isspace((unsigned char)c)) { out.push_back(line); break; }
+  }
+  return out;
+}
+
+static std::string read_text(const std::string &path) {
+  std::ifstream f(path, std::ios::binary);
+  if (!f) fail(MZ_ERR_IO, "cannot open file: " + path);
+  std::ostringstream ss;
+  ss << f.rdbuf();
+  return ss.str();
+}
+
+void parse_pot(const std::string &text, Pot &pot) {
+  // PotList::init (pot_list.cpp:84-142) for one #P block.
+  std::vector<std::string> L = split_lines(text);
+  if (L.size() < 3) fail(MZ_ERR_FORMAT, "potential file too short");
+  size_t ln = 0;
+  pot.comment = L[ln++];
+  if (L[ln].substr(0, 2) != "#T") fail(MZ_ERR_FORMAT, "potential type line (#T ...) missing");
+  {
+    std::istringstream is(L[ln++]);
+    std::string lab;
+    is >> lab >> pot.type_name >> pot.ntypes;
+    if (is.fail()) fail(MZ_ERR_FORMAT, "pot type line (#T ...) is incorrect");
+  }
+  if (pot.ntypes < 1 || pot.ntypes > 8) fail(MZ_ERR_FORMAT, "number of atom types must be 1..8");
+  int nt = pot.ntypes, npair = nt * (nt + 1) / 2;
+  std::vector<int> nalloy;
+  if (pot.type_name == "meam/spline") {
+    pot.style = MZ_STYLE_MEAM_SPLINE;
+    nalloy = {npair, nt, nt, npair, nt};
+  } else if (pot.type_name == "eam/spline") {
+    pot.style = MZ_STYLE_EAM_SPLINE;
+    nalloy = {npair, nt, nt};
+  } else {
+    fail(MZ_ERR_UNSUPPORTED, "potential style \"" + pot.type_name +
+                                 "\" is not implemented (eam/spline, meam/spline)");
+  }
+  pot.ngroups = (int)nalloy.size();
+  if (ln >= L.size() || L[ln++].substr(0, 2) != "#P") fail(MZ_ERR_FORMAT, "potential line (#P ...) missing");
+  pot.groups.assign(pot.ngroups, {});
+  for (int g = 0; g < pot.ngroups; ++g) {
+    for (int a = 0; a < nalloy[g]; ++a) {
+      // PotFns::read_pot_fns (pot_fns.cpp:439-465) + Spline3Eq::read_basis
+      if (ln >= L.size() || L[ln].substr(0, 2) != "#B") fail(MZ_ERR_FORMAT, "potential line (#B ...) missing");
+      {
+        std::istringstream is(L[ln++]);
+        std::string lab, basis;
+        is >> lab >> basis;
+        if (is.fail()) fail(MZ_ERR_FORMAT, "incorrect basis definition, use format (#B <basis type>)");
+        if (basis != "spline3eq") fail(MZ_ERR_UNSUPPORTED, "basis \"" + basis + "\" is not implemented (spline3eq)");
+      }
+      Spline3 s;
+      if (ln + 2 >= L.size()) fail(MZ_ERR_FORMAT, "unexpected end of potential file");
+      {
+        std::istringstream is(L[ln++]);
+        is >> s.left >> s.right >> s.nknots;
+        if (is.fail()) fail(MZ_ERR_FORMAT, "incorrect spline definition, use format (<left x> <right x> <nknots>)");
+      }
+      if (s.nknots < 3 || s.nknots > 64) fail(MZ_ERR_FORMAT, "spline knot count must be 3..64");
+      {
+        std::istringstream is(L[ln++]);
+        int lc, rc;
+        is >> lc >> rc;
+        if (is.fail()) fail(MZ_ERR_FORMAT, "incorrect boundary condition constraint line");
+        int c[2] = {lc, rc};
+        for (int e = 0; e < 2; ++e) {
+          if (c[e] == -1) s.nat[e] = 1;
+          else if (c[e] == 0) s.grad_fixed[e] = 0;
+          else if (c[e] == 1) s.grad_fixed[e] = 1;
+          else fail(MZ_ERR_FORMAT, "boundary condition constraint line has an incorrect constraint value");
+        }
+      }
+      {
+        std::istringstream is(L[ln++]);
+        is >> s.grad[0] >> s.grad[1];
+        if (is.fail()) fail(MZ_ERR_FORMAT, "incorrect boundary condition line, format is (<left grad> <right grad>)");
+      }
+      s.y.assign(s.nknots, 0.0);
+      s.y_fixed.assign(s.nknots, 0);
+      for (int k = 0; k < s.nknots; ++k) {
+        if (ln >= L.size()) fail(MZ_ERR_FORMAT, "unexpected end of potential file");
+        std::istringstream is(L[ln++]);
+        is >> s.y_fixed[k] >> s.y[k];
+        if (is.fail()) fail(MZ_ERR_FORMAT, "incorrect spline knot line, format is (<is y fixed?> <y-value>)");
+      }
+      s.set_grid();
+      pot.groups[g].push_back(std::move(s));
+    }
+  }
+}
+
+std::string write_pot_text(const Pot &pot) {
+  // Potential::write_pots (potential.cpp:721-732) + Spline3Eq::write_basis_fn
+  // (spline3eq.cpp:248-273): scientific, 15 digits.
+  std::ostringstream os;
+  os << pot.comment << "\n#T " << pot.type_name << " " << pot.ntypes << "\n#P\n";
+  char buf[128];
+  for (auto &g : pot.groups)
+    for (auto &s : g) {
+      os << "#B spline3eq\n";
+      std::snprintf(buf, sizeof buf, "%.15e %.15e %d\n", s.x[0], s.x[s.nknots - 1], s.nknots);
+      os << buf;
+      int c[2];
+      for (int e = 0; e < 2; ++e) c[e] = s.nat[e] ? -1 : s.grad_fixed[e];
+      os << c[0] << " " << c[1] << "\n";
+      std::snprintf(buf, sizeof buf, "%.15e %.15e\n", s.grad[0], s.grad[1]);
+      os << buf;
+      for (int k = 0; k < s.nknots; ++k) {
+        std::snprintf(buf, sizeof buf, "%d %.15e\n", s.y_fixed[k], s.y[k]);
+        os << buf;
+      }
+      os << "\n";
+    }
+  os << "\n";
+  return os.str();
+}
+
+// ------------------------------------------------------------ configuration
+
+void read_config_file(const std::string &path, int ntypes, std::vector<int> &cell_natoms,
+                      std::vector<double> &lattice, std::vector<double> &e0,
+                      std::vector<double> &s0, std::vector<double> &w, std::vector<double> &ew,
+                      std::vector<double> &sw, std::vector<int> &types, std::vector<double> &pos,
+                      std::vector<double> &f0) {
+  // Cell::read_cell (cell.cpp:39-136), cell after cell until the end.
+  std::vector<std::string> L = split_lines(read_text(path));
+  size_t ln = 0, end = L.size();
+  int cell = 0;
+  auto err = [&](const std::string &m) {
+    fail(MZ_ERR_FORMAT, m + " - cell=" + std::to_string(cell) + " (file=" + path + ")");
+  };
+  while (ln < end) {
+    std::istringstream is(L[ln]);
+    std::string lab;
+    int n = 0, useforce = 1;
+    is >> lab >> n >> useforce;
+    if (lab != "#N") err("ERROR: number line (#N ...) is missing");
+    if (is.fail()) err("ERROR: number line (#N ...) is incorrect");
+    if (ln + 1 == end) err("ERROR: unexpected end of config file");
+    double a[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0}, E = 0, S[6] = {0, 0, 0, 0, 0, 0}, W = 1, EW = 1, SW = 1;
+    while (L[++ln].substr(0, 2) != "#F") {
+      if (ln + 1 == end) err("ERROR: unexpected end of config file");
+      std::istringstream hs(L[ln]);
+      hs >> lab;
+      if (lab == "#X") { hs >> a[0] >> a[1] >> a[2]; if (hs.fail()) err("ERROR: box_x vector (#X ...) incorrect"); }
+      else if (lab == "#Y") { hs >> a[3] >> a[4] >> a[5]; if (hs.fail()) err("ERROR: box_y vector (#Y ...) incorrect"); }
+      else if (lab == "#Z") { hs >> a[6] >> a[7] >> a[8]; if (hs.fail()) err("ERROR: box_z vector (#Z ...) incorrect"); }
+      else if (lab == "#E") { hs >> E; if (hs.fail()) err("ERROR: energy (#E ...) incorrect"); }
+      else if (lab == "#S") {
+        for (int k = 0; k < 6; ++k) hs >> S[k];
+        if (hs.fail()) err("ERROR: stress tensor (#S ...) incorrect");
+      } else if (lab == "#W") { hs >> W; if (hs.fail()) err("ERROR: configuration weight (#W ...) incorrect"); }
+      else if (lab == "#EW") { hs >> EW; if (hs.fail()) err("ERROR: configuration energy weight (#EW ...) incorrect"); }
+      else if (lab == "#SW") { hs >> SW; if (hs.fail()) err("ERROR: configuration stress weight (#SW ...) incorrect"); }
+    }
+    if (ln + n >= end) err("ERROR: unexpected end of config file");
+    cell_natoms.push_back(n);
+    lattice.insert(lattice.end(), a, a + 9);
+    e0.push_back(E);
+    s0.insert(s0.end(), S, S + 6);
+    w.push_back(W);
+    ew.push_back(EW);
+    sw.push_back(SW);
+    for (int i = 0; i < n; ++i) {
+      const std::string &al = L[++ln];
+      if (al[0] == '#') err("ERROR: too few atoms");
+      std::istringstream as(al);
+      int t;
+      double p[3], f[3];
+      as >> t >> p[0] >> p[1] >> p[2] >> f[0] >> f[1] >> f[2];
+      if (as.fail()) err("ERROR: atom line incorrect - atom=" + std::to_string(i));
+      if (t < 0 || t >= ntypes) err("ERROR: incorrect atom type specified - atom=" + std::to_string(i));
+      types.push_back(t);
+      pos.insert(pos.end(), p, p + 3);
+      f0.insert(f0.end(), f, f + 3);
+    }
+    ++ln;
+    if (ln < end && L[ln].substr(0, 2) != "#N") err("ERROR: too many atoms");
+    ++cell;
+  }
+}
+
+// --------------------------------------------------------------- neighbours
+
+namespace {
+struct V3 {
+  double x, y, z;
+};
+inline double dot(const V3 &a, const V3 &b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+inline V3 cross(const V3 &a, const V3 &b) {
+  return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
+}
+inline double mag(const V3 &v) { return std::sqrt(dot(v, v)); }
+
+struct CellPairs {
+  std::vector<int> nbr;
+  std::vector<double> r, u, shift;
+  std::vector<int8_t> knot;
+  std::vector<int> row_len;
+  int status = MZ_OK;
+  std::string msg;
+};
+}  // namespace
+
+void build_db(const mz_cells_desc &c, const Pot &pot, Db &db) {
+  if (c.ncells <= 0 || c.natoms <= 0 || !c.cell_natoms || !c.cell_lattice || !c.atom_type || !c.atom_pos)
+    fail(MZ_ERR_ARG, "empty or incomplete cell description");
+  const bool meam = pot.style == MZ_STYLE_MEAM_SPLINE;
+  db.ncells = c.ncells;
+  db.natoms = c.natoms;
+  db.cell_atom0.assign(c.ncells + 1, 0);
+  for (int i = 0; i < c.ncells; ++i) {
+    if (c.cell_natoms[i] <= 0) fail(MZ_ERR_FORMAT, "cell with no atoms: cell=" + std::to_string(i));
+    db.cell_atom0[i + 1] = db.cell_atom0[i] + c.cell_natoms[i];
+  }
+  if (db.cell_atom0[c.ncells] != c.natoms) fail(MZ_ERR_ARG, "cell atom counts do not sum to natoms");
+  auto opt = [&](const double *p, int i, double d) { return p ? p[i] : d; };
+  db.cell_vol.resize(c.ncells);
+  db.cell_weight.resize(c.ncells);
+  db.cell_eweight.resize(c.ncells);
+  db.cell_sweight.resize(c.ncells);
+  db.cell_energy0.resize(c.ncells);
+  db.cell_stress0.assign(6 * (size_t)c.ncells, 0.0);
+  db.cell_lattice.assign(c.cell_lattice, c.cell_lattice + 9 * (size_t)c.ncells);
+  for (int i = 0; i < c.ncells; ++i) {
+    db.cell_weight[i] = opt(c.cell_weight, i, 1.0);
+    db.cell_eweight[i] = opt(c.cell_eweight, i, 1.0);
+    db.cell_sweight[i] = opt(c.cell_sweight, i, 1.0);
+    db.cell_energy0[i] = opt(c.cell_energy0, i, 0.0);
+    for (int k = 0; k < 6; ++k) db.cell_stress0[6 * i + k] = c.cell_stress0 ? c.cell_stress0[6 * i + k] : 0.0;
+  }
+  db.atom_type.assign(c.atom_type, c.atom_type + c.natoms);
+  db.atom_cell.resize(c.natoms);
+  db.atom_pos.assign(c.atom_pos, c.atom_pos + 3 * (size_t)c.natoms);
+  if (c.atom_force0) db.atom_force0.assign(c.atom_force0, c.atom_force0 + 3 * (size_t)c.natoms);
+  else db.atom_force0.assign(3 * (size_t)c.natoms, 0.0);
+  for (int i = 0; i < c.ncells; ++i)
+    for (int a = db.cell_atom0[i]; a < db.cell_atom0[i + 1]; ++a) {
+      if (db.atom_type[a] < 0 || db.atom_type[a] >= pot.ntypes)
+        fail(MZ_ERR_FORMAT, "incorrect atom type specified - cell=" + std::to_string(i));
+      db.atom_cell[a] = i;
+    }
+
+  const double max_rcut = pot.max_rcut();
+  const int sphi0 = pot.spline_index(G_PHI, 0), srho0 = pot.spline_index(G_RHO, 0);
+  const int sf0 = meam ? pot.spline_index(G_F, 0) : -1;
+
+  std::vector<CellPairs> per(c.ncells);
+  std::atomic<int> next(0);
+  auto work = [&]() {
+    for (;;) {
+      int ci = next.fetch_add(1);
+      if (ci >= c.ncells) return;
+      CellPairs &out = per[ci];
+      const double *A = c.cell_lattice + 9 * (size_t)ci;
+      V3 a0{A[0], A[1], A[2]}, a1{A[3], A[4], A[5]}, a2{A[6], A[7], A[8]};
+      // Cell::compute_vol (cell.cpp:191-194) and Cell::find_scale (cell.cpp:158-170)
+      double vol = std::abs(dot(a0, cross(a1, a2)));
+      db.cell_vol[ci] = vol;
+      double ihx = mag(cross(a1, a2)) / vol, ihy = mag(cross(a2, a0)) / vol, ihz = mag(cross(a0, a1)) / vol;
+      double sx = int(std::ceil(max_rcut * ihx)), sy = int(std::ceil(max_rcut * ihy)),
+             sz = int(std::ceil(max_rcut * ihz));
+      if (!(sx > 0 && sy > 0 && sz > 0)) {
+        out.status = MZ_ERR_RANGE;
+        out.msg = "ERROR: Cell #" + std::to_string(ci) + " is too small or potential is too big";
+        return;
+      }
+      const int a_lo = db.cell_atom0[ci], na = db.cell_atom0[ci + 1] - a_lo;
+      // Config::find_pairs (config.cpp:143-234), double counted (j0 = 0)
+      for (int i = 0; i < na && out.status == MZ_OK; ++i) {
+        const double *pi = c.atom_pos + 3 * (size_t)(a_lo + i);
+        const int ti = c.atom_type[a_lo + i];
+        int row = 0;
+        for (int j = 0; j < na; ++j) {
+          const double *pj = c.atom_pos + 3 * (size_t)(a_lo + j);
+          const int tj = c.atom_type[a_lo + j];
+          for (int ix = -sx; ix <= sx; ++ix)
+            for (int iy = -sy; iy <= sy; ++iy)
+              for (int iz = -sz; iz <= sz; ++iz) {
+                if (i == j && ix == 0 && iy == 0 && iz == 0) continue;
+                V3 d;
+                d.x = pj[0] + ix * a0.x + iy * a1.x + iz * a2.x - pi[0];
+                d.y = pj[1] + ix * a0.y + iy * a1.y + iz * a2.y - pi[1];
+                d.z = pj[2] + ix * a0.z + iy * a1.z + iz * a2.z - pi[2];
+                double r = mag(d);
+                if (r >= max_rcut) continue;
+                // Pair::setup_pair (pair.cpp:35-42)
+                double rr = mag(d);
+                V3 u{d.x / rr, d.y / rr, d.z / rr};
+                // check_pair (pair_meam_spline.cpp:50-99 / pair_eam_spline.cpp:50-86)
+                int sidx[3] = {sphi0 + pot.idx_pair_ij(ti, tj), srho0 + tj,
+                               meam ? sf0 + pot.idx_pair_ij(ti, tj) : -1};
+                const char *nm[3] = {"phi", "rho", "f"};
+                int kn[3] = {-1, -1, -1};
+                double sh[3] = {0, 0, 0};
+                bool bad = false;
+                for (int q = 0; q < (meam ? 3 : 2); ++q) {
+                  const Spline3 &sp = pot.spline(sidx[q]);
+                  if (rr < sp.x[0]) {
+                    char buf[256];
+                    std::snprintf(buf, sizeof buf,
+                                  "ERROR: Pair distance too short for potential (r=%g, pot=%s[%d]) - cell=%d atom=%d neigh=%d",
+                                  rr, nm[q], q == 1 ? tj : pot.idx_pair_ij(ti, tj), ci, i, j);
+                    out.status = MZ_ERR_RANGE;
+                    out.msg = buf;
+                    bad = true;
+                    break;
+                  }
+                  kn[q] = sp.knotshift(rr, &sh[q]);
+                }
+                if (bad) return;
+                if (kn[0] == -1 && kn[1] == -1 && kn[2] == -1) continue;
+                out.nbr.push_back(a_lo + j);
+                out.r.push_back(rr);
+                out.u.push_back(u.x);
+                out.u.push_back(u.y);
+                out.u.push_back(u.z);
+                for (int q = 0; q < 3; ++q) {
+                  out.knot.push_back((int8_t)kn[q]);
+                  out.shift.push_back(kn[q] >= 0 ? sh[q] : 0.0);
+                }
+                ++row;
+              }
+        }
+        out.row_len.push_back(row);
+      }
+    }
+  };
+  unsigned nth = std::max(1u, std::min(64u, std::thread::hardware_concurrency()));
+  std::vector<std::thread> th;
+  for (unsigned t = 0; t < nth; ++t) th.emplace_back(work);
+  for (auto &t : th) t.join();
+  for (int ci = 0; ci < c.ncells; ++ci)
+    if (per[ci].status != MZ_OK) fail(per[ci].status, per[ci].msg);
+
+  // Concatenate rows in atom order.
+  db.pair_off.assign(c.natoms + 1, 0);
+  int64_t np = 0;
+  db.max_row = 0;
+  db.ntriplets = 0;
+  for (int ci = 0; ci < c.ncells; ++ci) {
+    const int a_lo = db.cell_atom0[ci];
+    for (size_t i = 0; i < per[ci].row_len.size(); ++i) {
+      int n = per[ci].row_len[i];
+      db.pair_off[a_lo + i + 1] = db.pair_off[a_lo + i] + n;
+      db.max_row = std::max(db.max_row, n);
+      if (meam) db.ntriplets += (int64_t)n * (n - 1) / 2;
+    }
+    np += (int64_t)per[ci].nbr.size();
+  }
+  db.npairs = np;
+  db.pair_nbr.resize(np);
+  db.pair_r.resize(np);
+  db.pair_u.resize(3 * np);
+  db.pair_knot.resize(3 * np);
+  db.pair_shift.resize(3 * np);
+  int64_t o = 0;
+  for (int ci = 0; ci < c.ncells; ++ci) {
+    CellPairs &p = per[ci];
+    size_t n = p.nbr.size();
+    std::copy(p.nbr.begin(), p.nbr.end(), db.pair_nbr.begin() + o);
+    std::copy(p.r.begin(), p.r.end(), db.pair_r.begin() + o);
+    std::copy(p.u.begin(), p.u.end(), db.pair_u.begin() + 3 * o);
+    std::copy(p.knot.begin(), p.knot.end(), db.pair_knot.begin() + 3 * o);
+    std::copy(p.shift.begin(), p.shift.end(), db.pair_shift.begin() + 3 * o);
+    o += (int64_t)n;
+    CellPairs().nbr.swap(p.nbr);
+  }
+  // Incoming lists (counting sort by neighbour, slot order kept).
+  db.in_off.assign(c.natoms + 1, 0);
+  for (int64_t s = 0; s < np; ++s) db.in_off[db.pair_nbr[s] + 1]++;
+  for (int a = 0; a < c.natoms; ++a) db.in_off[a + 1] += db.in_off[a];
+  db.in_slot.resize(np);
+  std::vector<int64_t> fill(db.in_off.begin(), db.in_off.end() - 1);
+  for (int64_t s = 0; s < np; ++s) db.in_slot[fill[db.pair_nbr[s]]++] = s;
+}
+
+}  // namespace mzb
+
+// ------------------------------------------------------------------ C ABI
+
+using namespace mzb;
+
+template <class F>
+static mz_status guarded(F &&f) {
+  try {
+    f();
+    set_error("");
+    return MZ_OK;
+  } catch (const Failure &e) {
+    set_error(e.msg);
+    return e.status;
+  } catch (const std::bad_alloc &) {
+    set_error("host allocation failed");
+    return MZ_ERR_NOMEM;
+  } catch (const std::exception &e) {
+    set_error(e.what());
+    return MZ_ERR_ARG;
+  }
+}
+
+extern "C" {
+
+const char *mz_last_error(void) { return g_last_error.c_str(); }
+
+mz_status mz_pot_parse(const char *text, mz_pot **out) {
+  return guarded([&] {
+    if (!text || !out) fail(MZ_ERR_ARG, "null argument");
+    auto *p = new mz_pot;
+    try {
+      parse_pot(text, p->pot);
+    } catch (...) {
+      delete p;
+      throw;
+    }
+    *out = p;
+  });
+}
+
+mz_status mz_pot_read(const char *path, mz_pot **out) {
+  return guarded([&] {
+    if (!path || !out) fail(MZ_ERR_ARG, "null argument");
+    std::string t = read_text(path);
+    auto *p = new mz_pot;
+    try {
+      parse_pot(t, p->pot);
+    } catch (...) {
+      delete p;
+      throw;
+    }
+    *out = p;
+  });
+}
+
+void mz_pot_free(mz_pot *pot) { delete pot; }
+
+mz_status mz_pot_info(const mz_pot *pot, int *style, int *ntypes, int *nsplines) {
+  return guarded([&] {
+    if (!pot) fail(MZ_ERR_ARG, "null potential");
+    if (style) *style = pot->pot.style;
+    if (ntypes) *ntypes = pot->pot.ntypes;
+    if (nsplines) *nsplines = pot->pot.nsplines();
+  });
+}
+
+mz_status mz_pot_ncoeff(const mz_pot *pot, int *n) {
+  return guarded([&] {
+    if (!pot || !n) fail(MZ_ERR_ARG, "null argument");
+    *n = pot->pot.ncoeff();
+  });
+}
+
+mz_status mz_pot_get_coeffs(const mz_pot *pot, double *x) {
+  return guarded([&] {
+    if (!pot || !x) fail(MZ_ERR_ARG, "null argument");
+    pot->pot.get_coeffs(x);
+  });
+}
+
+mz_status mz_pot_set_coeffs(mz_pot *pot, const double *x) {
+  return guarded([&] {
+    if (!pot || !x) fail(MZ_ERR_ARG, "null argument");
+    pot->pot.set_coeffs(x);
+  });
+}
+
+mz_status mz_pot_write(const mz_pot *pot, const char *path) {
+  return guarded([&] {
+    if (!pot || !path) fail(MZ_ERR_ARG, "null argument");
+    std::ofstream f(path);
+    if (!f) fail(MZ_ERR_IO, std::string("cannot write ") + path);
+    f << write_pot_text(pot->pot);
+  });
+}
+
+mz_status mz_pot_spline_eval(const mz_pot *pot, int s, double x, double *val, double *grad) {
+  return guarded([&] {
+    if (!pot || !val || !grad) fail(MZ_ERR_ARG, "null argument");
+    if (s < 0 || s >= pot->pot.nsplines()) fail(MZ_ERR_ARG, "spline index out of range");
+    const Spline3 &sp = pot->pot.spline(s);
+    std::vector<double> ypp;
+    sp.refresh(ypp);
+    *val = sp.eval(ypp, x, grad);
+  });
+}
+
+mz_status mz_db_build(const mz_cells_desc *cells, const mz_pot *pot, mz_db **out) {
+  return guarded([&] {
+    if (!cells || !pot || !out) fail(MZ_ERR_ARG, "null argument");
+    auto *d = new mz_db;
+    try {
+      build_db(*cells, pot->pot, d->db);
+    } catch (...) {
+      delete d;
+      throw;
+    }
+    *out = d;
+  });
+}
+
+mz_status mz_db_read(const char *path, const mz_pot *pot, mz_db **out) {
+  return guarded([&] {
+    if (!path || !pot || !out) fail(MZ_ERR_ARG, "null argument");
+    std::vector<int> cn, types;
+    std::vector<double> lat, e0, s0, w, ew, sw, pos, f0;
+    read_config_file(path, pot->pot.ntypes, cn, lat, e0, s0, w, ew, sw, types, pos, f0);
+    mz_cells_desc c;
+    c.ncells = (int)cn.size();
+    c.natoms = (int)types.size();
+    c.cell_natoms = cn.data();
+    c.cell_lattice = lat.data();
+    c.cell_energy0 = e0.data();
+    c.cell_stress0 = s0.data();
+    c.cell_weight = w.data();
+    c.cell_eweight = ew.data();
+    c.cell_sweight = sw.data();
+    c.atom_type = types.data();
+    c.atom_pos = pos.data();
+    c.atom_force0 = f0.data();
+    auto *d = new mz_db;
+    try {
+      build_db(c, pot->pot, d->db);
+    } catch (...) {
+      delete d;
+      throw;
+    }
+    *out = d;
+  });
+}
+
+void mz_db_free(mz_db *db) { delete db; }
+
+mz_status mz_db_info(const mz_db *db, mz_db_stats *st) {
+  return guarded([&] {
+    if (!db || !st) fail(MZ_ERR_ARG, "null argument");
+    st->ncells = db->db.ncells;
+    st->natoms = db->db.natoms;
+    st->npairs = db->db.npairs;
+    st->ntriplets = db->db.ntriplets;
+    st->max_row = db->db.max_row;
+    st->esize = 7 * db->db.ncells + 3 * db->db.natoms + db->db.ncells;  // + style penalties
+  });
+}
+
+mz_status mz_db_get_view(const mz_db *dbh, mz_db_view *v) {
+  return guarded([&] {
+    if (!dbh || !v) fail(MZ_ERR_ARG, "null argument");
+    const Db &d = dbh->db;
+    v->ncells = d.ncells;
+    v->natoms = d.natoms;
+    v->npairs = d.npairs;
+    v->cell_atom0 = d.cell_atom0.data();
+    v->cell_vol = d.cell_vol.data();
+    v->cell_weight = d.cell_weight.data();
+    v->cell_eweight = d.cell_eweight.data();
+    v->cell_sweight = d.cell_sweight.data();
+    v->cell_energy0 = d.cell_energy0.data();
+    v->cell_stress0 = d.cell_stress0.data();
+    v->cell_lattice = d.cell_lattice.data();
+    v->atom_type = d.atom_type.data();
+    v->atom_cell = d.atom_cell.data();
+    v->atom_pos = d.atom_pos.data();
+    v->atom_force0 = d.atom_force0.data();
+    v->pair_off = d.pair_off.data();
+    v->pair_nbr = d.pair_nbr.data();
+    v->pair_r = d.pair_r.data();
+    v->pair_u = d.pair_u.data();
+    v->pair_knot = d.pair_knot.data();
+    v->pair_shift = d.pair_shift.data();
+    v->in_off = d.in_off.data();
+    v->in_slot = d.in_slot.data();
+  });
+}
+
+mz_status mz_pot_get_spline(const mz_pot *pot, int s, mz_spline_view *v) {
+  return guarded([&] {
+    if (!pot || !v) fail(MZ_ERR_ARG, "null argument");
+    if (s < 0 || s >= pot->pot.nsplines()) fail(MZ_ERR_ARG, "spline index out of range");
+    int g = 0, a = s;
+    while (a >= (int)pot->pot.groups[g].size()) a -= (int)pot->pot.groups[g++].size();
+    const Spline3 &sp = pot->pot.spline(s);
+    v->group = g;
+    v->alloy = a;
+    v->nknots = sp.nknots;
+    v->left = sp.left;
+    v->right = sp.right;
+    v->nat[0] = sp.nat[0];
+    v->nat[1] = sp.nat[1];
+    v->grad_fixed[0] = sp.grad_fixed[0];
+    v->grad_fixed[1] = sp.grad_fixed[1];
+    v->grad[0] = sp.grad[0];
+    v->grad[1] = sp.grad[1];
+    v->y_fixed = sp.y_fixed.data();
+    v->y = sp.y.data();
+  });
+}
+
+mz_status mz_db_set_targets(mz_db *db, const double *e0, const double *s0, const double *f0) {
+  return guarded([&] {
+    if (!db) fail(MZ_ERR_ARG, "null database");
+    if (e0) std::copy(e0, e0 + db->db.ncells, db->db.cell_energy0.begin());
+    if (s0) std::copy(s0, s0 + 6 * (size_t)db->db.ncells, db->db.cell_stress0.begin());
+    if (f0) std::copy(f0, f0 + 3 * (size_t)db->db.natoms, db->db.atom_force0.begin());
+  });
+}
+
+}  // extern "C"

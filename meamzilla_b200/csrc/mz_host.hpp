@@ -1,0 +1,122 @@
+// Host-side model of the potential and the configuration database.
+//
+// These are the B200 evaluator's own data structures; the arithmetic that
+// fixes parity with the reference (knot grid, knot/shift bisection, second
+// derivative refresh, periodic image search) is restated here from the
+// reference files cited at each function.  Compile this code with
+// -ffp-contract=off: the neighbour distances and shifts must round exactly
+// as the reference's do, so that the lists are identical.
+#pragma once
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "mz_b200.h"
+
+namespace mzb {
+
+struct Spline3 {
+  // Definition read from the file (spline3eq.cpp:54-106).
+  double left = 0, right = 0;
+  int nknots = 0;
+  int nat[2] = {0, 0};         // natural end (bc -1)
+  int grad_fixed[2] = {1, 1};  // end slope fixed (bc 1) ; bc 0 -> free
+  double grad[2] = {0, 0};
+  std::vector<int> y_fixed;
+  std::vector<double> y;
+  // Knot grid exactly as Spline3Eq::set_spline (spline3eq.cpp:354-370).
+  double step = 0, invstep = 0;
+  std::vector<double> x;
+
+  void set_grid();
+  int ncoeff() const;
+  // Bisection knot + shift (Spline::get_knotshift, spline.cpp:74-99); -1 if
+  // r lies beyond the last knot by more than the reference's 1e-8 slack.
+  int knotshift(double r, double *shift) const;
+  // Second derivatives (Spline3Eq::refresh_basis, spline3eq.cpp:192-225).
+  void refresh(std::vector<double> &ypp) const;
+  // Value + slope at x with linear extrapolation (spline3eq.h:204-236).
+  double eval(const std::vector<double> &ypp, double xv, double *g) const;
+};
+
+// Function groups in file order.  MEAM: phi(Pair_ij) rho(Pair_j) U(Atom/Pair_i)
+// f(Pair_ij) g(Triplet_i) (pot_meam.cpp:31-47, pot_eam.cpp:30-46,
+// pot_pair.cpp:25-37).  EAM: the first three.
+enum Group { G_PHI = 0, G_RHO = 1, G_U = 2, G_F = 3, G_G = 4 };
+
+struct Pot {
+  int style = MZ_STYLE_MEAM_SPLINE;
+  int ntypes = 1;
+  std::string comment, type_name;
+  int ngroups = 5;
+  std::vector<std::vector<Spline3>> groups;  // [group][alloy index]
+
+  // Flattened spline list (group-major) and the coefficient layout.
+  int nsplines() const;
+  const Spline3 &spline(int s) const;
+  Spline3 &spline(int s);
+  int spline_index(int group, int alloy) const;
+  int ncoeff() const;
+  void get_coeffs(double *out) const;
+  void set_coeffs(const double *in);
+  double max_rcut() const;  // Potential::get_max_rcut (potential.cpp:72-82), radial groups
+
+  // alloy indices (pot_fns.cpp:240-296)
+  int idx_pair_ij(int ti, int tj) const {
+    return (ti <= tj) ? ti * ntypes + tj - (ti * (ti + 1)) / 2 : tj * ntypes + ti - (tj * (tj + 1)) / 2;
+  }
+};
+
+// Configuration database in CSR / structure-of-arrays form, atoms in
+// configuration order.  Each atom's neighbour row is the reference's pair
+// list for that atom in the same order (config.cpp:186-228).
+struct Db {
+  int ncells = 0, natoms = 0;
+  int64_t npairs = 0, ntriplets = 0;
+  int max_row = 0;
+  // cells
+  std::vector<int> cell_atom0;     // [ncells+1]
+  std::vector<double> cell_vol, cell_weight, cell_eweight, cell_sweight, cell_energy0;
+  std::vector<double> cell_stress0;  // [6*ncells]
+  std::vector<double> cell_lattice;  // [9*ncells]
+  // atoms
+  std::vector<int> atom_type, atom_cell;
+  std::vector<double> atom_pos, atom_force0;  // [3N]
+  std::vector<int64_t> pair_off;              // [N+1]
+  // pairs
+  std::vector<int> pair_nbr;                  // neighbour atom index
+  std::vector<double> pair_r, pair_u;         // r, unit vector [3Np]
+  std::vector<int8_t> pair_knot;              // [3Np] phi, rho, f (f: MEAM only)
+  std::vector<double> pair_shift;             // [3Np]
+  // incoming lists: for every atom, the pair slots whose neighbour it is
+  std::vector<int64_t> in_off;                // [N+1]
+  std::vector<int64_t> in_slot;               // [Np]
+};
+
+// Build lists (throws std::runtime_error with an mz status prefix).
+void build_db(const mz_cells_desc &cells, const Pot &pot, Db &db);
+void parse_pot(const std::string &text, Pot &pot);
+std::string write_pot_text(const Pot &pot);
+void read_config_file(const std::string &path, int ntypes, std::vector<int> &cell_natoms,
+                      std::vector<double> &lattice, std::vector<double> &e0,
+                      std::vector<double> &s0, std::vector<double> &w, std::vector<double> &ew,
+                      std::vector<double> &sw, std::vector<int> &types, std::vector<double> &pos,
+                      std::vector<double> &f0);
+
+struct Failure {
+  int status;
+  std::string msg;
+};
+
+void set_error(const std::string &msg);
+
+}  // namespace mzb
+
+// Opaque handles of the C ABI.
+struct mz_pot {
+  mzb::Pot pot;
+};
+struct mz_db {
+  mzb::Db db;
+};

@@ -1,0 +1,365 @@
+/* TEST ORACLE -- see mz_oracle.h.  CPU restatement of the reference
+ * objective used only to check the CUDA evaluator.  Compiled with
+ * -ffp-contract=off so its arithmetic rounds like the reference's parity
+ * build (oracle/Makefile). */
+#include "mz_oracle.h"
+
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+#define DUMMY_WEIGHT 100.0 /* PotPair::DUMMY_WEIGHT, pot_pair.h:39 */
+
+typedef struct {
+  int n;
+  double step, invstep;
+  double *x, *y, *ypp;
+  double grad[2];
+  int nat[2];
+} sp_t;
+
+/* Spline3Eq::set_spline (spline3eq.cpp:354-370) + coefficients in
+ * Spline::coeff / Spline3Eq::bc_coeff order (spline.cpp:105-114,
+ * spline3eq.cpp:376-382) + Spline3Eq::refresh_basis (spline3eq.cpp:192-225). */
+static void sp_setup(sp_t *s, const mzo_spline *in, const double *coeffs, int *ci) {
+  int n = in->nknots, i, k;
+  s->n = n;
+  s->x = (double *)malloc(sizeof(double) * n);
+  s->y = (double *)malloc(sizeof(double) * n);
+  s->ypp = (double *)malloc(sizeof(double) * n);
+  s->step = (in->right - in->left) / (n - 1);
+  s->invstep = 1. / s->step;
+  s->x[0] = in->left;
+  s->x[n - 1] = in->right;
+  for (i = 1; i < n - 1; ++i) s->x[i] = in->left + s->step * i;
+  for (k = 0; k < n; ++k) s->y[k] = in->y[k];
+  s->grad[0] = in->grad[0];
+  s->grad[1] = in->grad[1];
+  s->nat[0] = in->nat[0];
+  s->nat[1] = in->nat[1];
+  if (coeffs) {
+    for (k = 0; k < n; ++k)
+      if (!in->y_fixed[k]) s->y[k] = coeffs[(*ci)++];
+    for (i = 0; i < 2; ++i)
+      if (!in->grad_fixed[i] && !in->nat[i]) s->grad[i] = coeffs[(*ci)++];
+  }
+  {
+    double p, qn, un;
+    double *u = (double *)calloc(n, sizeof(double));
+    double *ypp = s->ypp, *y = s->y, invstep = s->invstep;
+    if (s->nat[0]) {
+      ypp[0] = 0;
+    } else {
+      ypp[0] = -0.5;
+      u[0] = (3.0 * invstep) * ((y[1] - y[0]) * invstep - s->grad[0]);
+    }
+    for (i = 1; i < n - 1; ++i) {
+      p = 0.5 * ypp[i - 1] + 2.0;
+      ypp[i] = (-0.5) / p;
+      u[i] = (y[i + 1] - y[i]) * invstep - (y[i] - y[i - 1]) * invstep;
+      u[i] = (6.0 * u[i] * 0.5 * invstep - 0.5 * u[i - 1]) / p;
+    }
+    if (s->nat[1]) {
+      qn = un = 0.0;
+    } else {
+      qn = 0.5;
+      un = (3.0 * invstep) * (s->grad[1] - (y[n - 1] - y[n - 2]) * invstep);
+    }
+    ypp[n - 1] = (un - qn * u[n - 2]) / (qn * ypp[n - 2] + 1.0);
+    for (k = n - 2; k >= 0; --k) ypp[k] = ypp[k] * ypp[k + 1] + u[k];
+    free(u);
+  }
+}
+
+static void sp_free(sp_t *s) {
+  free(s->x);
+  free(s->y);
+  free(s->ypp);
+}
+
+/* Spline::get_knotshift (spline.cpp:74-99) */
+static int sp_knotshift(const sp_t *s, double r, double *shift) {
+  int knot = -1;
+  if (r < s->x[s->n - 1] * (1. + 1.e-8)) {
+    int klo = 0, khi = s->n - 1;
+    while (khi - klo > 1) {
+      int k = (khi + klo) >> 1;
+      if (s->x[k] > r) khi = k;
+      else klo = k;
+    }
+    knot = klo;
+    *shift = (r - s->x[klo]) / (s->x[khi] - s->x[klo]);
+  }
+  return knot;
+}
+
+/* Spline3Eq::splint_comb(int, double, double*) (spline3eq.h:110-122) */
+static double sp_comb_k(const sp_t *s, int knot, double shift, double *grad) {
+  double a = 1.0 - shift;
+  double p1 = s->y[knot], d21 = s->ypp[knot];
+  double p2 = s->y[knot + 1], d22 = s->ypp[knot + 1];
+  *grad = (p2 - p1) * s->invstep + ((3 * shift * shift - 1) * d22 - (3 * a * a - 1) * d21) * s->step / 6.0;
+  return a * p1 + shift * p2 + ((a * a * a - a) * d21 + (shift * shift * shift - shift) * d22) * s->step * s->step / 6.0;
+}
+
+/* Spline3Eq::splint_comb(double, double*) (spline3eq.h:204-236) */
+static double sp_comb_x(const sp_t *s, double r, double *grad) {
+  int n = s->n, k;
+  double dr, b, a, p1, d21, p2, d22;
+  if (r < s->x[0]) {
+    *grad = s->grad[0];
+    return s->y[0] + s->grad[0] * (r - s->x[0]);
+  } else if (r > s->x[n - 1]) {
+    *grad = s->grad[1];
+    return s->y[n - 1] + s->grad[1] * (r - s->x[n - 1]);
+  }
+  dr = r - s->x[0];
+  if (dr < 0) k = 0;
+  else {
+    k = (int)(dr * s->invstep);
+    if (k >= n - 1) k = n - 2;
+  }
+  b = (dr - k * s->step) * s->invstep;
+  a = 1.0 - b;
+  p1 = s->y[k];
+  d21 = s->ypp[k];
+  p2 = s->y[k + 1];
+  d22 = s->ypp[k + 1];
+  *grad = (p2 - p1) * s->invstep + ((3 * (b * b) - 1) * d22 - (3 * (a * a) - 1) * d21) * s->step / 6.0;
+  return a * p1 + b * p2 + ((a * a * a - a) * d21 + (b * b * b - b) * d22) * (s->step * s->step) / 6.0;
+}
+
+static int pair_ij(int nt, int ti, int tj) {
+  return (ti <= tj) ? ti * nt + tj - (ti * (ti + 1)) / 2 : tj * nt + ti - (tj * (tj + 1)) / 2;
+}
+
+int mzo_ncoeff(const mzo_pot *pot) {
+  int n = 0, s, k, e;
+  for (s = 0; s < pot->nsplines; ++s) {
+    const mzo_spline *sp = &pot->splines[s];
+    for (k = 0; k < sp->nknots; ++k) n += sp->y_fixed[k] ? 0 : 1;
+    for (e = 0; e < 2; ++e) n += (!sp->grad_fixed[e] && !sp->nat[e]) ? 1 : 0;
+  }
+  return n;
+}
+
+int mzo_esize(const mzo_db *db, const mzo_pot *pot) {
+  return 8 * db->ncells + 3 * db->natoms + (pot->style == 1 ? 1 : pot->ntypes);
+}
+
+double mzo_objective(const mzo_db *db, const mzo_pot *pot, const double *coeffs, double *errvec_out,
+                     double *forces_out, double *energy_out, double *stress_out, double *dens_out) {
+  const int meam = pot->style == 1;
+  const int nt = pot->ntypes, npair = nt * (nt + 1) / 2;
+  const int N = db->natoms, NC = db->ncells;
+  int s, ci = 0, i;
+  sp_t *sp = (sp_t *)malloc(sizeof(sp_t) * pot->nsplines);
+  for (s = 0; s < pot->nsplines; ++s) sp_setup(&sp[s], &pot->splines[s], coeffs, &ci);
+  const sp_t *phi = sp, *rho = sp + npair, *U = sp + npair + nt;
+  const sp_t *ff = meam ? sp + npair + 2 * nt : NULL, *gg = meam ? sp + 2 * npair + 2 * nt : NULL;
+
+  /* initialize_compute (potential.cpp:388-408) */
+  double *energy = (double *)calloc(NC, sizeof(double));
+  double *stress = (double *)calloc(6 * (size_t)NC, sizeof(double));
+  double *force = (double *)calloc(3 * (size_t)N, sizeof(double));
+  double *constraint = (double *)calloc(NC, sizeof(double));
+  int maxrow = 0;
+  for (i = 0; i < N; ++i) {
+    int n = (int)(db->pair_off[i + 1] - db->pair_off[i]);
+    if (n > maxrow) maxrow = n;
+  }
+  double *drho = (double *)calloc(maxrow + 1, sizeof(double));
+  double *fv = (double *)calloc(maxrow + 1, sizeof(double));
+  double *dfv = (double *)calloc(maxrow + 1, sizeof(double));
+  size_t maxtrip = (size_t)maxrow * (maxrow > 0 ? maxrow - 1 : 0) / 2 + 1;
+  int *tj_ = (int *)malloc(sizeof(int) * maxtrip), *tk_ = (int *)malloc(sizeof(int) * maxtrip);
+  double *tg = (double *)malloc(sizeof(double) * maxtrip), *tdg = (double *)malloc(sizeof(double) * maxtrip);
+  double *tcos = (double *)malloc(sizeof(double) * maxtrip);
+
+  /* loop over atoms (pot_meam_spline.cpp:143-270) */
+  for (i = 0; i < N; ++i) {
+    const int cell = db->atom_cell[i], ti = db->atom_type[i];
+    const int64_t p0 = db->pair_off[i];
+    const int n = (int)(db->pair_off[i + 1] - p0);
+    double *Fi = force + 3 * (size_t)i, *S = stress + 6 * (size_t)cell;
+    double rho_val = 0.0, dF = 0.0;
+    int p, ntrip = 0, t;
+    for (p = 0; p < n; ++p) {
+      const int64_t q = p0 + p;
+      const int j = db->pair_nbr[q], tj = db->atom_type[j];
+      const double *u = db->pair_u + 3 * q, r = db->pair_r[q];
+      const int kphi = db->pair_knot[3 * q], krho = db->pair_knot[3 * q + 1], kf = db->pair_knot[3 * q + 2];
+      double *Fj = force + 3 * (size_t)j;
+      if (kphi != -1) {
+        double phigrad, tmp[3], tr[3];
+        double phival = 0.5 * sp_comb_k(&phi[pair_ij(nt, ti, tj)], kphi, db->pair_shift[3 * q], &phigrad);
+        phigrad *= 0.5;
+        energy[cell] += phival;
+        tmp[0] = u[0] * phigrad; tmp[1] = u[1] * phigrad; tmp[2] = u[2] * phigrad;
+        Fi[0] += tmp[0]; Fi[1] += tmp[1]; Fi[2] += tmp[2];
+        Fj[0] -= tmp[0]; Fj[1] -= tmp[1]; Fj[2] -= tmp[2];
+        tr[0] = tmp[0] * r; tr[1] = tmp[1] * r; tr[2] = tmp[2] * r;
+        /* Stress operator& (stress.h:134-137) */
+        S[0] -= u[0] * tr[0]; S[1] -= u[1] * tr[1]; S[2] -= u[2] * tr[2];
+        S[3] -= u[0] * tr[1]; S[4] -= u[1] * tr[2]; S[5] -= u[2] * tr[0];
+      }
+      if (krho != -1) rho_val += sp_comb_k(&rho[tj], krho, db->pair_shift[3 * q + 1], &drho[p]);
+      else drho[p] = 0.0;
+      if (meam) {
+        if (kf != -1) fv[p] = sp_comb_k(&ff[pair_ij(nt, ti, tj)], kf, db->pair_shift[3 * q + 2], &dfv[p]);
+        else fv[p] = dfv[p] = 0.0;
+      }
+    }
+    if (meam) {
+      /* Config::find_triplets (config.cpp:262-281) with
+       * TripletMEAMSpline::check_triplet (triplet_meam_spline.cpp:49-73):
+       * every j<k pair whose cos has a g knot. */
+      const sp_t *g = &gg[ti];
+      int j, k;
+      for (j = 0; j < n - 1; ++j)
+        for (k = j + 1; k < n; ++k) {
+          const double *uj = db->pair_u + 3 * (p0 + j), *uk = db->pair_u + 3 * (p0 + k);
+          double c = uj[0] * uk[0] + uj[1] * uk[1] + uj[2] * uk[2];
+          double gs;
+          int gk = sp_knotshift(g, c, &gs);
+          if (gk == -1) continue;
+          tj_[ntrip] = j;
+          tk_[ntrip] = k;
+          tcos[ntrip] = c;
+          tg[ntrip] = sp_comb_k(g, gk, gs, &tdg[ntrip]);
+          rho_val += fv[j] * fv[k] * tg[ntrip];
+          ++ntrip;
+        }
+    }
+    if (dens_out) dens_out[i] = rho_val;
+    /* embedding (pot_meam_spline.cpp:208-223) */
+    {
+      const sp_t *Ui = &U[ti];
+      const double w = db->cell_weight[cell];
+      if (rho_val < Ui->x[0]) {
+        double rho_i = Ui->x[0];
+        constraint[cell] += w * DUMMY_WEIGHT * 10. * (rho_i - rho_val) * (rho_i - rho_val);
+        if (!pot->embed_extrap) rho_val = rho_i;
+      } else if (rho_val > Ui->x[Ui->n - 1]) {
+        double rho_f = Ui->x[Ui->n - 1];
+        constraint[cell] += w * DUMMY_WEIGHT * 10. * (rho_val - rho_f) * (rho_val - rho_f);
+        if (!pot->embed_extrap) rho_val = rho_f;
+      }
+      energy[cell] += sp_comb_x(Ui, rho_val, &dF);
+    }
+    /* 2nd loop over pairs (pot_meam_spline.cpp:226-237) */
+    for (p = 0; p < n; ++p) {
+      const int64_t q = p0 + p;
+      const int j = db->pair_nbr[q];
+      const double *u = db->pair_u + 3 * q, r = db->pair_r[q];
+      double *Fj = force + 3 * (size_t)j, tmp[3], tr[3];
+      tmp[0] = u[0] * drho[p] * dF; tmp[1] = u[1] * drho[p] * dF; tmp[2] = u[2] * drho[p] * dF;
+      Fi[0] += tmp[0]; Fi[1] += tmp[1]; Fi[2] += tmp[2];
+      Fj[0] -= tmp[0]; Fj[1] -= tmp[1]; Fj[2] -= tmp[2];
+      tr[0] = tmp[0] * r; tr[1] = tmp[1] * r; tr[2] = tmp[2] * r;
+      S[0] -= u[0] * tr[0]; S[1] -= u[1] * tr[1]; S[2] -= u[2] * tr[2];
+      S[3] -= u[0] * tr[1]; S[4] -= u[1] * tr[2]; S[5] -= u[2] * tr[0];
+    }
+    /* 2nd loop over triplets (pot_meam_spline.cpp:240-269) */
+    for (t = 0; t < ntrip; ++t) {
+      const int j = tj_[t], k = tk_[t];
+      const int64_t qj = p0 + j, qk = p0 + k;
+      const double *uj = db->pair_u + 3 * qj, *uk = db->pair_u + 3 * qk;
+      const double rj = db->pair_r[qj], rk = db->pair_r[qk];
+      const double invrj = 1.0 / rj, invrk = 1.0 / rk;
+      double *Fj = force + 3 * (size_t)db->pair_nbr[qj], *Fk = force + 3 * (size_t)db->pair_nbr[qk];
+      double dV3j = tg[t] * dfv[j] * fv[k] * dF;
+      double dV3k = tg[t] * fv[j] * dfv[k] * dF;
+      double V3 = tdg[t] * fv[j] * fv[k] * dF;
+      double vlj = V3 * invrj, vlk = V3 * invrk;
+      double vv3j = dV3j - vlj * tcos[t], vv3k = dV3k - vlk * tcos[t];
+      double dfj[3], dfk[3];
+      int d;
+      for (d = 0; d < 3; ++d) {
+        dfj[d] = uj[d] * vv3j + uk[d] * vlj;
+        dfk[d] = uk[d] * vv3k + uj[d] * vlk;
+        Fi[d] += dfj[d] + dfk[d];
+        Fj[d] -= dfj[d];
+        Fk[d] -= dfk[d];
+      }
+      for (d = 0; d < 3; ++d) {
+        dfj[d] *= rj;
+        dfk[d] *= rk;
+      }
+      S[0] -= uj[0] * dfj[0]; S[1] -= uj[1] * dfj[1]; S[2] -= uj[2] * dfj[2];
+      S[3] -= uj[0] * dfj[1]; S[4] -= uj[1] * dfj[2]; S[5] -= uj[2] * dfj[0];
+      S[0] -= uk[0] * dfk[0]; S[1] -= uk[1] * dfk[1]; S[2] -= uk[2] * dfk[2];
+      S[3] -= uk[0] * dfk[1]; S[4] -= uk[1] * dfk[2]; S[5] -= uk[2] * dfk[0];
+    }
+  }
+
+  /* accumulate_error (potential.cpp:415-491) */
+  const int esize = mzo_esize(db, pot);
+  double *ev = (double *)malloc(sizeof(double) * esize);
+  double sum = 0.0;
+  int c, idx = 0;
+  for (c = 0; c < NC; ++c) {
+    const int a0 = db->cell_atom0[c], na = db->cell_atom0[c + 1] - a0;
+    const double w = db->cell_weight[c];
+    int q, a, d;
+    energy[c] = energy[c] / na;
+    ev[idx] = w * db->cell_eweight[c] * pot->energy_weight * na * (energy[c] - db->cell_energy0[c]);
+    sum += ev[idx] * ev[idx];
+    ++idx;
+    for (q = 0; q < 6; ++q) {
+      stress[6 * c + q] = stress[6 * c + q] / db->cell_vol[c];
+      ev[idx] = w * db->cell_sweight[c] * pot->stress_weight * (stress[6 * c + q] - db->cell_stress0[6 * c + q]);
+      sum += ev[idx] * ev[idx];
+      ++idx;
+    }
+    for (a = a0; a < a0 + na; ++a)
+      for (d = 0; d < 3; ++d) {
+        ev[idx] = w * (force[3 * a + d] - db->atom_force0[3 * a + d]);
+        sum += ev[idx] * ev[idx];
+        ++idx;
+      }
+  }
+  for (c = 0; c < NC; ++c) {
+    ev[idx] = constraint[c];
+    sum += ev[idx] * ev[idx];
+    ++idx;
+  }
+  if (meam) {
+    /* pot_meam_spline.cpp:274-278 with PotFns::get_max_y_mag (pot_fns.cpp:223-234)
+     * and Spline::get_max_y_mag (spline.cpp:58-67) */
+    double my = 0.0;
+    int f, k;
+    for (f = 0; f < npair; ++f) {
+      double m = 0.0;
+      for (k = 0; k < ff[f].n; ++k)
+        if (fabs(m) < fabs(ff[f].y[k])) m = ff[f].y[k];
+      if (fabs(my) < fabs(m)) my = m;
+    }
+    double mag = fabs(my);
+    double fe = DUMMY_WEIGHT * 25. * (1.0 - mag) * (1.0 - mag);
+    sum += fe * fe;
+    ev[idx++] = fe;
+  } else {
+    /* pot_eam_spline.cpp:211-218 */
+    int t;
+    for (t = 0; t < nt; ++t) {
+      double g, mid = 0.5 * (U[t].x[0] + U[t].x[U[t].n - 1]);
+      sp_comb_x(&U[t], mid, &g);
+      double e = DUMMY_WEIGHT * g;
+      sum += e * e;
+      ev[idx++] = e;
+    }
+  }
+  if (errvec_out) memcpy(errvec_out, ev, sizeof(double) * esize);
+  if (forces_out) memcpy(forces_out, force, sizeof(double) * 3 * (size_t)N);
+  if (energy_out) memcpy(energy_out, energy, sizeof(double) * NC);
+  if (stress_out) memcpy(stress_out, stress, sizeof(double) * 6 * (size_t)NC);
+
+  free(ev);
+  free(tj_); free(tk_); free(tg); free(tdg); free(tcos);
+  free(drho); free(fv); free(dfv);
+  free(energy); free(stress); free(force); free(constraint);
+  for (s = 0; s < pot->nsplines; ++s) sp_free(&sp[s]);
+  free(sp);
+  return sum;
+}

@@ -1,0 +1,157 @@
+// Test-oracle harness around the UNMODIFIED reference program (compiled from
+// its own sources by oracle/Makefile into oracle/_ref/).  It is test
+// infrastructure: only tests/, the smoke check and bench.py's CPU-baseline
+// leg run it.
+//
+// It builds a Meamzilla object exactly as src/main.cpp does (parameter file,
+// potential file, configuration file, pair/triplet lists) and then drives the
+// objective through the reference's own public interface:
+//   Potential::compute(const Comm&, ErrorVec*)    src/potential.h:67
+//   Potential::coeff(int)                          src/potential.h:60
+//   PotEAM::compute_densities                      src/pots/pot_eam/pot_eam.h:45
+//
+// Usage:
+//   mzref -p <param> [-x <coeff.bin>] [-o <prefix>] [-reps K] [-fd h] [-q]
+//     -x     raw float64 file with get_ncoeff() values, applied via coeff(i)
+//     -o     write <prefix>.{obj,errvec,energy,stress,force,dens,coeff}.bin
+//            (raw little-endian float64; forces in configuration order)
+//     -reps  time K back-to-back compute() calls (no ErrorVec) after one
+//            warm-up; prints "seconds_per_eval <t>"
+//     -fd    central finite-difference gradient of the objective with step h
+//            for every coefficient -> <prefix>.fdgrad.bin
+#define protected public
+#include "meamzilla.h"
+#include "universe.h"
+#include "config.h"
+#include "cell.h"
+#include "atom.h"
+#include "pot_list.h"
+#include "potential.h"
+#include "pots/pot_eam/pot_eam.h"
+#undef protected
+
+#include <chrono>
+#include <fcntl.h>
+#include <iostream>
+#include <unistd.h>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
+using namespace MEAMZ_NS;
+
+static void dump(const std::string &path, const std::vector<double> &v) {
+  FILE *f = std::fopen(path.c_str(), "wb");
+  if (!f) { std::fprintf(stderr, "mzref: cannot write %s\n", path.c_str()); std::exit(2); }
+  if (!v.empty()) std::fwrite(v.data(), sizeof(double), v.size(), f);
+  std::fclose(f);
+}
+
+int main(int argc, char **argv) {
+  std::string param, xfile, prefix;
+  int reps = 0, quiet = 0;
+  double fd_h = 0.0;
+  for (int i = 1; i < argc; ++i) {
+    std::string a = argv[i];
+    if (a == "-p" && i + 1 < argc) param = argv[++i];
+    else if (a == "-x" && i + 1 < argc) xfile = argv[++i];
+    else if (a == "-o" && i + 1 < argc) prefix = argv[++i];
+    else if (a == "-reps" && i + 1 < argc) reps = std::atoi(argv[++i]);
+    else if (a == "-fd" && i + 1 < argc) fd_h = std::atof(argv[++i]);
+    else if (a == "-q") quiet = 1;
+    else { std::fprintf(stderr, "mzref: bad argument %s\n", a.c_str()); return 2; }
+  }
+  if (param.empty()) { std::fprintf(stderr, "mzref: -p <param> required\n"); return 2; }
+
+  MPI_Init(&argc, &argv);
+  // Silence the reference's progress prints when asked (they go to stdout).
+  int saved_stdout = -1;
+  if (quiet) {
+    std::fflush(stdout);
+    saved_stdout = dup(1);
+    int devnull = open("/dev/null", O_WRONLY);
+    dup2(devnull, 1);
+    close(devnull);
+  }
+  char *margv[3] = {argv[0], (char *)"-p", (char *)param.c_str()};
+  Meamzilla *mmz = new Meamzilla(3, margv, MPI_COMM_WORLD);
+  if (quiet) {
+    std::cout.flush();
+    std::fflush(stdout);
+    dup2(saved_stdout, 1);
+    close(saved_stdout);
+  }
+
+  const Comm &comm = mmz->universe->comm_inter;
+  Potential *pot = mmz->potlist->at(0);
+  const int ncoeff = pot->get_ncoeff();
+
+  if (!xfile.empty()) {
+    std::vector<double> x(ncoeff);
+    FILE *f = std::fopen(xfile.c_str(), "rb");
+    if (!f || std::fread(x.data(), sizeof(double), ncoeff, f) != (size_t)ncoeff) {
+      std::fprintf(stderr, "mzref: cannot read %d coefficients from %s\n", ncoeff, xfile.c_str());
+      return 2;
+    }
+    std::fclose(f);
+    for (int i = 0; i < ncoeff; ++i) pot->coeff(i) = x[i];
+  }
+
+  ErrorVec evec;
+  double obj = pot->compute(comm, &evec);
+  std::fprintf(stderr, "objective %.17g ncoeff %d esize %zu natoms %d ncells %d\n", obj, ncoeff,
+               evec.size(), mmz->config->total_natoms, mmz->config->ncells);
+
+  if (!prefix.empty()) {
+    dump(prefix + ".obj.bin", std::vector<double>{obj});
+    dump(prefix + ".errvec.bin", evec);
+    std::vector<double> en, st, fo, co(ncoeff);
+    for (Cell *c : mmz->config->cells) {
+      en.push_back(c->energy);
+      st.push_back(c->stress.xx); st.push_back(c->stress.yy); st.push_back(c->stress.zz);
+      st.push_back(c->stress.xy); st.push_back(c->stress.yz); st.push_back(c->stress.zx);
+      for (Atom *a : c->atoms) { fo.push_back(a->force.x); fo.push_back(a->force.y); fo.push_back(a->force.z); }
+    }
+    for (int i = 0; i < ncoeff; ++i) co[i] = pot->coeff(i);
+    dump(prefix + ".energy.bin", en);
+    dump(prefix + ".stress.bin", st);
+    dump(prefix + ".force.bin", fo);
+    dump(prefix + ".coeff.bin", co);
+    PotEAM *eam = dynamic_cast<PotEAM *>(pot);
+    if (eam) {
+      std::vector<double> dens;
+      eam->compute_densities(comm, &dens);
+      dump(prefix + ".dens.bin", dens);
+    }
+  }
+
+  if (fd_h > 0.0) {
+    std::vector<double> g(ncoeff);
+    for (int i = 0; i < ncoeff; ++i) {
+      double keep = pot->coeff(i);
+      pot->coeff(i) = keep + fd_h;
+      double fp = pot->compute(comm);
+      pot->coeff(i) = keep - fd_h;
+      double fm = pot->compute(comm);
+      pot->coeff(i) = keep;
+      g[i] = (fp - fm) / (2.0 * fd_h);
+    }
+    if (!prefix.empty()) dump(prefix + ".fdgrad.bin", g);
+  }
+
+  if (reps > 0) {
+    pot->compute(comm);
+    auto t0 = std::chrono::steady_clock::now();
+    for (int r = 0; r < reps; ++r) pot->compute(comm);
+    auto t1 = std::chrono::steady_clock::now();
+    double s = std::chrono::duration<double>(t1 - t0).count() / reps;
+    std::printf("seconds_per_eval %.9g\n", s);
+    std::fflush(stdout);
+  }
+
+  delete mmz;
+  MPI_Finalize();
+  return 0;
+}

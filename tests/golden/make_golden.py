@@ -1,0 +1,128 @@
+"""Generate the golden fixtures under tests/golden/ from the REFERENCE itself.
+
+Each case directory holds the reference-format inputs (start.pot, db.conf,
+param with relative file names) and golden.npz with what the compiled,
+unmodified reference (oracle/_ref/mzref, built by oracle/Makefile) returns
+through Potential::compute for two coefficient vectors:
+
+    obj, errvec, force, energy, stress, dens, coeff       (file coefficients)
+    obj2, errvec2, force2, energy2, stress2, coeff2      (perturbed vector)
+    fdgrad (central differences of the objective, h = 1e-6; small cases)
+
+Run here (needs the reference sources to build mzref):
+    make -C oracle && python tests/golden/make_golden.py
+"""
+from __future__ import annotations
+
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+from meamzilla_b200 import synth  # noqa: E402
+import oracle  # noqa: E402
+
+
+def _targets(cells, seed):
+    rng = np.random.default_rng(seed)
+    for c in cells:
+        c.energy0 = float(rng.normal(-3.0, 0.1))
+        c.force0 = rng.normal(0.0, 0.3, (c.natoms, 3))
+        c.stress0 = rng.normal(0.0, 1e-3, 6)
+
+
+def _write(name, pot, cells, fd=False, perturb=0.02, **param_kw):
+    d = os.path.join(HERE, name)
+    os.makedirs(d, exist_ok=True)
+    synth.write_pot(os.path.join(d, "start.pot"), pot)
+    synth.write_config(os.path.join(d, "db.conf"), cells)
+    lines = ["config db.conf", "startpot start.pot", "tempfile tempfile", "endpot endpot"]
+    lines += ["energy_weight %s" % param_kw.get("energy_weight", 1.0),
+              "stress_weight %s" % param_kw.get("stress_weight", 1.0), "rescale 0"]
+    if param_kw.get("embed_extrap"):
+        lines.append("embed_extrap %d" % param_kw["embed_extrap"])
+    with open(os.path.join(d, "param"), "w") as fh:
+        fh.write("\n".join(lines) + "\n")
+    ref = oracle.run_reference("param", cwd=d, fd_h=1e-6 if fd else 0.0)
+    out = dict(obj=ref["obj"], errvec=ref["errvec"], force=ref["force"], energy=ref["energy"], stress=ref["stress"],
+               coeff=ref["coeff"])
+    if "dens" in ref:
+        out["dens"] = ref["dens"]
+    if fd:
+        out["fdgrad"] = ref["fdgrad"]
+    rng = np.random.default_rng(99)
+    x2 = ref["coeff"] + rng.normal(0.0, perturb, ref["coeff"].size)
+    ref2 = oracle.run_reference("param", cwd=d, coeffs=x2)
+    out.update(obj2=ref2["obj"], errvec2=ref2["errvec"], force2=ref2["force"], energy2=ref2["energy"],
+               stress2=ref2["stress"], coeff2=x2)
+    np.savez_compressed(os.path.join(d, "golden.npz"), **out)
+    print(name, "obj", ref["obj"], "natoms", sum(c.natoms for c in cells), "esize", ref["errvec"].size)
+
+
+def in_range_meam(pot):
+    """Scale rho and f knots so densities fall inside U's [-1, 1] range (the
+    teacher's densities lie far outside it)."""
+    p = pot.copy()
+    for s in p.groups[1]:
+        s.y *= 0.02
+        s.grad *= 0.02
+    for s in p.groups[3]:
+        s.y *= 0.12
+        s.grad *= 0.12
+    return p
+
+
+def main():
+    # 1. EAM, 3 bcc cells (the eam54 rules)
+    pot, cells = synth.make_workload("eam54", seed=3, ncells=3)
+    _targets(cells, 1)
+    _write("eam_bcc3", pot, cells, fd=True)
+
+    # 2. MEAM, 6 cells of the meam200 mixture
+    pot, cells = synth.make_workload("meam200", seed=3, ncells=6)
+    _targets(cells, 2)
+    _write("meam_mix6", pot, cells, fd=True)
+
+    # 3. MEAM in range (no density punishment), embed_extrap, per-cell weights
+    pot, cells = synth.make_workload("meam200", seed=4, ncells=4)
+    _targets(cells, 3)
+    for i, c in enumerate(cells):
+        c.weight, c.eweight, c.sweight = 1.0 + 0.5 * i, 2.0 - 0.3 * i, 0.5 + 0.2 * i
+    _write("meam_inrange_w", in_range_meam(pot), cells, fd=True, energy_weight=2.5, stress_weight=0.7)
+
+    # 4. two-species MEAM (meam2k rules), natural and fixed ends, fixed knots,
+    #    a g grid narrower than [-1, 1] (cos beyond it is not a triplet; below
+    #    it the cubic is extrapolated), embed_extrap 1
+    pot, cells = synth.make_workload("meam2k", seed=5, ncells=3)
+    _targets(cells, 4)
+    p = pot.copy()
+    p.groups[0][1].bc = (-1, 1)                 # phi_AB: natural left, fixed right slope
+    p.groups[1][0].bc = (1, -1)                 # rho_A: fixed left, natural right
+    p.groups[3][2].fixed = np.zeros(10, dtype=int)
+    p.groups[3][2].fixed[[0, 4, 9]] = 1         # f_BB: three fixed knots
+    g = p.groups[4][1]
+    p.groups[4][1] = synth.Spline(-0.5, 0.9, np.interp(np.linspace(-0.5, 0.9, 8), np.linspace(-1, 1, 8), g.y),
+                                  g.grad.copy())
+    _write("meam2_edge", p, cells, embed_extrap=1)
+
+    # 5. isolated atoms: a sparse cell where some atoms have no neighbours,
+    #    and a one-atom cell whose only neighbours are its own images
+    lat = np.eye(3) * 12.0
+    pos = np.array([[0.0, 0.0, 0.0], [2.6, 0.0, 0.0], [6.0, 6.0, 6.0], [9.0, 2.0, 5.0]])
+    c1 = synth.Cell(lattice=lat, types=np.zeros(4, dtype=np.int64), pos=pos, force0=np.zeros((4, 3)))
+    c2 = synth.Cell(lattice=np.diag([2.9, 3.1, 3.3]), types=np.zeros(1, dtype=np.int64),
+                    pos=np.array([[0.1, 0.2, 0.3]]), force0=np.zeros((1, 3)))
+    cells = [c1, c2]
+    _targets(cells, 5)
+    pot = synth.teacher_potential("meam/spline", 1, 4.5, seed=11)
+    _write("meam_sparse", pot, cells, fd=True)
+    pot = synth.teacher_potential("eam/spline", 1, 5.0, seed=12)
+    _write("eam_sparse", pot, cells)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,132 @@
+"""CUDA evaluator against the reference goldens and the CPU oracle.
+
+Tolerances: FP64 objective 1e-12 relative and forces 1e-10 eV/A (the plain
+path's bar); mixed precision objective 1e-6 relative and forces 1e-5 eV/A
+against FP64."""
+import numpy as np
+import pytest
+
+from conftest import CASES, load_case, oracle_for, rel
+
+pytestmark = pytest.mark.gpu
+
+FP64_OBJ = 1e-12
+FP64_FORCE = 1e-10
+MIX_OBJ = 1e-6
+MIX_FORCE = 1e-5
+
+
+def _ev(case, ncand=1):
+    from meamzilla_b200.potential import Evaluator
+    return Evaluator(case["db"], case["pot"], max_candidates=ncand, **case["weights"])
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_fp64_matches_reference_goldens(name):
+    from meamzilla_b200.potential import MZ_FP64
+    case = load_case(name)
+    g = case["gold"]
+    ev = _ev(case, 2)
+    x = np.stack([g["coeff"], g["coeff2"]])
+    out = ev.objective(x, MZ_FP64, errvec=True, forces=True, energy=True, stress=True)
+    for c, sfx in enumerate(("", "2")):
+        assert rel(out["obj"][c], float(g["obj" + sfx])) <= FP64_OBJ, (name, sfx, out["obj"][c], g["obj" + sfx])
+        e = g["errvec" + sfx]
+        assert np.max(np.abs(out["errvec"][c] - e) / np.maximum(np.abs(e), 1.0)) <= 1e-11
+        assert np.max(np.abs(out["forces"][c].ravel() - g["force" + sfx])) <= FP64_FORCE
+        assert np.allclose(out["energy"][c], g["energy" + sfx], rtol=1e-12, atol=1e-12)
+        assert np.allclose(out["stress"][c].ravel(), g["stress" + sfx], rtol=1e-10, atol=1e-13)
+    if "dens" in g:
+        d = ev.densities(g["coeff"])
+        assert np.allclose(d, g["dens"], rtol=1e-13, atol=1e-13)
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_mixed_within_tolerance(name):
+    from meamzilla_b200.potential import MZ_FP64, MZ_MIXED
+    case = load_case(name)
+    g = case["gold"]
+    ev = _ev(case, 2)
+    x = np.stack([g["coeff"], g["coeff2"]])
+    a = ev.objective(x, MZ_FP64, forces=True)
+    b = ev.objective(x, MZ_MIXED, forces=True)
+    for c in range(2):
+        assert rel(b["obj"][c], a["obj"][c]) <= MIX_OBJ
+        assert np.max(np.abs(b["forces"][c] - a["forces"][c])) <= MIX_FORCE
+
+
+def test_batched_candidates_match_oracle():
+    """A population of 24 perturbed candidates in one launch: each equals the
+    oracle's objective for that vector; chunking over candidates is exact."""
+    from meamzilla_b200.potential import MZ_FP64, MZ_MIXED
+    case = load_case("meam2_edge")
+    orc = oracle_for(case)
+    x0 = case["gold"]["coeff"]
+    rng = np.random.default_rng(7)
+    X = x0[None, :] + rng.normal(0, 0.05, (24, x0.size))
+    ev = _ev(case, 24)
+    o64 = ev.objective(X, MZ_FP64)
+    o32 = ev.objective(X, MZ_MIXED)
+    for c in range(X.shape[0]):
+        ref = orc.objective(X[c])
+        assert rel(o64[c], ref) <= FP64_OBJ
+        assert rel(o32[c], ref) <= MIX_OBJ
+    ev1 = _ev(case, 5)  # candidates split over several launches
+    assert np.array_equal(ev1.objective(X, MZ_FP64), o64)
+
+
+def test_repeatable_bit_for_bit():
+    from meamzilla_b200.potential import MZ_FP64
+    case = load_case("meam_mix6")
+    ev = _ev(case, 1)
+    x = case["gold"]["coeff"]
+    a = ev.objective(x, MZ_FP64, forces=True)
+    b = ev.objective(x, MZ_FP64, forces=True)
+    assert a["obj"][0] == b["obj"][0]
+    assert np.array_equal(a["forces"], b["forces"])
+
+
+def test_larger_two_species_database_vs_oracle():
+    """40 cells of the two-species 2000-cell workload rules (rows up to ~60
+    neighbours, ~1800 triplets per atom)."""
+    from meamzilla_b200 import synth
+    from meamzilla_b200.potential import MZ_FP64, MZ_MIXED, Database, Evaluator, PotentialFile
+    import oracle
+    spec, cells = synth.make_workload("meam2k", seed=2, ncells=40)
+    rng = np.random.default_rng(3)
+    for c in cells:
+        c.energy0 = rng.normal(-3, 0.1)
+        c.force0 = rng.normal(0, 0.3, (c.natoms, 3))
+        c.stress0 = rng.normal(0, 1e-3, 6)
+    pot = PotentialFile.from_spec(spec)
+    db = Database.from_cells(cells, pot)
+    ev = Evaluator(db, pot, 1.0, 1.0, 0, max_candidates=2)
+    orc = oracle.CRestatement.for_evaluator(ev)
+    x = pot.coeffs()
+    X = np.stack([x, x + rng.normal(0, 0.05, x.size)])
+    out = ev.objective(X, MZ_FP64, forces=True, errvec=True)
+    mix = ev.objective(X, MZ_MIXED, forces=True)
+    for c in range(2):
+        r = orc.objective(X[c], full=True)
+        assert rel(out["obj"][c], r["obj"]) <= FP64_OBJ
+        assert np.max(np.abs(out["forces"][c] - r["forces"])) <= FP64_FORCE
+        assert rel(mix["obj"][c], r["obj"]) <= MIX_OBJ
+        assert np.max(np.abs(mix["forces"][c] - r["forces"])) <= MIX_FORCE
+
+
+def test_potential_interface_compute_and_dir():
+    """The reference-shaped Potential: compute(ErrorVec), coeff, set_dir,
+    compute_dir on a clone (potential.cpp:268-292)."""
+    from meamzilla_b200.potential import Evaluator, Potential
+    case = load_case("meam_inrange_w")
+    orc = oracle_for(case)
+    ev = _ev(case, 1)
+    pot = Potential(ev)
+    evec = []
+    val = pot.compute(evec)
+    assert rel(val, float(case["gold"]["obj"])) <= FP64_OBJ
+    assert len(evec) == ev.esize
+    d = np.linspace(-1, 1, pot.get_ncoeff()) * 1e-3
+    v2 = pot.compute_dir(None, d, 0.5)
+    assert rel(v2, orc.objective(pot.x + 0.5 * d)) <= FP64_OBJ
+    assert pot.get_error() == val  # compute_dir works on a clone
