@@ -1,0 +1,438 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 MEAM objective evaluator.
+
+Metric: MEAM objective+gradient evaluations per second, batched in mixed
+precision (FP32 spline and triplet arithmetic, FP64 sums), on the
+two-species 2000-cell spline MEAM database (seeded synthetic data with the
+generation rules of meamzilla_b200/synth.py, 136 coefficients), 64 candidate
+coefficient vectors per step.  The FP64 plain objective rate (one candidate
+per launch) is reported beside it, with the ratio.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl mine|reference]
+
+One step = one objective+gradient launch sequence over all 64 candidates,
+inputs resident on the device, timed with CUDA events on the evaluator's
+stream.  `e2e` measures the same through the host API (host coefficient
+vectors in, host objectives and gradients out).  Under torchrun each rank
+evaluates its own 64 candidates (weak scaling, no collective on the data
+path); the time is the maximum over ranks.
+
+`--impl reference` times the reference program (compiled from its own
+sources, oracle/_ref/mzref_fast) on the host cores: independent processes on
+disjoint samples of the same database, its objective+gradient being the
+objective plus one forward difference per coefficient as its Powell
+optimizer forms it (opt_powell.cpp:363-384).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "MEAM objective+gradient evals/s, mixed-batched vs FP64 plain GPU, rel err≤1e-6"
+WORKLOAD = ("meam2k: two-species spline MEAM (meam/spline 2), 2000 periodic cells, atom count log-uniform "
+            "in [8, 1024], 50/50 species, radial functions on [1.8, 5.5] A, 12 splines, 136 coefficients")
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="mine", choices=["mine", "reference"])
+    ap.add_argument("--ncand", type=int, default=64)
+    ap.add_argument("--ncells", type=int, default=2000)
+    ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+# ------------------------------------------------------------------ helpers
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu: int):
+        self.gpu = gpu
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.FIELDS, "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        with open(self.path) as fh:
+            for line in fh:
+                p = [x.strip() for x in line.split(",")]
+                if len(p) < 9:
+                    continue
+                try:
+                    sm.append(float(p[1]))
+                    smax.append(float(p[2]))
+                except ValueError:
+                    continue
+                for nm, v in zip(names, p[5:9]):
+                    if v.lower().startswith("active"):
+                        reasons.add(nm)
+        os.unlink(self.path)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "samples": len(sm), "reasons": sorted(reasons)}
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as fh:
+            d = json.load(fh)
+        return d.get("hbm_gbs", 6650.0), "measured"
+    return 6650.0, "fallback"
+
+
+def build_workload(args, device):
+    """Teacher potential, database with teacher targets + noise, evaluator."""
+    from meamzilla_b200 import synth
+    from meamzilla_b200.potential import MZ_FP64, Database, Evaluator, PotentialFile
+    spec, cells = synth.make_workload("meam2k", seed=args.seed, ncells=args.ncells)
+    pot = PotentialFile.from_spec(spec)
+    db = Database.from_cells(cells, pot)
+    ev0 = Evaluator(db, pot, 1.0, 1.0, 0, device=device, max_candidates=1)
+    out = ev0.objective(pot.coeffs()[None, :], MZ_FP64, forces=True, energy=True, stress=True)
+    del ev0
+    rng = np.random.default_rng(3000 + args.seed)
+    nc = len(cells)
+    e0 = out["energy"][0] + rng.normal(0.0, 1e-3, nc)
+    s0 = out["stress"][0] + rng.normal(0.0, 0.01, (nc, 6)) / synth.GPA_PER_EV_A3
+    f0 = out["forces"][0] + rng.normal(0.0, 0.01, out["forces"][0].shape)
+    db.set_targets(e0, s0.ravel(), f0.ravel())
+    a0 = np.cumsum([0] + [c.natoms for c in cells])
+    for i, c in enumerate(cells):  # keep the python copy consistent for the CPU baseline files
+        c.energy0, c.stress0, c.force0 = float(e0[i]), s0[i], f0[a0[i]:a0[i + 1]]
+    ev = Evaluator(db, pot, 1.0, 1.0, 0, device=device, max_candidates=args.ncand)
+    return spec, cells, pot, db, ev
+
+
+def algorithmic(stats, ncand, P):
+    """Fixed algorithmic bytes and flops of one batched objective+gradient step
+    (per-pair / per-triplet / per-atom / per-cell figures of the design notes)."""
+    Np, Nt, N, nc = stats["npairs"], stats["ntriplets"], stats["natoms"], stats["ncells"]
+    b32 = 20 * Np + 4 * Nt + 48 * N + 112 * nc + ncand * (8 + 8 * P + 8 * P)
+    fwd = 145 * Np + 111 * Nt + 40 * N
+    return b32, fwd
+
+
+# --------------------------------------------------------- CPU reference arm
+
+def cpu_reference(spec, cells, stats, P, reps, target_triplets=1.0e7, max_procs=64):
+    """Time the compiled reference (oracle/_ref/mzref_fast) on disjoint samples
+    of the database, one single-threaded process per host core (the
+    reference's MPI atom decomposition without its communication).  Returns
+    objective evals/s of the full database, extrapolated by triplet count."""
+    import oracle
+    from meamzilla_b200 import synth
+    exe = oracle.MZREF_FAST
+    if not os.path.exists(exe):
+        return None, "oracle/_ref/mzref_fast not built"
+    try:
+        import psutil
+        avail_gb = psutil.virtual_memory().available / 2 ** 30
+    except Exception:
+        avail_gb = 16.0
+    ncores = os.cpu_count() or 1
+    nproc = int(max(1, min(ncores, max_procs, avail_gb // 3)))
+    # triplets per cell (j<k pairs of every row, the reference's triplet count)
+    rows = stats["rows_per_cell"]
+    trip = [int(sum(n * (n - 1) // 2 for n in r)) for r in rows]
+    samples, i = [], 0
+    while len(samples) < nproc and i < len(cells):
+        lo, t = i, 0
+        while i < len(cells) and t < target_triplets:
+            t += trip[i]
+            i += 1
+        samples.append((lo, i, t))
+    tmp = tempfile.mkdtemp(prefix="mzref_")
+    procs = []
+    for k, (lo, hi, t) in enumerate(samples):
+        d = os.path.join(tmp, "s%d" % k)
+        par = synth.write_case(d, spec, cells[lo:hi])
+        procs.append((subprocess.Popen([exe, "-p", par, "-reps", str(reps), "-q"], stdout=subprocess.PIPE,
+                                       stderr=subprocess.DEVNULL, text=True), t))
+    rate = 0.0
+    sample_trip = 0
+    for pr, t in procs:
+        out, _ = pr.communicate(timeout=1800)
+        sec = None
+        for line in out.splitlines():
+            if line.startswith("seconds_per_eval"):
+                sec = float(line.split()[1])
+        if sec is None or pr.returncode != 0:
+            return None, "reference run failed"
+        rate += t / sec
+        sample_trip += t
+    subprocess.run(["rm", "-rf", tmp])
+    obj_evals = rate / stats["ntriplets"]
+    desc = ("%d concurrent single-thread processes of the reference (-Ofast -march=x86-64-v3), each on a disjoint "
+            "run of cells (%d cells, %.3g triplets in all), %d timed compute() calls each after one warm-up; "
+            "objective evals/s of the full database extrapolated by triplet count; objective+gradient = "
+            "objective + %d forward differences" % (len(procs), samples[-1][1] - samples[0][0], sample_trip,
+                                                     reps, P))
+    return {"obj_evals_per_s": obj_evals, "objgrad_evals_per_s": obj_evals / (P + 1), "cores": len(procs),
+            "sample": desc}, None
+
+
+# ------------------------------------------------------------------- arms
+
+def run_reference_arm(args, world, rank):
+    if rank != 0:
+        return
+    from meamzilla_b200 import synth
+    from meamzilla_b200.potential import Database, PotentialFile
+    spec, cells = synth.make_workload("meam2k", seed=args.seed, ncells=args.ncells)
+    pot = PotentialFile.from_spec(spec)
+    db = Database.from_cells(cells, pot)
+    stats = db.stats()
+    v = db.view()
+    stats["rows_per_cell"] = _rows_per_cell(v)
+    P = pot.ncoeff
+    t0 = time.time()
+    res, err = cpu_reference(spec, cells, stats, P, reps=max(1, args.steps))
+    wall = time.time() - t0
+    if res is None:
+        print(json.dumps({"impl": "reference", "unavailable": err}))
+        return
+    line = {
+        "impl": "reference", "metric": METRIC, "value": res["objgrad_evals_per_s"], "unit": "evals/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 / res["objgrad_evals_per_s"], "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+        "config": {"workload": WORKLOAD, "ncells": stats["ncells"], "natoms": stats["natoms"],
+                   "npairs": stats["npairs"], "ntriplets": stats["ntriplets"], "ncoeff": P},
+        "objective_evals_per_s": res["obj_evals_per_s"],
+        "cpu_baseline": {"value": res["objgrad_evals_per_s"], "unit": "evals/s", "cores": res["cores"],
+                         "kind": "reference", "sample": res["sample"]},
+        "e2e": {"value": res["objgrad_evals_per_s"], "unit": "evals/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+        "wall_s": wall,
+    }
+    print(json.dumps(line))
+
+
+def _rows_per_cell(v):
+    off = v["pair_off"]
+    n = np.diff(off)
+    a0 = v["cell_atom0"]
+    return [n[a0[c]:a0[c + 1]] for c in range(v["ncells"])]
+
+
+def run_mine(args, world, rank, local):
+    import torch
+    from meamzilla_b200 import synth
+    from meamzilla_b200.potential import MZ_FP64, MZ_MIXED, alu_peak
+    if not torch.cuda.is_available():
+        raise RuntimeError("bench.py needs a CUDA device")
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    spec, cells, pot, db, ev = build_workload(args, local)
+    stats = db.stats()
+    P = pot.ncoeff
+    x0 = pot.coeffs()
+    X = synth.perturbed(x0, args.ncand, 0.05, seed=1 + rank)
+    dev = torch.device("cuda", local)
+    Xd = torch.tensor(X, dtype=torch.float64, device=dev)
+    obj = torch.empty(args.ncand, dtype=torch.float64, device=dev)
+    grad = torch.empty((args.ncand, P), dtype=torch.float64, device=dev)
+    stream = torch.cuda.ExternalStream(ev.stream())
+
+    # accuracy of the mixed path against FP64 on these candidates
+    o64 = ev.objective(X, MZ_FP64)
+    o32 = ev.objective(X, MZ_MIXED)
+    f64 = ev.objective(X[:1], MZ_FP64, forces=True)["forces"][0]
+    f32 = ev.objective(X[:1], MZ_MIXED, forces=True)["forces"][0]
+    _, g64 = ev.objective_grad(X[:2], MZ_FP64)
+    _, g32 = ev.objective_grad(X[:2], MZ_MIXED)
+    accuracy = {"obj_rel_err_max": float(np.max(np.abs(o32 - o64) / np.abs(o64))),
+                "force_err_max_eV_per_A": float(np.max(np.abs(f32 - f64))),
+                "grad_err_max_rel_to_max": float(np.max(np.abs(g32 - g64)) / np.max(np.abs(g64)))}
+
+    def barrier():
+        if world > 1:
+            torch.distributed.barrier()
+
+    def max_over_ranks(v):
+        if world == 1:
+            return v
+        t = torch.tensor([v], dtype=torch.float64, device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        return float(t.item())
+
+    # ---- batched mixed objective + gradient (the metric)
+    for _ in range(args.warmup):
+        ev.objective_grad_device(Xd, obj, grad, MZ_MIXED)
+    ev.sync()
+    barrier()
+    torch.cuda.synchronize()
+    ev.sync()
+    ev.kernel_times()
+    ev.profile(True)
+    l0 = ev.launches()
+    clocks = ClockSampler(local)
+    clocks.start()
+    start = torch.cuda.Event(enable_timing=True)
+    end = torch.cuda.Event(enable_timing=True)
+    start.record(stream)
+    for _ in range(args.steps):
+        ev.objective_grad_device(Xd, obj, grad, MZ_MIXED)
+    end.record(stream)
+    end.synchronize()
+    ev.sync()
+    clk = clocks.stop()
+    launches = ev.launches() - l0
+    kt = ev.kernel_times()
+    ev.profile(False)
+    barrier()
+    torch.cuda.synchronize()
+    ms = max_over_ranks(start.elapsed_time(end))
+    value = world * args.ncand * args.steps / (ms * 1e-3)
+
+    # ---- FP64 plain objective, one candidate per launch
+    x1 = Xd[:1].contiguous()
+    o1 = torch.empty(1, dtype=torch.float64, device=dev)
+    for _ in range(max(3, args.warmup)):
+        ev.objective_device(x1, o1, MZ_FP64)
+    ev.sync()
+    barrier()
+    k64 = max(5, 4 * args.steps)
+    s2 = torch.cuda.Event(enable_timing=True)
+    e2 = torch.cuda.Event(enable_timing=True)
+    s2.record(stream)
+    for _ in range(k64):
+        ev.objective_device(x1, o1, MZ_FP64)
+    e2.record(stream)
+    e2.synchronize()
+    ms64 = max_over_ranks(s2.elapsed_time(e2))
+    fp64_rate = world * k64 / (ms64 * 1e-3)
+
+    # ---- end to end through the host API (pinned host buffers)
+    ph = torch.tensor(X, dtype=torch.float64).pin_memory()
+    oh = torch.empty(args.ncand, dtype=torch.float64).pin_memory()
+    gh = torch.empty((args.ncand, P), dtype=torch.float64).pin_memory()
+    from meamzilla_b200._lib import check, lib
+    import ctypes as C
+
+    def host_step():
+        check(lib().mz_objective_grad(ev.handle, args.ncand, C.c_void_p(ph.data_ptr()), MZ_MIXED,
+                                      C.c_void_p(oh.data_ptr()), C.c_void_p(gh.data_ptr())))
+    host_step()
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        host_step()
+    t_e2e = max_over_ranks(time.perf_counter() - t0)
+    e2e = world * args.ncand * args.steps / t_e2e
+
+    if rank != 0:
+        if world > 1:
+            torch.distributed.destroy_process_group()
+        return
+
+    # ---- roofline of the dominant kernel
+    hbm, hbm_src = measured_peaks()
+    fp32_peak = alu_peak(local, MZ_MIXED)
+    fp64_peak = alu_peak(local, MZ_FP64)
+    b32, fwd = algorithmic(stats, args.ncand, P)
+    dom = max(kt, key=lambda k: kt[k][0])
+    dom_ms = kt[dom][0] / kt[dom][1]
+    # flops of the dominant kernel: the forward pass is 1x, the adjoint 2x of the forward count
+    kflops = {"k_atoms": fwd * args.ncand, "k_adj": 2 * fwd * args.ncand}.get(dom, 3 * fwd * args.ncand)
+    roof = {"bound": "hbm", "kernel": dom, "achieved": b32 / (dom_ms * 1e-3) / 1e9, "peak": hbm, "unit": "GB/s",
+            "frac": b32 / (dom_ms * 1e-3) / 1e9 / hbm, "traffic": None, "algorithmic_bytes": b32,
+            "peak_source": hbm_src + " (MEASURED_PEAKS.json hbm_gbs)"}
+    roof_alu = {"bound": "fp32", "kernel": dom, "achieved": kflops / (dom_ms * 1e-3) / 1e12, "peak": fp32_peak,
+                "unit": "TFLOP/s", "frac": kflops / (dom_ms * 1e-3) / 1e12 / fp32_peak, "algorithmic_flops": kflops,
+                "peak_source": "measured FMA stream, FP32 (FP64: %.1f TFLOP/s)" % fp64_peak}
+
+    line = {
+        "metric": METRIC, "value": value, "unit": "evals/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic (seeded generator, meamzilla_b200/synth.py)",
+        "config": {"workload": WORKLOAD, "ncells": stats["ncells"], "natoms": stats["natoms"],
+                   "npairs": stats["npairs"], "ntriplets": stats["ntriplets"], "ncoeff": P,
+                   "candidates_per_step_per_gpu": args.ncand, "precision": "mixed (FP32 splines, FP64 sums)",
+                   "l2": "inputs larger than L2: pair streams %.2f GB" % (stats["npairs"] * 36 / 1e9)},
+        "fp64_plain": {"value": fp64_rate, "unit": "objective evals/s", "ms_per_eval": ms64 / k64,
+                       "candidates_per_launch": 1},
+        "ratio_vs_fp64_plain": value / fp64_rate,
+        "accuracy_vs_fp64": accuracy,
+        "kernels_ms_per_step": {k: kt[k][0] / args.steps for k in kt},
+        "roofline": roof,
+        "roofline_alu": roof_alu,
+        "e2e": {"value": e2e, "unit": "evals/s", "h2d_bytes_per_step": args.ncand * P * 8,
+                "d2h_bytes_per_step": args.ncand * (P + 1) * 8},
+        "gpu_launches": launches,
+        "clocks": clk,
+    }
+    if world == 1 and not args.no_cpu_baseline:
+        stats["rows_per_cell"] = _rows_per_cell(db.view())
+        res, err = cpu_reference(spec, cells, stats, P, reps=3)
+        if res is not None:
+            line["cpu_baseline"] = {"value": res["objgrad_evals_per_s"], "unit": "evals/s", "cores": res["cores"],
+                                    "kind": "reference", "sample": res["sample"],
+                                    "objective_evals_per_s": res["obj_evals_per_s"]}
+        else:
+            line["cpu_baseline"] = {"value": None, "unavailable": err}
+    print(json.dumps(line))
+    if world > 1:
+        torch.distributed.destroy_process_group()
+
+
+def main():
+    args = parse_args()
+    world, rank, local = dist_setup(args)
+    if args.impl == "reference":
+        run_reference_arm(args, world, rank)
+    else:
+        run_mine(args, world, rank, local)
+
+
+if __name__ == "__main__":
+    main()

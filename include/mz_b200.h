@@ -232,6 +232,30 @@ void *mz_stream(mz_ctx *ctx);
 /* Counters since mz_create: kernel launches issued by this context. */
 mz_status mz_launch_count(const mz_ctx *ctx, int64_t *launches);
 
+/* Kernels of the evaluator, for per-kernel timing. */
+enum {
+  MZ_K_PREP = 0,    /* coefficients -> knot and evaluation tables          */
+  MZ_K_ATOMS,       /* densities, embedding, per-slot reaction vectors      */
+  MZ_K_GATHER,      /* per-atom forces, force residuals                     */
+  MZ_K_CELLS,       /* per-cell energy, stress, residual entries            */
+  MZ_K_FINAL,       /* sum of squares + punishments                         */
+  MZ_K_ADJ,         /* adjoint pass over the neighbour rows                 */
+  MZ_K_GRAD_FINAL,  /* table gradient -> coefficient gradient               */
+  MZ_NKERNELS
+};
+const char *mz_kernel_name(int kernel);
+/* With on != 0 the context brackets every kernel it launches with CUDA
+ * events on its own stream.  mz_kernel_times waits for the stream, adds the
+ * elapsed times of the launches recorded since the last call to ms[kernel]
+ * and their count to launches[kernel] (arrays of MZ_NKERNELS, zeroed by the
+ * caller), and forgets them. */
+mz_status mz_profile(mz_ctx *ctx, int on);
+mz_status mz_kernel_times(mz_ctx *ctx, double *ms, int64_t *launches);
+
+/* Measured CUDA-core throughput of the device (dependent-free FMA streams in
+ * FP64 or FP32, MZ_FP64 / MZ_MIXED), in TFLOP/s (2 flops per FMA). */
+mz_status mz_alu_peak(int device, int precision, double *tflops);
+
 #ifdef __cplusplus
 }
 #endif

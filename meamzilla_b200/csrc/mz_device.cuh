@@ -9,18 +9,26 @@ namespace mzb {
 constexpr int MAX_SPLINES = 64;     // splines in one potential (8 types MEAM: 36+8+8+36+8)
 constexpr int BLOCK_SLOTS = 256;    // pair slots (threads) of one atom block
 constexpr int BLOCK_ATOMS = 64;     // atoms of one atom block
+constexpr int MAX_G_KNOTS = 16;     // g spline knots the adjoint's per-thread tables hold
+constexpr int ADJ_WARPS = BLOCK_SLOTS / 32;
 
 // Geometry of one spline, shared by every candidate (knot positions never
 // change: Potential::check_if_similar, pot_list.cpp:165-174).
 struct SplineGeom {
   double x0, xN, step, invstep;
   double cut;   // xN * (1 + 1e-8): knot == -1 beyond it (spline.cpp:79)
+  float cutf;   // the same cut for FP32 cosines, widened by 4 FP32 ulps
   int n;        // knots
   int toff;     // offset of this spline in a candidate's table
+  int moff;     // offset of its refresh matrix d(ypp)/d(y, grad) [n][n+2]
+  int poff;     // offset of its per-interval cubic coefficients [n-1][4]
 };
 
 // A candidate's table, per spline at toff: y[n], ypp[n], grad[2]
-// (total tab_stride doubles per candidate).
+// (total tab_stride doubles per candidate).  Its evaluation table, per spline
+// at poff: for each knot interval k the cubic in the shift b,
+//   S = c0 + b (c1 + b (c2 + b c3)),   dS/dr = (c1 + b (2 c2 + 3 b c3)) / h,
+// (pow_stride doubles per candidate), computed in FP64 from y and ypp.
 
 struct DevDb {
   int ncells, natoms, nblocks;
@@ -48,6 +56,7 @@ struct DevPot {
   int ntypes;
   int nsplines;
   int tab_stride;     // doubles per candidate table
+  int pow_stride;     // doubles per candidate evaluation table
   int s_phi, s_rho, s_U, s_f, s_g;  // first spline of each group
   int embed_extrap;
   double energy_weight, stress_weight;

@@ -1,0 +1,520 @@
+// Forward kernels of the objective (see mz_device.cu for the call sequence).
+#pragma once
+
+#include "mz_spline.cuh"
+
+namespace mzb {
+
+// Per-atom outputs, [cand][AO_COUNT][natoms].
+enum { AO_AX = 0, AO_AY, AO_AZ, AO_E, AO_S0, AO_PEN = AO_S0 + 6, AO_RHO, AO_FSQ, AO_COUNT };
+// Per-slot triplet sums kept for the adjoint, [cand][AUX_COUNT][npairs]:
+//   G_p = sum_k g f_k,  H_p = sum_k g' f_k cos,  vk_p = sum_k g' f_k u_k.
+enum { AUX_G = 0, AUX_H, AUX_VX, AUX_VY, AUX_VZ, AUX_COUNT };
+// Per-cell adjoint seeds, [cand][CS_COUNT][ncells]: dF/dE_atom, dF/dS (6), dF/dpen.
+enum { CS_EPS = 0, CS_MU0, CS_KAPPA = CS_MU0 + 6, CS_COUNT };
+
+// ------------------------------------------------------------------ k_prep
+
+// Coefficient vectors -> per-candidate knot tables.  cmap has the table's
+// layout: cmap[toff+k] (knot k) and cmap[toff+2n+e] (end e) hold the
+// coefficient index, or -1 where the value is fixed and comes from base.
+__global__ void k_prep(int ncand, int P, const double *__restrict__ params, const double *__restrict__ base,
+                       const int *__restrict__ cmap, const SplineGeom *__restrict__ geom,
+                       const int *__restrict__ nat, int nsplines, int stride, double *__restrict__ tabs,
+                       int pstride, double *__restrict__ ptabs) {
+  const int c = blockIdx.x;
+  const int s = threadIdx.x;
+  if (c >= ncand || s >= nsplines) return;
+  const SplineGeom g = geom[s];
+  const double *pc = params + (size_t)c * P;
+  double *t = tabs + (size_t)c * stride + g.toff;
+  const double *bt = base + g.toff;
+  const int *cm = cmap + g.toff;
+  const int n = g.n;
+  for (int k = 0; k < n; ++k) t[k] = cm[k] >= 0 ? pc[cm[k]] : bt[k];
+  for (int e = 0; e < 2; ++e) t[2 * n + e] = cm[2 * n + e] >= 0 ? pc[cm[2 * n + e]] : bt[2 * n + e];
+  // Spline3Eq::refresh_basis (spline3eq.cpp:192-225)
+  double u[64];
+  double *y = t, *ypp = t + n;
+  const double inv = g.invstep;
+  const double gl = t[2 * n], gr = t[2 * n + 1];
+  if (nat[2 * s]) {
+    ypp[0] = 0;
+    u[0] = 0;
+  } else {
+    ypp[0] = -0.5;
+    u[0] = (3.0 * inv) * ((y[1] - y[0]) * inv - gl);
+  }
+  for (int i = 1; i < n - 1; ++i) {
+    double p = 0.5 * ypp[i - 1] + 2.0;
+    ypp[i] = (-0.5) / p;
+    double ui = (y[i + 1] - y[i]) * inv - (y[i] - y[i - 1]) * inv;
+    u[i] = (6.0 * ui * 0.5 * inv - 0.5 * u[i - 1]) / p;
+  }
+  double qn, un;
+  if (nat[2 * s + 1]) {
+    qn = un = 0.0;
+  } else {
+    qn = 0.5;
+    un = (3.0 * inv) * (gr - (y[n - 1] - y[n - 2]) * inv);
+  }
+  ypp[n - 1] = (un - qn * u[n - 2]) / (qn * ypp[n - 2] + 1.0);
+  for (int k = n - 2; k >= 0; --k) ypp[k] = ypp[k] * ypp[k + 1] + u[k];
+  // evaluation table: the cubic of every interval in its shift
+  double *pc4 = ptabs + (size_t)c * pstride + g.poff;
+  const double H = g.step * g.step / 6.0;
+  for (int k = 0; k < n - 1; ++k) {
+    pc4[4 * k] = y[k];
+    pc4[4 * k + 1] = y[k + 1] - y[k] - (2.0 * ypp[k] + ypp[k + 1]) * H;
+    pc4[4 * k + 2] = 3.0 * ypp[k] * H;
+    pc4[4 * k + 3] = (ypp[k + 1] - ypp[k]) * H;
+  }
+}
+
+// ----------------------------------------------------------- atom blocks
+
+// Shared state of one atom block, common to the forward and adjoint kernels.
+struct BlockRows {
+  int atom_lo, na, slot_lo, nslot;
+};
+
+__device__ __forceinline__ BlockRows block_rows(const DevDb &db, int blk) {
+  BlockRows b;
+  b.atom_lo = db.blk_atom0[blk];
+  b.na = db.blk_atom0[blk + 1] - b.atom_lo;
+  b.slot_lo = db.pair_off[b.atom_lo];
+  b.nslot = db.pair_off[b.atom_lo + b.na] - b.slot_lo;
+  return b;
+}
+
+// Owner atom of slot t: the last a with a_lo[a] <= t.
+__device__ __forceinline__ int slot_owner(const int *a_lo, int na, int t) {
+  int lo = 0, hi = na;
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (a_lo[mid] <= t) lo = mid;
+    else hi = mid;
+  }
+  return lo;
+}
+
+__device__ __forceinline__ int pair_ij_index(int ti, int tj, int nt) {
+  return (ti <= tj) ? ti * nt + tj - (ti * (ti + 1)) / 2 : tj * nt + ti - (tj * (tj + 1)) / 2;
+}
+
+// Pair functions of one slot: phi, rho, f with slopes (pot_meam_spline.cpp:152-191).
+template <bool MEAM, typename R>
+struct PairEval {
+  R ux, uy, uz, r, invr;
+  R phi, dphi, rho, drho, f, df;
+  int kphi, krho, kf, tj, pij;
+  R bphi, brho, bf;
+};
+
+template <bool MEAM, typename R>
+__device__ __forceinline__ PairEval<MEAM, R> eval_pair(const DevDb &db, const DevPot &pot, const SplineGeom *sg,
+                                                      const R *ptab, int64_t gs, int ti) {
+  PairEval<MEAM, R> p;
+  const int64_t Np = db.npairs;
+  if (sizeof(R) == 8) {
+    p.ux = (R)db.pair_ux[gs]; p.uy = (R)db.pair_uy[gs]; p.uz = (R)db.pair_uz[gs]; p.r = (R)db.pair_r[gs];
+  } else {
+    p.ux = (R)db.pair_uxf[gs]; p.uy = (R)db.pair_uyf[gs]; p.uz = (R)db.pair_uzf[gs]; p.r = (R)db.pair_rf[gs];
+  }
+  p.invr = R(1) / p.r;
+  const int kn = db.pair_knot[gs];
+  p.kphi = (kn & 0xff) - 1;
+  p.krho = ((kn >> 8) & 0xff) - 1;
+  p.kf = ((kn >> 16) & 0xff) - 1;
+  p.tj = db.atom_type[db.pair_nbr[gs]];
+  p.pij = pair_ij_index(ti, p.tj, pot.ntypes);
+  p.phi = p.dphi = p.rho = p.drho = p.f = p.df = R(0);
+  p.bphi = p.brho = p.bf = R(0);
+  if (p.kphi >= 0) {
+    const SplineGeom &g = sg[pot.s_phi + p.pij];
+    p.bphi = sizeof(R) == 8 ? (R)db.pair_shift[gs] : (R)db.pair_shiftf[gs];
+    p.phi = cubic_val_grad<R>(ptab + g.poff, p.kphi, p.bphi, (R)g.invstep, p.dphi);
+  }
+  if (p.krho >= 0) {
+    const SplineGeom &g = sg[pot.s_rho + p.tj];
+    p.brho = sizeof(R) == 8 ? (R)db.pair_shift[Np + gs] : (R)db.pair_shiftf[Np + gs];
+    p.rho = cubic_val_grad<R>(ptab + g.poff, p.krho, p.brho, (R)g.invstep, p.drho);
+  }
+  if (MEAM && p.kf >= 0) {
+    const SplineGeom &g = sg[pot.s_f + p.pij];
+    p.bf = sizeof(R) == 8 ? (R)db.pair_shift[2 * Np + gs] : (R)db.pair_shiftf[2 * Np + gs];
+    p.f = cubic_val_grad<R>(ptab + g.poff, p.kf, p.bf, (R)g.invstep, p.df);
+  }
+  return p;
+}
+
+// ------------------------------------------------------------------ k_atoms
+
+// Shared-memory layout of k_atoms (dynamic), see atoms_smem_bytes():
+//   double red[11][BLOCK_SLOTS]       per-slot partials for the per-atom sums
+//   double a_dF[BLOCK_ATOMS], a_U[BLOCK_ATOMS]
+//   SplineGeom sg[nsplines]
+//   int a_lo[BLOCK_ATOMS+2]
+//   R ptab[pstride]                    this candidate's evaluation table
+//   R sx,sy,sz,sf[BLOCK_SLOTS]         pair data of the block
+template <typename R>
+__host__ __device__ inline size_t atoms_smem_bytes(int nsplines, int pstride) {
+  size_t b = sizeof(double) * (11 * BLOCK_SLOTS + 2 * BLOCK_ATOMS);
+  b += sizeof(SplineGeom) * nsplines;
+  b += sizeof(int) * (BLOCK_ATOMS + 2);
+  b = (b + 15) & ~size_t(15);
+  b += sizeof(R) * (pstride + 4);
+  b = (b + 15) & ~size_t(15);
+  b += sizeof(R) * 4 * BLOCK_SLOTS;
+  return b;
+}
+
+// One CTA per (atom block, candidate), one thread per pair slot.  A single
+// pass over each slot's row gives G_p, H_p and vk_p; the density
+// rho_i = sum_p rho_p + 1/2 sum_p f_p G_p (each j<k triplet seen from both
+// ends) and every force term follow from them (pot_meam_spline.cpp:143-269):
+//   V_p = u_p (phi'_p/2 + rho'_p U') + U' [u_p (f'_p G_p - f_p H_p / r_p)
+//                                          + f_p vk_p / r_p]
+// is the force atom i's terms add to atom i along slot p; the neighbour
+// receives -V_p (k_gather).
+template <bool MEAM, typename R, bool AUX>
+__global__ void __launch_bounds__(BLOCK_SLOTS)
+    k_atoms(DevDb db, DevPot pot, const SplineGeom *__restrict__ geom, const double *__restrict__ tabs,
+            const double *__restrict__ ptabs, double *__restrict__ Vout, double *__restrict__ aout,
+            double *__restrict__ aux) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int cand = blockIdx.y;
+  const int tid = threadIdx.x;
+  const int N = db.natoms;
+  const int64_t Np = db.npairs;
+
+  double *red = reinterpret_cast<double *>(smem_raw);
+  double *a_dF = red + 11 * BLOCK_SLOTS;
+  double *a_U = a_dF + BLOCK_ATOMS;
+  SplineGeom *sg = reinterpret_cast<SplineGeom *>(a_U + BLOCK_ATOMS);
+  int *a_lo = reinterpret_cast<int *>(sg + pot.nsplines);
+  size_t off = sizeof(double) * (11 * BLOCK_SLOTS + 2 * BLOCK_ATOMS) + sizeof(SplineGeom) * pot.nsplines +
+               sizeof(int) * (BLOCK_ATOMS + 2);
+  off = (off + 15) & ~size_t(15);
+  R *ptab = reinterpret_cast<R *>(smem_raw + off);
+  off += sizeof(R) * (pot.pow_stride + 4);
+  off = (off + 15) & ~size_t(15);
+  R *sx = reinterpret_cast<R *>(smem_raw + off);
+  R *sy = sx + BLOCK_SLOTS, *sz = sy + BLOCK_SLOTS, *sf = sz + BLOCK_SLOTS;
+
+  const BlockRows br = block_rows(db, blockIdx.x);
+  const double *tc = tabs + (size_t)cand * pot.tab_stride;
+  const double *pc = ptabs + (size_t)cand * pot.pow_stride;
+  for (int i = tid; i < pot.pow_stride; i += blockDim.x) ptab[i] = (R)pc[i];
+  for (int i = tid; i < pot.nsplines; i += blockDim.x) sg[i] = geom[i];
+  for (int a = tid; a <= br.na; a += blockDim.x) a_lo[a] = db.pair_off[br.atom_lo + a] - br.slot_lo;
+  __syncthreads();
+
+  const bool have = tid < br.nslot;
+  const int me = have ? slot_owner(a_lo, br.na, tid) : 0;
+  const int ti = db.atom_type[br.atom_lo + me];
+  const int64_t gs = (int64_t)br.slot_lo + tid;
+
+  PairEval<MEAM, R> pe;
+  if (have) {
+    pe = eval_pair<MEAM, R>(db, pot, sg, ptab, gs, ti);
+    sx[tid] = pe.ux; sy[tid] = pe.uy; sz[tid] = pe.uz; sf[tid] = pe.f;
+  }
+  __syncthreads();
+
+  // ---- the one pass over the row: G_p, H_p, vk_p
+  double G = 0, H = 0, vkx = 0, vky = 0, vkz = 0;
+  if (MEAM && have && (AUX || pe.f != R(0) || pe.df != R(0))) {
+    const SplineGeom gg = sg[pot.s_g + ti];
+    const R *gpc = ptab + gg.poff;
+    const R gx0 = (R)gg.x0, ginv = (R)gg.invstep;
+    const R gcut = g_cut<R>(gg);
+    const int row_lo = a_lo[me], row_hi = a_lo[me + 1];
+    for (int k = row_lo; k < row_hi; ++k) {
+      if (k == tid) continue;
+      const R fk = sf[k];
+      if (fk == R(0)) continue;
+      const R kx = sx[k], ky = sy[k], kz = sz[k];
+      const R cs = cos_exact(pe.ux, pe.uy, pe.uz, kx, ky, kz);
+      if (!(cs < gcut)) continue;  // g_knot == -1: not a triplet (triplet_meam_spline.cpp:66-70)
+      R b;
+      const int kk = g_knot<R>(cs, gx0, ginv, gg.n, b);
+      R dg;
+      const R gv = cubic_val_grad<R>(gpc, kk, b, ginv, dg);
+      const R dgfk = dg * fk;
+      G += (double)(gv * fk);
+      H += (double)(dgfk * cs);
+      vkx += (double)(dgfk * kx);
+      vky += (double)(dgfk * ky);
+      vkz += (double)(dgfk * kz);
+    }
+    if (AUX) {
+      double *ax = aux + (size_t)cand * AUX_COUNT * Np;
+      ax[AUX_G * Np + gs] = G;
+      ax[AUX_H * Np + gs] = H;
+      ax[AUX_VX * Np + gs] = vkx;
+      ax[AUX_VY * Np + gs] = vky;
+      ax[AUX_VZ * Np + gs] = vkz;
+    }
+  }
+  if (have) red[tid] = (double)pe.rho + (MEAM ? 0.5 * (double)pe.f * G : 0.0);
+  __syncthreads();
+
+  // ---- embedding (pot_meam_spline.cpp:208-223): one thread per atom
+  if (tid < br.na) {
+    const int ia = br.atom_lo + tid;
+    double rho = 0.0;
+    for (int s = a_lo[tid]; s < a_lo[tid + 1]; ++s) rho += red[s];
+    const SplineGeom &gU = sg[pot.s_U + db.atom_type[ia]];
+    const double w = db.cell_w[db.atom_cell[ia]];
+    double pen = 0.0;
+    const double lo = gU.x0, hi = gU.xN;
+    const double rho_raw = rho;
+    if (rho < lo) {
+      pen = w * 100.0 * 10. * (lo - rho) * (lo - rho);
+      if (!pot.embed_extrap) rho = lo;
+    } else if (rho > hi) {
+      pen = w * 100.0 * 10. * (rho - hi) * (rho - hi);
+      if (!pot.embed_extrap) rho = hi;
+    }
+    const PointEval U = spl_point(tc, gU, rho);  // FP64 table of this candidate
+    a_dF[tid] = U.grad;
+    a_U[tid] = U.val;
+    double *ao = aout + (size_t)cand * AO_COUNT * N;
+    ao[AO_PEN * N + ia] = pen;
+    ao[AO_RHO * N + ia] = rho_raw;
+  }
+  __syncthreads();
+
+  // ---- V_p and the slot's stress (stress.h:134-137; pot_meam_spline.cpp:171-173, 234-236, 265-268)
+  if (have) {
+    const double dF = a_dF[me];
+    const double ux = (double)pe.ux, uy = (double)pe.uy, uz = (double)pe.uz;
+    double cu = 0.5 * (double)pe.dphi + (double)pe.drho * dF;
+    double Vx = 0, Vy = 0, Vz = 0;
+    if (MEAM) {
+      const double ip = (double)pe.invr, fp = (double)pe.f;
+      cu += dF * ((double)pe.df * G - fp * ip * H);
+      const double ck = dF * fp * ip;
+      Vx = ck * vkx;
+      Vy = ck * vky;
+      Vz = ck * vkz;
+    }
+    Vx += ux * cu;
+    Vy += uy * cu;
+    Vz += uz * cu;
+    double *Vc = Vout + (size_t)cand * 3 * Np;
+    Vc[gs] = Vx;
+    Vc[Np + gs] = Vy;
+    Vc[2 * Np + gs] = Vz;
+    const double rr = db.pair_r[gs];
+    const double dx = db.pair_ux[gs], dy = db.pair_uy[gs], dz = db.pair_uz[gs];
+    red[1 * BLOCK_SLOTS + tid] = Vx;
+    red[2 * BLOCK_SLOTS + tid] = Vy;
+    red[3 * BLOCK_SLOTS + tid] = Vz;
+    red[4 * BLOCK_SLOTS + tid] = 0.5 * (double)pe.phi;
+    red[5 * BLOCK_SLOTS + tid] = -(dx * (Vx * rr));
+    red[6 * BLOCK_SLOTS + tid] = -(dy * (Vy * rr));
+    red[7 * BLOCK_SLOTS + tid] = -(dz * (Vz * rr));
+    red[8 * BLOCK_SLOTS + tid] = -(dx * (Vy * rr));
+    red[9 * BLOCK_SLOTS + tid] = -(dy * (Vz * rr));
+    red[10 * BLOCK_SLOTS + tid] = -(dz * (Vx * rr));
+  }
+  __syncthreads();
+  if (tid < br.na) {
+    const int ia = br.atom_lo + tid;
+    double acc[10];
+#pragma unroll
+    for (int q = 0; q < 10; ++q) acc[q] = 0.0;
+    for (int s = a_lo[tid]; s < a_lo[tid + 1]; ++s) {
+#pragma unroll
+      for (int q = 0; q < 10; ++q) acc[q] += red[(q + 1) * BLOCK_SLOTS + s];
+    }
+    double *ao = aout + (size_t)cand * AO_COUNT * N;
+    ao[AO_AX * N + ia] = acc[0];
+    ao[AO_AY * N + ia] = acc[1];
+    ao[AO_AZ * N + ia] = acc[2];
+    ao[AO_E * N + ia] = acc[3] + a_U[tid];
+#pragma unroll
+    for (int q = 0; q < 6; ++q) ao[(AO_S0 + q) * N + ia] = acc[4 + q];
+  }
+}
+
+// ----------------------------------------------------------------- k_gather
+
+// F_i = sum of V over the atom's own slots - sum of V over the slots whose
+// neighbour is i; then the force residual w (F - F0) (potential.cpp:468-478)
+// and, for the adjoint, lambda_i = dF/dF_i = 2 w e_i.
+__global__ void k_gather(DevDb db, const double *__restrict__ V, double *__restrict__ aout,
+                         double *__restrict__ forces, double *__restrict__ errvec, int esize,
+                         double *__restrict__ lam) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int c = blockIdx.y;
+  const int N = db.natoms;
+  if (i >= N) return;
+  const int64_t Np = db.npairs;
+  double *ao = aout + (size_t)c * AO_COUNT * N;
+  const double *Vc = V + (size_t)c * 3 * Np;
+  double fx = ao[AO_AX * N + i], fy = ao[AO_AY * N + i], fz = ao[AO_AZ * N + i];
+  for (int q = db.in_off[i]; q < db.in_off[i + 1]; ++q) {
+    const int s = db.in_slot[q];
+    fx -= Vc[s];
+    fy -= Vc[Np + s];
+    fz -= Vc[2 * Np + s];
+  }
+  const int cell = db.atom_cell[i];
+  const double w = db.cell_w[cell];
+  const double rx = w * (fx - db.force0[3 * i]);
+  const double ry = w * (fy - db.force0[3 * i + 1]);
+  const double rz = w * (fz - db.force0[3 * i + 2]);
+  ao[AO_FSQ * N + i] = rx * rx + ry * ry + rz * rz;
+  if (forces) {
+    double *F = forces + (size_t)c * 3 * N;
+    F[3 * i] = fx;
+    F[3 * i + 1] = fy;
+    F[3 * i + 2] = fz;
+  }
+  if (errvec) {
+    const int a0 = db.cell_atom0[cell];
+    double *e = errvec + (size_t)c * esize + 7 * (cell + 1) + 3 * a0 + 3 * (i - a0);
+    e[0] = rx;
+    e[1] = ry;
+    e[2] = rz;
+  }
+  if (lam) {
+    double *L = lam + (size_t)c * 3 * N;
+    L[i] = 2.0 * w * rx;
+    L[N + i] = 2.0 * w * ry;
+    L[2 * N + i] = 2.0 * w * rz;
+  }
+}
+
+// ------------------------------------------------------------------ k_cells
+
+// One warp per cell (potential.cpp:450-485); with `seeds`, also the adjoint
+// seeds dF/dE_atom, dF/dS_cell and dF/dpen of the cell.
+__global__ void k_cells(DevDb db, DevPot pot, const double *__restrict__ aout, double *__restrict__ cellobj,
+                        double *__restrict__ errvec, int esize, double *__restrict__ energy,
+                        double *__restrict__ stress, double *__restrict__ seeds) {
+  const int cell = blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32;
+  const int lane = threadIdx.x & 31;
+  const int c = blockIdx.y;
+  if (cell >= db.ncells) return;
+  const int N = db.natoms;
+  const double *ao = aout + (size_t)c * AO_COUNT * N;
+  const int a0 = db.cell_atom0[cell], a1 = db.cell_atom0[cell + 1];
+  double v[9];
+#pragma unroll
+  for (int q = 0; q < 9; ++q) v[q] = 0.0;
+  for (int a = a0 + lane; a < a1; a += 32) {
+    v[0] += ao[AO_E * N + a];
+#pragma unroll
+    for (int q = 0; q < 6; ++q) v[1 + q] += ao[(AO_S0 + q) * N + a];
+    v[7] += ao[AO_PEN * N + a];
+    v[8] += ao[AO_FSQ * N + a];
+  }
+#pragma unroll
+  for (int q = 0; q < 9; ++q)
+    for (int o = 16; o > 0; o >>= 1) v[q] += __shfl_down_sync(0xffffffffu, v[q], o);
+  if (lane == 0) {
+    const int na = a1 - a0;
+    const double w = db.cell_w[cell];
+    const double E = v[0] / na;
+    const double ew = w * db.cell_ew[cell] * pot.energy_weight;
+    const double eE = ew * na * (E - db.cell_e0[cell]);
+    double sum = eE * eE;
+    double eS[6], sig[6];
+    const double sw = w * db.cell_sw[cell] * pot.stress_weight;
+    for (int q = 0; q < 6; ++q) {
+      sig[q] = v[1 + q] / db.cell_vol[cell];
+      eS[q] = sw * (sig[q] - db.cell_s0[6 * cell + q]);
+      sum += eS[q] * eS[q];
+    }
+    sum += v[8];
+    const double cons = v[7];
+    sum += cons * cons;
+    cellobj[(size_t)c * db.ncells + cell] = sum;
+    if (errvec) {
+      double *e = errvec + (size_t)c * esize + 7 * cell + 3 * a0;
+      e[0] = eE;
+      for (int q = 0; q < 6; ++q) e[1 + q] = eS[q];
+      errvec[(size_t)c * esize + 7 * db.ncells + 3 * N + cell] = cons;
+    }
+    if (energy) energy[(size_t)c * db.ncells + cell] = E;
+    if (stress)
+      for (int q = 0; q < 6; ++q) stress[((size_t)c * db.ncells + cell) * 6 + q] = sig[q];
+    if (seeds) {
+      double *sd = seeds + (size_t)c * CS_COUNT * db.ncells;
+      sd[CS_EPS * db.ncells + cell] = 2.0 * eE * ew;
+      for (int q = 0; q < 6; ++q) sd[(CS_MU0 + q) * db.ncells + cell] = 2.0 * eS[q] * sw / db.cell_vol[cell];
+      sd[CS_KAPPA * db.ncells + cell] = 2.0 * cons;
+    }
+  }
+}
+
+// ------------------------------------------------------------------ k_final
+
+// Sum of squares over cells + the style's punishment entries.
+__device__ __forceinline__ double f_max_y(const DevPot &pot, const SplineGeom *geom, const double *tab, int *which) {
+  // signed largest-|y| knot over the f splines (spline.cpp:58-67, pot_fns.cpp:223-234)
+  double my = 0.0;
+  int at = -1;
+  const int nf = pot.ntypes * (pot.ntypes + 1) / 2;
+  for (int f = 0; f < nf; ++f) {
+    const SplineGeom &g = geom[pot.s_f + f];
+    double sm = 0.0;
+    int sat = -1;
+    for (int k = 0; k < g.n; ++k) {
+      const double y = tab[g.toff + k];
+      if (fabs(sm) < fabs(y)) {
+        sm = y;
+        sat = g.toff + k;
+      }
+    }
+    if (fabs(my) < fabs(sm)) {
+      my = sm;
+      at = sat;
+    }
+  }
+  if (which) *which = at;
+  return my;
+}
+
+__global__ void k_final(DevDb db, DevPot pot, const SplineGeom *__restrict__ geom,
+                        const double *__restrict__ tabs, const double *__restrict__ cellobj,
+                        double *__restrict__ obj, double *__restrict__ errvec, int esize) {
+  __shared__ double part[256];
+  const int c = blockIdx.x;
+  const int t = threadIdx.x;
+  double s = 0.0;
+  for (int i = t; i < db.ncells; i += blockDim.x) s += cellobj[(size_t)c * db.ncells + i];
+  part[t] = s;
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if (t < o) part[t] += part[t + o];
+    __syncthreads();
+  }
+  if (t == 0) {
+    double total = part[0];
+    const double *tab = tabs + (size_t)c * pot.tab_stride;
+    double *ev = errvec ? errvec + (size_t)c * esize + 8 * db.ncells + 3 * db.natoms : nullptr;
+    if (pot.style == MZ_STYLE_MEAM_SPLINE) {
+      // f-potential magnitude punishment (pot_meam_spline.cpp:274-278)
+      const double m = fabs(f_max_y(pot, geom, tab, nullptr));
+      const double fe = 100. * 25. * (1.0 - m) * (1.0 - m);
+      total += fe * fe;
+      if (ev) ev[0] = fe;
+    } else {
+      // U'(mid-range) punishment per type (pot_eam_spline.cpp:211-218)
+      for (int ty = 0; ty < pot.ntypes; ++ty) {
+        const SplineGeom &g = geom[pot.s_U + ty];
+        const double e = 100. * spl_point(tab, g, 0.5 * (g.x0 + g.xN)).grad;
+        total += e * e;
+        if (ev) ev[ty] = e;
+      }
+    }
+    obj[c] = total;
+  }
+}
+
+}  // namespace mzb

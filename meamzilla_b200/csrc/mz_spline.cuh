@@ -1,0 +1,166 @@
+// Device-side equidistant cubic spline arithmetic (value, slope, second
+// derivative, and the weights of each with respect to the knot table), plus
+// the exact triplet cosine.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "mz_device.cuh"
+
+namespace mzb {
+
+// Value and slope from (knot, shift): Spline3Eq::splint_comb(int, double,
+// double*) (spline3eq.h:110-122).
+template <typename R>
+__device__ __forceinline__ R spl_val_grad(const R *y, const R *ypp, int k, R b, R step6, R stepsq6,
+                                          R invstep, R &grad) {
+  const R a = R(1) - b;
+  const R p1 = y[k], p2 = y[k + 1], d1 = ypp[k], d2 = ypp[k + 1];
+  grad = (p2 - p1) * invstep + ((R(3) * b * b - R(1)) * d2 - (R(3) * a * a - R(1)) * d1) * step6;
+  return a * p1 + b * p2 + ((a * a * a - a) * d1 + (b * b * b - b) * d2) * stepsq6;
+}
+
+// Value and slope from the per-interval cubic c = (c0, c1, c2, c3) of the
+// evaluation table -- the same polynomial as above, with
+//   c0 = y[k], c1 = y[k+1] - y[k] - (2 ypp[k] + ypp[k+1]) h^2/6,
+//   c2 = 3 ypp[k] h^2/6, c3 = (ypp[k+1] - ypp[k]) h^2/6,
+// formed once in FP64 so that FP32 evaluation rounds only once per term.
+__device__ __forceinline__ void load_cubic(const float *c, float &c0, float &c1, float &c2, float &c3) {
+  const float4 q = *reinterpret_cast<const float4 *>(c);
+  c0 = q.x; c1 = q.y; c2 = q.z; c3 = q.w;
+}
+__device__ __forceinline__ void load_cubic(const double *c, double &c0, double &c1, double &c2, double &c3) {
+  const double2 q0 = *reinterpret_cast<const double2 *>(c), q1 = *reinterpret_cast<const double2 *>(c + 2);
+  c0 = q0.x; c1 = q0.y; c2 = q1.x; c3 = q1.y;
+}
+template <typename R>
+__device__ __forceinline__ R cubic_val_grad(const R *ptab, int k, R b, R invstep, R &grad) {
+  R c0, c1, c2, c3;
+  load_cubic(ptab + 4 * k, c0, c1, c2, c3);
+  grad = (c1 + b * (R(2) * c2 + R(3) * b * c3)) * invstep;
+  return c0 + b * (c1 + b * (c2 + b * c3));
+}
+template <typename R>
+__device__ __forceinline__ R cubic_val(const R *ptab, int k, R b) {
+  R c0, c1, c2, c3;
+  load_cubic(ptab + 4 * k, c0, c1, c2, c3);
+  return c0 + b * (c1 + b * (c2 + b * c3));
+}
+
+// Weights of the value (w*) and of the slope (d*) on the table entries
+// y[k], y[k+1], ypp[k], ypp[k+1] at shift b -- the transposes of the two
+// formulas above, used by the adjoint.
+template <typename R>
+struct SplW {
+  R wa, wb, wA, wB, da, db, dA, dB;
+};
+template <typename R>
+__device__ __forceinline__ SplW<R> spl_weights(R b, R step, R invstep) {
+  SplW<R> w;
+  const R a = R(1) - b, h6 = step / R(6), hh6 = step * step / R(6);
+  w.wa = a;
+  w.wb = b;
+  w.wA = (a * a * a - a) * hh6;
+  w.wB = (b * b * b - b) * hh6;
+  w.da = -invstep;
+  w.db = invstep;
+  w.dA = -(R(3) * a * a - R(1)) * h6;
+  w.dB = (R(3) * b * b - R(1)) * h6;
+  return w;
+}
+
+// Point evaluation with linear extrapolation beyond the end knots:
+// Spline3Eq::splint_comb(double, double*) (spline3eq.h:204-236) and
+// Spline3Eq::splint_grad2(double) (spline3eq.h:241-266).  FP64.
+struct PointEval {
+  double val, grad, grad2;
+  int k;          // interval, or -1 left / -2 right of the knots
+  double b;       // shift inside the interval
+};
+__device__ __forceinline__ PointEval spl_point(const double *tab, const SplineGeom &g, double r) {
+  const double *y = tab + g.toff, *ypp = y + g.n, *ge = y + 2 * g.n;
+  PointEval e;
+  if (r < g.x0) {
+    e.grad = ge[0];
+    e.val = y[0] + ge[0] * (r - g.x0);
+    e.grad2 = 0.0;
+    e.k = -1;
+    e.b = 0.0;
+    return e;
+  } else if (r > g.xN) {
+    e.grad = ge[1];
+    e.val = y[g.n - 1] + ge[1] * (r - g.xN);
+    e.grad2 = 0.0;
+    e.k = -2;
+    e.b = 0.0;
+    return e;
+  }
+  const double dr = r - g.x0;
+  int k = (dr < 0) ? 0 : int(dr * g.invstep);
+  if (k >= g.n - 1) k = g.n - 2;
+  const double b = (dr - k * g.step) * g.invstep;
+  e.val = spl_val_grad<double>(y, ypp, k, b, g.step / 6.0, g.step * g.step / 6.0, g.invstep, e.grad);
+  e.grad2 = (1.0 - b) * ypp[k] + b * ypp[k + 1];
+  e.k = k;
+  e.b = b;
+  return e;
+}
+
+// Adds cv * d(value)/d(table) + cd * d(slope)/d(table) of a point evaluation
+// to the spline's table gradient `acc` (same layout as its table slice).
+template <class Add>
+__device__ __forceinline__ void spl_point_adjoint(const SplineGeom &g, const PointEval &e, double r, double cv,
+                                                  double cd, Add add) {
+  const int n = g.n;
+  if (e.k == -1) {  // y0 + grad0 (r - x0)
+    add(0, cv);
+    add(2 * n, cv * (r - g.x0) + cd);
+  } else if (e.k == -2) {
+    add(n - 1, cv);
+    add(2 * n + 1, cv * (r - g.xN) + cd);
+  } else {
+    const SplW<double> w = spl_weights<double>(e.b, g.step, g.invstep);
+    add(e.k, cv * w.wa + cd * w.da);
+    add(e.k + 1, cv * w.wb + cd * w.db);
+    add(n + e.k, cv * w.wA + cd * w.dA);
+    add(n + e.k + 1, cv * w.wB + cd * w.dB);
+  }
+}
+
+// Knot + shift of cos(theta) on the g grid.  The reference bisects
+// (spline.cpp:74-99); the interval found here is the same except within an
+// ulp of a knot, where the spline's value and slope agree to rounding.
+template <typename R>
+__device__ __forceinline__ int g_knot(R c, R x0, R invstep, int n, R &b) {
+  const R t = (c - x0) * invstep;
+  int k = (int)floor(t);
+  k = k < 0 ? 0 : (k > n - 2 ? n - 2 : k);
+  b = t - R(k);
+  return k;
+}
+
+// cos(theta) exactly as Triplet::setup_triplet: x*x' + y*y' + z*z' with no
+// fused multiply-add (triplet.cpp:34-40, vect.h:137-141).
+__device__ __forceinline__ double cos_exact(double ax, double ay, double az, double bx, double by, double bz) {
+  return __dadd_rn(__dadd_rn(__dmul_rn(ax, bx), __dmul_rn(ay, by)), __dmul_rn(az, bz));
+}
+__device__ __forceinline__ float cos_exact(float ax, float ay, float az, float bx, float by, float bz) {
+  return __fadd_rn(__fadd_rn(__fmul_rn(ax, bx), __fmul_rn(ay, by)), __fmul_rn(az, bz));
+}
+
+// Upper cut of the g grid in the kernel's arithmetic.  FP64 uses the
+// reference's x_N (1 + 1e-8) (spline.cpp:79).  In FP32 a cosine of
+// collinear neighbours rounds to 1.0f, which must stay a triplet as it is in
+// FP64, so the cut is widened by a few FP32 ulps.
+template <typename R>
+__device__ __forceinline__ R g_cut(const SplineGeom &g);
+template <>
+__device__ __forceinline__ double g_cut<double>(const SplineGeom &g) {
+  return g.cut;
+}
+template <>
+__device__ __forceinline__ float g_cut<float>(const SplineGeom &g) {
+  return g.cutf;
+}
+
+}  // namespace mzb

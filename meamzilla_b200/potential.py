@@ -27,6 +27,17 @@ __all__ = ["PotentialFile", "Database", "Evaluator", "Potential", "read_param", 
            "MZ_FP64", "MZ_MIXED", "MzError"]
 
 
+def _release(obj, fn: str) -> None:
+    """Free a handle; silent during interpreter shutdown."""
+    h = getattr(obj, "_h", None)
+    obj._h = None
+    if h and _lib._lib is not None:
+        try:
+            getattr(_lib._lib, fn)(h)
+        except Exception:
+            pass
+
+
 def read_param(path: str) -> Dict[str, List[str]]:
     """Parameter file as key -> tokens (Input::parse, src/input.h:47-77: the
     first line whose first token is the key wins; blank lines are dropped)."""
@@ -68,9 +79,7 @@ class PotentialFile:
             return cls.read(p)
 
     def __del__(self):
-        if getattr(self, "_h", None) and lib is not None:
-            lib().mz_pot_free(self._h)
-            self._h = None
+        _release(self, "mz_pot_free")
 
     @property
     def handle(self):
@@ -174,9 +183,7 @@ class Database:
         return cls(h, pot)
 
     def __del__(self):
-        if getattr(self, "_h", None):
-            lib().mz_db_free(self._h)
-            self._h = None
+        _release(self, "mz_db_free")
 
     @property
     def handle(self):
@@ -236,9 +243,7 @@ class Evaluator:
         self.esize = st["esize_cells"] + self.npen
 
     def __del__(self):
-        if getattr(self, "_h", None):
-            lib().mz_destroy(self._h)
-            self._h = None
+        _release(self, "mz_destroy")
 
     @property
     def handle(self):
@@ -282,6 +287,43 @@ class Evaluator:
         n = C.c_int64()
         check(lib().mz_launch_count(self._h, C.byref(n)))
         return n.value
+
+    # --- device-pointer interface (torch CUDA tensors), enqueued on stream()
+    def stream(self) -> int:
+        """The context's CUDA stream (cudaStream_t as an integer)."""
+        return lib().mz_stream(self._h) or 0
+
+    def objective_device(self, params, obj, precision=MZ_MIXED) -> None:
+        """params: (n, ncoeff) float64 CUDA tensor; obj: (n,) float64 CUDA tensor."""
+        n = params.shape[0]
+        check(lib().mz_objective_device(self._h, n, C.c_void_p(params.data_ptr()), int(precision),
+                                        C.c_void_p(obj.data_ptr()), None, None))
+
+    def objective_grad_device(self, params, obj, grad, precision=MZ_MIXED) -> None:
+        n = params.shape[0]
+        check(lib().mz_objective_grad_device(self._h, n, C.c_void_p(params.data_ptr()), int(precision),
+                                             C.c_void_p(obj.data_ptr()), C.c_void_p(grad.data_ptr())))
+
+    def sync(self) -> None:
+        check(lib().mz_sync(self._h))
+
+    def profile(self, on: bool = True) -> None:
+        check(lib().mz_profile(self._h, 1 if on else 0))
+
+    def kernel_times(self) -> dict:
+        """{kernel name: (total ms, launches)} since the last call."""
+        ms = np.zeros(_lib.MZ_NKERNELS)
+        cnt = np.zeros(_lib.MZ_NKERNELS, dtype=np.int64)
+        check(lib().mz_kernel_times(self._h, ptr(ms), ptr(cnt)))
+        return {lib().mz_kernel_name(k).decode(): (float(ms[k]), int(cnt[k])) for k in range(_lib.MZ_NKERNELS)
+                if cnt[k] > 0}
+
+
+def alu_peak(device: int = 0, precision=MZ_MIXED) -> float:
+    """Measured FMA throughput of the device in TFLOP/s (FP64 or FP32)."""
+    t = C.c_double()
+    check(lib().mz_alu_peak(int(device), int(precision), C.byref(t)))
+    return t.value
 
 
 class Potential:
