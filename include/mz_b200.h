@@ -252,6 +252,31 @@ const char *mz_kernel_name(int kernel);
 mz_status mz_profile(mz_ctx *ctx, int on);
 mz_status mz_kernel_times(mz_ctx *ctx, double *ms, int64_t *launches);
 
+/* Objective of one coefficient vector without allocating any device memory.
+ *
+ * This entry point has no counterpart in the reference.  It exists for
+ * callers that cannot call cudaMalloc: code running where the device
+ * allocator is off limits (inside another framework's memory pool or
+ * allocator hooks, in processes with a fixed device-memory budget, or on a
+ * path that must not add allocations or implicit synchronisation).  Instead
+ * of the context's buffers it uses one file-scope device array of
+ * MZ_NOALLOC_SCRATCH_BYTES (64 MiB) that every GPU loading the library holds
+ * until exit; the database, the potential's tables and all per-slot and
+ * per-atom scratch are staged there.  Databases that do not fit are rejected
+ * with MZ_ERR_RANGE (roughly up to 1e5 atoms / 2e5 pairs).
+ *
+ * Inputs and outputs are host memory: params[ncoeff] in, obj (the value
+ * Potential::compute returns) and, if non-null, forces[natoms][3] out.  FP64,
+ * synchronous, on the device named by settings->device, using the default
+ * stream.  The first call on a device looks up the array's device address
+ * (once per device); make that first call before any stream capture.  Every
+ * call reuses the same array and leaves the last call's contents in it, so
+ * calls that overlap on the GPU (from several host threads) race: serialise
+ * them. */
+#define MZ_NOALLOC_SCRATCH_BYTES (64u << 20)
+mz_status mz_objective_noalloc(const mz_db *db, const mz_pot *pot, const mz_settings *settings,
+                               const double *params, double *obj, double *forces);
+
 /* Measured CUDA-core throughput of the device (dependent-free FMA streams in
  * FP64 or FP32, MZ_FP64 / MZ_MIXED), in TFLOP/s (2 flops per FMA). */
 mz_status mz_alu_peak(int device, int precision, double *tflops);

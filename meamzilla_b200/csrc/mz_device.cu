@@ -32,6 +32,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -681,3 +682,257 @@ mz_status mz_launch_count(const mz_ctx *ctx, int64_t *launches) {
 }
 
 }  // extern "C"
+
+// ======================================================== no-allocation path
+
+// The one device array of mz_objective_noalloc.  In host code its name is
+// only a host-side stand-in; kernels get the device address looked up once
+// per device below.
+static __device__ __align__(256) unsigned char g_noalloc_scratch[MZ_NOALLOC_SCRATCH_BYTES];
+
+namespace {
+
+std::mutex g_noalloc_mutex;
+void *g_noalloc_addr[64] = {nullptr};
+
+// Sub-array placement inside the scratch array: 256-byte aligned slots.
+struct Carve {
+  size_t used = 0;
+  template <class T>
+  size_t take(size_t n) {
+    const size_t at = (used + 255) & ~size_t(255);
+    used = at + std::max<size_t>(n, 1) * sizeof(T);
+    return at;
+  }
+};
+
+}  // namespace
+
+extern "C" mz_status mz_objective_noalloc(const mz_db *dbh, const mz_pot *poth, const mz_settings *set,
+                                          const double *params, double *obj, double *forces) {
+  return guarded([&] {
+    if (!dbh || !poth || !set || !params || !obj) throw Failure{MZ_ERR_ARG, "null argument"};
+    const Db &db = dbh->db;
+    const Pot &pot = poth->pot;
+    const bool meam = pot.style == MZ_STYLE_MEAM_SPLINE;
+    if (db.max_row > BLOCK_SLOTS)
+      throw Failure{MZ_ERR_RANGE, "neighbour row of " + std::to_string(db.max_row) +
+                                      " pairs exceeds the kernel limit of " + std::to_string(BLOCK_SLOTS)};
+    if (pot.nsplines() > MAX_SPLINES) throw Failure{MZ_ERR_RANGE, "too many splines"};
+    const int N = db.natoms, NC = db.ncells, ns = pot.nsplines();
+    const int64_t Np = db.npairs;
+
+    // ---- host images of the potential structure (as mz_create builds them)
+    std::vector<SplineGeom> geom(ns);
+    std::vector<int> nat(2 * ns);
+    int toff = 0, poff = 0;
+    for (int s = 0; s < ns; ++s) {
+      const Spline3 &sp = pot.spline(s);
+      SplineGeom &g = geom[s];
+      g.x0 = sp.x[0];
+      g.xN = sp.x[sp.nknots - 1];
+      g.step = sp.step;
+      g.invstep = sp.invstep;
+      g.cut = sp.x.back() * (1. + 1.e-8);
+      g.cutf = (float)g.cut;
+      g.n = sp.nknots;
+      g.toff = toff;
+      g.moff = 0;
+      g.poff = poff;
+      toff += 2 * sp.nknots + 2;
+      poff += 4 * (sp.nknots - 1);
+      nat[2 * s] = sp.nat[0];
+      nat[2 * s + 1] = sp.nat[1];
+    }
+    const int stride = toff, pstride = poff;
+    std::vector<double> base(stride, 0.0);
+    std::vector<int> cmap(stride, -1);
+    int ci = 0;
+    for (int s = 0; s < ns; ++s) {
+      const Spline3 &sp = pot.spline(s);
+      const int o = geom[s].toff, n = sp.nknots;
+      for (int k = 0; k < n; ++k) {
+        base[o + k] = sp.y[k];
+        if (!sp.y_fixed[k]) cmap[o + k] = ci++;
+      }
+      for (int e = 0; e < 2; ++e) {
+        base[o + 2 * n + e] = sp.grad[e];
+        if (!sp.grad_fixed[e] && !sp.nat[e]) cmap[o + 2 * n + e] = ci++;
+      }
+    }
+    const int P = ci;
+    DevPot dp{};
+    dp.style = pot.style;
+    dp.ntypes = pot.ntypes;
+    dp.nsplines = ns;
+    dp.tab_stride = stride;
+    dp.pow_stride = pstride;
+    dp.s_phi = pot.spline_index(G_PHI, 0);
+    dp.s_rho = pot.spline_index(G_RHO, 0);
+    dp.s_U = pot.spline_index(G_U, 0);
+    dp.s_f = meam ? pot.spline_index(G_F, 0) : 0;
+    dp.s_g = meam ? pot.spline_index(G_G, 0) : 0;
+    dp.embed_extrap = set->embed_extrap;
+    dp.energy_weight = set->energy_weight;
+    dp.stress_weight = set->stress_weight;
+
+    // ---- host images of the database
+    std::vector<int> off32(N + 1), inoff32(N + 1), inslot32(Np), knot32(Np);
+    for (int i = 0; i <= N; ++i) {
+      off32[i] = (int)db.pair_off[i];
+      inoff32[i] = (int)db.in_off[i];
+    }
+    std::vector<double> ux(Np), uy(Np), uz(Np), sh(3 * Np);
+    for (int64_t q = 0; q < Np; ++q) {
+      inslot32[q] = (int)db.in_slot[q];
+      knot32[q] = (db.pair_knot[3 * q] + 1) | ((db.pair_knot[3 * q + 1] + 1) << 8) |
+                  ((db.pair_knot[3 * q + 2] + 1) << 16);
+      ux[q] = db.pair_u[3 * q];
+      uy[q] = db.pair_u[3 * q + 1];
+      uz[q] = db.pair_u[3 * q + 2];
+      for (int k = 0; k < 3; ++k) sh[k * Np + q] = db.pair_shift[3 * q + k];
+    }
+    std::vector<int> blk(1, 0);
+    {
+      int slots = 0, atoms = 0;
+      for (int i = 0; i < N; ++i) {
+        const int n = (int)(db.pair_off[i + 1] - db.pair_off[i]);
+        if (atoms > 0 && (slots + n > BLOCK_SLOTS || atoms + 1 > BLOCK_ATOMS)) {
+          blk.push_back(i);
+          slots = 0;
+          atoms = 0;
+        }
+        slots += n;
+        atoms += 1;
+      }
+      blk.push_back(N);
+    }
+    const int nblocks = (int)blk.size() - 1;
+
+    // ---- placement inside the scratch array (size check before any device work)
+    Carve cv;
+    const size_t o_params = cv.take<double>(P), o_tabs = cv.take<double>(stride), o_ptabs = cv.take<double>(pstride),
+                 o_base = cv.take<double>(stride), o_cmap = cv.take<int>(stride), o_nat = cv.take<int>(2 * ns),
+                 o_geom = cv.take<SplineGeom>(ns);
+    const size_t o_atom0 = cv.take<int>(NC + 1), o_vol = cv.take<double>(NC), o_w = cv.take<double>(NC),
+                 o_ew = cv.take<double>(NC), o_sw = cv.take<double>(NC), o_e0 = cv.take<double>(NC),
+                 o_s0 = cv.take<double>(6 * (size_t)NC);
+    const size_t o_type = cv.take<int>(N), o_cell = cv.take<int>(N), o_f0 = cv.take<double>(3 * (size_t)N),
+                 o_off = cv.take<int>(N + 1), o_inoff = cv.take<int>(N + 1), o_inslot = cv.take<int>(Np),
+                 o_knot = cv.take<int>(Np), o_nbr = cv.take<int>(Np), o_r = cv.take<double>(Np),
+                 o_ux = cv.take<double>(Np), o_uy = cv.take<double>(Np), o_uz = cv.take<double>(Np),
+                 o_sh = cv.take<double>(3 * (size_t)Np), o_blk = cv.take<int>(nblocks + 1);
+    const size_t o_V = cv.take<double>(3 * (size_t)Np), o_aout = cv.take<double>((size_t)AO_COUNT * N),
+                 o_forces = cv.take<double>(3 * (size_t)N), o_cellobj = cv.take<double>(NC),
+                 o_obj = cv.take<double>(1);
+    if (cv.used > (size_t)MZ_NOALLOC_SCRATCH_BYTES)
+      throw Failure{MZ_ERR_RANGE, "database needs " + std::to_string(cv.used) +
+                                      " bytes of scratch; the no-allocation entry point holds " +
+                                      std::to_string((size_t)MZ_NOALLOC_SCRATCH_BYTES)};
+
+    // ---- per-device set-up: the array's device address, with that device current
+    ck(cudaSetDevice(set->device), "cudaSetDevice");
+    if (set->device < 0 || set->device >= 64) throw Failure{MZ_ERR_ARG, "device ordinal out of range"};
+    unsigned char *base_ptr = nullptr;
+    {
+      std::lock_guard<std::mutex> lk(g_noalloc_mutex);
+      if (!g_noalloc_addr[set->device]) {
+        void *p = nullptr;
+        ck(cudaGetSymbolAddress(&p, g_noalloc_scratch), "cudaGetSymbolAddress");
+        const size_t sa = atoms_smem_bytes<double>(ns, pstride);
+        ck(cudaFuncSetAttribute(k_atoms<true, double, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sa),
+           "smem attribute");
+        ck(cudaFuncSetAttribute(k_atoms<false, double, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sa),
+           "smem attribute");
+        g_noalloc_addr[set->device] = p;
+      }
+      base_ptr = static_cast<unsigned char *>(g_noalloc_addr[set->device]);
+    }
+    const size_t sa = atoms_smem_bytes<double>(ns, pstride);
+    ck(cudaFuncSetAttribute(meam ? (const void *)k_atoms<true, double, false> : (const void *)k_atoms<false, double, false>,
+                            cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sa),
+       "smem attribute");
+    auto put = [&](size_t at, const void *src, size_t bytes) {
+      if (bytes) ck(cudaMemcpy(base_ptr + at, src, bytes, cudaMemcpyHostToDevice), "cudaMemcpy H2D");
+    };
+    put(o_params, params, sizeof(double) * P);
+    put(o_base, base.data(), sizeof(double) * stride);
+    put(o_cmap, cmap.data(), sizeof(int) * stride);
+    put(o_nat, nat.data(), sizeof(int) * 2 * ns);
+    put(o_geom, geom.data(), sizeof(SplineGeom) * ns);
+    put(o_atom0, db.cell_atom0.data(), sizeof(int) * (NC + 1));
+    put(o_vol, db.cell_vol.data(), sizeof(double) * NC);
+    put(o_w, db.cell_weight.data(), sizeof(double) * NC);
+    put(o_ew, db.cell_eweight.data(), sizeof(double) * NC);
+    put(o_sw, db.cell_sweight.data(), sizeof(double) * NC);
+    put(o_e0, db.cell_energy0.data(), sizeof(double) * NC);
+    put(o_s0, db.cell_stress0.data(), sizeof(double) * 6 * NC);
+    put(o_type, db.atom_type.data(), sizeof(int) * N);
+    put(o_cell, db.atom_cell.data(), sizeof(int) * N);
+    put(o_f0, db.atom_force0.data(), sizeof(double) * 3 * N);
+    put(o_off, off32.data(), sizeof(int) * (N + 1));
+    put(o_inoff, inoff32.data(), sizeof(int) * (N + 1));
+    put(o_inslot, inslot32.data(), sizeof(int) * Np);
+    put(o_knot, knot32.data(), sizeof(int) * Np);
+    put(o_nbr, db.pair_nbr.data(), sizeof(int) * Np);
+    put(o_r, db.pair_r.data(), sizeof(double) * Np);
+    put(o_ux, ux.data(), sizeof(double) * Np);
+    put(o_uy, uy.data(), sizeof(double) * Np);
+    put(o_uz, uz.data(), sizeof(double) * Np);
+    put(o_sh, sh.data(), sizeof(double) * 3 * Np);
+    put(o_blk, blk.data(), sizeof(int) * (nblocks + 1));
+    // Nothing else needs clearing: every slot, atom and cell output below is
+    // written by its kernel before it is read.
+
+    auto D = [&](size_t at) { return static_cast<void *>(base_ptr + at); };
+    DevDb d{};
+    d.ncells = NC;
+    d.natoms = N;
+    d.npairs = Np;
+    d.nblocks = nblocks;
+    d.cell_atom0 = (const int *)D(o_atom0);
+    d.cell_vol = (const double *)D(o_vol);
+    d.cell_w = (const double *)D(o_w);
+    d.cell_ew = (const double *)D(o_ew);
+    d.cell_sw = (const double *)D(o_sw);
+    d.cell_e0 = (const double *)D(o_e0);
+    d.cell_s0 = (const double *)D(o_s0);
+    d.atom_type = (const int *)D(o_type);
+    d.atom_cell = (const int *)D(o_cell);
+    d.force0 = (const double *)D(o_f0);
+    d.pair_off = (const int *)D(o_off);
+    d.in_off = (const int *)D(o_inoff);
+    d.in_slot = (const int *)D(o_inslot);
+    d.pair_nbr = (const int *)D(o_nbr);
+    d.pair_r = (const double *)D(o_r);
+    d.pair_ux = (const double *)D(o_ux);
+    d.pair_uy = (const double *)D(o_uy);
+    d.pair_uz = (const double *)D(o_uz);
+    d.pair_shift = (const double *)D(o_sh);
+    d.pair_knot = (const int *)D(o_knot);
+    d.blk_atom0 = (const int *)D(o_blk);
+    const SplineGeom *dgeom = (const SplineGeom *)D(o_geom);
+    double *tabs = (double *)D(o_tabs), *ptabs = (double *)D(o_ptabs), *V = (double *)D(o_V),
+           *aout = (double *)D(o_aout), *dforces = (double *)D(o_forces), *cellobj = (double *)D(o_cellobj),
+           *dobj = (double *)D(o_obj);
+
+    k_prep<<<1, std::max(32, ((ns + 31) / 32) * 32)>>>(1, P, (const double *)D(o_params), (const double *)D(o_base),
+                                                       (const int *)D(o_cmap), dgeom, (const int *)D(o_nat), ns,
+                                                       stride, tabs, pstride, ptabs);
+    ck(cudaGetLastError(), "k_prep launch");
+    dim3 ga(nblocks, 1);
+    if (meam)
+      k_atoms<true, double, false><<<ga, BLOCK_SLOTS, sa>>>(d, dp, dgeom, tabs, ptabs, V, aout, nullptr);
+    else
+      k_atoms<false, double, false><<<ga, BLOCK_SLOTS, sa>>>(d, dp, dgeom, tabs, ptabs, V, aout, nullptr);
+    ck(cudaGetLastError(), "k_atoms launch");
+    k_gather<<<dim3((N + 255) / 256, 1), 256>>>(d, V, aout, dforces, nullptr, 0, nullptr);
+    ck(cudaGetLastError(), "k_gather launch");
+    k_cells<<<dim3((NC + 7) / 8, 1), 256>>>(d, dp, aout, cellobj, nullptr, 0, nullptr, nullptr, nullptr);
+    ck(cudaGetLastError(), "k_cells launch");
+    k_final<<<1, 256>>>(d, dp, dgeom, tabs, cellobj, dobj, nullptr, 0);
+    ck(cudaGetLastError(), "k_final launch");
+    ck(cudaMemcpy(obj, dobj, sizeof(double), cudaMemcpyDeviceToHost), "cudaMemcpy D2H");
+    if (forces) ck(cudaMemcpy(forces, dforces, sizeof(double) * 3 * N, cudaMemcpyDeviceToHost), "cudaMemcpy D2H");
+  });
+}
