@@ -19,64 +19,133 @@
 
 namespace mzb {
 
-// Shared-memory layout of k_adj (dynamic), see adj_smem_bytes().
+// g-table gradient of one knot interval in the cubic's power basis:
+// dc_q accumulates dF/dc_q of S(b) = c0 + c1 b + c2 b^2 + c3 b^3.  Its map to
+// the knot table follows from c0 = y_m, c1 = y_m+1 - y_m - (2 y''_m + y''_m+1) H,
+// c2 = 3 y''_m H, c3 = (y''_m+1 - y''_m) H with H = h^2/6.
+template <class Add>
+__device__ __forceinline__ void power_to_table(const SplineGeom &g, int m, double d0, double d1, double d2,
+                                               double d3, Add add) {
+  const double H = g.step * g.step / 6.0;
+  add(m, d0 - d1);
+  add(m + 1, d1);
+  add(g.n + m, -2.0 * H * d1 + 3.0 * H * d2 - H * d3);
+  add(g.n + m + 1, -H * d1 + H * d3);
+}
+
+constexpr int GACC_FLUSH_BLOCKS = 16;  // atom blocks between flushes of the per-thread g tables
+
+// Shared-memory layout of k_adj (dynamic), see adj_smem_bytes():
+//   double wtab[ADJ_WARPS][stride]          per-warp table gradients (FP64)
+//   float  ftab[ADJ_WARPS][stride]          per-warp pair-function gradients of one block (FP32)
+//   R4 gacc[gslots][MAX_G_KNOTS-1][BLOCK_SLOTS]  per-thread g-table gradients, power basis;
+//                                           gslots = ntypes (kept across blocks) or 1 (flushed each block)
+//   double red[BLOCK_SLOTS], a_chi[BLOCK_ATOMS], a_dF[BLOCK_ATOMS]
+//   SplineGeom sg[nsplines]; int a_lo[BLOCK_ATOMS+2]
+//   R ptab[pstride]
+//   R4 srow[BLOCK_SLOTS+8]  (u_x, u_y, u_z, f)              of every slot (zero padded)
+//   R4 sadj[BLOCK_SLOTS+8]  (a f', a f / r, Q_x, Q_y)        with Q = f Lambda / r
+//   R  sqz[BLOCK_SLOTS+8]   Q_z
 template <typename R>
-__host__ __device__ inline size_t adj_smem_bytes(int nsplines, int stride, int pstride, bool meam) {
-  size_t b = sizeof(double) * (size_t)ADJ_WARPS * stride;               // per-warp gradient tables
-  if (meam) b += sizeof(double) * 2 * MAX_G_KNOTS * BLOCK_SLOTS;         // per-thread g tables
-  b += sizeof(double) * (BLOCK_SLOTS + 2 * BLOCK_ATOMS);                 // red, a_chi, a_dF
+__host__ __device__ inline int adj_gslots(int ntypes, int ng) {
+  // keep one table per atom type while they fit in 64 KiB, else one, flushed every block
+  return ((size_t)ntypes * (ng - 1) * BLOCK_SLOTS * 4 * sizeof(R) <= 65536) ? ntypes : 1;
+}
+template <typename R>
+__host__ __device__ inline size_t adj_smem_bytes(int nsplines, int stride, int pstride, bool meam, int ntypes,
+                                                 int ng) {
+  size_t b = sizeof(double) * (size_t)ADJ_WARPS * stride + sizeof(float) * (size_t)ADJ_WARPS * stride;
+  b = (b + 31) & ~size_t(31);
+  if (meam) b += 4 * sizeof(R) * (size_t)adj_gslots<R>(ntypes, ng) * (ng - 1) * BLOCK_SLOTS;
+  b += sizeof(double) * (BLOCK_SLOTS + 2 * BLOCK_ATOMS);
   b += sizeof(SplineGeom) * nsplines;
   b += sizeof(int) * (BLOCK_ATOMS + 2);
-  b = (b + 15) & ~size_t(15);
+  b = (b + 31) & ~size_t(31);
   b += sizeof(R) * (pstride + 4);
-  b = (b + 15) & ~size_t(15);
-  b += sizeof(R) * 9 * BLOCK_SLOTS;
+  b = (b + 31) & ~size_t(31);
+  b += 9 * sizeof(R) * (BLOCK_SLOTS + 8);
   return b;
 }
 
 template <bool MEAM, typename R>
-__global__ void __launch_bounds__(BLOCK_SLOTS)
+__global__ void __launch_bounds__(BLOCK_SLOTS, 2)
     k_adj(DevDb db, DevPot pot, const SplineGeom *__restrict__ geom, const double *__restrict__ tabs,
-          const double *__restrict__ ptabs, const double *__restrict__ aout, const double *__restrict__ aux, const double *__restrict__ lam,
-          const double *__restrict__ seeds, double *__restrict__ partial) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+          const double *__restrict__ ptabs, const double *__restrict__ aout, const double *__restrict__ aux,
+          const double *__restrict__ lam, const double *__restrict__ seeds, double *__restrict__ partial) {
+  using R4 = typename Vec4<R>::T;
+  extern __shared__ __align__(32) unsigned char smem_raw[];
   const int cand = blockIdx.y;
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarp = blockDim.x >> 5;
   const int N = db.natoms, NC = db.ncells;
   const int64_t Np = db.npairs;
   const int stride = pot.tab_stride;
+  const int ng = MEAM ? pot.g_nmax : 2;  // per-thread tables sized by the largest g spline
+  const int nint = ng - 1;
+  const int gslots = MEAM ? adj_gslots<R>(pot.ntypes, ng) : 1;
 
   double *wtab = reinterpret_cast<double *>(smem_raw);
-  double *gpriv = wtab + (size_t)ADJ_WARPS * stride;
-  double *red = gpriv + (MEAM ? 2 * MAX_G_KNOTS * BLOCK_SLOTS : 0);
+  float *ftab = reinterpret_cast<float *>(wtab + (size_t)ADJ_WARPS * stride);
+  size_t off = sizeof(double) * (size_t)ADJ_WARPS * stride + sizeof(float) * (size_t)ADJ_WARPS * stride;
+  off = (off + 31) & ~size_t(31);
+  R4 *gacc = reinterpret_cast<R4 *>(smem_raw + off);
+  if (MEAM) off += 4 * sizeof(R) * (size_t)gslots * nint * BLOCK_SLOTS;
+  double *red = reinterpret_cast<double *>(smem_raw + off);
   double *a_chi = red + BLOCK_SLOTS;
   double *a_dF = a_chi + BLOCK_ATOMS;
   SplineGeom *sg = reinterpret_cast<SplineGeom *>(a_dF + BLOCK_ATOMS);
   int *a_lo = reinterpret_cast<int *>(sg + pot.nsplines);
-  size_t off = reinterpret_cast<unsigned char *>(a_lo + BLOCK_ATOMS + 2) - smem_raw;
-  off = (off + 15) & ~size_t(15);
+  off = reinterpret_cast<unsigned char *>(a_lo + BLOCK_ATOMS + 2) - smem_raw;
+  off = (off + 31) & ~size_t(31);
   R *ptab = reinterpret_cast<R *>(smem_raw + off);
   off += sizeof(R) * (pot.pow_stride + 4);
-  off = (off + 15) & ~size_t(15);
-  R *sx = reinterpret_cast<R *>(smem_raw + off);
-  R *sy = sx + BLOCK_SLOTS, *sz = sy + BLOCK_SLOTS, *sf = sz + BLOCK_SLOTS, *sal = sf + BLOCK_SLOTS,
-    *sbe = sal + BLOCK_SLOTS, *sqx = sbe + BLOCK_SLOTS, *sqy = sqx + BLOCK_SLOTS, *sqz = sqy + BLOCK_SLOTS;
+  off = (off + 31) & ~size_t(31);
+  R4 *srow = reinterpret_cast<R4 *>(smem_raw + off);
+  R4 *sadj = srow + BLOCK_SLOTS + 8;
+  R *sqz = reinterpret_cast<R *>(sadj + BLOCK_SLOTS + 8);
 
   const double *tc = tabs + (size_t)cand * stride;
   const double *pcand = ptabs + (size_t)cand * pot.pow_stride;
   for (int i = tid; i < pot.pow_stride; i += blockDim.x) ptab[i] = (R)pcand[i];
-  for (int i = tid; i < ADJ_WARPS * stride; i += blockDim.x) wtab[i] = 0.0;
+  for (int i = tid; i < ADJ_WARPS * stride; i += blockDim.x) {
+    wtab[i] = 0.0;
+    ftab[i] = 0.f;
+  }
   if (MEAM)
-    for (int i = tid; i < 2 * MAX_G_KNOTS * BLOCK_SLOTS; i += blockDim.x) gpriv[i] = 0.0;
+    for (int i = tid; i < gslots * nint * BLOCK_SLOTS; i += blockDim.x) gacc[i] = R4{};
   for (int i = tid; i < pot.nsplines; i += blockDim.x) sg[i] = geom[i];
   double *wt = wtab + (size_t)warp * stride;
-  auto add_w = [&](int idx, double v) { atomicAdd(wt + idx, v); };
+  float *ft = ftab + (size_t)warp * stride;
+  auto add_f = [&](int idx, double v) { atomicAdd(ft + idx, (float)v); };
 
   const double *ao = aout + (size_t)cand * AO_COUNT * N;
   const double *ax = aux + (size_t)cand * AUX_COUNT * Np;
   const double *L = lam + (size_t)cand * 3 * N;
   const double *sd = seeds + (size_t)cand * CS_COUNT * NC;
 
+  // Flush of the per-thread g tables (power basis) into the warp's FP64
+  // table: one warp-wide sum per (type, interval, coefficient).
+  auto flush_gacc = [&](bool have_t, int t_mine) {
+    for (int t = 0; t < pot.ntypes; ++t) {
+      const int slot = gslots == 1 ? 0 : t;
+      const SplineGeom &gg = sg[pot.s_g + t];
+      for (int m = 0; m < gg.n - 1; ++m) {
+        R4 v = R4{};
+        if (gslots > 1 || (have_t && t_mine == t)) v = gacc[(slot * nint + m) * BLOCK_SLOTS + tid];
+        double d[4] = {(double)v.x, (double)v.y, (double)v.z, (double)v.w};
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+          for (int o = 16; o > 0; o >>= 1) d[q] += __shfl_down_sync(0xffffffffu, d[q], o);
+        if (lane == 0) power_to_table(gg, m, d[0], d[1], d[2], d[3], [&](int idx, double x) { wt[gg.toff + idx] += x; });
+      }
+      if (gslots > 1) {
+        for (int m = 0; m < nint; ++m) gacc[(slot * nint + m) * BLOCK_SLOTS + tid] = R4{};
+      }
+    }
+    if (gslots == 1)
+      for (int m = 0; m < nint; ++m) gacc[m * BLOCK_SLOTS + tid] = R4{};
+  };
+
+  int since_flush = 0;
   for (int blk = blockIdx.x; blk < db.nblocks; blk += gridDim.x) {
     const BlockRows br = block_rows(db, blk);
     __syncthreads();  // previous block done with the shared arrays
@@ -92,6 +161,16 @@ __global__ void __launch_bounds__(BLOCK_SLOTS)
 
     PairEval<MEAM, R> pe;
     double Lx = 0, Ly = 0, Lz = 0, a_p = 0, G = 0, H = 0, J = 0;
+    if (MEAM) {  // zero rows for idle threads and the padding
+      srow[tid] = R4{};
+      sadj[tid] = R4{};
+      sqz[tid] = R(0);
+      if (tid < 8) {
+        srow[BLOCK_SLOTS + tid] = R4{};
+        sadj[BLOCK_SLOTS + tid] = R4{};
+        sqz[BLOCK_SLOTS + tid] = R(0);
+      }
+    }
     if (have) {
       pe = eval_pair<MEAM, R>(db, pot, sg, ptab, gs, ti);
       const int j = db.pair_nbr[gs];
@@ -111,40 +190,46 @@ __global__ void __launch_bounds__(BLOCK_SLOTS)
         J = Lx * ax[AUX_VX * Np + gs] + Ly * ax[AUX_VY * Np + gs] + Lz * ax[AUX_VZ * Np + gs];
         const double ip = (double)pe.invr, fp = (double)pe.f;
         kp += a_p * (double)pe.df * G - a_p * fp * ip * H + fp * ip * J;
-        sx[tid] = pe.ux; sy[tid] = pe.uy; sz[tid] = pe.uz; sf[tid] = pe.f;
-        sal[tid] = (R)(a_p * (double)pe.df);
-        sbe[tid] = (R)(a_p * fp * ip);
-        sqx[tid] = (R)(fp * ip * Lx);
-        sqy[tid] = (R)(fp * ip * Ly);
+        R4 v;
+        v.x = pe.ux; v.y = pe.uy; v.z = pe.uz; v.w = pe.f;
+        srow[tid] = v;
+        R4 q;
+        q.x = (R)(a_p * (double)pe.df);
+        q.y = (R)(a_p * fp * ip);
+        q.z = (R)(fp * ip * Lx);
+        q.w = (R)(fp * ip * Ly);
+        sadj[tid] = q;
         sqz[tid] = (R)(fp * ip * Lz);
       }
       red[tid] = kp;
     }
     __syncthreads();
 
-    // ---- per atom: K_i, rho, U', U'', chi = dL/drho; U table gradient
-    if (tid < br.na) {
-      const int i = br.atom_lo + tid;
-      double K = 0.0;
-      for (int s = a_lo[tid]; s < a_lo[tid + 1]; ++s) K += red[s];
-      const double rho = ao[AO_RHO * N + i];
-      const int c = db.atom_cell[i];
-      const SplineGeom &gU = sg[pot.s_U + db.atom_type[i]];
-      const double w = db.cell_w[c];
-      double rt = rho, dpen = 0.0, drt = 1.0;
-      if (rho < gU.x0) {
-        dpen = -w * 100.0 * 10. * 2.0 * (gU.x0 - rho);
-        if (!pot.embed_extrap) { rt = gU.x0; drt = 0.0; }
-      } else if (rho > gU.xN) {
-        dpen = w * 100.0 * 10. * 2.0 * (rho - gU.xN);
-        if (!pot.embed_extrap) { rt = gU.xN; drt = 0.0; }
+    // ---- per atom (one warp each): K_i, rho, U', U'', chi = dL/drho; U table gradient
+    for (int a = warp; a < br.na; a += nwarp) {
+      double K;
+      warp_slot_sums<1>(red, a_lo[a], a_lo[a + 1], lane, &K);
+      if (lane == 0) {
+        const int i = br.atom_lo + a;
+        const double rho = ao[AO_RHO * N + i];
+        const int c = db.atom_cell[i];
+        const SplineGeom &gU = sg[pot.s_U + db.atom_type[i]];
+        const double w = db.cell_w[c];
+        double rt = rho, dpen = 0.0, drt = 1.0;
+        if (rho < gU.x0) {
+          dpen = -w * 100.0 * 10. * 2.0 * (gU.x0 - rho);
+          if (!pot.embed_extrap) { rt = gU.x0; drt = 0.0; }
+        } else if (rho > gU.xN) {
+          dpen = w * 100.0 * 10. * 2.0 * (rho - gU.xN);
+          if (!pot.embed_extrap) { rt = gU.xN; drt = 0.0; }
+        }
+        const PointEval U = spl_point(tc, gU, rt);
+        const double eps = sd[CS_EPS * NC + c], kap = sd[CS_KAPPA * NC + c];
+        a_chi[a] = (eps * U.grad + U.grad2 * K) * drt + kap * dpen;
+        a_dF[a] = U.grad;
+        const int toffU = gU.toff;
+        spl_point_adjoint(gU, U, rt, eps, K, [&](int idx, double v) { wt[toffU + idx] += v; });
       }
-      const PointEval U = spl_point(tc, gU, rt);
-      const double eps = sd[CS_EPS * NC + c], kap = sd[CS_KAPPA * NC + c];
-      a_chi[tid] = (eps * U.grad + U.grad2 * K) * drt + kap * dpen;
-      a_dF[tid] = U.grad;
-      const int toffU = gU.toff;
-      spl_point_adjoint(gU, U, rt, eps, K, [&](int idx, double v) { add_w(toffU + idx, v); });
     }
     __syncthreads();
 
@@ -154,37 +239,48 @@ __global__ void __launch_bounds__(BLOCK_SLOTS)
       if (MEAM) {
         const SplineGeom gg = sg[pot.s_g + ti];
         const R *gpc = ptab + gg.poff;
-        const R gx0 = (R)gg.x0, ginv = (R)gg.invstep, gst = (R)gg.step;
+        const R gx0 = (R)gg.x0, ginv = (R)gg.invstep;
         const R gcut = g_cut<R>(gg);
-        const int ng = gg.n;
+        const int ngt = gg.n;
         const double fp = (double)pe.f, ip = (double)pe.invr;
-        const double gam = 0.5 * chi * fp + dF * a_p * (double)pe.df;
-        const double del = dF * fp * ip;
-        double *gp = gpriv + tid;
+        const R gam = (R)(0.5 * chi * fp + dF * a_p * (double)pe.df);
+        const R del = (R)(dF * fp * ip);
+        const R lx = (R)Lx, ly = (R)Ly, lz = (R)Lz, ap = (R)a_p;
+        R4 *ga = gacc + (size_t)(gslots == 1 ? 0 : ti) * nint * BLOCK_SLOTS + tid;
         const int row_lo = a_lo[me], row_hi = a_lo[me + 1];
-        for (int k = row_lo; k < row_hi; ++k) {
-          if (k == tid) continue;
-          const R fk = sf[k], alk = sal[k];
-          if (fk == R(0) && alk == R(0)) continue;
-          const R kx = sx[k], ky = sy[k], kz = sz[k];
-          const R cs = cos_exact(pe.ux, pe.uy, pe.uz, kx, ky, kz);
-          if (!(cs < gcut)) continue;
-          R b;
-          const int m = g_knot<R>(cs, gx0, ginv, ng, b);
-          R dg;
-          const R gv = cubic_val_grad<R>(gpc, m, b, ginv, dg);
-          // d K / d f_p from the triplet terms of slot k
-          const R qu = sqx[k] * pe.ux + sqy[k] * pe.uy + sqz[k] * pe.uz;
-          dKdf += (double)(alk * gv - sbe[k] * dg * cs + dg * qu);
-          // g table: value weight cg, slope weight cgp of this ordered pair
-          const double bpk = Lx * (double)kx + Ly * (double)ky + Lz * (double)kz;
-          const double cg = (double)fk * gam;
-          const double cgp = (double)fk * del * (bpk - a_p * (double)cs);
-          const SplW<R> w = spl_weights<R>(b, gst, ginv);
-          gp[m * BLOCK_SLOTS] += cg * (double)w.wa + cgp * (double)w.da;
-          gp[(m + 1) * BLOCK_SLOTS] += cg * (double)w.wb + cgp * (double)w.db;
-          gp[(ng + m) * BLOCK_SLOTS] += cg * (double)w.wA + cgp * (double)w.dA;
-          gp[(ng + m + 1) * BLOCK_SLOTS] += cg * (double)w.wB + cgp * (double)w.dB;
+        for (int kb = row_lo; kb < row_hi; kb += 8) {
+          R dk8 = 0;
+          // Branch-free chunk of 8 partners (zero weight when not a triplet
+          // of this row; the shared rows are padded with zeros).
+#pragma unroll
+          for (int u = 0; u < 8; ++u) {
+            const int k = kb + u;
+            const R4 o = srow[k];
+            const R4 q = sadj[k];
+            const R cs = cos_dot(pe.ux, pe.uy, pe.uz, o.x, o.y, o.z);
+            const bool ok = (k < row_hi) && (k != tid) && (cs < gcut);
+            const R wk = ok ? R(1) : R(0);
+            R b;
+            const int m = g_knot<R>(cs, gx0, ginv, ngt, b);
+            R dg;
+            const R gv = cubic_val_grad<R>(gpc, m, b, ginv, dg);
+            // d K / d f_p from the triplet terms of slot k
+            const R qu = q.z * pe.ux + q.w * pe.uy + sqz[k] * pe.uz;
+            dk8 += wk * (q.x * gv - q.y * dg * cs + dg * qu);
+            // g table (power basis): value weight cg, slope weight cgp / h
+            const R bpk = lx * o.x + ly * o.y + lz * o.z;
+            const R fk = wk * o.w;
+            const R cg = fk * gam;
+            const R cs1 = fk * del * (bpk - ap * cs) * ginv;
+            const R b2 = b * b;
+            R4 d = ga[m * BLOCK_SLOTS];
+            d.x += cg;
+            d.y += cg * b + cs1;
+            d.z += cg * b2 + R(2) * cs1 * b;
+            d.w += cg * b2 * b + R(3) * cs1 * b2;
+            ga[m * BLOCK_SLOTS] = d;
+          }
+          dKdf += (double)dk8;
         }
         dKdf += ip * (J - a_p * H);
       }
@@ -192,10 +288,10 @@ __global__ void __launch_bounds__(BLOCK_SLOTS)
       auto pair_adj = [&](int s, int k, R b, double cv, double cd) {
         const SplineGeom &g = sg[s];
         const SplW<double> w = spl_weights<double>((double)b, g.step, g.invstep);
-        add_w(g.toff + k, cv * w.wa + cd * w.da);
-        add_w(g.toff + k + 1, cv * w.wb + cd * w.db);
-        add_w(g.toff + g.n + k, cv * w.wA + cd * w.dA);
-        add_w(g.toff + g.n + k + 1, cv * w.wB + cd * w.dB);
+        add_f(g.toff + k, cv * w.wa + cd * w.da);
+        add_f(g.toff + k + 1, cv * w.wb + cd * w.db);
+        add_f(g.toff + g.n + k, cv * w.wA + cd * w.dA);
+        add_f(g.toff + g.n + k + 1, cv * w.wB + cd * w.dB);
       };
       const double eps = sd[CS_EPS * NC + cell];
       if (pe.kphi >= 0) pair_adj(pot.s_phi + pe.pij, pe.kphi, pe.bphi, 0.5 * eps, 0.5 * a_p);
@@ -203,24 +299,22 @@ __global__ void __launch_bounds__(BLOCK_SLOTS)
       if (MEAM && pe.kf >= 0) pair_adj(pot.s_f + pe.pij, pe.kf, pe.bf, chi * G + dF * dKdf, dF * a_p * G);
     }
     __syncwarp();
-    if (MEAM) {
-      // flush the per-thread g tables into the warp's table, per g spline
-      for (int t = 0; t < pot.ntypes; ++t) {
-        const SplineGeom &gg = sg[pot.s_g + t];
-        const int ng = gg.n;
-        for (int e = 0; e < 2 * ng; ++e) {
-          double v = (have && ti == t) ? gpriv[e * BLOCK_SLOTS + tid] : 0.0;
-          for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-          if (lane == 0 && v != 0.0) wt[gg.toff + e] += v;
-        }
-      }
-      if (have) {
-        const int ng = sg[pot.s_g + ti].n;
-        for (int e = 0; e < 2 * ng; ++e) gpriv[e * BLOCK_SLOTS + tid] = 0.0;
-      }
+    // the block's FP32 pair-function sums into the warp's FP64 table
+    for (int e = lane; e < stride; e += 32) {
+      wt[e] += (double)ft[e];
+      ft[e] = 0.f;
+    }
+    __syncwarp();
+    if (MEAM && (gslots == 1 || ++since_flush == GACC_FLUSH_BLOCKS)) {
+      flush_gacc(have, ti);
+      since_flush = 0;
     }
   }
   __syncthreads();
+  if (MEAM && gslots > 1 && since_flush > 0) {
+    flush_gacc(false, 0);
+    __syncthreads();
+  }
   double *out = partial + ((size_t)cand * gridDim.x + blockIdx.x) * stride;
   for (int e = tid; e < stride; e += blockDim.x) {
     double s = 0.0;

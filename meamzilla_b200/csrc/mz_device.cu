@@ -323,9 +323,10 @@ mz_status mz_create(const mz_db *dbh, const mz_pot *poth, const mz_settings *set
     if (pot.nsplines() > MAX_SPLINES) throw Failure{MZ_ERR_RANGE, "too many splines"};
     const bool meam = pot.style == MZ_STYLE_MEAM_SPLINE;
     if (meam)
-      for (auto &g : pot.groups[G_G])
+      for (auto &g : pot.groups[G_G]) {
         if (g.nknots > MAX_G_KNOTS)
           throw Failure{MZ_ERR_RANGE, "g spline with more than " + std::to_string(MAX_G_KNOTS) + " knots"};
+      }
     ctx = new mz_ctx;
     ctx->device = set->device;
     ck(cudaSetDevice(ctx->device), "cudaSetDevice");
@@ -487,8 +488,12 @@ mz_status mz_create(const mz_db *dbh, const mz_pot *poth, const mz_settings *set
     // ---- shared memory of the kernels
     ctx->smem_atoms[0] = atoms_smem_bytes<double>(ns, ctx->pstride);
     ctx->smem_atoms[1] = atoms_smem_bytes<float>(ns, ctx->pstride);
-    ctx->smem_adj[0] = adj_smem_bytes<double>(ns, stride, ctx->pstride, meam);
-    ctx->smem_adj[1] = adj_smem_bytes<float>(ns, stride, ctx->pstride, meam);
+    int ng = 2;
+    if (meam)
+      for (auto &g : pot.groups[G_G]) ng = std::max(ng, g.nknots);
+    dp.g_nmax = ng;
+    ctx->smem_adj[0] = adj_smem_bytes<double>(ns, stride, ctx->pstride, meam, pot.ntypes, ng);
+    ctx->smem_adj[1] = adj_smem_bytes<float>(ns, stride, ctx->pstride, meam, pot.ntypes, ng);
     int smem_max = 0;
     ck(cudaDeviceGetAttribute(&smem_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx->device), "attribute");
     if (ctx->smem_adj[0] > (size_t)smem_max || ctx->smem_atoms[0] > (size_t)smem_max)

@@ -59,6 +59,7 @@ struct DevPot {
   int pow_stride;     // doubles per candidate evaluation table
   int s_phi, s_rho, s_U, s_f, s_g;  // first spline of each group
   int embed_extrap;
+  int g_nmax;         // largest g-spline knot count (MEAM)
   double energy_weight, stress_weight;
 };
 

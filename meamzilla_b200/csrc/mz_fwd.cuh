@@ -151,22 +151,57 @@ __device__ __forceinline__ PairEval<MEAM, R> eval_pair(const DevDb &db, const De
 // ------------------------------------------------------------------ k_atoms
 
 // Shared-memory layout of k_atoms (dynamic), see atoms_smem_bytes():
-//   double red[11][BLOCK_SLOTS]       per-slot partials for the per-atom sums
+//   double red[10][BLOCK_SLOTS]       per-slot partials for the per-atom sums
 //   double a_dF[BLOCK_ATOMS], a_U[BLOCK_ATOMS]
 //   SplineGeom sg[nsplines]
 //   int a_lo[BLOCK_ATOMS+2]
 //   R ptab[pstride]                    this candidate's evaluation table
-//   R sx,sy,sz,sf[BLOCK_SLOTS]         pair data of the block
+//   R4 srow[BLOCK_SLOTS]               (u_x, u_y, u_z, f) of every slot of the block
+template <typename R>
+struct Vec4;
+template <>
+struct Vec4<float> {
+  using T = float4;
+};
+template <>
+struct Vec4<double> {
+  using T = double4;
+};
+
 template <typename R>
 __host__ __device__ inline size_t atoms_smem_bytes(int nsplines, int pstride) {
-  size_t b = sizeof(double) * (11 * BLOCK_SLOTS + 2 * BLOCK_ATOMS);
+  size_t b = sizeof(double) * (10 * BLOCK_SLOTS + 2 * BLOCK_ATOMS);
   b += sizeof(SplineGeom) * nsplines;
   b += sizeof(int) * (BLOCK_ATOMS + 2);
-  b = (b + 15) & ~size_t(15);
+  b = (b + 31) & ~size_t(31);
   b += sizeof(R) * (pstride + 4);
-  b = (b + 15) & ~size_t(15);
-  b += sizeof(R) * 4 * BLOCK_SLOTS;
+  b = (b + 31) & ~size_t(31);
+  b += 4 * sizeof(R) * (BLOCK_SLOTS + 8);
   return b;
+}
+
+// Dot product of unit vectors: exact (no fused multiply-add, as the
+// reference computes Triplet::cos) in FP64, fused in FP32.
+__device__ __forceinline__ double cos_dot(double ax, double ay, double az, double bx, double by, double bz) {
+  return cos_exact(ax, ay, az, bx, by, bz);
+}
+__device__ __forceinline__ float cos_dot(float ax, float ay, float az, float bx, float by, float bz) {
+  return fmaf(ax, bx, fmaf(ay, by, az * bz));
+}
+
+// Warp-cooperative sum over the slots [lo, hi) of `n` per-slot arrays
+// red[q * BLOCK_SLOTS + s]; the result is valid on lane 0.  Fixed order.
+template <int NQ>
+__device__ __forceinline__ void warp_slot_sums(const double *red, int lo, int hi, int lane, double *out) {
+#pragma unroll
+  for (int q = 0; q < NQ; ++q) out[q] = 0.0;
+  for (int s = lo + lane; s < hi; s += 32) {
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) out[q] += red[q * BLOCK_SLOTS + s];
+  }
+#pragma unroll
+  for (int q = 0; q < NQ; ++q)
+    for (int o = 16; o > 0; o >>= 1) out[q] += __shfl_down_sync(0xffffffffu, out[q], o);
 }
 
 // One CTA per (atom block, candidate), one thread per pair slot.  A single
@@ -176,31 +211,32 @@ __host__ __device__ inline size_t atoms_smem_bytes(int nsplines, int pstride) {
 //   V_p = u_p (phi'_p/2 + rho'_p U') + U' [u_p (f'_p G_p - f_p H_p / r_p)
 //                                          + f_p vk_p / r_p]
 // is the force atom i's terms add to atom i along slot p; the neighbour
-// receives -V_p (k_gather).
+// receives -V_p (k_gather).  In FP32 the row sums are taken in chunks of 8
+// terms, each chunk added to an FP64 total.
 template <bool MEAM, typename R, bool AUX>
-__global__ void __launch_bounds__(BLOCK_SLOTS)
+__global__ void __launch_bounds__(BLOCK_SLOTS, 3)
     k_atoms(DevDb db, DevPot pot, const SplineGeom *__restrict__ geom, const double *__restrict__ tabs,
             const double *__restrict__ ptabs, double *__restrict__ Vout, double *__restrict__ aout,
             double *__restrict__ aux) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+  using R4 = typename Vec4<R>::T;
+  extern __shared__ __align__(32) unsigned char smem_raw[];
   const int cand = blockIdx.y;
-  const int tid = threadIdx.x;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarp = blockDim.x >> 5;
   const int N = db.natoms;
   const int64_t Np = db.npairs;
 
   double *red = reinterpret_cast<double *>(smem_raw);
-  double *a_dF = red + 11 * BLOCK_SLOTS;
+  double *a_dF = red + 10 * BLOCK_SLOTS;
   double *a_U = a_dF + BLOCK_ATOMS;
   SplineGeom *sg = reinterpret_cast<SplineGeom *>(a_U + BLOCK_ATOMS);
   int *a_lo = reinterpret_cast<int *>(sg + pot.nsplines);
-  size_t off = sizeof(double) * (11 * BLOCK_SLOTS + 2 * BLOCK_ATOMS) + sizeof(SplineGeom) * pot.nsplines +
+  size_t off = sizeof(double) * (10 * BLOCK_SLOTS + 2 * BLOCK_ATOMS) + sizeof(SplineGeom) * pot.nsplines +
                sizeof(int) * (BLOCK_ATOMS + 2);
-  off = (off + 15) & ~size_t(15);
+  off = (off + 31) & ~size_t(31);
   R *ptab = reinterpret_cast<R *>(smem_raw + off);
   off += sizeof(R) * (pot.pow_stride + 4);
-  off = (off + 15) & ~size_t(15);
-  R *sx = reinterpret_cast<R *>(smem_raw + off);
-  R *sy = sx + BLOCK_SLOTS, *sz = sy + BLOCK_SLOTS, *sf = sz + BLOCK_SLOTS;
+  off = (off + 31) & ~size_t(31);
+  R4 *srow = reinterpret_cast<R4 *>(smem_raw + off);
 
   const BlockRows br = block_rows(db, blockIdx.x);
   const double *tc = tabs + (size_t)cand * pot.tab_stride;
@@ -216,9 +252,15 @@ __global__ void __launch_bounds__(BLOCK_SLOTS)
   const int64_t gs = (int64_t)br.slot_lo + tid;
 
   PairEval<MEAM, R> pe;
-  if (have) {
-    pe = eval_pair<MEAM, R>(db, pot, sg, ptab, gs, ti);
-    sx[tid] = pe.ux; sy[tid] = pe.uy; sz[tid] = pe.uz; sf[tid] = pe.f;
+  {
+    R4 v;
+    v.x = v.y = v.z = v.w = R(0);
+    if (have) {
+      pe = eval_pair<MEAM, R>(db, pot, sg, ptab, gs, ti);
+      v.x = pe.ux; v.y = pe.uy; v.z = pe.uz; v.w = pe.f;
+    }
+    srow[tid] = v;
+    if (tid < 8) srow[BLOCK_SLOTS + tid] = R4{};
   }
   __syncthreads();
 
@@ -230,23 +272,34 @@ __global__ void __launch_bounds__(BLOCK_SLOTS)
     const R gx0 = (R)gg.x0, ginv = (R)gg.invstep;
     const R gcut = g_cut<R>(gg);
     const int row_lo = a_lo[me], row_hi = a_lo[me + 1];
-    for (int k = row_lo; k < row_hi; ++k) {
-      if (k == tid) continue;
-      const R fk = sf[k];
-      if (fk == R(0)) continue;
-      const R kx = sx[k], ky = sy[k], kz = sz[k];
-      const R cs = cos_exact(pe.ux, pe.uy, pe.uz, kx, ky, kz);
-      if (!(cs < gcut)) continue;  // g_knot == -1: not a triplet (triplet_meam_spline.cpp:66-70)
-      R b;
-      const int kk = g_knot<R>(cs, gx0, ginv, gg.n, b);
-      R dg;
-      const R gv = cubic_val_grad<R>(gpc, kk, b, ginv, dg);
-      const R dgfk = dg * fk;
-      G += (double)(gv * fk);
-      H += (double)(dgfk * cs);
-      vkx += (double)(dgfk * kx);
-      vky += (double)(dgfk * ky);
-      vkz += (double)(dgfk * kz);
+    for (int kb = row_lo; kb < row_hi; kb += 8) {
+      R g8 = 0, h8 = 0, x8 = 0, y8 = 0, z8 = 0;
+      // Branch-free chunk of 8 partners: a partner that is this slot, past
+      // the row, or not a triplet contributes with weight zero.  srow is
+      // padded with zero rows past the block's last slot.
+#pragma unroll
+      for (int u = 0; u < 8; ++u) {
+        const int k = kb + u;
+        const R4 o = srow[k];
+        const R cs = cos_dot(pe.ux, pe.uy, pe.uz, o.x, o.y, o.z);
+        const bool ok = (k < row_hi) && (k != tid) && (cs < gcut);  // triplet_meam_spline.cpp:66-70
+        const R fk = ok ? o.w : R(0);
+        R b;
+        const int kk = g_knot<R>(cs, gx0, ginv, gg.n, b);
+        R dg;
+        const R gv = cubic_val_grad<R>(gpc, kk, b, ginv, dg);
+        const R dgfk = dg * fk;
+        g8 += gv * fk;
+        h8 += dgfk * cs;
+        x8 += dgfk * o.x;
+        y8 += dgfk * o.y;
+        z8 += dgfk * o.z;
+      }
+      G += (double)g8;
+      H += (double)h8;
+      vkx += (double)x8;
+      vky += (double)y8;
+      vkz += (double)z8;
     }
     if (AUX) {
       double *ax = aux + (size_t)cand * AUX_COUNT * Np;
@@ -260,29 +313,31 @@ __global__ void __launch_bounds__(BLOCK_SLOTS)
   if (have) red[tid] = (double)pe.rho + (MEAM ? 0.5 * (double)pe.f * G : 0.0);
   __syncthreads();
 
-  // ---- embedding (pot_meam_spline.cpp:208-223): one thread per atom
-  if (tid < br.na) {
-    const int ia = br.atom_lo + tid;
-    double rho = 0.0;
-    for (int s = a_lo[tid]; s < a_lo[tid + 1]; ++s) rho += red[s];
-    const SplineGeom &gU = sg[pot.s_U + db.atom_type[ia]];
-    const double w = db.cell_w[db.atom_cell[ia]];
-    double pen = 0.0;
-    const double lo = gU.x0, hi = gU.xN;
-    const double rho_raw = rho;
-    if (rho < lo) {
-      pen = w * 100.0 * 10. * (lo - rho) * (lo - rho);
-      if (!pot.embed_extrap) rho = lo;
-    } else if (rho > hi) {
-      pen = w * 100.0 * 10. * (rho - hi) * (rho - hi);
-      if (!pot.embed_extrap) rho = hi;
+  // ---- embedding (pot_meam_spline.cpp:208-223): one warp per atom
+  for (int a = warp; a < br.na; a += nwarp) {
+    double rho;
+    warp_slot_sums<1>(red, a_lo[a], a_lo[a + 1], lane, &rho);
+    if (lane == 0) {
+      const int ia = br.atom_lo + a;
+      const SplineGeom &gU = sg[pot.s_U + db.atom_type[ia]];
+      const double w = db.cell_w[db.atom_cell[ia]];
+      double pen = 0.0;
+      const double lo = gU.x0, hi = gU.xN;
+      const double rho_raw = rho;
+      if (rho < lo) {
+        pen = w * 100.0 * 10. * (lo - rho) * (lo - rho);
+        if (!pot.embed_extrap) rho = lo;
+      } else if (rho > hi) {
+        pen = w * 100.0 * 10. * (rho - hi) * (rho - hi);
+        if (!pot.embed_extrap) rho = hi;
+      }
+      const PointEval U = spl_point(tc, gU, rho);  // FP64 table of this candidate
+      a_dF[a] = U.grad;
+      a_U[a] = U.val;
+      double *ao = aout + (size_t)cand * AO_COUNT * N;
+      ao[AO_PEN * N + ia] = pen;
+      ao[AO_RHO * N + ia] = rho_raw;
     }
-    const PointEval U = spl_point(tc, gU, rho);  // FP64 table of this candidate
-    a_dF[tid] = U.grad;
-    a_U[tid] = U.val;
-    double *ao = aout + (size_t)cand * AO_COUNT * N;
-    ao[AO_PEN * N + ia] = pen;
-    ao[AO_RHO * N + ia] = rho_raw;
   }
   __syncthreads();
 
@@ -309,34 +364,31 @@ __global__ void __launch_bounds__(BLOCK_SLOTS)
     Vc[2 * Np + gs] = Vz;
     const double rr = db.pair_r[gs];
     const double dx = db.pair_ux[gs], dy = db.pair_uy[gs], dz = db.pair_uz[gs];
-    red[1 * BLOCK_SLOTS + tid] = Vx;
-    red[2 * BLOCK_SLOTS + tid] = Vy;
-    red[3 * BLOCK_SLOTS + tid] = Vz;
-    red[4 * BLOCK_SLOTS + tid] = 0.5 * (double)pe.phi;
-    red[5 * BLOCK_SLOTS + tid] = -(dx * (Vx * rr));
-    red[6 * BLOCK_SLOTS + tid] = -(dy * (Vy * rr));
-    red[7 * BLOCK_SLOTS + tid] = -(dz * (Vz * rr));
-    red[8 * BLOCK_SLOTS + tid] = -(dx * (Vy * rr));
-    red[9 * BLOCK_SLOTS + tid] = -(dy * (Vz * rr));
-    red[10 * BLOCK_SLOTS + tid] = -(dz * (Vx * rr));
+    red[0 * BLOCK_SLOTS + tid] = Vx;
+    red[1 * BLOCK_SLOTS + tid] = Vy;
+    red[2 * BLOCK_SLOTS + tid] = Vz;
+    red[3 * BLOCK_SLOTS + tid] = 0.5 * (double)pe.phi;
+    red[4 * BLOCK_SLOTS + tid] = -(dx * (Vx * rr));
+    red[5 * BLOCK_SLOTS + tid] = -(dy * (Vy * rr));
+    red[6 * BLOCK_SLOTS + tid] = -(dz * (Vz * rr));
+    red[7 * BLOCK_SLOTS + tid] = -(dx * (Vy * rr));
+    red[8 * BLOCK_SLOTS + tid] = -(dy * (Vz * rr));
+    red[9 * BLOCK_SLOTS + tid] = -(dz * (Vx * rr));
   }
   __syncthreads();
-  if (tid < br.na) {
-    const int ia = br.atom_lo + tid;
+  for (int a = warp; a < br.na; a += nwarp) {
     double acc[10];
+    warp_slot_sums<10>(red, a_lo[a], a_lo[a + 1], lane, acc);
+    if (lane == 0) {
+      const int ia = br.atom_lo + a;
+      double *ao = aout + (size_t)cand * AO_COUNT * N;
+      ao[AO_AX * N + ia] = acc[0];
+      ao[AO_AY * N + ia] = acc[1];
+      ao[AO_AZ * N + ia] = acc[2];
+      ao[AO_E * N + ia] = acc[3] + a_U[a];
 #pragma unroll
-    for (int q = 0; q < 10; ++q) acc[q] = 0.0;
-    for (int s = a_lo[tid]; s < a_lo[tid + 1]; ++s) {
-#pragma unroll
-      for (int q = 0; q < 10; ++q) acc[q] += red[(q + 1) * BLOCK_SLOTS + s];
+      for (int q = 0; q < 6; ++q) ao[(AO_S0 + q) * N + ia] = acc[4 + q];
     }
-    double *ao = aout + (size_t)cand * AO_COUNT * N;
-    ao[AO_AX * N + ia] = acc[0];
-    ao[AO_AY * N + ia] = acc[1];
-    ao[AO_AZ * N + ia] = acc[2];
-    ao[AO_E * N + ia] = acc[3] + a_U[tid];
-#pragma unroll
-    for (int q = 0; q < 6; ++q) ao[(AO_S0 + q) * N + ia] = acc[4 + q];
   }
 }
 
