@@ -185,6 +185,10 @@ typedef struct {
   int embed_extrap;       /* param key embed_extrap (pot_eam.cpp:71), default 0 */
   int device;             /* CUDA device ordinal                               */
   int max_candidates;     /* largest ncand per call (sizes device buffers)     */
+  int omit_punishments;   /* nonzero: leave out the style punishment entries   */
+                          /* (f-max for MEAM, U'(mid) for EAM; their ErrorVec */
+                          /* entries read 0) -- for all but one shard of a    */
+                          /* database split over several evaluators           */
 } mz_settings;
 
 /* Copy the database and the potential's fixed structure to the device. */

@@ -73,7 +73,7 @@ class SplineView(C.Structure):
 
 class Settings(C.Structure):
     _fields_ = [("energy_weight", C.c_double), ("stress_weight", C.c_double), ("embed_extrap", C.c_int),
-                ("device", C.c_int), ("max_candidates", C.c_int)]
+                ("device", C.c_int), ("max_candidates", C.c_int), ("omit_punishments", C.c_int)]
 
 
 _lib = None

@@ -342,7 +342,7 @@ __global__ void k_grad_final(DevPot pot, const SplineGeom *__restrict__ geom, co
   }
   __syncthreads();
   const double *tab = tabs + (size_t)c * stride;
-  if (t == 0) {
+  if (t == 0 && !pot.omit_pen) {
     if (pot.style == MZ_STYLE_MEAM_SPLINE) {
       int at = -1;
       const double my = f_max_y(pot, geom, tab, &at);

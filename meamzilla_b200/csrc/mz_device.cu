@@ -404,6 +404,7 @@ mz_status mz_create(const mz_db *dbh, const mz_pot *poth, const mz_settings *set
     dp.embed_extrap = set->embed_extrap;
     dp.energy_weight = set->energy_weight;
     dp.stress_weight = set->stress_weight;
+    dp.omit_pen = set->omit_punishments;
     ctx->npen = meam ? 1 : pot.ntypes;
     ctx->esize = 8 * db.ncells + 3 * db.natoms + ctx->npen;
 
@@ -780,6 +781,7 @@ extern "C" mz_status mz_objective_noalloc(const mz_db *dbh, const mz_pot *poth, 
     dp.embed_extrap = set->embed_extrap;
     dp.energy_weight = set->energy_weight;
     dp.stress_weight = set->stress_weight;
+    dp.omit_pen = set->omit_punishments;
 
     // ---- host images of the database
     std::vector<int> off32(N + 1), inoff32(N + 1), inslot32(Np), knot32(Np);

@@ -60,6 +60,7 @@ struct DevPot {
   int s_phi, s_rho, s_U, s_f, s_g;  // first spline of each group
   int embed_extrap;
   int g_nmax;         // largest g-spline knot count (MEAM)
+  int omit_pen;       // leave out the style punishments (sharded databases)
   double energy_weight, stress_weight;
 };
 

@@ -550,7 +550,10 @@ __global__ void k_final(DevDb db, DevPot pot, const SplineGeom *__restrict__ geo
     double total = part[0];
     const double *tab = tabs + (size_t)c * pot.tab_stride;
     double *ev = errvec ? errvec + (size_t)c * esize + 8 * db.ncells + 3 * db.natoms : nullptr;
-    if (pot.style == MZ_STYLE_MEAM_SPLINE) {
+    if (pot.omit_pen) {
+      if (ev)
+        for (int q = 0; q < (pot.style == MZ_STYLE_MEAM_SPLINE ? 1 : pot.ntypes); ++q) ev[q] = 0.0;
+    } else if (pot.style == MZ_STYLE_MEAM_SPLINE) {
       // f-potential magnitude punishment (pot_meam_spline.cpp:274-278)
       const double m = fabs(f_max_y(pot, geom, tab, nullptr));
       const double fe = 100. * 25. * (1.0 - m) * (1.0 - m);

@@ -192,10 +192,10 @@ static std::string read_text(const std::string &path) {
 void parse_pot(const std::string &text, Pot &pot) {
   // PotList::init (pot_list.cpp:84-142) for one #P block.
   std::vector<std::string> L = split_lines(text);
-  if (L.size() < 3) fail(MZ_ERR_FORMAT, "potential file too short");
+  if (L.empty()) fail(MZ_ERR_FORMAT, "empty potential file");
   size_t ln = 0;
   pot.comment = L[ln++];
-  if (L[ln].substr(0, 2) != "#T") fail(MZ_ERR_FORMAT, "potential type line (#T ...) missing");
+  if (ln >= L.size() || L[ln].substr(0, 2) != "#T") fail(MZ_ERR_FORMAT, "potential type line (#T ...) missing");
   {
     std::istringstream is(L[ln++]);
     std::string lab;

@@ -138,6 +138,19 @@ __device__ __forceinline__ int g_knot(R c, R x0, R invstep, int n, R &b) {
   b = t - R(k);
   return k;
 }
+// FP32: floor through the float format instead of conversion instructions.
+// For 0 <= t < 2^22, t + (2^23 - 1/2) rounds to the integer 2^23 + floor(t)
+// (exact halves, where t is an integer, round to even: the interval below
+// with b = 1, which evaluates to the same spline value); its bit pattern
+// minus that of 2^23 is floor(t).  t slightly below 0 gives -1, clamped.
+template <>
+__device__ __forceinline__ int g_knot<float>(float c, float x0, float invstep, int n, float &b) {
+  const float t = (c - x0) * invstep;
+  int k = __float_as_int(t + 8388607.5f) - 0x4B000000;
+  k = k < 0 ? 0 : (k > n - 2 ? n - 2 : k);
+  b = t - (__int_as_float(k + 0x4B000000) - 8388608.0f);
+  return k;
+}
 
 // cos(theta) exactly as Triplet::setup_triplet: x*x' + y*y' + z*z' with no
 // fused multiply-add (triplet.cpp:34-40, vect.h:137-141).

@@ -1,0 +1,71 @@
+"""Powell vs L-BFGS from the same start, on a seeded synthetic workload.
+
+    python -m meamzilla_b200.fitcmp [--workload meam200] [--seed 0] [--powell-steps 20]
+
+Builds the workload (teacher potential, targets = teacher energies / forces /
+stresses + noise), starts both fits from teacher + N(0, 0.1), runs Powell
+(FP64, batched Jacobian) and then L-BFGS on the adjoint with Powell's final
+objective as its target, and prints one JSON line: final objectives, wall
+seconds, objective evaluations.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import time
+
+import numpy as np
+
+from . import synth
+from .optimize import lbfgs_fit, powell_fit
+from .potential import MZ_FP64, MZ_MIXED, Database, Evaluator, PotentialFile
+
+
+def build(workload: str, seed: int, ncells=None, max_candidates=1):
+    spec, cells = synth.make_workload(workload, seed=seed, ncells=ncells)
+    pot = PotentialFile.from_spec(spec)
+    db = Database.from_cells(cells, pot)
+    ev0 = Evaluator(db, pot, 1.0, 1.0, 0, max_candidates=1)
+    out = ev0.objective(pot.coeffs()[None, :], MZ_FP64, forces=True, energy=True, stress=True)
+    del ev0
+    rng = np.random.default_rng(3000 + seed)
+    nc = len(cells)
+    e0 = out["energy"][0] + rng.normal(0.0, 1e-3, nc)
+    s0 = out["stress"][0] + rng.normal(0.0, 0.01, (nc, 6)) / synth.GPA_PER_EV_A3
+    f0 = out["forces"][0] + rng.normal(0.0, 0.01, out["forces"][0].shape)
+    db.set_targets(e0, s0.ravel(), f0.ravel())
+    ev = Evaluator(db, pot, 1.0, 1.0, 0, max_candidates=max_candidates)
+    return pot, db, ev
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--workload", default="meam200")
+    ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--ncells", type=int, default=None)
+    ap.add_argument("--powell-steps", type=int, default=20)
+    ap.add_argument("--start-sigma", type=float, default=0.1)
+    args = ap.parse_args()
+    pot, db, _ = build(args.workload, args.seed, args.ncells, max_candidates=1)
+    P = pot.ncoeff
+    _, _, ev = build(args.workload, args.seed, args.ncells, max_candidates=P)
+    rng = np.random.default_rng(77 + args.seed)
+    x0 = pot.coeffs() + rng.normal(0.0, args.start_sigma, P)
+    F0 = float(ev.objective(x0[None, :])[0])
+    xp, Fp, ip = powell_fit(ev, x0, max_steps=args.powell_steps)
+    xl, Fl, il = lbfgs_fit(ev, x0, MZ_FP64, maxiter=20000, target=Fp)
+    xm, Fm, im = lbfgs_fit(ev, x0, MZ_MIXED, maxiter=20000, target=Fp)
+    st = db.stats()
+    print(json.dumps({
+        "workload": args.workload, "natoms": st["natoms"], "ntriplets": st["ntriplets"], "ncoeff": P,
+        "start_objective": F0,
+        "powell": {"objective": Fp, "seconds": ip["seconds"], "evals": ip["evals"], "outer": ip["outer"]},
+        "lbfgs_fp64": {"objective": Fl, "seconds": il["seconds"], "evals": il["evals"],
+                       "reached_powell": bool(Fl <= Fp)},
+        "lbfgs_mixed": {"objective": Fm, "seconds": im["seconds"], "evals": im["evals"],
+                        "reached_powell": bool(Fm <= Fp)},
+    }))
+
+
+if __name__ == "__main__":
+    main()

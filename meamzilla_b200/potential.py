@@ -227,9 +227,9 @@ class Evaluator:
     order; many of them are evaluated per launch."""
 
     def __init__(self, db: Database, pot: PotentialFile, energy_weight=0.0, stress_weight=0.0,
-                 embed_extrap=0, device=0, max_candidates=1):
+                 embed_extrap=0, device=0, max_candidates=1, omit_punishments=False):
         s = _lib.Settings(float(energy_weight), float(stress_weight), int(embed_extrap), int(device),
-                          int(max_candidates))
+                          int(max_candidates), 1 if omit_punishments else 0)
         h = C.c_void_p()
         check(lib().mz_create(db.handle, pot.handle, C.byref(s), C.byref(h)))
         self._h = h
@@ -293,11 +293,14 @@ class Evaluator:
         """The context's CUDA stream (cudaStream_t as an integer)."""
         return lib().mz_stream(self._h) or 0
 
-    def objective_device(self, params, obj, precision=MZ_MIXED) -> None:
-        """params: (n, ncoeff) float64 CUDA tensor; obj: (n,) float64 CUDA tensor."""
+    def objective_device(self, params, obj, precision=MZ_MIXED, errvec=None, forces=None) -> None:
+        """params: (n, ncoeff) float64 CUDA tensor; obj: (n,) float64 CUDA tensor;
+        optional errvec (n, esize) and forces (n, natoms, 3) CUDA tensors."""
         n = params.shape[0]
+        ev = None if errvec is None else C.c_void_p(errvec.data_ptr())
+        fo = None if forces is None else C.c_void_p(forces.data_ptr())
         check(lib().mz_objective_device(self._h, n, C.c_void_p(params.data_ptr()), int(precision),
-                                        C.c_void_p(obj.data_ptr()), None, None))
+                                        C.c_void_p(obj.data_ptr()), ev, fo))
 
     def objective_grad_device(self, params, obj, grad, precision=MZ_MIXED) -> None:
         n = params.shape[0]

@@ -26,7 +26,7 @@ def _noalloc(case, x):
     from meamzilla_b200 import _lib
     from meamzilla_b200._lib import check, lib, ptr
     w = case["weights"]
-    s = _lib.Settings(w["energy_weight"], w["stress_weight"], w["embed_extrap"], 0, 1)
+    s = _lib.Settings(w["energy_weight"], w["stress_weight"], w["embed_extrap"], 0, 1, 0)
     n = case["db"].stats()["natoms"]
     obj = np.zeros(1)
     forces = np.zeros((n, 3))
