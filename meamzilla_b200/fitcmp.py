@@ -21,8 +21,10 @@ from .optimize import lbfgs_fit, powell_fit
 from .potential import MZ_FP64, MZ_MIXED, Database, Evaluator, PotentialFile
 
 
-def build(workload: str, seed: int, ncells=None, max_candidates=1):
+def build(workload: str, seed: int, ncells=None, max_candidates=1, in_range=False):
     spec, cells = synth.make_workload(workload, seed=seed, ncells=ncells)
+    if in_range:
+        spec = synth.in_range_variant(spec)
     pot = PotentialFile.from_spec(spec)
     db = Database.from_cells(cells, pot)
     ev0 = Evaluator(db, pot, 1.0, 1.0, 0, max_candidates=1)
@@ -45,10 +47,12 @@ def main():
     ap.add_argument("--ncells", type=int, default=None)
     ap.add_argument("--powell-steps", type=int, default=20)
     ap.add_argument("--start-sigma", type=float, default=0.1)
+    ap.add_argument("--in-range", action="store_true",
+                    help="supplementary variant with densities inside U's range (synth.in_range_variant)")
     args = ap.parse_args()
-    pot, db, _ = build(args.workload, args.seed, args.ncells, max_candidates=1)
+    pot, db, ev = build(args.workload, args.seed, args.ncells, max_candidates=1, in_range=args.in_range)
     P = pot.ncoeff
-    _, _, ev = build(args.workload, args.seed, args.ncells, max_candidates=P)
+    pot, db, ev = build(args.workload, args.seed, args.ncells, max_candidates=P, in_range=args.in_range)
     rng = np.random.default_rng(77 + args.seed)
     x0 = pot.coeffs() + rng.normal(0.0, args.start_sigma, P)
     F0 = float(ev.objective(x0[None, :])[0])
@@ -57,7 +61,7 @@ def main():
     xm, Fm, im = lbfgs_fit(ev, x0, MZ_MIXED, maxiter=20000, target=Fp)
     st = db.stats()
     print(json.dumps({
-        "workload": args.workload, "natoms": st["natoms"], "ntriplets": st["ntriplets"], "ncoeff": P,
+        "workload": args.workload + (" (in-range variant)" if args.in_range else ""), "natoms": st["natoms"], "ntriplets": st["ntriplets"], "ncoeff": P,
         "start_objective": F0,
         "powell": {"objective": Fp, "seconds": ip["seconds"], "evals": ip["evals"], "outer": ip["outer"]},
         "lbfgs_fp64": {"objective": Fl, "seconds": il["seconds"], "evals": il["evals"],

@@ -164,13 +164,16 @@ class _DeviceResiduals:
 
 
 def powell_fit(ev: Evaluator, x0, max_steps: int = 1000, d_eps: float = 0.0, precision=MZ_FP64,
-               log: Optional[Callable[[str], None]] = None, max_evals: Optional[int] = None):
+               log: Optional[Callable[[str], None]] = None, max_evals: Optional[int] = None,
+               residuals: Optional[Callable] = None):
     """Powell least-squares fit of the coefficient vector x0.
 
+    `residuals(X) -> (obj[n], errvec[n, esize])` as torch tensors evaluates
+    many candidates at once; by default the evaluator's device residuals.
     Returns (x, F, info) with info = {outer, evals, seconds, history}."""
     import torch
     t0 = time.time()
-    res = _DeviceResiduals(ev, precision)
+    res = _DeviceResiduals(ev, precision) if residuals is None else residuals
     P = ev.ncoeff
     x = np.array(x0, dtype=np.float64)
     evals = [0]

@@ -293,9 +293,18 @@ class Evaluator:
         """The context's CUDA stream (cudaStream_t as an integer)."""
         return lib().mz_stream(self._h) or 0
 
+    @staticmethod
+    def _after_torch(t) -> None:
+        """The evaluator runs on its own stream: finish the work torch queued
+        on its current stream (e.g. the copy that produced `t`) first."""
+        import torch
+        torch.cuda.current_stream(t.device).synchronize()
+
     def objective_device(self, params, obj, precision=MZ_MIXED, errvec=None, forces=None) -> None:
         """params: (n, ncoeff) float64 CUDA tensor; obj: (n,) float64 CUDA tensor;
-        optional errvec (n, esize) and forces (n, natoms, 3) CUDA tensors."""
+        optional errvec (n, esize) and forces (n, natoms, 3) CUDA tensors.
+        Enqueued on stream(); call sync() before reading the outputs."""
+        self._after_torch(params)
         n = params.shape[0]
         ev = None if errvec is None else C.c_void_p(errvec.data_ptr())
         fo = None if forces is None else C.c_void_p(forces.data_ptr())
@@ -303,6 +312,8 @@ class Evaluator:
                                         C.c_void_p(obj.data_ptr()), ev, fo))
 
     def objective_grad_device(self, params, obj, grad, precision=MZ_MIXED) -> None:
+        """As objective_device, with grad an (n, ncoeff) float64 CUDA tensor."""
+        self._after_torch(params)
         n = params.shape[0]
         check(lib().mz_objective_grad_device(self._h, n, C.c_void_p(params.data_ptr()), int(precision),
                                              C.c_void_p(obj.data_ptr()), C.c_void_p(grad.data_ptr())))

@@ -293,6 +293,23 @@ def make_workload(name: str, seed: int = 0, ncells: Optional[int] = None):
     return pot, cells
 
 
+def in_range_variant(pot: PotSpec, rho_scale: float = 0.01, g_scale: float = 0.0025) -> PotSpec:
+    """Supplementary variant (labelled as such wherever used): the teacher's
+    rho and g scaled so that every embedding density of the MEAM workloads
+    falls inside U's knot range [-1, 1].  With the teacher as generated the
+    densities lie far outside it (20-150), the objective is almost all
+    density punishment and U's interior knots do not affect it."""
+    p = pot.copy()
+    for s in p.groups[1]:
+        s.y = s.y * rho_scale
+        s.grad = s.grad * rho_scale
+    if len(p.groups) > 4:
+        for s in p.groups[4]:
+            s.y = s.y * g_scale
+            s.grad = s.grad * g_scale
+    return p
+
+
 def perturbed(pot_coeffs: np.ndarray, n: int, sigma: float, seed: int) -> np.ndarray:
     """n candidate parameter vectors: coeffs + N(0, sigma) (GA population)."""
     rng = np.random.default_rng(seed)
