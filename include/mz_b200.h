@@ -236,6 +236,12 @@ void *mz_stream(mz_ctx *ctx);
 /* Counters since mz_create: kernel launches issued by this context. */
 mz_status mz_launch_count(const mz_ctx *ctx, int64_t *launches);
 
+/* Which mixed-precision MEAM forward the context runs: 1 = the tensor-core
+ * (tcgen05, TF32 split) triplet sums, opted into with the environment variable
+ * MZ_TC=1 when the context is created; 0 = the CUDA-core one-pass forward.
+ * No reference counterpart. */
+mz_status mz_tensor_core_forward(const mz_ctx *ctx, int *on);
+
 /* Kernels of the evaluator, for per-kernel timing. */
 enum {
   MZ_K_PREP = 0,    /* coefficients -> knot and evaluation tables          */

@@ -107,6 +107,7 @@ _SIGS = {
     "mz_sync": (C.c_int, [C.c_void_p]),
     "mz_stream": (C.c_void_p, [C.c_void_p]),
     "mz_launch_count": (C.c_int, [C.c_void_p, C.POINTER(C.c_int64)]),
+    "mz_tensor_core_forward": (C.c_int, [C.c_void_p, C.POINTER(C.c_int)]),
     "mz_kernel_name": (C.c_char_p, [C.c_int]),
     "mz_profile": (C.c_int, [C.c_void_p, C.c_int]),
     "mz_kernel_times": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),

@@ -31,6 +31,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <string>
@@ -40,6 +41,7 @@
 #include "mz_device.cuh"
 #include "mz_host.hpp"
 #include "mz_adj.cuh"
+#include "mz_tc_fwd.cuh"
 
 // ================================================================= context
 
@@ -64,6 +66,11 @@ struct mz_ctx {
   double *d_forces = nullptr, *d_cellobj = nullptr, *d_obj = nullptr, *d_errvec = nullptr;
   double *d_energy = nullptr, *d_stress = nullptr;
   double *d_aux = nullptr, *d_lam = nullptr, *d_seeds = nullptr, *d_partial = nullptr, *d_grad = nullptr;
+  float *d_ptabf = nullptr, *d_wtab = nullptr;  // FP32 evaluation tables, g B-spline coefficients
+  int *d_err = nullptr;                         // device-side failure flag (bounded waits)
+  TcParams tc{};                                // tensor-core forward plan
+  bool tc_ok = false;
+  int nsm = 1;
   size_t smem_atoms[2] = {0, 0};  // [FP64, MIXED]
   size_t smem_adj[2] = {0, 0};
   bool profiling = false;
@@ -132,6 +139,16 @@ void release(mz_ctx *ctx) {
   ctx->stream = nullptr;
 }
 
+// A kernel that gave up on a bounded wait sets the context's flag.
+void check_device_flag(mz_ctx *ctx) {
+  int e = 0;
+  ck(cudaMemcpy(&e, ctx->d_err, sizeof(int), cudaMemcpyDeviceToHost), "flag D2H");
+  if (e) {
+    ck(cudaMemset(ctx->d_err, 0, sizeof(int)), "flag reset");
+    throw Failure{MZ_ERR_CUDA, "a tensor-core completion wait timed out on the device"};
+  }
+}
+
 // Brackets one kernel launch with events when the context is profiling.
 struct Bracket {
   mz_ctx *ctx;
@@ -178,13 +195,25 @@ void enqueue(mz_ctx *ctx, int n, const double *d_params, int precision, double *
     Bracket b(ctx, MZ_K_PREP);
     k_prep<<<n, std::max(32, ((ctx->nsplines + 31) / 32) * 32), 0, st>>>(
         n, ctx->P, d_params, ctx->d_base, ctx->d_cmap, ctx->d_geom, ctx->d_nat, ctx->nsplines, ctx->stride,
-        ctx->d_tabs, ctx->pstride, ctx->d_ptabs);
+        ctx->d_tabs, ctx->pstride, ctx->d_ptabs, ctx->d_ptabf, meam ? ctx->d_wtab : nullptr, ctx->pot.s_g,
+        ctx->pot.ntypes, TC_NB);
     ck(cudaGetLastError(), "k_prep launch");
   }
   {
     Bracket b(ctx, MZ_K_ATOMS);
     const size_t sa = ctx->smem_atoms[mixed ? 1 : 0];
-    if (meam) {
+    if (meam && mixed && ctx->tc_ok) {
+      dim3 gt(std::min(ctx->nsm, ctx->natoms), (n + TC_CANDS - 1) / TC_CANDS);
+      const size_t st_bytes = (size_t)ctx->tc.smem_bytes;
+      if (grad)
+        k_atoms_tc<TC_NB, true><<<gt, TC_THREADS, st_bytes, st>>>(ctx->db, ctx->pot, ctx->tc, ctx->d_geom, ctx->d_tabs,
+                                                                 ctx->d_ptabf, ctx->d_wtab, n, ctx->d_V,
+                                                                 ctx->d_aout, ctx->d_aux, ctx->d_err);
+      else
+        k_atoms_tc<TC_NB, false><<<gt, TC_THREADS, st_bytes, st>>>(ctx->db, ctx->pot, ctx->tc, ctx->d_geom,
+                                                                  ctx->d_tabs, ctx->d_ptabf, ctx->d_wtab, n,
+                                                                  ctx->d_V, ctx->d_aout, ctx->d_aux, ctx->d_err);
+    } else if (meam) {
       if (mixed) grad ? launch_atoms<true, float, true>(ctx, n, sa) : launch_atoms<true, float, false>(ctx, n, sa);
       else grad ? launch_atoms<true, double, true>(ctx, n, sa) : launch_atoms<true, double, false>(ctx, n, sa);
     } else {
@@ -303,6 +332,7 @@ void run_host(mz_ctx *ctx, int ncand, const double *params, int precision, doubl
                          cudaMemcpyDeviceToHost, ctx->stream),
          "stress D2H");
     ck(cudaStreamSynchronize(ctx->stream), "objective");
+    check_device_flag(ctx);
   }
 }
 
@@ -514,6 +544,18 @@ mz_status mz_create(const mz_db *dbh, const mz_pot *poth, const mz_settings *set
     ck(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_adj<true, double>, BLOCK_SLOTS, ctx->smem_adj[0]),
        "occupancy");
     ctx->adj_ctas = std::max(1, std::min(d.nblocks, nsm * std::max(1, per_sm)));
+    ctx->nsm = nsm;
+    // tensor-core forward (mixed precision, MEAM with TC_NB B-spline coefficients per g spline)
+    {
+      const char *env = std::getenv("MZ_TC");  // opt-in: "1"
+      const bool allowed = env && env[0] == '1';
+      ctx->tc = tc_plan(db.max_row, TC_NB, pot.ntypes, ns, smem_max);
+      ctx->tc_ok = allowed && meam && ng + 2 == TC_NB && ctx->tc.smem_bytes > 0;
+      if (ctx->tc_ok) {
+        smem_attr(k_atoms_tc<TC_NB, false>, (size_t)ctx->tc.smem_bytes);
+        smem_attr(k_atoms_tc<TC_NB, true>, (size_t)ctx->tc.smem_bytes);
+      }
+    }
 
     // ---- work buffers: candidates per launch bounded by device memory
     size_t freeb = 0, totalb = 0;
@@ -542,6 +584,10 @@ mz_status mz_create(const mz_db *dbh, const mz_pot *poth, const mz_settings *set
     ctx->d_seeds = dalloc<double>(ctx, C * CS_COUNT * db.ncells);
     ctx->d_partial = dalloc<double>(ctx, C * (size_t)ctx->adj_ctas * stride);
     ctx->d_grad = dalloc<double>(ctx, C * ctx->P);
+    ctx->d_ptabf = dalloc<float>(ctx, C * ctx->pstride);
+    ctx->d_wtab = meam ? dalloc<float>(ctx, C * pot.ntypes * (2 * TC_NB - 1)) : nullptr;
+    ctx->d_err = dalloc<int>(ctx, 1);
+    ck(cudaMemset(ctx->d_err, 0, sizeof(int)), "flag init");
     *out = ctx;
   });
   if (st != MZ_OK && ctx) {
@@ -613,6 +659,7 @@ mz_status mz_sync(mz_ctx *ctx) {
   return guarded([&] {
     if (!ctx) throw Failure{MZ_ERR_ARG, "null context"};
     ck(cudaStreamSynchronize(ctx->stream), "sync");
+    check_device_flag(ctx);
   });
 }
 
@@ -677,6 +724,13 @@ mz_status mz_alu_peak(int device, int precision, double *tflops) {
     cudaEventDestroy(b);
     cudaFree(out);
     *tflops = 2.0 * 8.0 * (double)iters * threads * blocks / (best * 1e-3) / 1e12;
+  });
+}
+
+mz_status mz_tensor_core_forward(const mz_ctx *ctx, int *on) {
+  return guarded([&] {
+    if (!ctx || !on) throw Failure{MZ_ERR_ARG, "null argument"};
+    *on = ctx->tc_ok ? 1 : 0;
   });
 }
 

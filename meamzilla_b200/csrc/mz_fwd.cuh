@@ -21,7 +21,8 @@ enum { CS_EPS = 0, CS_MU0, CS_KAPPA = CS_MU0 + 6, CS_COUNT };
 __global__ void k_prep(int ncand, int P, const double *__restrict__ params, const double *__restrict__ base,
                        const int *__restrict__ cmap, const SplineGeom *__restrict__ geom,
                        const int *__restrict__ nat, int nsplines, int stride, double *__restrict__ tabs,
-                       int pstride, double *__restrict__ ptabs) {
+                       int pstride, double *__restrict__ ptabs, float *__restrict__ ptabf = nullptr,
+                       float *__restrict__ wtab = nullptr, int s_g = 0, int ng = 0, int nbp = 0) {
   const int c = blockIdx.x;
   const int s = threadIdx.x;
   if (c >= ncand || s >= nsplines) return;
@@ -68,6 +69,26 @@ __global__ void k_prep(int ncand, int P, const double *__restrict__ params, cons
     pc4[4 * k + 1] = y[k + 1] - y[k] - (2.0 * ypp[k] + ypp[k + 1]) * H;
     pc4[4 * k + 2] = 3.0 * ypp[k] * H;
     pc4[4 * k + 3] = (ypp[k + 1] - ypp[k]) * H;
+  }
+  if (ptabf) {  // FP32 copy of the evaluation table (mixed precision)
+    float *pf = ptabf + (size_t)c * pstride + g.poff;
+    for (int k = 0; k < 4 * (n - 1); ++k) pf[k] = (float)pc4[k];
+  }
+  if (wtab && s >= s_g && s < s_g + ng) {
+    // Cubic B-spline coefficients of g on its uniform grid (basis function m
+    // centred on knot m-1): S(x_i) = (w_i + 4 w_i+1 + w_i+2)/6 and
+    // S''(x_i) = (w_i - 2 w_i+1 + w_i+2)/h^2 give w_i+1 = y_i - h^2/6 y''_i,
+    // and the two outer coefficients follow from S'' at the end knots.
+    // Their differences are the coefficients of g' (times h) in the
+    // quadratic B-spline basis; both are stored: [w_0 .. w_nbp-1, dw_0 .. dw_nbp-2].
+    float *w = wtab + ((size_t)c * ng + (s - s_g)) * (2 * nbp - 1);
+    const double h2 = g.step * g.step;
+    double wm[66];
+    for (int i = 0; i < n; ++i) wm[i + 1] = y[i] - h2 / 6.0 * ypp[i];
+    wm[0] = h2 * ypp[0] + 2.0 * wm[1] - wm[2];
+    wm[n + 1] = h2 * ypp[n - 1] + 2.0 * wm[n] - wm[n - 1];
+    for (int i = 0; i < nbp; ++i) w[i] = i < n + 2 ? (float)wm[i] : 0.f;
+    for (int i = 0; i + 1 < nbp; ++i) w[nbp + i] = i + 1 < n + 2 ? (float)(wm[i + 1] - wm[i]) : 0.f;
   }
 }
 
@@ -214,7 +235,7 @@ __device__ __forceinline__ void warp_slot_sums(const double *red, int lo, int hi
 // receives -V_p (k_gather).  In FP32 the row sums are taken in chunks of 8
 // terms, each chunk added to an FP64 total.
 template <bool MEAM, typename R, bool AUX>
-__global__ void __launch_bounds__(BLOCK_SLOTS, 3)
+__global__ void __launch_bounds__(BLOCK_SLOTS, sizeof(R) == 4 ? 4 : 3)
     k_atoms(DevDb db, DevPot pot, const SplineGeom *__restrict__ geom, const double *__restrict__ tabs,
             const double *__restrict__ ptabs, double *__restrict__ Vout, double *__restrict__ aout,
             double *__restrict__ aux) {

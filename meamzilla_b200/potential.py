@@ -283,6 +283,13 @@ class Evaluator:
         check(lib().mz_densities(self._h, ptr(x), ptr(d)))
         return d
 
+    def tensor_core_forward(self) -> bool:
+        """True when the mixed MEAM forward runs its triplet sums on the
+        tensor cores (opt-in: MZ_TC=1 in the environment at construction)."""
+        on = C.c_int()
+        check(lib().mz_tensor_core_forward(self._h, C.byref(on)))
+        return bool(on.value)
+
     def launches(self) -> int:
         n = C.c_int64()
         check(lib().mz_launch_count(self._h, C.byref(n)))

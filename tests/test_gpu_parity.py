@@ -130,3 +130,25 @@ def test_potential_interface_compute_and_dir():
     v2 = pot.compute_dir(None, d, 0.5)
     assert rel(v2, orc.objective(pot.x + 0.5 * d)) <= FP64_OBJ
     assert pot.get_error() == val  # compute_dir works on a clone
+
+
+@pytest.mark.parametrize("name", ["meam2_edge", "meam_mix6"])
+def test_tensor_core_forward_opt_in(name, monkeypatch):
+    """The opt-in tensor-core forward (tcgen05 TF32 MMAs, split hi/lo operands)
+    against FP64.  The MMA's FP32 accumulation truncates (measured on B200:
+    each K-step result lies 0 to 0.5 ulp below the exact sum), so its
+    accuracy sits above the CUDA-core path's; these bounds record it."""
+    from meamzilla_b200.potential import MZ_FP64, MZ_MIXED, Evaluator
+    case = load_case(name)
+    g = case["gold"]
+    x = np.stack([g["coeff"], g["coeff2"]])
+    monkeypatch.setenv("MZ_TC", "1")
+    ev = Evaluator(case["db"], case["pot"], max_candidates=2, **case["weights"])
+    monkeypatch.delenv("MZ_TC")
+    ref = Evaluator(case["db"], case["pot"], max_candidates=2, **case["weights"])
+    assert ev.tensor_core_forward() and not ref.tensor_core_forward()
+    a = ref.objective(x, MZ_FP64, forces=True)
+    b = ev.objective(x, MZ_MIXED, forces=True)
+    for c in range(2):
+        assert rel(b["obj"][c], a["obj"][c]) <= 3e-6
+        assert np.max(np.abs(b["forces"][c] - a["forces"][c])) <= 5e-5
