@@ -122,6 +122,12 @@ typedef struct {
 mz_status mz_db_build(const mz_cells_desc *cells, const mz_pot *pot, mz_db **out);
 /* Read a configuration file (#N/#X/#Y/#Z/#E/#S/#W/#EW/#SW/#F) and build. */
 mz_status mz_db_read(const char *config_path, const mz_pot *pot, mz_db **out);
+/* The same two, with the periodic-image pair search and knot / shift set-up
+ * run on GPU `device` (one thread per atom, the host builder's loop order and
+ * rounding): the resulting database is identical, array for array, to
+ * mz_db_build's, and the same errors are reported. */
+mz_status mz_db_build_device(const mz_cells_desc *cells, const mz_pot *pot, int device, mz_db **out);
+mz_status mz_db_read_device(const char *config_path, const mz_pot *pot, int device, mz_db **out);
 void mz_db_free(mz_db *db);
 
 typedef struct {

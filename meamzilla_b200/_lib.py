@@ -92,6 +92,8 @@ _SIGS = {
     "mz_pot_get_spline": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(SplineView)]),
     "mz_db_build": (C.c_int, [C.POINTER(CellsDesc), C.c_void_p, C.POINTER(C.c_void_p)]),
     "mz_db_read": (C.c_int, [C.c_char_p, C.c_void_p, C.POINTER(C.c_void_p)]),
+    "mz_db_build_device": (C.c_int, [C.POINTER(CellsDesc), C.c_void_p, C.c_int, C.POINTER(C.c_void_p)]),
+    "mz_db_read_device": (C.c_int, [C.c_char_p, C.c_void_p, C.c_int, C.POINTER(C.c_void_p)]),
     "mz_db_free": (None, [C.c_void_p]),
     "mz_db_info": (C.c_int, [C.c_void_p, C.POINTER(DbStats)]),
     "mz_db_get_view": (C.c_int, [C.c_void_p, C.POINTER(DbView)]),

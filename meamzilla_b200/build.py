@@ -21,7 +21,7 @@ LIB = os.path.join(HERE, "libmz_b200.so")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
-SOURCES = ["mz_host.cpp", "mz_device.cu"]
+SOURCES = ["mz_host.cpp", "mz_device.cu", "mz_nbr.cu"]
 
 
 def nvcc() -> str:

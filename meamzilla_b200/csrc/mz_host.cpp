@@ -382,7 +382,7 @@ struct CellPairs {
 };
 }  // namespace
 
-void build_db(const mz_cells_desc &c, const Pot &pot, Db &db) {
+void build_db_setup(const mz_cells_desc &c, const Pot &pot, Db &db) {
   if (c.ncells <= 0 || c.natoms <= 0 || !c.cell_natoms || !c.cell_lattice || !c.atom_type || !c.atom_pos)
     fail(MZ_ERR_ARG, "empty or incomplete cell description");
   const bool meam = pot.style == MZ_STYLE_MEAM_SPLINE;
@@ -420,7 +420,46 @@ void build_db(const mz_cells_desc &c, const Pot &pot, Db &db) {
         fail(MZ_ERR_FORMAT, "incorrect atom type specified - cell=" + std::to_string(i));
       db.atom_cell[a] = i;
     }
+}
 
+bool cell_scale(const double *A, double max_rcut, double *vol, int s[3]) {
+  // Cell::compute_vol (cell.cpp:191-194) and Cell::find_scale (cell.cpp:158-170)
+  V3 a0{A[0], A[1], A[2]}, a1{A[3], A[4], A[5]}, a2{A[6], A[7], A[8]};
+  *vol = std::abs(dot(a0, cross(a1, a2)));
+  double ihx = mag(cross(a1, a2)) / *vol, ihy = mag(cross(a2, a0)) / *vol, ihz = mag(cross(a0, a1)) / *vol;
+  s[0] = int(std::ceil(max_rcut * ihx));
+  s[1] = int(std::ceil(max_rcut * ihy));
+  s[2] = int(std::ceil(max_rcut * ihz));
+  return s[0] > 0 && s[1] > 0 && s[2] > 0;
+}
+
+std::string cell_too_small_msg(int ci) {
+  return "ERROR: Cell #" + std::to_string(ci) + " is too small or potential is too big";
+}
+
+std::string pair_too_short_msg(const Pot &pot, int q, double rr, int ti, int tj, int ci, int i, int j) {
+  static const char *nm[3] = {"phi", "rho", "f"};
+  char buf[256];
+  std::snprintf(buf, sizeof buf,
+                "ERROR: Pair distance too short for potential (r=%g, pot=%s[%d]) - cell=%d atom=%d neigh=%d", rr,
+                nm[q], q == 1 ? tj : pot.idx_pair_ij(ti, tj), ci, i, j);
+  return buf;
+}
+
+void build_incoming(Db &db) {
+  // Incoming lists (counting sort by neighbour, slot order kept).
+  const int64_t np = db.npairs;
+  db.in_off.assign(db.natoms + 1, 0);
+  for (int64_t s = 0; s < np; ++s) db.in_off[db.pair_nbr[s] + 1]++;
+  for (int a = 0; a < db.natoms; ++a) db.in_off[a + 1] += db.in_off[a];
+  db.in_slot.resize(np);
+  std::vector<int64_t> fill(db.in_off.begin(), db.in_off.end() - 1);
+  for (int64_t s = 0; s < np; ++s) db.in_slot[fill[db.pair_nbr[s]]++] = s;
+}
+
+void build_db(const mz_cells_desc &c, const Pot &pot, Db &db) {
+  build_db_setup(c, pot, db);
+  const bool meam = pot.style == MZ_STYLE_MEAM_SPLINE;
   const double max_rcut = pot.max_rcut();
   const int sphi0 = pot.spline_index(G_PHI, 0), srho0 = pot.spline_index(G_RHO, 0);
   const int sf0 = meam ? pot.spline_index(G_F, 0) : -1;
@@ -434,17 +473,13 @@ void build_db(const mz_cells_desc &c, const Pot &pot, Db &db) {
       CellPairs &out = per[ci];
       const double *A = c.cell_lattice + 9 * (size_t)ci;
       V3 a0{A[0], A[1], A[2]}, a1{A[3], A[4], A[5]}, a2{A[6], A[7], A[8]};
-      // Cell::compute_vol (cell.cpp:191-194) and Cell::find_scale (cell.cpp:158-170)
-      double vol = std::abs(dot(a0, cross(a1, a2)));
-      db.cell_vol[ci] = vol;
-      double ihx = mag(cross(a1, a2)) / vol, ihy = mag(cross(a2, a0)) / vol, ihz = mag(cross(a0, a1)) / vol;
-      double sx = int(std::ceil(max_rcut * ihx)), sy = int(std::ceil(max_rcut * ihy)),
-             sz = int(std::ceil(max_rcut * ihz));
-      if (!(sx > 0 && sy > 0 && sz > 0)) {
+      int sc[3];
+      if (!cell_scale(A, max_rcut, &db.cell_vol[ci], sc)) {
         out.status = MZ_ERR_RANGE;
-        out.msg = "ERROR: Cell #" + std::to_string(ci) + " is too small or potential is too big";
+        out.msg = cell_too_small_msg(ci);
         return;
       }
+      const int sx = sc[0], sy = sc[1], sz = sc[2];
       const int a_lo = db.cell_atom0[ci], na = db.cell_atom0[ci + 1] - a_lo;
       // Config::find_pairs (config.cpp:143-234), double counted (j0 = 0)
       for (int i = 0; i < na && out.status == MZ_OK; ++i) {
@@ -470,19 +505,14 @@ void build_db(const mz_cells_desc &c, const Pot &pot, Db &db) {
                 // check_pair (pair_meam_spline.cpp:50-99 / pair_eam_spline.cpp:50-86)
                 int sidx[3] = {sphi0 + pot.idx_pair_ij(ti, tj), srho0 + tj,
                                meam ? sf0 + pot.idx_pair_ij(ti, tj) : -1};
-                const char *nm[3] = {"phi", "rho", "f"};
                 int kn[3] = {-1, -1, -1};
                 double sh[3] = {0, 0, 0};
                 bool bad = false;
                 for (int q = 0; q < (meam ? 3 : 2); ++q) {
                   const Spline3 &sp = pot.spline(sidx[q]);
                   if (rr < sp.x[0]) {
-                    char buf[256];
-                    std::snprintf(buf, sizeof buf,
-                                  "ERROR: Pair distance too short for potential (r=%g, pot=%s[%d]) - cell=%d atom=%d neigh=%d",
-                                  rr, nm[q], q == 1 ? tj : pot.idx_pair_ij(ti, tj), ci, i, j);
                     out.status = MZ_ERR_RANGE;
-                    out.msg = buf;
+                    out.msg = pair_too_short_msg(pot, q, rr, ti, tj, ci, i, j);
                     bad = true;
                     break;
                   }
@@ -546,13 +576,7 @@ void build_db(const mz_cells_desc &c, const Pot &pot, Db &db) {
     o += (int64_t)n;
     CellPairs().nbr.swap(p.nbr);
   }
-  // Incoming lists (counting sort by neighbour, slot order kept).
-  db.in_off.assign(c.natoms + 1, 0);
-  for (int64_t s = 0; s < np; ++s) db.in_off[db.pair_nbr[s] + 1]++;
-  for (int a = 0; a < c.natoms; ++a) db.in_off[a + 1] += db.in_off[a];
-  db.in_slot.resize(np);
-  std::vector<int64_t> fill(db.in_off.begin(), db.in_off.end() - 1);
-  for (int64_t s = 0; s < np; ++s) db.in_slot[fill[db.pair_nbr[s]]++] = s;
+  build_incoming(db);
 }
 
 }  // namespace mzb
@@ -664,23 +688,34 @@ mz_status mz_pot_spline_eval(const mz_pot *pot, int s, double x, double *val, do
   });
 }
 
+static void build_any(const mz_cells_desc &c, const mz_pot *pot, int device, mz_db **out) {
+  auto *d = new mz_db;
+  try {
+    if (device >= 0) build_db_device(c, pot->pot, d->db, device);
+    else build_db(c, pot->pot, d->db);
+  } catch (...) {
+    delete d;
+    throw;
+  }
+  *out = d;
+}
+
 mz_status mz_db_build(const mz_cells_desc *cells, const mz_pot *pot, mz_db **out) {
   return guarded([&] {
     if (!cells || !pot || !out) fail(MZ_ERR_ARG, "null argument");
-    auto *d = new mz_db;
-    try {
-      build_db(*cells, pot->pot, d->db);
-    } catch (...) {
-      delete d;
-      throw;
-    }
-    *out = d;
+    build_any(*cells, pot, -1, out);
   });
 }
 
-mz_status mz_db_read(const char *path, const mz_pot *pot, mz_db **out) {
+mz_status mz_db_build_device(const mz_cells_desc *cells, const mz_pot *pot, int device, mz_db **out) {
   return guarded([&] {
-    if (!path || !pot || !out) fail(MZ_ERR_ARG, "null argument");
+    if (!cells || !pot || !out || device < 0) fail(MZ_ERR_ARG, "null argument or negative device");
+    build_any(*cells, pot, device, out);
+  });
+}
+
+static void read_any(const char *path, const mz_pot *pot, int device, mz_db **out) {
+  {
     std::vector<int> cn, types;
     std::vector<double> lat, e0, s0, w, ew, sw, pos, f0;
     read_config_file(path, pot->pot.ntypes, cn, lat, e0, s0, w, ew, sw, types, pos, f0);
@@ -697,14 +732,21 @@ mz_status mz_db_read(const char *path, const mz_pot *pot, mz_db **out) {
     c.atom_type = types.data();
     c.atom_pos = pos.data();
     c.atom_force0 = f0.data();
-    auto *d = new mz_db;
-    try {
-      build_db(c, pot->pot, d->db);
-    } catch (...) {
-      delete d;
-      throw;
-    }
-    *out = d;
+    build_any(c, pot, device, out);
+  }
+}
+
+mz_status mz_db_read(const char *path, const mz_pot *pot, mz_db **out) {
+  return guarded([&] {
+    if (!path || !pot || !out) fail(MZ_ERR_ARG, "null argument");
+    read_any(path, pot, -1, out);
+  });
+}
+
+mz_status mz_db_read_device(const char *path, const mz_pot *pot, int device, mz_db **out) {
+  return guarded([&] {
+    if (!path || !pot || !out || device < 0) fail(MZ_ERR_ARG, "null argument or negative device");
+    read_any(path, pot, device, out);
   });
 }
 

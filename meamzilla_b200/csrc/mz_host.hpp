@@ -96,6 +96,16 @@ struct Db {
 
 // Build lists (throws std::runtime_error with an mz status prefix).
 void build_db(const mz_cells_desc &cells, const Pot &pot, Db &db);
+// The same lists from the GPU (mz_nbr.cu); identical arrays.
+void build_db_device(const mz_cells_desc &cells, const Pot &pot, Db &db, int device);
+// Pieces shared by both builders: cells / atoms / validation, the periodic
+// image range of one cell (false when the cell is too small), the incoming
+// lists, and the reference's error texts.
+void build_db_setup(const mz_cells_desc &cells, const Pot &pot, Db &db);
+bool cell_scale(const double *lattice9, double max_rcut, double *vol, int s[3]);
+void build_incoming(Db &db);
+std::string cell_too_small_msg(int ci);
+std::string pair_too_short_msg(const Pot &pot, int q, double rr, int ti, int tj, int ci, int i, int j);
 void parse_pot(const std::string &text, Pot &pot);
 std::string write_pot_text(const Pot &pot);
 void read_config_file(const std::string &path, int ntypes, std::vector<int> &cell_natoms,

@@ -145,14 +145,20 @@ class Database:
         self.pot = pot
 
     @classmethod
-    def read(cls, config_path: str, pot: PotentialFile) -> "Database":
+    def read(cls, config_path: str, pot: PotentialFile, device: Optional[int] = None) -> "Database":
+        """Read a configuration file; with `device`, the neighbour lists are
+        built on that GPU (identical result)."""
         h = C.c_void_p()
-        check(lib().mz_db_read(config_path.encode(), pot.handle, C.byref(h)))
+        if device is None:
+            check(lib().mz_db_read(config_path.encode(), pot.handle, C.byref(h)))
+        else:
+            check(lib().mz_db_read_device(config_path.encode(), pot.handle, int(device), C.byref(h)))
         return cls(h, pot)
 
     @classmethod
-    def from_cells(cls, cells: Sequence, pot: PotentialFile) -> "Database":
-        """From a list of synth.Cell (lattice rows, types, positions, targets)."""
+    def from_cells(cls, cells: Sequence, pot: PotentialFile, device: Optional[int] = None) -> "Database":
+        """From a list of synth.Cell (lattice rows, types, positions, targets);
+        with `device`, the neighbour lists are built on that GPU."""
         nat = np.array([c.natoms for c in cells], dtype=np.int32)
         lat = np.ascontiguousarray(np.stack([np.asarray(c.lattice, dtype=np.float64) for c in cells]))
         e0 = np.array([c.energy0 for c in cells], dtype=np.float64)
@@ -179,7 +185,10 @@ class Database:
         d.atom_pos = pos.ctypes.data_as(dp)
         d.atom_force0 = f0.ctypes.data_as(dp)
         h = C.c_void_p()
-        check(lib().mz_db_build(C.byref(d), pot.handle, C.byref(h)))
+        if device is None:
+            check(lib().mz_db_build(C.byref(d), pot.handle, C.byref(h)))
+        else:
+            check(lib().mz_db_build_device(C.byref(d), pot.handle, int(device), C.byref(h)))
         return cls(h, pot)
 
     def __del__(self):
