@@ -77,6 +77,8 @@ mz_status mz_pot_read(const char *path, mz_pot **out);
 /* Same from the file's text held in memory. */
 mz_status mz_pot_parse(const char *text, mz_pot **out);
 void mz_pot_free(mz_pot *pot);
+/* An independent copy of a potential (Potential::clone, src/potential.h:43). */
+mz_status mz_pot_clone(const mz_pot *pot, mz_pot **out);
 /* Style (MZ_STYLE_*), number of atom types, number of splines. */
 mz_status mz_pot_info(const mz_pot *pot, int *style, int *ntypes, int *nsplines);
 /* Number of adjustable coefficients: Potential::get_ncoeff (potential.h:59). */
@@ -91,6 +93,26 @@ mz_status mz_pot_write(const mz_pot *pot, const char *path);
  * Spline3Eq::splint_comb(double, double*) (spline3eq.h:204-236), linear
  * extrapolation outside the knots.  Host-side, for tests and tools. */
 mz_status mz_pot_spline_eval(const mz_pot *pot, int spline, double x, double *val, double *grad);
+
+/* Potential::rescale (src/potential.h:68) for the spline styles, in place:
+ * PotMEAM::rescale (pot_meam.cpp:281-375, with rescale_3body :497-525) or
+ * PotEAM::rescale (pot_eam.cpp:257-389, with the U'(mid) = 0 gauge).  The
+ * per-atom densities of the potential's current coefficients (mz_densities)
+ * and the database's atom types drive it; flag as the reference's (< 0
+ * never, 0 when needed, 1 always).  *rescaled = the reference's return value;
+ * factors[0] = embedding scale a, factors[1] = MEAM f scale b (0 if unused).
+ * U's knot grid changes, so evaluators must be re-created afterwards. */
+mz_status mz_pot_rescale(mz_pot *pot, const mz_db *db, const double *densities, int flag, int *rescaled,
+                         double *factors);
+
+/* Potential::write_data (src/potential.cpp:325-342): the .rho, .energy,
+ * .stress, .force, .error and .punish files of one evaluated potential
+ * (<prefix>.<ext>, or <prefix>.<ext>.<num> when num >= 0), formatted as the
+ * reference writes them, from the outputs of one FP64 mz_objective call
+ * (errvec, per-cell energy per atom and stress, forces) and mz_densities. */
+mz_status mz_write_data(const mz_db *db, const mz_pot *pot, double energy_weight, double stress_weight,
+                        const double *errvec, const double *energy, const double *stress, const double *forces,
+                        const double *densities, const char *prefix, int num);
 
 /* ----------------------------------------------------------------- database */
 
@@ -176,6 +198,8 @@ typedef struct {
   double grad[2];
   const int *y_fixed;
   const double *y;
+  const double *x;    /* knot positions [nknots] (rescale moves them)  */
+  double step;        /* knot spacing                                   */
 } mz_spline_view;
 mz_status mz_pot_get_spline(const mz_pot *pot, int spline, mz_spline_view *view);
 

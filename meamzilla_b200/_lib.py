@@ -68,7 +68,8 @@ class DbView(C.Structure):
 class SplineView(C.Structure):
     _fields_ = [("group", C.c_int), ("alloy", C.c_int), ("nknots", C.c_int), ("left", C.c_double),
                 ("right", C.c_double), ("nat", C.c_int * 2), ("grad_fixed", C.c_int * 2),
-                ("grad", C.c_double * 2), ("y_fixed", C.POINTER(C.c_int)), ("y", C.POINTER(C.c_double))]
+                ("grad", C.c_double * 2), ("y_fixed", C.POINTER(C.c_int)), ("y", C.POINTER(C.c_double)),
+                ("x", C.POINTER(C.c_double)), ("step", C.c_double)]
 
 
 class Settings(C.Structure):
@@ -92,6 +93,10 @@ _SIGS = {
     "mz_pot_get_spline": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(SplineView)]),
     "mz_db_build": (C.c_int, [C.POINTER(CellsDesc), C.c_void_p, C.POINTER(C.c_void_p)]),
     "mz_db_read": (C.c_int, [C.c_char_p, C.c_void_p, C.POINTER(C.c_void_p)]),
+    "mz_write_data": (C.c_int, [C.c_void_p, C.c_void_p, C.c_double, C.c_double] + [C.c_void_p] * 5 +
+                      [C.c_char_p, C.c_int]),
+    "mz_pot_clone": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
+    "mz_pot_rescale": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.POINTER(C.c_int), C.c_void_p]),
     "mz_db_build_device": (C.c_int, [C.POINTER(CellsDesc), C.c_void_p, C.c_int, C.POINTER(C.c_void_p)]),
     "mz_db_read_device": (C.c_int, [C.c_char_p, C.c_void_p, C.c_int, C.POINTER(C.c_void_p)]),
     "mz_db_free": (None, [C.c_void_p]),

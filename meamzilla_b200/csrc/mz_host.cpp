@@ -10,6 +10,7 @@
 #include <cstdio>
 #include <cstring>
 #include <fstream>
+#include <iomanip>
 #include <sstream>
 #include <stdexcept>
 #include <thread>
@@ -103,6 +104,100 @@ double Spline3::eval(const std::vector<double> &ypp, double r, double *g) const 
   double p1 = y[k], d21 = ypp[k], p2 = y[k + 1], d22 = ypp[k + 1];
   *g = (p2 - p1) * invstep + ((3 * (b * b) - 1) * d22 - (3 * (a * a) - 1) * d21) * step / 6.0;
   return a * p1 + b * p2 + ((a * a * a - a) * d21 + (b * b * b - b) * d22) * (step * step) / 6.0;
+}
+
+void Spline3::readjust_x(double l, double r) {
+  // Spline3Eq::readjust_x (spline3eq.cpp:112-143)
+  std::vector<double> ypp;
+  refresh(ypp);
+  const Spline3 old = *this;
+  step = (r - l) / (nknots - 1);
+  invstep = 1.0 / step;
+  x[0] = l;
+  x[nknots - 1] = r;
+  for (int i = 1; i < nknots - 1; ++i) x[i] = l + i * step;
+  double g;
+  for (int i = 0; i < nknots; ++i) y[i] = old.eval(ypp, x[i], &g);
+  if (!nat[0]) {
+    old.eval(ypp, l, &g);
+    grad[0] = g;
+  }
+  if (!nat[1]) {
+    old.eval(ypp, r, &g);
+    grad[1] = g;
+  }
+  left = x[0];
+  right = x[nknots - 1];
+}
+
+void Spline3::rescale_x(double scale) {
+  // Spline3Eq::rescale_x (spline3eq.cpp:150-171)
+  step *= std::abs(scale);
+  invstep = 1.0 / step;
+  for (int i = 0; i < nknots; ++i) x[i] *= scale;
+  if (!nat[0]) grad[0] /= scale;
+  if (!nat[1]) grad[1] /= scale;
+  if (scale < 0.0) {
+    std::reverse(x.begin(), x.end());
+    std::reverse(y.begin(), y.end());
+    std::swap(nat[0], nat[1]);
+    std::reverse(y_fixed.begin(), y_fixed.end());
+    std::swap(grad[0], grad[1]);
+    std::swap(grad_fixed[0], grad_fixed[1]);
+  }
+  left = x[0];
+  right = x[nknots - 1];
+}
+
+void Spline3::scale_y(double f) {
+  // Spline3Eq::operator*= (spline3eq.cpp:301-313)
+  for (int i = 0; i < nknots; ++i) y[i] *= f;
+  if (!nat[0]) grad[0] *= f;
+  if (!nat[1]) grad[1] *= f;
+}
+
+void Spline3::divide_y(double f) {
+  // Spline3Eq::operator/= (spline3eq.cpp:318-330)
+  for (int i = 0; i < nknots; ++i) y[i] /= f;
+  if (!nat[0]) grad[0] /= f;
+  if (!nat[1]) grad[1] /= f;
+}
+
+void Spline3::add(const Spline3 &rhs, const std::vector<double> &rhs_ypp) {
+  // Spline3Eq::operator+= (spline3eq.cpp:335-348)
+  const double rmax = rhs.x.back();
+  double g;
+  for (int i = 0; i < nknots; ++i) y[i] += (x[i] < rmax) ? rhs.eval(rhs_ypp, x[i], &g) : 0.;
+  if (!nat[0]) {
+    double v = 0.;
+    if (x[0] < rmax) {
+      rhs.eval(rhs_ypp, x[0], &g);
+      v = g;
+    }
+    grad[0] += v;
+  }
+  if (!nat[1]) {
+    double v = 0.;
+    if (x.back() < rmax) {
+      rhs.eval(rhs_ypp, x.back(), &g);
+      v = g;
+    }
+    grad[1] += v;
+  }
+}
+
+void Spline3::add_linear(double a) {
+  // Spline3Eq::add_linear (spline3eq.cpp:177-186)
+  for (int i = 0; i < nknots; ++i) y[i] += a * x[i];
+  if (!nat[0]) grad[0] += a;
+  if (!nat[1]) grad[1] += a;
+}
+
+double Spline3::max_y_mag() const {
+  double m = 0.0;
+  for (double v : y)
+    if (std::abs(m) < std::abs(v)) m = v;
+  return m;
 }
 
 // ---------------------------------------------------------------------- Pot
@@ -360,6 +455,261 @@ void read_config_file(const std::string &path, int ntypes, std::vector<int> &cel
   }
 }
 
+// ------------------------------------------------------------------ rescale
+
+int rescale_pot(Pot &pot, const int *atom_type, int natoms, const double *dens, int flag, double factors[2]) {
+  // PotMEAM::rescale (pot_meam.cpp:281-375) / PotEAM::rescale (pot_eam.cpp:257-389)
+  factors[0] = factors[1] = 0.0;
+  if (flag < 0) return 0;
+  const bool meam = pot.style == MZ_STYLE_MEAM_SPLINE;
+  std::vector<Spline3> &F = pot.groups[G_U];
+  const int Fs = (int)F.size();
+  std::vector<double> minrho(Fs, 1e100), maxrho(Fs, -1e100);
+  for (int i = 0; i < natoms; ++i) {
+    const int t = atom_type[i];
+    maxrho[t] = std::max(dens[i], maxrho[t]);
+    minrho[t] = std::min(dens[i], minrho[t]);
+  }
+  double min_density = 1e100, max_density = -1e100;
+  int min_idx = -1, max_idx = -1;
+  for (int i = 0; i < Fs; ++i) {
+    if (maxrho[i] > max_density) {
+      max_density = maxrho[i];
+      max_idx = i;
+    }
+    if (minrho[i] < min_density) {
+      min_density = minrho[i];
+      min_idx = i;
+    }
+  }
+  if (max_idx < 0 || min_idx < 0) return 0;  // no atoms: nothing to measure
+  const int sign = (max_density >= -min_density) ? 1 : -1;
+  std::vector<double> L(Fs), R(Fs);
+  for (int i = 0; i < Fs; ++i) {
+    const double rho_i = F[i].x[0], rho_f = F[i].x.back(), length = rho_f - rho_i;
+    L[i] = minrho[i] - 0.01 * length;
+    R[i] = maxrho[i] + 0.01 * length;
+    if (flag || minrho[i] - rho_i < 0. || minrho[i] - rho_i > 0.05 * length || maxrho[i] - rho_f > 0. ||
+        maxrho[i] - rho_f < -0.05 * length)
+      flag = 1;
+    if (R[i] - rho_f > 100.0 || L[i] - rho_i < -100.0) return 0;  // bounds too big
+  }
+  const double a = (sign == 1) ? 1.0 / R[max_idx] : 1.0 / L[min_idx];
+  if (flag || std::abs(a) > 1.05 || std::abs(a) < 0.95) flag = 1;
+  if (meam && flag) {
+    // PotMEAM::rescale_3body (pot_meam.cpp:497-525): f*f*g = (b f)(b f)(g / b^2),
+    // b = 1 / signed largest-|y| knot of the f group (PotFns::get_max_y_mag, pot_fns.cpp:100-111)
+    double m = 0.0;
+    for (const Spline3 &sp : pot.groups[G_F]) {
+      const double v = sp.max_y_mag();
+      if (std::abs(m) < std::abs(v)) m = v;
+    }
+    const double b = 1.0 / m;
+    for (Spline3 &sp : pot.groups[G_F]) sp.scale_y(b);
+    for (Spline3 &sp : pot.groups[G_G]) sp.divide_y(b * b);
+    factors[1] = b;
+  }
+  if (!flag) return 0;
+  for (int i = 0; i < Fs; ++i) {
+    F[i].readjust_x(L[i], R[i]);
+    F[i].rescale_x(a);
+  }
+  for (Spline3 &sp : pot.groups[G_RHO]) sp.scale_y(a);
+  if (meam)
+    for (Spline3 &sp : pot.groups[G_G]) sp.scale_y(a);
+  factors[0] = a;
+  if (!meam) {
+    // Gauge U'(mid) = 0 (pot_eam.cpp:336-383): lambda_i = U_i'(mid of its range),
+    // phi_ij += lambda_j rho_i + lambda_i rho_j, U_i -= lambda_i n.  The
+    // reference adds a copy of rho scaled in y whose second derivatives are
+    // the unscaled rho's; so does this.
+    std::vector<Spline3> &rho = pot.groups[G_RHO];
+    std::vector<Spline3> &phi = pot.groups[G_PHI];
+    std::vector<std::vector<double>> rho_ypp(rho.size());
+    for (size_t i = 0; i < rho.size(); ++i) rho[i].refresh(rho_ypp[i]);
+    std::vector<double> lam(Fs);
+    for (int i = 0; i < Fs; ++i) {
+      std::vector<double> ypp;
+      F[i].refresh(ypp);
+      double g;
+      F[i].eval(ypp, 0.5 * (F[i].x[0] + F[i].x.back()), &g);
+      lam[i] = g;
+    }
+    int count = 0;
+    for (int i = 0; i < Fs; ++i)
+      for (int j = i; j < Fs; ++j) {
+        Spline3 t = rho[i];
+        t.scale_y(lam[j]);
+        phi[count].add(t, rho_ypp[i]);
+        Spline3 t2 = rho[j];
+        t2.scale_y(lam[i]);
+        phi[count].add(t2, rho_ypp[j]);
+        ++count;
+      }
+    for (int i = 0; i < Fs; ++i) F[i].add_linear(-1.0 * lam[i]);
+  }
+  return 1;
+}
+
+// -------------------------------------------------------------- data files
+
+namespace {
+std::string data_name(const std::string &prefix, const char *ext, int num) {
+  std::ostringstream oss;
+  oss << prefix << ext;
+  if (num >= 0) oss << "." << num;
+  return oss.str();
+}
+std::ofstream open_out(const std::string &path) {
+  std::ofstream f(path, std::ios_base::out);
+  if (!f) throw Failure{MZ_ERR_IO, "cannot write " + path};
+  return f;
+}
+}  // namespace
+
+void write_data_files(const Db &db, const Pot &pot, double energy_weight, double stress_weight, const double *e,
+                      const double *energy, const double *stress, const double *force, const double *dens,
+                      const std::string &prefix, int num) {
+  // Potential::write_data (potential.cpp:325-342): .rho (PotEAM::write_densities
+  // pot_eam.cpp:506-540), .energy (:497-543), .stress (:548-592), .force
+  // (:597-642), .error (:647-708), .punish (PotEAM / PotMEAM::write_punish).
+  const int NC = db.ncells, N = db.natoms;
+  const bool meam = pot.style == MZ_STYLE_MEAM_SPLINE;
+  const int npen = meam ? 1 : pot.ntypes;
+  const int esize = 8 * NC + 3 * N + npen;
+  {
+    std::ofstream f = open_out(data_name(prefix, ".rho", num));
+    f << std::setw(6) << std::right << "conf:" << std::setw(5) << std::right << "atom" << std::setw(8) << std::right
+      << "type" << std::setw(15) << std::right << "rho" << std::endl;
+    for (int c = 0; c < NC; ++c)
+      for (int i = 0; i < db.cell_atom0[c + 1] - db.cell_atom0[c]; ++i) {
+        const int a = db.cell_atom0[c] + i;
+        f << std::setw(5) << std::right << c << ":" << std::setw(5) << std::right << i << std::setw(8) << std::right
+          << db.atom_type[a] << std::setw(15) << std::right << std::fixed << dens[a] << std::endl;
+      }
+  }
+  {
+    std::ofstream f = open_out(data_name(prefix, ".energy", num));
+    f << "Global energy weight is " << std::fixed << energy_weight << std::endl;
+    f << std::setw(3) << std::right << "#" << std::setw(11) << std::right << "conf_w" << std::setw(11) << std::right
+      << "conf_ew" << std::setw(9) << std::right << "natoms" << std::setw(15) << std::right << "energy error"
+      << std::setw(18) << std::right << "e" << std::setw(18) << std::right << "e0" << std::setw(15) << std::right
+      << "|e-e0|" << std::setw(15) << std::right << "e-e0" << std::setw(15) << std::right << "de/e0" << std::endl;
+    int idx = 0;
+    for (int c = 0; c < NC; ++c) {
+      const int na = db.cell_atom0[c + 1] - db.cell_atom0[c];
+      const double en = energy[c], e0 = db.cell_energy0[c];
+      f << std::setw(3) << std::right << c << std::fixed << std::setw(11) << std::right << std::setprecision(4)
+        << db.cell_weight[c] << std::setw(11) << std::right << std::setprecision(4) << db.cell_eweight[c]
+        << std::setw(9) << std::right << na << std::setw(15) << std::right << std::setprecision(6) << e[idx] * e[idx]
+        << std::setw(18) << std::right << std::setprecision(10) << en << std::setw(18) << std::right
+        << std::setprecision(10) << e0 << std::setw(15) << std::right << std::setprecision(6) << std::abs(en - e0)
+        << std::setw(15) << std::right << std::setprecision(6) << en - e0;
+      if (e0 == 0) f << std::setw(15) << std::right << "inf";
+      else f << std::setw(15) << std::right << std::setprecision(6) << (e0 - en) / e0;
+      f << std::endl;
+      idx += 7 + 3 * na;
+    }
+  }
+  {
+    std::ofstream f = open_out(data_name(prefix, ".stress", num));
+    f << "Global stress weight is " << std::fixed << stress_weight << std::endl;
+    f << std::setw(3) << std::right << "#" << std::setw(11) << std::right << "conf_w" << std::setw(11) << std::right
+      << "conf_sw" << std::setw(15) << std::right << "stress error" << std::setw(18) << std::right << "s"
+      << std::setw(18) << std::right << "s0" << std::setw(15) << std::right << "ds/s0" << std::endl;
+    int idx = 0;
+    for (int c = 0; c < NC; ++c) {
+      ++idx;
+      for (int d = 0; d < 6; ++d) {
+        const double s = stress[6 * c + d], s0 = db.cell_stress0[6 * c + d];
+        f << std::setw(3) << std::right << c << std::fixed << std::setw(11) << std::right << std::setprecision(4)
+          << db.cell_weight[c] << std::setw(11) << std::right << std::setprecision(4) << db.cell_sweight[c]
+          << std::setw(15) << std::right << std::setprecision(6) << e[idx] * e[idx] << std::setw(18) << std::right
+          << std::setprecision(10) << s << std::setw(18) << std::right << std::setprecision(10) << s0;
+        if (s0 == 0) f << std::setw(15) << std::right << "inf";
+        else f << std::setw(15) << std::right << std::setprecision(6) << (s0 - s) / s0;
+        f << std::endl;
+        ++idx;
+      }
+      idx += 3 * (db.cell_atom0[c + 1] - db.cell_atom0[c]);
+    }
+  }
+  {
+    std::ofstream f = open_out(data_name(prefix, ".force", num));
+    f << std::setw(6) << std::right << "conf:" << std::setw(5) << std::right << "atom" << std::setw(8) << std::right
+      << "type" << std::setw(15) << std::right << "force error" << std::setw(15) << std::right << "f"
+      << std::setw(15) << std::right << "f0" << std::setw(15) << std::right << "df/f0" << std::endl;
+    int idx = 0;
+    for (int c = 0; c < NC; ++c) {
+      idx += 7;
+      for (int i = 0; i < db.cell_atom0[c + 1] - db.cell_atom0[c]; ++i) {
+        const int a = db.cell_atom0[c] + i;
+        for (int d = 0; d < 3; ++d) {
+          const double fv = force[3 * a + d], f0 = db.atom_force0[3 * a + d];
+          f << std::setw(5) << std::right << c << ":" << std::setw(5) << std::right << i << std::setw(8) << std::right
+            << db.atom_type[a] << std::setw(15) << std::right << std::fixed << e[idx] * e[idx] << std::setw(15)
+            << std::right << std::fixed << fv << std::setw(15) << std::right << std::fixed << f0;
+          if (f0 == 0) f << std::setw(15) << std::right << "inf";
+          else f << std::setw(15) << std::right << std::fixed << (f0 - fv) / f0;
+          f << std::endl;
+          ++idx;
+        }
+      }
+    }
+  }
+  {
+    double se = 0.0, ss = 0.0, sf = 0.0, sp = 0.0;
+    int idx = 0;
+    for (int c = 0; c < NC; ++c) {
+      se += e[idx] * e[idx];
+      ++idx;
+      for (int d = 0; d < 6; ++d, ++idx) ss += e[idx] * e[idx];
+      for (int i = 0; i < 3 * (db.cell_atom0[c + 1] - db.cell_atom0[c]); ++i, ++idx) sf += e[idx] * e[idx];
+    }
+    for (int i = idx; i < esize; ++i) sp += e[i] * e[i];
+    const double total = se + ss + sf + sp;
+    const int npunish = esize - 3 * N - 6 * NC - NC;
+    std::ofstream f = open_out(data_name(prefix, ".error", num));
+    f << "Total error sum " << std::fixed << total << " count " << esize << " (" << 3 * N << " forces, " << 6 * NC
+      << " stresses, " << NC << " energies";
+    if (npunish == 0) f << ")" << std::endl;
+    else f << ", " << npunish << " punishments)" << std::endl;
+    f << "Sum of force errors  = " << std::fixed << sf << std::endl;
+    f << "Sum of energy errors = " << std::fixed << se << std::endl;
+    f << "Sum of stress errors = " << std::fixed << ss << std::endl;
+    if (npunish) f << "Sum of punish errors = " << std::fixed << sp << std::endl;
+  }
+  {
+    std::ofstream f = open_out(data_name(prefix, ".punish", num));
+    f << "Limiting constraints (atomic density lies inside F boundaries)" << std::endl;
+    f << std::setw(3) << std::right << "#" << std::setw(11) << std::right << "conf_w" << std::setw(15) << std::right
+      << "punish error" << std::setw(15) << std::right << "punishment" << std::endl;
+    int idx = 7 * NC + 3 * N;
+    for (int c = 0; c < NC; ++c, ++idx)
+      f << std::setw(3) << std::right << c << std::fixed << std::setw(11) << std::right << std::setprecision(4)
+        << db.cell_weight[c] << std::setw(15) << std::right << std::setprecision(6) << e[idx] * e[idx]
+        << std::setw(15) << std::right << std::setprecision(6) << e[idx] / db.cell_weight[c] << std::endl;
+    if (meam) {
+      double m = 0.0;
+      for (const Spline3 &sp : pot.groups[G_F]) {
+        const double v = sp.max_y_mag();
+        if (std::abs(m) < std::abs(v)) m = v;
+      }
+      f << std::endl << "Dummy constraints (|f_max(r)| = 1)" << std::endl;
+      f << std::setw(15) << std::right << "punish error" << std::setw(15) << std::right << "|f_max(r)|" << std::endl;
+      f << std::fixed << std::setw(15) << std::right << std::setprecision(6) << e[idx] * e[idx] << std::setw(15)
+        << std::right << std::setprecision(6) << std::abs(std::abs(m)) << std::endl;
+    } else {
+      f << std::endl << "Dummy constraints (F'(n_avg) = 0)" << std::endl;
+      f << std::setw(7) << std::right << "element" << std::setw(15) << std::right << "punish error" << std::setw(15)
+        << std::right << "F'(n_avg)" << std::endl;
+      for (int t = 0; t < pot.ntypes; ++t, ++idx)
+        f << std::setw(7) << std::right << t << std::fixed << std::setw(15) << std::right << std::setprecision(6)
+          << e[idx] * e[idx] << std::setw(15) << std::right << std::setprecision(6) << e[idx] / 100. << std::endl;
+    }
+  }
+}
+
 // --------------------------------------------------------------- neighbours
 
 namespace {
@@ -607,6 +957,13 @@ extern "C" {
 
 const char *mz_last_error(void) { return g_last_error.c_str(); }
 
+mz_status mz_pot_clone(const mz_pot *pot, mz_pot **out) {
+  return guarded([&] {
+    if (!pot || !out) fail(MZ_ERR_ARG, "null argument");
+    *out = new mz_pot(*pot);
+  });
+}
+
 mz_status mz_pot_parse(const char *text, mz_pot **out) {
   return guarded([&] {
     if (!text || !out) fail(MZ_ERR_ARG, "null argument");
@@ -698,6 +1055,28 @@ static void build_any(const mz_cells_desc &c, const mz_pot *pot, int device, mz_
     throw;
   }
   *out = d;
+}
+
+mz_status mz_pot_rescale(mz_pot *pot, const mz_db *db, const double *densities, int flag, int *rescaled,
+                         double *factors) {
+  return guarded([&] {
+    if (!pot || !db || !densities || !rescaled || !factors) fail(MZ_ERR_ARG, "null argument");
+    for (auto &g : pot->pot.groups)
+      for (auto &sp : g)
+        if (sp.nknots < 2) fail(MZ_ERR_ARG, "spline with fewer than two knots");
+    *rescaled = rescale_pot(pot->pot, db->db.atom_type.data(), db->db.natoms, densities, flag, factors);
+  });
+}
+
+mz_status mz_write_data(const mz_db *db, const mz_pot *pot, double energy_weight, double stress_weight,
+                        const double *errvec, const double *energy, const double *stress, const double *forces,
+                        const double *densities, const char *prefix, int num) {
+  return guarded([&] {
+    if (!db || !pot || !errvec || !energy || !stress || !forces || !densities || !prefix)
+      fail(MZ_ERR_ARG, "null argument");
+    write_data_files(db->db, pot->pot, energy_weight, stress_weight, errvec, energy, stress, forces, densities,
+                     prefix, num);
+  });
 }
 
 mz_status mz_db_build(const mz_cells_desc *cells, const mz_pot *pot, mz_db **out) {
@@ -814,6 +1193,8 @@ mz_status mz_pot_get_spline(const mz_pot *pot, int s, mz_spline_view *v) {
     v->grad[1] = sp.grad[1];
     v->y_fixed = sp.y_fixed.data();
     v->y = sp.y.data();
+    v->x = sp.x.data();
+    v->step = sp.step;
   });
 }
 

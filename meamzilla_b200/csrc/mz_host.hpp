@@ -38,6 +38,18 @@ struct Spline3 {
   void refresh(std::vector<double> &ypp) const;
   // Value + slope at x with linear extrapolation (spline3eq.h:204-236).
   double eval(const std::vector<double> &ypp, double xv, double *g) const;
+
+  // Operations of the reference's rescale (spline3eq.cpp:112-186, 301-350):
+  // new end knots with values re-interpolated, x scaled (reversed when the
+  // factor is negative), y scaled, a spline added (values / slopes of `rhs`
+  // evaluated with the second derivatives `rhs_ypp` it carries), a*x added.
+  void readjust_x(double left, double right);
+  void rescale_x(double scale);
+  void scale_y(double f);
+  void divide_y(double f);
+  void add(const Spline3 &rhs, const std::vector<double> &rhs_ypp);
+  void add_linear(double a);
+  double max_y_mag() const;  // Spline::get_max_y_mag (spline.cpp:58-67)
 };
 
 // Function groups in file order.  MEAM: phi(Pair_ij) rho(Pair_j) U(Atom/Pair_i)
@@ -93,6 +105,17 @@ struct Db {
   std::vector<int64_t> in_off;                // [N+1]
   std::vector<int64_t> in_slot;               // [Np]
 };
+
+// Potential::rescale for the spline styles (PotMEAM::rescale
+// pot_meam.cpp:281-375 with rescale_3body :497-525; PotEAM::rescale
+// pot_eam.cpp:257-389) from per-atom densities of the current potential.
+// Returns 1 when the potential changed; factors = {embedding a, MEAM f b}.
+int rescale_pot(Pot &pot, const int *atom_type, int natoms, const double *densities, int flag, double factors[2]);
+
+// Potential::write_data's text files (potential.cpp:325-342 and the writers it calls).
+void write_data_files(const Db &db, const Pot &pot, double energy_weight, double stress_weight, const double *errvec,
+                      const double *energy, const double *stress, const double *forces, const double *densities,
+                      const std::string &prefix, int num);
 
 // Build lists (throws std::runtime_error with an mz status prefix).
 void build_db(const mz_cells_desc &cells, const Pot &pot, Db &db);

@@ -119,6 +119,26 @@ class PotentialFile:
             raise ValueError("expected %d coefficients" % self.ncoeff)
         check(lib().mz_pot_set_coeffs(self._h, ptr(x)))
 
+    def copy(self) -> "PotentialFile":
+        """An independent copy (Potential::clone, potential.h:43)."""
+        h = C.c_void_p()
+        check(lib().mz_pot_clone(self._h, C.byref(h)))
+        return PotentialFile(h)
+
+    def rescale(self, db: "Database", densities, flag: int = 1):
+        """Potential::rescale in place (PotMEAM::rescale pot_meam.cpp:281-375,
+        PotEAM::rescale pot_eam.cpp:257-389) from the per-atom densities of
+        the current coefficients.  Returns (rescaled, a, b): the reference's
+        return value, the embedding scale factor and the MEAM f scale (0 when
+        not applied).  Evaluators built before must be re-created."""
+        d = np.ascontiguousarray(densities, dtype=np.float64)
+        if d.size != db.stats()["natoms"]:
+            raise ValueError("one density per atom expected")
+        r = C.c_int()
+        f = np.zeros(2)
+        check(lib().mz_pot_rescale(self._h, db.handle, ptr(d), int(flag), C.byref(r), ptr(f)))
+        return bool(r.value), float(f[0]), float(f[1])
+
     def write(self, path: str) -> None:
         check(lib().mz_pot_write(self._h, path.encode()))
 
@@ -129,7 +149,8 @@ class PotentialFile:
         return dict(group=v.group, alloy=v.alloy, nknots=n, left=v.left, right=v.right,
                     nat=(v.nat[0], v.nat[1]), grad_fixed=(v.grad_fixed[0], v.grad_fixed[1]),
                     grad=np.array([v.grad[0], v.grad[1]]),
-                    y_fixed=_lib.as_array(v.y_fixed, n, np.int32), y=_lib.as_array(v.y, n, np.float64))
+                    y_fixed=_lib.as_array(v.y_fixed, n, np.int32), y=_lib.as_array(v.y, n, np.float64),
+                    x=_lib.as_array(v.x, n, np.float64), step=v.step)
 
     def spline_eval(self, s: int, x: float):
         val, grad = C.c_double(), C.c_double()
@@ -245,6 +266,7 @@ class Evaluator:
         self.db = db
         self.pot = pot
         self.energy_weight, self.stress_weight, self.embed_extrap = float(energy_weight), float(stress_weight), int(embed_extrap)
+        self.device, self.max_candidates, self.omit_punishments = int(device), int(max_candidates), bool(omit_punishments)
         st = db.stats()
         self.natoms, self.ncells = st["natoms"], st["ncells"]
         self.ncoeff = pot.ncoeff
@@ -437,6 +459,27 @@ class Potential:
     def compute_densities(self) -> np.ndarray:
         return self.ev.densities(self.x)
 
+    # --- Potential::rescale (potential.h:68)
+    def rescale(self, flag: int = 1, out=None) -> int:
+        """Rescale this potential (PotMEAM::rescale / PotEAM::rescale) from its
+        GPU densities.  The reference rescales only the potential it is
+        called on, so a copy of the potential file is rescaled and this
+        object gets its own evaluator when anything changed."""
+        ev = self.ev
+        dens = ev.densities(self.x)
+        pot = ev.pot.copy()
+        pot.set_coeffs(self.x)
+        changed, a, b = pot.rescale(ev.db, dens, flag)
+        if changed:
+            if out is not None:
+                if b:
+                    out.write("MEAM potential scaling factor %f\n" % b)
+                out.write("Embedding function scaling factor %f\n" % a)
+            self.ev = Evaluator(ev.db, pot, ev.energy_weight, ev.stress_weight, ev.embed_extrap, device=ev.device,
+                                max_candidates=ev.max_candidates, omit_punishments=ev.omit_punishments)
+            self.x = pot.coeffs()
+        return int(changed)
+
     # --- output
     def write_pot(self, path: str, num: int = -1) -> None:
         pot = self.ev.pot
@@ -446,6 +489,17 @@ class Potential:
             pot.write(path if num < 0 else "%s.%d" % (path, num))
         finally:
             pot.set_coeffs(keep)
+
+    def write_data(self, prefix: str, num: int = -1) -> None:
+        """Potential::write_data (potential.cpp:325-342): .rho .energy .stress
+        .force .error .punish files from one FP64 evaluation on the GPU."""
+        ev = self.ev
+        out = ev.objective(self.x[None, :], MZ_FP64, errvec=True, forces=True, energy=True, stress=True)
+        dens = np.ascontiguousarray(ev.densities(self.x), dtype=np.float64)
+        pot = ev.pot.copy()
+        pot.set_coeffs(self.x)
+        write_data_arrays(ev.db, pot, ev.energy_weight, ev.stress_weight, out["errvec"][0], out["energy"][0],
+                          out["stress"][0], out["forces"][0], dens, prefix, num)
 
     def error_breakdown(self) -> dict:
         """Force / energy / stress / punish sums as the .error file reports them
@@ -487,3 +541,11 @@ def from_param_file(path: str, device: int = 0, max_candidates: int = 1, precisi
     ee = int(p.get("embed_extrap", ["0"])[0])
     ev = Evaluator(db, pot, ew, sw, ee, device=device, max_candidates=max_candidates)
     return Potential(ev, precision=precision)
+
+
+def write_data_arrays(db: Database, pot: PotentialFile, energy_weight: float, stress_weight: float, errvec, energy,
+                      stress, forces, densities, prefix: str, num: int = -1) -> None:
+    """The reference's data files from evaluated arrays (mz_write_data)."""
+    arrs = [np.ascontiguousarray(a, dtype=np.float64).ravel() for a in (errvec, energy, stress, forces, densities)]
+    check(lib().mz_write_data(db.handle, pot.handle, float(energy_weight), float(stress_weight),
+                              *[ptr(a) for a in arrs], prefix.encode(), int(num)))

@@ -142,7 +142,7 @@ class CRestatement:
 
 
 def run_reference(param_path: str, coeffs=None, fd_h: float = 0.0, reps: int = 0, fast: bool = False,
-                  timeout: float = 600.0, cwd=None) -> dict:
+                  timeout: float = 600.0, cwd=None, rescale=None, write_prefix=None) -> dict:
     """Run the compiled reference on a parameter file; returns its outputs."""
     exe = MZREF_FAST if fast else MZREF
     if not os.path.exists(exe):
@@ -158,11 +158,15 @@ def run_reference(param_path: str, coeffs=None, fd_h: float = 0.0, reps: int = 0
             cmd += ["-fd", repr(float(fd_h))]
         if reps > 0:
             cmd += ["-reps", str(reps)]
+        if rescale is not None:
+            cmd += ["-rescale", str(int(rescale))]
+        if write_prefix is not None:
+            cmd += ["-write", os.path.abspath(write_prefix)]
         res = subprocess.run(cmd, capture_output=True, text=True, timeout=timeout, cwd=cwd)
         if res.returncode != 0:
             raise RuntimeError("mzref failed (%d): %s %s" % (res.returncode, res.stdout[-2000:], res.stderr[-2000:]))
         out = {}
-        for k in ("obj", "errvec", "energy", "stress", "force", "dens", "coeff", "fdgrad"):
+        for k in ("obj", "errvec", "energy", "stress", "force", "dens", "coeff", "fdgrad", "rescale"):
             f = "%s.%s.bin" % (prefix, k)
             if os.path.exists(f):
                 out[k] = np.fromfile(f, dtype=np.float64)

@@ -19,6 +19,12 @@
 //            warm-up; prints "seconds_per_eval <t>"
 //     -fd    central finite-difference gradient of the objective with step h
 //            for every coefficient -> <prefix>.fdgrad.bin
+//     -write P  Potential::write_data(comm, P, -1) (src/potential.cpp:325-342):
+//            P.rho/.energy/.stress/.force/.error/.punish, after -x / -rescale
+//     -rescale F  call Potential::rescale(comm, out, F) (src/potential.h:68)
+//            after -x, then dump every spline -> <prefix>.rescale.bin:
+//            [returned value, nsplines, per spline: n, x[n], y[n], grad[2],
+//            natural[2], step] (function groups in file order)
 #define protected public
 #include "meamzilla.h"
 #include "universe.h"
@@ -28,6 +34,8 @@
 #include "pot_list.h"
 #include "potential.h"
 #include "pots/pot_eam/pot_eam.h"
+#include "pot_fns.h"
+#include "spline3eq.h"
 #undef protected
 
 #include <chrono>
@@ -50,8 +58,9 @@ static void dump(const std::string &path, const std::vector<double> &v) {
 }
 
 int main(int argc, char **argv) {
-  std::string param, xfile, prefix;
-  int reps = 0, quiet = 0;
+  std::string param, xfile, prefix, write_prefix;
+  int reps = 0, quiet = 0, rescale_flag = 0;
+  bool do_rescale = false;
   double fd_h = 0.0;
   for (int i = 1; i < argc; ++i) {
     std::string a = argv[i];
@@ -60,6 +69,8 @@ int main(int argc, char **argv) {
     else if (a == "-o" && i + 1 < argc) prefix = argv[++i];
     else if (a == "-reps" && i + 1 < argc) reps = std::atoi(argv[++i]);
     else if (a == "-fd" && i + 1 < argc) fd_h = std::atof(argv[++i]);
+    else if (a == "-write" && i + 1 < argc) write_prefix = argv[++i];
+    else if (a == "-rescale" && i + 1 < argc) rescale_flag = std::atoi(argv[++i]), do_rescale = true;
     else if (a == "-q") quiet = 1;
     else { std::fprintf(stderr, "mzref: bad argument %s\n", a.c_str()); return 2; }
   }
@@ -98,6 +109,30 @@ int main(int argc, char **argv) {
     std::fclose(f);
     for (int i = 0; i < ncoeff; ++i) pot->coeff(i) = x[i];
   }
+
+  if (do_rescale) {
+    const int ret = pot->rescale(comm, &std::cerr, rescale_flag);
+    std::vector<double> out{(double)ret, 0.0};
+    int nspl = 0;
+    for (PotFns &pf : pot->pot_fns_)
+      for (Basis *b : pf.fns) {
+        Spline3Eq *sp = dynamic_cast<Spline3Eq *>(b);
+        if (!sp) { std::fprintf(stderr, "mzref: rescale dump supports spline3eq only\n"); return 2; }
+        out.push_back((double)sp->nknots_);
+        out.insert(out.end(), sp->x_.begin(), sp->x_.end());
+        out.insert(out.end(), sp->y_.begin(), sp->y_.end());
+        out.push_back(sp->grad_[0]);
+        out.push_back(sp->grad_[1]);
+        out.push_back((double)sp->is_nat_[0]);
+        out.push_back((double)sp->is_nat_[1]);
+        out.push_back(sp->step_);
+        ++nspl;
+      }
+    out[1] = (double)nspl;
+    if (!prefix.empty()) dump(prefix + ".rescale.bin", out);
+  }
+
+  if (!write_prefix.empty()) pot->write_data(comm, write_prefix, -1);
 
   ErrorVec evec;
   double obj = pot->compute(comm, &evec);

@@ -76,6 +76,33 @@ def in_range_meam(pot):
     return p
 
 
+def data_goldens():
+    """ref.{rho,energy,stress,force,error,punish}: the text files the
+    reference's Potential::write_data writes for the start potential."""
+    for name in sorted(os.listdir(HERE)):
+        d = os.path.join(HERE, name)
+        if os.path.isfile(os.path.join(d, "param")):
+            oracle.run_reference("param", cwd=d, write_prefix=os.path.join(d, "ref"))
+            print(name, "data files written")
+
+
+def rescale_goldens():
+    """rescale.npz of every case: the reference's Potential::rescale with
+    flag 0 (when needed) and 1 (always), run on the start potential, dumped
+    spline by spline by the harness (oracle/ref_harness.cpp -rescale)."""
+    for name in sorted(os.listdir(HERE)):
+        d = os.path.join(HERE, name)
+        if not os.path.isfile(os.path.join(d, "param")):
+            continue
+        out = {}
+        for flag in (0, 1):
+            r = oracle.run_reference("param", cwd=d, rescale=flag)
+            out["flag%d" % flag] = r["rescale"]
+            out["obj%d" % flag] = r["obj"]  # Potential::compute after the rescale
+        np.savez_compressed(os.path.join(d, "rescale.npz"), **out)
+        print(name, "rescale returns", out["flag0"][0], out["flag1"][0])
+
+
 def main():
     # 1. EAM, 3 bcc cells (the eam54 rules)
     pot, cells = synth.make_workload("eam54", seed=3, ncells=3)
@@ -125,4 +152,9 @@ def main():
 
 
 if __name__ == "__main__":
-    main()
+    import sys
+    if "--rescale-only" not in sys.argv and "--data-only" not in sys.argv:
+        main()
+    if "--data-only" not in sys.argv:
+        rescale_goldens()
+    data_goldens()

@@ -3,6 +3,8 @@
 Tolerances: FP64 objective 1e-12 relative and forces 1e-10 eV/A (the plain
 path's bar); mixed precision objective 1e-6 relative and forces 1e-5 eV/A
 against FP64."""
+import os
+
 import numpy as np
 import pytest
 
@@ -152,3 +154,46 @@ def test_tensor_core_forward_opt_in(name, monkeypatch):
     for c in range(2):
         assert rel(b["obj"][c], a["obj"][c]) <= 3e-6
         assert np.max(np.abs(b["forces"][c] - a["forces"][c])) <= 5e-5
+
+
+@pytest.mark.parametrize("name", ["meam_mix6", "eam_bcc3"])
+def test_rescale_then_objective_matches_reference(name):
+    """Potential.rescale on the GPU densities, then the objective of the
+    rescaled potential, against the reference's rescale + compute."""
+    from meamzilla_b200.potential import MZ_FP64, Evaluator, Potential
+    case = load_case(name)
+    ev = Evaluator(case["db"], case["pot"], max_candidates=1, **case["weights"])
+    p = Potential(ev, precision=MZ_FP64)
+    ref = np.load(os.path.join(case["dir"], "rescale.npz"))
+    assert p.rescale(1) == int(ref["flag1"][0])
+    assert p.ev is not ev and ev.pot.coeffs().size == case["pot"].ncoeff
+    assert rel(p.compute(), float(ref["obj1"])) <= 1e-12
+
+
+def _same_layout(ours: str, ref: str):
+    """Same lines with every digit masked (the reference's fixed-width columns
+    run together for large values, so numbers are not tokenised)."""
+    import re
+    la, lb = ours.splitlines(), ref.splitlines()
+    assert len(la) == len(lb)
+    for x, y in zip(la, lb):
+        assert re.sub(r"[0-9]", "0", x) == re.sub(r"[0-9]", "0", y), (x, y)
+
+
+@pytest.mark.parametrize("name", ["meam_mix6", "eam_bcc3", "meam2_edge"])
+def test_write_data_from_gpu_matches_reference_files(name, tmp_path):
+    """Potential.write_data evaluates on the GPU (FP64) and writes the
+    reference's data files: the same layout as the reference's files, and the
+    error sums to 1e-10 (the byte-exact formatting is pinned on CPU by
+    tests/test_data_files.py)."""
+    from meamzilla_b200.potential import MZ_FP64, Evaluator, Potential
+    case = load_case(name)
+    ev = Evaluator(case["db"], case["pot"], max_candidates=1, **case["weights"])
+    prefix = str(tmp_path / "out")
+    Potential(ev, precision=MZ_FP64).write_data(prefix)
+    for ext in ("rho", "energy", "stress", "force", "error", "punish"):
+        with open(prefix + "." + ext) as a, open(os.path.join(case["dir"], "ref." + ext)) as b:
+            _same_layout(a.read(), b.read())
+    with open(prefix + ".error") as a, open(os.path.join(case["dir"], "ref.error")) as b:
+        for x, y in zip(a.read().splitlines()[1:], b.read().splitlines()[1:]):  # the four sums
+            assert rel(float(x.split("=")[1]), float(y.split("=")[1])) <= 1e-10
