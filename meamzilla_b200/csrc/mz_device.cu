@@ -33,6 +33,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <map>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -71,6 +72,14 @@ struct mz_ctx {
   TcParams tc{};                                // tensor-core forward plan
   bool tc_ok = false;
   int nsm = 1;
+  // Kernel sequences of the host-buffer entry points captured as CUDA graphs,
+  // one per (candidates, precision, outputs); replayed on later calls.
+  bool use_graphs = true;
+  struct Graph {
+    cudaGraphExec_t exec;
+    int64_t kernels;
+  };
+  std::map<uint64_t, Graph> graphs;
   size_t smem_atoms[2] = {0, 0};  // [FP64, MIXED]
   size_t smem_adj[2] = {0, 0};
   bool profiling = false;
@@ -133,6 +142,8 @@ void release(mz_ctx *ctx) {
     cudaEventDestroy(m.stop);
   }
   ctx->marks.clear();
+  for (auto &g : ctx->graphs) cudaGraphExecDestroy(g.second.exec);
+  ctx->graphs.clear();
   for (void *p : ctx->allocs) cudaFree(p);
   ctx->allocs.clear();
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
@@ -296,6 +307,50 @@ void refresh_matrix(const Spline3 &sp, std::vector<double> &M) {
   }
 }
 
+// The kernels of one objective call on the context's own buffers: captured
+// into a CUDA graph the first time a shape is seen, replayed afterwards (not
+// while profiling, whose per-kernel events are recorded around launches).
+constexpr size_t MAX_GRAPHS = 32;
+void launch_objective(mz_ctx *ctx, int n, int precision, bool ev, bool fo, bool en, bool st, bool gr) {
+  auto go = [&] {
+    enqueue(ctx, n, ctx->d_params, precision, ctx->d_obj, ev ? ctx->d_errvec : nullptr, fo ? ctx->d_forces : nullptr,
+            en ? ctx->d_energy : nullptr, st ? ctx->d_stress : nullptr, gr ? ctx->d_grad : nullptr);
+  };
+  if (!ctx->use_graphs || ctx->profiling) {
+    go();
+    return;
+  }
+  const uint64_t key = ((uint64_t)n << 8) | ((uint64_t)precision << 5) | ((uint64_t)ev << 4) | ((uint64_t)fo << 3) |
+                       ((uint64_t)en << 2) | ((uint64_t)st << 1) | (uint64_t)gr;
+  auto it = ctx->graphs.find(key);
+  if (it == ctx->graphs.end()) {
+    if (ctx->graphs.size() >= MAX_GRAPHS) {
+      go();
+      return;
+    }
+    const int64_t l0 = ctx->launches;
+    cudaGraph_t g = nullptr;
+    ck(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal), "graph capture");
+    try {
+      go();
+    } catch (...) {
+      cudaStreamEndCapture(ctx->stream, &g);
+      if (g) cudaGraphDestroy(g);
+      throw;
+    }
+    ck(cudaStreamEndCapture(ctx->stream, &g), "graph capture end");
+    cudaGraphExec_t ex = nullptr;
+    const cudaError_t ie = cudaGraphInstantiate(&ex, g, 0);
+    cudaGraphDestroy(g);
+    ck(ie, "graph instantiate");
+    const int64_t nk = ctx->launches - l0;
+    ctx->launches = l0;
+    it = ctx->graphs.emplace(key, mz_ctx::Graph{ex, nk}).first;
+  }
+  ck(cudaGraphLaunch(it->second.exec, ctx->stream), "graph launch");
+  ctx->launches += it->second.kernels;
+}
+
 void run_host(mz_ctx *ctx, int ncand, const double *params, int precision, double *obj, double *errvec,
               double *forces, double *energy, double *stress, double *grad) {
   if (!ctx || !params || !obj || ncand <= 0) throw Failure{MZ_ERR_ARG, "bad argument"};
@@ -307,9 +362,8 @@ void run_host(mz_ctx *ctx, int ncand, const double *params, int precision, doubl
     ck(cudaMemcpyAsync(ctx->d_params, params + (size_t)c0 * P, sizeof(double) * n * P, cudaMemcpyHostToDevice,
                        ctx->stream),
        "params H2D");
-    enqueue(ctx, n, ctx->d_params, precision, ctx->d_obj, errvec ? ctx->d_errvec : nullptr,
-            forces ? ctx->d_forces : nullptr, energy ? ctx->d_energy : nullptr, stress ? ctx->d_stress : nullptr,
-            grad ? ctx->d_grad : nullptr);
+    launch_objective(ctx, n, precision, errvec != nullptr, forces != nullptr, energy != nullptr, stress != nullptr,
+                     grad != nullptr);
     ck(cudaMemcpyAsync(obj + c0, ctx->d_obj, sizeof(double) * n, cudaMemcpyDeviceToHost, ctx->stream), "obj D2H");
     if (grad)
       ck(cudaMemcpyAsync(grad + (size_t)c0 * P, ctx->d_grad, sizeof(double) * n * P, cudaMemcpyDeviceToHost,
@@ -545,6 +599,10 @@ mz_status mz_create(const mz_db *dbh, const mz_pot *poth, const mz_settings *set
        "occupancy");
     ctx->adj_ctas = std::max(1, std::min(d.nblocks, nsm * std::max(1, per_sm)));
     ctx->nsm = nsm;
+    {
+      const char *env = std::getenv("MZ_GRAPH");
+      ctx->use_graphs = !(env && env[0] == '0');
+    }
     // tensor-core forward (mixed precision, MEAM with TC_NB B-spline coefficients per g spline)
     {
       const char *env = std::getenv("MZ_TC");  // opt-in: "1"

@@ -197,3 +197,27 @@ def test_write_data_from_gpu_matches_reference_files(name, tmp_path):
     with open(prefix + ".error") as a, open(os.path.join(case["dir"], "ref.error")) as b:
         for x, y in zip(a.read().splitlines()[1:], b.read().splitlines()[1:]):  # the four sums
             assert rel(float(x.split("=")[1]), float(y.split("=")[1])) <= 1e-10
+
+
+def test_graph_replay_is_bitwise_identical(monkeypatch):
+    """The host-buffer entry points capture their kernel sequence once per
+    call shape and replay it; results and launch counts equal those of
+    direct launches (MZ_GRAPH=0), call after call."""
+    from meamzilla_b200.potential import MZ_FP64, MZ_MIXED, Evaluator
+    case = load_case("meam_mix6")
+    g = case["gold"]
+    X = np.stack([g["coeff"], g["coeff2"]])
+    monkeypatch.setenv("MZ_GRAPH", "0")
+    direct = Evaluator(case["db"], case["pot"], max_candidates=2, **case["weights"])
+    monkeypatch.delenv("MZ_GRAPH")
+    graph = Evaluator(case["db"], case["pot"], max_candidates=2, **case["weights"])
+    for rep in range(3):
+        for prec in (MZ_FP64, MZ_MIXED):
+            a = direct.objective(X, prec, errvec=True, forces=True)
+            b = graph.objective(X, prec, errvec=True, forces=True)
+            for k in ("obj", "errvec", "forces"):
+                assert np.array_equal(a[k], b[k]), (rep, prec, k)
+            oa, ga = direct.objective_grad(X, prec)
+            ob, gb = graph.objective_grad(X, prec)
+            assert np.array_equal(oa, ob) and np.array_equal(ga, gb)
+    assert direct.launches() == graph.launches()
