@@ -34,32 +34,29 @@ __device__ __forceinline__ void power_to_table(const SplineGeom &g, int m, doubl
 }
 
 constexpr int GACC_FLUSH_BLOCKS = 16;  // atom blocks between flushes of the per-thread g tables
+// The adjoint walks type-pure atom blocks (DevDb::adj_*), so each thread keeps
+// one g table (its block's type), flushed when the CTA moves to a block of
+// another type and every GACC_FLUSH_BLOCKS blocks.
 
 // Shared-memory layout of k_adj (dynamic), see adj_smem_bytes():
 //   double wtab[ADJ_WARPS][stride]          per-warp table gradients (FP64)
 //   float  ftab[ADJ_WARPS][stride]          per-warp pair-function gradients of one block (FP32)
-//   R4 gacc[gslots][MAX_G_KNOTS-1][BLOCK_SLOTS]  per-thread g-table gradients, power basis;
-//                                           gslots = ntypes (kept across blocks) or 1 (flushed each block)
+//   R4 gacc[ng-1][BLOCK_SLOTS]              per-thread g-table gradients of one type, power basis
 //   double red[BLOCK_SLOTS], a_chi[BLOCK_ATOMS], a_dF[BLOCK_ATOMS]
-//   SplineGeom sg[nsplines]; int a_lo[BLOCK_ATOMS+2]
+//   SplineGeom sg[nsplines]; int a_lo[BLOCK_ATOMS+2], a_idx[BLOCK_ATOMS], a_len[BLOCK_ATOMS]
 //   R ptab[pstride]
 //   R4 srow[BLOCK_SLOTS+8]  (u_x, u_y, u_z, f)              of every slot (zero padded)
 //   R4 sadj[BLOCK_SLOTS+8]  (a f', a f / r, Q_x, Q_y)        with Q = f Lambda / r
 //   R  sqz[BLOCK_SLOTS+8]   Q_z
 template <typename R>
-__host__ __device__ inline int adj_gslots(int ntypes, int ng) {
-  // keep one table per atom type while they fit in 64 KiB, else one, flushed every block
-  return ((size_t)ntypes * (ng - 1) * BLOCK_SLOTS * 4 * sizeof(R) <= 65536) ? ntypes : 1;
-}
-template <typename R>
 __host__ __device__ inline size_t adj_smem_bytes(int nsplines, int stride, int pstride, bool meam, int ntypes,
                                                  int ng) {
   size_t b = sizeof(double) * (size_t)ADJ_WARPS * stride + sizeof(float) * (size_t)ADJ_WARPS * stride;
   b = (b + 31) & ~size_t(31);
-  if (meam) b += 4 * sizeof(R) * (size_t)adj_gslots<R>(ntypes, ng) * (ng - 1) * BLOCK_SLOTS;
+  if (meam) b += 4 * sizeof(R) * (size_t)(ng - 1) * BLOCK_SLOTS;
   b += sizeof(double) * (BLOCK_SLOTS + 2 * BLOCK_ATOMS);
   b += sizeof(SplineGeom) * nsplines;
-  b += sizeof(int) * (BLOCK_ATOMS + 2);
+  b += sizeof(int) * (3 * BLOCK_ATOMS + 2);
   b = (b + 31) & ~size_t(31);
   b += sizeof(R) * (pstride + 4);
   b = (b + 31) & ~size_t(31);
@@ -68,7 +65,7 @@ __host__ __device__ inline size_t adj_smem_bytes(int nsplines, int stride, int p
 }
 
 template <bool MEAM, typename R>
-__global__ void __launch_bounds__(BLOCK_SLOTS, 2)
+__global__ void __launch_bounds__(BLOCK_SLOTS, sizeof(R) == 4 ? 3 : 2)
     k_adj(DevDb db, DevPot pot, const SplineGeom *__restrict__ geom, const double *__restrict__ tabs,
           const double *__restrict__ ptabs, const double *__restrict__ aout, const double *__restrict__ aux,
           const double *__restrict__ lam, const double *__restrict__ seeds, double *__restrict__ partial) {
@@ -81,20 +78,21 @@ __global__ void __launch_bounds__(BLOCK_SLOTS, 2)
   const int stride = pot.tab_stride;
   const int ng = MEAM ? pot.g_nmax : 2;  // per-thread tables sized by the largest g spline
   const int nint = ng - 1;
-  const int gslots = MEAM ? adj_gslots<R>(pot.ntypes, ng) : 1;
 
   double *wtab = reinterpret_cast<double *>(smem_raw);
   float *ftab = reinterpret_cast<float *>(wtab + (size_t)ADJ_WARPS * stride);
   size_t off = sizeof(double) * (size_t)ADJ_WARPS * stride + sizeof(float) * (size_t)ADJ_WARPS * stride;
   off = (off + 31) & ~size_t(31);
   R4 *gacc = reinterpret_cast<R4 *>(smem_raw + off);
-  if (MEAM) off += 4 * sizeof(R) * (size_t)gslots * nint * BLOCK_SLOTS;
+  if (MEAM) off += 4 * sizeof(R) * (size_t)nint * BLOCK_SLOTS;
   double *red = reinterpret_cast<double *>(smem_raw + off);
   double *a_chi = red + BLOCK_SLOTS;
   double *a_dF = a_chi + BLOCK_ATOMS;
   SplineGeom *sg = reinterpret_cast<SplineGeom *>(a_dF + BLOCK_ATOMS);
   int *a_lo = reinterpret_cast<int *>(sg + pot.nsplines);
-  off = reinterpret_cast<unsigned char *>(a_lo + BLOCK_ATOMS + 2) - smem_raw;
+  int *a_idx = a_lo + BLOCK_ATOMS + 2;
+  int *a_len = a_idx + BLOCK_ATOMS;
+  off = reinterpret_cast<unsigned char *>(a_len + BLOCK_ATOMS) - smem_raw;
   off = (off + 31) & ~size_t(31);
   R *ptab = reinterpret_cast<R *>(smem_raw + off);
   off += sizeof(R) * (pot.pow_stride + 4);
@@ -111,7 +109,7 @@ __global__ void __launch_bounds__(BLOCK_SLOTS, 2)
     ftab[i] = 0.f;
   }
   if (MEAM)
-    for (int i = tid; i < gslots * nint * BLOCK_SLOTS; i += blockDim.x) gacc[i] = R4{};
+    for (int i = tid; i < nint * BLOCK_SLOTS; i += blockDim.x) gacc[i] = R4{};
   for (int i = tid; i < pot.nsplines; i += blockDim.x) sg[i] = geom[i];
   double *wt = wtab + (size_t)warp * stride;
   float *ft = ftab + (size_t)warp * stride;
@@ -122,41 +120,56 @@ __global__ void __launch_bounds__(BLOCK_SLOTS, 2)
   const double *L = lam + (size_t)cand * 3 * N;
   const double *sd = seeds + (size_t)cand * CS_COUNT * NC;
 
-  // Flush of the per-thread g tables (power basis) into the warp's FP64
-  // table: one warp-wide sum per (type, interval, coefficient).
-  auto flush_gacc = [&](bool have_t, int t_mine) {
-    for (int t = 0; t < pot.ntypes; ++t) {
-      const int slot = gslots == 1 ? 0 : t;
-      const SplineGeom &gg = sg[pot.s_g + t];
-      for (int m = 0; m < gg.n - 1; ++m) {
-        R4 v = R4{};
-        if (gslots > 1 || (have_t && t_mine == t)) v = gacc[(slot * nint + m) * BLOCK_SLOTS + tid];
-        double d[4] = {(double)v.x, (double)v.y, (double)v.z, (double)v.w};
+  // Flush of the per-thread g table of type t (power basis) into the warp's
+  // FP64 table: one warp-wide sum per (interval, coefficient).
+  auto flush_gacc = [&](int t) {
+    const SplineGeom &gg = sg[pot.s_g + t];
+    for (int m = 0; m < gg.n - 1; ++m) {
+      const R4 v = gacc[m * BLOCK_SLOTS + tid];
+      double d[4] = {(double)v.x, (double)v.y, (double)v.z, (double)v.w};
 #pragma unroll
-        for (int q = 0; q < 4; ++q)
-          for (int o = 16; o > 0; o >>= 1) d[q] += __shfl_down_sync(0xffffffffu, d[q], o);
-        if (lane == 0) power_to_table(gg, m, d[0], d[1], d[2], d[3], [&](int idx, double x) { wt[gg.toff + idx] += x; });
-      }
-      if (gslots > 1) {
-        for (int m = 0; m < nint; ++m) gacc[(slot * nint + m) * BLOCK_SLOTS + tid] = R4{};
-      }
+      for (int q = 0; q < 4; ++q)
+        for (int o = 16; o > 0; o >>= 1) d[q] += __shfl_down_sync(0xffffffffu, d[q], o);
+      if (lane == 0) power_to_table(gg, m, d[0], d[1], d[2], d[3], [&](int idx, double x) { wt[gg.toff + idx] += x; });
     }
-    if (gslots == 1)
-      for (int m = 0; m < nint; ++m) gacc[m * BLOCK_SLOTS + tid] = R4{};
+    for (int m = 0; m < nint; ++m) gacc[m * BLOCK_SLOTS + tid] = R4{};
   };
 
-  int since_flush = 0;
-  for (int blk = blockIdx.x; blk < db.nblocks; blk += gridDim.x) {
-    const BlockRows br = block_rows(db, blk);
+  int since_flush = 0, tab_t = -1;
+  for (int blk = blockIdx.x; blk < db.adj_nblocks; blk += gridDim.x) {
+    const int b0 = db.adj_blk0[blk], na = db.adj_blk0[blk + 1] - b0;
     __syncthreads();  // previous block done with the shared arrays
-    for (int a = tid; a <= br.na; a += blockDim.x) a_lo[a] = db.pair_off[br.atom_lo + a] - br.slot_lo;
+    if (tid < na) {
+      const int at = db.adj_atoms[b0 + tid];
+      a_idx[tid] = at;
+      a_len[tid] = db.pair_off[at + 1] - db.pair_off[at];
+    }
     __syncthreads();
+    if (warp == 0) {  // row starts in the block's slot numbering (na <= 64: two atoms per lane)
+      const int v0 = 2 * lane < na ? a_len[2 * lane] : 0, v1 = 2 * lane + 1 < na ? a_len[2 * lane + 1] : 0;
+      int inc = v0 + v1;
+      for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, inc, o);
+        if (lane >= o) inc += y;
+      }
+      const int exc = inc - v0 - v1;
+      if (2 * lane <= na) a_lo[2 * lane] = exc;
+      if (2 * lane + 1 <= na) a_lo[2 * lane + 1] = exc + v0;
+      if (lane == 31) a_lo[na] = inc;
+    }
+    __syncthreads();
+    const int nslot = a_lo[na];
+    const int ti = db.atom_type[a_idx[0]];  // every atom of the block
+    if (MEAM && tab_t >= 0 && ti != tab_t) {
+      flush_gacc(tab_t);
+      since_flush = 0;
+    }
+    tab_t = ti;
 
-    const bool have = tid < br.nslot;
-    const int me = have ? slot_owner(a_lo, br.na, tid) : 0;
-    const int ia = br.atom_lo + me;
-    const int ti = db.atom_type[ia];
-    const int64_t gs = (int64_t)br.slot_lo + tid;
+    const bool have = tid < nslot;
+    const int me = have ? slot_owner(a_lo, na, tid) : 0;
+    const int ia = a_idx[me];
+    const int64_t gs = (int64_t)db.pair_off[ia] + (tid - a_lo[me]);
     const int cell = db.atom_cell[ia];
 
     PairEval<MEAM, R> pe;
@@ -206,11 +219,11 @@ __global__ void __launch_bounds__(BLOCK_SLOTS, 2)
     __syncthreads();
 
     // ---- per atom (one warp each): K_i, rho, U', U'', chi = dL/drho; U table gradient
-    for (int a = warp; a < br.na; a += nwarp) {
+    for (int a = warp; a < na; a += nwarp) {
       double K;
       warp_slot_sums<1>(red, a_lo[a], a_lo[a + 1], lane, &K);
       if (lane == 0) {
-        const int i = br.atom_lo + a;
+        const int i = a_idx[a];
         const double rho = ao[AO_RHO * N + i];
         const int c = db.atom_cell[i];
         const SplineGeom &gU = sg[pot.s_U + db.atom_type[i]];
@@ -246,7 +259,7 @@ __global__ void __launch_bounds__(BLOCK_SLOTS, 2)
         const R gam = (R)(0.5 * chi * fp + dF * a_p * (double)pe.df);
         const R del = (R)(dF * fp * ip);
         const R lx = (R)Lx, ly = (R)Ly, lz = (R)Lz, ap = (R)a_p;
-        R4 *ga = gacc + (size_t)(gslots == 1 ? 0 : ti) * nint * BLOCK_SLOTS + tid;
+        R4 *ga = gacc + tid;
         const int row_lo = a_lo[me], row_hi = a_lo[me + 1];
         for (int kb = row_lo; kb < row_hi; kb += 8) {
           R dk8 = 0;
@@ -305,14 +318,14 @@ __global__ void __launch_bounds__(BLOCK_SLOTS, 2)
       ft[e] = 0.f;
     }
     __syncwarp();
-    if (MEAM && (gslots == 1 || ++since_flush == GACC_FLUSH_BLOCKS)) {
-      flush_gacc(have, ti);
+    if (MEAM && ++since_flush == GACC_FLUSH_BLOCKS) {
+      flush_gacc(tab_t);
       since_flush = 0;
     }
   }
   __syncthreads();
-  if (MEAM && gslots > 1 && since_flush > 0) {
-    flush_gacc(false, 0);
+  if (MEAM && since_flush > 0 && tab_t >= 0) {
+    flush_gacc(tab_t);
     __syncthreads();
   }
   double *out = partial + ((size_t)cand * gridDim.x + blockIdx.x) * stride;

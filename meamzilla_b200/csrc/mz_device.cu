@@ -569,6 +569,31 @@ mz_status mz_create(const mz_db *dbh, const mz_pot *poth, const mz_settings *set
     }
     d.nblocks = (int)blk.size() - 1;
     d.blk_atom0 = dupload(ctx, blk.data(), blk.size());
+    // type-pure atom blocks of the adjoint (one g-table type per block)
+    {
+      std::vector<int> order(N);
+      for (int i = 0; i < N; ++i) order[i] = i;
+      std::stable_sort(order.begin(), order.end(),
+                       [&](int a, int b) { return db.atom_type[a] < db.atom_type[b]; });
+      std::vector<int> b0(1, 0);
+      int slots = 0, atoms = 0, ty = -1;
+      for (int q = 0; q < N; ++q) {
+        const int i = order[q];
+        const int n = (int)(db.pair_off[i + 1] - db.pair_off[i]);
+        if (atoms > 0 && (db.atom_type[i] != ty || slots + n > BLOCK_SLOTS || atoms + 1 > BLOCK_ATOMS)) {
+          b0.push_back(q);
+          slots = 0;
+          atoms = 0;
+        }
+        ty = db.atom_type[i];
+        slots += n;
+        atoms += 1;
+      }
+      b0.push_back(N);
+      d.adj_nblocks = (int)b0.size() - 1;
+      d.adj_atoms = dupload(ctx, order.data(), order.size());
+      d.adj_blk0 = dupload(ctx, b0.data(), b0.size());
+    }
 
     // ---- shared memory of the kernels
     ctx->smem_atoms[0] = atoms_smem_bytes<double>(ns, ctx->pstride);
@@ -595,9 +620,9 @@ mz_status mz_create(const mz_db *dbh, const mz_pot *poth, const mz_settings *set
     smem_attr(k_adj<false, float>, ctx->smem_adj[1]);
     int nsm = 0, per_sm = 0;
     ck(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, ctx->device), "attribute");
-    ck(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_adj<true, double>, BLOCK_SLOTS, ctx->smem_adj[0]),
+    ck(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_adj<true, float>, BLOCK_SLOTS, ctx->smem_adj[1]),
        "occupancy");
-    ctx->adj_ctas = std::max(1, std::min(d.nblocks, nsm * std::max(1, per_sm)));
+    ctx->adj_ctas = std::max(1, std::min(d.adj_nblocks, nsm * std::max(1, per_sm)));
     ctx->nsm = nsm;
     {
       const char *env = std::getenv("MZ_GRAPH");

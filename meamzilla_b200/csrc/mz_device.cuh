@@ -49,6 +49,12 @@ struct DevDb {
   const float *pair_rf, *pair_uxf, *pair_uyf, *pair_uzf, *pair_shiftf;  // FP32 copies
   // atom blocks
   const int *blk_atom0;           // [nblocks+1]
+  // atom blocks of the adjoint: atoms grouped by type (adj_atoms, a
+  // permutation), each block of one type, <= BLOCK_SLOTS slots and
+  // <= BLOCK_ATOMS atoms; block b holds adj_atoms[adj_blk0[b] .. adj_blk0[b+1])
+  int adj_nblocks;
+  const int *adj_atoms;
+  const int *adj_blk0;
 };
 
 struct DevPot {
