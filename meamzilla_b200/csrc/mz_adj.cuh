@@ -39,7 +39,7 @@ constexpr int GACC_FLUSH_BLOCKS = 16;  // atom blocks between flushes of the per
 // another type and every GACC_FLUSH_BLOCKS blocks.
 
 // Shared-memory layout of k_adj (dynamic), see adj_smem_bytes():
-//   double wtab[ADJ_WARPS][stride]          per-warp table gradients (FP64)
+//   double wtab[stride]                     the CTA's table gradients (FP64, shared-memory atomics)
 //   float  ftab[ADJ_WARPS][stride]          per-warp pair-function gradients of one block (FP32)
 //   R4 gacc[ng-1][BLOCK_SLOTS]              per-thread g-table gradients of one type, power basis
 //   double red[BLOCK_SLOTS], a_chi[BLOCK_ATOMS], a_dF[BLOCK_ATOMS]
@@ -51,7 +51,7 @@ constexpr int GACC_FLUSH_BLOCKS = 16;  // atom blocks between flushes of the per
 template <typename R>
 __host__ __device__ inline size_t adj_smem_bytes(int nsplines, int stride, int pstride, bool meam, int ntypes,
                                                  int ng) {
-  size_t b = sizeof(double) * (size_t)ADJ_WARPS * stride + sizeof(float) * (size_t)ADJ_WARPS * stride;
+  size_t b = sizeof(double) * (size_t)stride + sizeof(float) * (size_t)ADJ_WARPS * stride;
   b = (b + 31) & ~size_t(31);
   if (meam) b += 4 * sizeof(R) * (size_t)(ng - 1) * BLOCK_SLOTS;
   b += sizeof(double) * (BLOCK_SLOTS + 2 * BLOCK_ATOMS);
@@ -65,7 +65,7 @@ __host__ __device__ inline size_t adj_smem_bytes(int nsplines, int stride, int p
 }
 
 template <bool MEAM, typename R>
-__global__ void __launch_bounds__(BLOCK_SLOTS, sizeof(R) == 4 ? 3 : 2)
+__global__ void __launch_bounds__(BLOCK_SLOTS, sizeof(R) == 4 ? 4 : 2)
     k_adj(DevDb db, DevPot pot, const SplineGeom *__restrict__ geom, const double *__restrict__ tabs,
           const double *__restrict__ ptabs, const double *__restrict__ aout, const double *__restrict__ aux,
           const double *__restrict__ lam, const double *__restrict__ seeds, double *__restrict__ partial) {
@@ -80,8 +80,8 @@ __global__ void __launch_bounds__(BLOCK_SLOTS, sizeof(R) == 4 ? 3 : 2)
   const int nint = ng - 1;
 
   double *wtab = reinterpret_cast<double *>(smem_raw);
-  float *ftab = reinterpret_cast<float *>(wtab + (size_t)ADJ_WARPS * stride);
-  size_t off = sizeof(double) * (size_t)ADJ_WARPS * stride + sizeof(float) * (size_t)ADJ_WARPS * stride;
+  float *ftab = reinterpret_cast<float *>(wtab + (size_t)stride);
+  size_t off = sizeof(double) * (size_t)stride + sizeof(float) * (size_t)ADJ_WARPS * stride;
   off = (off + 31) & ~size_t(31);
   R4 *gacc = reinterpret_cast<R4 *>(smem_raw + off);
   if (MEAM) off += 4 * sizeof(R) * (size_t)nint * BLOCK_SLOTS;
@@ -104,14 +104,12 @@ __global__ void __launch_bounds__(BLOCK_SLOTS, sizeof(R) == 4 ? 3 : 2)
   const double *tc = tabs + (size_t)cand * stride;
   const double *pcand = ptabs + (size_t)cand * pot.pow_stride;
   for (int i = tid; i < pot.pow_stride; i += blockDim.x) ptab[i] = (R)pcand[i];
-  for (int i = tid; i < ADJ_WARPS * stride; i += blockDim.x) {
-    wtab[i] = 0.0;
-    ftab[i] = 0.f;
-  }
+  for (int i = tid; i < stride; i += blockDim.x) wtab[i] = 0.0;
+  for (int i = tid; i < ADJ_WARPS * stride; i += blockDim.x) ftab[i] = 0.f;
   if (MEAM)
     for (int i = tid; i < nint * BLOCK_SLOTS; i += blockDim.x) gacc[i] = R4{};
   for (int i = tid; i < pot.nsplines; i += blockDim.x) sg[i] = geom[i];
-  double *wt = wtab + (size_t)warp * stride;
+  double *wt = wtab;
   float *ft = ftab + (size_t)warp * stride;
   auto add_f = [&](int idx, double v) { atomicAdd(ft + idx, (float)v); };
 
@@ -130,7 +128,8 @@ __global__ void __launch_bounds__(BLOCK_SLOTS, sizeof(R) == 4 ? 3 : 2)
 #pragma unroll
       for (int q = 0; q < 4; ++q)
         for (int o = 16; o > 0; o >>= 1) d[q] += __shfl_down_sync(0xffffffffu, d[q], o);
-      if (lane == 0) power_to_table(gg, m, d[0], d[1], d[2], d[3], [&](int idx, double x) { wt[gg.toff + idx] += x; });
+      if (lane == 0)
+        power_to_table(gg, m, d[0], d[1], d[2], d[3], [&](int idx, double x) { atomicAdd(wt + gg.toff + idx, x); });
     }
     for (int m = 0; m < nint; ++m) gacc[m * BLOCK_SLOTS + tid] = R4{};
   };
@@ -241,7 +240,7 @@ __global__ void __launch_bounds__(BLOCK_SLOTS, sizeof(R) == 4 ? 3 : 2)
         a_chi[a] = (eps * U.grad + U.grad2 * K) * drt + kap * dpen;
         a_dF[a] = U.grad;
         const int toffU = gU.toff;
-        spl_point_adjoint(gU, U, rt, eps, K, [&](int idx, double v) { wt[toffU + idx] += v; });
+        spl_point_adjoint(gU, U, rt, eps, K, [&](int idx, double v) { atomicAdd(wt + toffU + idx, v); });
       }
     }
     __syncthreads();
@@ -314,7 +313,8 @@ __global__ void __launch_bounds__(BLOCK_SLOTS, sizeof(R) == 4 ? 3 : 2)
     __syncwarp();
     // the block's FP32 pair-function sums into the warp's FP64 table
     for (int e = lane; e < stride; e += 32) {
-      wt[e] += (double)ft[e];
+      const float v = ft[e];
+      if (v != 0.f) atomicAdd(wt + e, (double)v);
       ft[e] = 0.f;
     }
     __syncwarp();
@@ -330,9 +330,7 @@ __global__ void __launch_bounds__(BLOCK_SLOTS, sizeof(R) == 4 ? 3 : 2)
   }
   double *out = partial + ((size_t)cand * gridDim.x + blockIdx.x) * stride;
   for (int e = tid; e < stride; e += blockDim.x) {
-    double s = 0.0;
-    for (int w = 0; w < ADJ_WARPS; ++w) s += wtab[(size_t)w * stride + e];
-    out[e] = s;
+    out[e] = wtab[e];
   }
 }
 
