@@ -59,7 +59,7 @@ enum {
 };
 
 /* potential styles (the #T string of the potential file) */
-enum { MZ_STYLE_EAM_SPLINE = 0, MZ_STYLE_MEAM_SPLINE = 1 };
+enum { MZ_STYLE_EAM_SPLINE = 0, MZ_STYLE_MEAM_SPLINE = 1, MZ_STYLE_GMEAM_SPLINE = 2 };
 
 typedef struct mz_pot mz_pot;  /* a potential: splines + parameter layout        */
 typedef struct mz_db mz_db;    /* configuration database + neighbour lists       */

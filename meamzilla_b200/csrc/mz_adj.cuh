@@ -39,21 +39,25 @@ constexpr int GACC_FLUSH_BLOCKS = 16;  // atom blocks between flushes of the per
 // another type and every GACC_FLUSH_BLOCKS blocks.
 
 // Shared-memory layout of k_adj (dynamic), see adj_smem_bytes():
-//   double wtab[stride]                     the CTA's table gradients (FP64, shared-memory atomics)
+//   double wtab[ADJ_WARPS][stride]          per-warp table gradients (FP64; lane 0 / distinct
+//                                           lanes write, so the sums are bit-reproducible)
 //   float  ftab[ADJ_WARPS][stride]          per-warp pair-function gradients of one block (FP32)
-//   R4 gacc[ng-1][BLOCK_SLOTS]              per-thread g-table gradients of one type, power basis
+//   R4 gacc[gtabs][ng-1][BLOCK_SLOTS]       per-thread g-table gradients, power basis: one table
+//                                           (the block's type) for MEAM; one per partner type for
+//                                           GMEAM, flushed every block
 //   double red[BLOCK_SLOTS], a_chi[BLOCK_ATOMS], a_dF[BLOCK_ATOMS]
 //   SplineGeom sg[nsplines]; int a_lo[BLOCK_ATOMS+2], a_idx[BLOCK_ATOMS], a_len[BLOCK_ATOMS]
 //   R ptab[pstride]
 //   R4 srow[BLOCK_SLOTS+8]  (u_x, u_y, u_z, f)              of every slot (zero padded)
 //   R4 sadj[BLOCK_SLOTS+8]  (a f', a f / r, Q_x, Q_y)        with Q = f Lambda / r
 //   R  sqz[BLOCK_SLOTS+8]   Q_z
+//   int stype[BLOCK_SLOTS+8] neighbour type of every slot (GMEAM)
 template <typename R>
-__host__ __device__ inline size_t adj_smem_bytes(int nsplines, int stride, int pstride, bool meam, int ntypes,
+__host__ __device__ inline size_t adj_smem_bytes(int nsplines, int stride, int pstride, bool meam, int gtabs,
                                                  int ng) {
-  size_t b = sizeof(double) * (size_t)stride + sizeof(float) * (size_t)ADJ_WARPS * stride;
+  size_t b = sizeof(double) * (size_t)ADJ_WARPS * stride + sizeof(float) * (size_t)ADJ_WARPS * stride;
   b = (b + 31) & ~size_t(31);
-  if (meam) b += 4 * sizeof(R) * (size_t)(ng - 1) * BLOCK_SLOTS;
+  if (meam) b += 4 * sizeof(R) * (size_t)gtabs * (ng - 1) * BLOCK_SLOTS;
   b += sizeof(double) * (BLOCK_SLOTS + 2 * BLOCK_ATOMS);
   b += sizeof(SplineGeom) * nsplines;
   b += sizeof(int) * (3 * BLOCK_ATOMS + 2);
@@ -61,11 +65,12 @@ __host__ __device__ inline size_t adj_smem_bytes(int nsplines, int stride, int p
   b += sizeof(R) * (pstride + 4);
   b = (b + 31) & ~size_t(31);
   b += 9 * sizeof(R) * (BLOCK_SLOTS + 8);
+  b += sizeof(int) * (BLOCK_SLOTS + 8);
   return b;
 }
 
-template <bool MEAM, typename R>
-__global__ void __launch_bounds__(BLOCK_SLOTS, sizeof(R) == 4 ? 4 : 2)
+template <bool MEAM, typename R, bool GM = false>
+__global__ void __launch_bounds__(BLOCK_SLOTS, sizeof(R) == 4 ? 3 : 2)
     k_adj(DevDb db, DevPot pot, const SplineGeom *__restrict__ geom, const double *__restrict__ tabs,
           const double *__restrict__ ptabs, const double *__restrict__ aout, const double *__restrict__ aux,
           const double *__restrict__ lam, const double *__restrict__ seeds, double *__restrict__ partial) {
@@ -78,13 +83,14 @@ __global__ void __launch_bounds__(BLOCK_SLOTS, sizeof(R) == 4 ? 4 : 2)
   const int stride = pot.tab_stride;
   const int ng = MEAM ? pot.g_nmax : 2;  // per-thread tables sized by the largest g spline
   const int nint = ng - 1;
+  const int gtabs = GM ? pot.ntypes : 1;
 
   double *wtab = reinterpret_cast<double *>(smem_raw);
-  float *ftab = reinterpret_cast<float *>(wtab + (size_t)stride);
-  size_t off = sizeof(double) * (size_t)stride + sizeof(float) * (size_t)ADJ_WARPS * stride;
+  float *ftab = reinterpret_cast<float *>(wtab + (size_t)ADJ_WARPS * stride);
+  size_t off = sizeof(double) * (size_t)ADJ_WARPS * stride + sizeof(float) * (size_t)ADJ_WARPS * stride;
   off = (off + 31) & ~size_t(31);
   R4 *gacc = reinterpret_cast<R4 *>(smem_raw + off);
-  if (MEAM) off += 4 * sizeof(R) * (size_t)nint * BLOCK_SLOTS;
+  if (MEAM) off += 4 * sizeof(R) * (size_t)gtabs * nint * BLOCK_SLOTS;
   double *red = reinterpret_cast<double *>(smem_raw + off);
   double *a_chi = red + BLOCK_SLOTS;
   double *a_dF = a_chi + BLOCK_ATOMS;
@@ -100,16 +106,19 @@ __global__ void __launch_bounds__(BLOCK_SLOTS, sizeof(R) == 4 ? 4 : 2)
   R4 *srow = reinterpret_cast<R4 *>(smem_raw + off);
   R4 *sadj = srow + BLOCK_SLOTS + 8;
   R *sqz = reinterpret_cast<R *>(sadj + BLOCK_SLOTS + 8);
+  int *stype = reinterpret_cast<int *>(sqz + BLOCK_SLOTS + 8);
 
   const double *tc = tabs + (size_t)cand * stride;
   const double *pcand = ptabs + (size_t)cand * pot.pow_stride;
   for (int i = tid; i < pot.pow_stride; i += blockDim.x) ptab[i] = (R)pcand[i];
-  for (int i = tid; i < stride; i += blockDim.x) wtab[i] = 0.0;
-  for (int i = tid; i < ADJ_WARPS * stride; i += blockDim.x) ftab[i] = 0.f;
+  for (int i = tid; i < ADJ_WARPS * stride; i += blockDim.x) {
+    wtab[i] = 0.0;
+    ftab[i] = 0.f;
+  }
   if (MEAM)
-    for (int i = tid; i < nint * BLOCK_SLOTS; i += blockDim.x) gacc[i] = R4{};
+    for (int i = tid; i < gtabs * nint * BLOCK_SLOTS; i += blockDim.x) gacc[i] = R4{};
   for (int i = tid; i < pot.nsplines; i += blockDim.x) sg[i] = geom[i];
-  double *wt = wtab;
+  double *wt = wtab + (size_t)warp * stride;
   float *ft = ftab + (size_t)warp * stride;
   auto add_f = [&](int idx, double v) { atomicAdd(ft + idx, (float)v); };
 
@@ -129,9 +138,29 @@ __global__ void __launch_bounds__(BLOCK_SLOTS, sizeof(R) == 4 ? 4 : 2)
       for (int q = 0; q < 4; ++q)
         for (int o = 16; o > 0; o >>= 1) d[q] += __shfl_down_sync(0xffffffffu, d[q], o);
       if (lane == 0)
-        power_to_table(gg, m, d[0], d[1], d[2], d[3], [&](int idx, double x) { atomicAdd(wt + gg.toff + idx, x); });
+        power_to_table(gg, m, d[0], d[1], d[2], d[3], [&](int idx, double x) { wt[gg.toff + idx] += x; });
     }
     for (int m = 0; m < nint; ++m) gacc[m * BLOCK_SLOTS + tid] = R4{};
+  };
+  // GMEAM: this thread's table tk holds triplets (i; j, k) with j its slot's
+  // neighbour type (tj_mine) and k of type tk, i.e. g spline (t; tj_mine, tk).
+  auto flush_gacc_gm = [&](int t, bool have_t, int tj_mine) {
+    for (int v = 0; v < pot.ntypes; ++v)
+      for (int tk = 0; tk < pot.ntypes; ++tk) {
+        const SplineGeom &g2 = sg[gmeam_g_index(pot, t, v, tk)];
+        for (int m = 0; m < g2.n - 1; ++m) {
+          R4 val = R4{};
+          if (have_t && tj_mine == v) val = gacc[(tk * nint + m) * BLOCK_SLOTS + tid];
+          double d[4] = {(double)val.x, (double)val.y, (double)val.z, (double)val.w};
+#pragma unroll
+          for (int q = 0; q < 4; ++q)
+            for (int o = 16; o > 0; o >>= 1) d[q] += __shfl_down_sync(0xffffffffu, d[q], o);
+          if (lane == 0)
+            power_to_table(g2, m, d[0], d[1], d[2], d[3],
+                           [&](int idx, double x) { wt[g2.toff + idx] += x; });
+        }
+      }
+    for (int i = 0; i < gtabs * nint; ++i) gacc[i * BLOCK_SLOTS + tid] = R4{};
   };
 
   int since_flush = 0, tab_t = -1;
@@ -159,7 +188,7 @@ __global__ void __launch_bounds__(BLOCK_SLOTS, sizeof(R) == 4 ? 4 : 2)
     __syncthreads();
     const int nslot = a_lo[na];
     const int ti = db.atom_type[a_idx[0]];  // every atom of the block
-    if (MEAM && tab_t >= 0 && ti != tab_t) {
+    if (MEAM && !GM && tab_t >= 0 && ti != tab_t) {
       flush_gacc(tab_t);
       since_flush = 0;
     }
@@ -177,10 +206,12 @@ __global__ void __launch_bounds__(BLOCK_SLOTS, sizeof(R) == 4 ? 4 : 2)
       srow[tid] = R4{};
       sadj[tid] = R4{};
       sqz[tid] = R(0);
+      if (GM) stype[tid] = 0;
       if (tid < 8) {
         srow[BLOCK_SLOTS + tid] = R4{};
         sadj[BLOCK_SLOTS + tid] = R4{};
         sqz[BLOCK_SLOTS + tid] = R(0);
+        if (GM) stype[BLOCK_SLOTS + tid] = 0;
       }
     }
     if (have) {
@@ -212,6 +243,7 @@ __global__ void __launch_bounds__(BLOCK_SLOTS, sizeof(R) == 4 ? 4 : 2)
         q.w = (R)(fp * ip * Ly);
         sadj[tid] = q;
         sqz[tid] = (R)(fp * ip * Lz);
+        if (GM) stype[tid] = pe.tj;
       }
       red[tid] = kp;
     }
@@ -240,7 +272,7 @@ __global__ void __launch_bounds__(BLOCK_SLOTS, sizeof(R) == 4 ? 4 : 2)
         a_chi[a] = (eps * U.grad + U.grad2 * K) * drt + kap * dpen;
         a_dF[a] = U.grad;
         const int toffU = gU.toff;
-        spl_point_adjoint(gU, U, rt, eps, K, [&](int idx, double v) { atomicAdd(wt + toffU + idx, v); });
+        spl_point_adjoint(gU, U, rt, eps, K, [&](int idx, double v) { wt[toffU + idx] += v; });
       }
     }
     __syncthreads();
@@ -248,7 +280,49 @@ __global__ void __launch_bounds__(BLOCK_SLOTS, sizeof(R) == 4 ? 4 : 2)
     if (have) {
       const double chi = a_chi[me], dF = a_dF[me];
       double dKdf = 0.0;
-      if (MEAM) {
+      if (GM) {
+        // GMEAM: g spline (i; j, k) per partner, table by the partner's type
+        const double fp = (double)pe.f, ip = (double)pe.invr;
+        const R gam = (R)(0.5 * chi * fp + dF * a_p * (double)pe.df);
+        const R del = (R)(dF * fp * ip);
+        const R lx = (R)Lx, ly = (R)Ly, lz = (R)Lz, ap = (R)a_p;
+        const int row_lo = a_lo[me], row_hi = a_lo[me + 1];
+        for (int kb = row_lo; kb < row_hi; kb += 8) {
+          R dk8 = 0;
+#pragma unroll
+          for (int u = 0; u < 8; ++u) {
+            const int k = kb + u;
+            const R4 o = srow[k];
+            const R4 q = sadj[k];
+            const int tk = stype[k];
+            const SplineGeom &g2 = sg[gmeam_g_index(pot, ti, pe.tj, tk)];
+            const R ginv = (R)g2.invstep;
+            const R cs = cos_dot(pe.ux, pe.uy, pe.uz, o.x, o.y, o.z);
+            const bool ok = (k < row_hi) && (k != tid) && (cs < g_cut<R>(g2));
+            const R wk = ok ? R(1) : R(0);
+            R b;
+            const int m = g_knot<R>(cs, (R)g2.x0, ginv, g2.n, b);
+            R dg;
+            const R gv = cubic_val_grad<R>(ptab + g2.poff, m, b, ginv, dg);
+            const R qu = q.z * pe.ux + q.w * pe.uy + sqz[k] * pe.uz;
+            dk8 += wk * (q.x * gv - q.y * dg * cs + dg * qu);
+            const R bpk = lx * o.x + ly * o.y + lz * o.z;
+            const R fk = wk * o.w;
+            const R cg = fk * gam;
+            const R cs1 = fk * del * (bpk - ap * cs) * ginv;
+            const R b2 = b * b;
+            R4 *ga = gacc + (size_t)(tk * nint + m) * BLOCK_SLOTS + tid;
+            R4 d = *ga;
+            d.x += cg;
+            d.y += cg * b + cs1;
+            d.z += cg * b2 + R(2) * cs1 * b;
+            d.w += cg * b2 * b + R(3) * cs1 * b2;
+            *ga = d;
+          }
+          dKdf += (double)dk8;
+        }
+        dKdf += ip * (J - a_p * H);
+      } else if (MEAM) {
         const SplineGeom gg = sg[pot.s_g + ti];
         const R *gpc = ptab + gg.poff;
         const R gx0 = (R)gg.x0, ginv = (R)gg.invstep;
@@ -313,24 +387,27 @@ __global__ void __launch_bounds__(BLOCK_SLOTS, sizeof(R) == 4 ? 4 : 2)
     __syncwarp();
     // the block's FP32 pair-function sums into the warp's FP64 table
     for (int e = lane; e < stride; e += 32) {
-      const float v = ft[e];
-      if (v != 0.f) atomicAdd(wt + e, (double)v);
+      wt[e] += (double)ft[e];
       ft[e] = 0.f;
     }
     __syncwarp();
-    if (MEAM && ++since_flush == GACC_FLUSH_BLOCKS) {
+    if (GM) {
+      flush_gacc_gm(tab_t, have, have ? pe.tj : 0);
+    } else if (MEAM && ++since_flush == GACC_FLUSH_BLOCKS) {
       flush_gacc(tab_t);
       since_flush = 0;
     }
   }
   __syncthreads();
-  if (MEAM && since_flush > 0 && tab_t >= 0) {
+  if (MEAM && !GM && since_flush > 0 && tab_t >= 0) {
     flush_gacc(tab_t);
     __syncthreads();
   }
   double *out = partial + ((size_t)cand * gridDim.x + blockIdx.x) * stride;
   for (int e = tid; e < stride; e += blockDim.x) {
-    out[e] = wtab[e];
+    double s = 0.0;
+    for (int w = 0; w < ADJ_WARPS; ++w) s += wtab[(size_t)w * stride + e];
+    out[e] = s;
   }
 }
 
@@ -354,7 +431,15 @@ __global__ void k_grad_final(DevPot pot, const SplineGeom *__restrict__ geom, co
   __syncthreads();
   const double *tab = tabs + (size_t)c * stride;
   if (t == 0 && !pot.omit_pen) {
-    if (pot.style == MZ_STYLE_MEAM_SPLINE) {
+    if (pot.gmeam) {
+      for (int f = 0; f < pot.npair; ++f) {
+        int at = -1;
+        const double my = spline_max_y(geom[pot.s_f + f], tab, &at);
+        const double m = fabs(my);
+        const double fe = 100. * 25. * (1.0 - m) * (1.0 - m);
+        if (at >= 0) ext[at] += 2.0 * fe * (-5000.0) * (1.0 - m) * (my > 0 ? 1.0 : (my < 0 ? -1.0 : 0.0));
+      }
+    } else if (pot.style == MZ_STYLE_MEAM_SPLINE) {
       int at = -1;
       const double my = f_max_y(pot, geom, tab, &at);
       const double m = fabs(my);

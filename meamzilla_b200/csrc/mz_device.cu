@@ -182,16 +182,26 @@ struct Bracket {
 template <bool MEAM, typename R, bool AUX>
 void launch_atoms(mz_ctx *ctx, int n, size_t smem) {
   dim3 ga(ctx->db.nblocks, n);
-  k_atoms<MEAM, R, AUX><<<ga, BLOCK_SLOTS, smem, ctx->stream>>>(ctx->db, ctx->pot, ctx->d_geom, ctx->d_tabs,
-                                                                 ctx->d_ptabs, ctx->d_V, ctx->d_aout, ctx->d_aux);
+  if (MEAM && ctx->pot.gmeam)
+    k_atoms<MEAM, R, AUX, true><<<ga, BLOCK_SLOTS, smem, ctx->stream>>>(ctx->db, ctx->pot, ctx->d_geom, ctx->d_tabs,
+                                                                       ctx->d_ptabs, ctx->d_V, ctx->d_aout,
+                                                                       ctx->d_aux);
+  else
+    k_atoms<MEAM, R, AUX><<<ga, BLOCK_SLOTS, smem, ctx->stream>>>(ctx->db, ctx->pot, ctx->d_geom, ctx->d_tabs,
+                                                                   ctx->d_ptabs, ctx->d_V, ctx->d_aout, ctx->d_aux);
 }
 
 template <bool MEAM, typename R>
 void launch_adj(mz_ctx *ctx, int n, size_t smem) {
   dim3 ga(ctx->adj_ctas, n);
-  k_adj<MEAM, R><<<ga, BLOCK_SLOTS, smem, ctx->stream>>>(ctx->db, ctx->pot, ctx->d_geom, ctx->d_tabs, ctx->d_ptabs,
-                                                          ctx->d_aout, ctx->d_aux, ctx->d_lam, ctx->d_seeds,
-                                                          ctx->d_partial);
+  if (MEAM && ctx->pot.gmeam)
+    k_adj<MEAM, R, true><<<ga, BLOCK_SLOTS, smem, ctx->stream>>>(ctx->db, ctx->pot, ctx->d_geom, ctx->d_tabs,
+                                                                  ctx->d_ptabs, ctx->d_aout, ctx->d_aux, ctx->d_lam,
+                                                                  ctx->d_seeds, ctx->d_partial);
+  else
+    k_adj<MEAM, R><<<ga, BLOCK_SLOTS, smem, ctx->stream>>>(ctx->db, ctx->pot, ctx->d_geom, ctx->d_tabs, ctx->d_ptabs,
+                                                            ctx->d_aout, ctx->d_aux, ctx->d_lam, ctx->d_seeds,
+                                                            ctx->d_partial);
 }
 
 // Enqueue the objective (and, with d_grad, its gradient) of n candidates
@@ -199,14 +209,14 @@ void launch_adj(mz_ctx *ctx, int n, size_t smem) {
 void enqueue(mz_ctx *ctx, int n, const double *d_params, int precision, double *d_obj, double *d_errvec,
              double *d_forces, double *d_energy, double *d_stress, double *d_grad) {
   cudaStream_t st = ctx->stream;
-  const bool meam = ctx->pot.style == MZ_STYLE_MEAM_SPLINE;
+  const bool meam = style_meam(ctx->pot.style);
   const bool mixed = precision == MZ_MIXED;
   const bool grad = d_grad != nullptr;
   {
     Bracket b(ctx, MZ_K_PREP);
     k_prep<<<n, std::max(32, ((ctx->nsplines + 31) / 32) * 32), 0, st>>>(
         n, ctx->P, d_params, ctx->d_base, ctx->d_cmap, ctx->d_geom, ctx->d_nat, ctx->nsplines, ctx->stride,
-        ctx->d_tabs, ctx->pstride, ctx->d_ptabs, ctx->d_ptabf, meam ? ctx->d_wtab : nullptr, ctx->pot.s_g,
+        ctx->d_tabs, ctx->pstride, ctx->d_ptabs, ctx->d_ptabf, ctx->tc_ok ? ctx->d_wtab : nullptr, ctx->pot.s_g,
         ctx->pot.ntypes, TC_NB);
     ck(cudaGetLastError(), "k_prep launch");
   }
@@ -405,7 +415,7 @@ mz_status mz_create(const mz_db *dbh, const mz_pot *poth, const mz_settings *set
       throw Failure{MZ_ERR_RANGE, "neighbour row of " + std::to_string(db.max_row) +
                                       " pairs exceeds the kernel limit of " + std::to_string(BLOCK_SLOTS)};
     if (pot.nsplines() > MAX_SPLINES) throw Failure{MZ_ERR_RANGE, "too many splines"};
-    const bool meam = pot.style == MZ_STYLE_MEAM_SPLINE;
+    const bool meam = style_meam(pot.style);
     if (meam)
       for (auto &g : pot.groups[G_G]) {
         if (g.nknots > MAX_G_KNOTS)
@@ -489,7 +499,9 @@ mz_status mz_create(const mz_db *dbh, const mz_pot *poth, const mz_settings *set
     dp.energy_weight = set->energy_weight;
     dp.stress_weight = set->stress_weight;
     dp.omit_pen = set->omit_punishments;
-    ctx->npen = meam ? 1 : pot.ntypes;
+    dp.gmeam = pot.style == MZ_STYLE_GMEAM_SPLINE;
+    dp.npair = pot.ntypes * (pot.ntypes + 1) / 2;
+    ctx->npen = style_npen(pot.style, pot.ntypes);
     ctx->esize = 8 * db.ncells + 3 * db.natoms + ctx->npen;
 
     // ---- database
@@ -602,8 +614,9 @@ mz_status mz_create(const mz_db *dbh, const mz_pot *poth, const mz_settings *set
     if (meam)
       for (auto &g : pot.groups[G_G]) ng = std::max(ng, g.nknots);
     dp.g_nmax = ng;
-    ctx->smem_adj[0] = adj_smem_bytes<double>(ns, stride, ctx->pstride, meam, pot.ntypes, ng);
-    ctx->smem_adj[1] = adj_smem_bytes<float>(ns, stride, ctx->pstride, meam, pot.ntypes, ng);
+    const int gtabs = dp.gmeam ? pot.ntypes : 1;
+    ctx->smem_adj[0] = adj_smem_bytes<double>(ns, stride, ctx->pstride, meam, gtabs, ng);
+    ctx->smem_adj[1] = adj_smem_bytes<float>(ns, stride, ctx->pstride, meam, gtabs, ng);
     int smem_max = 0;
     ck(cudaDeviceGetAttribute(&smem_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx->device), "attribute");
     if (ctx->smem_adj[0] > (size_t)smem_max || ctx->smem_atoms[0] > (size_t)smem_max)
@@ -618,6 +631,12 @@ mz_status mz_create(const mz_db *dbh, const mz_pot *poth, const mz_settings *set
     smem_attr(k_adj<false, double>, ctx->smem_adj[0]);
     smem_attr(k_adj<true, float>, ctx->smem_adj[1]);
     smem_attr(k_adj<false, float>, ctx->smem_adj[1]);
+    smem_attr(k_atoms<true, double, false, true>, ctx->smem_atoms[0]);
+    smem_attr(k_atoms<true, double, true, true>, ctx->smem_atoms[0]);
+    smem_attr(k_atoms<true, float, false, true>, ctx->smem_atoms[1]);
+    smem_attr(k_atoms<true, float, true, true>, ctx->smem_atoms[1]);
+    smem_attr(k_adj<true, double, true>, ctx->smem_adj[0]);
+    smem_attr(k_adj<true, float, true>, ctx->smem_adj[1]);
     int nsm = 0, per_sm = 0;
     ck(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, ctx->device), "attribute");
     ck(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_adj<true, float>, BLOCK_SLOTS, ctx->smem_adj[1]),
@@ -633,7 +652,7 @@ mz_status mz_create(const mz_db *dbh, const mz_pot *poth, const mz_settings *set
       const char *env = std::getenv("MZ_TC");  // opt-in: "1"
       const bool allowed = env && env[0] == '1';
       ctx->tc = tc_plan(db.max_row, TC_NB, pot.ntypes, ns, smem_max);
-      ctx->tc_ok = allowed && meam && ng + 2 == TC_NB && ctx->tc.smem_bytes > 0;
+      ctx->tc_ok = allowed && pot.style == MZ_STYLE_MEAM_SPLINE && ng + 2 == TC_NB && ctx->tc.smem_bytes > 0;
       if (ctx->tc_ok) {
         smem_attr(k_atoms_tc<TC_NB, false>, (size_t)ctx->tc.smem_bytes);
         smem_attr(k_atoms_tc<TC_NB, true>, (size_t)ctx->tc.smem_bytes);
@@ -858,6 +877,8 @@ extern "C" mz_status mz_objective_noalloc(const mz_db *dbh, const mz_pot *poth, 
     const Db &db = dbh->db;
     const Pot &pot = poth->pot;
     const bool meam = pot.style == MZ_STYLE_MEAM_SPLINE;
+    if (pot.style == MZ_STYLE_GMEAM_SPLINE)
+      throw Failure{MZ_ERR_UNSUPPORTED, "the no-allocation objective supports eam/spline and meam/spline"};
     if (db.max_row > BLOCK_SLOTS)
       throw Failure{MZ_ERR_RANGE, "neighbour row of " + std::to_string(db.max_row) +
                                       " pairs exceeds the kernel limit of " + std::to_string(BLOCK_SLOTS)};
@@ -919,6 +940,8 @@ extern "C" mz_status mz_objective_noalloc(const mz_db *dbh, const mz_pot *poth, 
     dp.energy_weight = set->energy_weight;
     dp.stress_weight = set->stress_weight;
     dp.omit_pen = set->omit_punishments;
+    dp.gmeam = 0;
+    dp.npair = pot.ntypes * (pot.ntypes + 1) / 2;
 
     // ---- host images of the database
     std::vector<int> off32(N + 1), inoff32(N + 1), inslot32(Np), knot32(Np);

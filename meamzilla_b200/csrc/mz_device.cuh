@@ -67,6 +67,8 @@ struct DevPot {
   int embed_extrap;
   int g_nmax;         // largest g-spline knot count (MEAM)
   int omit_pen;       // leave out the style punishments (sharded databases)
+  int gmeam;          // g indexed by (i; j, k) types and one f punishment per f spline
+  int npair;          // ntypes (ntypes + 1) / 2
   double energy_weight, stress_weight;
 };
 

@@ -198,7 +198,14 @@ __host__ __device__ inline size_t atoms_smem_bytes(int nsplines, int pstride) {
   b += sizeof(R) * (pstride + 4);
   b = (b + 31) & ~size_t(31);
   b += 4 * sizeof(R) * (BLOCK_SLOTS + 8);
+  b += sizeof(int) * (BLOCK_SLOTS + 8);  // neighbour type of every slot (GMEAM's g index)
   return b;
+}
+
+// g spline of the triplet (i; j, k) in GMEAM: Triplet_i_jk
+// (PotFns::get_3body_alloy_idx, pot_fns.cpp:166-168).
+__device__ __forceinline__ int gmeam_g_index(const DevPot &pot, int ti, int tj, int tk) {
+  return pot.s_g + ti * pot.npair + pair_ij_index(tj, tk, pot.ntypes);
 }
 
 // Dot product of unit vectors: exact (no fused multiply-add, as the
@@ -234,7 +241,7 @@ __device__ __forceinline__ void warp_slot_sums(const double *red, int lo, int hi
 // is the force atom i's terms add to atom i along slot p; the neighbour
 // receives -V_p (k_gather).  In FP32 the row sums are taken in chunks of 8
 // terms, each chunk added to an FP64 total.
-template <bool MEAM, typename R, bool AUX>
+template <bool MEAM, typename R, bool AUX, bool GM = false>
 __global__ void __launch_bounds__(BLOCK_SLOTS, sizeof(R) == 4 ? 4 : 3)
     k_atoms(DevDb db, DevPot pot, const SplineGeom *__restrict__ geom, const double *__restrict__ tabs,
             const double *__restrict__ ptabs, double *__restrict__ Vout, double *__restrict__ aout,
@@ -258,6 +265,7 @@ __global__ void __launch_bounds__(BLOCK_SLOTS, sizeof(R) == 4 ? 4 : 3)
   off += sizeof(R) * (pot.pow_stride + 4);
   off = (off + 31) & ~size_t(31);
   R4 *srow = reinterpret_cast<R4 *>(smem_raw + off);
+  int *stype = reinterpret_cast<int *>(srow + BLOCK_SLOTS + 8);
 
   const BlockRows br = block_rows(db, blockIdx.x);
   const double *tc = tabs + (size_t)cand * pot.tab_stride;
@@ -282,12 +290,55 @@ __global__ void __launch_bounds__(BLOCK_SLOTS, sizeof(R) == 4 ? 4 : 3)
     }
     srow[tid] = v;
     if (tid < 8) srow[BLOCK_SLOTS + tid] = R4{};
+    if (GM) {
+      stype[tid] = have ? pe.tj : 0;
+      if (tid < 8) stype[BLOCK_SLOTS + tid] = 0;
+    }
   }
   __syncthreads();
 
   // ---- the one pass over the row: G_p, H_p, vk_p
   double G = 0, H = 0, vkx = 0, vky = 0, vkz = 0;
-  if (MEAM && have && (AUX || pe.f != R(0) || pe.df != R(0))) {
+  if (GM && have && (AUX || pe.f != R(0) || pe.df != R(0))) {
+    // GMEAM: the g spline depends on the partner's neighbour type as well
+    const int row_lo = a_lo[me], row_hi = a_lo[me + 1];
+    for (int kb = row_lo; kb < row_hi; kb += 8) {
+      R g8 = 0, h8 = 0, x8 = 0, y8 = 0, z8 = 0;
+#pragma unroll
+      for (int u = 0; u < 8; ++u) {
+        const int k = kb + u;
+        const R4 o = srow[k];
+        const SplineGeom &g2 = sg[gmeam_g_index(pot, ti, pe.tj, stype[k])];
+        const R ginv = (R)g2.invstep;
+        const R cs = cos_dot(pe.ux, pe.uy, pe.uz, o.x, o.y, o.z);
+        const bool ok = (k < row_hi) && (k != tid) && (cs < g_cut<R>(g2));  // triplet_meam_spline.cpp:66-70
+        const R fk = ok ? o.w : R(0);
+        R b;
+        const int kk = g_knot<R>(cs, (R)g2.x0, ginv, g2.n, b);
+        R dg;
+        const R gv = cubic_val_grad<R>(ptab + g2.poff, kk, b, ginv, dg);
+        const R dgfk = dg * fk;
+        g8 += gv * fk;
+        h8 += dgfk * cs;
+        x8 += dgfk * o.x;
+        y8 += dgfk * o.y;
+        z8 += dgfk * o.z;
+      }
+      G += (double)g8;
+      H += (double)h8;
+      vkx += (double)x8;
+      vky += (double)y8;
+      vkz += (double)z8;
+    }
+    if (AUX) {
+      double *ax = aux + (size_t)cand * AUX_COUNT * Np;
+      ax[AUX_G * Np + gs] = G;
+      ax[AUX_H * Np + gs] = H;
+      ax[AUX_VX * Np + gs] = vkx;
+      ax[AUX_VY * Np + gs] = vky;
+      ax[AUX_VZ * Np + gs] = vkz;
+    }
+  } else if (!GM && MEAM && have && (AUX || pe.f != R(0) || pe.df != R(0))) {
     const SplineGeom gg = sg[pot.s_g + ti];
     const R *gpc = ptab + gg.poff;
     const R gx0 = (R)gg.x0, ginv = (R)gg.invstep;
@@ -528,22 +579,28 @@ __global__ void k_cells(DevDb db, DevPot pot, const double *__restrict__ aout, d
 // ------------------------------------------------------------------ k_final
 
 // Sum of squares over cells + the style's punishment entries.
+// Signed largest-|y| knot of one spline (Spline::get_max_y_mag, spline.cpp:58-67).
+__device__ __forceinline__ double spline_max_y(const SplineGeom &g, const double *tab, int *which) {
+  double sm = 0.0;
+  int sat = -1;
+  for (int k = 0; k < g.n; ++k) {
+    const double y = tab[g.toff + k];
+    if (fabs(sm) < fabs(y)) {
+      sm = y;
+      sat = g.toff + k;
+    }
+  }
+  if (which) *which = sat;
+  return sm;
+}
 __device__ __forceinline__ double f_max_y(const DevPot &pot, const SplineGeom *geom, const double *tab, int *which) {
-  // signed largest-|y| knot over the f splines (spline.cpp:58-67, pot_fns.cpp:223-234)
+  // signed largest-|y| knot over the f splines (pot_fns.cpp:100-111)
   double my = 0.0;
   int at = -1;
   const int nf = pot.ntypes * (pot.ntypes + 1) / 2;
   for (int f = 0; f < nf; ++f) {
-    const SplineGeom &g = geom[pot.s_f + f];
-    double sm = 0.0;
-    int sat = -1;
-    for (int k = 0; k < g.n; ++k) {
-      const double y = tab[g.toff + k];
-      if (fabs(sm) < fabs(y)) {
-        sm = y;
-        sat = g.toff + k;
-      }
-    }
+    int sat;
+    const double sm = spline_max_y(geom[pot.s_f + f], tab, &sat);
     if (fabs(my) < fabs(sm)) {
       my = sm;
       at = sat;
@@ -572,8 +629,18 @@ __global__ void k_final(DevDb db, DevPot pot, const SplineGeom *__restrict__ geo
     const double *tab = tabs + (size_t)c * pot.tab_stride;
     double *ev = errvec ? errvec + (size_t)c * esize + 8 * db.ncells + 3 * db.natoms : nullptr;
     if (pot.omit_pen) {
-      if (ev)
-        for (int q = 0; q < (pot.style == MZ_STYLE_MEAM_SPLINE ? 1 : pot.ntypes); ++q) ev[q] = 0.0;
+      if (ev) {
+        const int npen = pot.style == MZ_STYLE_MEAM_SPLINE ? 1 : pot.gmeam ? pot.npair : pot.ntypes;
+        for (int q = 0; q < npen; ++q) ev[q] = 0.0;
+      }
+    } else if (pot.gmeam) {
+      // one f-magnitude punishment per f spline (pot_gmeam_spline.cpp:173-178)
+      for (int f = 0; f < pot.npair; ++f) {
+        const double m = fabs(spline_max_y(geom[pot.s_f + f], tab, nullptr));
+        const double fe = 100. * 25. * (1.0 - m) * (1.0 - m);
+        total += fe * fe;
+        if (ev) ev[f] = fe;
+      }
     } else if (pot.style == MZ_STYLE_MEAM_SPLINE) {
       // f-potential magnitude punishment (pot_meam_spline.cpp:274-278)
       const double m = fabs(f_max_y(pot, geom, tab, nullptr));

@@ -303,12 +303,16 @@ void parse_pot(const std::string &text, Pot &pot) {
   if (pot.type_name == "meam/spline") {
     pot.style = MZ_STYLE_MEAM_SPLINE;
     nalloy = {npair, nt, nt, npair, nt};
+  } else if (pot.type_name == "gmeam/spline") {
+    // g_i_jk: n * n (n + 1) / 2 splines (pot_gmeam.cpp:31-36)
+    pot.style = MZ_STYLE_GMEAM_SPLINE;
+    nalloy = {npair, nt, nt, npair, nt * npair};
   } else if (pot.type_name == "eam/spline") {
     pot.style = MZ_STYLE_EAM_SPLINE;
     nalloy = {npair, nt, nt};
   } else {
     fail(MZ_ERR_UNSUPPORTED, "potential style \"" + pot.type_name +
-                                 "\" is not implemented (eam/spline, meam/spline)");
+                                 "\" is not implemented (eam/spline, meam/spline, gmeam/spline)");
   }
   pot.ngroups = (int)nalloy.size();
   if (ln >= L.size() || L[ln++].substr(0, 2) != "#P") fail(MZ_ERR_FORMAT, "potential line (#P ...) missing");
@@ -461,7 +465,7 @@ int rescale_pot(Pot &pot, const int *atom_type, int natoms, const double *dens, 
   // PotMEAM::rescale (pot_meam.cpp:281-375) / PotEAM::rescale (pot_eam.cpp:257-389)
   factors[0] = factors[1] = 0.0;
   if (flag < 0) return 0;
-  const bool meam = pot.style == MZ_STYLE_MEAM_SPLINE;
+  const bool meam = style_meam(pot.style);
   std::vector<Spline3> &F = pot.groups[G_U];
   const int Fs = (int)F.size();
   std::vector<double> minrho(Fs, 1e100), maxrho(Fs, -1e100);
@@ -496,7 +500,25 @@ int rescale_pot(Pot &pot, const int *atom_type, int natoms, const double *dens, 
   }
   const double a = (sign == 1) ? 1.0 / R[max_idx] : 1.0 / L[min_idx];
   if (flag || std::abs(a) > 1.05 || std::abs(a) < 0.95) flag = 1;
-  if (meam && flag) {
+  if (meam && flag && pot.style == MZ_STYLE_GMEAM_SPLINE) {
+    // PotGMEAM::rescale_3body (pot_gmeam.cpp:301-345): each f_ij by its own
+    // b = 1 / signed largest-|y| knot, and every g_i_jk whose f_ij or f_ik it
+    // is divided by b (twice when j and k give the same f)
+    const int nt = pot.ntypes;
+    std::vector<Spline3> &fg = pot.groups[G_F], &gg = pot.groups[G_G];
+    for (int fi = 0; fi < (int)fg.size(); ++fi) {
+      const double b = 1.0 / fg[fi].max_y_mag();
+      fg[fi].scale_y(b);
+      for (int i = 0; i < nt; ++i)
+        for (int j = 0; j < nt; ++j)
+          for (int k = j; k < nt; ++k) {
+            const int ijk = i * nt * (nt + 1) / 2 + pot.idx_pair_ij(j, k);
+            if (fi == pot.idx_pair_ij(i, j)) gg[ijk].divide_y(b);
+            if (fi == pot.idx_pair_ij(i, k)) gg[ijk].divide_y(b);
+          }
+      if (fi == 0) factors[1] = b;
+    }
+  } else if (meam && flag) {
     // PotMEAM::rescale_3body (pot_meam.cpp:497-525): f*f*g = (b f)(b f)(g / b^2),
     // b = 1 / signed largest-|y| knot of the f group (PotFns::get_max_y_mag, pot_fns.cpp:100-111)
     double m = 0.0;
@@ -574,8 +596,8 @@ void write_data_files(const Db &db, const Pot &pot, double energy_weight, double
   // pot_eam.cpp:506-540), .energy (:497-543), .stress (:548-592), .force
   // (:597-642), .error (:647-708), .punish (PotEAM / PotMEAM::write_punish).
   const int NC = db.ncells, N = db.natoms;
-  const bool meam = pot.style == MZ_STYLE_MEAM_SPLINE;
-  const int npen = meam ? 1 : pot.ntypes;
+  const bool meam = style_meam(pot.style);
+  const int npen = style_npen(pot.style, pot.ntypes);
   const int esize = 8 * NC + 3 * N + npen;
   {
     std::ofstream f = open_out(data_name(prefix, ".rho", num));
@@ -689,7 +711,16 @@ void write_data_files(const Db &db, const Pot &pot, double energy_weight, double
       f << std::setw(3) << std::right << c << std::fixed << std::setw(11) << std::right << std::setprecision(4)
         << db.cell_weight[c] << std::setw(15) << std::right << std::setprecision(6) << e[idx] * e[idx]
         << std::setw(15) << std::right << std::setprecision(6) << e[idx] / db.cell_weight[c] << std::endl;
-    if (meam) {
+    if (pot.style == MZ_STYLE_GMEAM_SPLINE) {
+      // PotGMEAM::write_punish (pot_gmeam.cpp:246-296): one line per f spline
+      f << std::endl << "Dummy constraints (|f_max(r)| = 1)" << std::endl;
+      f << std::setw(15) << std::right << "punish error" << std::setw(15) << std::right << "|f_max(r)|" << std::endl;
+      for (const Spline3 &sp : pot.groups[G_F]) {
+        f << std::fixed << std::setw(15) << std::right << std::setprecision(6) << e[idx] * e[idx] << std::setw(15)
+          << std::right << std::setprecision(6) << std::abs(std::abs(sp.max_y_mag())) << std::endl;
+        ++idx;
+      }
+    } else if (meam) {
       double m = 0.0;
       for (const Spline3 &sp : pot.groups[G_F]) {
         const double v = sp.max_y_mag();
@@ -735,7 +766,7 @@ struct CellPairs {
 void build_db_setup(const mz_cells_desc &c, const Pot &pot, Db &db) {
   if (c.ncells <= 0 || c.natoms <= 0 || !c.cell_natoms || !c.cell_lattice || !c.atom_type || !c.atom_pos)
     fail(MZ_ERR_ARG, "empty or incomplete cell description");
-  const bool meam = pot.style == MZ_STYLE_MEAM_SPLINE;
+  const bool meam = style_meam(pot.style);
   db.ncells = c.ncells;
   db.natoms = c.natoms;
   db.cell_atom0.assign(c.ncells + 1, 0);
@@ -809,7 +840,7 @@ void build_incoming(Db &db) {
 
 void build_db(const mz_cells_desc &c, const Pot &pot, Db &db) {
   build_db_setup(c, pot, db);
-  const bool meam = pot.style == MZ_STYLE_MEAM_SPLINE;
+  const bool meam = style_meam(pot.style);
   const double max_rcut = pot.max_rcut();
   const int sphi0 = pot.spline_index(G_PHI, 0), srho0 = pot.spline_index(G_RHO, 0);
   const int sf0 = meam ? pot.spline_index(G_F, 0) : -1;

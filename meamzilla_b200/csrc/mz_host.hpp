@@ -57,6 +57,15 @@ struct Spline3 {
 // pot_pair.cpp:25-37).  EAM: the first three.
 enum Group { G_PHI = 0, G_RHO = 1, G_U = 2, G_F = 3, G_G = 4 };
 
+// MEAM and GMEAM share the skeleton (three-body f f g); GMEAM indexes g by
+// the types of i and of the pair j, k (Triplet_i_jk, pot_fns.cpp:166-168) and
+// punishes every f spline (pot_gmeam_spline.cpp:173-178).
+inline bool style_meam(int style) { return style == MZ_STYLE_MEAM_SPLINE || style == MZ_STYLE_GMEAM_SPLINE; }
+// Entries after the per-cell constraints: MEAM 1, GMEAM one per f spline, EAM one per type.
+inline int style_npen(int style, int ntypes) {
+  return style == MZ_STYLE_MEAM_SPLINE ? 1 : style == MZ_STYLE_GMEAM_SPLINE ? ntypes * (ntypes + 1) / 2 : ntypes;
+}
+
 struct Pot {
   int style = MZ_STYLE_MEAM_SPLINE;
   int ntypes = 1;

@@ -174,7 +174,7 @@ struct DevBufs {
 
 void build_db_device(const mz_cells_desc &c, const Pot &pot, Db &db, int device) {
   build_db_setup(c, pot, db);
-  const bool meam = pot.style == MZ_STYLE_MEAM_SPLINE;
+  const bool meam = style_meam(pot.style);
   const double max_rcut = pot.max_rcut();
   const int N = c.natoms, NC = c.ncells;
   // image ranges per cell (host, as the host builder)

@@ -270,7 +270,8 @@ class Evaluator:
         st = db.stats()
         self.natoms, self.ncells = st["natoms"], st["ncells"]
         self.ncoeff = pot.ncoeff
-        self.npen = 1 if pot.style == _lib.MZ_STYLE_MEAM_SPLINE else pot.ntypes
+        self.npen = (1 if pot.style == _lib.MZ_STYLE_MEAM_SPLINE else
+                     pot.ntypes * (pot.ntypes + 1) // 2 if pot.style == _lib.MZ_STYLE_GMEAM_SPLINE else pot.ntypes)
         self.esize = st["esize_cells"] + self.npen
 
     def __del__(self):

@@ -97,16 +97,19 @@ TEACHER = {
 }
 
 
-def n_alloy(kind: str, ntypes: int) -> int:
-    """Number of alloy splines in a function group (src/pot_fns.cpp:403-433)."""
+def n_alloy(kind: str, ntypes: int, style: str = "meam/spline") -> int:
+    """Number of alloy splines in a function group (src/pot_fns.cpp:403-433);
+    gmeam/spline's g is Triplet_i_jk, n n (n + 1) / 2 splines (pot_gmeam.cpp:31-36)."""
     if kind in ("phi", "f"):
         return ntypes * (ntypes + 1) // 2
+    if kind == "g" and style == "gmeam/spline":
+        return ntypes * ntypes * (ntypes + 1) // 2
     return ntypes
 
 
 def teacher_potential(style: str, ntypes: int, rcut: float, seed: int) -> PotSpec:
     rng = np.random.default_rng(seed)
-    kinds = ["phi", "rho", "U"] + (["f", "g"] if style == "meam/spline" else [])
+    kinds = ["phi", "rho", "U"] + (["f", "g"] if style in ("meam/spline", "gmeam/spline") else [])
     groups = []
     for kind in kinds:
         fn, dfn = TEACHER[kind]
@@ -114,7 +117,7 @@ def teacher_potential(style: str, ntypes: int, rcut: float, seed: int) -> PotSpe
             left, right, n = -1.0, 1.0, 8
         else:
             left, right, n = 1.8, rcut, 10
-        groups.append([_spline_from_fn(fn, dfn, left, right, n, rng) for _ in range(n_alloy(kind, ntypes))])
+        groups.append([_spline_from_fn(fn, dfn, left, right, n, rng) for _ in range(n_alloy(kind, ntypes, style))])
     return PotSpec(style, ntypes, groups)
 
 

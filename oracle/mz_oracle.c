@@ -144,12 +144,14 @@ int mzo_ncoeff(const mzo_pot *pot) {
 }
 
 int mzo_esize(const mzo_db *db, const mzo_pot *pot) {
-  return 8 * db->ncells + 3 * db->natoms + (pot->style == 1 ? 1 : pot->ntypes);
+  /* MEAM: one f punishment; GMEAM: one per f spline (pot_gmeam_spline.cpp:173-178); EAM: one per type */
+  return 8 * db->ncells + 3 * db->natoms +
+         (pot->style == 1 ? 1 : pot->style == 2 ? pot->ntypes * (pot->ntypes + 1) / 2 : pot->ntypes);
 }
 
 double mzo_objective(const mzo_db *db, const mzo_pot *pot, const double *coeffs, double *errvec_out,
                      double *forces_out, double *energy_out, double *stress_out, double *dens_out) {
-  const int meam = pot->style == 1;
+  const int meam = pot->style == 1 || pot->style == 2, gmeam = pot->style == 2;
   const int nt = pot->ntypes, npair = nt * (nt + 1) / 2;
   const int N = db->natoms, NC = db->ncells;
   int s, ci = 0, i;
@@ -214,10 +216,13 @@ double mzo_objective(const mzo_db *db, const mzo_pot *pot, const double *coeffs,
       /* Config::find_triplets (config.cpp:262-281) with
        * TripletMEAMSpline::check_triplet (triplet_meam_spline.cpp:49-73):
        * every j<k pair whose cos has a g knot. */
-      const sp_t *g = &gg[ti];
       int j, k;
       for (j = 0; j < n - 1; ++j)
         for (k = j + 1; k < n; ++k) {
+          /* GMEAM: g of (i; j, k) types, Triplet_i_jk (pot_fns.cpp:166-168) */
+          const sp_t *g = gmeam ? &gg[ti * npair + pair_ij(nt, db->atom_type[db->pair_nbr[p0 + j]],
+                                                             db->atom_type[db->pair_nbr[p0 + k]])]
+                                : &gg[ti];
           const double *uj = db->pair_u + 3 * (p0 + j), *uk = db->pair_u + 3 * (p0 + k);
           double c = uj[0] * uk[0] + uj[1] * uk[1] + uj[2] * uk[2];
           double gs;
@@ -324,7 +329,19 @@ double mzo_objective(const mzo_db *db, const mzo_pot *pot, const double *coeffs,
     sum += ev[idx] * ev[idx];
     ++idx;
   }
-  if (meam) {
+  if (gmeam) {
+    /* pot_gmeam_spline.cpp:173-178: one punishment per f spline */
+    int f, k;
+    for (f = 0; f < npair; ++f) {
+      double m = 0.0;
+      for (k = 0; k < ff[f].n; ++k)
+        if (fabs(m) < fabs(ff[f].y[k])) m = ff[f].y[k];
+      double mag = fabs(m);
+      double fe = DUMMY_WEIGHT * 25. * (1.0 - mag) * (1.0 - mag);
+      sum += fe * fe;
+      ev[idx++] = fe;
+    }
+  } else if (meam) {
     /* pot_meam_spline.cpp:274-278 with PotFns::get_max_y_mag (pot_fns.cpp:223-234)
      * and Spline::get_max_y_mag (spline.cpp:58-67) */
     double my = 0.0;

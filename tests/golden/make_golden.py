@@ -76,6 +76,23 @@ def in_range_meam(pot):
     return p
 
 
+def gmeam_goldens():
+    """gmeam/spline: g indexed by (i; j, k) types, one f punishment per f spline."""
+    # 6. two species, cells of the two-species rule, teacher as generated
+    _, cells = synth.make_workload("meam2k", seed=8, ncells=3)
+    cells = [c for c in cells if c.natoms <= 400][:3] or cells[:1]
+    _targets(cells, 6)
+    pot = synth.teacher_potential("gmeam/spline", 2, 5.5, seed=21)
+    _write("gmeam_mix2", pot, cells, fd=True)
+    # 7. one species in range (no density punishment), per-cell weights
+    _, cells = synth.make_workload("meam200", seed=9, ncells=4)
+    _targets(cells, 7)
+    for i, c in enumerate(cells):
+        c.weight = 1.0 + 0.25 * i
+    pot = synth.teacher_potential("gmeam/spline", 1, 4.5, seed=22)
+    _write("gmeam_inrange1", in_range_meam(pot), cells, fd=True, energy_weight=1.5, stress_weight=0.5)
+
+
 def data_goldens():
     """ref.{rho,energy,stress,force,error,punish}: the text files the
     reference's Potential::write_data writes for the start potential."""
@@ -153,7 +170,9 @@ def main():
 
 if __name__ == "__main__":
     import sys
-    if "--rescale-only" not in sys.argv and "--data-only" not in sys.argv:
+    if "--gmeam" in sys.argv:
+        gmeam_goldens()
+    elif "--rescale-only" not in sys.argv and "--data-only" not in sys.argv:
         main()
     if "--data-only" not in sys.argv:
         rescale_goldens()
