@@ -272,6 +272,16 @@ def add_targets(cells, energy, stress, forces, rng):
         c.force0 = np.asarray(forces[i], dtype=np.float64) + rng.normal(0.0, 0.01, (c.natoms, 3))
 
 
+def set_teacher_targets(cells, energy, stress, forces, seed: int):
+    """Targets = teacher outputs (energy per atom [ncells], stress [ncells, 6]
+    in eV/A^3, forces [natoms, 3]) + the noise of add_targets, seeded."""
+    a0 = np.cumsum([0] + [c.natoms for c in cells])
+    forces = np.asarray(forces, dtype=np.float64).reshape(-1, 3)
+    stress = np.asarray(stress, dtype=np.float64).reshape(-1, 6)
+    add_targets(cells, np.asarray(energy, dtype=np.float64).ravel(), stress,
+                [forces[a0[i]:a0[i + 1]] for i in range(len(cells))], np.random.default_rng(seed))
+
+
 # ----------------------------------------------------------------------------
 # workloads
 # ----------------------------------------------------------------------------
@@ -294,6 +304,20 @@ def make_workload(name: str, seed: int = 0, ncells: Optional[int] = None):
     rng = np.random.default_rng(2000 + seed)
     cells = make_cells(n_cells, rule, rng, ntypes=ntypes, mix=mix)
     return pot, cells
+
+
+# The gradient check of the single-species MEAM workload (200 cells): the
+# teacher as generated or its in-range variant, targets = teacher outputs +
+# noise (seed below), 10 parameter points = teacher + N(0, sigma).
+GRAD10 = {"workload": "meam200", "seed": 0, "target_seed": 3100, "point_seed": 3200, "npoints": 10,
+          "sigma": {"raw": 0.05, "inrange": 0.005}}
+
+
+def grad10_workload(variant: str):
+    """(teacher PotSpec, cells without targets) of the gradient check;
+    variant "raw" (the teacher as generated) or "inrange"."""
+    pot, cells = make_workload(GRAD10["workload"], seed=GRAD10["seed"])
+    return (in_range_variant(pot) if variant == "inrange" else pot), cells
 
 
 def in_range_variant(pot: PotSpec, rho_scale: float = 0.01, g_scale: float = 0.0025) -> PotSpec:

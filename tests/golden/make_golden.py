@@ -10,7 +10,7 @@ through Potential::compute for two coefficient vectors:
     fdgrad (central differences of the objective, h = 1e-6; small cases)
 
 Run here (needs the reference sources to build mzref):
-    make -C oracle && python tests/golden/make_golden.py
+    make -C oracle && python tests/golden/make_golden.py [--gmeam | --grad10]
 """
 from __future__ import annotations
 
@@ -120,6 +120,42 @@ def rescale_goldens():
         print(name, "rescale returns", out["flag0"][0], out["flag1"][0])
 
 
+def grad10_goldens():
+    """The reference's central differences (h = 1e-6, ref_harness -fd) of the
+    objective at 10 seeded points on the 200-cell single-species MEAM
+    workload, for the teacher as generated and its in-range variant; targets
+    = the reference's teacher outputs + seeded noise (synth.GRAD10).  Only
+    the points and the reference's results are stored: the database is
+    regenerated from the seeds by synth.grad10_workload."""
+    import shutil
+    import tempfile
+    from concurrent.futures import ThreadPoolExecutor
+    out = {}
+    tmp = tempfile.mkdtemp()
+    try:
+        for variant in ("raw", "inrange"):
+            pot, cells = synth.grad10_workload(variant)
+            d = os.path.join(tmp, variant)
+            par = synth.write_case(d, pot, cells)
+            t = oracle.run_reference(par, cwd=d)
+            synth.set_teacher_targets(cells, t["energy"], t["stress"], t["force"], synth.GRAD10["target_seed"])
+            synth.write_config(os.path.join(d, "db.conf"), cells)
+            x0 = oracle.run_reference(par, cwd=d)["coeff"]
+            X = synth.perturbed(x0, synth.GRAD10["npoints"], synth.GRAD10["sigma"][variant],
+                                synth.GRAD10["point_seed"])
+            with ThreadPoolExecutor(max_workers=os.cpu_count() or 1) as pool:
+                res = list(pool.map(lambda x: oracle.run_reference(par, cwd=d, coeffs=x, fd_h=1e-6), X))
+            out["x_" + variant] = X
+            out["obj_" + variant] = np.array([r["obj"] for r in res])
+            out["fdgrad_" + variant] = np.stack([r["fdgrad"] for r in res])
+            print("grad10", variant, "natoms", sum(c.natoms for c in cells), "obj", out["obj_" + variant][:3])
+    finally:
+        shutil.rmtree(tmp)
+    d = os.path.join(HERE, "meam200_grad10")
+    os.makedirs(d, exist_ok=True)
+    np.savez_compressed(os.path.join(d, "grad10.npz"), **out)
+
+
 def main():
     # 1. EAM, 3 bcc cells (the eam54 rules)
     pot, cells = synth.make_workload("eam54", seed=3, ncells=3)
@@ -170,6 +206,9 @@ def main():
 
 if __name__ == "__main__":
     import sys
+    if "--grad10" in sys.argv:
+        grad10_goldens()
+        sys.exit(0)
     if "--gmeam" in sys.argv:
         gmeam_goldens()
     elif "--rescale-only" not in sys.argv and "--data-only" not in sys.argv:
