@@ -59,7 +59,7 @@ enum {
 };
 
 /* potential styles (the #T string of the potential file) */
-enum { MZ_STYLE_EAM_SPLINE = 0, MZ_STYLE_MEAM_SPLINE = 1, MZ_STYLE_GMEAM_SPLINE = 2 };
+enum { MZ_STYLE_EAM_SPLINE = 0, MZ_STYLE_MEAM_SPLINE = 1, MZ_STYLE_GMEAM_SPLINE = 2, MZ_STYLE_PAIR_SPLINE = 3 };
 
 typedef struct mz_pot mz_pot;  /* a potential: splines + parameter layout        */
 typedef struct mz_db mz_db;    /* configuration database + neighbour lists       */
@@ -72,7 +72,8 @@ const char *mz_last_error(void);
 
 /* Read a potential file (first #P block).  Replaces PotList::init
  * (src/pot_list.cpp:84-177) + Potential::read_pot (potential.cpp:153-161)
- * for the eam/spline and meam/spline styles with spline3eq bases. */
+ * for the eam/spline, meam/spline, gmeam/spline and pair/spline styles with
+ * spline3eq bases. */
 mz_status mz_pot_read(const char *path, mz_pot **out);
 /* Same from the file's text held in memory. */
 mz_status mz_pot_parse(const char *text, mz_pot **out);
@@ -101,7 +102,8 @@ mz_status mz_pot_spline_eval(const mz_pot *pot, int spline, double x, double *va
  * and the database's atom types drive it; flag as the reference's (< 0
  * never, 0 when needed, 1 always).  *rescaled = the reference's return value;
  * factors[0] = embedding scale a, factors[1] = MEAM f scale b (0 if unused).
- * U's knot grid changes, so evaluators must be re-created afterwards. */
+ * U's knot grid changes, so evaluators must be re-created afterwards.
+ * pair/spline never rescales (Potential::rescale, potential.cpp:258-261). */
 mz_status mz_pot_rescale(mz_pot *pot, const mz_db *db, const double *densities, int flag, int *rescaled,
                          double *factors);
 
@@ -109,7 +111,8 @@ mz_status mz_pot_rescale(mz_pot *pot, const mz_db *db, const double *densities, 
  * .stress, .force, .error and .punish files of one evaluated potential
  * (<prefix>.<ext>, or <prefix>.<ext>.<num> when num >= 0), formatted as the
  * reference writes them, from the outputs of one FP64 mz_objective call
- * (errvec, per-cell energy per atom and stress, forces) and mz_densities. */
+ * (errvec, per-cell energy per atom and stress, forces) and mz_densities.
+ * pair/spline writes no .rho and no .punish file; densities may be NULL. */
 mz_status mz_write_data(const mz_db *db, const mz_pot *pot, double energy_weight, double stress_weight,
                         const double *errvec, const double *energy, const double *stress, const double *forces,
                         const double *densities, const char *prefix, int num);
@@ -155,12 +158,14 @@ void mz_db_free(mz_db *db);
 typedef struct {
   int ncells;
   int natoms;
-  int64_t npairs;       /* entries of the full neighbour list             */
+  int64_t npairs;       /* entries of the full neighbour list (pair/spline: */
+                        /* each pair once, config.cpp:181-185)            */
   int64_t ntriplets;    /* j<k pairs of every row (= reference triplets)  */
   int max_row;          /* longest neighbour row                          */
   int esize;            /* residual entries of the cells: 8 ncells + 3    */
-                        /* natoms (the style penalties add 1 for MEAM,    */
-                        /* ntypes for EAM)                                */
+                        /* natoms, 7 ncells + 3 natoms for pair/spline    */
+                        /* (the style penalties add 1 for MEAM, ntypes    */
+                        /* for EAM, one per f spline for GMEAM)           */
 } mz_db_stats;
 mz_status mz_db_info(const mz_db *db, mz_db_stats *stats);
 
@@ -231,7 +236,8 @@ void mz_destroy(mz_ctx *ctx);
  *   errvec [ncand][esize]     the ErrorVec, layout of accumulate_error
  *                             (potential.cpp:415-491) + the style penalty
  *                             entries (pot_meam_spline.cpp:274-278 or
- *                             pot_eam_spline.cpp:211-218)
+ *                             pot_eam_spline.cpp:211-218; none for
+ *                             pair/spline)
  *   forces [ncand][natoms][3] per-atom forces in configuration order
  *   energy [ncand][ncells]    energy per atom of each cell
  *   stress [ncand][ncells][6] stress of each cell (xx yy zz xy yz zx)

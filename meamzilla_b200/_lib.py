@@ -20,6 +20,7 @@ MZ_MIXED = 1
 MZ_STYLE_EAM_SPLINE = 0
 MZ_STYLE_MEAM_SPLINE = 1
 MZ_STYLE_GMEAM_SPLINE = 2
+MZ_STYLE_PAIR_SPLINE = 3
 
 STATUS_NAMES = {
     0: "MZ_OK", 1: "MZ_ERR_ARG", 2: "MZ_ERR_IO", 3: "MZ_ERR_FORMAT", 4: "MZ_ERR_RANGE",

@@ -253,7 +253,9 @@ __global__ void __launch_bounds__(BLOCK_SLOTS, sizeof(R) == 4 ? 3 : 2)
     for (int a = warp; a < na; a += nwarp) {
       double K;
       warp_slot_sums<1>(red, a_lo[a], a_lo[a + 1], lane, &K);
-      if (lane == 0) {
+      if (lane == 0 && pot.pair) {
+        a_chi[a] = a_dF[a] = 0.0;
+      } else if (lane == 0) {
         const int i = a_idx[a];
         const double rho = ao[AO_RHO * N + i];
         const int c = db.atom_cell[i];
@@ -380,7 +382,8 @@ __global__ void __launch_bounds__(BLOCK_SLOTS, sizeof(R) == 4 ? 3 : 2)
         add_f(g.toff + g.n + k + 1, cv * w.wB + cd * w.dB);
       };
       const double eps = sd[CS_EPS * NC + cell];
-      if (pe.kphi >= 0) pair_adj(pot.s_phi + pe.pij, pe.kphi, pe.bphi, 0.5 * eps, 0.5 * a_p);
+      const double sp = phi_share(pot, db.pair_nbr[gs] == ia);
+      if (pe.kphi >= 0) pair_adj(pot.s_phi + pe.pij, pe.kphi, pe.bphi, sp * eps, sp * a_p);
       if (pe.krho >= 0) pair_adj(pot.s_rho + pe.tj, pe.krho, pe.brho, chi, dF * a_p);
       if (MEAM && pe.kf >= 0) pair_adj(pot.s_f + pe.pij, pe.kf, pe.bf, chi * G + dF * dKdf, dF * a_p * G);
     }
@@ -430,7 +433,7 @@ __global__ void k_grad_final(DevPot pot, const SplineGeom *__restrict__ geom, co
   }
   __syncthreads();
   const double *tab = tabs + (size_t)c * stride;
-  if (t == 0 && !pot.omit_pen) {
+  if (t == 0 && !pot.omit_pen && !pot.pair) {
     if (pot.gmeam) {
       for (int f = 0; f < pot.npair; ++f) {
         int at = -1;

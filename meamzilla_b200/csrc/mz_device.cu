@@ -416,6 +416,8 @@ mz_status mz_create(const mz_db *dbh, const mz_pot *poth, const mz_settings *set
                                       " pairs exceeds the kernel limit of " + std::to_string(BLOCK_SLOTS)};
     if (pot.nsplines() > MAX_SPLINES) throw Failure{MZ_ERR_RANGE, "too many splines"};
     const bool meam = style_meam(pot.style);
+    if (style_pair(db.style) != style_pair(pot.style) || (meam && !style_meam(db.style)))
+      throw Failure{MZ_ERR_ARG, "the database's lists were built for another potential style"};
     if (meam)
       for (auto &g : pot.groups[G_G]) {
         if (g.nknots > MAX_G_KNOTS)
@@ -490,9 +492,10 @@ mz_status mz_create(const mz_db *dbh, const mz_pot *poth, const mz_settings *set
     dp.nsplines = ns;
     dp.tab_stride = stride;
     dp.pow_stride = ctx->pstride;
+    dp.pair = style_pair(pot.style) ? 1 : 0;
     dp.s_phi = pot.spline_index(G_PHI, 0);
-    dp.s_rho = pot.spline_index(G_RHO, 0);
-    dp.s_U = pot.spline_index(G_U, 0);
+    dp.s_rho = dp.pair ? 0 : pot.spline_index(G_RHO, 0);
+    dp.s_U = dp.pair ? 0 : pot.spline_index(G_U, 0);
     dp.s_f = meam ? pot.spline_index(G_F, 0) : 0;
     dp.s_g = meam ? pot.spline_index(G_G, 0) : 0;
     dp.embed_extrap = set->embed_extrap;
@@ -502,7 +505,7 @@ mz_status mz_create(const mz_db *dbh, const mz_pot *poth, const mz_settings *set
     dp.gmeam = pot.style == MZ_STYLE_GMEAM_SPLINE;
     dp.npair = pot.ntypes * (pot.ntypes + 1) / 2;
     ctx->npen = style_npen(pot.style, pot.ntypes);
-    ctx->esize = 8 * db.ncells + 3 * db.natoms + ctx->npen;
+    ctx->esize = style_esize(pot.style, pot.ntypes, db.ncells, db.natoms);
 
     // ---- database
     const int N = db.natoms;
@@ -746,6 +749,8 @@ mz_status mz_objective_grad_device(mz_ctx *ctx, int ncand, const double *d_param
 mz_status mz_densities(mz_ctx *ctx, const double *params, double *dens) {
   return guarded([&] {
     if (!ctx || !params || !dens) throw Failure{MZ_ERR_ARG, "bad argument"};
+    if (ctx->pot.pair)  // PotPair has no compute_densities (pot_pair.h:25-42)
+      throw Failure{MZ_ERR_UNSUPPORTED, "pair/spline has no embedding densities"};
     ck(cudaSetDevice(ctx->device), "cudaSetDevice");
     ck(cudaMemcpyAsync(ctx->d_params, params, sizeof(double) * ctx->P, cudaMemcpyHostToDevice, ctx->stream),
        "params H2D");
@@ -878,7 +883,10 @@ extern "C" mz_status mz_objective_noalloc(const mz_db *dbh, const mz_pot *poth, 
     const Pot &pot = poth->pot;
     const bool meam = pot.style == MZ_STYLE_MEAM_SPLINE;
     if (pot.style == MZ_STYLE_GMEAM_SPLINE)
-      throw Failure{MZ_ERR_UNSUPPORTED, "the no-allocation objective supports eam/spline and meam/spline"};
+      throw Failure{MZ_ERR_UNSUPPORTED,
+                    "the no-allocation objective supports eam/spline, meam/spline and pair/spline"};
+    if (style_pair(db.style) != style_pair(pot.style) || (meam && !style_meam(db.style)))
+      throw Failure{MZ_ERR_ARG, "the database's lists were built for another potential style"};
     if (db.max_row > BLOCK_SLOTS)
       throw Failure{MZ_ERR_RANGE, "neighbour row of " + std::to_string(db.max_row) +
                                       " pairs exceeds the kernel limit of " + std::to_string(BLOCK_SLOTS)};
@@ -931,9 +939,10 @@ extern "C" mz_status mz_objective_noalloc(const mz_db *dbh, const mz_pot *poth, 
     dp.nsplines = ns;
     dp.tab_stride = stride;
     dp.pow_stride = pstride;
+    dp.pair = style_pair(pot.style) ? 1 : 0;
     dp.s_phi = pot.spline_index(G_PHI, 0);
-    dp.s_rho = pot.spline_index(G_RHO, 0);
-    dp.s_U = pot.spline_index(G_U, 0);
+    dp.s_rho = dp.pair ? 0 : pot.spline_index(G_RHO, 0);
+    dp.s_U = dp.pair ? 0 : pot.spline_index(G_U, 0);
     dp.s_f = meam ? pot.spline_index(G_F, 0) : 0;
     dp.s_g = meam ? pot.spline_index(G_G, 0) : 0;
     dp.embed_extrap = set->embed_extrap;

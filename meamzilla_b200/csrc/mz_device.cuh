@@ -69,6 +69,8 @@ struct DevPot {
   int omit_pen;       // leave out the style punishments (sharded databases)
   int gmeam;          // g indexed by (i; j, k) types and one f punishment per f spline
   int npair;          // ntypes (ntypes + 1) / 2
+  int pair;           // pair/spline: phi only over each pair once (self images at 1/2),
+                      // no embedding, no constraint or punishment entries
   double energy_weight, stress_weight;
 };
 

@@ -123,6 +123,13 @@ __device__ __forceinline__ int pair_ij_index(int ti, int tj, int nt) {
   return (ti <= tj) ? ti * nt + tj - (ti * (ti + 1)) / 2 : tj * nt + ti - (tj * (tj + 1)) / 2;
 }
 
+// Share of phi(r_p) in atom i's energy and forces: 1/2 in the double-counted
+// lists; in pair/spline's single list 1, or 1/2 for an image of atom i itself
+// (its two images +n and -n are both listed, pot_pair_spline.cpp:106-113).
+__device__ __forceinline__ double phi_share(const DevPot &pot, bool self) {
+  return pot.pair && !self ? 1.0 : 0.5;
+}
+
 // Pair functions of one slot: phi, rho, f with slopes (pot_meam_spline.cpp:152-191).
 template <bool MEAM, typename R>
 struct PairEval {
@@ -389,7 +396,12 @@ __global__ void __launch_bounds__(BLOCK_SLOTS, sizeof(R) == 4 ? 4 : 3)
   for (int a = warp; a < br.na; a += nwarp) {
     double rho;
     warp_slot_sums<1>(red, a_lo[a], a_lo[a + 1], lane, &rho);
-    if (lane == 0) {
+    if (lane == 0 && pot.pair) {
+      double *ao = aout + (size_t)cand * AO_COUNT * N;
+      a_dF[a] = a_U[a] = 0.0;
+      ao[AO_PEN * N + br.atom_lo + a] = 0.0;
+      ao[AO_RHO * N + br.atom_lo + a] = 0.0;
+    } else if (lane == 0) {
       const int ia = br.atom_lo + a;
       const SplineGeom &gU = sg[pot.s_U + db.atom_type[ia]];
       const double w = db.cell_w[db.atom_cell[ia]];
@@ -417,7 +429,8 @@ __global__ void __launch_bounds__(BLOCK_SLOTS, sizeof(R) == 4 ? 4 : 3)
   if (have) {
     const double dF = a_dF[me];
     const double ux = (double)pe.ux, uy = (double)pe.uy, uz = (double)pe.uz;
-    double cu = 0.5 * (double)pe.dphi + (double)pe.drho * dF;
+    const double sp = phi_share(pot, db.pair_nbr[gs] == br.atom_lo + me);
+    double cu = sp * (double)pe.dphi + (double)pe.drho * dF;
     double Vx = 0, Vy = 0, Vz = 0;
     if (MEAM) {
       const double ip = (double)pe.invr, fp = (double)pe.f;
@@ -439,7 +452,7 @@ __global__ void __launch_bounds__(BLOCK_SLOTS, sizeof(R) == 4 ? 4 : 3)
     red[0 * BLOCK_SLOTS + tid] = Vx;
     red[1 * BLOCK_SLOTS + tid] = Vy;
     red[2 * BLOCK_SLOTS + tid] = Vz;
-    red[3 * BLOCK_SLOTS + tid] = 0.5 * (double)pe.phi;
+    red[3 * BLOCK_SLOTS + tid] = sp * (double)pe.phi;
     red[4 * BLOCK_SLOTS + tid] = -(dx * (Vx * rr));
     red[5 * BLOCK_SLOTS + tid] = -(dy * (Vy * rr));
     red[6 * BLOCK_SLOTS + tid] = -(dz * (Vz * rr));
@@ -562,7 +575,7 @@ __global__ void k_cells(DevDb db, DevPot pot, const double *__restrict__ aout, d
       double *e = errvec + (size_t)c * esize + 7 * cell + 3 * a0;
       e[0] = eE;
       for (int q = 0; q < 6; ++q) e[1 + q] = eS[q];
-      errvec[(size_t)c * esize + 7 * db.ncells + 3 * N + cell] = cons;
+      if (!pot.pair) errvec[(size_t)c * esize + 7 * db.ncells + 3 * N + cell] = cons;
     }
     if (energy) energy[(size_t)c * db.ncells + cell] = E;
     if (stress)
@@ -628,7 +641,9 @@ __global__ void k_final(DevDb db, DevPot pot, const SplineGeom *__restrict__ geo
     double total = part[0];
     const double *tab = tabs + (size_t)c * pot.tab_stride;
     double *ev = errvec ? errvec + (size_t)c * esize + 8 * db.ncells + 3 * db.natoms : nullptr;
-    if (pot.omit_pen) {
+    if (pot.pair) {
+      // no punishments (PotPairSpline::fast_compute, pot_pair_spline.cpp:133)
+    } else if (pot.omit_pen) {
       if (ev) {
         const int npen = pot.style == MZ_STYLE_MEAM_SPLINE ? 1 : pot.gmeam ? pot.npair : pot.ntypes;
         for (int q = 0; q < npen; ++q) ev[q] = 0.0;

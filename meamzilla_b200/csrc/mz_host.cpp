@@ -310,9 +310,12 @@ void parse_pot(const std::string &text, Pot &pot) {
   } else if (pot.type_name == "eam/spline") {
     pot.style = MZ_STYLE_EAM_SPLINE;
     nalloy = {npair, nt, nt};
+  } else if (pot.type_name == "pair/spline") {
+    pot.style = MZ_STYLE_PAIR_SPLINE;
+    nalloy = {npair};
   } else {
     fail(MZ_ERR_UNSUPPORTED, "potential style \"" + pot.type_name +
-                                 "\" is not implemented (eam/spline, meam/spline, gmeam/spline)");
+                                 "\" is not implemented (eam/spline, meam/spline, gmeam/spline, pair/spline)");
   }
   pot.ngroups = (int)nalloy.size();
   if (ln >= L.size() || L[ln++].substr(0, 2) != "#P") fail(MZ_ERR_FORMAT, "potential line (#P ...) missing");
@@ -464,7 +467,7 @@ void read_config_file(const std::string &path, int ntypes, std::vector<int> &cel
 int rescale_pot(Pot &pot, const int *atom_type, int natoms, const double *dens, int flag, double factors[2]) {
   // PotMEAM::rescale (pot_meam.cpp:281-375) / PotEAM::rescale (pot_eam.cpp:257-389)
   factors[0] = factors[1] = 0.0;
-  if (flag < 0) return 0;
+  if (flag < 0 || style_pair(pot.style)) return 0;  // PotPair: Potential::rescale (potential.cpp:258-261)
   const bool meam = style_meam(pot.style);
   std::vector<Spline3> &F = pot.groups[G_U];
   const int Fs = (int)F.size();
@@ -595,11 +598,12 @@ void write_data_files(const Db &db, const Pot &pot, double energy_weight, double
   // Potential::write_data (potential.cpp:325-342): .rho (PotEAM::write_densities
   // pot_eam.cpp:506-540), .energy (:497-543), .stress (:548-592), .force
   // (:597-642), .error (:647-708), .punish (PotEAM / PotMEAM::write_punish).
+  // pair/spline writes neither .rho nor .punish (Potential::write_extras and
+  // write_punish do nothing, potential.cpp:713-725).
   const int NC = db.ncells, N = db.natoms;
-  const bool meam = style_meam(pot.style);
-  const int npen = style_npen(pot.style, pot.ntypes);
-  const int esize = 8 * NC + 3 * N + npen;
-  {
+  const bool meam = style_meam(pot.style), pair = style_pair(pot.style);
+  const int esize = style_esize(pot.style, pot.ntypes, NC, N);
+  if (!pair) {
     std::ofstream f = open_out(data_name(prefix, ".rho", num));
     f << std::setw(6) << std::right << "conf:" << std::setw(5) << std::right << "atom" << std::setw(8) << std::right
       << "type" << std::setw(15) << std::right << "rho" << std::endl;
@@ -701,7 +705,7 @@ void write_data_files(const Db &db, const Pot &pot, double energy_weight, double
     f << "Sum of stress errors = " << std::fixed << ss << std::endl;
     if (npunish) f << "Sum of punish errors = " << std::fixed << sp << std::endl;
   }
-  {
+  if (!pair) {
     std::ofstream f = open_out(data_name(prefix, ".punish", num));
     f << "Limiting constraints (atomic density lies inside F boundaries)" << std::endl;
     f << std::setw(3) << std::right << "#" << std::setw(11) << std::right << "conf_w" << std::setw(15) << std::right
@@ -767,6 +771,7 @@ void build_db_setup(const mz_cells_desc &c, const Pot &pot, Db &db) {
   if (c.ncells <= 0 || c.natoms <= 0 || !c.cell_natoms || !c.cell_lattice || !c.atom_type || !c.atom_pos)
     fail(MZ_ERR_ARG, "empty or incomplete cell description");
   const bool meam = style_meam(pot.style);
+  db.style = pot.style;
   db.ncells = c.ncells;
   db.natoms = c.natoms;
   db.cell_atom0.assign(c.ncells + 1, 0);
@@ -840,9 +845,10 @@ void build_incoming(Db &db) {
 
 void build_db(const mz_cells_desc &c, const Pot &pot, Db &db) {
   build_db_setup(c, pot, db);
-  const bool meam = style_meam(pot.style);
+  const bool meam = style_meam(pot.style), half = style_pair(pot.style);
+  const int nq = half ? 1 : meam ? 3 : 2;  // radial functions checked per pair: phi (rho, f)
   const double max_rcut = pot.max_rcut();
-  const int sphi0 = pot.spline_index(G_PHI, 0), srho0 = pot.spline_index(G_RHO, 0);
+  const int sphi0 = pot.spline_index(G_PHI, 0), srho0 = half ? -1 : pot.spline_index(G_RHO, 0);
   const int sf0 = meam ? pot.spline_index(G_F, 0) : -1;
 
   std::vector<CellPairs> per(c.ncells);
@@ -862,12 +868,13 @@ void build_db(const mz_cells_desc &c, const Pot &pot, Db &db) {
       }
       const int sx = sc[0], sy = sc[1], sz = sc[2];
       const int a_lo = db.cell_atom0[ci], na = db.cell_atom0[ci + 1] - a_lo;
-      // Config::find_pairs (config.cpp:143-234), double counted (j0 = 0)
+      // Config::find_pairs (config.cpp:143-234): double counted (j0 = 0), or
+      // for pair/spline each pair once (j0 = the atom's own index)
       for (int i = 0; i < na && out.status == MZ_OK; ++i) {
         const double *pi = c.atom_pos + 3 * (size_t)(a_lo + i);
         const int ti = c.atom_type[a_lo + i];
         int row = 0;
-        for (int j = 0; j < na; ++j) {
+        for (int j = half ? i : 0; j < na; ++j) {
           const double *pj = c.atom_pos + 3 * (size_t)(a_lo + j);
           const int tj = c.atom_type[a_lo + j];
           for (int ix = -sx; ix <= sx; ++ix)
@@ -883,13 +890,14 @@ void build_db(const mz_cells_desc &c, const Pot &pot, Db &db) {
                 // Pair::setup_pair (pair.cpp:35-42)
                 double rr = mag(d);
                 V3 u{d.x / rr, d.y / rr, d.z / rr};
-                // check_pair (pair_meam_spline.cpp:50-99 / pair_eam_spline.cpp:50-86)
+                // check_pair (pair_meam_spline.cpp:50-99 / pair_eam_spline.cpp:50-86 /
+                // pair_pair_spline.cpp:48-72)
                 int sidx[3] = {sphi0 + pot.idx_pair_ij(ti, tj), srho0 + tj,
                                meam ? sf0 + pot.idx_pair_ij(ti, tj) : -1};
                 int kn[3] = {-1, -1, -1};
                 double sh[3] = {0, 0, 0};
                 bool bad = false;
-                for (int q = 0; q < (meam ? 3 : 2); ++q) {
+                for (int q = 0; q < nq; ++q) {
                   const Spline3 &sp = pot.spline(sidx[q]);
                   if (rr < sp.x[0]) {
                     out.status = MZ_ERR_RANGE;
@@ -1103,7 +1111,8 @@ mz_status mz_write_data(const mz_db *db, const mz_pot *pot, double energy_weight
                         const double *errvec, const double *energy, const double *stress, const double *forces,
                         const double *densities, const char *prefix, int num) {
   return guarded([&] {
-    if (!db || !pot || !errvec || !energy || !stress || !forces || !densities || !prefix)
+    if (!db || !pot || !errvec || !energy || !stress || !forces || !prefix ||
+        (!densities && !style_pair(pot->pot.style)))
       fail(MZ_ERR_ARG, "null argument");
     write_data_files(db->db, pot->pot, energy_weight, stress_weight, errvec, energy, stress, forces, densities,
                      prefix, num);
@@ -1170,7 +1179,8 @@ mz_status mz_db_info(const mz_db *db, mz_db_stats *st) {
     st->npairs = db->db.npairs;
     st->ntriplets = db->db.ntriplets;
     st->max_row = db->db.max_row;
-    st->esize = 7 * db->db.ncells + 3 * db->db.natoms + db->db.ncells;  // + style penalties
+    // + the style's punishment entries
+    st->esize = 7 * db->db.ncells + 3 * db->db.natoms + (style_pair(db->db.style) ? 0 : db->db.ncells);
   });
 }
 

@@ -61,9 +61,21 @@ enum Group { G_PHI = 0, G_RHO = 1, G_U = 2, G_F = 3, G_G = 4 };
 // the types of i and of the pair j, k (Triplet_i_jk, pot_fns.cpp:166-168) and
 // punishes every f spline (pot_gmeam_spline.cpp:173-178).
 inline bool style_meam(int style) { return style == MZ_STYLE_MEAM_SPLINE || style == MZ_STYLE_GMEAM_SPLINE; }
+// pair/spline (PotPair, pot_pair.cpp:25-37; PotPairSpline::fast_compute,
+// pot_pair_spline.cpp:71-139): phi only, each pair once (dbl_cnt_pair_ = 0,
+// config.cpp:181-185), no embedding, no constraint or punishment entries.
+inline bool style_pair(int style) { return style == MZ_STYLE_PAIR_SPLINE; }
 // Entries after the per-cell constraints: MEAM 1, GMEAM one per f spline, EAM one per type.
 inline int style_npen(int style, int ntypes) {
-  return style == MZ_STYLE_MEAM_SPLINE ? 1 : style == MZ_STYLE_GMEAM_SPLINE ? ntypes * (ntypes + 1) / 2 : ntypes;
+  return style == MZ_STYLE_MEAM_SPLINE    ? 1
+         : style == MZ_STYLE_GMEAM_SPLINE ? ntypes * (ntypes + 1) / 2
+         : style == MZ_STYLE_PAIR_SPLINE  ? 0
+                                          : ntypes;
+}
+// ErrorVec length: per cell E, 6 S, 3 F per atom (potential.cpp:423-444), the
+// per-cell density constraints of the embedding styles, the punishments.
+inline int style_esize(int style, int ntypes, int ncells, int natoms) {
+  return 7 * ncells + 3 * natoms + (style_pair(style) ? 0 : ncells) + style_npen(style, ntypes);
 }
 
 struct Pot {
@@ -93,6 +105,7 @@ struct Pot {
 // configuration order.  Each atom's neighbour row is the reference's pair
 // list for that atom in the same order (config.cpp:186-228).
 struct Db {
+  int style = -1;  // potential style the lists were built for (pair/spline: each pair once)
   int ncells = 0, natoms = 0;
   int64_t npairs = 0, ntriplets = 0;
   int max_row = 0;

@@ -1,7 +1,8 @@
 // Neighbour lists on the GPU: the periodic-image pair search of
-// Config::find_pairs (config.cpp:143-234, full double-counted list) with the
-// per-pair knot / shift set-up of check_pair (pair_meam_spline.cpp:50-99,
-// pair_eam_spline.cpp:50-86, Spline::get_knotshift spline.cpp:74-99).
+// Config::find_pairs (config.cpp:143-234; the full double-counted list, or
+// each pair once for pair/spline) with the per-pair knot / shift set-up of
+// check_pair (pair_meam_spline.cpp:50-99, pair_eam_spline.cpp:50-86,
+// pair_pair_spline.cpp:48-72, Spline::get_knotshift spline.cpp:74-99).
 //
 // One thread per atom walks its cell's atoms and images in the reference's
 // order (neighbour j, then ix, iy, iz), so every row holds the same pairs in
@@ -26,7 +27,8 @@ namespace {
 
 struct NbrParams {
   int natoms;
-  int meam;
+  int nq;            // radial functions checked per pair: phi (rho, f)
+  int half;          // each pair once: neighbours j >= i of the cell (config.cpp:181-185)
   int ntypes;
   double max_rcut;
   int s[3];          // first spline of phi, rho, f
@@ -83,9 +85,9 @@ __global__ void k_find_pairs(NbrParams p, const int *__restrict__ cell_atom0, co
     const int ti = types[a];
     const double rc = p.max_rcut;
     const double rc2 = rc * rc * (1.0 + 1e-6);  // prefilter only; the test below is the reference's
-    const int nq = p.meam ? 3 : 2;
+    const int nq = p.nq;
     const int64_t o = FILL ? off[a] : 0;
-    for (int j = 0; j < na; ++j) {
+    for (int j = p.half ? i : 0; j < na; ++j) {
       const double *pj = pos + 3 * (size_t)(a_lo + j);
       const double pjx = pj[0], pjy = pj[1], pjz = pj[2];
       const int tj = types[a_lo + j];
@@ -205,11 +207,12 @@ void build_db_device(const mz_cells_desc &c, const Pot &pot, Db &db, int device)
   DevBufs B;
   NbrParams p{};
   p.natoms = N;
-  p.meam = meam ? 1 : 0;
+  p.half = style_pair(pot.style) ? 1 : 0;
+  p.nq = p.half ? 1 : meam ? 3 : 2;
   p.ntypes = pot.ntypes;
   p.max_rcut = max_rcut;
   p.s[0] = pot.spline_index(G_PHI, 0);
-  p.s[1] = pot.spline_index(G_RHO, 0);
+  p.s[1] = p.half ? 0 : pot.spline_index(G_RHO, 0);
   p.s[2] = meam ? pot.spline_index(G_F, 0) : 0;
   p.x = B.upload(xs.data(), xs.size());
   p.xoff = B.upload(xoff.data(), xoff.size());

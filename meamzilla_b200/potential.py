@@ -271,7 +271,8 @@ class Evaluator:
         self.natoms, self.ncells = st["natoms"], st["ncells"]
         self.ncoeff = pot.ncoeff
         self.npen = (1 if pot.style == _lib.MZ_STYLE_MEAM_SPLINE else
-                     pot.ntypes * (pot.ntypes + 1) // 2 if pot.style == _lib.MZ_STYLE_GMEAM_SPLINE else pot.ntypes)
+                     pot.ntypes * (pot.ntypes + 1) // 2 if pot.style == _lib.MZ_STYLE_GMEAM_SPLINE else
+                     0 if pot.style == _lib.MZ_STYLE_PAIR_SPLINE else pot.ntypes)
         self.esize = st["esize_cells"] + self.npen
 
     def __del__(self):
@@ -467,6 +468,8 @@ class Potential:
         called on, so a copy of the potential file is rescaled and this
         object gets its own evaluator when anything changed."""
         ev = self.ev
+        if ev.pot.style == _lib.MZ_STYLE_PAIR_SPLINE:
+            return 0  # Potential::rescale (potential.cpp:258-261)
         dens = ev.densities(self.x)
         pot = ev.pot.copy()
         pot.set_coeffs(self.x)
@@ -493,10 +496,12 @@ class Potential:
 
     def write_data(self, prefix: str, num: int = -1) -> None:
         """Potential::write_data (potential.cpp:325-342): .rho .energy .stress
-        .force .error .punish files from one FP64 evaluation on the GPU."""
+        .force .error .punish files from one FP64 evaluation on the GPU
+        (pair/spline: no .rho or .punish)."""
         ev = self.ev
         out = ev.objective(self.x[None, :], MZ_FP64, errvec=True, forces=True, energy=True, stress=True)
-        dens = np.ascontiguousarray(ev.densities(self.x), dtype=np.float64)
+        dens = (None if ev.pot.style == _lib.MZ_STYLE_PAIR_SPLINE else
+                np.ascontiguousarray(ev.densities(self.x), dtype=np.float64))
         pot = ev.pot.copy()
         pot.set_coeffs(self.x)
         write_data_arrays(ev.db, pot, ev.energy_weight, ev.stress_weight, out["errvec"][0], out["energy"][0],
@@ -546,7 +551,9 @@ def from_param_file(path: str, device: int = 0, max_candidates: int = 1, precisi
 
 def write_data_arrays(db: Database, pot: PotentialFile, energy_weight: float, stress_weight: float, errvec, energy,
                       stress, forces, densities, prefix: str, num: int = -1) -> None:
-    """The reference's data files from evaluated arrays (mz_write_data)."""
-    arrs = [np.ascontiguousarray(a, dtype=np.float64).ravel() for a in (errvec, energy, stress, forces, densities)]
+    """The reference's data files from evaluated arrays (mz_write_data);
+    densities None for pair/spline."""
+    arrs = [None if a is None else np.ascontiguousarray(a, dtype=np.float64).ravel()
+            for a in (errvec, energy, stress, forces, densities)]
     check(lib().mz_write_data(db.handle, pot.handle, float(energy_weight), float(stress_weight),
                               *[ptr(a) for a in arrs], prefix.encode(), int(num)))

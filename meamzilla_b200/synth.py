@@ -109,7 +109,8 @@ def n_alloy(kind: str, ntypes: int, style: str = "meam/spline") -> int:
 
 def teacher_potential(style: str, ntypes: int, rcut: float, seed: int) -> PotSpec:
     rng = np.random.default_rng(seed)
-    kinds = ["phi", "rho", "U"] + (["f", "g"] if style in ("meam/spline", "gmeam/spline") else [])
+    kinds = (["phi"] if style == "pair/spline" else
+             ["phi", "rho", "U"] + (["f", "g"] if style in ("meam/spline", "gmeam/spline") else []))
     groups = []
     for kind in kinds:
         fn, dfn = TEACHER[kind]

@@ -144,20 +144,22 @@ int mzo_ncoeff(const mzo_pot *pot) {
 }
 
 int mzo_esize(const mzo_db *db, const mzo_pot *pot) {
-  /* MEAM: one f punishment; GMEAM: one per f spline (pot_gmeam_spline.cpp:173-178); EAM: one per type */
+  /* MEAM: one f punishment; GMEAM: one per f spline (pot_gmeam_spline.cpp:173-178); EAM: one per type;
+   * pair/spline: neither density constraints nor punishments (pot_pair_spline.cpp:133) */
+  if (pot->style == 3) return 7 * db->ncells + 3 * db->natoms;
   return 8 * db->ncells + 3 * db->natoms +
          (pot->style == 1 ? 1 : pot->style == 2 ? pot->ntypes * (pot->ntypes + 1) / 2 : pot->ntypes);
 }
 
 double mzo_objective(const mzo_db *db, const mzo_pot *pot, const double *coeffs, double *errvec_out,
                      double *forces_out, double *energy_out, double *stress_out, double *dens_out) {
-  const int meam = pot->style == 1 || pot->style == 2, gmeam = pot->style == 2;
+  const int meam = pot->style == 1 || pot->style == 2, gmeam = pot->style == 2, pairpot = pot->style == 3;
   const int nt = pot->ntypes, npair = nt * (nt + 1) / 2;
   const int N = db->natoms, NC = db->ncells;
   int s, ci = 0, i;
   sp_t *sp = (sp_t *)malloc(sizeof(sp_t) * pot->nsplines);
   for (s = 0; s < pot->nsplines; ++s) sp_setup(&sp[s], &pot->splines[s], coeffs, &ci);
-  const sp_t *phi = sp, *rho = sp + npair, *U = sp + npair + nt;
+  const sp_t *phi = sp, *rho = pairpot ? NULL : sp + npair, *U = pairpot ? NULL : sp + npair + nt;
   const sp_t *ff = meam ? sp + npair + 2 * nt : NULL, *gg = meam ? sp + 2 * npair + 2 * nt : NULL;
 
   /* initialize_compute (potential.cpp:388-408) */
@@ -193,9 +195,18 @@ double mzo_objective(const mzo_db *db, const mzo_pot *pot, const double *coeffs,
       const int kphi = db->pair_knot[3 * q], krho = db->pair_knot[3 * q + 1], kf = db->pair_knot[3 * q + 2];
       double *Fj = force + 3 * (size_t)j;
       if (kphi != -1) {
-        double phigrad, tmp[3], tr[3];
-        double phival = 0.5 * sp_comb_k(&phi[pair_ij(nt, ti, tj)], kphi, db->pair_shift[3 * q], &phigrad);
-        phigrad *= 0.5;
+        double phigrad, tmp[3], tr[3], phival;
+        if (pairpot) {
+          /* each pair once; half for an image of atom i itself (pot_pair_spline.cpp:100-113) */
+          phival = sp_comb_k(&phi[pair_ij(nt, ti, tj)], kphi, db->pair_shift[3 * q], &phigrad);
+          if (j == i) {
+            phival *= 0.5;
+            phigrad *= 0.5;
+          }
+        } else {
+          phival = 0.5 * sp_comb_k(&phi[pair_ij(nt, ti, tj)], kphi, db->pair_shift[3 * q], &phigrad);
+          phigrad *= 0.5;
+        }
         energy[cell] += phival;
         tmp[0] = u[0] * phigrad; tmp[1] = u[1] * phigrad; tmp[2] = u[2] * phigrad;
         Fi[0] += tmp[0]; Fi[1] += tmp[1]; Fi[2] += tmp[2];
@@ -205,7 +216,7 @@ double mzo_objective(const mzo_db *db, const mzo_pot *pot, const double *coeffs,
         S[0] -= u[0] * tr[0]; S[1] -= u[1] * tr[1]; S[2] -= u[2] * tr[2];
         S[3] -= u[0] * tr[1]; S[4] -= u[1] * tr[2]; S[5] -= u[2] * tr[0];
       }
-      if (krho != -1) rho_val += sp_comb_k(&rho[tj], krho, db->pair_shift[3 * q + 1], &drho[p]);
+      if (!pairpot && krho != -1) rho_val += sp_comb_k(&rho[tj], krho, db->pair_shift[3 * q + 1], &drho[p]);
       else drho[p] = 0.0;
       if (meam) {
         if (kf != -1) fv[p] = sp_comb_k(&ff[pair_ij(nt, ti, tj)], kf, db->pair_shift[3 * q + 2], &dfv[p]);
@@ -237,6 +248,7 @@ double mzo_objective(const mzo_db *db, const mzo_pot *pot, const double *coeffs,
         }
     }
     if (dens_out) dens_out[i] = rho_val;
+    if (pairpot) continue;
     /* embedding (pot_meam_spline.cpp:208-223) */
     {
       const sp_t *Ui = &U[ti];
@@ -324,12 +336,14 @@ double mzo_objective(const mzo_db *db, const mzo_pot *pot, const double *coeffs,
         ++idx;
       }
   }
-  for (c = 0; c < NC; ++c) {
+  for (c = 0; c < NC && !pairpot; ++c) {
     ev[idx] = constraint[c];
     sum += ev[idx] * ev[idx];
     ++idx;
   }
-  if (gmeam) {
+  if (pairpot) {
+    /* no punishments */
+  } else if (gmeam) {
     /* pot_gmeam_spline.cpp:173-178: one punishment per f spline */
     int f, k;
     for (f = 0; f < npair; ++f) {

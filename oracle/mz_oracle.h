@@ -1,12 +1,14 @@
 /*
  * mz_oracle.h -- TEST ORACLE.  A plain-C, FP64, single-threaded restatement
- * of the reference's objective for the spline EAM/MEAM styles.  It exists to
+ * of the reference's objective for the spline EAM/MEAM/GMEAM/pair styles.  It exists to
  * check the CUDA evaluator: only tests, the smoke check and the benchmark's
  * CPU-baseline leg call it.  The product never links it.
  *
  * It follows the reference loop by loop, in the reference's own order:
  *   PotMEAMSpline::fast_compute   src/pots/pot_meam_spline/pot_meam_spline.cpp:102-283
  *   PotEAMSpline::fast_compute    src/pots/pot_eam_spline/pot_eam_spline.cpp:100-223
+ *   PotGMEAMSpline::fast_compute  src/pots/pot_gmeam_spline/pot_gmeam_spline.cpp:103-290
+ *   PotPairSpline::fast_compute   src/pots/pot_pair_spline/pot_pair_spline.cpp:71-139
  *   Potential::accumulate_error   src/potential.cpp:415-491
  *   Spline3Eq::refresh_basis      src/spline3eq.cpp:192-225
  *   Spline3Eq::splint_comb        src/spline3eq.h:110-122, 204-236
@@ -37,7 +39,7 @@ typedef struct {
 } mzo_spline;
 
 typedef struct {
-  int style;     /* 0 eam/spline, 1 meam/spline */
+  int style;     /* 0 eam/spline, 1 meam/spline, 2 gmeam/spline, 3 pair/spline */
   int ntypes;
   int nsplines;  /* group-major: phi, rho, U [, f, g] */
   const mzo_spline *splines;

@@ -10,7 +10,7 @@ through Potential::compute for two coefficient vectors:
     fdgrad (central differences of the objective, h = 1e-6; small cases)
 
 Run here (needs the reference sources to build mzref):
-    make -C oracle && python tests/golden/make_golden.py [--gmeam | --grad10]
+    make -C oracle && python tests/golden/make_golden.py [--gmeam | --grad10 | --pair]
 """
 from __future__ import annotations
 
@@ -93,21 +93,47 @@ def gmeam_goldens():
     _write("gmeam_inrange1", in_range_meam(pot), cells, fd=True, energy_weight=1.5, stress_weight=0.5)
 
 
-def data_goldens():
+def pair_goldens():
+    """pair/spline: phi only, each pair once, self images at one half."""
+    # 8. one species: three bcc cells of the eam54 rules and a one-atom cell
+    #    whose only neighbours are its own images
+    _, cells = synth.make_workload("eam54", seed=13, ncells=3)
+    cells.append(synth.Cell(lattice=np.diag([2.9, 3.1, 3.3]), types=np.zeros(1, dtype=np.int64),
+                            pos=np.array([[0.1, 0.2, 0.3]]), force0=np.zeros((1, 3))))
+    _targets(cells, 8)
+    pot = synth.teacher_potential("pair/spline", 1, 5.0, seed=23)
+    _write("pair_bcc1", pot, cells, fd=True)
+    # 9. two species, cells of the two-species rule; phi_AB's grid ends at
+    #    4.6 A, so A-B pairs between 4.6 and 5.5 A are not in the list
+    #    (check_pair drops them), phi_BB has a natural left end and two fixed knots
+    _, cells = synth.make_workload("meam2k", seed=14, ncells=4)
+    cells = [c for c in cells if c.natoms <= 300][:3] or cells[:1]
+    _targets(cells, 9)
+    pot = synth.teacher_potential("pair/spline", 2, 5.5, seed=24)
+    ab = pot.groups[0][1]
+    pot.groups[0][1] = synth.Spline(1.8, 4.6, np.interp(np.linspace(1.8, 4.6, 10), np.linspace(1.8, 5.5, 10), ab.y),
+                                    ab.grad.copy())
+    pot.groups[0][2].bc = (-1, 0)
+    pot.groups[0][2].fixed = np.zeros(10, dtype=int)
+    pot.groups[0][2].fixed[[2, 7]] = 1
+    _write("pair_mix2", pot, cells, fd=True, energy_weight=2.0, stress_weight=0.5)
+
+
+def data_goldens(names=None):
     """ref.{rho,energy,stress,force,error,punish}: the text files the
     reference's Potential::write_data writes for the start potential."""
-    for name in sorted(os.listdir(HERE)):
+    for name in sorted(names or os.listdir(HERE)):
         d = os.path.join(HERE, name)
         if os.path.isfile(os.path.join(d, "param")):
             oracle.run_reference("param", cwd=d, write_prefix=os.path.join(d, "ref"))
             print(name, "data files written")
 
 
-def rescale_goldens():
+def rescale_goldens(names=None):
     """rescale.npz of every case: the reference's Potential::rescale with
     flag 0 (when needed) and 1 (always), run on the start potential, dumped
     spline by spline by the harness (oracle/ref_harness.cpp -rescale)."""
-    for name in sorted(os.listdir(HERE)):
+    for name in sorted(names or os.listdir(HERE)):
         d = os.path.join(HERE, name)
         if not os.path.isfile(os.path.join(d, "param")):
             continue
@@ -208,6 +234,11 @@ if __name__ == "__main__":
     import sys
     if "--grad10" in sys.argv:
         grad10_goldens()
+        sys.exit(0)
+    if "--pair" in sys.argv:
+        pair_goldens()
+        rescale_goldens(["pair_bcc1", "pair_mix2"])
+        data_goldens(["pair_bcc1", "pair_mix2"])
         sys.exit(0)
     if "--gmeam" in sys.argv:
         gmeam_goldens()

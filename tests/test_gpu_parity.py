@@ -156,7 +156,7 @@ def test_tensor_core_forward_opt_in(name, monkeypatch):
         assert np.max(np.abs(b["forces"][c] - a["forces"][c])) <= 5e-5
 
 
-@pytest.mark.parametrize("name", ["meam_mix6", "eam_bcc3"])
+@pytest.mark.parametrize("name", ["meam_mix6", "eam_bcc3", "pair_bcc1"])
 def test_rescale_then_objective_matches_reference(name):
     """Potential.rescale on the GPU densities, then the objective of the
     rescaled potential, against the reference's rescale + compute."""
@@ -166,7 +166,7 @@ def test_rescale_then_objective_matches_reference(name):
     p = Potential(ev, precision=MZ_FP64)
     ref = np.load(os.path.join(case["dir"], "rescale.npz"))
     assert p.rescale(1) == int(ref["flag1"][0])
-    assert p.ev is not ev and ev.pot.coeffs().size == case["pot"].ncoeff
+    assert (p.ev is not ev) == bool(ref["flag1"][0]) and ev.pot.coeffs().size == case["pot"].ncoeff
     assert rel(p.compute(), float(ref["obj1"])) <= 1e-12
 
 
@@ -180,7 +180,7 @@ def _same_layout(ours: str, ref: str):
         assert re.sub(r"[0-9]", "0", x) == re.sub(r"[0-9]", "0", y), (x, y)
 
 
-@pytest.mark.parametrize("name", ["meam_mix6", "eam_bcc3", "meam2_edge"])
+@pytest.mark.parametrize("name", ["meam_mix6", "eam_bcc3", "meam2_edge", "pair_mix2"])
 def test_write_data_from_gpu_matches_reference_files(name, tmp_path):
     """Potential.write_data evaluates on the GPU (FP64) and writes the
     reference's data files: the same layout as the reference's files, and the
@@ -192,8 +192,11 @@ def test_write_data_from_gpu_matches_reference_files(name, tmp_path):
     prefix = str(tmp_path / "out")
     Potential(ev, precision=MZ_FP64).write_data(prefix)
     for ext in ("rho", "energy", "stress", "force", "error", "punish"):
-        with open(prefix + "." + ext) as a, open(os.path.join(case["dir"], "ref." + ext)) as b:
-            _same_layout(a.read(), b.read())
+        ref = os.path.join(case["dir"], "ref." + ext)
+        assert os.path.exists(prefix + "." + ext) == os.path.exists(ref), ext
+        if os.path.exists(ref):
+            with open(prefix + "." + ext) as a, open(ref) as b:
+                _same_layout(a.read(), b.read())
     with open(prefix + ".error") as a, open(os.path.join(case["dir"], "ref.error")) as b:
         for x, y in zip(a.read().splitlines()[1:], b.read().splitlines()[1:]):  # the four sums
             assert rel(float(x.split("=")[1]), float(y.split("=")[1])) <= 1e-10

@@ -102,7 +102,7 @@ def test_missing_files_are_io_errors(tmp_path):
 @pytest.mark.parametrize("text,status,phrase", [
     ("comment\n#X eam/spline 1\n", 3, "#T"),
     ("comment\n#T eam/spline 1\n#B spline3eq\n", 3, "#P"),
-    ("comment\n#T pair/spline 1\n#P\n", 5, "not implemented"),
+    ("comment\n#T jmeam/spline 1\n#P\n", 5, "not implemented"),
     ("comment\n#T eam/spline 1\n#P\n#B spline5eq\n1 2 3\n", 5, "spline5eq"),
     ("comment\n#T eam/spline 1\n#P\n#B spline3eq\n1.8 5.0 10\n0 7\n1 1\n0 1\n", 3, "constraint"),
     ("comment\n#T eam/spline 1\n#P\n#B spline3eq\n1.8 5.0 4\n0 0\n1 1\n0 1\n0 x\n", 3, "knot line"),
@@ -140,6 +140,40 @@ def test_pair_shorter_than_first_knot_is_range_error(tmp_path):
     body = "#N 2 1\n#X 8 0 0\n#Y 0 8 0\n#Z 0 0 8\n#F\n0 0 0 0 0 0 0\n0 1.5 0 0 0 0 0\n"
     st, msg = _status(Database.read, _conf(tmp_path, body), pot)
     assert st == 4 and "too short" in msg
+
+
+def test_pair_spline_lists_hold_each_pair_once():
+    """pair/spline lists every pair once (dbl_cnt_pair_ = 0, config.cpp:181-185):
+    for atom i of a cell the neighbours j >= i, the atom's own images
+    included; the double-counted list of the same cells holds every other
+    pair twice.  A database built for one kind of list is refused by an
+    evaluator of the other kind."""
+    from meamzilla_b200 import synth
+    from meamzilla_b200._lib import MzError
+    from meamzilla_b200.potential import Database, Evaluator, PotentialFile
+    case = load_case("pair_bcc1")
+    half = case["db"].view()
+    eam = PotentialFile.from_spec(synth.teacher_potential("eam/spline", 1, 5.0, seed=1))
+    full = Database.read(os.path.join(case["dir"], "db.conf"), eam).view()
+    a0 = half["cell_atom0"]
+
+    def pairs(v):
+        out = []
+        for i in range(v["natoms"]):
+            for s in range(v["pair_off"][i], v["pair_off"][i + 1]):
+                out.append((i, int(v["pair_nbr"][s]), round(float(v["pair_r"][s]), 9)))
+        return out
+
+    h, f = pairs(half), pairs(full)
+    assert all(j >= i for i, j, _ in h)
+    self_h = sorted(p for p in h if p[0] == p[1])
+    other_h = sorted(p for p in h if p[0] != p[1])
+    assert self_h == sorted(p for p in f if p[0] == p[1])
+    assert len(f) == len(self_h) + 2 * len(other_h)
+    assert a0[-1] == half["natoms"]
+    with pytest.raises(MzError) as e:
+        Evaluator(case["db"], eam)
+    assert "another potential style" in str(e.value)
 
 
 def test_read_param_first_key_wins(tmp_path):

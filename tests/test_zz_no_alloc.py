@@ -36,7 +36,7 @@ def _noalloc(case, x):
     return obj[0], forces
 
 
-@pytest.mark.parametrize("name", ["meam_mix6", "meam2_edge", "eam_bcc3"])
+@pytest.mark.parametrize("name", ["meam_mix6", "meam2_edge", "eam_bcc3", "pair_bcc1"])
 def test_noalloc_matches_objective_two_calls(name):
     from meamzilla_b200.potential import MZ_FP64, Evaluator
     case = load_case(name)
