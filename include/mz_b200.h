@@ -59,7 +59,14 @@ enum {
 };
 
 /* potential styles (the #T string of the potential file) */
-enum { MZ_STYLE_EAM_SPLINE = 0, MZ_STYLE_MEAM_SPLINE = 1, MZ_STYLE_GMEAM_SPLINE = 2, MZ_STYLE_PAIR_SPLINE = 3 };
+enum {
+  MZ_STYLE_EAM_SPLINE = 0,
+  MZ_STYLE_MEAM_SPLINE = 1,
+  MZ_STYLE_GMEAM_SPLINE = 2,
+  MZ_STYLE_PAIR_SPLINE = 3,
+  MZ_STYLE_JMEAM_SPLINE = 4,   /* MEAM + sum p_ij p_ik q(cos) in the energy             */
+  MZ_STYLE_JMEAM2_SPLINE = 5   /* MEAM + two such terms (p, q) and (p2, q2)             */
+};
 
 typedef struct mz_pot mz_pot;  /* a potential: splines + parameter layout        */
 typedef struct mz_db mz_db;    /* configuration database + neighbour lists       */
@@ -72,8 +79,8 @@ const char *mz_last_error(void);
 
 /* Read a potential file (first #P block).  Replaces PotList::init
  * (src/pot_list.cpp:84-177) + Potential::read_pot (potential.cpp:153-161)
- * for the eam/spline, meam/spline, gmeam/spline and pair/spline styles with
- * spline3eq bases. */
+ * for the eam/spline, meam/spline, gmeam/spline, jmeam/spline, jmeam2/spline and
+ * pair/spline styles with spline3eq bases. */
 mz_status mz_pot_read(const char *path, mz_pot **out);
 /* Same from the file's text held in memory. */
 mz_status mz_pot_parse(const char *text, mz_pot **out);
@@ -101,7 +108,8 @@ mz_status mz_pot_spline_eval(const mz_pot *pot, int spline, double x, double *va
  * per-atom densities of the potential's current coefficients (mz_densities)
  * and the database's atom types drive it; flag as the reference's (< 0
  * never, 0 when needed, 1 always).  *rescaled = the reference's return value;
- * factors[0] = embedding scale a, factors[1] = MEAM f scale b (0 if unused).
+ * factors[4]: embedding scale a, MEAM f scale b, JMEAM p and p2 scales
+ * (0 where unused).
  * U's knot grid changes, so evaluators must be re-created afterwards.
  * pair/spline never rescales (Potential::rescale, potential.cpp:258-261). */
 mz_status mz_pot_rescale(mz_pot *pot, const mz_db *db, const double *densities, int flag, int *rescaled,
@@ -165,16 +173,18 @@ typedef struct {
   int esize;            /* residual entries of the cells: 8 ncells + 3    */
                         /* natoms, 7 ncells + 3 natoms for pair/spline    */
                         /* (the style penalties add 1 for MEAM, ntypes    */
-                        /* for EAM, one per f spline for GMEAM)           */
+                        /* for EAM, one per f spline for GMEAM, 2 / 3 for */
+                        /* JMEAM / JMEAM2)                                */
 } mz_db_stats;
 mz_status mz_db_info(const mz_db *db, mz_db_stats *stats);
 
 /* Read-only view of the built database (pointers into the mz_db, valid
  * until mz_db_free).  Pair data of atom i occupy slots
  * [pair_off[i], pair_off[i+1]) in the reference's pair order; pair_knot and
- * pair_shift hold (phi, rho, f) per slot, knot -1 where the reference's is
- * -1 (f unused for EAM).  in_off/in_slot list, per atom, the slots whose
- * neighbour it is. */
+ * pair_shift hold nfun values per slot -- phi, rho, f (+ p for jmeam/spline,
+ * + p, p2 for jmeam2/spline) -- knot -1 where the reference's is -1 (f unused
+ * for EAM, rho and f for pair/spline).  in_off/in_slot list, per atom, the
+ * slots whose neighbour it is. */
 typedef struct {
   int ncells, natoms;
   int64_t npairs;
@@ -187,9 +197,10 @@ typedef struct {
   const int64_t *pair_off;               /* [natoms+1] */
   const int *pair_nbr;
   const double *pair_r, *pair_u;         /* u: [npairs][3] */
-  const int8_t *pair_knot;               /* [npairs][3] */
-  const double *pair_shift;              /* [npairs][3] */
+  const int8_t *pair_knot;               /* [npairs][nfun] */
+  const double *pair_shift;              /* [npairs][nfun] */
   const int64_t *in_off, *in_slot;
+  int nfun;                              /* radial functions per slot: 3, 4 or 5 */
 } mz_db_view;
 mz_status mz_db_get_view(const mz_db *db, mz_db_view *view);
 

@@ -21,6 +21,8 @@ MZ_STYLE_EAM_SPLINE = 0
 MZ_STYLE_MEAM_SPLINE = 1
 MZ_STYLE_GMEAM_SPLINE = 2
 MZ_STYLE_PAIR_SPLINE = 3
+MZ_STYLE_JMEAM_SPLINE = 4
+MZ_STYLE_JMEAM2_SPLINE = 5
 
 STATUS_NAMES = {
     0: "MZ_OK", 1: "MZ_ERR_ARG", 2: "MZ_ERR_IO", 3: "MZ_ERR_FORMAT", 4: "MZ_ERR_RANGE",
@@ -64,6 +66,7 @@ class DbView(C.Structure):
         ("pair_r", C.POINTER(C.c_double)), ("pair_u", C.POINTER(C.c_double)),
         ("pair_knot", C.POINTER(C.c_int8)), ("pair_shift", C.POINTER(C.c_double)),
         ("in_off", C.POINTER(C.c_int64)), ("in_slot", C.POINTER(C.c_int64)),
+        ("nfun", C.c_int),
     ]
 
 

@@ -13,6 +13,9 @@
 // so one more pass over each row (for d K / d f and the g table) is all the
 // adjoint needs; G, H and vk come from the forward pass.  Densities and
 // embedding derivatives are recomputed, nothing per triplet is stored.
+// JMEAM's terms sum p_j p_k q(cos) enter E_i directly and V_p without U':
+// each is the g channel with (chi, U', f, g) replaced by (eps, 1, p, q) and
+// runs as one more pass over the row with the same shared-memory rows.
 #pragma once
 
 #include "mz_fwd.cuh"
@@ -69,8 +72,8 @@ __host__ __device__ inline size_t adj_smem_bytes(int nsplines, int stride, int p
   return b;
 }
 
-template <bool MEAM, typename R, bool GM = false>
-__global__ void __launch_bounds__(BLOCK_SLOTS, sizeof(R) == 4 ? 3 : 2)
+template <bool MEAM, typename R, bool GM = false, bool JM = false>
+__global__ void __launch_bounds__(BLOCK_SLOTS, JM ? 2 : sizeof(R) == 4 ? 3 : 2)
     k_adj(DevDb db, DevPot pot, const SplineGeom *__restrict__ geom, const double *__restrict__ tabs,
           const double *__restrict__ ptabs, const double *__restrict__ aout, const double *__restrict__ aux,
           const double *__restrict__ lam, const double *__restrict__ seeds, double *__restrict__ partial) {
@@ -123,14 +126,14 @@ __global__ void __launch_bounds__(BLOCK_SLOTS, sizeof(R) == 4 ? 3 : 2)
   auto add_f = [&](int idx, double v) { atomicAdd(ft + idx, (float)v); };
 
   const double *ao = aout + (size_t)cand * AO_COUNT * N;
-  const double *ax = aux + (size_t)cand * AUX_COUNT * Np;
+  const double *ax = aux + (size_t)cand * (JM ? pot.aux_rows : (int)AUX_COUNT) * Np;
   const double *L = lam + (size_t)cand * 3 * N;
   const double *sd = seeds + (size_t)cand * CS_COUNT * NC;
 
   // Flush of the per-thread g table of type t (power basis) into the warp's
   // FP64 table: one warp-wide sum per (interval, coefficient).
-  auto flush_gacc = [&](int t) {
-    const SplineGeom &gg = sg[pot.s_g + t];
+  auto flush_gacc_spline = [&](int s) {
+    const SplineGeom &gg = sg[s];
     for (int m = 0; m < gg.n - 1; ++m) {
       const R4 v = gacc[m * BLOCK_SLOTS + tid];
       double d[4] = {(double)v.x, (double)v.y, (double)v.z, (double)v.w};
@@ -142,6 +145,7 @@ __global__ void __launch_bounds__(BLOCK_SLOTS, sizeof(R) == 4 ? 3 : 2)
     }
     for (int m = 0; m < nint; ++m) gacc[m * BLOCK_SLOTS + tid] = R4{};
   };
+  auto flush_gacc = [&](int t) { flush_gacc_spline(pot.s_g + t); };
   // GMEAM: this thread's table tk holds triplets (i; j, k) with j its slot's
   // neighbour type (tj_mine) and k of type tk, i.e. g spline (t; tj_mine, tk).
   auto flush_gacc_gm = [&](int t, bool have_t, int tj_mine) {
@@ -382,10 +386,92 @@ __global__ void __launch_bounds__(BLOCK_SLOTS, sizeof(R) == 4 ? 3 : 2)
         add_f(g.toff + g.n + k + 1, cv * w.wB + cd * w.dB);
       };
       const double eps = sd[CS_EPS * NC + cell];
-      const double sp = phi_share(pot, db.pair_nbr[gs] == ia);
+      const double sp = MEAM ? 0.5 : phi_share(pot, db.pair_nbr[gs] == ia);
       if (pe.kphi >= 0) pair_adj(pot.s_phi + pe.pij, pe.kphi, pe.bphi, sp * eps, sp * a_p);
       if (pe.krho >= 0) pair_adj(pot.s_rho + pe.tj, pe.krho, pe.brho, chi, dF * a_p);
       if (MEAM && pe.kf >= 0) pair_adj(pot.s_f + pe.pij, pe.kf, pe.bf, chi * G + dF * dKdf, dF * a_p * G);
+    }
+    if (JM) {
+      // ---- JMEAM (p, q) terms: the per-thread tables hold this block's g
+      // gradients; flush them, then one pass per term with the rows of p
+      flush_gacc(tab_t);
+      since_flush = 0;
+      if (have) eval_pair_p<MEAM, R>(db, pot, sg, ptab, gs, pe);
+      const double eps = sd[CS_EPS * NC + cell];
+      for (int ch = 0; ch < pot.nj; ++ch) {
+        const double *axm = ax + (size_t)AUX_COUNT * (1 + ch) * Np;
+        double G2 = 0, H2 = 0, J2 = 0;
+        const double pm = have ? (double)pe.p[ch] : 0.0, ip = have ? (double)pe.invr : 0.0;
+        __syncthreads();  // every thread is done with the previous rows
+        if (have) {
+          G2 = axm[AUX_G * Np + gs];
+          H2 = axm[AUX_H * Np + gs];
+          J2 = Lx * axm[AUX_VX * Np + gs] + Ly * axm[AUX_VY * Np + gs] + Lz * axm[AUX_VZ * Np + gs];
+          R4 v;
+          v.x = pe.ux; v.y = pe.uy; v.z = pe.uz; v.w = pe.p[ch];
+          srow[tid] = v;
+          R4 q;
+          q.x = (R)(a_p * (double)pe.dp[ch]);
+          q.y = (R)(a_p * pm * ip);
+          q.z = (R)(pm * ip * Lx);
+          q.w = (R)(pm * ip * Ly);
+          sadj[tid] = q;
+          sqz[tid] = (R)(pm * ip * Lz);
+        }
+        __syncthreads();
+        const SplineGeom qg = sg[pot.s_q[ch] + ti];
+        if (have) {
+          const R *qpc = ptab + qg.poff;
+          const R qx0 = (R)qg.x0, qinv = (R)qg.invstep, qcut = g_cut<R>(qg);
+          const R gam = (R)(0.5 * eps * pm + a_p * (double)pe.dp[ch]);
+          const R del = (R)(pm * ip);
+          const R lx = (R)Lx, ly = (R)Ly, lz = (R)Lz, ap = (R)a_p;
+          R4 *ga = gacc + tid;
+          const int row_lo = a_lo[me], row_hi = a_lo[me + 1];
+          double dKdp = 0.0;
+          for (int kb = row_lo; kb < row_hi; kb += 8) {
+            R dk8 = 0;
+#pragma unroll
+            for (int u = 0; u < 8; ++u) {
+              const int k = kb + u;
+              const R4 o = srow[k];
+              const R4 q = sadj[k];
+              const R cs = cos_dot(pe.ux, pe.uy, pe.uz, o.x, o.y, o.z);
+              const bool ok = (k < row_hi) && (k != tid) && (cs < qcut);
+              const R wk = ok ? R(1) : R(0);
+              R b;
+              const int m = g_knot<R>(cs, qx0, qinv, qg.n, b);
+              R dq;
+              const R qv = cubic_val_grad<R>(qpc, m, b, qinv, dq);
+              const R qu = q.z * pe.ux + q.w * pe.uy + sqz[k] * pe.uz;
+              dk8 += wk * (q.x * qv - q.y * dq * cs + dq * qu);
+              const R bpk = lx * o.x + ly * o.y + lz * o.z;
+              const R pk = wk * o.w;
+              const R cg = pk * gam;
+              const R cs1 = pk * del * (bpk - ap * cs) * qinv;
+              const R b2 = b * b;
+              R4 d = ga[m * BLOCK_SLOTS];
+              d.x += cg;
+              d.y += cg * b + cs1;
+              d.z += cg * b2 + R(2) * cs1 * b;
+              d.w += cg * b2 * b + R(3) * cs1 * b2;
+              ga[m * BLOCK_SLOTS] = d;
+            }
+            dKdp += (double)dk8;
+          }
+          dKdp += ip * (J2 - a_p * H2);
+          if (pe.kp[ch] >= 0) {
+            const SplineGeom &g = sg[pot.s_p[ch] + pe.pij];
+            const SplW<double> w = spl_weights<double>((double)pe.bp[ch], g.step, g.invstep);
+            const double cv = eps * G2 + dKdp, cd = a_p * G2;
+            add_f(g.toff + pe.kp[ch], cv * w.wa + cd * w.da);
+            add_f(g.toff + pe.kp[ch] + 1, cv * w.wb + cd * w.db);
+            add_f(g.toff + g.n + pe.kp[ch], cv * w.wA + cd * w.dA);
+            add_f(g.toff + g.n + pe.kp[ch] + 1, cv * w.wB + cd * w.dB);
+          }
+        }
+        flush_gacc_spline(pot.s_q[ch] + ti);
+      }
     }
     __syncwarp();
     // the block's FP32 pair-function sums into the warp's FP64 table
@@ -442,12 +528,14 @@ __global__ void k_grad_final(DevPot pot, const SplineGeom *__restrict__ geom, co
         const double fe = 100. * 25. * (1.0 - m) * (1.0 - m);
         if (at >= 0) ext[at] += 2.0 * fe * (-5000.0) * (1.0 - m) * (my > 0 ? 1.0 : (my < 0 ? -1.0 : 0.0));
       }
-    } else if (pot.style == MZ_STYLE_MEAM_SPLINE) {
-      int at = -1;
-      const double my = f_max_y(pot, geom, tab, &at);
-      const double m = fabs(my);
-      const double fe = 100. * 25. * (1.0 - m) * (1.0 - m);
-      if (at >= 0) ext[at] += 2.0 * fe * (-5000.0) * (1.0 - m) * (my > 0 ? 1.0 : (my < 0 ? -1.0 : 0.0));
+    } else if (pot.style == MZ_STYLE_MEAM_SPLINE || pot.nj > 0) {
+      for (int q = 0; q <= pot.nj; ++q) {  // f, then JMEAM's p (p2)
+        int at = -1;
+        const double my = group_max_y(pot, q == 0 ? pot.s_f : pot.s_p[q - 1], geom, tab, &at);
+        const double m = fabs(my);
+        const double fe = 100. * 25. * (1.0 - m) * (1.0 - m);
+        if (at >= 0) ext[at] += 2.0 * fe * (-5000.0) * (1.0 - m) * (my > 0 ? 1.0 : (my < 0 ? -1.0 : 0.0));
+      }
     } else {
       for (int ty = 0; ty < pot.ntypes; ++ty) {
         const SplineGeom &g = geom[pot.s_U + ty];

@@ -182,6 +182,13 @@ struct Bracket {
 template <bool MEAM, typename R, bool AUX>
 void launch_atoms(mz_ctx *ctx, int n, size_t smem) {
   dim3 ga(ctx->db.nblocks, n);
+  if constexpr (MEAM) {
+    if (ctx->pot.nj > 0) {
+      k_atoms<MEAM, R, AUX, false, true><<<ga, BLOCK_SLOTS, smem, ctx->stream>>>(
+          ctx->db, ctx->pot, ctx->d_geom, ctx->d_tabs, ctx->d_ptabs, ctx->d_V, ctx->d_aout, ctx->d_aux);
+      return;
+    }
+  }
   if (MEAM && ctx->pot.gmeam)
     k_atoms<MEAM, R, AUX, true><<<ga, BLOCK_SLOTS, smem, ctx->stream>>>(ctx->db, ctx->pot, ctx->d_geom, ctx->d_tabs,
                                                                        ctx->d_ptabs, ctx->d_V, ctx->d_aout,
@@ -194,6 +201,14 @@ void launch_atoms(mz_ctx *ctx, int n, size_t smem) {
 template <bool MEAM, typename R>
 void launch_adj(mz_ctx *ctx, int n, size_t smem) {
   dim3 ga(ctx->adj_ctas, n);
+  if constexpr (MEAM) {
+    if (ctx->pot.nj > 0) {
+      k_adj<MEAM, R, false, true><<<ga, BLOCK_SLOTS, smem, ctx->stream>>>(
+          ctx->db, ctx->pot, ctx->d_geom, ctx->d_tabs, ctx->d_ptabs, ctx->d_aout, ctx->d_aux, ctx->d_lam,
+          ctx->d_seeds, ctx->d_partial);
+      return;
+    }
+  }
   if (MEAM && ctx->pot.gmeam)
     k_adj<MEAM, R, true><<<ga, BLOCK_SLOTS, smem, ctx->stream>>>(ctx->db, ctx->pot, ctx->d_geom, ctx->d_tabs,
                                                                   ctx->d_ptabs, ctx->d_aout, ctx->d_aux, ctx->d_lam,
@@ -419,10 +434,12 @@ mz_status mz_create(const mz_db *dbh, const mz_pot *poth, const mz_settings *set
     if (style_pair(db.style) != style_pair(pot.style) || (meam && !style_meam(db.style)))
       throw Failure{MZ_ERR_ARG, "the database's lists were built for another potential style"};
     if (meam)
-      for (auto &g : pot.groups[G_G]) {
-        if (g.nknots > MAX_G_KNOTS)
-          throw Failure{MZ_ERR_RANGE, "g spline with more than " + std::to_string(MAX_G_KNOTS) + " knots"};
-      }
+      for (int gi : {(int)G_G, (int)G_Q1, (int)G_Q2})
+        if (gi < (int)pot.groups.size())
+          for (auto &g : pot.groups[gi]) {
+            if (g.nknots > MAX_G_KNOTS)
+              throw Failure{MZ_ERR_RANGE, "angular spline with more than " + std::to_string(MAX_G_KNOTS) + " knots"};
+          }
     ctx = new mz_ctx;
     ctx->device = set->device;
     ck(cudaSetDevice(ctx->device), "cudaSetDevice");
@@ -504,6 +521,12 @@ mz_status mz_create(const mz_db *dbh, const mz_pot *poth, const mz_settings *set
     dp.omit_pen = set->omit_punishments;
     dp.gmeam = pot.style == MZ_STYLE_GMEAM_SPLINE;
     dp.npair = pot.ntypes * (pot.ntypes + 1) / 2;
+    dp.nj = style_nj(pot.style);
+    for (int m = 0; m < 2; ++m) {
+      dp.s_p[m] = m < dp.nj ? pot.spline_index(m == 0 ? G_P1 : G_P2, 0) : 0;
+      dp.s_q[m] = m < dp.nj ? pot.spline_index(m == 0 ? G_Q1 : G_Q2, 0) : 0;
+    }
+    dp.aux_rows = AUX_COUNT * (1 + dp.nj);
     ctx->npen = style_npen(pot.style, pot.ntypes);
     ctx->esize = style_esize(pot.style, pot.ntypes, db.ncells, db.natoms);
 
@@ -524,24 +547,28 @@ mz_status mz_create(const mz_db *dbh, const mz_pot *poth, const mz_settings *set
     d.atom_type = dupload(ctx, db.atom_type.data(), db.atom_type.size());
     d.atom_cell = dupload(ctx, db.atom_cell.data(), db.atom_cell.size());
     d.force0 = dupload(ctx, db.atom_force0.data(), db.atom_force0.size());
+    const int nf = db.nfun;
     std::vector<int> off32(N + 1), inoff32(N + 1), inslot32(Np), knot32(Np);
+    std::vector<signed char> knotp2(nf > 4 ? Np : 0);
     for (int i = 0; i <= N; ++i) {
       off32[i] = (int)db.pair_off[i];
       inoff32[i] = (int)db.in_off[i];
     }
     for (int64_t s = 0; s < Np; ++s) {
       inslot32[s] = (int)db.in_slot[s];
-      knot32[s] = (db.pair_knot[3 * s] + 1) | ((db.pair_knot[3 * s + 1] + 1) << 8) |
-                  ((db.pair_knot[3 * s + 2] + 1) << 16);
+      knot32[s] = (db.pair_knot[nf * s] + 1) | ((db.pair_knot[nf * s + 1] + 1) << 8) |
+                  ((db.pair_knot[nf * s + 2] + 1) << 16) | (nf > 3 ? (db.pair_knot[nf * s + 3] + 1) << 24 : 0);
+      if (nf > 4) knotp2[s] = db.pair_knot[nf * s + 4];
     }
+    d.pair_knot_p2 = nf > 4 ? dupload(ctx, knotp2.data(), knotp2.size()) : nullptr;
     d.pair_off = dupload(ctx, off32.data(), off32.size());
     d.in_off = dupload(ctx, inoff32.data(), inoff32.size());
     d.in_slot = dupload(ctx, inslot32.data(), inslot32.size());
     d.pair_knot = dupload(ctx, knot32.data(), knot32.size());
     d.pair_nbr = dupload(ctx, db.pair_nbr.data(), db.pair_nbr.size());
     {
-      std::vector<double> ux(Np), uy(Np), uz(Np), sh(3 * Np);
-      std::vector<float> rf(Np), uxf(Np), uyf(Np), uzf(Np), shf(3 * Np);
+      std::vector<double> ux(Np), uy(Np), uz(Np), sh(nf * Np);
+      std::vector<float> rf(Np), uxf(Np), uyf(Np), uzf(Np), shf(nf * Np);
       for (int64_t s = 0; s < Np; ++s) {
         ux[s] = db.pair_u[3 * s];
         uy[s] = db.pair_u[3 * s + 1];
@@ -550,21 +577,21 @@ mz_status mz_create(const mz_db *dbh, const mz_pot *poth, const mz_settings *set
         uxf[s] = (float)ux[s];
         uyf[s] = (float)uy[s];
         uzf[s] = (float)uz[s];
-        for (int q = 0; q < 3; ++q) {
-          sh[q * Np + s] = db.pair_shift[3 * s + q];
-          shf[q * Np + s] = (float)db.pair_shift[3 * s + q];
+        for (int q = 0; q < nf; ++q) {
+          sh[q * Np + s] = db.pair_shift[nf * s + q];
+          shf[q * Np + s] = (float)db.pair_shift[nf * s + q];
         }
       }
       d.pair_r = dupload(ctx, db.pair_r.data(), Np);
       d.pair_ux = dupload(ctx, ux.data(), Np);
       d.pair_uy = dupload(ctx, uy.data(), Np);
       d.pair_uz = dupload(ctx, uz.data(), Np);
-      d.pair_shift = dupload(ctx, sh.data(), 3 * Np);
+      d.pair_shift = dupload(ctx, sh.data(), nf * Np);
       d.pair_rf = dupload(ctx, rf.data(), Np);
       d.pair_uxf = dupload(ctx, uxf.data(), Np);
       d.pair_uyf = dupload(ctx, uyf.data(), Np);
       d.pair_uzf = dupload(ctx, uzf.data(), Np);
-      d.pair_shiftf = dupload(ctx, shf.data(), 3 * Np);
+      d.pair_shiftf = dupload(ctx, shf.data(), nf * Np);
     }
     // atom blocks: consecutive atoms, <= BLOCK_SLOTS slots and <= BLOCK_ATOMS atoms
     std::vector<int> blk(1, 0);
@@ -611,11 +638,13 @@ mz_status mz_create(const mz_db *dbh, const mz_pot *poth, const mz_settings *set
     }
 
     // ---- shared memory of the kernels
-    ctx->smem_atoms[0] = atoms_smem_bytes<double>(ns, ctx->pstride);
-    ctx->smem_atoms[1] = atoms_smem_bytes<float>(ns, ctx->pstride);
-    int ng = 2;
+    ctx->smem_atoms[0] = atoms_smem_bytes<double>(ns, ctx->pstride, dp.nj);
+    ctx->smem_atoms[1] = atoms_smem_bytes<float>(ns, ctx->pstride, dp.nj);
+    int ng = 2;  // the adjoint's per-thread tables hold the largest angular spline (g, q, q2)
     if (meam)
-      for (auto &g : pot.groups[G_G]) ng = std::max(ng, g.nknots);
+      for (int gi : {(int)G_G, (int)G_Q1, (int)G_Q2})
+        if (gi < (int)pot.groups.size())
+          for (auto &g : pot.groups[gi]) ng = std::max(ng, g.nknots);
     dp.g_nmax = ng;
     const int gtabs = dp.gmeam ? pot.ntypes : 1;
     ctx->smem_adj[0] = adj_smem_bytes<double>(ns, stride, ctx->pstride, meam, gtabs, ng);
@@ -640,6 +669,12 @@ mz_status mz_create(const mz_db *dbh, const mz_pot *poth, const mz_settings *set
     smem_attr(k_atoms<true, float, true, true>, ctx->smem_atoms[1]);
     smem_attr(k_adj<true, double, true>, ctx->smem_adj[0]);
     smem_attr(k_adj<true, float, true>, ctx->smem_adj[1]);
+    smem_attr(k_atoms<true, double, false, false, true>, ctx->smem_atoms[0]);
+    smem_attr(k_atoms<true, double, true, false, true>, ctx->smem_atoms[0]);
+    smem_attr(k_atoms<true, float, false, false, true>, ctx->smem_atoms[1]);
+    smem_attr(k_atoms<true, float, true, false, true>, ctx->smem_atoms[1]);
+    smem_attr(k_adj<true, double, false, true>, ctx->smem_adj[0]);
+    smem_attr(k_adj<true, float, false, true>, ctx->smem_adj[1]);
     int nsm = 0, per_sm = 0;
     ck(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, ctx->device), "attribute");
     ck(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_adj<true, float>, BLOCK_SLOTS, ctx->smem_adj[1]),
@@ -666,7 +701,7 @@ mz_status mz_create(const mz_db *dbh, const mz_pot *poth, const mz_settings *set
     size_t freeb = 0, totalb = 0;
     ck(cudaMemGetInfo(&freeb, &totalb), "cudaMemGetInfo");
     const size_t per_cand =
-        sizeof(double) * ((size_t)(3 + (meam ? AUX_COUNT : 0)) * Np + (size_t)(AO_COUNT + 3 + 3) * N +
+        sizeof(double) * ((size_t)(3 + (meam ? dp.aux_rows : 0)) * Np + (size_t)(AO_COUNT + 3 + 3) * N +
                           (size_t)ctx->esize + (size_t)(8 + 1 + CS_COUNT) * db.ncells + 2 * (size_t)stride + ctx->pstride +
                           (size_t)ctx->adj_ctas * stride + 2 * (size_t)ctx->P + 1);
     const size_t budget = (size_t)(0.6 * (double)freeb);
@@ -684,7 +719,7 @@ mz_status mz_create(const mz_db *dbh, const mz_pot *poth, const mz_settings *set
     ctx->d_errvec = dalloc<double>(ctx, C * ctx->esize);
     ctx->d_energy = dalloc<double>(ctx, C * db.ncells);
     ctx->d_stress = dalloc<double>(ctx, C * 6 * db.ncells);
-    ctx->d_aux = meam ? dalloc<double>(ctx, C * AUX_COUNT * Np) : nullptr;
+    ctx->d_aux = meam ? dalloc<double>(ctx, C * dp.aux_rows * Np) : nullptr;
     ctx->d_lam = dalloc<double>(ctx, C * 3 * N);
     ctx->d_seeds = dalloc<double>(ctx, C * CS_COUNT * db.ncells);
     ctx->d_partial = dalloc<double>(ctx, C * (size_t)ctx->adj_ctas * stride);
@@ -882,7 +917,7 @@ extern "C" mz_status mz_objective_noalloc(const mz_db *dbh, const mz_pot *poth, 
     const Db &db = dbh->db;
     const Pot &pot = poth->pot;
     const bool meam = pot.style == MZ_STYLE_MEAM_SPLINE;
-    if (pot.style == MZ_STYLE_GMEAM_SPLINE)
+    if (pot.style == MZ_STYLE_GMEAM_SPLINE || style_nj(pot.style) > 0)
       throw Failure{MZ_ERR_UNSUPPORTED,
                     "the no-allocation objective supports eam/spline, meam/spline and pair/spline"};
     if (style_pair(db.style) != style_pair(pot.style) || (meam && !style_meam(db.style)))
@@ -961,12 +996,12 @@ extern "C" mz_status mz_objective_noalloc(const mz_db *dbh, const mz_pot *poth, 
     std::vector<double> ux(Np), uy(Np), uz(Np), sh(3 * Np);
     for (int64_t q = 0; q < Np; ++q) {
       inslot32[q] = (int)db.in_slot[q];
-      knot32[q] = (db.pair_knot[3 * q] + 1) | ((db.pair_knot[3 * q + 1] + 1) << 8) |
-                  ((db.pair_knot[3 * q + 2] + 1) << 16);
+      knot32[q] = (db.pair_knot[db.nfun * q] + 1) | ((db.pair_knot[db.nfun * q + 1] + 1) << 8) |
+                  ((db.pair_knot[db.nfun * q + 2] + 1) << 16);
       ux[q] = db.pair_u[3 * q];
       uy[q] = db.pair_u[3 * q + 1];
       uz[q] = db.pair_u[3 * q + 2];
-      for (int k = 0; k < 3; ++k) sh[k * Np + q] = db.pair_shift[3 * q + k];
+      for (int k = 0; k < 3; ++k) sh[k * Np + q] = db.pair_shift[db.nfun * q + k];
     }
     std::vector<int> blk(1, 0);
     {

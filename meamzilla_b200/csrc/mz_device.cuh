@@ -44,8 +44,9 @@ struct DevDb {
   // pairs
   const int *pair_nbr;
   const double *pair_r, *pair_ux, *pair_uy, *pair_uz;
-  const double *pair_shift;       // [3][Np] phi, rho, f
-  const int *pair_knot;           // packed: (phi+1) | (rho+1) << 8 | (f+1) << 16
+  const double *pair_shift;       // [nfun][Np] phi, rho, f (+ p, p2 for JMEAM)
+  const int *pair_knot;           // packed: (phi+1) | (rho+1) << 8 | (f+1) << 16 | (p+1) << 24
+  const signed char *pair_knot_p2;  // JMEAM2: knot of p2 (-1: none), else null
   const float *pair_rf, *pair_uxf, *pair_uyf, *pair_uzf, *pair_shiftf;  // FP32 copies
   // atom blocks
   const int *blk_atom0;           // [nblocks+1]
@@ -71,6 +72,9 @@ struct DevPot {
   int npair;          // ntypes (ntypes + 1) / 2
   int pair;           // pair/spline: phi only over each pair once (self images at 1/2),
                       // no embedding, no constraint or punishment entries
+  int nj;             // JMEAM direct three-body terms sum p_ij p_ik q_i(cos): 0, 1 or 2
+  int s_p[2], s_q[2]; // first spline of p, q (p2, q2)
+  int aux_rows;       // per-slot adjoint sums kept per candidate: 5 (1 + nj)
   double energy_weight, stress_weight;
 };
 

@@ -7,8 +7,9 @@ namespace mzb {
 
 // Per-atom outputs, [cand][AO_COUNT][natoms].
 enum { AO_AX = 0, AO_AY, AO_AZ, AO_E, AO_S0, AO_PEN = AO_S0 + 6, AO_RHO, AO_FSQ, AO_COUNT };
-// Per-slot triplet sums kept for the adjoint, [cand][AUX_COUNT][npairs]:
-//   G_p = sum_k g f_k,  H_p = sum_k g' f_k cos,  vk_p = sum_k g' f_k u_k.
+// Per-slot triplet sums kept for the adjoint, [cand][aux_rows][npairs]:
+//   G_p = sum_k g f_k,  H_p = sum_k g' f_k cos,  vk_p = sum_k g' f_k u_k,
+// and for each JMEAM term m the same with (q_m, p_m) at rows AUX_COUNT (1 + m) + ...
 enum { AUX_G = 0, AUX_H, AUX_VX, AUX_VY, AUX_VZ, AUX_COUNT };
 // Per-cell adjoint seeds, [cand][CS_COUNT][ncells]: dF/dE_atom, dF/dS (6), dF/dpen.
 enum { CS_EPS = 0, CS_MU0, CS_KAPPA = CS_MU0 + 6, CS_COUNT };
@@ -137,6 +138,8 @@ struct PairEval {
   R phi, dphi, rho, drho, f, df;
   int kphi, krho, kf, tj, pij;
   R bphi, brho, bf;
+  R p[2], dp[2], bp[2];  // JMEAM p (p2) (pot_jmeam_spline.cpp:196-202)
+  int kp[2];
 };
 
 template <bool MEAM, typename R>
@@ -176,6 +179,24 @@ __device__ __forceinline__ PairEval<MEAM, R> eval_pair(const DevDb &db, const De
   return p;
 }
 
+// The JMEAM radial functions p (p2) of one slot.
+template <bool MEAM, typename R>
+__device__ __forceinline__ void eval_pair_p(const DevDb &db, const DevPot &pot, const SplineGeom *sg, const R *ptab,
+                                            int64_t gs, PairEval<MEAM, R> &p) {
+  const int64_t Np = db.npairs;
+  const int kn = db.pair_knot[gs];
+  p.kp[0] = ((kn >> 24) & 0xff) - 1;
+  p.kp[1] = pot.nj > 1 ? (int)db.pair_knot_p2[gs] : -1;
+  for (int m = 0; m < 2; ++m) {
+    p.p[m] = p.dp[m] = p.bp[m] = R(0);
+    if (m < pot.nj && p.kp[m] >= 0) {
+      const SplineGeom &g = sg[pot.s_p[m] + p.pij];
+      p.bp[m] = sizeof(R) == 8 ? (R)db.pair_shift[(3 + m) * Np + gs] : (R)db.pair_shiftf[(3 + m) * Np + gs];
+      p.p[m] = cubic_val_grad<R>(ptab + g.poff, p.kp[m], p.bp[m], (R)g.invstep, p.dp[m]);
+    }
+  }
+}
+
 // ------------------------------------------------------------------ k_atoms
 
 // Shared-memory layout of k_atoms (dynamic), see atoms_smem_bytes():
@@ -185,6 +206,8 @@ __device__ __forceinline__ PairEval<MEAM, R> eval_pair(const DevDb &db, const De
 //   int a_lo[BLOCK_ATOMS+2]
 //   R ptab[pstride]                    this candidate's evaluation table
 //   R4 srow[BLOCK_SLOTS]               (u_x, u_y, u_z, f) of every slot of the block
+//   int stype[BLOCK_SLOTS+8]           neighbour type of every slot (GMEAM)
+//   R spv[nj][BLOCK_SLOTS+8]           JMEAM p (p2) of every slot
 template <typename R>
 struct Vec4;
 template <>
@@ -197,7 +220,7 @@ struct Vec4<double> {
 };
 
 template <typename R>
-__host__ __device__ inline size_t atoms_smem_bytes(int nsplines, int pstride) {
+__host__ __device__ inline size_t atoms_smem_bytes(int nsplines, int pstride, int nj = 0) {
   size_t b = sizeof(double) * (10 * BLOCK_SLOTS + 2 * BLOCK_ATOMS);
   b += sizeof(SplineGeom) * nsplines;
   b += sizeof(int) * (BLOCK_ATOMS + 2);
@@ -206,6 +229,7 @@ __host__ __device__ inline size_t atoms_smem_bytes(int nsplines, int pstride) {
   b = (b + 31) & ~size_t(31);
   b += 4 * sizeof(R) * (BLOCK_SLOTS + 8);
   b += sizeof(int) * (BLOCK_SLOTS + 8);  // neighbour type of every slot (GMEAM's g index)
+  b += sizeof(R) * (size_t)nj * (BLOCK_SLOTS + 8);
   return b;
 }
 
@@ -223,6 +247,46 @@ __device__ __forceinline__ double cos_dot(double ax, double ay, double az, doubl
 __device__ __forceinline__ float cos_dot(float ax, float ay, float az, float bx, float by, float bz) {
   return fmaf(ax, bx, fmaf(ay, by, az * bz));
 }
+
+// Row sums of one angular channel for slot `tid`: with w_k the partner's
+// radial weight (f_k for g, p_k for a JMEAM q) and s the channel's spline,
+//   S = sum_k s(cos) w_k,  T = sum_k s'(cos) w_k cos,  v = sum_k s'(cos) w_k u_k
+// over the row's other slots whose cosine has a knot of s.  FP32 chunks of 8
+// terms are added to FP64 totals (as the g loop of k_atoms).
+template <typename R, typename R4, class W>
+__device__ __forceinline__ void channel_row_sums(const R4 *srow, W weight, int row_lo, int row_hi, int tid, R ux,
+                                                 R uy, R uz, const SplineGeom &gs, const R *spc, double &S, double &T,
+                                                 double &vx, double &vy, double &vz) {
+  const R x0 = (R)gs.x0, inv = (R)gs.invstep, cut = g_cut<R>(gs);
+  S = T = vx = vy = vz = 0.0;
+  for (int kb = row_lo; kb < row_hi; kb += 8) {
+    R s8 = 0, t8 = 0, x8 = 0, y8 = 0, z8 = 0;
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const int k = kb + u;
+      const R4 o = srow[k];
+      const R cs = cos_dot(ux, uy, uz, o.x, o.y, o.z);
+      const bool ok = (k < row_hi) && (k != tid) && (cs < cut);
+      const R wk = ok ? weight(k) : R(0);
+      R b;
+      const int kk = g_knot<R>(cs, x0, inv, gs.n, b);
+      R ds;
+      const R sv = cubic_val_grad<R>(spc, kk, b, inv, ds);
+      const R dsw = ds * wk;
+      s8 += sv * wk;
+      t8 += dsw * cs;
+      x8 += dsw * o.x;
+      y8 += dsw * o.y;
+      z8 += dsw * o.z;
+    }
+    S += (double)s8;
+    T += (double)t8;
+    vx += (double)x8;
+    vy += (double)y8;
+    vz += (double)z8;
+  }
+}
+
 
 // Warp-cooperative sum over the slots [lo, hi) of `n` per-slot arrays
 // red[q * BLOCK_SLOTS + s]; the result is valid on lane 0.  Fixed order.
@@ -248,8 +312,8 @@ __device__ __forceinline__ void warp_slot_sums(const double *red, int lo, int hi
 // is the force atom i's terms add to atom i along slot p; the neighbour
 // receives -V_p (k_gather).  In FP32 the row sums are taken in chunks of 8
 // terms, each chunk added to an FP64 total.
-template <bool MEAM, typename R, bool AUX, bool GM = false>
-__global__ void __launch_bounds__(BLOCK_SLOTS, sizeof(R) == 4 ? 4 : 3)
+template <bool MEAM, typename R, bool AUX, bool GM = false, bool JM = false>
+__global__ void __launch_bounds__(BLOCK_SLOTS, JM ? 2 : sizeof(R) == 4 ? 4 : 3)
     k_atoms(DevDb db, DevPot pot, const SplineGeom *__restrict__ geom, const double *__restrict__ tabs,
             const double *__restrict__ ptabs, double *__restrict__ Vout, double *__restrict__ aout,
             double *__restrict__ aux) {
@@ -273,6 +337,7 @@ __global__ void __launch_bounds__(BLOCK_SLOTS, sizeof(R) == 4 ? 4 : 3)
   off = (off + 31) & ~size_t(31);
   R4 *srow = reinterpret_cast<R4 *>(smem_raw + off);
   int *stype = reinterpret_cast<int *>(srow + BLOCK_SLOTS + 8);
+  R *spv = reinterpret_cast<R *>(stype + BLOCK_SLOTS + 8);
 
   const BlockRows br = block_rows(db, blockIdx.x);
   const double *tc = tabs + (size_t)cand * pot.tab_stride;
@@ -300,6 +365,13 @@ __global__ void __launch_bounds__(BLOCK_SLOTS, sizeof(R) == 4 ? 4 : 3)
     if (GM) {
       stype[tid] = have ? pe.tj : 0;
       if (tid < 8) stype[BLOCK_SLOTS + tid] = 0;
+    }
+    if (JM) {
+      if (have) eval_pair_p<MEAM, R>(db, pot, sg, ptab, gs, pe);
+      for (int m = 0; m < pot.nj; ++m) {
+        spv[m * (BLOCK_SLOTS + 8) + tid] = have ? pe.p[m] : R(0);
+        if (tid < 8) spv[m * (BLOCK_SLOTS + 8) + BLOCK_SLOTS + tid] = R(0);
+      }
     }
   }
   __syncthreads();
@@ -338,7 +410,7 @@ __global__ void __launch_bounds__(BLOCK_SLOTS, sizeof(R) == 4 ? 4 : 3)
       vkz += (double)z8;
     }
     if (AUX) {
-      double *ax = aux + (size_t)cand * AUX_COUNT * Np;
+      double *ax = aux + (size_t)cand * (JM ? pot.aux_rows : (int)AUX_COUNT) * Np;
       ax[AUX_G * Np + gs] = G;
       ax[AUX_H * Np + gs] = H;
       ax[AUX_VX * Np + gs] = vkx;
@@ -381,12 +453,31 @@ __global__ void __launch_bounds__(BLOCK_SLOTS, sizeof(R) == 4 ? 4 : 3)
       vkz += (double)z8;
     }
     if (AUX) {
-      double *ax = aux + (size_t)cand * AUX_COUNT * Np;
+      double *ax = aux + (size_t)cand * (JM ? pot.aux_rows : (int)AUX_COUNT) * Np;
       ax[AUX_G * Np + gs] = G;
       ax[AUX_H * Np + gs] = H;
       ax[AUX_VX * Np + gs] = vkx;
       ax[AUX_VY * Np + gs] = vky;
       ax[AUX_VZ * Np + gs] = vkz;
+    }
+  }
+  // ---- JMEAM: the same row sums for each (p, q) term (pot_jmeam_spline.cpp:208-219)
+  double G2[2] = {0, 0}, H2[2] = {0, 0}, v2x[2] = {0, 0}, v2y[2] = {0, 0}, v2z[2] = {0, 0};
+  if (JM && have) {
+    for (int m = 0; m < pot.nj; ++m) {
+      if (!AUX && pe.p[m] == R(0) && pe.dp[m] == R(0)) continue;
+      const SplineGeom qg = sg[pot.s_q[m] + ti];
+      const R *wm = spv + m * (BLOCK_SLOTS + 8);
+      channel_row_sums<R>(srow, [&](int k) { return wm[k]; }, a_lo[me], a_lo[me + 1], tid, pe.ux, pe.uy, pe.uz,
+                          qg, ptab + qg.poff, G2[m], H2[m], v2x[m], v2y[m], v2z[m]);
+      if (AUX) {
+        double *ax = aux + ((size_t)cand * pot.aux_rows + AUX_COUNT * (1 + m)) * Np;
+        ax[AUX_G * Np + gs] = G2[m];
+        ax[AUX_H * Np + gs] = H2[m];
+        ax[AUX_VX * Np + gs] = v2x[m];
+        ax[AUX_VY * Np + gs] = v2y[m];
+        ax[AUX_VZ * Np + gs] = v2z[m];
+      }
     }
   }
   if (have) red[tid] = (double)pe.rho + (MEAM ? 0.5 * (double)pe.f * G : 0.0);
@@ -429,9 +520,10 @@ __global__ void __launch_bounds__(BLOCK_SLOTS, sizeof(R) == 4 ? 4 : 3)
   if (have) {
     const double dF = a_dF[me];
     const double ux = (double)pe.ux, uy = (double)pe.uy, uz = (double)pe.uz;
-    const double sp = phi_share(pot, db.pair_nbr[gs] == br.atom_lo + me);
+    const double sp = MEAM ? 0.5 : phi_share(pot, db.pair_nbr[gs] == br.atom_lo + me);
     double cu = sp * (double)pe.dphi + (double)pe.drho * dF;
     double Vx = 0, Vy = 0, Vz = 0;
+    double e3 = 0.0;  // JMEAM: 1/2 sum_m p_m G2_m, this slot's share of the p p q energy
     if (MEAM) {
       const double ip = (double)pe.invr, fp = (double)pe.f;
       cu += dF * ((double)pe.df * G - fp * ip * H);
@@ -439,6 +531,16 @@ __global__ void __launch_bounds__(BLOCK_SLOTS, sizeof(R) == 4 ? 4 : 3)
       Vx = ck * vkx;
       Vy = ck * vky;
       Vz = ck * vkz;
+      if (JM)
+        for (int m = 0; m < pot.nj; ++m) {
+          // the q terms' dfj without U' (pot_jmeam_spline.cpp:263-273)
+          const double pm = (double)pe.p[m];
+          cu += (double)pe.dp[m] * G2[m] - pm * ip * H2[m];
+          Vx += pm * ip * v2x[m];
+          Vy += pm * ip * v2y[m];
+          Vz += pm * ip * v2z[m];
+          e3 += 0.5 * pm * G2[m];
+        }
     }
     Vx += ux * cu;
     Vy += uy * cu;
@@ -452,7 +554,7 @@ __global__ void __launch_bounds__(BLOCK_SLOTS, sizeof(R) == 4 ? 4 : 3)
     red[0 * BLOCK_SLOTS + tid] = Vx;
     red[1 * BLOCK_SLOTS + tid] = Vy;
     red[2 * BLOCK_SLOTS + tid] = Vz;
-    red[3 * BLOCK_SLOTS + tid] = sp * (double)pe.phi;
+    red[3 * BLOCK_SLOTS + tid] = sp * (double)pe.phi + e3;
     red[4 * BLOCK_SLOTS + tid] = -(dx * (Vx * rr));
     red[5 * BLOCK_SLOTS + tid] = -(dy * (Vy * rr));
     red[6 * BLOCK_SLOTS + tid] = -(dz * (Vz * rr));
@@ -606,14 +708,16 @@ __device__ __forceinline__ double spline_max_y(const SplineGeom &g, const double
   if (which) *which = sat;
   return sm;
 }
-__device__ __forceinline__ double f_max_y(const DevPot &pot, const SplineGeom *geom, const double *tab, int *which) {
-  // signed largest-|y| knot over the f splines (pot_fns.cpp:100-111)
+// Signed largest-|y| knot over a Pair_ij group (PotFns::get_max_y_mag,
+// pot_fns.cpp:100-111) whose first spline is s0: f, or JMEAM's p (p2).
+__device__ __forceinline__ double group_max_y(const DevPot &pot, int s0, const SplineGeom *geom, const double *tab,
+                                              int *which) {
   double my = 0.0;
   int at = -1;
   const int nf = pot.ntypes * (pot.ntypes + 1) / 2;
   for (int f = 0; f < nf; ++f) {
     int sat;
-    const double sm = spline_max_y(geom[pot.s_f + f], tab, &sat);
+    const double sm = spline_max_y(geom[s0 + f], tab, &sat);
     if (fabs(my) < fabs(sm)) {
       my = sm;
       at = sat;
@@ -645,7 +749,10 @@ __global__ void k_final(DevDb db, DevPot pot, const SplineGeom *__restrict__ geo
       // no punishments (PotPairSpline::fast_compute, pot_pair_spline.cpp:133)
     } else if (pot.omit_pen) {
       if (ev) {
-        const int npen = pot.style == MZ_STYLE_MEAM_SPLINE ? 1 : pot.gmeam ? pot.npair : pot.ntypes;
+        const int npen = pot.style == MZ_STYLE_MEAM_SPLINE ? 1
+                         : pot.nj > 0                     ? 1 + pot.nj
+                         : pot.gmeam                      ? pot.npair
+                                                          : pot.ntypes;
         for (int q = 0; q < npen; ++q) ev[q] = 0.0;
       }
     } else if (pot.gmeam) {
@@ -656,12 +763,15 @@ __global__ void k_final(DevDb db, DevPot pot, const SplineGeom *__restrict__ geo
         total += fe * fe;
         if (ev) ev[f] = fe;
       }
-    } else if (pot.style == MZ_STYLE_MEAM_SPLINE) {
-      // f-potential magnitude punishment (pot_meam_spline.cpp:274-278)
-      const double m = fabs(f_max_y(pot, geom, tab, nullptr));
-      const double fe = 100. * 25. * (1.0 - m) * (1.0 - m);
-      total += fe * fe;
-      if (ev) ev[0] = fe;
+    } else if (pot.style == MZ_STYLE_MEAM_SPLINE || pot.nj > 0) {
+      // f-potential magnitude punishment (pot_meam_spline.cpp:274-278), and
+      // JMEAM's p (p2) magnitude punishments (pot_jmeam_spline.cpp:286-299)
+      for (int q = 0; q <= pot.nj; ++q) {
+        const double m = fabs(group_max_y(pot, q == 0 ? pot.s_f : pot.s_p[q - 1], geom, tab, nullptr));
+        const double fe = 100. * 25. * (1.0 - m) * (1.0 - m);
+        total += fe * fe;
+        if (ev) ev[q] = fe;
+      }
     } else {
       // U'(mid-range) punishment per type (pot_eam_spline.cpp:211-218)
       for (int ty = 0; ty < pot.ntypes; ++ty) {

@@ -253,10 +253,10 @@ void Pot::set_coeffs(const double *in) {
 }
 
 double Pot::max_rcut() const {
-  // radial groups: phi, rho and (MEAM) f
+  // radial groups: phi, rho, (MEAM) f, (JMEAM) p, p2
   double m = 0.0;
   for (int gi = 0; gi < (int)groups.size(); ++gi) {
-    if (gi == G_U || gi == G_G) continue;
+    if (gi == G_U || gi == G_G || gi == G_Q1 || gi == G_Q2) continue;
     for (auto &s : groups[gi]) m = std::max(m, s.x.back());
   }
   return m;
@@ -310,12 +310,21 @@ void parse_pot(const std::string &text, Pot &pot) {
   } else if (pot.type_name == "eam/spline") {
     pot.style = MZ_STYLE_EAM_SPLINE;
     nalloy = {npair, nt, nt};
+  } else if (pot.type_name == "jmeam/spline") {
+    // + p (Pair_ij), q (Triplet_i) (pot_jmeam.cpp:31-45)
+    pot.style = MZ_STYLE_JMEAM_SPLINE;
+    nalloy = {npair, nt, nt, npair, nt, npair, nt};
+  } else if (pot.type_name == "jmeam2/spline") {
+    // + p2, q2 (pot_jmeam2.cpp:31-45)
+    pot.style = MZ_STYLE_JMEAM2_SPLINE;
+    nalloy = {npair, nt, nt, npair, nt, npair, nt, npair, nt};
   } else if (pot.type_name == "pair/spline") {
     pot.style = MZ_STYLE_PAIR_SPLINE;
     nalloy = {npair};
   } else {
     fail(MZ_ERR_UNSUPPORTED, "potential style \"" + pot.type_name +
-                                 "\" is not implemented (eam/spline, meam/spline, gmeam/spline, pair/spline)");
+                                 "\" is not implemented (eam/spline, meam/spline, gmeam/spline, jmeam/spline, "
+                                 "jmeam2/spline, pair/spline)");
   }
   pot.ngroups = (int)nalloy.size();
   if (ln >= L.size() || L[ln++].substr(0, 2) != "#P") fail(MZ_ERR_FORMAT, "potential line (#P ...) missing");
@@ -464,9 +473,9 @@ void read_config_file(const std::string &path, int ntypes, std::vector<int> &cel
 
 // ------------------------------------------------------------------ rescale
 
-int rescale_pot(Pot &pot, const int *atom_type, int natoms, const double *dens, int flag, double factors[2]) {
+int rescale_pot(Pot &pot, const int *atom_type, int natoms, const double *dens, int flag, double factors[4]) {
   // PotMEAM::rescale (pot_meam.cpp:281-375) / PotEAM::rescale (pot_eam.cpp:257-389)
-  factors[0] = factors[1] = 0.0;
+  factors[0] = factors[1] = factors[2] = factors[3] = 0.0;
   if (flag < 0 || style_pair(pot.style)) return 0;  // PotPair: Potential::rescale (potential.cpp:258-261)
   const bool meam = style_meam(pot.style);
   std::vector<Spline3> &F = pot.groups[G_U];
@@ -533,6 +542,20 @@ int rescale_pot(Pot &pot, const int *atom_type, int natoms, const double *dens, 
     for (Spline3 &sp : pot.groups[G_F]) sp.scale_y(b);
     for (Spline3 &sp : pot.groups[G_G]) sp.divide_y(b * b);
     factors[1] = b;
+    // PotJMEAM::rescale_3body (pot_jmeam.cpp:375-401), PotJMEAM2::rescale_3body
+    // (pot_jmeam2.cpp:416-442): p p q = (b p)(b p)(q / b^2) likewise, b from the p (p2) group
+    for (int t = 0; t < style_nj(pot.style); ++t) {
+      const int gp = t == 0 ? G_P1 : G_P2, gq = t == 0 ? G_Q1 : G_Q2;
+      double mp = 0.0;
+      for (const Spline3 &sp : pot.groups[gp]) {
+        const double v = sp.max_y_mag();
+        if (std::abs(mp) < std::abs(v)) mp = v;
+      }
+      const double bp = 1.0 / mp;
+      for (Spline3 &sp : pot.groups[gp]) sp.scale_y(bp);
+      for (Spline3 &sp : pot.groups[gq]) sp.divide_y(bp * bp);
+      factors[2 + t] = bp;
+    }
   }
   if (!flag) return 0;
   for (int i = 0; i < Fs; ++i) {
@@ -725,15 +748,22 @@ void write_data_files(const Db &db, const Pot &pot, double energy_weight, double
         ++idx;
       }
     } else if (meam) {
-      double m = 0.0;
-      for (const Spline3 &sp : pot.groups[G_F]) {
-        const double v = sp.max_y_mag();
-        if (std::abs(m) < std::abs(v)) m = v;
+      // PotMEAM::write_punish; PotJMEAM / PotJMEAM2::write_punish add the p
+      // (p2) magnitudes (pot_jmeam.cpp:309-366, pot_jmeam2.cpp:337-410)
+      static const char *name[3] = {"f", "p", "p2"};
+      const int grp[3] = {G_F, G_P1, G_P2};
+      for (int t = 0; t <= style_nj(pot.style); ++t, ++idx) {
+        double m = 0.0;
+        for (const Spline3 &sp : pot.groups[grp[t]]) {
+          const double v = sp.max_y_mag();
+          if (std::abs(m) < std::abs(v)) m = v;
+        }
+        f << std::endl << "Dummy constraints (|" << name[t] << "_max(r)| = 1)" << std::endl;
+        f << std::setw(15) << std::right << "punish error" << std::setw(15) << std::right
+          << (std::string("|") + name[t] + "_max(r)|") << std::endl;
+        f << std::fixed << std::setw(15) << std::right << std::setprecision(6) << e[idx] * e[idx] << std::setw(15)
+          << std::right << std::setprecision(6) << std::abs(std::abs(m)) << std::endl;
       }
-      f << std::endl << "Dummy constraints (|f_max(r)| = 1)" << std::endl;
-      f << std::setw(15) << std::right << "punish error" << std::setw(15) << std::right << "|f_max(r)|" << std::endl;
-      f << std::fixed << std::setw(15) << std::right << std::setprecision(6) << e[idx] * e[idx] << std::setw(15)
-        << std::right << std::setprecision(6) << std::abs(std::abs(m)) << std::endl;
     } else {
       f << std::endl << "Dummy constraints (F'(n_avg) = 0)" << std::endl;
       f << std::setw(7) << std::right << "element" << std::setw(15) << std::right << "punish error" << std::setw(15)
@@ -772,6 +802,7 @@ void build_db_setup(const mz_cells_desc &c, const Pot &pot, Db &db) {
     fail(MZ_ERR_ARG, "empty or incomplete cell description");
   const bool meam = style_meam(pot.style);
   db.style = pot.style;
+  db.nfun = 3 + style_nj(pot.style);
   db.ncells = c.ncells;
   db.natoms = c.natoms;
   db.cell_atom0.assign(c.ncells + 1, 0);
@@ -824,7 +855,7 @@ std::string cell_too_small_msg(int ci) {
 }
 
 std::string pair_too_short_msg(const Pot &pot, int q, double rr, int ti, int tj, int ci, int i, int j) {
-  static const char *nm[3] = {"phi", "rho", "f"};
+  static const char *nm[5] = {"phi", "rho", "f", "p", "p2"};
   char buf[256];
   std::snprintf(buf, sizeof buf,
                 "ERROR: Pair distance too short for potential (r=%g, pot=%s[%d]) - cell=%d atom=%d neigh=%d", rr,
@@ -846,10 +877,13 @@ void build_incoming(Db &db) {
 void build_db(const mz_cells_desc &c, const Pot &pot, Db &db) {
   build_db_setup(c, pot, db);
   const bool meam = style_meam(pot.style), half = style_pair(pot.style);
-  const int nq = half ? 1 : meam ? 3 : 2;  // radial functions checked per pair: phi (rho, f)
+  const int nj = style_nj(pot.style), nf = db.nfun;
+  // radial functions checked per pair: phi (rho, f, p, p2)
+  const int nq = half ? 1 : meam ? 3 + nj : 2;
   const double max_rcut = pot.max_rcut();
   const int sphi0 = pot.spline_index(G_PHI, 0), srho0 = half ? -1 : pot.spline_index(G_RHO, 0);
   const int sf0 = meam ? pot.spline_index(G_F, 0) : -1;
+  const int sp0[2] = {nj > 0 ? pot.spline_index(G_P1, 0) : -1, nj > 1 ? pot.spline_index(G_P2, 0) : -1};
 
   std::vector<CellPairs> per(c.ncells);
   std::atomic<int> next(0);
@@ -891,11 +925,11 @@ void build_db(const mz_cells_desc &c, const Pot &pot, Db &db) {
                 double rr = mag(d);
                 V3 u{d.x / rr, d.y / rr, d.z / rr};
                 // check_pair (pair_meam_spline.cpp:50-99 / pair_eam_spline.cpp:50-86 /
-                // pair_pair_spline.cpp:48-72)
-                int sidx[3] = {sphi0 + pot.idx_pair_ij(ti, tj), srho0 + tj,
-                               meam ? sf0 + pot.idx_pair_ij(ti, tj) : -1};
-                int kn[3] = {-1, -1, -1};
-                double sh[3] = {0, 0, 0};
+                // pair_pair_spline.cpp:48-72 / pair_jmeam_spline.cpp:48-110)
+                const int pij = pot.idx_pair_ij(ti, tj);
+                int sidx[5] = {sphi0 + pij, srho0 + tj, meam ? sf0 + pij : -1, sp0[0] + pij, sp0[1] + pij};
+                int kn[5] = {-1, -1, -1, -1, -1};
+                double sh[5] = {0, 0, 0, 0, 0};
                 bool bad = false;
                 for (int q = 0; q < nq; ++q) {
                   const Spline3 &sp = pot.spline(sidx[q]);
@@ -908,13 +942,13 @@ void build_db(const mz_cells_desc &c, const Pot &pot, Db &db) {
                   kn[q] = sp.knotshift(rr, &sh[q]);
                 }
                 if (bad) return;
-                if (kn[0] == -1 && kn[1] == -1 && kn[2] == -1) continue;
+                if (kn[0] == -1 && kn[1] == -1 && kn[2] == -1 && kn[3] == -1 && kn[4] == -1) continue;
                 out.nbr.push_back(a_lo + j);
                 out.r.push_back(rr);
                 out.u.push_back(u.x);
                 out.u.push_back(u.y);
                 out.u.push_back(u.z);
-                for (int q = 0; q < 3; ++q) {
+                for (int q = 0; q < nf; ++q) {
                   out.knot.push_back((int8_t)kn[q]);
                   out.shift.push_back(kn[q] >= 0 ? sh[q] : 0.0);
                 }
@@ -951,8 +985,8 @@ void build_db(const mz_cells_desc &c, const Pot &pot, Db &db) {
   db.pair_nbr.resize(np);
   db.pair_r.resize(np);
   db.pair_u.resize(3 * np);
-  db.pair_knot.resize(3 * np);
-  db.pair_shift.resize(3 * np);
+  db.pair_knot.resize(nf * np);
+  db.pair_shift.resize(nf * np);
   int64_t o = 0;
   for (int ci = 0; ci < c.ncells; ++ci) {
     CellPairs &p = per[ci];
@@ -960,8 +994,8 @@ void build_db(const mz_cells_desc &c, const Pot &pot, Db &db) {
     std::copy(p.nbr.begin(), p.nbr.end(), db.pair_nbr.begin() + o);
     std::copy(p.r.begin(), p.r.end(), db.pair_r.begin() + o);
     std::copy(p.u.begin(), p.u.end(), db.pair_u.begin() + 3 * o);
-    std::copy(p.knot.begin(), p.knot.end(), db.pair_knot.begin() + 3 * o);
-    std::copy(p.shift.begin(), p.shift.end(), db.pair_shift.begin() + 3 * o);
+    std::copy(p.knot.begin(), p.knot.end(), db.pair_knot.begin() + nf * o);
+    std::copy(p.shift.begin(), p.shift.end(), db.pair_shift.begin() + nf * o);
     o += (int64_t)n;
     CellPairs().nbr.swap(p.nbr);
   }
@@ -1211,6 +1245,7 @@ mz_status mz_db_get_view(const mz_db *dbh, mz_db_view *v) {
     v->pair_shift = d.pair_shift.data();
     v->in_off = d.in_off.data();
     v->in_slot = d.in_slot.data();
+    v->nfun = d.nfun;
   });
 }
 

@@ -55,19 +55,31 @@ struct Spline3 {
 // Function groups in file order.  MEAM: phi(Pair_ij) rho(Pair_j) U(Atom/Pair_i)
 // f(Pair_ij) g(Triplet_i) (pot_meam.cpp:31-47, pot_eam.cpp:30-46,
 // pot_pair.cpp:25-37).  EAM: the first three.
-enum Group { G_PHI = 0, G_RHO = 1, G_U = 2, G_F = 3, G_G = 4 };
+// JMEAM adds p (Pair_ij, radial) and q (Triplet_i) after g, JMEAM2 a second
+// pair p2, q2 (pot_jmeam.cpp:31-45, pot_jmeam2.cpp:31-45).
+enum Group { G_PHI = 0, G_RHO = 1, G_U = 2, G_F = 3, G_G = 4, G_P1 = 5, G_Q1 = 6, G_P2 = 7, G_Q2 = 8 };
 
 // MEAM and GMEAM share the skeleton (three-body f f g); GMEAM indexes g by
 // the types of i and of the pair j, k (Triplet_i_jk, pot_fns.cpp:166-168) and
 // punishes every f spline (pot_gmeam_spline.cpp:173-178).
-inline bool style_meam(int style) { return style == MZ_STYLE_MEAM_SPLINE || style == MZ_STYLE_GMEAM_SPLINE; }
+inline bool style_meam(int style) {
+  return style == MZ_STYLE_MEAM_SPLINE || style == MZ_STYLE_GMEAM_SPLINE || style == MZ_STYLE_JMEAM_SPLINE ||
+         style == MZ_STYLE_JMEAM2_SPLINE;
+}
+// Direct three-body energy terms sum_{j<k} p_ij p_ik q_i(cos) of the JMEAM
+// styles (PotJMEAMSpline::fast_compute, pot_jmeam_spline.cpp:208-219):
+// jmeam/spline one (p, q), jmeam2/spline two.
+inline int style_nj(int style) {
+  return style == MZ_STYLE_JMEAM_SPLINE ? 1 : style == MZ_STYLE_JMEAM2_SPLINE ? 2 : 0;
+}
 // pair/spline (PotPair, pot_pair.cpp:25-37; PotPairSpline::fast_compute,
 // pot_pair_spline.cpp:71-139): phi only, each pair once (dbl_cnt_pair_ = 0,
 // config.cpp:181-185), no embedding, no constraint or punishment entries.
 inline bool style_pair(int style) { return style == MZ_STYLE_PAIR_SPLINE; }
 // Entries after the per-cell constraints: MEAM 1, GMEAM one per f spline, EAM one per type.
 inline int style_npen(int style, int ntypes) {
-  return style == MZ_STYLE_MEAM_SPLINE    ? 1
+  return style_nj(style) > 0              ? 1 + style_nj(style)  // f-max, then p-max per (p, q)
+         : style == MZ_STYLE_MEAM_SPLINE  ? 1
          : style == MZ_STYLE_GMEAM_SPLINE ? ntypes * (ntypes + 1) / 2
          : style == MZ_STYLE_PAIR_SPLINE  ? 0
                                           : ntypes;
@@ -106,6 +118,7 @@ struct Pot {
 // list for that atom in the same order (config.cpp:186-228).
 struct Db {
   int style = -1;  // potential style the lists were built for (pair/spline: each pair once)
+  int nfun = 3;    // radial functions per pair in pair_knot / pair_shift: phi, rho, f (+ p, p2)
   int ncells = 0, natoms = 0;
   int64_t npairs = 0, ntriplets = 0;
   int max_row = 0;
@@ -121,8 +134,8 @@ struct Db {
   // pairs
   std::vector<int> pair_nbr;                  // neighbour atom index
   std::vector<double> pair_r, pair_u;         // r, unit vector [3Np]
-  std::vector<int8_t> pair_knot;              // [3Np] phi, rho, f (f: MEAM only)
-  std::vector<double> pair_shift;             // [3Np]
+  std::vector<int8_t> pair_knot;              // [Np][nfun] phi, rho, f (f: MEAM only), p, p2 (JMEAM)
+  std::vector<double> pair_shift;             // [Np][nfun]
   // incoming lists: for every atom, the pair slots whose neighbour it is
   std::vector<int64_t> in_off;                // [N+1]
   std::vector<int64_t> in_slot;               // [Np]

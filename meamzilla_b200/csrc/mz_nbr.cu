@@ -27,11 +27,12 @@ namespace {
 
 struct NbrParams {
   int natoms;
-  int nq;            // radial functions checked per pair: phi (rho, f)
+  int nq;            // radial functions checked per pair: phi (rho, f, p, p2)
+  int nf;            // values stored per pair (Db::nfun)
   int half;          // each pair once: neighbours j >= i of the cell (config.cpp:181-185)
   int ntypes;
   double max_rcut;
-  int s[3];          // first spline of phi, rho, f
+  int s[5];          // first spline of phi, rho, f, p, p2
   const double *x;   // knot grids of all splines, concatenated
   const int *xoff;   // [nsplines] offset of each grid in x
   const int *xn;     // [nsplines] knots of each grid
@@ -92,7 +93,7 @@ __global__ void k_find_pairs(NbrParams p, const int *__restrict__ cell_atom0, co
       const double pjx = pj[0], pjy = pj[1], pjz = pj[2];
       const int tj = types[a_lo + j];
       const int pij = pair_ij(ti, tj, p.ntypes);
-      const int sidx[3] = {p.s[0] + pij, p.s[1] + tj, p.s[2] + pij};
+      const int sidx[5] = {p.s[0] + pij, p.s[1] + tj, p.s[2] + pij, p.s[3] + pij, p.s[4] + pij};
       for (int ix = -sx; ix <= sx; ++ix)
         for (int iy = -sy; iy <= sy; ++iy)
           for (int iz = -sz; iz <= sz; ++iz) {
@@ -108,8 +109,8 @@ __global__ void k_find_pairs(NbrParams p, const int *__restrict__ cell_atom0, co
             if (dx * dx + dy * dy + dz * dz > rc2) continue;
             const double r = dmag(dx, dy, dz);
             if (r >= rc) continue;
-            int kn[3] = {-1, -1, -1};
-            double sh[3] = {0.0, 0.0, 0.0};
+            int kn[5] = {-1, -1, -1, -1, -1};
+            double sh[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
             for (int q = 0; q < nq; ++q) {
               const double *x = p.x + p.xoff[sidx[q]];
               if (r < x[0]) {  // check_pair throws (pair_meam_spline.cpp:61-65)
@@ -124,7 +125,7 @@ __global__ void k_find_pairs(NbrParams p, const int *__restrict__ cell_atom0, co
               }
               kn[q] = knotshift(x, p.xn[sidx[q]], r, &sh[q]);
             }
-            if (kn[0] == -1 && kn[1] == -1 && kn[2] == -1) continue;
+            if (kn[0] == -1 && kn[1] == -1 && kn[2] == -1 && kn[3] == -1 && kn[4] == -1) continue;
             if (FILL) {
               const int64_t s = o + row;
               nbr[s] = a_lo + j;
@@ -132,10 +133,9 @@ __global__ void k_find_pairs(NbrParams p, const int *__restrict__ cell_atom0, co
               u_out[3 * s] = __ddiv_rn(dx, r);
               u_out[3 * s + 1] = __ddiv_rn(dy, r);
               u_out[3 * s + 2] = __ddiv_rn(dz, r);
-#pragma unroll
-              for (int q = 0; q < 3; ++q) {
-                knot_out[3 * s + q] = (int8_t)kn[q];
-                shift_out[3 * s + q] = kn[q] >= 0 ? sh[q] : 0.0;
+              for (int q = 0; q < p.nf; ++q) {
+                knot_out[p.nf * s + q] = (int8_t)kn[q];
+                shift_out[p.nf * s + q] = kn[q] >= 0 ? sh[q] : 0.0;
               }
             }
             ++row;
@@ -208,12 +208,16 @@ void build_db_device(const mz_cells_desc &c, const Pot &pot, Db &db, int device)
   NbrParams p{};
   p.natoms = N;
   p.half = style_pair(pot.style) ? 1 : 0;
-  p.nq = p.half ? 1 : meam ? 3 : 2;
+  const int nj = style_nj(pot.style);
+  p.nq = p.half ? 1 : meam ? 3 + nj : 2;
+  p.nf = db.nfun;
   p.ntypes = pot.ntypes;
   p.max_rcut = max_rcut;
   p.s[0] = pot.spline_index(G_PHI, 0);
   p.s[1] = p.half ? 0 : pot.spline_index(G_RHO, 0);
   p.s[2] = meam ? pot.spline_index(G_F, 0) : 0;
+  p.s[3] = nj > 0 ? pot.spline_index(G_P1, 0) : 0;
+  p.s[4] = nj > 1 ? pot.spline_index(G_P2, 0) : 0;
   p.x = B.upload(xs.data(), xs.size());
   p.xoff = B.upload(xoff.data(), xoff.size());
   p.xn = B.upload(xn.data(), xn.size());
@@ -263,21 +267,22 @@ void build_db_device(const mz_cells_desc &c, const Pot &pot, Db &db, int device)
   int *d_nbr = B.alloc<int>(np);
   double *d_r = B.alloc<double>(np);
   double *d_u = B.alloc<double>(3 * (size_t)np);
-  int8_t *d_kn = B.alloc<int8_t>(3 * (size_t)np);
-  double *d_sh = B.alloc<double>(3 * (size_t)np);
+  const size_t nf = (size_t)db.nfun;
+  int8_t *d_kn = B.alloc<int8_t>(nf * np);
+  double *d_sh = B.alloc<double>(nf * np);
   k_find_pairs<true><<<G, T>>>(p, d_c0, d_ac, d_lat, d_img, d_ty, d_pos, nullptr, d_off, d_nbr, d_r, d_u, d_kn, d_sh,
                                nullptr, nullptr, nullptr);
   ck(cudaGetLastError(), "pair fill launch");
   db.pair_nbr.resize(np);
   db.pair_r.resize(np);
   db.pair_u.resize(3 * (size_t)np);
-  db.pair_knot.resize(3 * (size_t)np);
-  db.pair_shift.resize(3 * (size_t)np);
+  db.pair_knot.resize(nf * np);
+  db.pair_shift.resize(nf * np);
   ck(cudaMemcpy(db.pair_nbr.data(), d_nbr, sizeof(int) * np, cudaMemcpyDeviceToHost), "pair lists D2H");
   ck(cudaMemcpy(db.pair_r.data(), d_r, sizeof(double) * np, cudaMemcpyDeviceToHost), "pair lists D2H");
   ck(cudaMemcpy(db.pair_u.data(), d_u, sizeof(double) * 3 * np, cudaMemcpyDeviceToHost), "pair lists D2H");
-  ck(cudaMemcpy(db.pair_knot.data(), d_kn, 3 * np, cudaMemcpyDeviceToHost), "pair lists D2H");
-  ck(cudaMemcpy(db.pair_shift.data(), d_sh, sizeof(double) * 3 * np, cudaMemcpyDeviceToHost), "pair lists D2H");
+  ck(cudaMemcpy(db.pair_knot.data(), d_kn, nf * np, cudaMemcpyDeviceToHost), "pair lists D2H");
+  ck(cudaMemcpy(db.pair_shift.data(), d_sh, sizeof(double) * nf * np, cudaMemcpyDeviceToHost), "pair lists D2H");
   build_incoming(db);
 }
 

@@ -38,6 +38,15 @@ def _release(obj, fn: str) -> None:
             pass
 
 
+def style_npen(style: int, ntypes: int) -> int:
+    """Punishment entries after the per-cell constraints: MEAM the f
+    magnitude, GMEAM one per f spline, JMEAM / JMEAM2 f and p (p2)
+    magnitudes, EAM U'(mid) per type, pair/spline none."""
+    return {_lib.MZ_STYLE_MEAM_SPLINE: 1, _lib.MZ_STYLE_GMEAM_SPLINE: ntypes * (ntypes + 1) // 2,
+            _lib.MZ_STYLE_JMEAM_SPLINE: 2, _lib.MZ_STYLE_JMEAM2_SPLINE: 3, _lib.MZ_STYLE_PAIR_SPLINE: 0}.get(
+        style, ntypes)
+
+
 def read_param(path: str) -> Dict[str, List[str]]:
     """Parameter file as key -> tokens (Input::parse, src/input.h:47-77: the
     first line whose first token is the key wins; blank lines are dropped)."""
@@ -130,13 +139,16 @@ class PotentialFile:
         PotEAM::rescale pot_eam.cpp:257-389) from the per-atom densities of
         the current coefficients.  Returns (rescaled, a, b): the reference's
         return value, the embedding scale factor and the MEAM f scale (0 when
-        not applied).  Evaluators built before must be re-created."""
+        not applied); the JMEAM p (p2) scales (pot_jmeam.cpp:375-401) are
+        left in self.jmeam_factors.  Evaluators built before must be
+        re-created."""
         d = np.ascontiguousarray(densities, dtype=np.float64)
         if d.size != db.stats()["natoms"]:
             raise ValueError("one density per atom expected")
         r = C.c_int()
-        f = np.zeros(2)
+        f = np.zeros(4)
         check(lib().mz_pot_rescale(self._h, db.handle, ptr(d), int(flag), C.byref(r), ptr(f)))
+        self.jmeam_factors = (float(f[2]), float(f[3]))
         return bool(r.value), float(f[0]), float(f[1])
 
     def write(self, path: str) -> None:
@@ -229,7 +241,7 @@ class Database:
         """Copies of the built arrays (CSR rows in the reference's pair order)."""
         v = _lib.DbView()
         check(lib().mz_db_get_view(self._h, C.byref(v)))
-        N, NC, Np = v.natoms, v.ncells, v.npairs
+        N, NC, Np, nf = v.natoms, v.ncells, v.npairs, v.nfun
         a = _lib.as_array
         return dict(
             ncells=NC, natoms=N, npairs=Np,
@@ -241,7 +253,7 @@ class Database:
             atom_pos=a(v.atom_pos, 3 * N, np.float64), atom_force0=a(v.atom_force0, 3 * N, np.float64),
             pair_off=a(v.pair_off, N + 1, np.int64), pair_nbr=a(v.pair_nbr, Np, np.int32),
             pair_r=a(v.pair_r, Np, np.float64), pair_u=a(v.pair_u, 3 * Np, np.float64),
-            pair_knot=a(v.pair_knot, 3 * Np, np.int8), pair_shift=a(v.pair_shift, 3 * Np, np.float64),
+            pair_knot=a(v.pair_knot, nf * Np, np.int8), pair_shift=a(v.pair_shift, nf * Np, np.float64), nfun=nf,
             in_off=a(v.in_off, N + 1, np.int64), in_slot=a(v.in_slot, Np, np.int64),
         )
 
@@ -270,9 +282,7 @@ class Evaluator:
         st = db.stats()
         self.natoms, self.ncells = st["natoms"], st["ncells"]
         self.ncoeff = pot.ncoeff
-        self.npen = (1 if pot.style == _lib.MZ_STYLE_MEAM_SPLINE else
-                     pot.ntypes * (pot.ntypes + 1) // 2 if pot.style == _lib.MZ_STYLE_GMEAM_SPLINE else
-                     0 if pot.style == _lib.MZ_STYLE_PAIR_SPLINE else pot.ntypes)
+        self.npen = style_npen(pot.style, pot.ntypes)
         self.esize = st["esize_cells"] + self.npen
 
     def __del__(self):
@@ -478,6 +488,9 @@ class Potential:
             if out is not None:
                 if b:
                     out.write("MEAM potential scaling factor %f\n" % b)
+                for name, bp in zip(("JMEAM", "JMEAM2"), pot.jmeam_factors):
+                    if bp:
+                        out.write("%s potential scaling factor %f\n" % (name, bp))
                 out.write("Embedding function scaling factor %f\n" % a)
             self.ev = Evaluator(ev.db, pot, ev.energy_weight, ev.stress_weight, ev.embed_extrap, device=ev.device,
                                 max_candidates=ev.max_candidates, omit_punishments=ev.omit_punishments)

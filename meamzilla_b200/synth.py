@@ -94,13 +94,18 @@ TEACHER = {
     "U": (lambda n: -np.sqrt(n + 1.1), lambda n: -0.5 / np.sqrt(n + 1.1)),
     "f": (lambda r: np.exp(-(r - 2.5)), lambda r: -np.exp(-(r - 2.5))),
     "g": (lambda c: 1.0 + 0.3 * c * c, lambda c: 0.6 * c),
+    # JMEAM's direct three-body terms p_ij p_ik q_i(cos) (and p2, q2)
+    "p": (lambda r: np.exp(-1.2 * (r - 2.5)), lambda r: -1.2 * np.exp(-1.2 * (r - 2.5))),
+    "q": (lambda c: 0.05 * (c + 0.3) ** 2, lambda c: 0.1 * (c + 0.3)),
+    "p2": (lambda r: np.exp(-0.8 * (r - 2.5)), lambda r: -0.8 * np.exp(-0.8 * (r - 2.5))),
+    "q2": (lambda c: -0.02 * (1.0 + c), lambda c: -0.02 + 0.0 * c),
 }
 
 
 def n_alloy(kind: str, ntypes: int, style: str = "meam/spline") -> int:
     """Number of alloy splines in a function group (src/pot_fns.cpp:403-433);
     gmeam/spline's g is Triplet_i_jk, n n (n + 1) / 2 splines (pot_gmeam.cpp:31-36)."""
-    if kind in ("phi", "f"):
+    if kind in ("phi", "f", "p", "p2"):
         return ntypes * (ntypes + 1) // 2
     if kind == "g" and style == "gmeam/spline":
         return ntypes * ntypes * (ntypes + 1) // 2
@@ -110,11 +115,13 @@ def n_alloy(kind: str, ntypes: int, style: str = "meam/spline") -> int:
 def teacher_potential(style: str, ntypes: int, rcut: float, seed: int) -> PotSpec:
     rng = np.random.default_rng(seed)
     kinds = (["phi"] if style == "pair/spline" else
-             ["phi", "rho", "U"] + (["f", "g"] if style in ("meam/spline", "gmeam/spline") else []))
+             ["phi", "rho", "U"] + (["f", "g"] if style in ("meam/spline", "gmeam/spline", "jmeam/spline",
+                                                           "jmeam2/spline") else []))
+    kinds += {"jmeam/spline": ["p", "q"], "jmeam2/spline": ["p", "q", "p2", "q2"]}.get(style, [])
     groups = []
     for kind in kinds:
         fn, dfn = TEACHER[kind]
-        if kind in ("U", "g"):
+        if kind in ("U", "g", "q", "q2"):
             left, right, n = -1.0, 1.0, 8
         else:
             left, right, n = 1.8, rcut, 10

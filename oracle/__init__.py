@@ -53,7 +53,7 @@ class _Db(C.Structure):
                 ("atom_cell", C.POINTER(C.c_int)), ("atom_force0", C.POINTER(C.c_double)),
                 ("pair_off", C.POINTER(C.c_int64)), ("pair_nbr", C.POINTER(C.c_int)),
                 ("pair_r", C.POINTER(C.c_double)), ("pair_u", C.POINTER(C.c_double)),
-                ("pair_knot", C.POINTER(C.c_int8)), ("pair_shift", C.POINTER(C.c_double))]
+                ("pair_knot", C.POINTER(C.c_int8)), ("pair_shift", C.POINTER(C.c_double)), ("nfun", C.c_int)]
 
 
 _liboracle = None
@@ -107,6 +107,7 @@ class CRestatement:
         self._v = v
         d = _Db()
         d.ncells, d.natoms, d.npairs = v["ncells"], v["natoms"], v["npairs"]
+        d.nfun = v.get("nfun", 3)
         for name, t in (("cell_atom0", C.c_int), ("cell_vol", C.c_double), ("cell_weight", C.c_double),
                         ("cell_eweight", C.c_double), ("cell_sweight", C.c_double), ("cell_energy0", C.c_double),
                         ("cell_stress0", C.c_double), ("atom_type", C.c_int), ("atom_cell", C.c_int),

@@ -147,13 +147,18 @@ int mzo_esize(const mzo_db *db, const mzo_pot *pot) {
   /* MEAM: one f punishment; GMEAM: one per f spline (pot_gmeam_spline.cpp:173-178); EAM: one per type;
    * pair/spline: neither density constraints nor punishments (pot_pair_spline.cpp:133) */
   if (pot->style == 3) return 7 * db->ncells + 3 * db->natoms;
+  /* JMEAM: f and p magnitudes; JMEAM2: f, p and p2 (pot_jmeam_spline.cpp:286-299) */
+  if (pot->style == 4 || pot->style == 5) return 8 * db->ncells + 3 * db->natoms + (pot->style == 4 ? 2 : 3);
   return 8 * db->ncells + 3 * db->natoms +
          (pot->style == 1 ? 1 : pot->style == 2 ? pot->ntypes * (pot->ntypes + 1) / 2 : pot->ntypes);
 }
 
 double mzo_objective(const mzo_db *db, const mzo_pot *pot, const double *coeffs, double *errvec_out,
                      double *forces_out, double *energy_out, double *stress_out, double *dens_out) {
-  const int meam = pot->style == 1 || pot->style == 2, gmeam = pot->style == 2, pairpot = pot->style == 3;
+  const int meam = pot->style == 1 || pot->style == 2 || pot->style == 4 || pot->style == 5;
+  const int gmeam = pot->style == 2, pairpot = pot->style == 3;
+  const int nj = pot->style == 4 ? 1 : pot->style == 5 ? 2 : 0; /* (p, q) pairs of JMEAM / JMEAM2 */
+  const int nf = db->nfun;
   const int nt = pot->ntypes, npair = nt * (nt + 1) / 2;
   const int N = db->natoms, NC = db->ncells;
   int s, ci = 0, i;
@@ -161,6 +166,13 @@ double mzo_objective(const mzo_db *db, const mzo_pot *pot, const double *coeffs,
   for (s = 0; s < pot->nsplines; ++s) sp_setup(&sp[s], &pot->splines[s], coeffs, &ci);
   const sp_t *phi = sp, *rho = pairpot ? NULL : sp + npair, *U = pairpot ? NULL : sp + npair + nt;
   const sp_t *ff = meam ? sp + npair + 2 * nt : NULL, *gg = meam ? sp + 2 * npair + 2 * nt : NULL;
+  /* JMEAM groups after g: p (Pair_ij), q (Triplet_i) [, p2, q2] (pot_jmeam.cpp:31-45) */
+  const sp_t *pp[2] = {NULL, NULL}, *qq[2] = {NULL, NULL};
+  int m;
+  for (m = 0; m < nj; ++m) {
+    pp[m] = sp + 2 * npair + 3 * nt + m * (npair + nt);
+    qq[m] = pp[m] + npair;
+  }
 
   /* initialize_compute (potential.cpp:388-408) */
   double *energy = (double *)calloc(NC, sizeof(double));
@@ -175,7 +187,10 @@ double mzo_objective(const mzo_db *db, const mzo_pot *pot, const double *coeffs,
   double *drho = (double *)calloc(maxrow + 1, sizeof(double));
   double *fv = (double *)calloc(maxrow + 1, sizeof(double));
   double *dfv = (double *)calloc(maxrow + 1, sizeof(double));
+  double *pv = (double *)calloc(2 * (size_t)(maxrow + 1), sizeof(double));
+  double *dpv = (double *)calloc(2 * (size_t)(maxrow + 1), sizeof(double));
   size_t maxtrip = (size_t)maxrow * (maxrow > 0 ? maxrow - 1 : 0) / 2 + 1;
+  double *tq = (double *)malloc(sizeof(double) * 2 * maxtrip), *tdq = (double *)malloc(sizeof(double) * 2 * maxtrip);
   int *tj_ = (int *)malloc(sizeof(int) * maxtrip), *tk_ = (int *)malloc(sizeof(int) * maxtrip);
   double *tg = (double *)malloc(sizeof(double) * maxtrip), *tdg = (double *)malloc(sizeof(double) * maxtrip);
   double *tcos = (double *)malloc(sizeof(double) * maxtrip);
@@ -192,19 +207,19 @@ double mzo_objective(const mzo_db *db, const mzo_pot *pot, const double *coeffs,
       const int64_t q = p0 + p;
       const int j = db->pair_nbr[q], tj = db->atom_type[j];
       const double *u = db->pair_u + 3 * q, r = db->pair_r[q];
-      const int kphi = db->pair_knot[3 * q], krho = db->pair_knot[3 * q + 1], kf = db->pair_knot[3 * q + 2];
+      const int kphi = db->pair_knot[nf * q], krho = db->pair_knot[nf * q + 1], kf = db->pair_knot[nf * q + 2];
       double *Fj = force + 3 * (size_t)j;
       if (kphi != -1) {
         double phigrad, tmp[3], tr[3], phival;
         if (pairpot) {
           /* each pair once; half for an image of atom i itself (pot_pair_spline.cpp:100-113) */
-          phival = sp_comb_k(&phi[pair_ij(nt, ti, tj)], kphi, db->pair_shift[3 * q], &phigrad);
+          phival = sp_comb_k(&phi[pair_ij(nt, ti, tj)], kphi, db->pair_shift[nf * q], &phigrad);
           if (j == i) {
             phival *= 0.5;
             phigrad *= 0.5;
           }
         } else {
-          phival = 0.5 * sp_comb_k(&phi[pair_ij(nt, ti, tj)], kphi, db->pair_shift[3 * q], &phigrad);
+          phival = 0.5 * sp_comb_k(&phi[pair_ij(nt, ti, tj)], kphi, db->pair_shift[nf * q], &phigrad);
           phigrad *= 0.5;
         }
         energy[cell] += phival;
@@ -216,11 +231,17 @@ double mzo_objective(const mzo_db *db, const mzo_pot *pot, const double *coeffs,
         S[0] -= u[0] * tr[0]; S[1] -= u[1] * tr[1]; S[2] -= u[2] * tr[2];
         S[3] -= u[0] * tr[1]; S[4] -= u[1] * tr[2]; S[5] -= u[2] * tr[0];
       }
-      if (!pairpot && krho != -1) rho_val += sp_comb_k(&rho[tj], krho, db->pair_shift[3 * q + 1], &drho[p]);
+      if (!pairpot && krho != -1) rho_val += sp_comb_k(&rho[tj], krho, db->pair_shift[nf * q + 1], &drho[p]);
       else drho[p] = 0.0;
       if (meam) {
-        if (kf != -1) fv[p] = sp_comb_k(&ff[pair_ij(nt, ti, tj)], kf, db->pair_shift[3 * q + 2], &dfv[p]);
+        if (kf != -1) fv[p] = sp_comb_k(&ff[pair_ij(nt, ti, tj)], kf, db->pair_shift[nf * q + 2], &dfv[p]);
         else fv[p] = dfv[p] = 0.0;
+      }
+      for (m = 0; m < nj; ++m) { /* p (p2): pot_jmeam_spline.cpp:196-202 */
+        const int kp = db->pair_knot[nf * q + 3 + m];
+        if (kp != -1) pv[2 * p + m] = sp_comb_k(&pp[m][pair_ij(nt, ti, tj)], kp, db->pair_shift[nf * q + 3 + m],
+                                                &dpv[2 * p + m]);
+        else pv[2 * p + m] = dpv[2 * p + m] = 0.0;
       }
     }
     if (meam) {
@@ -236,14 +257,29 @@ double mzo_objective(const mzo_db *db, const mzo_pot *pot, const double *coeffs,
                                 : &gg[ti];
           const double *uj = db->pair_u + 3 * (p0 + j), *uk = db->pair_u + 3 * (p0 + k);
           double c = uj[0] * uk[0] + uj[1] * uk[1] + uj[2] * uk[2];
-          double gs;
-          int gk = sp_knotshift(g, c, &gs);
-          if (gk == -1) continue;
+          double gs, qs[2];
+          int gk = sp_knotshift(g, c, &gs), qk[2] = {-1, -1}, anyq = 0;
+          for (m = 0; m < nj; ++m) {
+            qk[m] = sp_knotshift(&qq[m][ti], c, &qs[m]);
+            anyq |= qk[m] != -1;
+          }
+          /* TripletJMEAMSpline::check_triplet (triplet_jmeam_spline.cpp:49-86): a
+           * triplet when g or q has a knot.  Where one of them has none the
+           * reference evaluates that spline at knot -1 (out of its table); here
+           * that term is zero. */
+          if (gk == -1 && !anyq) continue;
           tj_[ntrip] = j;
           tk_[ntrip] = k;
           tcos[ntrip] = c;
-          tg[ntrip] = sp_comb_k(g, gk, gs, &tdg[ntrip]);
+          if (gk != -1) tg[ntrip] = sp_comb_k(g, gk, gs, &tdg[ntrip]);
+          else tg[ntrip] = tdg[ntrip] = 0.0;
+          for (m = 0; m < nj; ++m) {
+            if (qk[m] != -1) tq[2 * ntrip + m] = sp_comb_k(&qq[m][ti], qk[m], qs[m], &tdq[2 * ntrip + m]);
+            else tq[2 * ntrip + m] = tdq[2 * ntrip + m] = 0.0;
+          }
           rho_val += fv[j] * fv[k] * tg[ntrip];
+          /* pot_jmeam_spline.cpp:216-219 */
+          for (m = 0; m < nj; ++m) energy[cell] += pv[2 * j + m] * pv[2 * k + m] * tq[2 * ntrip + m];
           ++ntrip;
         }
     }
@@ -288,6 +324,12 @@ double mzo_objective(const mzo_db *db, const mzo_pot *pot, const double *coeffs,
       double dV3j = tg[t] * dfv[j] * fv[k] * dF;
       double dV3k = tg[t] * fv[j] * dfv[k] * dF;
       double V3 = tdg[t] * fv[j] * fv[k] * dF;
+      /* pot_jmeam_spline.cpp:263-265 */
+      for (m = 0; m < nj; ++m) {
+        dV3j += tq[2 * t + m] * dpv[2 * j + m] * pv[2 * k + m];
+        dV3k += tq[2 * t + m] * pv[2 * j + m] * dpv[2 * k + m];
+        V3 += tdq[2 * t + m] * pv[2 * j + m] * pv[2 * k + m];
+      }
       double vlj = V3 * invrj, vlk = V3 * invrk;
       double vv3j = dV3j - vlj * tcos[t], vv3k = dV3k - vlk * tcos[t];
       double dfj[3], dfk[3];
@@ -357,19 +399,24 @@ double mzo_objective(const mzo_db *db, const mzo_pot *pot, const double *coeffs,
     }
   } else if (meam) {
     /* pot_meam_spline.cpp:274-278 with PotFns::get_max_y_mag (pot_fns.cpp:223-234)
-     * and Spline::get_max_y_mag (spline.cpp:58-67) */
-    double my = 0.0;
-    int f, k;
-    for (f = 0; f < npair; ++f) {
-      double m = 0.0;
-      for (k = 0; k < ff[f].n; ++k)
-        if (fabs(m) < fabs(ff[f].y[k])) m = ff[f].y[k];
-      if (fabs(my) < fabs(m)) my = m;
+     * and Spline::get_max_y_mag (spline.cpp:58-67); JMEAM adds the same for
+     * p (and p2), pot_jmeam_spline.cpp:286-299 */
+    int grp;
+    for (grp = 0; grp <= nj; ++grp) {
+      const sp_t *G = grp == 0 ? ff : pp[grp - 1];
+      double my = 0.0;
+      int f, k;
+      for (f = 0; f < npair; ++f) {
+        double mm = 0.0;
+        for (k = 0; k < G[f].n; ++k)
+          if (fabs(mm) < fabs(G[f].y[k])) mm = G[f].y[k];
+        if (fabs(my) < fabs(mm)) my = mm;
+      }
+      double mag = fabs(my);
+      double fe = DUMMY_WEIGHT * 25. * (1.0 - mag) * (1.0 - mag);
+      sum += fe * fe;
+      ev[idx++] = fe;
     }
-    double mag = fabs(my);
-    double fe = DUMMY_WEIGHT * 25. * (1.0 - mag) * (1.0 - mag);
-    sum += fe * fe;
-    ev[idx++] = fe;
   } else {
     /* pot_eam_spline.cpp:211-218 */
     int t;
@@ -388,7 +435,7 @@ double mzo_objective(const mzo_db *db, const mzo_pot *pot, const double *coeffs,
 
   free(ev);
   free(tj_); free(tk_); free(tg); free(tdg); free(tcos);
-  free(drho); free(fv); free(dfv);
+  free(drho); free(fv); free(dfv); free(pv); free(dpv); free(tq); free(tdq);
   free(energy); free(stress); free(force); free(constraint);
   for (s = 0; s < pot->nsplines; ++s) sp_free(&sp[s]);
   free(sp);

@@ -1,6 +1,6 @@
 /*
  * mz_oracle.h -- TEST ORACLE.  A plain-C, FP64, single-threaded restatement
- * of the reference's objective for the spline EAM/MEAM/GMEAM/pair styles.  It exists to
+ * of the reference's objective for the spline EAM/MEAM/GMEAM/JMEAM/pair styles.  It exists to
  * check the CUDA evaluator: only tests, the smoke check and the benchmark's
  * CPU-baseline leg call it.  The product never links it.
  *
@@ -9,6 +9,8 @@
  *   PotEAMSpline::fast_compute    src/pots/pot_eam_spline/pot_eam_spline.cpp:100-223
  *   PotGMEAMSpline::fast_compute  src/pots/pot_gmeam_spline/pot_gmeam_spline.cpp:103-290
  *   PotPairSpline::fast_compute   src/pots/pot_pair_spline/pot_pair_spline.cpp:71-139
+ *   PotJMEAMSpline::fast_compute  src/pots/pot_jmeam_spline/pot_jmeam_spline.cpp:103-306
+ *   PotJMEAM2Spline::fast_compute src/pots/pot_jmeam2_spline/pot_jmeam2_spline.cpp
  *   Potential::accumulate_error   src/potential.cpp:415-491
  *   Spline3Eq::refresh_basis      src/spline3eq.cpp:192-225
  *   Spline3Eq::splint_comb        src/spline3eq.h:110-122, 204-236
@@ -39,7 +41,8 @@ typedef struct {
 } mzo_spline;
 
 typedef struct {
-  int style;     /* 0 eam/spline, 1 meam/spline, 2 gmeam/spline, 3 pair/spline */
+  int style;     /* 0 eam/spline, 1 meam/spline, 2 gmeam/spline, 3 pair/spline, 4 jmeam/spline,
+                    5 jmeam2/spline */
   int ntypes;
   int nsplines;  /* group-major: phi, rho, U [, f, g] */
   const mzo_spline *splines;
@@ -57,8 +60,9 @@ typedef struct {
   const int64_t *pair_off;
   const int *pair_nbr;
   const double *pair_r, *pair_u;  /* u [npairs][3] */
-  const int8_t *pair_knot;        /* [npairs][3] phi rho f */
-  const double *pair_shift;       /* [npairs][3] */
+  const int8_t *pair_knot;        /* [npairs][nfun] phi rho f (p p2) */
+  const double *pair_shift;       /* [npairs][nfun] */
+  int nfun;                       /* radial functions per slot: phi, rho, f (+ p, p2) */
 } mzo_db;
 
 /* Objective of the coefficient vector `coeffs` (Potential::coeff order).

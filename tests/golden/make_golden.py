@@ -10,7 +10,7 @@ through Potential::compute for two coefficient vectors:
     fdgrad (central differences of the objective, h = 1e-6; small cases)
 
 Run here (needs the reference sources to build mzref):
-    make -C oracle && python tests/golden/make_golden.py [--gmeam | --grad10 | --pair]
+    make -C oracle && python tests/golden/make_golden.py [--gmeam | --grad10 | --pair | --jmeam]
 """
 from __future__ import annotations
 
@@ -117,6 +117,27 @@ def pair_goldens():
     pot.groups[0][2].fixed = np.zeros(10, dtype=int)
     pot.groups[0][2].fixed[[2, 7]] = 1
     _write("pair_mix2", pot, cells, fd=True, energy_weight=2.0, stress_weight=0.5)
+
+
+JMEAM_CASES = ["jmeam_inrange1", "jmeam_mix2", "jmeam2_mix2"]
+
+
+def jmeam_goldens():
+    """jmeam/spline and jmeam2/spline: MEAM + sum_{j<k} p_ij p_ik q_i(cos)
+    (and a second such term) in the energy, f and p magnitude punishments."""
+    # 10. one species, densities in range (rho and f scaled), per-cell weights
+    _, cells = synth.make_workload("meam200", seed=15, ncells=4)
+    _targets(cells, 10)
+    for i, c in enumerate(cells):
+        c.weight = 1.0 + 0.2 * i
+    pot = synth.teacher_potential("jmeam/spline", 1, 4.5, seed=25)
+    _write(JMEAM_CASES[0], in_range_meam(pot), cells, fd=True, energy_weight=1.5, stress_weight=0.8)
+    # 11./12. two species, cells of the two-species rule, teacher as generated
+    _, cells = synth.make_workload("meam2k", seed=16, ncells=4)
+    cells = [c for c in cells if c.natoms <= 300][:3] or cells[:1]
+    _targets(cells, 11)
+    _write(JMEAM_CASES[1], synth.teacher_potential("jmeam/spline", 2, 5.5, seed=26), cells, fd=True)
+    _write(JMEAM_CASES[2], synth.teacher_potential("jmeam2/spline", 2, 5.5, seed=27), cells, fd=True)
 
 
 def data_goldens(names=None):
@@ -234,6 +255,11 @@ if __name__ == "__main__":
     import sys
     if "--grad10" in sys.argv:
         grad10_goldens()
+        sys.exit(0)
+    if "--jmeam" in sys.argv:
+        jmeam_goldens()
+        rescale_goldens(JMEAM_CASES)
+        data_goldens(JMEAM_CASES)
         sys.exit(0)
     if "--pair" in sys.argv:
         pair_goldens()

@@ -51,7 +51,8 @@ def test_fp64_gradient_vs_finite_differences(name):
         assert _err(grad[0], g["fdgrad"]) <= GRAD_REF_FD
 
 
-@pytest.mark.parametrize("name", ["meam_mix6", "meam2_edge", "eam_bcc3", "pair_mix2"])
+@pytest.mark.parametrize("name", ["meam_mix6", "meam2_edge", "eam_bcc3", "pair_mix2", "jmeam_inrange1",
+                                  "jmeam2_mix2"])
 def test_mixed_gradient_vs_fp64(name):
     from meamzilla_b200.potential import MZ_FP64, MZ_MIXED, Evaluator
     case = load_case(name)

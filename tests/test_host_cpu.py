@@ -102,7 +102,7 @@ def test_missing_files_are_io_errors(tmp_path):
 @pytest.mark.parametrize("text,status,phrase", [
     ("comment\n#X eam/spline 1\n", 3, "#T"),
     ("comment\n#T eam/spline 1\n#B spline3eq\n", 3, "#P"),
-    ("comment\n#T jmeam/spline 1\n#P\n", 5, "not implemented"),
+    ("comment\n#T meam 1\n#P\n", 5, "not implemented"),
     ("comment\n#T eam/spline 1\n#P\n#B spline5eq\n1 2 3\n", 5, "spline5eq"),
     ("comment\n#T eam/spline 1\n#P\n#B spline3eq\n1.8 5.0 10\n0 7\n1 1\n0 1\n", 3, "constraint"),
     ("comment\n#T eam/spline 1\n#P\n#B spline3eq\n1.8 5.0 4\n0 0\n1 1\n0 1\n0 x\n", 3, "knot line"),
