@@ -99,7 +99,8 @@ mz_status mz_pot_set_coeffs(mz_pot *pot, const double *coeffs);
 mz_status mz_pot_write(const mz_pot *pot, const char *path);
 /* Evaluate spline s of the potential at x: value and slope.  Mirrors
  * Spline3Eq::splint_comb(double, double*) (spline3eq.h:204-236), linear
- * extrapolation outside the knots.  Host-side, for tests and tools. */
+ * extrapolation outside the knots (spline5eq: spline5eq.h:226-255, quadratic
+ * outside).  Host-side, for tests and tools. */
 mz_status mz_pot_spline_eval(const mz_pot *pot, int spline, double x, double *val, double *grad);
 
 /* Potential::rescale (src/potential.h:68) for the spline styles, in place:
@@ -216,6 +217,8 @@ typedef struct {
   const double *y;
   const double *x;    /* knot positions [nknots] (rescale moves them)  */
   double step;        /* knot spacing                                   */
+  int quintic;        /* spline5eq basis (spline5eq.cpp)                */
+  double grad2[2];    /* spline5eq: y'' at the ends                      */
 } mz_spline_view;
 mz_status mz_pot_get_spline(const mz_pot *pot, int spline, mz_spline_view *view);
 

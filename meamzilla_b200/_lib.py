@@ -74,7 +74,8 @@ class SplineView(C.Structure):
     _fields_ = [("group", C.c_int), ("alloy", C.c_int), ("nknots", C.c_int), ("left", C.c_double),
                 ("right", C.c_double), ("nat", C.c_int * 2), ("grad_fixed", C.c_int * 2),
                 ("grad", C.c_double * 2), ("y_fixed", C.POINTER(C.c_int)), ("y", C.POINTER(C.c_double)),
-                ("x", C.POINTER(C.c_double)), ("step", C.c_double)]
+                ("x", C.POINTER(C.c_double)), ("step", C.c_double), ("quintic", C.c_int),
+                ("grad2", C.c_double * 2)]
 
 
 class Settings(C.Structure):

@@ -71,6 +71,7 @@ struct mz_ctx {
   int *d_err = nullptr;                         // device-side failure flag (bounded waits)
   TcParams tc{};                                // tensor-core forward plan
   bool tc_ok = false;
+  bool q5 = false;  // spline5eq potential: objective only (no adjoint)
   int nsm = 1;
   // Kernel sequences of the host-buffer entry points captured as CUDA graphs,
   // one per (candidates, precision, outputs); replayed on later calls.
@@ -182,6 +183,13 @@ struct Bracket {
 template <bool MEAM, typename R, bool AUX>
 void launch_atoms(mz_ctx *ctx, int n, size_t smem) {
   dim3 ga(ctx->db.nblocks, n);
+  if constexpr (!AUX) {
+    if (ctx->q5) {  // spline5eq pieces (objective only)
+      k_atoms<MEAM, R, false, false, false, true><<<ga, BLOCK_SLOTS, smem, ctx->stream>>>(
+          ctx->db, ctx->pot, ctx->d_geom, ctx->d_tabs, ctx->d_ptabs, ctx->d_V, ctx->d_aout, ctx->d_aux);
+      return;
+    }
+  }
   if constexpr (MEAM) {
     if (ctx->pot.nj > 0) {
       k_atoms<MEAM, R, AUX, false, true><<<ga, BLOCK_SLOTS, smem, ctx->stream>>>(
@@ -232,7 +240,7 @@ void enqueue(mz_ctx *ctx, int n, const double *d_params, int precision, double *
     k_prep<<<n, std::max(32, ((ctx->nsplines + 31) / 32) * 32), 0, st>>>(
         n, ctx->P, d_params, ctx->d_base, ctx->d_cmap, ctx->d_geom, ctx->d_nat, ctx->nsplines, ctx->stride,
         ctx->d_tabs, ctx->pstride, ctx->d_ptabs, ctx->d_ptabf, ctx->tc_ok ? ctx->d_wtab : nullptr, ctx->pot.s_g,
-        ctx->pot.ntypes, TC_NB);
+        ctx->pot.ntypes, TC_NB, ctx->d_M);
     ck(cudaGetLastError(), "k_prep launch");
   }
   {
@@ -329,6 +337,27 @@ void refresh_matrix(const Spline3 &sp, std::vector<double> &M) {
     else s.grad[col - n] = 1.0;
     s.refresh(ypp);
     for (int r = 0; r < n; ++r) M[(size_t)r * (n + 2) + col] = ypp[r];
+  }
+}
+
+// d(ypp, yp4)/d(y, slope_left, slope_right, y''_left, y''_right) of one
+// spline5eq spline, [2n][n+4]: Spline5Eq::refresh_basis is linear in them.
+void refresh_matrix5(const Spline3 &sp, std::vector<double> &M) {
+  const int n = sp.nknots, nc = n + 4;
+  M.assign((size_t)2 * n * nc, 0.0);
+  Spline3 s = sp;
+  std::vector<double> ypp, yp4;
+  for (int col = 0; col < nc; ++col) {
+    std::fill(s.y.begin(), s.y.end(), 0.0);
+    s.grad[0] = s.grad[1] = s.grad2[0] = s.grad2[1] = 0.0;
+    if (col < n) s.y[col] = 1.0;
+    else if (col < n + 2) s.grad[col - n] = 1.0;
+    else s.grad2[col - n - 2] = 1.0;
+    s.refresh5(ypp, yp4);
+    for (int r = 0; r < n; ++r) {
+      M[(size_t)r * nc + col] = ypp[r];
+      M[(size_t)(n + r) * nc + col] = yp4[r];
+    }
   }
 }
 
@@ -467,14 +496,16 @@ mz_status mz_create(const mz_db *dbh, const mz_pot *poth, const mz_settings *set
       for (int u = 0; u < 4; ++u) cf = std::nextafter(cf, INFINITY);
       g.cutf = cf;
       g.n = sp.nknots;
+      g.q5 = sp.quintic;
       g.toff = toff;
-      toff += 2 * sp.nknots + 2;
+      toff += (sp.quintic ? 3 : 2) * sp.nknots + (sp.quintic ? 4 : 2);
       g.poff = poff;
-      poff += 4 * (sp.nknots - 1);
+      poff += (sp.quintic ? 6 : 4) * (sp.nknots - 1);
       nat[2 * s] = sp.nat[0];
       nat[2 * s + 1] = sp.nat[1];
       std::vector<double> M;
-      refresh_matrix(sp, M);
+      if (sp.quintic) refresh_matrix5(sp, M);
+      else refresh_matrix(sp, M);
       g.moff = (int)Mall.size();
       Mall.insert(Mall.end(), M.begin(), M.end());
     }
@@ -482,20 +513,25 @@ mz_status mz_create(const mz_db *dbh, const mz_pot *poth, const mz_settings *set
     ctx->pstride = poff;
     std::vector<double> base(stride, 0.0);
     std::vector<int> cmap(stride, -1);
-    int ci = 0;
     for (int s = 0; s < ns; ++s) {
       const Spline3 &sp = pot.spline(s);
       const int o = geom[s].toff, n = sp.nknots;
-      for (int k = 0; k < n; ++k) {
-        base[o + k] = sp.y[k];
-        if (!sp.y_fixed[k]) cmap[o + k] = ci++;
-      }
-      for (int e = 0; e < 2; ++e) {
-        base[o + 2 * n + e] = sp.grad[e];
-        if (!sp.grad_fixed[e] && !sp.nat[e]) cmap[o + 2 * n + e] = ci++;
-      }
+      for (int k = 0; k < n; ++k) base[o + k] = sp.y[k];
+      for (int e = 0; e < 2; ++e) base[o + 2 * n + e] = sp.grad[e];
+      if (sp.quintic)
+        for (int e = 0; e < 2; ++e) base[o + 3 * n + 2 + e] = sp.grad2[e];
+    }
+    // coefficient i -> table entry, in Potential::coeff's order
+    int ci = 0;
+    for (auto &cs : pot.coeff_slots()) {
+      const int o = geom[cs.first].toff, n = geom[cs.first].n, slot = cs.second;
+      const int at = slot < n ? o + slot : slot < n + 2 ? o + 2 * n + (slot - n) : o + 3 * n + 2 + (slot - n - 2);
+      cmap[at] = ci++;
     }
     ctx->P = ci;
+    ctx->q5 = ns > 0 && pot.spline(0).quintic;
+    if (ctx->q5 && (style_meam(pot.style) && pot.style != MZ_STYLE_MEAM_SPLINE))
+      throw Failure{MZ_ERR_UNSUPPORTED, "spline5eq is implemented for eam/spline, meam/spline and pair/spline"};
     ctx->nsplines = ns;
     ctx->stride = stride;
     ctx->d_geom = dupload(ctx, geom.data(), ns);
@@ -675,6 +711,10 @@ mz_status mz_create(const mz_db *dbh, const mz_pot *poth, const mz_settings *set
     smem_attr(k_atoms<true, float, true, false, true>, ctx->smem_atoms[1]);
     smem_attr(k_adj<true, double, false, true>, ctx->smem_adj[0]);
     smem_attr(k_adj<true, float, false, true>, ctx->smem_adj[1]);
+    smem_attr(k_atoms<true, double, false, false, false, true>, ctx->smem_atoms[0]);
+    smem_attr(k_atoms<false, double, false, false, false, true>, ctx->smem_atoms[0]);
+    smem_attr(k_atoms<true, float, false, false, false, true>, ctx->smem_atoms[1]);
+    smem_attr(k_atoms<false, float, false, false, false, true>, ctx->smem_atoms[1]);
     int nsm = 0, per_sm = 0;
     ck(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, ctx->device), "attribute");
     ck(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_adj<true, float>, BLOCK_SLOTS, ctx->smem_adj[1]),
@@ -690,7 +730,8 @@ mz_status mz_create(const mz_db *dbh, const mz_pot *poth, const mz_settings *set
       const char *env = std::getenv("MZ_TC");  // opt-in: "1"
       const bool allowed = env && env[0] == '1';
       ctx->tc = tc_plan(db.max_row, TC_NB, pot.ntypes, ns, smem_max);
-      ctx->tc_ok = allowed && pot.style == MZ_STYLE_MEAM_SPLINE && ng + 2 == TC_NB && ctx->tc.smem_bytes > 0;
+      ctx->tc_ok =
+          allowed && pot.style == MZ_STYLE_MEAM_SPLINE && !ctx->q5 && ng + 2 == TC_NB && ctx->tc.smem_bytes > 0;
       if (ctx->tc_ok) {
         smem_attr(k_atoms_tc<TC_NB, false>, (size_t)ctx->tc.smem_bytes);
         smem_attr(k_atoms_tc<TC_NB, true>, (size_t)ctx->tc.smem_bytes);
@@ -751,6 +792,7 @@ mz_status mz_objective(mz_ctx *ctx, int ncand, const double *params, int precisi
 mz_status mz_objective_grad(mz_ctx *ctx, int ncand, const double *params, int precision, double *obj, double *grad) {
   return guarded([&] {
     if (!grad) throw Failure{MZ_ERR_ARG, "null gradient buffer"};
+    if (ctx && ctx->q5) throw Failure{MZ_ERR_UNSUPPORTED, "the gradient is not implemented for spline5eq potentials"};
     run_host(ctx, ncand, params, precision, obj, nullptr, nullptr, nullptr, nullptr, grad);
   });
 }
@@ -772,6 +814,7 @@ mz_status mz_objective_grad_device(mz_ctx *ctx, int ncand, const double *d_param
                                    double *d_grad) {
   return guarded([&] {
     if (!ctx || !d_params || !d_obj || !d_grad || ncand <= 0) throw Failure{MZ_ERR_ARG, "bad argument"};
+    if (ctx->q5) throw Failure{MZ_ERR_UNSUPPORTED, "the gradient is not implemented for spline5eq potentials"};
     if (ncand > ctx->cand_cap)
       throw Failure{MZ_ERR_RANGE,
                     "ncand exceeds the candidates one launch can hold (" + std::to_string(ctx->cand_cap) + ")"};
@@ -917,9 +960,9 @@ extern "C" mz_status mz_objective_noalloc(const mz_db *dbh, const mz_pot *poth, 
     const Db &db = dbh->db;
     const Pot &pot = poth->pot;
     const bool meam = pot.style == MZ_STYLE_MEAM_SPLINE;
-    if (pot.style == MZ_STYLE_GMEAM_SPLINE || style_nj(pot.style) > 0)
+    if (pot.style == MZ_STYLE_GMEAM_SPLINE || style_nj(pot.style) > 0 || (pot.nsplines() && pot.spline(0).quintic))
       throw Failure{MZ_ERR_UNSUPPORTED,
-                    "the no-allocation objective supports eam/spline, meam/spline and pair/spline"};
+                    "the no-allocation objective supports eam/spline, meam/spline and pair/spline with spline3eq"};
     if (style_pair(db.style) != style_pair(pot.style) || (meam && !style_meam(db.style)))
       throw Failure{MZ_ERR_ARG, "the database's lists were built for another potential style"};
     if (db.max_row > BLOCK_SLOTS)

@@ -21,14 +21,18 @@ struct SplineGeom {
   int n;        // knots
   int toff;     // offset of this spline in a candidate's table
   int moff;     // offset of its refresh matrix d(ypp)/d(y, grad) [n][n+2]
-  int poff;     // offset of its per-interval cubic coefficients [n-1][4]
+                // (spline5eq: d(ypp, y'''')/d(y, grad, y''_end) [2n][n+4])
+  int poff;     // offset of its per-interval polynomial coefficients [n-1][4] (spline5eq [n-1][6])
+  int q5;       // spline5eq (quintic pieces)
 };
 
-// A candidate's table, per spline at toff: y[n], ypp[n], grad[2]
-// (total tab_stride doubles per candidate).  Its evaluation table, per spline
-// at poff: for each knot interval k the cubic in the shift b,
+// A candidate's table, per spline at toff: y[n], ypp[n], grad[2], and for
+// spline5eq also yp4[n] (y''''), grad2[2] (y'' at the ends) (total tab_stride
+// doubles per candidate).  Its evaluation table, per spline at poff: for each
+// knot interval k the polynomial in the shift b,
 //   S = c0 + b (c1 + b (c2 + b c3)),   dS/dr = (c1 + b (2 c2 + 3 b c3)) / h,
-// (pow_stride doubles per candidate), computed in FP64 from y and ypp.
+// (quintic: six coefficients, the same Horner form) (pow_stride doubles per
+// candidate), computed in FP64 from y, ypp (and yp4).
 
 struct DevDb {
   int ncells, natoms, nblocks;

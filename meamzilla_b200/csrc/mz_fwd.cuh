@@ -23,7 +23,8 @@ __global__ void k_prep(int ncand, int P, const double *__restrict__ params, cons
                        const int *__restrict__ cmap, const SplineGeom *__restrict__ geom,
                        const int *__restrict__ nat, int nsplines, int stride, double *__restrict__ tabs,
                        int pstride, double *__restrict__ ptabs, float *__restrict__ ptabf = nullptr,
-                       float *__restrict__ wtab = nullptr, int s_g = 0, int ng = 0, int nbp = 0) {
+                       float *__restrict__ wtab = nullptr, int s_g = 0, int ng = 0, int nbp = 0,
+                       const double *__restrict__ M = nullptr) {
   const int c = blockIdx.x;
   const int s = threadIdx.x;
   if (c >= ncand || s >= nsplines) return;
@@ -35,6 +36,40 @@ __global__ void k_prep(int ncand, int P, const double *__restrict__ params, cons
   const int n = g.n;
   for (int k = 0; k < n; ++k) t[k] = cm[k] >= 0 ? pc[cm[k]] : bt[k];
   for (int e = 0; e < 2; ++e) t[2 * n + e] = cm[2 * n + e] >= 0 ? pc[cm[2 * n + e]] : bt[2 * n + e];
+  if (g.q5) {
+    // spline5eq: y'' at the ends, then (ypp, yp4) = M (y, grad, grad2) -- the
+    // refresh of Spline5Eq::refresh_basis (spline5eq.cpp:209-293) is linear
+    // in them; M is solved once on the host
+    double *g2 = t + 3 * n + 2, *yp4 = t + 2 * n + 2;
+    for (int e = 0; e < 2; ++e) g2[e] = cm[3 * n + 2 + e] >= 0 ? pc[cm[3 * n + 2 + e]] : bt[3 * n + 2 + e];
+    const double *Ms = M + g.moff;
+    const int nc = n + 4;
+    for (int r = 0; r < 2 * n; ++r) {
+      const double *row = Ms + (size_t)r * nc;
+      double acc = 0.0;
+      for (int c = 0; c < n; ++c) acc += row[c] * t[c];
+      acc += row[n] * t[2 * n] + row[n + 1] * t[2 * n + 1] + row[n + 2] * g2[0] + row[n + 3] * g2[1];
+      if (r < n) t[n + r] = acc;
+      else yp4[r - n] = acc;
+    }
+    double *pc6 = ptabs + (size_t)c * pstride + g.poff;
+    const double H2 = g.step * g.step / 6.0, H4 = g.step * g.step * g.step * g.step / 360.0;
+    for (int k = 0; k < n - 1; ++k) {
+      const double p1 = t[k], p2 = t[k + 1], d21 = t[n + k], d22 = t[n + k + 1], d41 = yp4[k], d42 = yp4[k + 1];
+      double *q = pc6 + 6 * k;
+      q[0] = p1;
+      q[1] = p2 - p1 + H2 * (-2.0 * d21 - d22) + H4 * (8.0 * d41 + 7.0 * d42);
+      q[2] = 3.0 * H2 * d21;
+      q[3] = H2 * (d22 - d21) + H4 * (-20.0 * d41 - 10.0 * d42);
+      q[4] = 15.0 * H4 * d41;
+      q[5] = H4 * (3.0 * d42 - 3.0 * d41);
+    }
+    if (ptabf) {
+      float *pf = ptabf + (size_t)c * pstride + g.poff;
+      for (int k = 0; k < 6 * (n - 1); ++k) pf[k] = (float)pc6[k];
+    }
+    return;
+  }
   // Spline3Eq::refresh_basis (spline3eq.cpp:192-225)
   double u[64];
   double *y = t, *ypp = t + n;
@@ -142,7 +177,7 @@ struct PairEval {
   int kp[2];
 };
 
-template <bool MEAM, typename R>
+template <bool MEAM, typename R, bool Q5 = false>
 __device__ __forceinline__ PairEval<MEAM, R> eval_pair(const DevDb &db, const DevPot &pot, const SplineGeom *sg,
                                                       const R *ptab, int64_t gs, int ti) {
   PairEval<MEAM, R> p;
@@ -164,17 +199,17 @@ __device__ __forceinline__ PairEval<MEAM, R> eval_pair(const DevDb &db, const De
   if (p.kphi >= 0) {
     const SplineGeom &g = sg[pot.s_phi + p.pij];
     p.bphi = sizeof(R) == 8 ? (R)db.pair_shift[gs] : (R)db.pair_shiftf[gs];
-    p.phi = cubic_val_grad<R>(ptab + g.poff, p.kphi, p.bphi, (R)g.invstep, p.dphi);
+    p.phi = piece_val_grad<Q5, R>(ptab + g.poff, p.kphi, p.bphi, (R)g.invstep, p.dphi);
   }
   if (p.krho >= 0) {
     const SplineGeom &g = sg[pot.s_rho + p.tj];
     p.brho = sizeof(R) == 8 ? (R)db.pair_shift[Np + gs] : (R)db.pair_shiftf[Np + gs];
-    p.rho = cubic_val_grad<R>(ptab + g.poff, p.krho, p.brho, (R)g.invstep, p.drho);
+    p.rho = piece_val_grad<Q5, R>(ptab + g.poff, p.krho, p.brho, (R)g.invstep, p.drho);
   }
   if (MEAM && p.kf >= 0) {
     const SplineGeom &g = sg[pot.s_f + p.pij];
     p.bf = sizeof(R) == 8 ? (R)db.pair_shift[2 * Np + gs] : (R)db.pair_shiftf[2 * Np + gs];
-    p.f = cubic_val_grad<R>(ptab + g.poff, p.kf, p.bf, (R)g.invstep, p.df);
+    p.f = piece_val_grad<Q5, R>(ptab + g.poff, p.kf, p.bf, (R)g.invstep, p.df);
   }
   return p;
 }
@@ -253,7 +288,7 @@ __device__ __forceinline__ float cos_dot(float ax, float ay, float az, float bx,
 //   S = sum_k s(cos) w_k,  T = sum_k s'(cos) w_k cos,  v = sum_k s'(cos) w_k u_k
 // over the row's other slots whose cosine has a knot of s.  FP32 chunks of 8
 // terms are added to FP64 totals (as the g loop of k_atoms).
-template <typename R, typename R4, class W>
+template <typename R, typename R4, class W, bool Q5 = false>
 __device__ __forceinline__ void channel_row_sums(const R4 *srow, W weight, int row_lo, int row_hi, int tid, R ux,
                                                  R uy, R uz, const SplineGeom &gs, const R *spc, double &S, double &T,
                                                  double &vx, double &vy, double &vz) {
@@ -271,7 +306,7 @@ __device__ __forceinline__ void channel_row_sums(const R4 *srow, W weight, int r
       R b;
       const int kk = g_knot<R>(cs, x0, inv, gs.n, b);
       R ds;
-      const R sv = cubic_val_grad<R>(spc, kk, b, inv, ds);
+      const R sv = piece_val_grad<Q5, R>(spc, kk, b, inv, ds);
       const R dsw = ds * wk;
       s8 += sv * wk;
       t8 += dsw * cs;
@@ -312,7 +347,7 @@ __device__ __forceinline__ void warp_slot_sums(const double *red, int lo, int hi
 // is the force atom i's terms add to atom i along slot p; the neighbour
 // receives -V_p (k_gather).  In FP32 the row sums are taken in chunks of 8
 // terms, each chunk added to an FP64 total.
-template <bool MEAM, typename R, bool AUX, bool GM = false, bool JM = false>
+template <bool MEAM, typename R, bool AUX, bool GM = false, bool JM = false, bool Q5 = false>
 __global__ void __launch_bounds__(BLOCK_SLOTS, JM ? 2 : sizeof(R) == 4 ? 4 : 3)
     k_atoms(DevDb db, DevPot pot, const SplineGeom *__restrict__ geom, const double *__restrict__ tabs,
             const double *__restrict__ ptabs, double *__restrict__ Vout, double *__restrict__ aout,
@@ -357,7 +392,7 @@ __global__ void __launch_bounds__(BLOCK_SLOTS, JM ? 2 : sizeof(R) == 4 ? 4 : 3)
     R4 v;
     v.x = v.y = v.z = v.w = R(0);
     if (have) {
-      pe = eval_pair<MEAM, R>(db, pot, sg, ptab, gs, ti);
+      pe = eval_pair<MEAM, R, Q5>(db, pot, sg, ptab, gs, ti);
       v.x = pe.ux; v.y = pe.uy; v.z = pe.uz; v.w = pe.f;
     }
     srow[tid] = v;
@@ -395,7 +430,7 @@ __global__ void __launch_bounds__(BLOCK_SLOTS, JM ? 2 : sizeof(R) == 4 ? 4 : 3)
         R b;
         const int kk = g_knot<R>(cs, (R)g2.x0, ginv, g2.n, b);
         R dg;
-        const R gv = cubic_val_grad<R>(ptab + g2.poff, kk, b, ginv, dg);
+        const R gv = piece_val_grad<Q5, R>(ptab + g2.poff, kk, b, ginv, dg);
         const R dgfk = dg * fk;
         g8 += gv * fk;
         h8 += dgfk * cs;
@@ -438,7 +473,7 @@ __global__ void __launch_bounds__(BLOCK_SLOTS, JM ? 2 : sizeof(R) == 4 ? 4 : 3)
         R b;
         const int kk = g_knot<R>(cs, gx0, ginv, gg.n, b);
         R dg;
-        const R gv = cubic_val_grad<R>(gpc, kk, b, ginv, dg);
+        const R gv = piece_val_grad<Q5, R>(gpc, kk, b, ginv, dg);
         const R dgfk = dg * fk;
         g8 += gv * fk;
         h8 += dgfk * cs;

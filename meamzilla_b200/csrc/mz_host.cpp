@@ -106,10 +106,148 @@ double Spline3::eval(const std::vector<double> &ypp, double r, double *g) const 
   return a * p1 + b * p2 + ((a * a * a - a) * d21 + (b * b * b - b) * d22) * (step * step) / 6.0;
 }
 
+void Spline3::refresh5(std::vector<double> &ypp, std::vector<double> &yp4) const {
+  // Spline5Eq::refresh_basis (spline5eq.cpp:209-293): unknowns h^2 y'' (rows
+  // 0..n-1) and -h^4 y'''' (n..2n-1); interior rows are the continuity of
+  // y' and y''' of the quintic pieces, end rows natural (y''' = y'''' = 0)
+  // or clamped (y' and y'' given).
+  const int n = nknots, m = 2 * n;
+  std::vector<double> A((size_t)m * m, 0.0), b(m, 0.0);
+  auto a = [&](int r, int c) -> double & { return A[(size_t)r * m + c]; };
+  for (int i = 1; i < n - 1; ++i) {
+    a(i, i - 1) = 1. / 12;
+    a(i, i) = 10. / 12;
+    a(i, i + 1) = 1. / 12;
+    a(i, n + i - 1) = 1. / 180;
+    a(i, n + i) = -1. / 90;
+    a(i, n + i + 1) = 1. / 180;
+    a(n + i, i - 1) = 1.;
+    a(n + i, i) = -2.;
+    a(n + i, i + 1) = 1.;
+    a(n + i, n + i - 1) = 1. / 6;
+    a(n + i, n + i) = 2. / 3;
+    a(n + i, n + i + 1) = 1. / 6;
+    b[i] = y[i + 1] - 2 * y[i] + y[i - 1];
+    b[n + i] = 0.;
+  }
+  if (nat[0]) {
+    a(0, 0) = -1.;
+    a(0, 1) = 1.;
+    a(0, n) = 1. / 3;
+    a(0, n + 1) = 1. / 6;
+    b[0] = 0.;
+    a(n, n) = 1.;
+    b[n] = 0.;
+  } else {
+    a(0, 0) = 1. / 3;
+    a(0, 1) = 1. / 6;
+    a(0, n) = 1. / 45;
+    a(0, n + 1) = 7. / 360;
+    b[0] = y[1] - y[0] - grad[0] * step;
+    a(n, 0) = 1.;
+    b[n] = grad2[0] * (step * step);
+  }
+  if (nat[1]) {
+    a(n - 1, n - 2) = -1.;
+    a(n - 1, n - 1) = 1.;
+    a(n - 1, 2 * n - 2) = -1. / 6;
+    a(n - 1, 2 * n - 1) = -1. / 3;
+    b[n - 1] = 0.;
+    a(2 * n - 1, 2 * n - 1) = 1.;
+    b[2 * n - 1] = 0.;
+  } else {
+    a(n - 1, n - 2) = -1. / 6;
+    a(n - 1, n - 1) = -1. / 3;
+    a(n - 1, 2 * n - 2) = -7. / 360;
+    a(n - 1, 2 * n - 1) = -1. / 45;
+    b[n - 1] = y[n - 1] - y[n - 2] - grad[1] * step;
+    a(2 * n - 1, n - 1) = 1.;
+    b[2 * n - 1] = grad2[1] * (step * step);
+  }
+  // elimination with row pivoting on the largest |entry| of each column
+  for (int k = 0; k < m; ++k) {
+    int p = k;
+    for (int r = k + 1; r < m; ++r)
+      if (std::abs(a(r, k)) > std::abs(a(p, k))) p = r;
+    if (p != k) {
+      for (int c = 0; c < m; ++c) std::swap(a(k, c), a(p, c));
+      std::swap(b[k], b[p]);
+    }
+    const double piv = a(k, k);
+    if (piv == 0.0) continue;  // singular column: left as is (the reference does not check either)
+    for (int r = k + 1; r < m; ++r) {
+      const double f = a(r, k) / piv;
+      if (f == 0.0) continue;
+      for (int c = k + 1; c < m; ++c) a(r, c) -= f * a(k, c);
+      b[r] -= f * b[k];
+    }
+  }
+  for (int k = m - 1; k >= 0; --k) {
+    double s = b[k];
+    for (int c = k + 1; c < m; ++c) s -= a(k, c) * b[c];
+    b[k] = a(k, k) != 0.0 ? s / a(k, k) : 0.0;
+  }
+  ypp.assign(n, 0.0);
+  yp4.assign(n, 0.0);
+  for (int i = 0; i < n; ++i) {
+    ypp[i] = b[i] * (invstep * invstep);
+    yp4[i] = -b[n + i] * (invstep * invstep * invstep * invstep);
+  }
+}
+
+void Spline3::refresh_any(SplineDerivs &d) const {
+  if (quintic) refresh5(d.ypp, d.yp4);
+  else {
+    refresh(d.ypp);
+    d.yp4.assign(nknots, 0.0);
+  }
+}
+
+double Spline3::eval_any(const SplineDerivs &d, double r, double *g) const {
+  if (!quintic) return eval(d.ypp, r, g);
+  // Spline5Eq::splint_comb(double, double*) (spline5eq.h:226-255)
+  const int n = nknots;
+  if (r < x[0]) {
+    *g = grad[0] + grad2[0] * (r - x[0]);
+    return y[0] + grad[0] * (r - x[0]) + 0.5 * grad2[0] * (r - x[0]) * (r - x[0]);
+  } else if (r > x[n - 1]) {
+    *g = grad[1] + grad2[1] * (r - x[n - 1]);
+    return y[n - 1] + grad[1] * (r - x[n - 1]) + 0.5 * grad2[1] * (r - x[n - 1]) * (r - x[n - 1]);
+  }
+  double dr = r - x[0];
+  int k = (dr < 0) ? 0 : int(dr * invstep);
+  if (k >= n - 1) k = n - 2;
+  double b = (dr - k * step) * invstep, a = 1.0 - b;
+  double p1 = y[k], d21 = d.ypp[k], d41 = d.yp4[k], p2 = y[k + 1], d22 = d.ypp[k + 1], d42 = d.yp4[k + 1];
+  *g = (p2 - p1) * invstep + ((3 * b * b - 1) * d22 - (3 * a * a - 1) * d21) * step / 6.0 +
+       ((15 * b * b * b * b - 30 * b * b + 7) * d42 - (15 * a * a * a * a - 30 * a * a + 7) * d41) *
+           (step * step * step) / 360.0;
+  return a * p1 + b * p2 + ((a * a * a - a) * d21 + (b * b * b - b) * d22) * (step * step) / 6.0 +
+         ((3 * a * a * a * a * a - 10 * a * a * a + 7 * a) * d41 + (3 * b * b * b * b * b - 10 * b * b * b + 7 * b) * d42) *
+             (step * step * step * step) / 360.0;
+}
+
+double Spline3::eval_grad2_any(const SplineDerivs &d, double r) const {
+  // Spline5Eq::splint_grad2(double) (spline5eq.h:260-291); cubic: the
+  // interpolated y'' (spline3eq.h:241-266), 0 beyond the ends
+  const int n = nknots;
+  if (r < x[0]) return quintic ? grad2[0] : 0.0;
+  if (r > x[n - 1]) return quintic ? grad2[1] : 0.0;
+  double dr = r - x[0];
+  int k = (dr < 0) ? 0 : int(dr * invstep);
+  if (k >= n - 1) k = n - 2;
+  double b = (dr - k * step) * invstep, a = 1.0 - b;
+  double d21 = d.ypp[k], d22 = d.ypp[k + 1];
+  if (!quintic) return a * d21 + b * d22;
+  double d41 = d.yp4[k], d42 = d.yp4[k + 1];
+  return a * d21 + b * d22 + ((a * a * a - a) * d41 + (b * b * b - b) * d42) * (step * step) / 6.0;
+}
+
 void Spline3::readjust_x(double l, double r) {
-  // Spline3Eq::readjust_x (spline3eq.cpp:112-143)
-  std::vector<double> ypp;
-  refresh(ypp);
+  // Spline3Eq::readjust_x (spline3eq.cpp:112-143), Spline5Eq::readjust_x
+  // (spline5eq.cpp:121-157: the ends' y'' re-evaluated as well)
+  SplineDerivs d;
+  refresh_any(d);
   const Spline3 old = *this;
   step = (r - l) / (nknots - 1);
   invstep = 1.0 / step;
@@ -117,72 +255,97 @@ void Spline3::readjust_x(double l, double r) {
   x[nknots - 1] = r;
   for (int i = 1; i < nknots - 1; ++i) x[i] = l + i * step;
   double g;
-  for (int i = 0; i < nknots; ++i) y[i] = old.eval(ypp, x[i], &g);
+  for (int i = 0; i < nknots; ++i) y[i] = old.eval_any(d, x[i], &g);
   if (!nat[0]) {
-    old.eval(ypp, l, &g);
+    old.eval_any(d, l, &g);
     grad[0] = g;
+    if (quintic) grad2[0] = old.eval_grad2_any(d, l);
   }
   if (!nat[1]) {
-    old.eval(ypp, r, &g);
+    old.eval_any(d, r, &g);
     grad[1] = g;
+    if (quintic) grad2[1] = old.eval_grad2_any(d, r);
   }
   left = x[0];
   right = x[nknots - 1];
 }
 
 void Spline3::rescale_x(double scale) {
-  // Spline3Eq::rescale_x (spline3eq.cpp:150-171)
+  // Spline3Eq::rescale_x (spline3eq.cpp:150-171), Spline5Eq::rescale_x
+  // (spline5eq.cpp:163-189).  For a negative factor the reference reverses
+  // x, y and the knot flags; its reversals of the two-element end arrays
+  // (natural flags, slopes, slope flags) span one element and leave them
+  // as they are, and so does this.
   step *= std::abs(scale);
   invstep = 1.0 / step;
   for (int i = 0; i < nknots; ++i) x[i] *= scale;
-  if (!nat[0]) grad[0] /= scale;
-  if (!nat[1]) grad[1] /= scale;
+  if (!nat[0]) {
+    grad[0] /= scale;
+    if (quintic) grad2[0] /= scale * scale;
+  }
+  if (!nat[1]) {
+    grad[1] /= scale;
+    if (quintic) grad2[1] /= scale * scale;
+  }
   if (scale < 0.0) {
     std::reverse(x.begin(), x.end());
     std::reverse(y.begin(), y.end());
-    std::swap(nat[0], nat[1]);
     std::reverse(y_fixed.begin(), y_fixed.end());
-    std::swap(grad[0], grad[1]);
-    std::swap(grad_fixed[0], grad_fixed[1]);
   }
   left = x[0];
   right = x[nknots - 1];
 }
 
 void Spline3::scale_y(double f) {
-  // Spline3Eq::operator*= (spline3eq.cpp:301-313)
+  // Spline3Eq::operator*= (spline3eq.cpp:301-313), Spline5Eq::operator*=
+  // (spline5eq.cpp:381-396, the ends' y'' too)
   for (int i = 0; i < nknots; ++i) y[i] *= f;
-  if (!nat[0]) grad[0] *= f;
-  if (!nat[1]) grad[1] *= f;
+  if (!nat[0]) {
+    grad[0] *= f;
+    if (quintic) grad2[0] *= f;
+  }
+  if (!nat[1]) {
+    grad[1] *= f;
+    if (quintic) grad2[1] *= f;
+  }
 }
 
 void Spline3::divide_y(double f) {
-  // Spline3Eq::operator/= (spline3eq.cpp:318-330)
+  // Spline3Eq::operator/= (spline3eq.cpp:318-330), Spline5Eq::operator/=
   for (int i = 0; i < nknots; ++i) y[i] /= f;
-  if (!nat[0]) grad[0] /= f;
-  if (!nat[1]) grad[1] /= f;
+  if (!nat[0]) {
+    grad[0] /= f;
+    if (quintic) grad2[0] /= f;
+  }
+  if (!nat[1]) {
+    grad[1] /= f;
+    if (quintic) grad2[1] /= f;
+  }
 }
 
-void Spline3::add(const Spline3 &rhs, const std::vector<double> &rhs_ypp) {
-  // Spline3Eq::operator+= (spline3eq.cpp:335-348)
+void Spline3::add(const Spline3 &rhs, const SplineDerivs &rhs_d) {
+  // Spline3Eq::operator+= (spline3eq.cpp:335-348), Spline5Eq::operator+=
+  // (spline5eq.cpp:424-441: y'' at the ends as well)
   const double rmax = rhs.x.back();
   double g;
-  for (int i = 0; i < nknots; ++i) y[i] += (x[i] < rmax) ? rhs.eval(rhs_ypp, x[i], &g) : 0.;
+  for (int i = 0; i < nknots; ++i) y[i] += (x[i] < rmax) ? rhs.eval_any(rhs_d, x[i], &g) : 0.;
   if (!nat[0]) {
     double v = 0.;
     if (x[0] < rmax) {
-      rhs.eval(rhs_ypp, x[0], &g);
+      rhs.eval_any(rhs_d, x[0], &g);
       v = g;
     }
     grad[0] += v;
+    if (quintic) grad2[0] += (x[0] < rmax) ? rhs.eval_grad2_any(rhs_d, x[0]) : 0.;
   }
   if (!nat[1]) {
     double v = 0.;
     if (x.back() < rmax) {
-      rhs.eval(rhs_ypp, x.back(), &g);
+      rhs.eval_any(rhs_d, x.back(), &g);
       v = g;
     }
     grad[1] += v;
+    if (quintic) grad2[1] += (x.back() < rmax) ? rhs.eval_grad2_any(rhs_d, x.back()) : 0.;
   }
 }
 
@@ -231,25 +394,35 @@ int Pot::ncoeff() const {
 // Coefficient order: Potential::coeff -> PotFns::coeff -> Spline::coeff ->
 // Spline3Eq::bc_coeff (potential.cpp:192-206, pot_fns.cpp:209-218,
 // spline.cpp:105-114, spline3eq.cpp:376-382).
-void Pot::get_coeffs(double *out) const {
-  int i = 0;
+std::vector<std::pair<int, int>> Pot::coeff_slots() const {
+  std::vector<std::pair<int, int>> w;
+  const int nc = ncoeff();
+  int si = 0;
   for (auto &g : groups)
     for (auto &s : g) {
       for (int k = 0; k < s.nknots; ++k)
-        if (!s.y_fixed[k]) out[i++] = s.y[k];
+        if (!s.y_fixed[k]) w.emplace_back(si, k);
       for (int e = 0; e < 2; ++e)
-        if (!s.grad_fixed[e] && !s.nat[e]) out[i++] = s.grad[e];
+        if (!s.grad_fixed[e] && !s.nat[e]) {
+          w.emplace_back(si, s.nknots + e);
+          if (s.quintic) w.emplace_back(si, s.nknots + 2 + e);
+        }
+      ++si;
     }
+  w.resize(std::min<size_t>(w.size(), (size_t)nc));
+  return w;
+}
+static double &slot_ref(Spline3 &s, int slot) {
+  return slot < s.nknots ? s.y[slot] : slot < s.nknots + 2 ? s.grad[slot - s.nknots] : s.grad2[slot - s.nknots - 2];
+}
+void Pot::get_coeffs(double *out) const {
+  Pot &self = const_cast<Pot &>(*this);
+  int i = 0;
+  for (auto &c : coeff_slots()) out[i++] = slot_ref(self.spline(c.first), c.second);
 }
 void Pot::set_coeffs(const double *in) {
   int i = 0;
-  for (auto &g : groups)
-    for (auto &s : g) {
-      for (int k = 0; k < s.nknots; ++k)
-        if (!s.y_fixed[k]) s.y[k] = in[i++];
-      for (int e = 0; e < 2; ++e)
-        if (!s.grad_fixed[e] && !s.nat[e]) s.grad[e] = in[i++];
-    }
+  for (auto &c : coeff_slots()) slot_ref(spline(c.first), c.second) = in[i++];
 }
 
 double Pot::max_rcut() const {
@@ -329,6 +502,7 @@ void parse_pot(const std::string &text, Pot &pot) {
   pot.ngroups = (int)nalloy.size();
   if (ln >= L.size() || L[ln++].substr(0, 2) != "#P") fail(MZ_ERR_FORMAT, "potential line (#P ...) missing");
   pot.groups.assign(pot.ngroups, {});
+  bool quintic = false, first_quintic = false;
   for (int g = 0; g < pot.ngroups; ++g) {
     for (int a = 0; a < nalloy[g]; ++a) {
       // PotFns::read_pot_fns (pot_fns.cpp:439-465) + Spline3Eq::read_basis
@@ -338,9 +512,15 @@ void parse_pot(const std::string &text, Pot &pot) {
         std::string lab, basis;
         is >> lab >> basis;
         if (is.fail()) fail(MZ_ERR_FORMAT, "incorrect basis definition, use format (#B <basis type>)");
-        if (basis != "spline3eq") fail(MZ_ERR_UNSUPPORTED, "basis \"" + basis + "\" is not implemented (spline3eq)");
+        if (basis != "spline3eq" && basis != "spline5eq")
+          fail(MZ_ERR_UNSUPPORTED, "basis \"" + basis + "\" is not implemented (spline3eq, spline5eq)");
+        quintic = basis == "spline5eq";
+        if (g == 0 && a == 0) first_quintic = quintic;
+        else if (quintic != first_quintic)
+          fail(MZ_ERR_UNSUPPORTED, "potentials mixing spline3eq and spline5eq bases are not implemented");
       }
       Spline3 s;
+      s.quintic = quintic ? 1 : 0;
       if (ln + 2 >= L.size()) fail(MZ_ERR_FORMAT, "unexpected end of potential file");
       {
         std::istringstream is(L[ln++]);
@@ -366,6 +546,13 @@ void parse_pot(const std::string &text, Pot &pot) {
         is >> s.grad[0] >> s.grad[1];
         if (is.fail()) fail(MZ_ERR_FORMAT, "incorrect boundary condition line, format is (<left grad> <right grad>)");
       }
+      if (s.quintic) {  // Spline5Eq::read_basis (spline5eq.cpp:97-102)
+        if (ln >= L.size()) fail(MZ_ERR_FORMAT, "unexpected end of potential file");
+        std::istringstream is(L[ln++]);
+        is >> s.grad2[0] >> s.grad2[1];
+        if (is.fail())
+          fail(MZ_ERR_FORMAT, "incorrect boundary condition line, format is (<left grad2> <right grad2>)");
+      }
       s.y.assign(s.nknots, 0.0);
       s.y_fixed.assign(s.nknots, 0);
       for (int k = 0; k < s.nknots; ++k) {
@@ -388,7 +575,7 @@ std::string write_pot_text(const Pot &pot) {
   char buf[128];
   for (auto &g : pot.groups)
     for (auto &s : g) {
-      os << "#B spline3eq\n";
+      os << (s.quintic ? "#B spline5eq\n" : "#B spline3eq\n");
       std::snprintf(buf, sizeof buf, "%.15e %.15e %d\n", s.x[0], s.x[s.nknots - 1], s.nknots);
       os << buf;
       int c[2];
@@ -396,6 +583,10 @@ std::string write_pot_text(const Pot &pot) {
       os << c[0] << " " << c[1] << "\n";
       std::snprintf(buf, sizeof buf, "%.15e %.15e\n", s.grad[0], s.grad[1]);
       os << buf;
+      if (s.quintic) {  // Spline5Eq::write_basis_fn (spline5eq.cpp:305-331)
+        std::snprintf(buf, sizeof buf, "%.15e %.15e\n", s.grad2[0], s.grad2[1]);
+        os << buf;
+      }
       for (int k = 0; k < s.nknots; ++k) {
         std::snprintf(buf, sizeof buf, "%d %.15e\n", s.y_fixed[k], s.y[k]);
         os << buf;
@@ -573,14 +764,14 @@ int rescale_pot(Pot &pot, const int *atom_type, int natoms, const double *dens, 
     // the unscaled rho's; so does this.
     std::vector<Spline3> &rho = pot.groups[G_RHO];
     std::vector<Spline3> &phi = pot.groups[G_PHI];
-    std::vector<std::vector<double>> rho_ypp(rho.size());
-    for (size_t i = 0; i < rho.size(); ++i) rho[i].refresh(rho_ypp[i]);
+    std::vector<SplineDerivs> rho_d(rho.size());
+    for (size_t i = 0; i < rho.size(); ++i) rho[i].refresh_any(rho_d[i]);
     std::vector<double> lam(Fs);
     for (int i = 0; i < Fs; ++i) {
-      std::vector<double> ypp;
-      F[i].refresh(ypp);
+      SplineDerivs d;
+      F[i].refresh_any(d);
       double g;
-      F[i].eval(ypp, 0.5 * (F[i].x[0] + F[i].x.back()), &g);
+      F[i].eval_any(d, 0.5 * (F[i].x[0] + F[i].x.back()), &g);
       lam[i] = g;
     }
     int count = 0;
@@ -588,10 +779,10 @@ int rescale_pot(Pot &pot, const int *atom_type, int natoms, const double *dens, 
       for (int j = i; j < Fs; ++j) {
         Spline3 t = rho[i];
         t.scale_y(lam[j]);
-        phi[count].add(t, rho_ypp[i]);
+        phi[count].add(t, rho_d[i]);
         Spline3 t2 = rho[j];
         t2.scale_y(lam[i]);
-        phi[count].add(t2, rho_ypp[j]);
+        phi[count].add(t2, rho_d[j]);
         ++count;
       }
     for (int i = 0; i < Fs; ++i) F[i].add_linear(-1.0 * lam[i]);
@@ -1112,9 +1303,9 @@ mz_status mz_pot_spline_eval(const mz_pot *pot, int s, double x, double *val, do
     if (!pot || !val || !grad) fail(MZ_ERR_ARG, "null argument");
     if (s < 0 || s >= pot->pot.nsplines()) fail(MZ_ERR_ARG, "spline index out of range");
     const Spline3 &sp = pot->pot.spline(s);
-    std::vector<double> ypp;
-    sp.refresh(ypp);
-    *val = sp.eval(ypp, x, grad);
+    SplineDerivs d;
+    sp.refresh_any(d);
+    *val = sp.eval_any(d, x, grad);
   });
 }
 
@@ -1267,6 +1458,9 @@ mz_status mz_pot_get_spline(const mz_pot *pot, int s, mz_spline_view *v) {
     v->grad_fixed[1] = sp.grad_fixed[1];
     v->grad[0] = sp.grad[0];
     v->grad[1] = sp.grad[1];
+    v->quintic = sp.quintic;
+    v->grad2[0] = sp.grad2[0];
+    v->grad2[1] = sp.grad2[1];
     v->y_fixed = sp.y_fixed.data();
     v->y = sp.y.data();
     v->x = sp.x.data();

@@ -10,19 +10,30 @@
 
 #include <cstdint>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "mz_b200.h"
 
 namespace mzb {
 
+// Second derivatives (and, for the quintic basis, fourth derivatives) that a
+// spline carries between refreshes.  The reference's rescale evaluates splines
+// whose y was scaled after their last refresh, so these travel separately.
+struct SplineDerivs {
+  std::vector<double> ypp, yp4;
+};
+
 struct Spline3 {
-  // Definition read from the file (spline3eq.cpp:54-106).
+  // Definition read from the file (spline3eq.cpp:54-106; spline5eq.cpp:57-115
+  // for the quintic basis, whose ends also carry y'').
   double left = 0, right = 0;
   int nknots = 0;
+  int quintic = 0;             // spline5eq
   int nat[2] = {0, 0};         // natural end (bc -1)
   int grad_fixed[2] = {1, 1};  // end slope fixed (bc 1) ; bc 0 -> free
   double grad[2] = {0, 0};
+  double grad2[2] = {0, 0};    // spline5eq: y'' at the ends
   std::vector<int> y_fixed;
   std::vector<double> y;
   // Knot grid exactly as Spline3Eq::set_spline (spline3eq.cpp:354-370).
@@ -38,6 +49,15 @@ struct Spline3 {
   void refresh(std::vector<double> &ypp) const;
   // Value + slope at x with linear extrapolation (spline3eq.h:204-236).
   double eval(const std::vector<double> &ypp, double xv, double *g) const;
+  // spline5eq: y'' and y'''' from the 2n x 2n system of
+  // Spline5Eq::refresh_basis (spline5eq.cpp:209-293), solved by Gaussian
+  // elimination with partial pivoting.
+  void refresh5(std::vector<double> &ypp, std::vector<double> &yp4) const;
+  // Either basis: refresh, value + slope (+ y'') at x (spline5eq.h:205-291
+  // for the quintic, quadratic beyond the ends).
+  void refresh_any(SplineDerivs &d) const;
+  double eval_any(const SplineDerivs &d, double xv, double *g) const;
+  double eval_grad2_any(const SplineDerivs &d, double xv) const;
 
   // Operations of the reference's rescale (spline3eq.cpp:112-186, 301-350):
   // new end knots with values re-interpolated, x scaled (reversed when the
@@ -47,7 +67,7 @@ struct Spline3 {
   void rescale_x(double scale);
   void scale_y(double f);
   void divide_y(double f);
-  void add(const Spline3 &rhs, const std::vector<double> &rhs_ypp);
+  void add(const Spline3 &rhs, const SplineDerivs &rhs_d);
   void add_linear(double a);
   double max_y_mag() const;  // Spline::get_max_y_mag (spline.cpp:58-67)
 };
@@ -105,6 +125,13 @@ struct Pot {
   int ncoeff() const;
   void get_coeffs(double *out) const;
   void set_coeffs(const double *in);
+  // The coefficient order as (spline, slot): slot k < n is knot y[k], n + e
+  // the end slope grad[e], n + 2 + e the quintic y''[e].  Potential::coeff
+  // walks free knots, then per free end its slope (and for spline5eq its
+  // y'', Spline5Eq::bc_coeff spline5eq.cpp:459-468), while get_ncoeff counts
+  // one per free end (spline5eq.cpp:81-85); the first ncoeff() of the walk
+  // are the coefficients.
+  std::vector<std::pair<int, int>> coeff_slots() const;
   double max_rcut() const;  // Potential::get_max_rcut (potential.cpp:72-82), radial groups
 
   // alloy indices (pot_fns.cpp:240-296)

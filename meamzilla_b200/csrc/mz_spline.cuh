@@ -47,6 +47,33 @@ __device__ __forceinline__ R cubic_val(const R *ptab, int k, R b) {
   return c0 + b * (c1 + b * (c2 + b * c3));
 }
 
+// spline5eq: the quintic of each interval (Spline5Eq::splint_comb,
+// spline5eq.h:110-127) as six coefficients c0..c5 in the shift b, formed in
+// FP64; loaded as 8-byte pairs (an interval starts on 24 or 48 bytes).
+__device__ __forceinline__ void load_quintic(const float *c, float *q) {
+  const float2 a = *reinterpret_cast<const float2 *>(c), b = *reinterpret_cast<const float2 *>(c + 2),
+               d = *reinterpret_cast<const float2 *>(c + 4);
+  q[0] = a.x; q[1] = a.y; q[2] = b.x; q[3] = b.y; q[4] = d.x; q[5] = d.y;
+}
+__device__ __forceinline__ void load_quintic(const double *c, double *q) {
+  const double2 a = *reinterpret_cast<const double2 *>(c), b = *reinterpret_cast<const double2 *>(c + 2),
+                d = *reinterpret_cast<const double2 *>(c + 4);
+  q[0] = a.x; q[1] = a.y; q[2] = b.x; q[3] = b.y; q[4] = d.x; q[5] = d.y;
+}
+template <typename R>
+__device__ __forceinline__ R quintic_val_grad(const R *ptab, int k, R b, R invstep, R &grad) {
+  R c[6];
+  load_quintic(ptab + 6 * k, c);
+  grad = (c[1] + b * (R(2) * c[2] + b * (R(3) * c[3] + b * (R(4) * c[4] + R(5) * b * c[5])))) * invstep;
+  return c[0] + b * (c[1] + b * (c[2] + b * (c[3] + b * (c[4] + b * c[5]))));
+}
+// The piece of the potential's basis: cubic, or quintic when Q5.
+template <bool Q5, typename R>
+__device__ __forceinline__ R piece_val_grad(const R *ptab, int k, R b, R invstep, R &grad) {
+  if constexpr (Q5) return quintic_val_grad<R>(ptab, k, b, invstep, grad);
+  else return cubic_val_grad<R>(ptab, k, b, invstep, grad);
+}
+
 // Weights of the value (w*) and of the slope (d*) on the table entries
 // y[k], y[k+1], ypp[k], ypp[k+1] at shift b -- the transposes of the two
 // formulas above, used by the adjoint.
@@ -77,7 +104,44 @@ struct PointEval {
   int k;          // interval, or -1 left / -2 right of the knots
   double b;       // shift inside the interval
 };
+__device__ __forceinline__ PointEval spl_point5(const double *tab, const SplineGeom &g, double r) {
+  // Spline5Eq::splint_comb(double, double*) and splint_grad2(double)
+  // (spline5eq.h:226-291): quadratic beyond the end knots
+  const double *y = tab + g.toff, *ypp = y + g.n, *ge = y + 2 * g.n, *yp4 = ge + 2, *g2 = yp4 + g.n;
+  PointEval e;
+  e.b = 0.0;
+  if (r < g.x0) {
+    e.grad = ge[0] + g2[0] * (r - g.x0);
+    e.val = y[0] + ge[0] * (r - g.x0) + 0.5 * g2[0] * (r - g.x0) * (r - g.x0);
+    e.grad2 = g2[0];
+    e.k = -1;
+    return e;
+  } else if (r > g.xN) {
+    e.grad = ge[1] + g2[1] * (r - g.xN);
+    e.val = y[g.n - 1] + ge[1] * (r - g.xN) + 0.5 * g2[1] * (r - g.xN) * (r - g.xN);
+    e.grad2 = g2[1];
+    e.k = -2;
+    return e;
+  }
+  const double dr = r - g.x0;
+  int k = (dr < 0) ? 0 : int(dr * g.invstep);
+  if (k >= g.n - 1) k = g.n - 2;
+  const double b = (dr - k * g.step) * g.invstep, a = 1.0 - b, h = g.step;
+  const double p1 = y[k], p2 = y[k + 1], d21 = ypp[k], d22 = ypp[k + 1], d41 = yp4[k], d42 = yp4[k + 1];
+  e.grad = (p2 - p1) * g.invstep + ((3 * b * b - 1) * d22 - (3 * a * a - 1) * d21) * h / 6.0 +
+           ((15 * b * b * b * b - 30 * b * b + 7) * d42 - (15 * a * a * a * a - 30 * a * a + 7) * d41) * (h * h * h) /
+               360.0;
+  e.val = a * p1 + b * p2 + ((a * a * a - a) * d21 + (b * b * b - b) * d22) * (h * h) / 6.0 +
+          ((3 * a * a * a * a * a - 10 * a * a * a + 7 * a) * d41 + (3 * b * b * b * b * b - 10 * b * b * b + 7 * b) * d42) *
+              (h * h * h * h) / 360.0;
+  e.grad2 = a * d21 + b * d22 + ((a * a * a - a) * d41 + (b * b * b - b) * d42) * (h * h) / 6.0;
+  e.k = k;
+  e.b = b;
+  return e;
+}
+
 __device__ __forceinline__ PointEval spl_point(const double *tab, const SplineGeom &g, double r) {
+  if (g.q5) return spl_point5(tab, g, r);
   const double *y = tab + g.toff, *ypp = y + g.n, *ge = y + 2 * g.n;
   PointEval e;
   if (r < g.x0) {

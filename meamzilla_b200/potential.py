@@ -162,7 +162,8 @@ class PotentialFile:
                     nat=(v.nat[0], v.nat[1]), grad_fixed=(v.grad_fixed[0], v.grad_fixed[1]),
                     grad=np.array([v.grad[0], v.grad[1]]),
                     y_fixed=_lib.as_array(v.y_fixed, n, np.int32), y=_lib.as_array(v.y, n, np.float64),
-                    x=_lib.as_array(v.x, n, np.float64), step=v.step)
+                    x=_lib.as_array(v.x, n, np.float64), step=v.step, quintic=v.quintic,
+                    grad2=np.array([v.grad2[0], v.grad2[1]]))
 
     def spline_eval(self, s: int, x: float):
         val, grad = C.c_double(), C.c_double()

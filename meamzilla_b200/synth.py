@@ -44,7 +44,8 @@ GPA_PER_EV_A3 = 160.2177
 
 @dataclasses.dataclass
 class Spline:
-    """One equidistant cubic spline (#B spline3eq block)."""
+    """One equidistant spline: cubic (#B spline3eq block) or, with grad2 set
+    (the y'' at the ends), quintic (#B spline5eq)."""
 
     left: float
     right: float
@@ -52,6 +53,7 @@ class Spline:
     grad: np.ndarray                   # end slopes [left, right]
     bc: Sequence[int] = (0, 0)         # -1 natural, 0 free slope, 1 fixed slope
     fixed: Optional[np.ndarray] = None  # per-knot 1 = fixed
+    grad2: Optional[np.ndarray] = None  # spline5eq: y'' at the ends
 
     @property
     def nknots(self) -> int:
@@ -59,7 +61,8 @@ class Spline:
 
     def copy(self) -> "Spline":
         return Spline(self.left, self.right, self.y.copy(), self.grad.copy(), tuple(self.bc),
-                      None if self.fixed is None else self.fixed.copy())
+                      None if self.fixed is None else self.fixed.copy(),
+                      None if self.grad2 is None else self.grad2.copy())
 
 
 @dataclasses.dataclass
@@ -328,6 +331,19 @@ def grad10_workload(variant: str):
     return (in_range_variant(pot) if variant == "inrange" else pot), cells
 
 
+def quintic_variant(pot: PotSpec, seed: int = 0) -> PotSpec:
+    """The same knots as spline5eq splines (Spline5Eq, spline5eq.cpp), with
+    end second derivatives from the knots' second differences."""
+    p = pot.copy()
+    rng = np.random.default_rng(seed)
+    for group in p.groups:
+        for s in group:
+            h = (s.right - s.left) / (s.nknots - 1)
+            d2 = np.diff(s.y, 2) / (h * h)
+            s.grad2 = np.array([d2[0], d2[-1]]) * (1.0 + 0.05 * rng.normal(size=2))
+    return p
+
+
 def in_range_variant(pot: PotSpec, rho_scale: float = 0.01, g_scale: float = 0.0025) -> PotSpec:
     """Supplementary variant (labelled as such wherever used): the teacher's
     rho and g scaled so that every embedding density of the MEAM workloads
@@ -364,10 +380,12 @@ def write_pot(path: str, pot: PotSpec, comment: str = "synthetic teacher potenti
     lines = [comment, "#T %s %d" % (pot.style, pot.ntypes), "#P"]
     for group in pot.groups:
         for s in group:
-            lines.append("#B spline3eq")
+            lines.append("#B spline5eq" if s.grad2 is not None else "#B spline3eq")
             lines.append("%s %s %d" % (_f(s.left), _f(s.right), s.nknots))
             lines.append("%d %d" % tuple(s.bc))
             lines.append("%s %s" % (_f(s.grad[0]), _f(s.grad[1])))
+            if s.grad2 is not None:
+                lines.append("%s %s" % (_f(s.grad2[0]), _f(s.grad2[1])))
             fixed = s.fixed if s.fixed is not None else np.zeros(s.nknots, dtype=int)
             for k in range(s.nknots):
                 lines.append("%d %s" % (int(fixed[k]), _f(s.y[k])))

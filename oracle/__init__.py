@@ -36,7 +36,7 @@ def build(reference_dir: str = "/root/reference") -> None:
 class _Spline(C.Structure):
     _fields_ = [("nknots", C.c_int), ("left", C.c_double), ("right", C.c_double), ("nat", C.c_int * 2),
                 ("grad_fixed", C.c_int * 2), ("grad", C.c_double * 2), ("y_fixed", C.POINTER(C.c_int)),
-                ("y", C.POINTER(C.c_double))]
+                ("y", C.POINTER(C.c_double)), ("quintic", C.c_int), ("grad2", C.c_double * 2)]
 
 
 class _Pot(C.Structure):
@@ -99,6 +99,9 @@ class CRestatement:
             sp.grad[0], sp.grad[1] = float(s["grad"][0]), float(s["grad"][1])
             sp.y_fixed = _p(yf, C.c_int)
             sp.y = _p(y, C.c_double)
+            sp.quintic = int(s.get("quintic", 0))
+            g2 = s.get("grad2", (0.0, 0.0))
+            sp.grad2[0], sp.grad2[1] = float(g2[0]), float(g2[1])
             arr.append(sp)
         self._splines = (_Spline * len(arr))(*arr)
         self.pot = _Pot(style, ntypes, len(arr), C.cast(self._splines, C.POINTER(_Spline)), embed_extrap,

@@ -11,22 +11,89 @@
 #define DUMMY_WEIGHT 100.0 /* PotPair::DUMMY_WEIGHT, pot_pair.h:39 */
 
 typedef struct {
-  int n;
+  int n, quintic;
   double step, invstep;
-  double *x, *y, *ypp;
-  double grad[2];
+  double *x, *y, *ypp, *yp4;
+  double grad[2], grad2[2];
   int nat[2];
 } sp_t;
+
+/* Spline5Eq::refresh_basis (spline5eq.cpp:209-293): the 2n x 2n system for
+ * h^2 y'' and -h^4 y'''', solved here by Gaussian elimination with partial
+ * pivoting (the reference calls LAPACK dgesv; the solutions agree to
+ * rounding). */
+static void sp_refresh5(sp_t *s) {
+  const int n = s->n, m = 2 * n;
+  double *A = (double *)calloc((size_t)m * m, sizeof(double)), *b = (double *)calloc(m, sizeof(double));
+  const double *y = s->y, step = s->step, inv = s->invstep;
+  int i, k, r, c;
+#define AA(r, c) A[(size_t)(r) * m + (c)]
+  for (i = 1; i < n - 1; ++i) {
+    AA(i, i - 1) = 1. / 12; AA(i, i) = 10. / 12; AA(i, i + 1) = 1. / 12;
+    AA(i, n + i - 1) = 1. / 180; AA(i, n + i) = -1. / 90; AA(i, n + i + 1) = 1. / 180;
+    AA(n + i, i - 1) = 1.; AA(n + i, i) = -2.; AA(n + i, i + 1) = 1.;
+    AA(n + i, n + i - 1) = 1. / 6; AA(n + i, n + i) = 2. / 3; AA(n + i, n + i + 1) = 1. / 6;
+    b[i] = y[i + 1] - 2 * y[i] + y[i - 1];
+  }
+  if (s->nat[0]) {
+    AA(0, 0) = -1.; AA(0, 1) = 1.; AA(0, n) = 1. / 3; AA(0, n + 1) = 1. / 6; b[0] = 0.;
+    AA(n, n) = 1.; b[n] = 0.;
+  } else {
+    AA(0, 0) = 1. / 3; AA(0, 1) = 1. / 6; AA(0, n) = 1. / 45; AA(0, n + 1) = 7. / 360;
+    b[0] = y[1] - y[0] - s->grad[0] * step;
+    AA(n, 0) = 1.; b[n] = s->grad2[0] * (step * step);
+  }
+  if (s->nat[1]) {
+    AA(n - 1, n - 2) = -1.; AA(n - 1, n - 1) = 1.; AA(n - 1, 2 * n - 2) = -1. / 6; AA(n - 1, 2 * n - 1) = -1. / 3;
+    b[n - 1] = 0.;
+    AA(2 * n - 1, 2 * n - 1) = 1.; b[2 * n - 1] = 0.;
+  } else {
+    AA(n - 1, n - 2) = -1. / 6; AA(n - 1, n - 1) = -1. / 3; AA(n - 1, 2 * n - 2) = -7. / 360;
+    AA(n - 1, 2 * n - 1) = -1. / 45;
+    b[n - 1] = y[n - 1] - y[n - 2] - s->grad[1] * step;
+    AA(2 * n - 1, n - 1) = 1.; b[2 * n - 1] = s->grad2[1] * (step * step);
+  }
+  for (k = 0; k < m; ++k) {
+    int p = k;
+    for (r = k + 1; r < m; ++r)
+      if (fabs(AA(r, k)) > fabs(AA(p, k))) p = r;
+    if (p != k) {
+      for (c = 0; c < m; ++c) { double t = AA(k, c); AA(k, c) = AA(p, c); AA(p, c) = t; }
+      { double t = b[k]; b[k] = b[p]; b[p] = t; }
+    }
+    if (AA(k, k) == 0.0) continue;
+    for (r = k + 1; r < m; ++r) {
+      double f = AA(r, k) / AA(k, k);
+      if (f == 0.0) continue;
+      for (c = k + 1; c < m; ++c) AA(r, c) -= f * AA(k, c);
+      b[r] -= f * b[k];
+    }
+  }
+  for (k = m - 1; k >= 0; --k) {
+    double acc = b[k];
+    for (c = k + 1; c < m; ++c) acc -= AA(k, c) * b[c];
+    b[k] = AA(k, k) != 0.0 ? acc / AA(k, k) : 0.0;
+  }
+#undef AA
+  for (i = 0; i < n; ++i) {
+    s->ypp[i] = b[i] * (inv * inv);
+    s->yp4[i] = -b[n + i] * (inv * inv * inv * inv);
+  }
+  free(A);
+  free(b);
+}
 
 /* Spline3Eq::set_spline (spline3eq.cpp:354-370) + coefficients in
  * Spline::coeff / Spline3Eq::bc_coeff order (spline.cpp:105-114,
  * spline3eq.cpp:376-382) + Spline3Eq::refresh_basis (spline3eq.cpp:192-225). */
-static void sp_setup(sp_t *s, const mzo_spline *in, const double *coeffs, int *ci) {
+static void sp_setup(sp_t *s, const mzo_spline *in, const double *coeffs, int *ci, int ncoeff) {
   int n = in->nknots, i, k;
   s->n = n;
+  s->quintic = in->quintic;
   s->x = (double *)malloc(sizeof(double) * n);
   s->y = (double *)malloc(sizeof(double) * n);
   s->ypp = (double *)malloc(sizeof(double) * n);
+  s->yp4 = (double *)calloc(n, sizeof(double));
   s->step = (in->right - in->left) / (n - 1);
   s->invstep = 1. / s->step;
   s->x[0] = in->left;
@@ -35,13 +102,25 @@ static void sp_setup(sp_t *s, const mzo_spline *in, const double *coeffs, int *c
   for (k = 0; k < n; ++k) s->y[k] = in->y[k];
   s->grad[0] = in->grad[0];
   s->grad[1] = in->grad[1];
+  s->grad2[0] = in->grad2[0];
+  s->grad2[1] = in->grad2[1];
   s->nat[0] = in->nat[0];
   s->nat[1] = in->nat[1];
   if (coeffs) {
+    /* Potential::coeff's walk: free knots, then per free end its slope and
+     * (spline5eq, Spline5Eq::bc_coeff spline5eq.cpp:459-468) its y''; only
+     * the first get_ncoeff() entries of the walk are coefficients */
     for (k = 0; k < n; ++k)
-      if (!in->y_fixed[k]) s->y[k] = coeffs[(*ci)++];
+      if (!in->y_fixed[k] && *ci < ncoeff) s->y[k] = coeffs[(*ci)++];
     for (i = 0; i < 2; ++i)
-      if (!in->grad_fixed[i] && !in->nat[i]) s->grad[i] = coeffs[(*ci)++];
+      if (!in->grad_fixed[i] && !in->nat[i]) {
+        if (*ci < ncoeff) s->grad[i] = coeffs[(*ci)++];
+        if (s->quintic && *ci < ncoeff) s->grad2[i] = coeffs[(*ci)++];
+      }
+  }
+  if (s->quintic) {
+    sp_refresh5(s);
+    return;
   }
   {
     double p, qn, un;
@@ -75,6 +154,7 @@ static void sp_free(sp_t *s) {
   free(s->x);
   free(s->y);
   free(s->ypp);
+  free(s->yp4);
 }
 
 /* Spline::get_knotshift (spline.cpp:74-99) */
@@ -93,8 +173,23 @@ static int sp_knotshift(const sp_t *s, double r, double *shift) {
   return knot;
 }
 
+/* Spline5Eq::splint_comb(int, double, double*) (spline5eq.h:110-127) */
+static double sp_comb_k5(const sp_t *s, int knot, double shift, double *grad) {
+  double a = 1.0 - shift, h = s->step;
+  double p1 = s->y[knot], d21 = s->ypp[knot], d41 = s->yp4[knot];
+  double p2 = s->y[knot + 1], d22 = s->ypp[knot + 1], d42 = s->yp4[knot + 1];
+  *grad = (p2 - p1) * s->invstep + ((3 * shift * shift - 1) * d22 - (3 * a * a - 1) * d21) * h / 6.0 +
+          ((15 * shift * shift * shift * shift - 30 * shift * shift + 7) * d42 -
+           (15 * a * a * a * a - 30 * a * a + 7) * d41) * (h * h * h) / 360.0;
+  return a * p1 + shift * p2 + ((a * a * a - a) * d21 + (shift * shift * shift - shift) * d22) * (h * h) / 6.0 +
+         ((3 * a * a * a * a * a - 10 * a * a * a + 7 * a) * d41 +
+          (3 * shift * shift * shift * shift * shift - 10 * shift * shift * shift + 7 * shift) * d42) *
+             (h * h * h * h) / 360.0;
+}
+
 /* Spline3Eq::splint_comb(int, double, double*) (spline3eq.h:110-122) */
 static double sp_comb_k(const sp_t *s, int knot, double shift, double *grad) {
+  if (s->quintic) return sp_comb_k5(s, knot, shift, grad);
   double a = 1.0 - shift;
   double p1 = s->y[knot], d21 = s->ypp[knot];
   double p2 = s->y[knot + 1], d22 = s->ypp[knot + 1];
@@ -106,6 +201,23 @@ static double sp_comb_k(const sp_t *s, int knot, double shift, double *grad) {
 static double sp_comb_x(const sp_t *s, double r, double *grad) {
   int n = s->n, k;
   double dr, b, a, p1, d21, p2, d22;
+  if (s->quintic) { /* Spline5Eq::splint_comb(double, double*) (spline5eq.h:226-255) */
+    if (r < s->x[0]) {
+      *grad = s->grad[0] + s->grad2[0] * (r - s->x[0]);
+      return s->y[0] + s->grad[0] * (r - s->x[0]) + 0.5 * s->grad2[0] * (r - s->x[0]) * (r - s->x[0]);
+    } else if (r > s->x[n - 1]) {
+      *grad = s->grad[1] + s->grad2[1] * (r - s->x[n - 1]);
+      return s->y[n - 1] + s->grad[1] * (r - s->x[n - 1]) + 0.5 * s->grad2[1] * (r - s->x[n - 1]) * (r - s->x[n - 1]);
+    }
+    dr = r - s->x[0];
+    if (dr < 0) k = 0;
+    else {
+      k = (int)(dr * s->invstep);
+      if (k >= n - 1) k = n - 2;
+    }
+    b = (dr - k * s->step) * s->invstep;
+    return sp_comb_k5(s, k, b, grad);
+  }
   if (r < s->x[0]) {
     *grad = s->grad[0];
     return s->y[0] + s->grad[0] * (r - s->x[0]);
@@ -163,7 +275,8 @@ double mzo_objective(const mzo_db *db, const mzo_pot *pot, const double *coeffs,
   const int N = db->natoms, NC = db->ncells;
   int s, ci = 0, i;
   sp_t *sp = (sp_t *)malloc(sizeof(sp_t) * pot->nsplines);
-  for (s = 0; s < pot->nsplines; ++s) sp_setup(&sp[s], &pot->splines[s], coeffs, &ci);
+  const int P = mzo_ncoeff(pot);
+  for (s = 0; s < pot->nsplines; ++s) sp_setup(&sp[s], &pot->splines[s], coeffs, &ci, P);
   const sp_t *phi = sp, *rho = pairpot ? NULL : sp + npair, *U = pairpot ? NULL : sp + npair + nt;
   const sp_t *ff = meam ? sp + npair + 2 * nt : NULL, *gg = meam ? sp + 2 * npair + 2 * nt : NULL;
   /* JMEAM groups after g: p (Pair_ij), q (Triplet_i) [, p2, q2] (pot_jmeam.cpp:31-45) */

@@ -14,6 +14,9 @@
  *   Potential::accumulate_error   src/potential.cpp:415-491
  *   Spline3Eq::refresh_basis      src/spline3eq.cpp:192-225
  *   Spline3Eq::splint_comb        src/spline3eq.h:110-122, 204-236
+ *   Spline5Eq::refresh_basis      src/spline5eq.cpp:209-293 (own Gaussian elimination
+ *                                 with partial pivoting in place of LAPACK dgesv)
+ *   Spline5Eq::splint_comb        src/spline5eq.h:110-127, 226-255
  *   Spline::get_knotshift         src/spline.cpp:74-99 (triplet cos knots)
  *   Triplet::setup_triplet        src/triplet.cpp:34-40
  *   Config::find_triplets         src/config.cpp:240-285 (all j<k pairs)
@@ -38,6 +41,8 @@ typedef struct {
   double grad[2];
   const int *y_fixed;
   const double *y;
+  int quintic;      /* spline5eq (spline5eq.cpp) */
+  double grad2[2];  /* spline5eq: y'' at the ends */
 } mzo_spline;
 
 typedef struct {

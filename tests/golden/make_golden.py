@@ -10,7 +10,7 @@ through Potential::compute for two coefficient vectors:
     fdgrad (central differences of the objective, h = 1e-6; small cases)
 
 Run here (needs the reference sources to build mzref):
-    make -C oracle && python tests/golden/make_golden.py [--gmeam | --grad10 | --pair | --jmeam]
+    make -C oracle && python tests/golden/make_golden.py [--gmeam | --grad10 | --pair | --jmeam | --quintic]
 """
 from __future__ import annotations
 
@@ -140,6 +140,37 @@ def jmeam_goldens():
     _write(JMEAM_CASES[2], synth.teacher_potential("jmeam2/spline", 2, 5.5, seed=27), cells, fd=True)
 
 
+Q5_CASES = ["eam_q5", "meam_q5_inrange", "pair_q5"]
+
+
+def quintic_goldens():
+    """spline5eq bases (Spline5Eq, spline5eq.cpp): end y'' read and written,
+    the 2n x 2n refresh, quadratic extrapolation of U, and the coefficient
+    walk that visits slope and y'' of every free end while get_ncoeff counts
+    one (spline5eq.cpp:81-85, 459-468)."""
+    # 13. EAM, three bcc cells; phi with both ends free, rho with a natural right end
+    _, cells = synth.make_workload("eam54", seed=17, ncells=3)
+    _targets(cells, 13)
+    pot = synth.quintic_variant(synth.teacher_potential("eam/spline", 1, 5.0, seed=28), seed=1)
+    pot.groups[0][0].bc = (0, 0)
+    pot.groups[1][0].bc = (0, -1)
+    _write(Q5_CASES[0], pot, cells)
+    # 14. MEAM in range (the start-up rescale runs), per-cell weights
+    _, cells = synth.make_workload("meam200", seed=18, ncells=3)
+    _targets(cells, 14)
+    for i, c in enumerate(cells):
+        c.weight = 1.0 + 0.3 * i
+    pot = synth.quintic_variant(in_range_meam(synth.teacher_potential("meam/spline", 1, 4.5, seed=29)), seed=2)
+    _write(Q5_CASES[1], pot, cells, energy_weight=1.2, stress_weight=0.6)
+    # 15. pair/spline, two species, one natural end
+    _, cells = synth.make_workload("meam2k", seed=19, ncells=4)
+    cells = [c for c in cells if c.natoms <= 300][:2] or cells[:1]
+    _targets(cells, 15)
+    pot = synth.quintic_variant(synth.teacher_potential("pair/spline", 2, 5.5, seed=30), seed=3)
+    pot.groups[0][1].bc = (-1, 0)
+    _write(Q5_CASES[2], pot, cells)
+
+
 def data_goldens(names=None):
     """ref.{rho,energy,stress,force,error,punish}: the text files the
     reference's Potential::write_data writes for the start potential."""
@@ -260,6 +291,11 @@ if __name__ == "__main__":
         jmeam_goldens()
         rescale_goldens(JMEAM_CASES)
         data_goldens(JMEAM_CASES)
+        sys.exit(0)
+    if "--quintic" in sys.argv:
+        quintic_goldens()
+        rescale_goldens(Q5_CASES)
+        data_goldens(Q5_CASES)
         sys.exit(0)
     if "--pair" in sys.argv:
         pair_goldens()

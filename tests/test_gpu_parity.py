@@ -156,7 +156,8 @@ def test_tensor_core_forward_opt_in(name, monkeypatch):
         assert np.max(np.abs(b["forces"][c] - a["forces"][c])) <= 5e-5
 
 
-@pytest.mark.parametrize("name", ["meam_mix6", "eam_bcc3", "pair_bcc1", "jmeam_inrange1"])
+@pytest.mark.parametrize("name", ["meam_mix6", "eam_bcc3", "pair_bcc1", "jmeam_inrange1", "eam_q5",
+                                  "meam_q5_inrange"])
 def test_rescale_then_objective_matches_reference(name):
     """Potential.rescale on the GPU densities, then the objective of the
     rescaled potential, against the reference's rescale + compute."""
@@ -180,7 +181,7 @@ def _same_layout(ours: str, ref: str):
         assert re.sub(r"[0-9]", "0", x) == re.sub(r"[0-9]", "0", y), (x, y)
 
 
-@pytest.mark.parametrize("name", ["meam_mix6", "eam_bcc3", "meam2_edge", "pair_mix2", "jmeam2_mix2"])
+@pytest.mark.parametrize("name", ["meam_mix6", "eam_bcc3", "meam2_edge", "pair_mix2", "jmeam2_mix2", "eam_q5"])
 def test_write_data_from_gpu_matches_reference_files(name, tmp_path):
     """Potential.write_data evaluates on the GPU (FP64) and writes the
     reference's data files: the same layout as the reference's files, and the
