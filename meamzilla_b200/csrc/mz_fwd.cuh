@@ -541,7 +541,7 @@ __global__ void __launch_bounds__(BLOCK_SLOTS, JM ? 2 : sizeof(R) == 4 ? 4 : 3)
         pen = w * 100.0 * 10. * (rho - hi) * (rho - hi);
         if (!pot.embed_extrap) rho = hi;
       }
-      const PointEval U = spl_point(tc, gU, rho);  // FP64 table of this candidate
+      const PointEval U = spl_point_t<Q5>(tc, gU, rho);  // FP64 table of this candidate
       a_dF[a] = U.grad;
       a_U[a] = U.val;
       double *ao = aout + (size_t)cand * AO_COUNT * N;
@@ -811,7 +811,7 @@ __global__ void k_final(DevDb db, DevPot pot, const SplineGeom *__restrict__ geo
       // U'(mid-range) punishment per type (pot_eam_spline.cpp:211-218)
       for (int ty = 0; ty < pot.ntypes; ++ty) {
         const SplineGeom &g = geom[pot.s_U + ty];
-        const double e = 100. * spl_point(tab, g, 0.5 * (g.x0 + g.xN)).grad;
+        const double e = 100. * spl_point_any(tab, g, 0.5 * (g.x0 + g.xN)).grad;
         total += e * e;
         if (ev) ev[ty] = e;
       }

@@ -141,7 +141,6 @@ __device__ __forceinline__ PointEval spl_point5(const double *tab, const SplineG
 }
 
 __device__ __forceinline__ PointEval spl_point(const double *tab, const SplineGeom &g, double r) {
-  if (g.q5) return spl_point5(tab, g, r);
   const double *y = tab + g.toff, *ypp = y + g.n, *ge = y + 2 * g.n;
   PointEval e;
   if (r < g.x0) {
@@ -168,6 +167,16 @@ __device__ __forceinline__ PointEval spl_point(const double *tab, const SplineGe
   e.k = k;
   e.b = b;
   return e;
+}
+
+// The basis chosen at compile time (the hot kernels) or from the spline.
+template <bool Q5>
+__device__ __forceinline__ PointEval spl_point_t(const double *tab, const SplineGeom &g, double r) {
+  if constexpr (Q5) return spl_point5(tab, g, r);
+  else return spl_point(tab, g, r);
+}
+__device__ __noinline__ PointEval spl_point_any(const double *tab, const SplineGeom &g, double r) {
+  return g.q5 ? spl_point5(tab, g, r) : spl_point(tab, g, r);
 }
 
 // Adds cv * d(value)/d(table) + cd * d(slope)/d(table) of a point evaluation
