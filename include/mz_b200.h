@@ -292,6 +292,20 @@ mz_status mz_launch_count(const mz_ctx *ctx, int64_t *launches);
  * No reference counterpart. */
 mz_status mz_tensor_core_forward(const mz_ctx *ctx, int *on);
 
+/* Launch variants chosen by the context's autotuner (no reference
+ * counterpart).  The first objective call of a precision, with or without
+ * the gradient, times on the caller's own candidates the forward kernel at
+ * three atom-block sizes (blocks of at most 256, 192 or 128 pair slots, a
+ * quarter as many atoms) and, for the gradient, the adjoint at the same three
+ * sizes and two persistent-grid sizes, and keeps the fastest for the
+ * context's lifetime (contexts of the same workload in one process share the
+ * choice).  The environment variable MZ_TUNE=0 at mz_create keeps the first
+ * variant of each.  The objective is the same for every variant; the
+ * gradient's table sums follow the block partition and may differ in the last
+ * bits between variants.  choice = {forward slots per block, adjoint slots
+ * per block, adjoint CTAs}, zeros before the first call. */
+mz_status mz_tuning(mz_ctx *ctx, int precision, int grad, int *choice);
+
 /* Kernels of the evaluator, for per-kernel timing. */
 enum {
   MZ_K_PREP = 0,    /* coefficients -> knot and evaluation tables          */

@@ -123,6 +123,7 @@ _SIGS = {
     "mz_tensor_core_forward": (C.c_int, [C.c_void_p, C.POINTER(C.c_int)]),
     "mz_kernel_name": (C.c_char_p, [C.c_int]),
     "mz_profile": (C.c_int, [C.c_void_p, C.c_int]),
+    "mz_tuning": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_void_p]),
     "mz_kernel_times": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
     "mz_alu_peak": (C.c_int, [C.c_int, C.c_int, C.POINTER(C.c_double)]),
     "mz_objective_noalloc": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(Settings), C.c_void_p, C.c_void_p,

@@ -83,6 +83,23 @@ struct mz_ctx {
   std::map<uint64_t, Graph> graphs;
   size_t smem_atoms[2] = {0, 0};  // [FP64, MIXED]
   size_t smem_adj[2] = {0, 0};
+  // Launch variants the autotuner picks from, per (precision, gradient):
+  // atoms per block of the forward and of the adjoint (partitions capped at
+  // TUNE_CAPS[i] pair slots and a quarter as many atoms) and the adjoint's
+  // persistent CTAs.  Every variant gives the same objective; the adjoint's
+  // FP64 table sums follow the partition (rounding-level differences).
+  static constexpr int NCAPS = 3;
+  const int *d_blk[NCAPS] = {};
+  int nblk[NCAPS] = {};
+  const int *d_adjblk[NCAPS] = {};
+  int nadjblk[NCAPS] = {};
+  int adj_ctas_max = 1, adj_per_sm = 1;
+  struct Tune {
+    bool done = false;
+    int fwd = 0, adj = 0, ctas = 0;
+  };
+  Tune tune[2][2];  // [precision][gradient]
+  bool autotune = true;
   bool profiling = false;
   struct Mark {
     int kernel;
@@ -92,6 +109,9 @@ struct mz_ctx {
 };
 
 namespace {
+
+// Atom-block caps (pair slots per block) the autotuner chooses among.
+constexpr int TUNE_CAPS[3] = {BLOCK_SLOTS, BLOCK_SLOTS * 3 / 4, BLOCK_SLOTS / 2};
 
 void ck(cudaError_t e, const char *what) {
   if (e != cudaSuccess) throw Failure{MZ_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e)};
@@ -361,11 +381,129 @@ void refresh_matrix5(const Spline3 &sp, std::vector<double> &M) {
   }
 }
 
+// ---------------------------------------------------------------- autotuner
+
+// Choices by workload, shared by the contexts of one process, so that
+// evaluators of the same database and potential structure launch the same
+// variants (and give bit-identical gradients).
+std::mutex g_tune_mu;
+std::map<std::vector<int64_t>, mz_ctx::Tune> g_tune_cache;
+
+void apply_variant(mz_ctx *ctx, const mz_ctx::Tune &t) {
+  ctx->db.nblocks = ctx->nblk[t.fwd];
+  ctx->db.blk_atom0 = ctx->d_blk[t.fwd];
+  ctx->db.adj_nblocks = ctx->nadjblk[t.adj];
+  ctx->db.adj_blk0 = ctx->d_adjblk[t.adj];
+  ctx->adj_ctas = t.ctas;
+}
+
+int adj_ctas_for(const mz_ctx *ctx, int v, int per_sm) {
+  return std::max(1, std::min(ctx->nadjblk[v], ctx->nsm * per_sm));
+}
+
+// One objective (+ gradient) with events around every kernel: the device
+// time of `kernel` in ms.  The caller's profiling marks are kept aside.
+double trial(mz_ctx *ctx, int n, const double *d_params, int precision, bool grad, int kernel) {
+  std::vector<mz_ctx::Mark> keep;
+  keep.swap(ctx->marks);
+  const bool prof = ctx->profiling;
+  ctx->profiling = true;
+  auto restore = [&] {
+    for (auto &m : ctx->marks) {
+      cudaEventDestroy(m.start);
+      cudaEventDestroy(m.stop);
+    }
+    ctx->marks.swap(keep);
+    ctx->profiling = prof;
+  };
+  double ms = 0.0;
+  try {
+    enqueue(ctx, n, d_params, precision, ctx->d_obj, nullptr, nullptr, nullptr, nullptr,
+            grad ? ctx->d_grad : nullptr);
+    ck(cudaStreamSynchronize(ctx->stream), "autotune trial");
+    for (auto &m : ctx->marks) {
+      float t = 0.f;
+      ck(cudaEventElapsedTime(&t, m.start, m.stop), "cudaEventElapsedTime");
+      if (m.kernel == kernel) ms += t;
+    }
+  } catch (...) {
+    restore();
+    throw;
+  }
+  restore();
+  return ms;
+}
+
+// Picks, once per (precision, gradient), the forward's atoms per block, then
+// the adjoint's atoms per block and persistent CTAs, by timing each on the
+// caller's own candidates; MZ_TUNE=0 keeps the first variant of each.
+void tune_variant(mz_ctx *ctx, int n, const double *d_params, int precision, bool grad) {
+  mz_ctx::Tune &t = ctx->tune[precision][grad ? 1 : 0];
+  if (!t.done) {
+    const std::vector<int64_t> key = {ctx->device,     ctx->natoms,    ctx->npairs, ctx->ncells, ctx->pot.style,
+                                      ctx->pot.ntypes, ctx->P,         precision,   grad,        ctx->q5,
+                                      ctx->autotune,   ctx->nblk[0],   ctx->nadjblk[0]};
+    bool cached = false;
+    {
+      std::lock_guard<std::mutex> lk(g_tune_mu);
+      auto it = g_tune_cache.find(key);
+      if (it != g_tune_cache.end()) {
+        t = it->second;
+        cached = true;
+      }
+    }
+    if (!cached) {
+      mz_ctx::Tune best;
+      best.ctas = adj_ctas_for(ctx, 0, ctx->adj_per_sm);
+      if (ctx->autotune) {
+        const int64_t l0 = ctx->launches;
+        apply_variant(ctx, best);
+        trial(ctx, n, d_params, precision, grad, MZ_K_ATOMS);  // warm-up
+        double bt = 1e300;
+        for (int v = 0; v < mz_ctx::NCAPS; ++v) {
+          mz_ctx::Tune c = best;
+          c.fwd = v;
+          apply_variant(ctx, c);
+          const double x = trial(ctx, n, d_params, precision, grad, MZ_K_ATOMS);
+          if (x < bt) {
+            bt = x;
+            best.fwd = v;
+          }
+        }
+        if (grad) {
+          double ba = 1e300;
+          for (int v = 0; v < mz_ctx::NCAPS; ++v)
+            for (int per = ctx->adj_per_sm; per >= std::max(1, ctx->adj_per_sm - 1); --per) {
+              mz_ctx::Tune c = best;
+              c.adj = v;
+              c.ctas = adj_ctas_for(ctx, v, per);
+              apply_variant(ctx, c);
+              const double x = trial(ctx, n, d_params, precision, grad, MZ_K_ADJ);
+              if (x < ba) {
+                ba = x;
+                best.adj = v;
+                best.ctas = c.ctas;
+              }
+            }
+        }
+        ctx->launches = l0;  // trials are not the caller's launches
+      }
+      best.done = true;
+      t = best;
+      std::lock_guard<std::mutex> lk(g_tune_mu);
+      g_tune_cache.emplace(key, best);
+    }
+    t.done = true;
+  }
+  apply_variant(ctx, t);
+}
+
 // The kernels of one objective call on the context's own buffers: captured
 // into a CUDA graph the first time a shape is seen, replayed afterwards (not
 // while profiling, whose per-kernel events are recorded around launches).
 constexpr size_t MAX_GRAPHS = 32;
 void launch_objective(mz_ctx *ctx, int n, int precision, bool ev, bool fo, bool en, bool st, bool gr) {
+  tune_variant(ctx, n, ctx->d_params, precision, gr);
   auto go = [&] {
     enqueue(ctx, n, ctx->d_params, precision, ctx->d_obj, ev ? ctx->d_errvec : nullptr, fo ? ctx->d_forces : nullptr,
             en ? ctx->d_energy : nullptr, st ? ctx->d_stress : nullptr, gr ? ctx->d_grad : nullptr);
@@ -629,13 +767,15 @@ mz_status mz_create(const mz_db *dbh, const mz_pot *poth, const mz_settings *set
       d.pair_uzf = dupload(ctx, uzf.data(), Np);
       d.pair_shiftf = dupload(ctx, shf.data(), nf * Np);
     }
-    // atom blocks: consecutive atoms, <= BLOCK_SLOTS slots and <= BLOCK_ATOMS atoms
-    std::vector<int> blk(1, 0);
-    {
+    // atom blocks: consecutive atoms, <= cap slots and <= cap / 4 atoms, for
+    // each of the autotuner's caps (a row longer than the cap is a block of its own)
+    for (int v = 0; v < mz_ctx::NCAPS; ++v) {
+      const int cap = TUNE_CAPS[v], acap = std::max(1, cap / 4);
+      std::vector<int> blk(1, 0);
       int slots = 0, atoms = 0;
       for (int i = 0; i < N; ++i) {
         const int n = (int)(db.pair_off[i + 1] - db.pair_off[i]);
-        if (atoms > 0 && (slots + n > BLOCK_SLOTS || atoms + 1 > BLOCK_ATOMS)) {
+        if (atoms > 0 && (slots + n > cap || atoms + 1 > acap)) {
           blk.push_back(i);
           slots = 0;
           atoms = 0;
@@ -644,33 +784,40 @@ mz_status mz_create(const mz_db *dbh, const mz_pot *poth, const mz_settings *set
         atoms += 1;
       }
       blk.push_back(N);
+      ctx->nblk[v] = (int)blk.size() - 1;
+      ctx->d_blk[v] = dupload(ctx, blk.data(), blk.size());
     }
-    d.nblocks = (int)blk.size() - 1;
-    d.blk_atom0 = dupload(ctx, blk.data(), blk.size());
+    d.nblocks = ctx->nblk[0];
+    d.blk_atom0 = ctx->d_blk[0];
     // type-pure atom blocks of the adjoint (one g-table type per block)
     {
       std::vector<int> order(N);
       for (int i = 0; i < N; ++i) order[i] = i;
       std::stable_sort(order.begin(), order.end(),
                        [&](int a, int b) { return db.atom_type[a] < db.atom_type[b]; });
-      std::vector<int> b0(1, 0);
-      int slots = 0, atoms = 0, ty = -1;
-      for (int q = 0; q < N; ++q) {
-        const int i = order[q];
-        const int n = (int)(db.pair_off[i + 1] - db.pair_off[i]);
-        if (atoms > 0 && (db.atom_type[i] != ty || slots + n > BLOCK_SLOTS || atoms + 1 > BLOCK_ATOMS)) {
-          b0.push_back(q);
-          slots = 0;
-          atoms = 0;
-        }
-        ty = db.atom_type[i];
-        slots += n;
-        atoms += 1;
-      }
-      b0.push_back(N);
-      d.adj_nblocks = (int)b0.size() - 1;
       d.adj_atoms = dupload(ctx, order.data(), order.size());
-      d.adj_blk0 = dupload(ctx, b0.data(), b0.size());
+      for (int v = 0; v < mz_ctx::NCAPS; ++v) {
+        const int cap = TUNE_CAPS[v], acap = std::max(1, cap / 4);
+        std::vector<int> b0(1, 0);
+        int slots = 0, atoms = 0, ty = -1;
+        for (int q = 0; q < N; ++q) {
+          const int i = order[q];
+          const int n = (int)(db.pair_off[i + 1] - db.pair_off[i]);
+          if (atoms > 0 && (db.atom_type[i] != ty || slots + n > cap || atoms + 1 > acap)) {
+            b0.push_back(q);
+            slots = 0;
+            atoms = 0;
+          }
+          ty = db.atom_type[i];
+          slots += n;
+          atoms += 1;
+        }
+        b0.push_back(N);
+        ctx->nadjblk[v] = (int)b0.size() - 1;
+        ctx->d_adjblk[v] = dupload(ctx, b0.data(), b0.size());
+      }
+      d.adj_nblocks = ctx->nadjblk[0];
+      d.adj_blk0 = ctx->d_adjblk[0];
     }
 
     // ---- shared memory of the kernels
@@ -719,8 +866,16 @@ mz_status mz_create(const mz_db *dbh, const mz_pot *poth, const mz_settings *set
     ck(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, ctx->device), "attribute");
     ck(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_adj<true, float>, BLOCK_SLOTS, ctx->smem_adj[1]),
        "occupancy");
-    ctx->adj_ctas = std::max(1, std::min(d.adj_nblocks, nsm * std::max(1, per_sm)));
+    ctx->adj_per_sm = std::max(1, per_sm);
+    int most_blocks = 0;
+    for (int v = 0; v < mz_ctx::NCAPS; ++v) most_blocks = std::max(most_blocks, ctx->nadjblk[v]);
+    ctx->adj_ctas_max = std::max(1, std::min(most_blocks, nsm * ctx->adj_per_sm));
+    ctx->adj_ctas = std::max(1, std::min(d.adj_nblocks, nsm * ctx->adj_per_sm));
     ctx->nsm = nsm;
+    {
+      const char *env = std::getenv("MZ_TUNE");
+      ctx->autotune = !(env && env[0] == '0');
+    }
     {
       const char *env = std::getenv("MZ_GRAPH");
       ctx->use_graphs = !(env && env[0] == '0');
@@ -744,7 +899,7 @@ mz_status mz_create(const mz_db *dbh, const mz_pot *poth, const mz_settings *set
     const size_t per_cand =
         sizeof(double) * ((size_t)(3 + (meam ? dp.aux_rows : 0)) * Np + (size_t)(AO_COUNT + 3 + 3) * N +
                           (size_t)ctx->esize + (size_t)(8 + 1 + CS_COUNT) * db.ncells + 2 * (size_t)stride + ctx->pstride +
-                          (size_t)ctx->adj_ctas * stride + 2 * (size_t)ctx->P + 1);
+                          (size_t)ctx->adj_ctas_max * stride + 2 * (size_t)ctx->P + 1);
     const size_t budget = (size_t)(0.6 * (double)freeb);
     const int cap = (int)std::max<size_t>(1, budget / std::max<size_t>(per_cand, 1));
     ctx->cand_cap = std::min(ctx->max_cand, cap);
@@ -763,7 +918,7 @@ mz_status mz_create(const mz_db *dbh, const mz_pot *poth, const mz_settings *set
     ctx->d_aux = meam ? dalloc<double>(ctx, C * dp.aux_rows * Np) : nullptr;
     ctx->d_lam = dalloc<double>(ctx, C * 3 * N);
     ctx->d_seeds = dalloc<double>(ctx, C * CS_COUNT * db.ncells);
-    ctx->d_partial = dalloc<double>(ctx, C * (size_t)ctx->adj_ctas * stride);
+    ctx->d_partial = dalloc<double>(ctx, C * (size_t)ctx->adj_ctas_max * stride);
     ctx->d_grad = dalloc<double>(ctx, C * ctx->P);
     ctx->d_ptabf = dalloc<float>(ctx, C * ctx->pstride);
     ctx->d_wtab = meam ? dalloc<float>(ctx, C * pot.ntypes * (2 * TC_NB - 1)) : nullptr;
@@ -806,6 +961,7 @@ mz_status mz_objective_device(mz_ctx *ctx, int ncand, const double *d_params, in
                     "ncand exceeds the candidates one launch can hold (" + std::to_string(ctx->cand_cap) + ")"};
     if (precision != MZ_FP64 && precision != MZ_MIXED) throw Failure{MZ_ERR_ARG, "unknown precision"};
     ck(cudaSetDevice(ctx->device), "cudaSetDevice");
+    tune_variant(ctx, ncand, d_params, precision, false);
     enqueue(ctx, ncand, d_params, precision, d_obj, d_errvec, d_forces, nullptr, nullptr, nullptr);
   });
 }
@@ -820,6 +976,7 @@ mz_status mz_objective_grad_device(mz_ctx *ctx, int ncand, const double *d_param
                     "ncand exceeds the candidates one launch can hold (" + std::to_string(ctx->cand_cap) + ")"};
     if (precision != MZ_FP64 && precision != MZ_MIXED) throw Failure{MZ_ERR_ARG, "unknown precision"};
     ck(cudaSetDevice(ctx->device), "cudaSetDevice");
+    tune_variant(ctx, ncand, d_params, precision, true);
     enqueue(ctx, ncand, d_params, precision, d_obj, nullptr, nullptr, nullptr, nullptr, d_grad);
   });
 }
@@ -832,6 +989,7 @@ mz_status mz_densities(mz_ctx *ctx, const double *params, double *dens) {
     ck(cudaSetDevice(ctx->device), "cudaSetDevice");
     ck(cudaMemcpyAsync(ctx->d_params, params, sizeof(double) * ctx->P, cudaMemcpyHostToDevice, ctx->stream),
        "params H2D");
+    tune_variant(ctx, 1, ctx->d_params, MZ_FP64, false);
     enqueue(ctx, 1, ctx->d_params, MZ_FP64, ctx->d_obj, nullptr, nullptr, nullptr, nullptr, nullptr);
     ck(cudaMemcpyAsync(dens, ctx->d_aout + (size_t)AO_RHO * ctx->natoms, sizeof(double) * ctx->natoms,
                        cudaMemcpyDeviceToHost, ctx->stream),
@@ -854,6 +1012,16 @@ const char *mz_kernel_name(int k) {
   static const char *names[MZ_NKERNELS] = {"k_prep", "k_atoms", "k_gather", "k_cells",
                                            "k_final", "k_adj", "k_grad_final"};
   return (k >= 0 && k < MZ_NKERNELS) ? names[k] : "?";
+}
+
+mz_status mz_tuning(mz_ctx *ctx, int precision, int grad, int *choice) {
+  return guarded([&] {
+    if (!ctx || !choice || (precision != MZ_FP64 && precision != MZ_MIXED)) throw Failure{MZ_ERR_ARG, "bad argument"};
+    const mz_ctx::Tune &t = ctx->tune[precision][grad ? 1 : 0];
+    choice[0] = t.done ? TUNE_CAPS[t.fwd] : 0;
+    choice[1] = t.done ? TUNE_CAPS[t.adj] : 0;
+    choice[2] = t.done ? t.ctas : 0;
+  });
 }
 
 mz_status mz_profile(mz_ctx *ctx, int on) {

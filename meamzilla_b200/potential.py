@@ -334,6 +334,14 @@ class Evaluator:
         check(lib().mz_tensor_core_forward(self._h, C.byref(on)))
         return bool(on.value)
 
+    def tuning(self, precision=MZ_MIXED, grad=True) -> dict:
+        """The autotuner's launch variant for (precision, gradient): forward
+        and adjoint pair slots per atom block, adjoint CTAs (zeros before
+        the first such call)."""
+        c = np.zeros(3, dtype=np.int32)
+        check(lib().mz_tuning(self._h, int(precision), 1 if grad else 0, ptr(c)))
+        return dict(forward_block_slots=int(c[0]), adjoint_block_slots=int(c[1]), adjoint_ctas=int(c[2]))
+
     def launches(self) -> int:
         n = C.c_int64()
         check(lib().mz_launch_count(self._h, C.byref(n)))
