@@ -42,6 +42,7 @@
 #include "mz_device.cuh"
 #include "mz_host.hpp"
 #include "mz_adj.cuh"
+#include "mz_fwd2.cuh"
 #include "mz_tc_fwd.cuh"
 
 // ================================================================= context
@@ -97,9 +98,13 @@ struct mz_ctx {
   struct Tune {
     bool done = false;
     int fwd = 0, adj = 0, ctas = 0;
+    int nc = 1;  // candidates per CTA of the forward (2: k_atoms2, mixed meam/spline)
   };
+  size_t smem_atoms2 = 0;
+  bool nc2_ok = false;  // k_atoms2 applies (meam/spline, spline3eq, CUDA-core forward)
+  int fwd_nc = 1;       // the variant in force
   Tune tune[2][2];  // [precision][gradient]
-  bool autotune = true;
+  int autotune = 1;  // MZ_TUNE: 1 time the variants, 0 the first variant, 2 the first with two candidates per CTA
   bool profiling = false;
   struct Mark {
     int kernel;
@@ -203,6 +208,14 @@ struct Bracket {
 template <bool MEAM, typename R, bool AUX>
 void launch_atoms(mz_ctx *ctx, int n, size_t smem) {
   dim3 ga(ctx->db.nblocks, n);
+  if constexpr (MEAM && sizeof(R) == 4) {
+    if (ctx->fwd_nc == 2 && ctx->nc2_ok) {  // two candidates per CTA, packed FP32 pairs
+      dim3 g2(ctx->db.nblocks, (n + 1) / 2);
+      k_atoms2<AUX><<<g2, BLOCK_SLOTS, ctx->smem_atoms2, ctx->stream>>>(
+          ctx->db, ctx->pot, ctx->d_geom, ctx->d_tabs, ctx->d_ptabs, ctx->d_V, ctx->d_aout, ctx->d_aux, n);
+      return;
+    }
+  }
   if constexpr (!AUX) {
     if (ctx->q5) {  // spline5eq pieces (objective only)
       k_atoms<MEAM, R, false, false, false, true><<<ga, BLOCK_SLOTS, smem, ctx->stream>>>(
@@ -390,6 +403,7 @@ std::mutex g_tune_mu;
 std::map<std::vector<int64_t>, mz_ctx::Tune> g_tune_cache;
 
 void apply_variant(mz_ctx *ctx, const mz_ctx::Tune &t) {
+  ctx->fwd_nc = t.nc;
   ctx->db.nblocks = ctx->nblk[t.fwd];
   ctx->db.blk_atom0 = ctx->d_blk[t.fwd];
   ctx->db.adj_nblocks = ctx->nadjblk[t.adj];
@@ -455,21 +469,26 @@ void tune_variant(mz_ctx *ctx, int n, const double *d_params, int precision, boo
     if (!cached) {
       mz_ctx::Tune best;
       best.ctas = adj_ctas_for(ctx, 0, ctx->adj_per_sm);
-      if (ctx->autotune) {
+      if (ctx->autotune == 2 && precision == MZ_MIXED && ctx->nc2_ok) best.nc = 2;
+      if (ctx->autotune == 1) {
         const int64_t l0 = ctx->launches;
         apply_variant(ctx, best);
         trial(ctx, n, d_params, precision, grad, MZ_K_ATOMS);  // warm-up
         double bt = 1e300;
-        for (int v = 0; v < mz_ctx::NCAPS; ++v) {
-          mz_ctx::Tune c = best;
-          c.fwd = v;
-          apply_variant(ctx, c);
-          const double x = trial(ctx, n, d_params, precision, grad, MZ_K_ATOMS);
-          if (x < bt) {
-            bt = x;
-            best.fwd = v;
+        const int ncs = (precision == MZ_MIXED && ctx->nc2_ok && n > 1) ? 2 : 1;
+        for (int nc = 1; nc <= ncs; ++nc)
+          for (int v = 0; v < mz_ctx::NCAPS; ++v) {
+            mz_ctx::Tune c = best;
+            c.fwd = v;
+            c.nc = nc;
+            apply_variant(ctx, c);
+            const double x = trial(ctx, n, d_params, precision, grad, MZ_K_ATOMS);
+            if (x < bt) {
+              bt = x;
+              best.fwd = v;
+              best.nc = nc;
+            }
           }
-        }
         if (grad) {
           double ba = 1e300;
           for (int v = 0; v < mz_ctx::NCAPS; ++v)
@@ -858,6 +877,12 @@ mz_status mz_create(const mz_db *dbh, const mz_pot *poth, const mz_settings *set
     smem_attr(k_atoms<true, float, true, false, true>, ctx->smem_atoms[1]);
     smem_attr(k_adj<true, double, false, true>, ctx->smem_adj[0]);
     smem_attr(k_adj<true, float, false, true>, ctx->smem_adj[1]);
+    ctx->smem_atoms2 = atoms2_smem_bytes(ns, ctx->pstride);
+    ctx->nc2_ok = pot.style == MZ_STYLE_MEAM_SPLINE && !ctx->q5 && ctx->smem_atoms2 <= (size_t)smem_max;
+    if (ctx->nc2_ok) {
+      smem_attr(k_atoms2<true>, ctx->smem_atoms2);
+      smem_attr(k_atoms2<false>, ctx->smem_atoms2);
+    }
     smem_attr(k_atoms<true, double, false, false, false, true>, ctx->smem_atoms[0]);
     smem_attr(k_atoms<false, double, false, false, false, true>, ctx->smem_atoms[0]);
     smem_attr(k_atoms<true, float, false, false, false, true>, ctx->smem_atoms[1]);
@@ -874,7 +899,7 @@ mz_status mz_create(const mz_db *dbh, const mz_pot *poth, const mz_settings *set
     ctx->nsm = nsm;
     {
       const char *env = std::getenv("MZ_TUNE");
-      ctx->autotune = !(env && env[0] == '0');
+      ctx->autotune = (env && env[0] == '0') ? 0 : (env && env[0] == '2') ? 2 : 1;
     }
     {
       const char *env = std::getenv("MZ_GRAPH");
@@ -1021,6 +1046,7 @@ mz_status mz_tuning(mz_ctx *ctx, int precision, int grad, int *choice) {
     choice[0] = t.done ? TUNE_CAPS[t.fwd] : 0;
     choice[1] = t.done ? TUNE_CAPS[t.adj] : 0;
     choice[2] = t.done ? t.ctas : 0;
+    choice[3] = t.done ? t.nc : 0;
   });
 }
 
