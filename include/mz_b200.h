@@ -299,16 +299,17 @@ mz_status mz_tensor_core_forward(const mz_ctx *ctx, int *on);
  * quarter as many atoms) and, for the gradient, the adjoint at the same three
  * sizes and two persistent-grid sizes, and keeps the fastest for the
  * context's lifetime (contexts of the same workload in one process share the
- * choice).  For meam/spline in mixed precision the forward is also timed with
- * two candidates per CTA (the triplet geometry shared, both candidates'
- * arithmetic as packed FP32 pairs).  The environment variable MZ_TUNE=0 at
+ * choice).  For meam/spline in mixed precision the forward and the adjoint
+ * are also timed with two candidates per CTA (the triplet geometry shared,
+ * both candidates' arithmetic as packed FP32 pairs).  The environment variable MZ_TUNE=0 at
  * mz_create keeps the first variant of each, MZ_TUNE=2 the first with two
  * candidates per CTA where that applies.  Block sizes leave the results
  * unchanged; two candidates per CTA change the order of FP32 additions
  * inside chunks of 8 partners, and the gradient's table sums follow the block
  * partition, so those may differ in the last bits between variants.
- * choice[4] = {forward slots per block, adjoint slots per block, adjoint
- * CTAs, forward candidates per CTA}, zeros before the first call. */
+ * choice[5] = {forward slots per block, adjoint slots per block, adjoint
+ * CTAs, forward candidates per CTA, adjoint candidates per CTA}, zeros
+ * before the first call. */
 mz_status mz_tuning(mz_ctx *ctx, int precision, int grad, int *choice);
 
 /* Kernels of the evaluator, for per-kernel timing. */

@@ -43,6 +43,7 @@
 #include "mz_host.hpp"
 #include "mz_adj.cuh"
 #include "mz_fwd2.cuh"
+#include "mz_adj2.cuh"
 #include "mz_tc_fwd.cuh"
 
 // ================================================================= context
@@ -98,11 +99,14 @@ struct mz_ctx {
   struct Tune {
     bool done = false;
     int fwd = 0, adj = 0, ctas = 0;
-    int nc = 1;  // candidates per CTA of the forward (2: k_atoms2, mixed meam/spline)
+    int nc = 1;      // candidates per CTA of the forward (2: k_atoms2, mixed meam/spline)
+    int adj_nc = 1;  // candidates per CTA of the adjoint (2: k_adj2)
   };
-  size_t smem_atoms2 = 0;
-  bool nc2_ok = false;  // k_atoms2 applies (meam/spline, spline3eq, CUDA-core forward)
-  int fwd_nc = 1;       // the variant in force
+  size_t smem_atoms2 = 0, smem_adj2 = 0;
+  bool nc2_ok = false;  // k_atoms2 / k_adj2 apply (meam/spline, spline3eq, CUDA-core forward)
+  int adj2_per_sm = 1;
+  double *d_wglob = nullptr;  // k_adj2's per-warp FP64 tables
+  int fwd_nc = 1, adj_nc = 1;  // the variants in force
   Tune tune[2][2];  // [precision][gradient]
   int autotune = 1;  // MZ_TUNE: 1 time the variants, 0 the first variant, 2 the first with two candidates per CTA
   bool profiling = false;
@@ -242,6 +246,15 @@ void launch_atoms(mz_ctx *ctx, int n, size_t smem) {
 template <bool MEAM, typename R>
 void launch_adj(mz_ctx *ctx, int n, size_t smem) {
   dim3 ga(ctx->adj_ctas, n);
+  if constexpr (MEAM && sizeof(R) == 4) {
+    if (ctx->adj_nc == 2 && ctx->nc2_ok) {  // two candidates per CTA, packed FP32 pairs
+      dim3 g2(ctx->adj_ctas, (n + 1) / 2);
+      k_adj2<<<g2, BLOCK_SLOTS, ctx->smem_adj2, ctx->stream>>>(ctx->db, ctx->pot, ctx->d_geom, ctx->d_tabs,
+                                                               ctx->d_ptabs, ctx->d_aout, ctx->d_aux, ctx->d_lam,
+                                                               ctx->d_seeds, ctx->d_wglob, ctx->d_partial, n);
+      return;
+    }
+  }
   if constexpr (MEAM) {
     if (ctx->pot.nj > 0) {
       k_adj<MEAM, R, false, true><<<ga, BLOCK_SLOTS, smem, ctx->stream>>>(
@@ -404,6 +417,7 @@ std::map<std::vector<int64_t>, mz_ctx::Tune> g_tune_cache;
 
 void apply_variant(mz_ctx *ctx, const mz_ctx::Tune &t) {
   ctx->fwd_nc = t.nc;
+  ctx->adj_nc = t.adj_nc;
   ctx->db.nblocks = ctx->nblk[t.fwd];
   ctx->db.blk_atom0 = ctx->d_blk[t.fwd];
   ctx->db.adj_nblocks = ctx->nadjblk[t.adj];
@@ -469,7 +483,11 @@ void tune_variant(mz_ctx *ctx, int n, const double *d_params, int precision, boo
     if (!cached) {
       mz_ctx::Tune best;
       best.ctas = adj_ctas_for(ctx, 0, ctx->adj_per_sm);
-      if (ctx->autotune == 2 && precision == MZ_MIXED && ctx->nc2_ok) best.nc = 2;
+      if (ctx->autotune == 2 && precision == MZ_MIXED && ctx->nc2_ok) {
+        best.nc = 2;
+        best.adj_nc = 2;
+        best.ctas = adj_ctas_for(ctx, 0, ctx->adj2_per_sm);
+      }
       if (ctx->autotune == 1) {
         const int64_t l0 = ctx->launches;
         apply_variant(ctx, best);
@@ -491,19 +509,25 @@ void tune_variant(mz_ctx *ctx, int n, const double *d_params, int precision, boo
           }
         if (grad) {
           double ba = 1e300;
-          for (int v = 0; v < mz_ctx::NCAPS; ++v)
-            for (int per = ctx->adj_per_sm; per >= std::max(1, ctx->adj_per_sm - 1); --per) {
-              mz_ctx::Tune c = best;
-              c.adj = v;
-              c.ctas = adj_ctas_for(ctx, v, per);
-              apply_variant(ctx, c);
-              const double x = trial(ctx, n, d_params, precision, grad, MZ_K_ADJ);
-              if (x < ba) {
-                ba = x;
-                best.adj = v;
-                best.ctas = c.ctas;
+          const int ancs = (precision == MZ_MIXED && ctx->nc2_ok && n > 1) ? 2 : 1;
+          for (int anc = 1; anc <= ancs; ++anc) {
+            const int pmax = anc == 2 ? ctx->adj2_per_sm : ctx->adj_per_sm;
+            for (int v = 0; v < mz_ctx::NCAPS; ++v)
+              for (int per = pmax; per >= std::max(1, pmax - 1); --per) {
+                mz_ctx::Tune c = best;
+                c.adj = v;
+                c.adj_nc = anc;
+                c.ctas = adj_ctas_for(ctx, v, per);
+                apply_variant(ctx, c);
+                const double x = trial(ctx, n, d_params, precision, grad, MZ_K_ADJ);
+                if (x < ba) {
+                  ba = x;
+                  best.adj = v;
+                  best.adj_nc = anc;
+                  best.ctas = c.ctas;
+                }
               }
-            }
+          }
         }
         ctx->launches = l0;  // trials are not the caller's launches
       }
@@ -878,10 +902,13 @@ mz_status mz_create(const mz_db *dbh, const mz_pot *poth, const mz_settings *set
     smem_attr(k_adj<true, double, false, true>, ctx->smem_adj[0]);
     smem_attr(k_adj<true, float, false, true>, ctx->smem_adj[1]);
     ctx->smem_atoms2 = atoms2_smem_bytes(ns, ctx->pstride);
-    ctx->nc2_ok = pot.style == MZ_STYLE_MEAM_SPLINE && !ctx->q5 && ctx->smem_atoms2 <= (size_t)smem_max;
+    ctx->smem_adj2 = adj2_smem_bytes(ns, stride, ctx->pstride, ng);
+    ctx->nc2_ok = pot.style == MZ_STYLE_MEAM_SPLINE && !ctx->q5 && ctx->smem_atoms2 <= (size_t)smem_max &&
+                  ctx->smem_adj2 <= (size_t)smem_max;
     if (ctx->nc2_ok) {
       smem_attr(k_atoms2<true>, ctx->smem_atoms2);
       smem_attr(k_atoms2<false>, ctx->smem_atoms2);
+      smem_attr(k_adj2, ctx->smem_adj2);
     }
     smem_attr(k_atoms<true, double, false, false, false, true>, ctx->smem_atoms[0]);
     smem_attr(k_atoms<false, double, false, false, false, true>, ctx->smem_atoms[0]);
@@ -892,6 +919,11 @@ mz_status mz_create(const mz_db *dbh, const mz_pot *poth, const mz_settings *set
     ck(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_adj<true, float>, BLOCK_SLOTS, ctx->smem_adj[1]),
        "occupancy");
     ctx->adj_per_sm = std::max(1, per_sm);
+    if (ctx->nc2_ok) {
+      int p2 = 0;
+      ck(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&p2, k_adj2, BLOCK_SLOTS, ctx->smem_adj2), "occupancy");
+      ctx->adj2_per_sm = std::max(1, p2);
+    }
     int most_blocks = 0;
     for (int v = 0; v < mz_ctx::NCAPS; ++v) most_blocks = std::max(most_blocks, ctx->nadjblk[v]);
     ctx->adj_ctas_max = std::max(1, std::min(most_blocks, nsm * ctx->adj_per_sm));
@@ -924,7 +956,8 @@ mz_status mz_create(const mz_db *dbh, const mz_pot *poth, const mz_settings *set
     const size_t per_cand =
         sizeof(double) * ((size_t)(3 + (meam ? dp.aux_rows : 0)) * Np + (size_t)(AO_COUNT + 3 + 3) * N +
                           (size_t)ctx->esize + (size_t)(8 + 1 + CS_COUNT) * db.ncells + 2 * (size_t)stride + ctx->pstride +
-                          (size_t)ctx->adj_ctas_max * stride + 2 * (size_t)ctx->P + 1);
+                          (size_t)ctx->adj_ctas_max * stride * (ctx->nc2_ok ? 1 + ADJ_WARPS : 1) +
+                          2 * (size_t)ctx->P + 1);
     const size_t budget = (size_t)(0.6 * (double)freeb);
     const int cap = (int)std::max<size_t>(1, budget / std::max<size_t>(per_cand, 1));
     ctx->cand_cap = std::min(ctx->max_cand, cap);
@@ -944,6 +977,7 @@ mz_status mz_create(const mz_db *dbh, const mz_pot *poth, const mz_settings *set
     ctx->d_lam = dalloc<double>(ctx, C * 3 * N);
     ctx->d_seeds = dalloc<double>(ctx, C * CS_COUNT * db.ncells);
     ctx->d_partial = dalloc<double>(ctx, C * (size_t)ctx->adj_ctas_max * stride);
+    if (ctx->nc2_ok) ctx->d_wglob = dalloc<double>(ctx, C * (size_t)ctx->adj_ctas_max * ADJ_WARPS * stride);
     ctx->d_grad = dalloc<double>(ctx, C * ctx->P);
     ctx->d_ptabf = dalloc<float>(ctx, C * ctx->pstride);
     ctx->d_wtab = meam ? dalloc<float>(ctx, C * pot.ntypes * (2 * TC_NB - 1)) : nullptr;
@@ -1047,6 +1081,7 @@ mz_status mz_tuning(mz_ctx *ctx, int precision, int grad, int *choice) {
     choice[1] = t.done ? TUNE_CAPS[t.adj] : 0;
     choice[2] = t.done ? t.ctas : 0;
     choice[3] = t.done ? t.nc : 0;
+    choice[4] = t.done ? t.adj_nc : 0;
   });
 }
 

@@ -336,12 +336,12 @@ class Evaluator:
 
     def tuning(self, precision=MZ_MIXED, grad=True) -> dict:
         """The autotuner's launch variant for (precision, gradient): forward
-        and adjoint pair slots per atom block, adjoint CTAs, forward
-        candidates per CTA (zeros before the first such call)."""
-        c = np.zeros(4, dtype=np.int32)
+        and adjoint pair slots per atom block, adjoint CTAs, forward and
+        adjoint candidates per CTA (zeros before the first such call)."""
+        c = np.zeros(5, dtype=np.int32)
         check(lib().mz_tuning(self._h, int(precision), 1 if grad else 0, ptr(c)))
         return dict(forward_block_slots=int(c[0]), adjoint_block_slots=int(c[1]), adjoint_ctas=int(c[2]),
-                    forward_candidates_per_cta=int(c[3]))
+                    forward_candidates_per_cta=int(c[3]), adjoint_candidates_per_cta=int(c[4]))
 
     def launches(self) -> int:
         n = C.c_int64()

@@ -58,11 +58,12 @@ def test_tuned_and_untuned_variants_agree(monkeypatch):
 
 @pytest.mark.parametrize("name", ["meam_mix6", "meam2_edge", "meam_inrange_w"])
 def test_two_candidates_per_cta_match_one(name, monkeypatch):
-    """k_atoms2 (two candidates per CTA, packed FP32 pairs) against k_atoms:
-    for an odd number of candidates (the last CTA holds one) both meet the
-    mixed-precision bars against FP64 (objective 1e-6, forces 1e-5 eV/A;
-    their FP32 roundings differ, so they are not bit-identical), the
-    gradients agree, and the FP64 path is untouched."""
+    """k_atoms2 / k_adj2 (two candidates per CTA, packed FP32 pairs) against
+    k_atoms / k_adj: for an odd number of candidates (the last CTA holds
+    one) both meet the mixed-precision bars against FP64 (objective 1e-6,
+    forces 1e-5 eV/A, gradient 1e-4 of its largest component; their FP32
+    roundings differ, so they are not bit-identical), and the FP64 path is
+    untouched."""
     from conftest import load_case
     from meamzilla_b200.potential import MZ_FP64, MZ_MIXED, Evaluator
     case = load_case(name)
@@ -83,6 +84,11 @@ def test_two_candidates_per_cta_match_one(name, monkeypatch):
         assert np.max(np.abs(r["forces"] - ref["forces"])) <= 1e-5
     oa, ga = one.objective_grad(X, MZ_MIXED)
     ob, gb = two.objective_grad(X, MZ_MIXED)
+    assert two.tuning(MZ_MIXED, True)["adjoint_candidates_per_cta"] == 2
     assert np.max(np.abs(oa - ob) / oa) <= 1e-6
     assert np.max(np.abs(ga - gb)) <= 1e-4 * np.max(np.abs(ga))
+    _, g64 = one.objective_grad(X, MZ_FP64)
+    assert np.max(np.abs(gb - g64)) <= 1e-4 * np.max(np.abs(g64))
+    # repeated calls of the two-candidate adjoint are bit-identical
+    assert np.array_equal(two.objective_grad(X, MZ_MIXED)[1], gb)
     assert np.array_equal(ref["obj"], two.objective(X, MZ_FP64))
