@@ -24,7 +24,7 @@ namespace mzb {
 //   float  ftab[2][ADJ_WARPS][stride]     per-warp pair-function gradients of one block
 //   double red[2][BLOCK_SLOTS], a_chi[2][BLOCK_ATOMS], a_dF[2][BLOCK_ATOMS]
 //   SplineGeom sg[nsplines]; int a_lo[BLOCK_ATOMS+2], a_idx[BLOCK_ATOMS], a_len[BLOCK_ATOMS]
-//   float pt2[2 pstride + 8]             both candidates' evaluation tables, interleaved
+//   float4 pt2[2][pstride / 4 + 1]       both candidates' evaluation tables, interleaved
 //   float4 srow[BLOCK_SLOTS+8]           (u_x, u_y, u_z, 0)
 //   float2 sf[BLOCK_SLOTS+8]             (f_A, f_B)
 //   float4 sq0[BLOCK_SLOTS+8]            (a f'_A, a f'_B, a f / r _A, a f / r _B)
@@ -38,7 +38,7 @@ __host__ __device__ inline size_t adj2_smem_bytes(int nsplines, int stride, int 
   b += sizeof(SplineGeom) * nsplines;
   b += sizeof(int) * (3 * BLOCK_ATOMS + 2);
   b = (b + 31) & ~size_t(31);
-  b += sizeof(float) * (2 * (size_t)pstride + 8);
+  b += sizeof(float4) * 2 * ((size_t)pstride / 4 + 1);
   b = (b + 31) & ~size_t(31);
   b += (3 * sizeof(float4) + 2 * sizeof(float2)) * (BLOCK_SLOTS + 8);
   return b;
@@ -75,8 +75,9 @@ __global__ void __launch_bounds__(BLOCK_SLOTS, 2)
   int *a_len = a_idx + BLOCK_ATOMS;
   off = reinterpret_cast<unsigned char *>(a_len + BLOCK_ATOMS) - smem_raw;
   off = (off + 31) & ~size_t(31);
-  float *pt2 = reinterpret_cast<float *>(smem_raw + off);
-  off += sizeof(float) * (2 * (size_t)pot.pow_stride + 8);
+  float4 *pt2 = reinterpret_cast<float4 *>(smem_raw + off);
+  const int npiece = pot.pow_stride / 4;
+  off += sizeof(float4) * 2 * ((size_t)npiece + 1);
   off = (off + 31) & ~size_t(31);
   float4 *srow = reinterpret_cast<float4 *>(smem_raw + off);
   float4 *sq0 = srow + BLOCK_SLOTS + 8;
@@ -84,11 +85,7 @@ __global__ void __launch_bounds__(BLOCK_SLOTS, 2)
   float2 *sf = reinterpret_cast<float2 *>(sq1 + BLOCK_SLOTS + 8);
   float2 *sqz = sf + BLOCK_SLOTS + 8;
 
-  const double *pcA = ptabs + (size_t)cA * pot.pow_stride, *pcB = ptabs + (size_t)cB * pot.pow_stride;
-  for (int i = tid; i < pot.pow_stride; i += blockDim.x) {
-    pt2[2 * i] = (float)pcA[i];
-    pt2[2 * i + 1] = (float)pcB[i];
-  }
+  load_pt2(pt2, ptabs + (size_t)cA * pot.pow_stride, ptabs + (size_t)cB * pot.pow_stride, pot.pow_stride);
   for (int i = tid; i < 2 * ADJ_WARPS * stride; i += blockDim.x) ftab[i] = 0.f;
   for (int i = tid; i < 2 * nint * BLOCK_SLOTS; i += blockDim.x) gacc[i] = make_float4(0.f, 0.f, 0.f, 0.f);
   for (int i = tid; i < pot.nsplines; i += blockDim.x) sg[i] = geom[i];
@@ -199,17 +196,17 @@ __global__ void __launch_bounds__(BLOCK_SLOTS, 2)
       if (kphi >= 0) {
         const SplineGeom &g = sg[pot.s_phi + pij];
         bphi = db.pair_shiftf[gs];
-        cubic2_val_grad(pt2, g.poff, kphi, bphi, (float)g.invstep, dphi);
+        cubic2_val_grad(pt2, npiece, g.poff, kphi, bphi, (float)g.invstep, dphi);
       }
       if (krho >= 0) {
         const SplineGeom &g = sg[pot.s_rho + tj];
         brho = db.pair_shiftf[Np + gs];
-        cubic2_val_grad(pt2, g.poff, krho, brho, (float)g.invstep, drho);
+        cubic2_val_grad(pt2, npiece, g.poff, krho, brho, (float)g.invstep, drho);
       }
       if (kf >= 0) {
         const SplineGeom &g = sg[pot.s_f + pij];
         bf = db.pair_shiftf[2 * Np + gs];
-        f = cubic2_val_grad(pt2, g.poff, kf, bf, (float)g.invstep, df);
+        f = cubic2_val_grad(pt2, npiece, g.poff, kf, bf, (float)g.invstep, df);
       }
       const double ux = db.pair_ux[gs], uy = db.pair_uy[gs], uz = db.pair_uz[gs], r = db.pair_r[gs];
       const double ip = (double)invr;
@@ -313,7 +310,7 @@ __global__ void __launch_bounds__(BLOCK_SLOTS, 2)
           float b;
           const int m = g_knot<float>(cs, gx0, ginv, ngt, b);
           float2 dg;
-          const float2 gv = cubic2_val_grad(pt2, goff, m, b, ginv, dg);
+          const float2 gv = cubic2_val_grad(pt2, npiece, goff, m, b, ginv, dg);
           const float4 q0 = sq0[k], q1 = sq1[k];
           const float2 qz = sqz[k];
           const float2 cs2 = bcast2(cs);

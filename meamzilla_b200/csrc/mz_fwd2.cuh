@@ -6,9 +6,10 @@
 // (slot, partner) and evaluates both candidates' pieces and row sums as FP32
 // pairs with the sm_100 packed instructions (__ffma2_rn and friends, one
 // instruction for two lanes of arithmetic).  The two candidates' evaluation
-// tables are interleaved in shared memory -- coefficient q of piece k of
-// candidate c at 2 (poff + 4 k + q) + c -- so that one 16-byte load brings a
-// coefficient pair of both.  Results per candidate are those of k_atoms'
+// tables are interleaved in shared memory -- for piece i (over all splines)
+// lo[i] = (c0 A, c0 B, c1 A, c1 B) and hi[i] = (c2 A, c2 B, c3 A, c3 B) in two
+// arrays with a 16-byte stride -- so that one 16-byte load brings two
+// coefficient pairs of both.  Results per candidate are those of k_atoms'
 // mixed path up to the order of FP32 additions inside each chunk of 8
 // partners (the chunk sums are added to FP64 totals as there).
 //
@@ -26,13 +27,14 @@ __device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __
 __device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
 __device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
 
-// Value and slope of piece k of the spline at evaluation-table offset `off`,
-// for both candidates of the interleaved table pt2.
-__device__ __forceinline__ float2 cubic2_val_grad(const float *pt2, int off, int k, float b, float inv,
+// Value and slope of piece k of the spline at evaluation-table offset `off`
+// (a multiple of 4), for both candidates of the interleaved table pt2: lo
+// pairs at pt2[i], hi pairs at pt2[npiece + i], i = off / 4 + k.
+__device__ __forceinline__ float2 cubic2_val_grad(const float4 *pt2, int npiece, int off, int k, float b, float inv,
                                                   float2 &grad) {
-  const float *c = pt2 + 2 * (off + 4 * k);
-  const float4 lo = *reinterpret_cast<const float4 *>(c);      // c0A c0B c1A c1B
-  const float4 hi = *reinterpret_cast<const float4 *>(c + 4);  // c2A c2B c3A c3B
+  const int i = (off >> 2) + k;
+  const float4 lo = pt2[i];           // c0A c0B c1A c1B
+  const float4 hi = pt2[npiece + i];  // c2A c2B c3A c3B
   const float2 c0 = pair2(lo.x, lo.y), c1 = pair2(lo.z, lo.w), c2 = pair2(hi.x, hi.y), c3 = pair2(hi.z, hi.w);
   const float2 bb = bcast2(b);
   const float2 slope = fma2(bb, fma2(bcast2(3.f * b), c3, add2(c2, c2)), c1);  // c1 + b (2 c2 + 3 b c3)
@@ -45,7 +47,7 @@ __device__ __forceinline__ float2 cubic2_val_grad(const float *pt2, int off, int
 //   double a_dF[2][BLOCK_ATOMS], a_U[2][BLOCK_ATOMS]
 //   SplineGeom sg[nsplines]
 //   int a_lo[BLOCK_ATOMS+2]
-//   float pt2[2 pstride + 8]           the two candidates' evaluation tables, interleaved
+//   float4 pt2[2][pstride / 4 + 1]     the two candidates' evaluation tables, interleaved
 //   float4 srow[BLOCK_SLOTS+8]         (u_x, u_y, u_z, 0) of every slot
 //   float2 sf[BLOCK_SLOTS+8]           (f of candidate A, f of candidate B) of every slot
 __host__ __device__ inline size_t atoms2_smem_bytes(int nsplines, int pstride) {
@@ -53,11 +55,21 @@ __host__ __device__ inline size_t atoms2_smem_bytes(int nsplines, int pstride) {
   b += sizeof(SplineGeom) * nsplines;
   b += sizeof(int) * (BLOCK_ATOMS + 2);
   b = (b + 31) & ~size_t(31);
-  b += sizeof(float) * (2 * (size_t)pstride + 8);
+  b += sizeof(float4) * 2 * ((size_t)pstride / 4 + 1);
   b = (b + 31) & ~size_t(31);
   b += sizeof(float4) * (BLOCK_SLOTS + 8);
   b += sizeof(float2) * (BLOCK_SLOTS + 8);
   return b;
+}
+
+// Both candidates' evaluation tables into the interleaved layout.
+__device__ __forceinline__ void load_pt2(float4 *pt2, const double *pcA, const double *pcB, int pstride) {
+  const int np = pstride / 4;
+  for (int i = threadIdx.x; i < np; i += blockDim.x) {
+    const double *a = pcA + 4 * i, *b = pcB + 4 * i;
+    pt2[i] = make_float4((float)a[0], (float)b[0], (float)a[1], (float)b[1]);
+    pt2[np + i] = make_float4((float)a[2], (float)b[2], (float)a[3], (float)b[3]);
+  }
 }
 
 // One CTA per (atom block, candidate pair), one thread per pair slot;
@@ -85,18 +97,15 @@ __global__ void __launch_bounds__(BLOCK_SLOTS, 3)
   size_t off = sizeof(double) * (10 * BLOCK_SLOTS + 4 * BLOCK_ATOMS) + sizeof(SplineGeom) * pot.nsplines +
                sizeof(int) * (BLOCK_ATOMS + 2);
   off = (off + 31) & ~size_t(31);
-  float *pt2 = reinterpret_cast<float *>(smem_raw + off);
-  off += sizeof(float) * (2 * (size_t)pot.pow_stride + 8);
+  float4 *pt2 = reinterpret_cast<float4 *>(smem_raw + off);
+  const int npiece = pot.pow_stride / 4;
+  off += sizeof(float4) * 2 * ((size_t)npiece + 1);
   off = (off + 31) & ~size_t(31);
   float4 *srow = reinterpret_cast<float4 *>(smem_raw + off);
   float2 *sf = reinterpret_cast<float2 *>(srow + BLOCK_SLOTS + 8);
 
   const BlockRows br = block_rows(db, blockIdx.x);
-  const double *pcA = ptabs + (size_t)cA * pot.pow_stride, *pcB = ptabs + (size_t)cB * pot.pow_stride;
-  for (int i = tid; i < pot.pow_stride; i += blockDim.x) {
-    pt2[2 * i] = (float)pcA[i];
-    pt2[2 * i + 1] = (float)pcB[i];
-  }
+  load_pt2(pt2, ptabs + (size_t)cA * pot.pow_stride, ptabs + (size_t)cB * pot.pow_stride, pot.pow_stride);
   for (int i = tid; i < pot.nsplines; i += blockDim.x) sg[i] = geom[i];
   for (int a = tid; a <= br.na; a += blockDim.x) a_lo[a] = db.pair_off[br.atom_lo + a] - br.slot_lo;
   __syncthreads();
@@ -120,15 +129,15 @@ __global__ void __launch_bounds__(BLOCK_SLOTS, 3)
     const int pij = pair_ij_index(ti, tj, pot.ntypes);
     if (kphi >= 0) {
       const SplineGeom &g = sg[pot.s_phi + pij];
-      phi = cubic2_val_grad(pt2, g.poff, kphi, db.pair_shiftf[gs], (float)g.invstep, dphi);
+      phi = cubic2_val_grad(pt2, npiece, g.poff, kphi, db.pair_shiftf[gs], (float)g.invstep, dphi);
     }
     if (krho >= 0) {
       const SplineGeom &g = sg[pot.s_rho + tj];
-      rho = cubic2_val_grad(pt2, g.poff, krho, db.pair_shiftf[Np + gs], (float)g.invstep, drho);
+      rho = cubic2_val_grad(pt2, npiece, g.poff, krho, db.pair_shiftf[Np + gs], (float)g.invstep, drho);
     }
     if (kf >= 0) {
       const SplineGeom &g = sg[pot.s_f + pij];
-      f = cubic2_val_grad(pt2, g.poff, kf, db.pair_shiftf[2 * Np + gs], (float)g.invstep, df);
+      f = cubic2_val_grad(pt2, npiece, g.poff, kf, db.pair_shiftf[2 * Np + gs], (float)g.invstep, df);
     }
   }
   srow[tid] = make_float4(ux, uy, uz, 0.f);
@@ -159,7 +168,7 @@ __global__ void __launch_bounds__(BLOCK_SLOTS, 3)
         float b;
         const int kk = g_knot<float>(cs, gx0, ginv, gg.n, b);
         float2 dg;
-        const float2 gv = cubic2_val_grad(pt2, goff, kk, b, ginv, dg);
+        const float2 gv = cubic2_val_grad(pt2, npiece, goff, kk, b, ginv, dg);
         const float2 dgfk = mul2(dg, fk);
         g8 = fma2(gv, fk, g8);
         h8 = fma2(dgfk, bcast2(cs), h8);
