@@ -18,6 +18,8 @@
 // runs as one more pass over the row with the same shared-memory rows.
 #pragma once
 
+#include <type_traits>
+
 #include "mz_fwd.cuh"
 
 namespace mzb {
@@ -36,6 +38,21 @@ __device__ __forceinline__ void power_to_table(const SplineGeom &g, int m, doubl
   add(g.n + m + 1, -H * d1 + H * d3);
 }
 
+// spline5eq: the same for the quintic's six power coefficients, from
+// c0 = y_m, c1 = y_m+1 - y_m + H2 (-2 y''_m - y''_m+1) + H4 (8 y4_m + 7 y4_m+1),
+// c2 = 3 H2 y''_m, c3 = H2 (y''_m+1 - y''_m) + H4 (-20 y4_m - 10 y4_m+1),
+// c4 = 15 H4 y4_m, c5 = 3 H4 (y4_m+1 - y4_m), H2 = h^2/6, H4 = h^4/360.
+template <class Add>
+__device__ __forceinline__ void power_to_table5(const SplineGeom &g, int m, const double *d, Add add) {
+  const double H2 = g.step * g.step / 6.0, H4 = g.step * g.step * g.step * g.step / 360.0;
+  add(m, d[0] - d[1]);
+  add(m + 1, d[1]);
+  add(g.n + m, H2 * (-2.0 * d[1] + 3.0 * d[2] - d[3]));
+  add(g.n + m + 1, H2 * (-d[1] + d[3]));
+  add(2 * g.n + 2 + m, H4 * (8.0 * d[1] - 20.0 * d[3] + 15.0 * d[4] - 3.0 * d[5]));
+  add(2 * g.n + 3 + m, H4 * (7.0 * d[1] - 10.0 * d[3] + 3.0 * d[5]));
+}
+
 constexpr int GACC_FLUSH_BLOCKS = 16;  // atom blocks between flushes of the per-thread g tables
 // The adjoint walks type-pure atom blocks (DevDb::adj_*), so each thread keeps
 // one g table (its block's type), flushed when the CTA moves to a block of
@@ -48,6 +65,7 @@ constexpr int GACC_FLUSH_BLOCKS = 16;  // atom blocks between flushes of the per
 //   R4 gacc[gtabs][ng-1][BLOCK_SLOTS]       per-thread g-table gradients, power basis: one table
 //                                           (the block's type) for MEAM; one per partner type for
 //                                           GMEAM, flushed every block
+//   R2 gacc5[ng-1][BLOCK_SLOTS]             spline5eq: the fifth and sixth power coefficients
 //   double red[BLOCK_SLOTS], a_chi[BLOCK_ATOMS], a_dF[BLOCK_ATOMS]
 //   SplineGeom sg[nsplines]; int a_lo[BLOCK_ATOMS+2], a_idx[BLOCK_ATOMS], a_len[BLOCK_ATOMS]
 //   R ptab[pstride]
@@ -57,10 +75,10 @@ constexpr int GACC_FLUSH_BLOCKS = 16;  // atom blocks between flushes of the per
 //   int stype[BLOCK_SLOTS+8] neighbour type of every slot (GMEAM)
 template <typename R>
 __host__ __device__ inline size_t adj_smem_bytes(int nsplines, int stride, int pstride, bool meam, int gtabs,
-                                                 int ng) {
+                                                 int ng, bool q5 = false) {
   size_t b = sizeof(double) * (size_t)ADJ_WARPS * stride + sizeof(float) * (size_t)ADJ_WARPS * stride;
   b = (b + 31) & ~size_t(31);
-  if (meam) b += 4 * sizeof(R) * (size_t)gtabs * (ng - 1) * BLOCK_SLOTS;
+  if (meam) b += (q5 ? 6 : 4) * sizeof(R) * (size_t)gtabs * (ng - 1) * BLOCK_SLOTS;
   b += sizeof(double) * (BLOCK_SLOTS + 2 * BLOCK_ATOMS);
   b += sizeof(SplineGeom) * nsplines;
   b += sizeof(int) * (3 * BLOCK_ATOMS + 2);
@@ -72,7 +90,7 @@ __host__ __device__ inline size_t adj_smem_bytes(int nsplines, int stride, int p
   return b;
 }
 
-template <bool MEAM, typename R, bool GM = false, bool JM = false>
+template <bool MEAM, typename R, bool GM = false, bool JM = false, bool Q5 = false>
 __global__ void __launch_bounds__(BLOCK_SLOTS, JM ? 2 : sizeof(R) == 4 ? 3 : 2)
     k_adj(DevDb db, DevPot pot, const SplineGeom *__restrict__ geom, const double *__restrict__ tabs,
           const double *__restrict__ ptabs, const double *__restrict__ aout, const double *__restrict__ aux,
@@ -92,8 +110,11 @@ __global__ void __launch_bounds__(BLOCK_SLOTS, JM ? 2 : sizeof(R) == 4 ? 3 : 2)
   float *ftab = reinterpret_cast<float *>(wtab + (size_t)ADJ_WARPS * stride);
   size_t off = sizeof(double) * (size_t)ADJ_WARPS * stride + sizeof(float) * (size_t)ADJ_WARPS * stride;
   off = (off + 31) & ~size_t(31);
+  using R2 = typename std::conditional<sizeof(R) == 4, float2, double2>::type;
   R4 *gacc = reinterpret_cast<R4 *>(smem_raw + off);
   if (MEAM) off += 4 * sizeof(R) * (size_t)gtabs * nint * BLOCK_SLOTS;
+  R2 *gacc5 = reinterpret_cast<R2 *>(smem_raw + off);
+  if (MEAM && Q5) off += 2 * sizeof(R) * (size_t)nint * BLOCK_SLOTS;
   double *red = reinterpret_cast<double *>(smem_raw + off);
   double *a_chi = red + BLOCK_SLOTS;
   double *a_dF = a_chi + BLOCK_ATOMS;
@@ -120,6 +141,8 @@ __global__ void __launch_bounds__(BLOCK_SLOTS, JM ? 2 : sizeof(R) == 4 ? 3 : 2)
   }
   if (MEAM)
     for (int i = tid; i < gtabs * nint * BLOCK_SLOTS; i += blockDim.x) gacc[i] = R4{};
+  if (MEAM && Q5)
+    for (int i = tid; i < nint * BLOCK_SLOTS; i += blockDim.x) gacc5[i] = R2{};
   for (int i = tid; i < pot.nsplines; i += blockDim.x) sg[i] = geom[i];
   double *wt = wtab + (size_t)warp * stride;
   float *ft = ftab + (size_t)warp * stride;
@@ -136,14 +159,23 @@ __global__ void __launch_bounds__(BLOCK_SLOTS, JM ? 2 : sizeof(R) == 4 ? 3 : 2)
     const SplineGeom &gg = sg[s];
     for (int m = 0; m < gg.n - 1; ++m) {
       const R4 v = gacc[m * BLOCK_SLOTS + tid];
-      double d[4] = {(double)v.x, (double)v.y, (double)v.z, (double)v.w};
+      double d[6] = {(double)v.x, (double)v.y, (double)v.z, (double)v.w, 0.0, 0.0};
+      if (Q5) {
+        const R2 v5 = gacc5[m * BLOCK_SLOTS + tid];
+        d[4] = (double)v5.x;
+        d[5] = (double)v5.y;
+      }
 #pragma unroll
-      for (int q = 0; q < 4; ++q)
+      for (int q = 0; q < (Q5 ? 6 : 4); ++q)
         for (int o = 16; o > 0; o >>= 1) d[q] += __shfl_down_sync(0xffffffffu, d[q], o);
-      if (lane == 0)
-        power_to_table(gg, m, d[0], d[1], d[2], d[3], [&](int idx, double x) { wt[gg.toff + idx] += x; });
+      if (lane == 0) {
+        if (Q5) power_to_table5(gg, m, d, [&](int idx, double x) { wt[gg.toff + idx] += x; });
+        else power_to_table(gg, m, d[0], d[1], d[2], d[3], [&](int idx, double x) { wt[gg.toff + idx] += x; });
+      }
     }
     for (int m = 0; m < nint; ++m) gacc[m * BLOCK_SLOTS + tid] = R4{};
+    if (Q5)
+      for (int m = 0; m < nint; ++m) gacc5[m * BLOCK_SLOTS + tid] = R2{};
   };
   auto flush_gacc = [&](int t) { flush_gacc_spline(pot.s_g + t); };
   // GMEAM: this thread's table tk holds triplets (i; j, k) with j its slot's
@@ -219,7 +251,7 @@ __global__ void __launch_bounds__(BLOCK_SLOTS, JM ? 2 : sizeof(R) == 4 ? 3 : 2)
       }
     }
     if (have) {
-      pe = eval_pair<MEAM, R>(db, pot, sg, ptab, gs, ti);
+      pe = eval_pair<MEAM, R, Q5>(db, pot, sg, ptab, gs, ti);
       const int j = db.pair_nbr[gs];
       const double ux = db.pair_ux[gs], uy = db.pair_uy[gs], uz = db.pair_uz[gs], r = db.pair_r[gs];
       // m_p: the slot's stress term -r (u_x V_x, u_y V_y, u_z V_z, u_x V_y, u_y V_z, u_z V_x) transposed
@@ -273,12 +305,13 @@ __global__ void __launch_bounds__(BLOCK_SLOTS, JM ? 2 : sizeof(R) == 4 ? 3 : 2)
           dpen = w * 100.0 * 10. * 2.0 * (rho - gU.xN);
           if (!pot.embed_extrap) { rt = gU.xN; drt = 0.0; }
         }
-        const PointEval U = spl_point(tc, gU, rt);
+        const PointEval U = spl_point_t<Q5>(tc, gU, rt);
         const double eps = sd[CS_EPS * NC + c], kap = sd[CS_KAPPA * NC + c];
         a_chi[a] = (eps * U.grad + U.grad2 * K) * drt + kap * dpen;
         a_dF[a] = U.grad;
         const int toffU = gU.toff;
-        spl_point_adjoint(gU, U, rt, eps, K, [&](int idx, double v) { wt[toffU + idx] += v; });
+        if (Q5) spl_point_adjoint5(gU, U, rt, eps, K, [&](int idx, double v) { wt[toffU + idx] += v; });
+        else spl_point_adjoint(gU, U, rt, eps, K, [&](int idx, double v) { wt[toffU + idx] += v; });
       }
     }
     __syncthreads();
@@ -355,7 +388,7 @@ __global__ void __launch_bounds__(BLOCK_SLOTS, JM ? 2 : sizeof(R) == 4 ? 3 : 2)
             R b;
             const int m = g_knot<R>(cs, gx0, ginv, ngt, b);
             R dg;
-            const R gv = cubic_val_grad<R>(gpc, m, b, ginv, dg);
+            const R gv = piece_val_grad<Q5, R>(gpc, m, b, ginv, dg);
             // d K / d f_p from the triplet terms of slot k
             const R qu = q.z * pe.ux + q.w * pe.uy + sqz[k] * pe.uz;
             dk8 += wk * (q.x * gv - q.y * dg * cs + dg * qu);
@@ -371,6 +404,13 @@ __global__ void __launch_bounds__(BLOCK_SLOTS, JM ? 2 : sizeof(R) == 4 ? 3 : 2)
             d.z += cg * b2 + R(2) * cs1 * b;
             d.w += cg * b2 * b + R(3) * cs1 * b2;
             ga[m * BLOCK_SLOTS] = d;
+            if (Q5) {  // quintic pieces: the b^4 and b^5 coefficients
+              R2 e = gacc5[m * BLOCK_SLOTS + tid];
+              const R b3 = b2 * b;
+              e.x += cg * b3 * b + R(4) * cs1 * b3;
+              e.y += cg * b3 * b2 + R(5) * cs1 * b3 * b;
+              gacc5[m * BLOCK_SLOTS + tid] = e;
+            }
           }
           dKdf += (double)dk8;
         }
@@ -379,6 +419,16 @@ __global__ void __launch_bounds__(BLOCK_SLOTS, JM ? 2 : sizeof(R) == 4 ? 3 : 2)
       // ---- pair-function tables: phi (energy + force), rho (density + force), f
       auto pair_adj = [&](int s, int k, R b, double cv, double cd) {
         const SplineGeom &g = sg[s];
+        if (Q5) {
+          const SplW5<double> w = spl_weights5<double>((double)b, g.step, g.invstep);
+          add_f(g.toff + k, cv * w.wa + cd * w.da);
+          add_f(g.toff + k + 1, cv * w.wb + cd * w.db);
+          add_f(g.toff + g.n + k, cv * w.wA + cd * w.dA);
+          add_f(g.toff + g.n + k + 1, cv * w.wB + cd * w.dB);
+          add_f(g.toff + 2 * g.n + 2 + k, cv * w.w4a + cd * w.d4a);
+          add_f(g.toff + 2 * g.n + 3 + k, cv * w.w4b + cd * w.d4b);
+          return;
+        }
         const SplW<double> w = spl_weights<double>((double)b, g.step, g.invstep);
         add_f(g.toff + k, cv * w.wa + cd * w.da);
         add_f(g.toff + k + 1, cv * w.wb + cd * w.db);
@@ -540,10 +590,11 @@ __global__ void k_grad_final(DevPot pot, const SplineGeom *__restrict__ geom, co
       for (int ty = 0; ty < pot.ntypes; ++ty) {
         const SplineGeom &g = geom[pot.s_U + ty];
         const double mid = 0.5 * (g.x0 + g.xN);
-        const PointEval e = spl_point(tab, g, mid);
+        const PointEval e = spl_point_any(tab, g, mid);
         const double ev = 100. * e.grad;
         const int to = g.toff;
-        spl_point_adjoint(g, e, mid, 0.0, 2.0 * ev * 100.0, [&](int idx, double v) { ext[to + idx] += v; });
+        if (g.q5) spl_point_adjoint5(g, e, mid, 0.0, 2.0 * ev * 100.0, [&](int idx, double v) { ext[to + idx] += v; });
+        else spl_point_adjoint(g, e, mid, 0.0, 2.0 * ev * 100.0, [&](int idx, double v) { ext[to + idx] += v; });
       }
     }
   }
@@ -552,6 +603,18 @@ __global__ void k_grad_final(DevPot pot, const SplineGeom *__restrict__ geom, co
   for (int s = t; s < pot.nsplines; s += blockDim.x) {
     const SplineGeom g = geom[s];
     const int n = g.n;
+    if (g.q5) {
+      // spline5eq: (ypp, yp4) = M (y, grad, grad2), M [2n][n+4]
+      for (int col = 0; col < n + 4; ++col) {
+        const int te = col < n ? g.toff + col : col < n + 2 ? g.toff + 2 * n + (col - n) : g.toff + 3 * n + 2 + (col - n - 2);
+        double acc = ext[te];
+        for (int r = 0; r < n; ++r) acc += M[g.moff + r * (n + 4) + col] * ext[g.toff + n + r];
+        for (int r = 0; r < n; ++r) acc += M[g.moff + (n + r) * (n + 4) + col] * ext[g.toff + 2 * n + 2 + r];
+        const int ci = cmap[te];
+        if (ci >= 0) gc[ci] = acc;
+      }
+      continue;
+    }
     for (int col = 0; col < n + 2; ++col) {
       double acc = col < n ? ext[g.toff + col] : ext[g.toff + 2 * n + (col - n)];
       for (int r = 0; r < n; ++r) acc += M[g.moff + r * (n + 2) + col] * ext[g.toff + n + r];

@@ -220,12 +220,10 @@ void launch_atoms(mz_ctx *ctx, int n, size_t smem) {
       return;
     }
   }
-  if constexpr (!AUX) {
-    if (ctx->q5) {  // spline5eq pieces (objective only)
-      k_atoms<MEAM, R, false, false, false, true><<<ga, BLOCK_SLOTS, smem, ctx->stream>>>(
-          ctx->db, ctx->pot, ctx->d_geom, ctx->d_tabs, ctx->d_ptabs, ctx->d_V, ctx->d_aout, ctx->d_aux);
-      return;
-    }
+  if (ctx->q5) {  // spline5eq pieces
+    k_atoms<MEAM, R, AUX, false, false, true><<<ga, BLOCK_SLOTS, smem, ctx->stream>>>(
+        ctx->db, ctx->pot, ctx->d_geom, ctx->d_tabs, ctx->d_ptabs, ctx->d_V, ctx->d_aout, ctx->d_aux);
+    return;
   }
   if constexpr (MEAM) {
     if (ctx->pot.nj > 0) {
@@ -246,6 +244,12 @@ void launch_atoms(mz_ctx *ctx, int n, size_t smem) {
 template <bool MEAM, typename R>
 void launch_adj(mz_ctx *ctx, int n, size_t smem) {
   dim3 ga(ctx->adj_ctas, n);
+  if (ctx->q5) {  // spline5eq pieces
+    k_adj<MEAM, R, false, false, true><<<ga, BLOCK_SLOTS, smem, ctx->stream>>>(
+        ctx->db, ctx->pot, ctx->d_geom, ctx->d_tabs, ctx->d_ptabs, ctx->d_aout, ctx->d_aux, ctx->d_lam,
+        ctx->d_seeds, ctx->d_partial);
+    return;
+  }
   if constexpr (MEAM && sizeof(R) == 4) {
     if (ctx->adj_nc == 2 && ctx->nc2_ok) {  // two candidates per CTA, packed FP32 pairs
       dim3 g2(ctx->adj_ctas, (n + 1) / 2);
@@ -873,8 +877,8 @@ mz_status mz_create(const mz_db *dbh, const mz_pot *poth, const mz_settings *set
           for (auto &g : pot.groups[gi]) ng = std::max(ng, g.nknots);
     dp.g_nmax = ng;
     const int gtabs = dp.gmeam ? pot.ntypes : 1;
-    ctx->smem_adj[0] = adj_smem_bytes<double>(ns, stride, ctx->pstride, meam, gtabs, ng);
-    ctx->smem_adj[1] = adj_smem_bytes<float>(ns, stride, ctx->pstride, meam, gtabs, ng);
+    ctx->smem_adj[0] = adj_smem_bytes<double>(ns, stride, ctx->pstride, meam, gtabs, ng, ctx->q5);
+    ctx->smem_adj[1] = adj_smem_bytes<float>(ns, stride, ctx->pstride, meam, gtabs, ng, ctx->q5);
     int smem_max = 0;
     ck(cudaDeviceGetAttribute(&smem_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx->device), "attribute");
     if (ctx->smem_adj[0] > (size_t)smem_max || ctx->smem_atoms[0] > (size_t)smem_max)
@@ -910,6 +914,12 @@ mz_status mz_create(const mz_db *dbh, const mz_pot *poth, const mz_settings *set
       smem_attr(k_atoms2<false>, ctx->smem_atoms2);
       smem_attr(k_adj2, ctx->smem_adj2);
     }
+    smem_attr(k_atoms<true, double, true, false, false, true>, ctx->smem_atoms[0]);
+    smem_attr(k_atoms<true, float, true, false, false, true>, ctx->smem_atoms[1]);
+    smem_attr(k_adj<true, double, false, false, true>, ctx->smem_adj[0]);
+    smem_attr(k_adj<false, double, false, false, true>, ctx->smem_adj[0]);
+    smem_attr(k_adj<true, float, false, false, true>, ctx->smem_adj[1]);
+    smem_attr(k_adj<false, float, false, false, true>, ctx->smem_adj[1]);
     smem_attr(k_atoms<true, double, false, false, false, true>, ctx->smem_atoms[0]);
     smem_attr(k_atoms<false, double, false, false, false, true>, ctx->smem_atoms[0]);
     smem_attr(k_atoms<true, float, false, false, false, true>, ctx->smem_atoms[1]);
@@ -1006,7 +1016,6 @@ mz_status mz_objective(mz_ctx *ctx, int ncand, const double *params, int precisi
 mz_status mz_objective_grad(mz_ctx *ctx, int ncand, const double *params, int precision, double *obj, double *grad) {
   return guarded([&] {
     if (!grad) throw Failure{MZ_ERR_ARG, "null gradient buffer"};
-    if (ctx && ctx->q5) throw Failure{MZ_ERR_UNSUPPORTED, "the gradient is not implemented for spline5eq potentials"};
     run_host(ctx, ncand, params, precision, obj, nullptr, nullptr, nullptr, nullptr, grad);
   });
 }
@@ -1029,7 +1038,6 @@ mz_status mz_objective_grad_device(mz_ctx *ctx, int ncand, const double *d_param
                                    double *d_grad) {
   return guarded([&] {
     if (!ctx || !d_params || !d_obj || !d_grad || ncand <= 0) throw Failure{MZ_ERR_ARG, "bad argument"};
-    if (ctx->q5) throw Failure{MZ_ERR_UNSUPPORTED, "the gradient is not implemented for spline5eq potentials"};
     if (ncand > ctx->cand_cap)
       throw Failure{MZ_ERR_RANGE,
                     "ncand exceeds the candidates one launch can hold (" + std::to_string(ctx->cand_cap) + ")"};

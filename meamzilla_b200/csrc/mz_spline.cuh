@@ -179,6 +179,61 @@ __device__ __noinline__ PointEval spl_point_any(const double *tab, const SplineG
   return g.q5 ? spl_point5(tab, g, r) : spl_point(tab, g, r);
 }
 
+// spline5eq: weights of the value and the slope on y[k], y[k+1], ypp[k],
+// ypp[k+1], yp4[k], yp4[k+1] at shift b (the transposes of the quintic
+// piece, spline5eq.h:110-127).
+template <typename R>
+struct SplW5 {
+  R wa, wb, wA, wB, w4a, w4b, da, db, dA, dB, d4a, d4b;
+};
+template <typename R>
+__device__ __forceinline__ SplW5<R> spl_weights5(R b, R step, R invstep) {
+  SplW5<R> w;
+  const R a = R(1) - b, h = step;
+  const R h6 = h / R(6), hh6 = h * h / R(6), h3 = h * h * h / R(360), h4 = h * h * h * h / R(360);
+  w.wa = a;
+  w.wb = b;
+  w.wA = (a * a * a - a) * hh6;
+  w.wB = (b * b * b - b) * hh6;
+  w.w4a = (R(3) * a * a * a * a * a - R(10) * a * a * a + R(7) * a) * h4;
+  w.w4b = (R(3) * b * b * b * b * b - R(10) * b * b * b + R(7) * b) * h4;
+  w.da = -invstep;
+  w.db = invstep;
+  w.dA = -(R(3) * a * a - R(1)) * h6;
+  w.dB = (R(3) * b * b - R(1)) * h6;
+  w.d4a = -(R(15) * a * a * a * a - R(30) * a * a + R(7)) * h3;
+  w.d4b = (R(15) * b * b * b * b - R(30) * b * b + R(7)) * h3;
+  return w;
+}
+
+// Adds cv * d(value)/d(table) + cd * d(slope)/d(table) of a spline5eq point
+// evaluation (quadratic beyond the ends) to the table gradient; table slice
+// layout y[n], ypp[n], grad[2], yp4[n], grad2[2].
+template <class Add>
+__device__ __forceinline__ void spl_point_adjoint5(const SplineGeom &g, const PointEval &e, double r, double cv,
+                                                   double cd, Add add) {
+  const int n = g.n;
+  if (e.k == -1) {  // y0 + g0 (r - x0) + g2_0 (r - x0)^2 / 2
+    const double d = r - g.x0;
+    add(0, cv);
+    add(2 * n, cv * d + cd);
+    add(3 * n + 2, cv * 0.5 * d * d + cd * d);
+  } else if (e.k == -2) {
+    const double d = r - g.xN;
+    add(n - 1, cv);
+    add(2 * n + 1, cv * d + cd);
+    add(3 * n + 3, cv * 0.5 * d * d + cd * d);
+  } else {
+    const SplW5<double> w = spl_weights5<double>(e.b, g.step, g.invstep);
+    add(e.k, cv * w.wa + cd * w.da);
+    add(e.k + 1, cv * w.wb + cd * w.db);
+    add(n + e.k, cv * w.wA + cd * w.dA);
+    add(n + e.k + 1, cv * w.wB + cd * w.dB);
+    add(2 * n + 2 + e.k, cv * w.w4a + cd * w.d4a);
+    add(2 * n + 3 + e.k, cv * w.w4b + cd * w.d4b);
+  }
+}
+
 // Adds cv * d(value)/d(table) + cd * d(slope)/d(table) of a point evaluation
 // to the spline's table gradient `acc` (same layout as its table slice).
 template <class Add>

@@ -41,12 +41,6 @@ def test_fp64_gradient_vs_finite_differences(name):
     g = case["gold"]
     ev = Evaluator(case["db"], case["pot"], max_candidates=2, **case["weights"])
     x = np.stack([g["coeff"], g["coeff2"]])
-    if case["pot"].spline(0)["quintic"]:  # spline5eq: objective only, the gradient is refused
-        from meamzilla_b200._lib import MzError
-        with pytest.raises(MzError) as e:
-            ev.objective_grad(x, MZ_FP64)
-        assert e.value.status == 5 and "spline5eq" in str(e.value)
-        return
     obj, grad = ev.objective_grad(x, MZ_FP64)
     orc = oracle_for(case)
     for c in range(2):
@@ -58,7 +52,7 @@ def test_fp64_gradient_vs_finite_differences(name):
 
 
 @pytest.mark.parametrize("name", ["meam_mix6", "meam2_edge", "eam_bcc3", "pair_mix2", "jmeam_inrange1",
-                                  "jmeam2_mix2"])
+                                  "jmeam2_mix2", "meam_q5_inrange", "eam_q5"])
 def test_mixed_gradient_vs_fp64(name):
     from meamzilla_b200.potential import MZ_FP64, MZ_MIXED, Evaluator
     case = load_case(name)
