@@ -357,6 +357,23 @@ def run_mine(args, world, rank, local):
     ms64 = max_over_ranks(s2.elapsed_time(e2))
     fp64_rate = world * k64 / (ms64 * 1e-3)
 
+    # ---- objective only, all candidates per launch (a GA population or annealing chains)
+    batched = {}
+    for name, prec in (("mixed", MZ_MIXED), ("fp64", MZ_FP64)):
+        for _ in range(2):
+            ev.objective_device(Xd, obj, prec)
+        ev.sync()
+        barrier()
+        s3 = torch.cuda.Event(enable_timing=True)
+        e3 = torch.cuda.Event(enable_timing=True)
+        s3.record(stream)
+        for _ in range(3):
+            ev.objective_device(Xd, obj, prec)
+        e3.record(stream)
+        e3.synchronize()
+        batched[name + "_evals_per_s"] = world * 3 * args.ncand / (max_over_ranks(s3.elapsed_time(e3)) * 1e-3)
+    batched["candidates_per_launch"] = args.ncand
+
     # ---- end to end through the host API (pinned host buffers)
     ph = torch.tensor(X, dtype=torch.float64).pin_memory()
     oh = torch.empty(args.ncand, dtype=torch.float64).pin_memory()
@@ -414,6 +431,7 @@ def run_mine(args, world, rank, local):
         "fp64_plain": {"value": fp64_rate, "unit": "objective evals/s", "ms_per_eval": ms64 / k64,
                        "candidates_per_launch": 1},
         "ratio_vs_fp64_plain": value / fp64_rate,
+        "objective_only_batched": batched,
         "accuracy_vs_fp64": accuracy,
         "kernels_ms_per_step": {k: kt[k][0] / args.steps for k in kt},
         "roofline": roof,

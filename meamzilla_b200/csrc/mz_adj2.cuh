@@ -351,11 +351,9 @@ __global__ void __launch_bounds__(BLOCK_SLOTS, 2)
           atomicAdd(ftc + g.toff + g.n + k + 1, (float)(cv * w.wB + cd * w.dB));
         };
         const double eps = sds[c][CS_EPS * NC + cell];
-        const double fp = c ? (double)f.y : (double)f.x;
         if (kphi >= 0) pair_adj(pot.s_phi + pij, kphi, bphi, 0.5 * eps, 0.5 * ap[c]);
         if (krho >= 0) pair_adj(pot.s_rho + tj, krho, brho, chi[c], dF[c] * ap[c]);
         if (kf >= 0) pair_adj(pot.s_f + pij, kf, bf, chi[c] * G[c] + dF[c] * dKdf[c], dF[c] * ap[c] * G[c]);
-        (void)fp;
       }
     }
     __syncwarp();
