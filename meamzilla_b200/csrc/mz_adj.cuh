@@ -58,9 +58,12 @@ constexpr int GACC_FLUSH_BLOCKS = 16;  // atom blocks between flushes of the per
 // one g table (its block's type), flushed when the CTA moves to a block of
 // another type and every GACC_FLUSH_BLOCKS blocks.
 
+// Per-warp FP64 table gradients live in global memory, one slice per
+// (candidate, CTA, warp) of wglob [ncand][gridDim.x][ADJ_WARPS][stride] (lane 0 /
+// distinct lanes write them, and the slices are summed in a fixed order, so
+// the gradient is bit-reproducible); keeping them out of shared memory lets
+// four CTAs share an SM.
 // Shared-memory layout of k_adj (dynamic), see adj_smem_bytes():
-//   double wtab[ADJ_WARPS][stride]          per-warp table gradients (FP64; lane 0 / distinct
-//                                           lanes write, so the sums are bit-reproducible)
 //   float  ftab[ADJ_WARPS][stride]          per-warp pair-function gradients of one block (FP32)
 //   R4 gacc[gtabs][ng-1][BLOCK_SLOTS]       per-thread g-table gradients, power basis: one table
 //                                           (the block's type) for MEAM; one per partner type for
@@ -76,7 +79,7 @@ constexpr int GACC_FLUSH_BLOCKS = 16;  // atom blocks between flushes of the per
 template <typename R>
 __host__ __device__ inline size_t adj_smem_bytes(int nsplines, int stride, int pstride, bool meam, int gtabs,
                                                  int ng, bool q5 = false) {
-  size_t b = sizeof(double) * (size_t)ADJ_WARPS * stride + sizeof(float) * (size_t)ADJ_WARPS * stride;
+  size_t b = sizeof(float) * (size_t)ADJ_WARPS * stride;
   b = (b + 31) & ~size_t(31);
   if (meam) b += (q5 ? 6 : 4) * sizeof(R) * (size_t)gtabs * (ng - 1) * BLOCK_SLOTS;
   b += sizeof(double) * (BLOCK_SLOTS + 2 * BLOCK_ATOMS);
@@ -91,10 +94,11 @@ __host__ __device__ inline size_t adj_smem_bytes(int nsplines, int stride, int p
 }
 
 template <bool MEAM, typename R, bool GM = false, bool JM = false, bool Q5 = false>
-__global__ void __launch_bounds__(BLOCK_SLOTS, JM ? 2 : sizeof(R) == 4 ? 3 : 2)
+__global__ void __launch_bounds__(BLOCK_SLOTS, JM || sizeof(R) == 8 ? 2 : (GM || Q5) ? 3 : 4)
     k_adj(DevDb db, DevPot pot, const SplineGeom *__restrict__ geom, const double *__restrict__ tabs,
           const double *__restrict__ ptabs, const double *__restrict__ aout, const double *__restrict__ aux,
-          const double *__restrict__ lam, const double *__restrict__ seeds, double *__restrict__ partial) {
+          const double *__restrict__ lam, const double *__restrict__ seeds, double *__restrict__ partial,
+          double *__restrict__ wglob) {
   using R4 = typename Vec4<R>::T;
   extern __shared__ __align__(32) unsigned char smem_raw[];
   const int cand = blockIdx.y;
@@ -106,9 +110,9 @@ __global__ void __launch_bounds__(BLOCK_SLOTS, JM ? 2 : sizeof(R) == 4 ? 3 : 2)
   const int nint = ng - 1;
   const int gtabs = GM ? pot.ntypes : 1;
 
-  double *wtab = reinterpret_cast<double *>(smem_raw);
-  float *ftab = reinterpret_cast<float *>(wtab + (size_t)ADJ_WARPS * stride);
-  size_t off = sizeof(double) * (size_t)ADJ_WARPS * stride + sizeof(float) * (size_t)ADJ_WARPS * stride;
+  double *wtab = wglob + ((size_t)cand * gridDim.x + blockIdx.x) * ADJ_WARPS * stride;
+  float *ftab = reinterpret_cast<float *>(smem_raw);
+  size_t off = sizeof(float) * (size_t)ADJ_WARPS * stride;
   off = (off + 31) & ~size_t(31);
   using R2 = typename std::conditional<sizeof(R) == 4, float2, double2>::type;
   R4 *gacc = reinterpret_cast<R4 *>(smem_raw + off);
@@ -524,10 +528,18 @@ __global__ void __launch_bounds__(BLOCK_SLOTS, JM ? 2 : sizeof(R) == 4 ? 3 : 2)
       }
     }
     __syncwarp();
-    // the block's FP32 pair-function sums into the warp's FP64 table
-    for (int e = lane; e < stride; e += 32) {
-      wt[e] += (double)ft[e];
-      ft[e] = 0.f;
+    // the block's FP32 pair-function sums into the warp's FP64 table (global
+    // memory): a lane's loads are all issued before its adds and stores
+    for (int e0 = lane; e0 < stride; e0 += 32 * 8) {
+      double v[8];
+#pragma unroll
+      for (int q = 0; q < 8; ++q) v[q] = e0 + 32 * q < stride ? wt[e0 + 32 * q] : 0.0;
+#pragma unroll
+      for (int q = 0; q < 8; ++q)
+        if (e0 + 32 * q < stride) {
+          wt[e0 + 32 * q] = v[q] + (double)ft[e0 + 32 * q];
+          ft[e0 + 32 * q] = 0.f;
+        }
     }
     __syncwarp();
     if (GM) {

@@ -105,7 +105,7 @@ struct mz_ctx {
   size_t smem_atoms2 = 0, smem_adj2 = 0;
   bool nc2_ok = false;  // k_atoms2 / k_adj2 apply (meam/spline, spline3eq, CUDA-core forward)
   int adj2_per_sm = 1;
-  double *d_wglob = nullptr;  // k_adj2's per-warp FP64 tables
+  double *d_wglob = nullptr;  // the adjoint kernels' per-warp FP64 tables
   int fwd_nc = 1, adj_nc = 1;  // the variants in force
   Tune tune[2][2];  // [precision][gradient]
   int autotune = 1;  // MZ_TUNE: 1 time the variants, 0 the first variant, 2 the first with two candidates per CTA
@@ -247,7 +247,7 @@ void launch_adj(mz_ctx *ctx, int n, size_t smem) {
   if (ctx->q5) {  // spline5eq pieces
     k_adj<MEAM, R, false, false, true><<<ga, BLOCK_SLOTS, smem, ctx->stream>>>(
         ctx->db, ctx->pot, ctx->d_geom, ctx->d_tabs, ctx->d_ptabs, ctx->d_aout, ctx->d_aux, ctx->d_lam,
-        ctx->d_seeds, ctx->d_partial);
+        ctx->d_seeds, ctx->d_partial, ctx->d_wglob);
     return;
   }
   if constexpr (MEAM && sizeof(R) == 4) {
@@ -263,18 +263,18 @@ void launch_adj(mz_ctx *ctx, int n, size_t smem) {
     if (ctx->pot.nj > 0) {
       k_adj<MEAM, R, false, true><<<ga, BLOCK_SLOTS, smem, ctx->stream>>>(
           ctx->db, ctx->pot, ctx->d_geom, ctx->d_tabs, ctx->d_ptabs, ctx->d_aout, ctx->d_aux, ctx->d_lam,
-          ctx->d_seeds, ctx->d_partial);
+          ctx->d_seeds, ctx->d_partial, ctx->d_wglob);
       return;
     }
   }
   if (MEAM && ctx->pot.gmeam)
     k_adj<MEAM, R, true><<<ga, BLOCK_SLOTS, smem, ctx->stream>>>(ctx->db, ctx->pot, ctx->d_geom, ctx->d_tabs,
                                                                   ctx->d_ptabs, ctx->d_aout, ctx->d_aux, ctx->d_lam,
-                                                                  ctx->d_seeds, ctx->d_partial);
+                                                                  ctx->d_seeds, ctx->d_partial, ctx->d_wglob);
   else
     k_adj<MEAM, R><<<ga, BLOCK_SLOTS, smem, ctx->stream>>>(ctx->db, ctx->pot, ctx->d_geom, ctx->d_tabs, ctx->d_ptabs,
                                                             ctx->d_aout, ctx->d_aux, ctx->d_lam, ctx->d_seeds,
-                                                            ctx->d_partial);
+                                                            ctx->d_partial, ctx->d_wglob);
 }
 
 // Enqueue the objective (and, with d_grad, its gradient) of n candidates
@@ -966,7 +966,7 @@ mz_status mz_create(const mz_db *dbh, const mz_pot *poth, const mz_settings *set
     const size_t per_cand =
         sizeof(double) * ((size_t)(3 + (meam ? dp.aux_rows : 0)) * Np + (size_t)(AO_COUNT + 3 + 3) * N +
                           (size_t)ctx->esize + (size_t)(8 + 1 + CS_COUNT) * db.ncells + 2 * (size_t)stride + ctx->pstride +
-                          (size_t)ctx->adj_ctas_max * stride * (ctx->nc2_ok ? 1 + ADJ_WARPS : 1) +
+                          (size_t)ctx->adj_ctas_max * stride * (1 + ADJ_WARPS) +
                           2 * (size_t)ctx->P + 1);
     const size_t budget = (size_t)(0.6 * (double)freeb);
     const int cap = (int)std::max<size_t>(1, budget / std::max<size_t>(per_cand, 1));
@@ -987,7 +987,7 @@ mz_status mz_create(const mz_db *dbh, const mz_pot *poth, const mz_settings *set
     ctx->d_lam = dalloc<double>(ctx, C * 3 * N);
     ctx->d_seeds = dalloc<double>(ctx, C * CS_COUNT * db.ncells);
     ctx->d_partial = dalloc<double>(ctx, C * (size_t)ctx->adj_ctas_max * stride);
-    if (ctx->nc2_ok) ctx->d_wglob = dalloc<double>(ctx, C * (size_t)ctx->adj_ctas_max * ADJ_WARPS * stride);
+    ctx->d_wglob = dalloc<double>(ctx, C * (size_t)ctx->adj_ctas_max * ADJ_WARPS * stride);
     ctx->d_grad = dalloc<double>(ctx, C * ctx->P);
     ctx->d_ptabf = dalloc<float>(ctx, C * ctx->pstride);
     ctx->d_wtab = meam ? dalloc<float>(ctx, C * pot.ntypes * (2 * TC_NB - 1)) : nullptr;

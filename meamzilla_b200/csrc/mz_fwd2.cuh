@@ -77,7 +77,7 @@ __device__ __forceinline__ void load_pt2(float4 *pt2, const double *pcA, const d
 // single candidate twice and writes it once).  The arithmetic of each
 // candidate follows k_atoms (pot_meam_spline.cpp:143-269).
 template <bool AUX>
-__global__ void __launch_bounds__(BLOCK_SLOTS, 3)
+__global__ void __launch_bounds__(BLOCK_SLOTS, 4)
     k_atoms2(DevDb db, DevPot pot, const SplineGeom *__restrict__ geom, const double *__restrict__ tabs,
              const double *__restrict__ ptabs, double *__restrict__ Vout, double *__restrict__ aout,
              double *__restrict__ aux, int ncand) {
