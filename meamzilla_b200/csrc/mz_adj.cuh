@@ -54,6 +54,9 @@ __device__ __forceinline__ void power_to_table5(const SplineGeom &g, int m, cons
 }
 
 constexpr int GACC_FLUSH_BLOCKS = 16;  // atom blocks between flushes of the per-thread g tables
+// atom blocks between flushes of the per-warp FP32 tables into FP64 (mixed
+// precision; the FP64 kernels flush after every block)
+constexpr int FT_FLUSH_BLOCKS = 4;
 // The adjoint walks type-pure atom blocks (DevDb::adj_*), so each thread keeps
 // one g table (its block's type), flushed when the CTA moves to a block of
 // another type and every GACC_FLUSH_BLOCKS blocks.
@@ -203,7 +206,25 @@ __global__ void __launch_bounds__(BLOCK_SLOTS, JM || sizeof(R) == 8 ? 2 : (GM ||
     for (int i = 0; i < gtabs * nint; ++i) gacc[i * BLOCK_SLOTS + tid] = R4{};
   };
 
-  int since_flush = 0, tab_t = -1;
+  // the warp's FP32 sums into its FP64 table (global memory): a lane's loads
+  // are all issued before its adds and stores
+  auto flush_ft = [&]() {
+    __syncwarp();
+    for (int e0 = lane; e0 < stride; e0 += 32 * 8) {
+      double v[8];
+#pragma unroll
+      for (int q = 0; q < 8; ++q) v[q] = e0 + 32 * q < stride ? wt[e0 + 32 * q] : 0.0;
+#pragma unroll
+      for (int q = 0; q < 8; ++q)
+        if (e0 + 32 * q < stride) {
+          wt[e0 + 32 * q] = v[q] + (double)ft[e0 + 32 * q];
+          ft[e0 + 32 * q] = 0.f;
+        }
+    }
+    __syncwarp();
+  };
+
+  int since_flush = 0, since_ft = 0, tab_t = -1;
   for (int blk = blockIdx.x; blk < db.adj_nblocks; blk += gridDim.x) {
     const int b0 = db.adj_blk0[blk], na = db.adj_blk0[blk + 1] - b0;
     __syncthreads();  // previous block done with the shared arrays
@@ -313,9 +334,11 @@ __global__ void __launch_bounds__(BLOCK_SLOTS, JM || sizeof(R) == 8 ? 2 : (GM ||
         const double eps = sd[CS_EPS * NC + c], kap = sd[CS_KAPPA * NC + c];
         a_chi[a] = (eps * U.grad + U.grad2 * K) * drt + kap * dpen;
         a_dF[a] = U.grad;
-        const int toffU = gU.toff;
-        if (Q5) spl_point_adjoint5(gU, U, rt, eps, K, [&](int idx, double v) { wt[toffU + idx] += v; });
-        else spl_point_adjoint(gU, U, rt, eps, K, [&](int idx, double v) { wt[toffU + idx] += v; });
+        // into the warp's FP32 table (lane 0 alone writes it in this phase), so
+        // that no global read-modify-write stands before the barrier
+        float *ftU = ft + gU.toff;
+        if (Q5) spl_point_adjoint5(gU, U, rt, eps, K, [&](int idx, double v) { ftU[idx] += (float)v; });
+        else spl_point_adjoint(gU, U, rt, eps, K, [&](int idx, double v) { ftU[idx] += (float)v; });
       }
     }
     __syncthreads();
@@ -527,21 +550,10 @@ __global__ void __launch_bounds__(BLOCK_SLOTS, JM || sizeof(R) == 8 ? 2 : (GM ||
         flush_gacc_spline(pot.s_q[ch] + ti);
       }
     }
-    __syncwarp();
-    // the block's FP32 pair-function sums into the warp's FP64 table (global
-    // memory): a lane's loads are all issued before its adds and stores
-    for (int e0 = lane; e0 < stride; e0 += 32 * 8) {
-      double v[8];
-#pragma unroll
-      for (int q = 0; q < 8; ++q) v[q] = e0 + 32 * q < stride ? wt[e0 + 32 * q] : 0.0;
-#pragma unroll
-      for (int q = 0; q < 8; ++q)
-        if (e0 + 32 * q < stride) {
-          wt[e0 + 32 * q] = v[q] + (double)ft[e0 + 32 * q];
-          ft[e0 + 32 * q] = 0.f;
-        }
+    if (sizeof(R) == 8 || ++since_ft == FT_FLUSH_BLOCKS) {
+      flush_ft();
+      since_ft = 0;
     }
-    __syncwarp();
     if (GM) {
       flush_gacc_gm(tab_t, have, have ? pe.tj : 0);
     } else if (MEAM && ++since_flush == GACC_FLUSH_BLOCKS) {
@@ -549,6 +561,7 @@ __global__ void __launch_bounds__(BLOCK_SLOTS, JM || sizeof(R) == 8 ? 2 : (GM ||
       since_flush = 0;
     }
   }
+  if (since_ft > 0) flush_ft();
   __syncthreads();
   if (MEAM && !GM && since_flush > 0 && tab_t >= 0) {
     flush_gacc(tab_t);

@@ -123,7 +123,34 @@ __global__ void __launch_bounds__(BLOCK_SLOTS, 2)
     for (int m = 0; m < 2 * nint; ++m) gacc[m * BLOCK_SLOTS + tid] = make_float4(0.f, 0.f, 0.f, 0.f);
   };
 
-  int since_flush = 0, tab_t = -1;
+  // the warp's FP32 sums into its FP64 tables (in global memory): all loads
+  // of a lane issued before its adds and stores
+  auto flush_ft = [&]() {
+    __syncwarp();
+    for (int c = 0; c < nc; ++c) {
+      double *__restrict__ w = wt[c];
+      float *__restrict__ fl = ft[c];
+      for (int e0 = lane; e0 < stride; e0 += 32 * 8) {
+        double v[8];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+          const int e = e0 + 32 * q;
+          v[q] = e < stride ? w[e] : 0.0;
+        }
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+          const int e = e0 + 32 * q;
+          if (e < stride) {
+            w[e] = v[q] + (double)fl[e];
+            fl[e] = 0.f;
+          }
+        }
+      }
+    }
+    __syncwarp();
+  };
+
+  int since_flush = 0, since_ft = 0, tab_t = -1;
   for (int blk = blockIdx.x; blk < db.adj_nblocks; blk += gridDim.x) {
     const int b0 = db.adj_blk0[blk], na = db.adj_blk0[blk + 1] - b0;
     __syncthreads();  // previous block done with the shared arrays
@@ -264,9 +291,9 @@ __global__ void __launch_bounds__(BLOCK_SLOTS, 2)
           const double eps = sds[c][CS_EPS * NC + c0], kap = sds[c][CS_KAPPA * NC + c0];
           a_chi[c * BLOCK_ATOMS + a] = (eps * U.grad + U.grad2 * K[c]) * drt + kap * dpen;
           a_dF[c * BLOCK_ATOMS + a] = U.grad;
-          const int toffU = gU.toff;
-          double *w2 = wt[c];
-          spl_point_adjoint(gU, U, rt, eps, K[c], [&](int idx, double v) { w2[toffU + idx] += v; });
+          // into the warp's FP32 table (lane 0 alone writes it in this phase)
+          float *fU = ft[c] + gU.toff;
+          spl_point_adjoint(gU, U, rt, eps, K[c], [&](int idx, double v) { fU[idx] += (float)v; });
         }
         if (!twoc) {  // keep the unused half defined
           a_chi[BLOCK_ATOMS + a] = a_chi[a];
@@ -356,35 +383,16 @@ __global__ void __launch_bounds__(BLOCK_SLOTS, 2)
         if (kf >= 0) pair_adj(pot.s_f + pij, kf, bf, chi[c] * G[c] + dF[c] * dKdf[c], dF[c] * ap[c] * G[c]);
       }
     }
-    __syncwarp();
-    // the block's FP32 pair-function sums into the warps' FP64 tables (in
-    // global memory): all loads of a lane issued before its adds and stores
-    for (int c = 0; c < nc; ++c) {
-      double *__restrict__ w = wt[c];
-      float *__restrict__ fl = ft[c];
-      for (int e0 = lane; e0 < stride; e0 += 32 * 8) {
-        double v[8];
-#pragma unroll
-        for (int q = 0; q < 8; ++q) {
-          const int e = e0 + 32 * q;
-          v[q] = e < stride ? w[e] : 0.0;
-        }
-#pragma unroll
-        for (int q = 0; q < 8; ++q) {
-          const int e = e0 + 32 * q;
-          if (e < stride) {
-            w[e] = v[q] + (double)fl[e];
-            fl[e] = 0.f;
-          }
-        }
-      }
+    if (++since_ft == FT_FLUSH_BLOCKS) {
+      flush_ft();
+      since_ft = 0;
     }
-    __syncwarp();
     if (++since_flush == GACC_FLUSH_BLOCKS) {
       flush_gacc(tab_t);
       since_flush = 0;
     }
   }
+  if (since_ft > 0) flush_ft();
   __syncthreads();
   if (since_flush > 0 && tab_t >= 0) flush_gacc(tab_t);
   __threadfence_block();
