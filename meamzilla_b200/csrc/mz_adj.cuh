@@ -73,7 +73,8 @@ constexpr int FT_FLUSH_BLOCKS = 4;
 //                                           GMEAM, flushed every block
 //   R2 gacc5[ng-1][BLOCK_SLOTS]             spline5eq: the fifth and sixth power coefficients
 //   double red[BLOCK_SLOTS], a_chi[BLOCK_ATOMS], a_dF[BLOCK_ATOMS]
-//   SplineGeom sg[nsplines]; int a_lo[BLOCK_ATOMS+2], a_idx[BLOCK_ATOMS], a_len[BLOCK_ATOMS]
+//   SplineGeom sg[nsplines]; int a_lo[BLOCK_ATOMS+2], a_idx[BLOCK_ATOMS+2], a_cell[BLOCK_ATOMS+2],
+//                            a_na (atom count | type << 8)
 //   R ptab[pstride]
 //   R4 srow[BLOCK_SLOTS+8]  (u_x, u_y, u_z, f)              of every slot (zero padded)
 //   R4 sadj[BLOCK_SLOTS+8]  (a f', a f / r, Q_x, Q_y)        with Q = f Lambda / r
@@ -87,7 +88,7 @@ __host__ __device__ inline size_t adj_smem_bytes(int nsplines, int stride, int p
   if (meam) b += (q5 ? 6 : 4) * sizeof(R) * (size_t)gtabs * (ng - 1) * BLOCK_SLOTS;
   b += sizeof(double) * (BLOCK_SLOTS + 2 * BLOCK_ATOMS);
   b += sizeof(SplineGeom) * nsplines;
-  b += sizeof(int) * (3 * BLOCK_ATOMS + 2);
+  b += sizeof(int) * (3 * BLOCK_ATOMS + 8);
   b = (b + 31) & ~size_t(31);
   b += sizeof(R) * (pstride + 4);
   b = (b + 31) & ~size_t(31);
@@ -128,8 +129,9 @@ __global__ void __launch_bounds__(BLOCK_SLOTS, JM || sizeof(R) == 8 ? 2 : (GM ||
   SplineGeom *sg = reinterpret_cast<SplineGeom *>(a_dF + BLOCK_ATOMS);
   int *a_lo = reinterpret_cast<int *>(sg + pot.nsplines);
   int *a_idx = a_lo + BLOCK_ATOMS + 2;
-  int *a_len = a_idx + BLOCK_ATOMS;
-  off = reinterpret_cast<unsigned char *>(a_len + BLOCK_ATOMS) - smem_raw;
+  int *a_cell = a_idx + BLOCK_ATOMS + 2;
+  int *a_na = a_cell + BLOCK_ATOMS + 2;
+  off = reinterpret_cast<unsigned char *>(a_na + 2) - smem_raw;
   off = (off + 31) & ~size_t(31);
   R *ptab = reinterpret_cast<R *>(smem_raw + off);
   off += sizeof(R) * (pot.pow_stride + 4);
@@ -224,31 +226,39 @@ __global__ void __launch_bounds__(BLOCK_SLOTS, JM || sizeof(R) == 8 ? 2 : (GM ||
     __syncwarp();
   };
 
+  // Block descriptors (atom, first slot, atom count | type << 8, cell; one more
+  // entry holds the slot count) are loaded a block ahead, and the start of the
+  // block after that two blocks ahead, so that no global load stands between
+  // the barriers of a block's prologue.  Threads past the block's count load
+  // entries of the following blocks, which nobody reads.
+  const int ndesc = N + db.adj_nblocks, amax = db.adj_amax;
+  int4 dn = make_int4(0, 0, 0, 0);
+  int nb = blockIdx.x;
+  if (nb < db.adj_nblocks) {
+    const int base = db.adj_blk0[nb] + nb;
+    if (tid < amax && base + tid < ndesc) dn = db.adj_desc[base + tid];
+  }
+  nb += gridDim.x;
+  int nbase = nb < db.adj_nblocks ? db.adj_blk0[nb] + nb : 0;
+
   int since_flush = 0, since_ft = 0, tab_t = -1;
   for (int blk = blockIdx.x; blk < db.adj_nblocks; blk += gridDim.x) {
-    const int b0 = db.adj_blk0[blk], na = db.adj_blk0[blk + 1] - b0;
     __syncthreads();  // previous block done with the shared arrays
-    if (tid < na) {
-      const int at = db.adj_atoms[b0 + tid];
-      a_idx[tid] = at;
-      a_len[tid] = db.pair_off[at + 1] - db.pair_off[at];
+    if (tid < amax) {
+      a_idx[tid] = dn.x;
+      a_lo[tid] = dn.y;
+      a_cell[tid] = dn.w;
     }
+    if (tid == 0) a_na[0] = dn.z;
     __syncthreads();
-    if (warp == 0) {  // row starts in the block's slot numbering (na <= 64: two atoms per lane)
-      const int v0 = 2 * lane < na ? a_len[2 * lane] : 0, v1 = 2 * lane + 1 < na ? a_len[2 * lane + 1] : 0;
-      int inc = v0 + v1;
-      for (int o = 1; o < 32; o <<= 1) {
-        const int y = __shfl_up_sync(0xffffffffu, inc, o);
-        if (lane >= o) inc += y;
-      }
-      const int exc = inc - v0 - v1;
-      if (2 * lane <= na) a_lo[2 * lane] = exc;
-      if (2 * lane + 1 <= na) a_lo[2 * lane + 1] = exc + v0;
-      if (lane == 31) a_lo[na] = inc;
+    if (nb < db.adj_nblocks) {  // the next block's descriptor, the start of the one after
+      if (tid < amax && nbase + tid < ndesc) dn = db.adj_desc[nbase + tid];
+      nb += gridDim.x;
+      nbase = nb < db.adj_nblocks ? db.adj_blk0[nb] + nb : 0;
     }
-    __syncthreads();
+    const int na = a_na[0] & 255;
     const int nslot = a_lo[na];
-    const int ti = db.atom_type[a_idx[0]];  // every atom of the block
+    const int ti = a_na[0] >> 8;  // every atom of the block
     if (MEAM && !GM && tab_t >= 0 && ti != tab_t) {
       flush_gacc(tab_t);
       since_flush = 0;
@@ -259,7 +269,7 @@ __global__ void __launch_bounds__(BLOCK_SLOTS, JM || sizeof(R) == 8 ? 2 : (GM ||
     const int me = have ? slot_owner(a_lo, na, tid) : 0;
     const int ia = a_idx[me];
     const int64_t gs = (int64_t)db.pair_off[ia] + (tid - a_lo[me]);
-    const int cell = db.atom_cell[ia];
+    const int cell = a_cell[me];
 
     PairEval<MEAM, R> pe;
     double Lx = 0, Ly = 0, Lz = 0, a_p = 0, G = 0, H = 0, J = 0;
@@ -319,8 +329,8 @@ __global__ void __launch_bounds__(BLOCK_SLOTS, JM || sizeof(R) == 8 ? 2 : (GM ||
       } else if (lane == 0) {
         const int i = a_idx[a];
         const double rho = ao[AO_RHO * N + i];
-        const int c = db.atom_cell[i];
-        const SplineGeom &gU = sg[pot.s_U + db.atom_type[i]];
+        const int c = a_cell[a];
+        const SplineGeom &gU = sg[pot.s_U + ti];
         const double w = db.cell_w[c];
         double rt = rho, dpen = 0.0, drt = 1.0;
         if (rho < gU.x0) {

@@ -95,6 +95,8 @@ struct mz_ctx {
   int nblk[NCAPS] = {};
   const int *d_adjblk[NCAPS] = {};
   int nadjblk[NCAPS] = {};
+  const int4 *d_adjdesc[NCAPS] = {};
+  int adjamax[NCAPS] = {};
   int adj_ctas_max = 1, adj_per_sm = 1;
   struct Tune {
     bool done = false;
@@ -426,6 +428,8 @@ void apply_variant(mz_ctx *ctx, const mz_ctx::Tune &t) {
   ctx->db.blk_atom0 = ctx->d_blk[t.fwd];
   ctx->db.adj_nblocks = ctx->nadjblk[t.adj];
   ctx->db.adj_blk0 = ctx->d_adjblk[t.adj];
+  ctx->db.adj_desc = ctx->d_adjdesc[t.adj];
+  ctx->db.adj_amax = ctx->adjamax[t.adj];
   ctx->adj_ctas = t.ctas;
 }
 
@@ -862,9 +866,29 @@ mz_status mz_create(const mz_db *dbh, const mz_pot *poth, const mz_settings *set
         b0.push_back(N);
         ctx->nadjblk[v] = (int)b0.size() - 1;
         ctx->d_adjblk[v] = dupload(ctx, b0.data(), b0.size());
+        // descriptors: na + 1 entries per block at b0[b] + b
+        std::vector<int4> desc;
+        desc.reserve((size_t)N + b0.size());
+        int amax = 1;
+        for (size_t b = 0; b + 1 < b0.size(); ++b) {
+          const int na = b0[b + 1] - b0[b];
+          const int tb = db.atom_type[order[b0[b]]];
+          int lo = 0;
+          for (int q = b0[b]; q < b0[b + 1]; ++q) {
+            const int i = order[q];
+            desc.push_back(make_int4(i, lo, na | tb << 8, db.atom_cell[i]));
+            lo += (int)(db.pair_off[i + 1] - db.pair_off[i]);
+          }
+          desc.push_back(make_int4(0, lo, na | tb << 8, 0));
+          amax = std::max(amax, na + 1);
+        }
+        ctx->adjamax[v] = amax;
+        ctx->d_adjdesc[v] = dupload(ctx, desc.data(), desc.size());
       }
       d.adj_nblocks = ctx->nadjblk[0];
       d.adj_blk0 = ctx->d_adjblk[0];
+      d.adj_desc = ctx->d_adjdesc[0];
+      d.adj_amax = ctx->adjamax[0];
     }
 
     // ---- shared memory of the kernels

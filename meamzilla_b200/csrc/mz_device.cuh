@@ -60,6 +60,11 @@ struct DevDb {
   int adj_nblocks;
   const int *adj_atoms;
   const int *adj_blk0;
+  // descriptor of adjoint block b at adj_desc[adj_blk0[b] + b + a], a = 0..na:
+  // (atom, first slot in the block, na | type << 8, cell) for a < na, and
+  // (0, slot count, na | type << 8, 0) for a = na; adj_amax = max na + 1
+  const int4 *adj_desc;
+  int adj_amax;
 };
 
 struct DevPot {
