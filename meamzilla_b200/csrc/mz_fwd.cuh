@@ -580,10 +580,10 @@ __global__ void __launch_bounds__(BLOCK_SLOTS, JM ? 2 : sizeof(R) == 4 ? 4 : 3)
     Vx += ux * cu;
     Vy += uy * cu;
     Vz += uz * cu;
-    double *Vc = Vout + (size_t)cand * 3 * Np;
-    Vc[gs] = Vx;
-    Vc[Np + gs] = Vy;
-    Vc[2 * Np + gs] = Vz;
+    double *Vc = Vout + (size_t)cand * 3 * Np + 3 * gs;  // (x, y, z) per slot
+    Vc[0] = Vx;
+    Vc[1] = Vy;
+    Vc[2] = Vz;
     const double rr = db.pair_r[gs];
     const double dx = db.pair_ux[gs], dy = db.pair_uy[gs], dz = db.pair_uz[gs];
     red[0 * BLOCK_SLOTS + tid] = Vx;
@@ -628,13 +628,13 @@ __global__ void k_gather(DevDb db, const double *__restrict__ V, double *__restr
   if (i >= N) return;
   const int64_t Np = db.npairs;
   double *ao = aout + (size_t)c * AO_COUNT * N;
-  const double *Vc = V + (size_t)c * 3 * Np;
+  const double *Vc = V + (size_t)c * 3 * Np;  // (x, y, z) per slot: one or two 32-byte sectors a read
   double fx = ao[AO_AX * N + i], fy = ao[AO_AY * N + i], fz = ao[AO_AZ * N + i];
   for (int q = db.in_off[i]; q < db.in_off[i + 1]; ++q) {
-    const int s = db.in_slot[q];
-    fx -= Vc[s];
-    fy -= Vc[Np + s];
-    fz -= Vc[2 * Np + s];
+    const double *v = Vc + 3 * (int64_t)db.in_slot[q];
+    fx -= v[0];
+    fy -= v[1];
+    fz -= v[2];
   }
   const int cell = db.atom_cell[i];
   const double w = db.cell_w[cell];

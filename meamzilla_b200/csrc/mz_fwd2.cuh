@@ -246,10 +246,10 @@ __global__ void __launch_bounds__(BLOCK_SLOTS, 4)
       const double ck = dF * fp * ip;
       const double Vx = ck * vx[c] + (double)ux * cu, Vy = ck * vy[c] + (double)uy * cu,
                    Vz = ck * vz[c] + (double)uz * cu;
-      double *Vc = Vout + (size_t)cand * 3 * Np;
-      Vc[gs] = Vx;
-      Vc[Np + gs] = Vy;
-      Vc[2 * Np + gs] = Vz;
+      double *Vc = Vout + (size_t)cand * 3 * Np + 3 * gs;  // (x, y, z) per slot
+      Vc[0] = Vx;
+      Vc[1] = Vy;
+      Vc[2] = Vz;
       const double r = db.pair_r[gs];
       const double dx = db.pair_ux[gs], dy = db.pair_uy[gs], dz = db.pair_uz[gs];
       red[0 * BLOCK_SLOTS + tid] = Vx;

@@ -386,10 +386,10 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
         const double cu = 0.5 * (double)dphi + (double)drho * dF + dF * (double)df * G;
         const double ck = dF * (double)f * ip;
         const double Vx = ux * cu + ck * vx, Vy = uy * cu + ck * vy, Vz = uz * cu + ck * vz;
-        double *Vc = Vout + (size_t)cand * 3 * Np;
-        Vc[s] = Vx;
-        Vc[Np + s] = Vy;
-        Vc[2 * Np + s] = Vz;
+        double *Vc = Vout + (size_t)cand * 3 * Np + 3 * (int64_t)s;  // (x, y, z) per slot
+        Vc[0] = Vx;
+        Vc[1] = Vy;
+        Vc[2] = Vz;
         if (AUX) {
           double *ax = aux + (size_t)cand * AUX_COUNT * Np;
           ax[AUX_G * Np + s] = G;
