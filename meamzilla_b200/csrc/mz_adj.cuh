@@ -21,6 +21,7 @@
 #include <type_traits>
 
 #include "mz_fwd.cuh"
+#include "mz_fwd2.cuh"
 
 namespace mzb {
 
@@ -97,6 +98,14 @@ __host__ __device__ inline size_t adj_smem_bytes(int nsplines, int stride, int p
   return b;
 }
 
+// g_knot<float> from t = (c - x0) / h: interval (clamped to [0, nmax]) and shift
+__device__ __forceinline__ int knot_of_t(float t, int nmax, float &b) {
+  int k = __float_as_int(t + 8388607.5f) - 0x4B000000;
+  k = k < 0 ? 0 : (k > nmax ? nmax : k);
+  b = t - (__int_as_float(k + 0x4B000000) - 8388608.0f);
+  return k;
+}
+
 template <bool MEAM, typename R, bool GM = false, bool JM = false, bool Q5 = false>
 __global__ void __launch_bounds__(BLOCK_SLOTS, JM || sizeof(R) == 8 ? 2 : (GM || Q5) ? 3 : 4)
     k_adj(DevDb db, DevPot pot, const SplineGeom *__restrict__ geom, const double *__restrict__ tabs,
@@ -140,6 +149,30 @@ __global__ void __launch_bounds__(BLOCK_SLOTS, JM || sizeof(R) == 8 ? 2 : (GM ||
   R4 *sadj = srow + BLOCK_SLOTS + 8;
   R *sqz = reinterpret_cast<R *>(sadj + BLOCK_SLOTS + 8);
   int *stype = reinterpret_cast<int *>(sqz + BLOCK_SLOTS + 8);
+  // meam/spline, spline3eq, FP32: the rows as pairs of slots (2 p, 2 p + 1),
+  // in the same storage -- rowA[p] = (u_x, u_x', u_y, u_y'), rowB[p] =
+  // (u_z, u_z', f, f'), adjA[p] = (a f', a f', -a f / r, -a f' / r'),
+  // adjB[p] = (Q_x, Q_x', Q_y, Q_y'), qz2[p] = (Q_z, Q_z')
+  constexpr bool PK = MEAM && !GM && !JM && !Q5 && sizeof(R) == 4;
+  constexpr int HP = (BLOCK_SLOTS + 8) / 2;
+  float4 *rowA = reinterpret_cast<float4 *>(srow), *rowB = rowA + HP;
+  float4 *adjA = reinterpret_cast<float4 *>(sadj), *adjB = adjA + HP;
+  const float2 *qz2 = reinterpret_cast<const float2 *>(sqz);
+  auto put_pair_row = [&](int k, float ux, float uy, float uz, float f, float qx, float qy, float qX, float qY,
+                          float qZ) {
+    float *fa = reinterpret_cast<float *>(rowA), *fb = reinterpret_cast<float *>(rowB);
+    float *ga = reinterpret_cast<float *>(adjA), *gb = reinterpret_cast<float *>(adjB);
+    const int o = 4 * (k >> 1) + (k & 1);
+    fa[o] = ux;
+    fa[o + 2] = uy;
+    fb[o] = uz;
+    fb[o + 2] = f;
+    ga[o] = qx;
+    ga[o + 2] = -qy;
+    gb[o] = qX;
+    gb[o + 2] = qY;
+    reinterpret_cast<float *>(sqz)[k] = qZ;
+  };
 
   const double *tc = tabs + (size_t)cand * stride;
   const double *pcand = ptabs + (size_t)cand * pot.pow_stride;
@@ -273,7 +306,10 @@ __global__ void __launch_bounds__(BLOCK_SLOTS, JM || sizeof(R) == 8 ? 2 : (GM ||
 
     PairEval<MEAM, R> pe;
     double Lx = 0, Ly = 0, Lz = 0, a_p = 0, G = 0, H = 0, J = 0;
-    if (MEAM) {  // zero rows for idle threads and the padding
+    if (PK) {  // zero rows for idle threads and the padding
+      put_pair_row(tid, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f);
+      if (tid < 8) put_pair_row(BLOCK_SLOTS + tid, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f);
+    } else if (MEAM) {  // zero rows for idle threads and the padding
       srow[tid] = R4{};
       sadj[tid] = R4{};
       sqz[tid] = R(0);
@@ -304,17 +340,22 @@ __global__ void __launch_bounds__(BLOCK_SLOTS, JM || sizeof(R) == 8 ? 2 : (GM ||
         J = Lx * ax[AUX_VX * Np + gs] + Ly * ax[AUX_VY * Np + gs] + Lz * ax[AUX_VZ * Np + gs];
         const double ip = (double)pe.invr, fp = (double)pe.f;
         kp += a_p * (double)pe.df * G - a_p * fp * ip * H + fp * ip * J;
-        R4 v;
-        v.x = pe.ux; v.y = pe.uy; v.z = pe.uz; v.w = pe.f;
-        srow[tid] = v;
-        R4 q;
-        q.x = (R)(a_p * (double)pe.df);
-        q.y = (R)(a_p * fp * ip);
-        q.z = (R)(fp * ip * Lx);
-        q.w = (R)(fp * ip * Ly);
-        sadj[tid] = q;
-        sqz[tid] = (R)(fp * ip * Lz);
-        if (GM) stype[tid] = pe.tj;
+        if constexpr (PK) {
+          put_pair_row(tid, pe.ux, pe.uy, pe.uz, pe.f, (float)(a_p * (double)pe.df), (float)(a_p * fp * ip),
+                       (float)(fp * ip * Lx), (float)(fp * ip * Ly), (float)(fp * ip * Lz));
+        } else {
+          R4 v;
+          v.x = pe.ux; v.y = pe.uy; v.z = pe.uz; v.w = pe.f;
+          srow[tid] = v;
+          R4 q;
+          q.x = (R)(a_p * (double)pe.df);
+          q.y = (R)(a_p * fp * ip);
+          q.z = (R)(fp * ip * Lx);
+          q.w = (R)(fp * ip * Ly);
+          sadj[tid] = q;
+          sqz[tid] = (R)(fp * ip * Lz);
+          if (GM) stype[tid] = pe.tj;
+        }
       }
       red[tid] = kp;
     }
@@ -396,6 +437,71 @@ __global__ void __launch_bounds__(BLOCK_SLOTS, JM || sizeof(R) == 8 ? 2 : (GM ||
             *ga = d;
           }
           dKdf += (double)dk8;
+        }
+        dKdf += ip * (J - a_p * H);
+      } else if constexpr (PK) {
+        // Two partners per step as packed FP32 pairs (sm_100 __ffma2_rn and
+        // friends); per partner the arithmetic of the branch below, with the
+        // interval search of g_knot<float> and the pieces evaluated one by one.
+        const SplineGeom gg = sg[pot.s_g + ti];
+        const float *gpc = ptab + gg.poff;
+        const float ginv = (float)gg.invstep, gcut = g_cut<float>(gg);
+        const int nmax = gg.n - 2;
+        const double fp = (double)pe.f, ip = (double)pe.invr;
+        const float2 UX = bcast2(pe.ux), UY = bcast2(pe.uy), UZ = bcast2(pe.uz);
+        const float2 LX = bcast2((float)Lx), LY = bcast2((float)Ly), LZ = bcast2((float)Lz);
+        const float2 NAP = bcast2(-(float)a_p);
+        const float2 GAM = bcast2((float)(0.5 * chi * fp + dF * a_p * (double)pe.df));
+        const float2 DELH = bcast2((float)(dF * fp * ip) * ginv);
+        const float2 GINV = bcast2(ginv), NX0 = bcast2(-(float)gg.x0);
+        float4 *ga = reinterpret_cast<float4 *>(gacc) + tid;
+        const int row_lo = a_lo[me], row_hi = a_lo[me + 1];
+        for (int pb = row_lo >> 1; 2 * pb < row_hi; pb += 4) {
+          float2 dk2 = bcast2(0.f);
+#pragma unroll
+          for (int u = 0; u < 4; ++u) {
+            const int p = pb + u, k0 = 2 * p, k1 = k0 + 1;
+            const float4 ra = rowA[p], rb = rowB[p], qa = adjA[p], qb = adjB[p];
+            const float2 ox = pair2(ra.x, ra.y), oy = pair2(ra.z, ra.w), oz = pair2(rb.x, rb.y);
+            const float2 cs = fma2(UX, ox, fma2(UY, oy, mul2(UZ, oz)));
+            // k0 >= row_lo - 1 and k1 >= row_lo by the start of the loop
+            const bool ok0 = k0 >= row_lo && k0 < row_hi && k0 != tid && cs.x < gcut;
+            const bool ok1 = k1 < row_hi && k1 != tid && cs.y < gcut;
+            const float2 w = pair2(ok0 ? 1.f : 0.f, ok1 ? 1.f : 0.f);
+            const float2 t = mul2(add2(cs, NX0), GINV);
+            float b0, b1;
+            const int m0 = knot_of_t(t.x, nmax, b0), m1 = knot_of_t(t.y, nmax, b1);
+            const float2 b = pair2(b0, b1);
+            float dg0, dg1;
+            const float gv0 = cubic_val_grad<float>(gpc, m0, b0, ginv, dg0);
+            const float gv1 = cubic_val_grad<float>(gpc, m1, b1, ginv, dg1);
+            const float2 gv = pair2(gv0, gv1), dg = pair2(dg0, dg1);
+            // d K / d f_p from the triplet terms of slot k
+            const float2 qu = fma2(pair2(qb.x, qb.y), UX, fma2(pair2(qb.z, qb.w), UY, mul2(qz2[p], UZ)));
+            dk2 = fma2(w, fma2(pair2(qa.x, qa.y), gv, mul2(dg, fma2(pair2(qa.z, qa.w), cs, qu))), dk2);
+            // g table (power basis): value weight cg, slope weight cs1 / h
+            const float2 bpk = fma2(LX, ox, fma2(LY, oy, mul2(LZ, oz)));
+            const float2 fk = mul2(w, pair2(rb.z, rb.w));
+            const float2 cg = mul2(fk, GAM);
+            const float2 cs1 = mul2(mul2(fk, DELH), fma2(NAP, cs, bpk));
+            // cg b^j + j cs1 b^(j-1), j = 0..3
+            const float2 c1 = fma2(cg, b, cs1);
+            const float2 c2 = mul2(b, add2(c1, cs1));
+            const float2 c3 = mul2(mul2(b, b), add2(c1, add2(cs1, cs1)));
+            float4 d = ga[m0 * BLOCK_SLOTS];
+            d.x += cg.x;
+            d.y += c1.x;
+            d.z += c2.x;
+            d.w += c3.x;
+            ga[m0 * BLOCK_SLOTS] = d;
+            d = ga[m1 * BLOCK_SLOTS];
+            d.x += cg.y;
+            d.y += c1.y;
+            d.z += c2.y;
+            d.w += c3.y;
+            ga[m1 * BLOCK_SLOTS] = d;
+          }
+          dKdf += (double)dk2.x + (double)dk2.y;
         }
         dKdf += ip * (J - a_p * H);
       } else if (MEAM) {
