@@ -456,10 +456,11 @@ __global__ void __launch_bounds__(BLOCK_SLOTS, JM || sizeof(R) == 8 ? 2 : (GM ||
         const float2 GINV = bcast2(ginv), NX0 = bcast2(-(float)gg.x0);
         float4 *ga = reinterpret_cast<float4 *>(gacc) + tid;
         const int row_lo = a_lo[me], row_hi = a_lo[me + 1];
-        for (int pb = row_lo >> 1; 2 * pb < row_hi; pb += 4) {
+        // steps of 2 pairs: at most 3 masked partners at the end of a row
+        for (int pb = row_lo >> 1; 2 * pb < row_hi; pb += 2) {
           float2 dk2 = bcast2(0.f);
 #pragma unroll
-          for (int u = 0; u < 4; ++u) {
+          for (int u = 0; u < 2; ++u) {
             const int p = pb + u, k0 = 2 * p, k1 = k0 + 1;
             const float4 ra = rowA[p], rb = rowB[p], qa = adjA[p], qb = adjB[p];
             const float2 ox = pair2(ra.x, ra.y), oy = pair2(ra.z, ra.w), oz = pair2(rb.x, rb.y);
