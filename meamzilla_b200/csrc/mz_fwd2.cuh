@@ -17,6 +17,8 @@
 // styles keep the one-candidate kernel.
 #pragma once
 
+#include <type_traits>
+
 #include "mz_fwd.cuh"
 
 namespace mzb {
@@ -156,10 +158,11 @@ __global__ void __launch_bounds__(BLOCK_SLOTS, 4)
     const float gx0 = (float)gg.x0, ginv = (float)gg.invstep, gcut = gg.cutf;
     const int row_lo = a_lo[me], row_hi = a_lo[me + 1];
     const float2 zero = bcast2(0.f);
-    for (int kb = row_lo; kb < row_hi; kb += 8) {
+    auto chunk = [&](int kb, auto NK) {
+      constexpr int nk = decltype(NK)::value;
       float2 g8 = zero, h8 = zero, x8 = zero, y8 = zero, z8 = zero;
 #pragma unroll
-      for (int u = 0; u < 8; ++u) {
+      for (int u = 0; u < nk; ++u) {
         const int k = kb + u;
         const float4 o = srow[k];
         const float cs = cos_dot(ux, uy, uz, o.x, o.y, o.z);
@@ -186,7 +189,15 @@ __global__ void __launch_bounds__(BLOCK_SLOTS, 4)
       vy[1] += (double)y8.y;
       vz[0] += (double)z8.x;
       vz[1] += (double)z8.y;
+    };
+    // steps of 8 partners, the rest of the row in steps of 4
+    int kb = row_lo;
+    for (; kb + 8 <= row_hi; kb += 8) chunk(kb, std::integral_constant<int, 8>{});
+    if (kb + 4 <= row_hi) {
+      chunk(kb, std::integral_constant<int, 4>{});
+      kb += 4;
     }
+    if (kb < row_hi) chunk(kb, std::integral_constant<int, 4>{});
     if (AUX)
       for (int c = 0; c < (twoc ? 2 : 1); ++c) {
         double *ax = aux + (size_t)(cA + c) * AUX_COUNT * Np;
