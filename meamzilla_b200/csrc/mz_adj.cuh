@@ -54,10 +54,10 @@ __device__ __forceinline__ void power_to_table5(const SplineGeom &g, int m, cons
   add(2 * g.n + 3 + m, H4 * (7.0 * d[1] - 10.0 * d[3] + 3.0 * d[5]));
 }
 
-constexpr int GACC_FLUSH_BLOCKS = 16;  // atom blocks between flushes of the per-thread g tables
+constexpr int GACC_FLUSH_BLOCKS = 32;  // atom blocks between flushes of the per-thread g tables
 // atom blocks between flushes of the per-warp FP32 tables into FP64 (mixed
 // precision; the FP64 kernels flush after every block)
-constexpr int FT_FLUSH_BLOCKS = 4;
+constexpr int FT_FLUSH_BLOCKS = 8;
 // The adjoint walks type-pure atom blocks (DevDb::adj_*), so each thread keeps
 // one g table (its block's type), flushed when the CTA moves to a block of
 // another type and every GACC_FLUSH_BLOCKS blocks.
