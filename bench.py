@@ -408,8 +408,8 @@ def run_mine(args, world, rank, local):
     kflops = {"k_atoms": fwd * args.ncand, "k_adj": 2 * fwd * args.ncand}.get(dom, 3 * fwd * args.ncand)
     # DRAM traffic per launch from ncu (dram__bytes_read.sum + dram__bytes_write.sum) on the 200-cell
     # case of this workload, 8 candidates, scaled by pair slots x candidates (the full launch is too
-    # large to capture): k_adj 2245.4 MB / 15.84 M slot-candidates; k_atoms 496.0 MB / 3.96 M.
-    per_slot_cand = {"k_adj": 2245.4e6 / 15.8433e6, "k_atoms": 496.0e6 / 3.9608e6}.get(dom)
+    # large to capture): k_adj 2480.3 MB / 15.84 M slot-candidates; k_atoms 496.0 MB / 3.96 M.
+    per_slot_cand = {"k_adj": 2480.3e6 / 15.8433e6, "k_atoms": 496.0e6 / 3.9608e6}.get(dom)
     traffic = per_slot_cand * stats["npairs"] * args.ncand if per_slot_cand else None
     roof = {"bound": "hbm", "kernel": dom, "achieved": b32 / (dom_ms * 1e-3) / 1e9, "peak": hbm, "unit": "GB/s",
             "frac": b32 / (dom_ms * 1e-3) / 1e9 / hbm, "traffic": traffic, "algorithmic_bytes": b32,
