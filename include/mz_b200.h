@@ -338,7 +338,7 @@ mz_status mz_kernel_times(mz_ctx *ctx, double *ms, int64_t *launches);
  * callers that cannot call cudaMalloc: code running where the device
  * allocator is off limits (inside another framework's memory pool or
  * allocator hooks, in processes with a fixed device-memory budget, or on a
- * path that must not add allocations or implicit synchronisation).  Instead
+ * path that must not add allocations).  Instead
  * of the context's buffers it uses one file-scope device array of
  * MZ_NOALLOC_SCRATCH_BYTES (64 MiB) that every GPU loading the library holds
  * until exit; the database, the potential's tables and all per-slot and
@@ -347,9 +347,12 @@ mz_status mz_kernel_times(mz_ctx *ctx, double *ms, int64_t *launches);
  *
  * Inputs and outputs are host memory: params[ncoeff] in, obj (the value
  * Potential::compute returns) and, if non-null, forces[natoms][3] out.  FP64,
- * synchronous, on the device named by settings->device, using the default
- * stream.  The first call on a device looks up the array's device address
- * (once per device); make that first call before any stream capture.  Every
+ * on the device named by settings->device (checked against the device count
+ * first; the caller's current device is restored on return).  Every call is
+ * synchronous: it copies with cudaMemcpy and launches on the legacy default
+ * stream, which synchronises with all blocking streams, so no call may run
+ * while a stream capture is in progress in any thread.  The first call on a
+ * device also looks up the array's device address (once per device).  Every
  * call reuses the same array and leaves the last call's contents in it, so
  * calls that overlap on the GPU (from several host threads) race: serialise
  * them. */

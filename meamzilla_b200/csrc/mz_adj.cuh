@@ -62,13 +62,24 @@ constexpr int FT_FLUSH_BLOCKS = 8;
 // one g table (its block's type), flushed when the CTA moves to a block of
 // another type and every GACC_FLUSH_BLOCKS blocks.
 
-// Per-warp FP64 table gradients live in global memory, one slice per
-// (candidate, CTA, warp) of wglob [ncand][gridDim.x][ADJ_WARPS][stride] (lane 0 /
-// distinct lanes write them, and the slices are summed in a fixed order, so
-// the gradient is bit-reproducible); keeping them out of shared memory lets
-// four CTAs share an SM.
+// Mixed precision: per-warp FP64 table gradients live in global memory, one
+// slice per (candidate, CTA, warp) of wglob [ncand][gridDim.x][ADJ_WARPS][stride]
+// (lane 0 / distinct lanes write them, and the slices are summed in a fixed
+// order); keeping them out of shared memory lets four CTAs share an SM.  The
+// pair-function and embedding gradients enter the warp's FP32 shared table
+// with shared-memory atomics (the order of same-address additions is not
+// fixed, so the mixed gradient can differ run to run at FP32 rounding level).
+//
+// FP64 (R = double): every table sum is FP64 and in a fixed order.  The
+// warp's table is FP64 in shared memory; each of its entries has an owner lane
+// (entry mod 32) that adds the warp's contributions in slot order; the
+// per-thread g tables are flushed into it after every block; and the blocks of
+// each group of db.adj_group consecutive blocks (256-slot partition, the one
+// partition the FP64 launches use) are summed into one partial per group, the
+// partials in group order.  The gradient is then bit-identical from call to
+// call and for any number of CTAs.
 // Shared-memory layout of k_adj (dynamic), see adj_smem_bytes():
-//   float  ftab[ADJ_WARPS][stride]          per-warp pair-function gradients of one block (FP32)
+//   FT     ftab[ADJ_WARPS][stride]          per-warp pair-function gradients (FP32; FP64 for R = double)
 //   R4 gacc[gtabs][ng-1][BLOCK_SLOTS]       per-thread g-table gradients, power basis: one table
 //                                           (the block's type) for MEAM; one per partner type for
 //                                           GMEAM, flushed every block
@@ -84,7 +95,7 @@ constexpr int FT_FLUSH_BLOCKS = 8;
 template <typename R>
 __host__ __device__ inline size_t adj_smem_bytes(int nsplines, int stride, int pstride, bool meam, int gtabs,
                                                  int ng, bool q5 = false) {
-  size_t b = sizeof(float) * (size_t)ADJ_WARPS * stride;
+  size_t b = (sizeof(R) == 8 ? sizeof(double) : sizeof(float)) * (size_t)ADJ_WARPS * stride;
   b = (b + 31) & ~size_t(31);
   if (meam) b += (q5 ? 6 : 4) * sizeof(R) * (size_t)gtabs * (ng - 1) * BLOCK_SLOTS;
   b += sizeof(double) * (BLOCK_SLOTS + 2 * BLOCK_ATOMS);
@@ -123,9 +134,11 @@ __global__ void __launch_bounds__(BLOCK_SLOTS, JM || sizeof(R) == 8 ? 2 : (GM ||
   const int nint = ng - 1;
   const int gtabs = GM ? pot.ntypes : 1;
 
-  double *wtab = wglob + ((size_t)cand * gridDim.x + blockIdx.x) * ADJ_WARPS * stride;
-  float *ftab = reinterpret_cast<float *>(smem_raw);
-  size_t off = sizeof(float) * (size_t)ADJ_WARPS * stride;
+  constexpr bool DET = sizeof(R) == 8;  // FP64: fixed-order FP64 table sums (see above)
+  using FT = typename std::conditional<DET, double, float>::type;
+  double *wtab = DET ? nullptr : wglob + ((size_t)cand * gridDim.x + blockIdx.x) * ADJ_WARPS * stride;
+  FT *ftab = reinterpret_cast<FT *>(smem_raw);
+  size_t off = sizeof(FT) * (size_t)ADJ_WARPS * stride;
   off = (off + 31) & ~size_t(31);
   using R2 = typename std::conditional<sizeof(R) == 4, float2, double2>::type;
   R4 *gacc = reinterpret_cast<R4 *>(smem_raw + off);
@@ -178,17 +191,50 @@ __global__ void __launch_bounds__(BLOCK_SLOTS, JM || sizeof(R) == 8 ? 2 : (GM ||
   const double *pcand = ptabs + (size_t)cand * pot.pow_stride;
   for (int i = tid; i < pot.pow_stride; i += blockDim.x) ptab[i] = (R)pcand[i];
   for (int i = tid; i < ADJ_WARPS * stride; i += blockDim.x) {
-    wtab[i] = 0.0;
-    ftab[i] = 0.f;
+    if (!DET) wtab[i] = 0.0;
+    ftab[i] = FT(0);
   }
   if (MEAM)
     for (int i = tid; i < gtabs * nint * BLOCK_SLOTS; i += blockDim.x) gacc[i] = R4{};
   if (MEAM && Q5)
     for (int i = tid; i < nint * BLOCK_SLOTS; i += blockDim.x) gacc5[i] = R2{};
   for (int i = tid; i < pot.nsplines; i += blockDim.x) sg[i] = geom[i];
-  double *wt = wtab + (size_t)warp * stride;
-  float *ft = ftab + (size_t)warp * stride;
-  auto add_f = [&](int idx, double v) { atomicAdd(ft + idx, (float)v); };
+  FT *ft = ftab + (size_t)warp * stride;
+  double *wt = DET ? reinterpret_cast<double *>(ft) : wtab + (size_t)warp * stride;
+  // Table contributions of this thread's slot.  Mixed: FP32 shared atomics.
+  // FP64: kept per thread (at most 24: phi, rho, f and JMEAM's p, p2 with four
+  // entries each, or three quintic pieces with six) and added by det_flush.
+  constexpr int NCONTRIB = DET ? 24 : 1;
+  int c_idx[NCONTRIB];
+  double c_val[NCONTRIB];
+  int c_n = 0;
+  auto add_f = [&](int idx, double v) {
+    if constexpr (DET) {
+      c_idx[c_n] = idx;
+      c_val[c_n] = v;
+      ++c_n;
+    } else {
+      atomicAdd(ft + idx, (float)v);
+    }
+  };
+  // Every lane of the warp: the contributions of lanes 0..31 in order, each
+  // entry added by its owner lane (idx mod 32), so each table entry receives
+  // its additions in a fixed order.
+  auto det_flush = [&]() {
+    if constexpr (DET) {
+      __syncwarp();
+      for (int src = 0; src < 32; ++src) {
+        const int n = __shfl_sync(0xffffffffu, c_n, src);
+        for (int e = 0; e < n; ++e) {
+          const int idx = __shfl_sync(0xffffffffu, e < c_n ? c_idx[e] : 0, src);
+          const double v = __shfl_sync(0xffffffffu, e < c_n ? c_val[e] : 0.0, src);
+          if ((idx & 31) == lane) ft[idx] += v;
+        }
+      }
+      c_n = 0;
+      __syncwarp();
+    }
+  };
 
   const double *ao = aout + (size_t)cand * AO_COUNT * N;
   const double *ax = aux + (size_t)cand * (JM ? pot.aux_rows : (int)AUX_COUNT) * Np;
@@ -265,17 +311,27 @@ __global__ void __launch_bounds__(BLOCK_SLOTS, JM || sizeof(R) == 8 ? 2 : (GM ||
   // the barriers of a block's prologue.  Threads past the block's count load
   // entries of the following blocks, which nobody reads.
   const int ndesc = N + db.adj_nblocks, amax = db.adj_amax;
+  // Block order of this CTA: blocks blockIdx.x + k gridDim.x (mixed), or the
+  // groups blockIdx.x + k gridDim.x of db.adj_group consecutive blocks (FP64).
+  const int GB = DET ? max(db.adj_group, 1) : 1;
+  const int ngroups = (db.adj_nblocks + GB - 1) / GB;
+  auto next_blk = [&](int b) {
+    if (!DET) return b + (int)gridDim.x;
+    const int nx = b + 1;
+    return (nx % GB) ? nx : nx + ((int)gridDim.x - 1) * GB;
+  };
+  const int first_blk = DET ? (int)blockIdx.x * GB : (int)blockIdx.x;
   int4 dn = make_int4(0, 0, 0, 0);
-  int nb = blockIdx.x;
+  int nb = first_blk;
   if (nb < db.adj_nblocks) {
     const int base = db.adj_blk0[nb] + nb;
     if (tid < amax && base + tid < ndesc) dn = db.adj_desc[base + tid];
   }
-  nb += gridDim.x;
+  nb = next_blk(nb);
   int nbase = nb < db.adj_nblocks ? db.adj_blk0[nb] + nb : 0;
 
   int since_flush = 0, since_ft = 0, tab_t = -1;
-  for (int blk = blockIdx.x; blk < db.adj_nblocks; blk += gridDim.x) {
+  for (int blk = first_blk; blk < db.adj_nblocks; blk = next_blk(blk)) {
     __syncthreads();  // previous block done with the shared arrays
     if (tid < amax) {
       a_idx[tid] = dn.x;
@@ -286,13 +342,13 @@ __global__ void __launch_bounds__(BLOCK_SLOTS, JM || sizeof(R) == 8 ? 2 : (GM ||
     __syncthreads();
     if (nb < db.adj_nblocks) {  // the next block's descriptor, the start of the one after
       if (tid < amax && nbase + tid < ndesc) dn = db.adj_desc[nbase + tid];
-      nb += gridDim.x;
+      nb = next_blk(nb);
       nbase = nb < db.adj_nblocks ? db.adj_blk0[nb] + nb : 0;
     }
     const int na = a_na[0] & 255;
     const int nslot = a_lo[na];
     const int ti = a_na[0] >> 8;  // every atom of the block
-    if (MEAM && !GM && tab_t >= 0 && ti != tab_t) {
+    if (!DET && MEAM && !GM && tab_t >= 0 && ti != tab_t) {
       flush_gacc(tab_t);
       since_flush = 0;
     }
@@ -387,9 +443,9 @@ __global__ void __launch_bounds__(BLOCK_SLOTS, JM || sizeof(R) == 8 ? 2 : (GM ||
         a_dF[a] = U.grad;
         // into the warp's FP32 table (lane 0 alone writes it in this phase), so
         // that no global read-modify-write stands before the barrier
-        float *ftU = ft + gU.toff;
-        if (Q5) spl_point_adjoint5(gU, U, rt, eps, K, [&](int idx, double v) { ftU[idx] += (float)v; });
-        else spl_point_adjoint(gU, U, rt, eps, K, [&](int idx, double v) { ftU[idx] += (float)v; });
+        FT *ftU = ft + gU.toff;
+        if (Q5) spl_point_adjoint5(gU, U, rt, eps, K, [&](int idx, double v) { ftU[idx] += (FT)v; });
+        else spl_point_adjoint(gU, U, rt, eps, K, [&](int idx, double v) { ftU[idx] += (FT)v; });
       }
     }
     __syncthreads();
@@ -667,28 +723,48 @@ __global__ void __launch_bounds__(BLOCK_SLOTS, JM || sizeof(R) == 8 ? 2 : (GM ||
         flush_gacc_spline(pot.s_q[ch] + ti);
       }
     }
-    if (sizeof(R) == 8 || ++since_ft == FT_FLUSH_BLOCKS) {
-      flush_ft();
-      since_ft = 0;
-    }
-    if (GM) {
-      flush_gacc_gm(tab_t, have, have ? pe.tj : 0);
-    } else if (MEAM && ++since_flush == GACC_FLUSH_BLOCKS) {
-      flush_gacc(tab_t);
-      since_flush = 0;
+    if constexpr (DET) {
+      det_flush();
+      if (GM) flush_gacc_gm(tab_t, have, have ? pe.tj : 0);
+      else if (MEAM) flush_gacc(tab_t);
+      if ((blk + 1) % GB == 0 || blk + 1 == db.adj_nblocks) {
+        // end of a group: its partial, the warp tables summed in warp order
+        __syncthreads();
+        double *out = partial + ((size_t)cand * ngroups + blk / GB) * stride;
+        for (int e = tid; e < stride; e += blockDim.x) {
+          double s = 0.0;
+          for (int w = 0; w < ADJ_WARPS; ++w) s += (double)ftab[(size_t)w * stride + e];
+          out[e] = s;
+        }
+        __syncthreads();
+        for (int i = tid; i < ADJ_WARPS * stride; i += blockDim.x) ftab[i] = FT(0);
+      }
+    } else {
+      if (++since_ft == FT_FLUSH_BLOCKS) {
+        flush_ft();
+        since_ft = 0;
+      }
+      if (GM) {
+        flush_gacc_gm(tab_t, have, have ? pe.tj : 0);
+      } else if (MEAM && ++since_flush == GACC_FLUSH_BLOCKS) {
+        flush_gacc(tab_t);
+        since_flush = 0;
+      }
     }
   }
-  if (since_ft > 0) flush_ft();
-  __syncthreads();
-  if (MEAM && !GM && since_flush > 0 && tab_t >= 0) {
-    flush_gacc(tab_t);
+  if constexpr (!DET) {
+    if (since_ft > 0) flush_ft();
     __syncthreads();
-  }
-  double *out = partial + ((size_t)cand * gridDim.x + blockIdx.x) * stride;
-  for (int e = tid; e < stride; e += blockDim.x) {
-    double s = 0.0;
-    for (int w = 0; w < ADJ_WARPS; ++w) s += wtab[(size_t)w * stride + e];
-    out[e] = s;
+    if (MEAM && !GM && since_flush > 0 && tab_t >= 0) {
+      flush_gacc(tab_t);
+      __syncthreads();
+    }
+    double *out = partial + ((size_t)cand * gridDim.x + blockIdx.x) * stride;
+    for (int e = tid; e < stride; e += blockDim.x) {
+      double s = 0.0;
+      for (int w = 0; w < ADJ_WARPS; ++w) s += wtab[(size_t)w * stride + e];
+      out[e] = s;
+    }
   }
 }
 

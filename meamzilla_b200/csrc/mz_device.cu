@@ -24,8 +24,10 @@
 // and for the gradient:
 //   k_adj        persistent CTAs over atom blocks, one thread per slot
 //   k_grad_final partial sums, punishment terms, transposed refresh.
-// Forward reductions run in a fixed order (bit-reproducible objective); the
-// gradient's table sums use shared-memory atomics.
+// Forward reductions run in a fixed order (bit-reproducible objective).  The
+// FP64 gradient's table sums are FP64 in a fixed order (bit-reproducible, for
+// any launch variant); the mixed-precision adjoint adds its pair-function and
+// embedding gradients with FP32 shared-memory atomics.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -111,6 +113,7 @@ struct mz_ctx {
   int fwd_nc = 1, adj_nc = 1;  // the variants in force
   Tune tune[2][2];  // [precision][gradient]
   int autotune = 1;  // MZ_TUNE: 1 time the variants, 0 the first variant, 2 the first with two candidates per CTA
+  int adj_ctas_force = 0;  // MZ_ADJ_CTAS: persistent CTAs of the adjoint, fixed (0: the tuner's)
   bool profiling = false;
   struct Mark {
     int kernel;
@@ -348,8 +351,11 @@ void enqueue(mz_ctx *ctx, int n, const double *d_params, int precision, double *
   }
   {
     Bracket b(ctx, MZ_K_GRAD_FINAL);
+    // FP64: one partial per group of adj_group blocks; mixed: one per CTA
+    const int nparts = mixed ? ctx->adj_ctas
+                             : (ctx->db.adj_nblocks + ctx->db.adj_group - 1) / std::max(ctx->db.adj_group, 1);
     k_grad_final<<<n, 256, sizeof(double) * ctx->stride, st>>>(ctx->pot, ctx->d_geom, ctx->d_tabs, ctx->d_partial,
-                                                                ctx->adj_ctas, ctx->d_M, ctx->d_cmap, ctx->P, d_grad);
+                                                                nparts, ctx->d_M, ctx->d_cmap, ctx->P, d_grad);
     ck(cudaGetLastError(), "k_grad_final launch");
   }
 }
@@ -413,6 +419,79 @@ void refresh_matrix5(const Spline3 &sp, std::vector<double> &M) {
   }
 }
 
+// Host image of a potential's structure for the device: per-spline geometry
+// (offsets of its knot table, evaluation table and refresh matrix), natural
+// ends, the fixed table values and the coefficient map (table entry ->
+// coefficient index in Potential::coeff's order, -1 where fixed).
+struct PotImage {
+  std::vector<SplineGeom> geom;
+  std::vector<int> nat;
+  std::vector<double> base, M;
+  std::vector<int> cmap;
+  int stride = 0, pstride = 0, P = 0;
+};
+
+PotImage pot_image(const Pot &pot) {
+  PotImage im;
+  const int ns = pot.nsplines();
+  im.geom.resize(ns);
+  im.nat.resize(2 * ns);
+  int toff = 0, poff = 0;
+  for (int s = 0; s < ns; ++s) {
+    const Spline3 &sp = pot.spline(s);
+    SplineGeom &g = im.geom[s];
+    g.x0 = sp.x[0];
+    g.xN = sp.x[sp.nknots - 1];
+    g.step = sp.step;
+    g.invstep = sp.invstep;
+    g.cut = sp.x.back() * (1. + 1.e-8);
+    float cf = (float)g.cut;
+    for (int u = 0; u < 4; ++u) cf = std::nextafter(cf, INFINITY);
+    g.cutf = cf;
+    g.n = sp.nknots;
+    g.q5 = sp.quintic;
+    g.toff = toff;
+    toff += (sp.quintic ? 3 : 2) * sp.nknots + (sp.quintic ? 4 : 2);
+    g.poff = poff;
+    poff += (sp.quintic ? 6 : 4) * (sp.nknots - 1);
+    im.nat[2 * s] = sp.nat[0];
+    im.nat[2 * s + 1] = sp.nat[1];
+    std::vector<double> M;
+    if (sp.quintic) refresh_matrix5(sp, M);
+    else refresh_matrix(sp, M);
+    g.moff = (int)im.M.size();
+    im.M.insert(im.M.end(), M.begin(), M.end());
+  }
+  im.stride = toff;
+  im.pstride = poff;
+  im.base.assign(toff, 0.0);
+  im.cmap.assign(toff, -1);
+  for (int s = 0; s < ns; ++s) {
+    const Spline3 &sp = pot.spline(s);
+    const int o = im.geom[s].toff, n = sp.nknots;
+    for (int k = 0; k < n; ++k) im.base[o + k] = sp.y[k];
+    for (int e = 0; e < 2; ++e) im.base[o + 2 * n + e] = sp.grad[e];
+    if (sp.quintic)
+      for (int e = 0; e < 2; ++e) im.base[o + 3 * n + 2 + e] = sp.grad2[e];
+  }
+  int ci = 0;
+  for (auto &cs : pot.coeff_slots()) {
+    const int o = im.geom[cs.first].toff, n = im.geom[cs.first].n, slot = cs.second;
+    const int at = slot < n ? o + slot : slot < n + 2 ? o + 2 * n + (slot - n) : o + 3 * n + 2 + (slot - n - 2);
+    im.cmap[at] = ci++;
+  }
+  im.P = ci;
+  return im;
+}
+
+// Knots of slot s packed as the kernels read them:
+// (phi+1) | (rho+1) << 8 | (f+1) << 16 | (p+1) << 24.
+int packed_knots(const Db &db, int64_t s) {
+  const int nf = db.nfun;
+  return (db.pair_knot[nf * s] + 1) | ((db.pair_knot[nf * s + 1] + 1) << 8) | ((db.pair_knot[nf * s + 2] + 1) << 16) |
+         (nf > 3 ? (db.pair_knot[nf * s + 3] + 1) << 24 : 0);
+}
+
 // ---------------------------------------------------------------- autotuner
 
 // Choices by workload, shared by the contexts of one process, so that
@@ -430,7 +509,7 @@ void apply_variant(mz_ctx *ctx, const mz_ctx::Tune &t) {
   ctx->db.adj_blk0 = ctx->d_adjblk[t.adj];
   ctx->db.adj_desc = ctx->d_adjdesc[t.adj];
   ctx->db.adj_amax = ctx->adjamax[t.adj];
-  ctx->adj_ctas = t.ctas;
+  ctx->adj_ctas = ctx->adj_ctas_force > 0 ? std::min(ctx->adj_ctas_force, ctx->adj_ctas_max) : t.ctas;
 }
 
 int adj_ctas_for(const mz_ctx *ctx, int v, int per_sm) {
@@ -520,7 +599,9 @@ void tune_variant(mz_ctx *ctx, int n, const double *d_params, int precision, boo
           const int ancs = (precision == MZ_MIXED && ctx->nc2_ok && n > 1) ? 2 : 1;
           for (int anc = 1; anc <= ancs; ++anc) {
             const int pmax = anc == 2 ? ctx->adj2_per_sm : ctx->adj_per_sm;
-            for (int v = 0; v < mz_ctx::NCAPS; ++v)
+            // the FP64 gradient's sums follow the 256-slot partition only
+            const int nv = precision == MZ_FP64 ? 1 : mz_ctx::NCAPS;
+            for (int v = 0; v < nv; ++v)
               for (int per = pmax; per >= std::max(1, pmax - 1); --per) {
                 mz_ctx::Tune c = best;
                 c.adj = v;
@@ -669,55 +750,13 @@ mz_status mz_create(const mz_db *dbh, const mz_pot *poth, const mz_settings *set
 
     // ---- potential structure
     const int ns = pot.nsplines();
-    std::vector<SplineGeom> geom(ns);
-    std::vector<int> nat(2 * ns);
-    std::vector<double> Mall;
-    int toff = 0, poff = 0;
-    for (int s = 0; s < ns; ++s) {
-      const Spline3 &sp = pot.spline(s);
-      SplineGeom &g = geom[s];
-      g.x0 = sp.x[0];
-      g.xN = sp.x[sp.nknots - 1];
-      g.step = sp.step;
-      g.invstep = sp.invstep;
-      g.cut = sp.x.back() * (1. + 1.e-8);
-      float cf = (float)g.cut;
-      for (int u = 0; u < 4; ++u) cf = std::nextafter(cf, INFINITY);
-      g.cutf = cf;
-      g.n = sp.nknots;
-      g.q5 = sp.quintic;
-      g.toff = toff;
-      toff += (sp.quintic ? 3 : 2) * sp.nknots + (sp.quintic ? 4 : 2);
-      g.poff = poff;
-      poff += (sp.quintic ? 6 : 4) * (sp.nknots - 1);
-      nat[2 * s] = sp.nat[0];
-      nat[2 * s + 1] = sp.nat[1];
-      std::vector<double> M;
-      if (sp.quintic) refresh_matrix5(sp, M);
-      else refresh_matrix(sp, M);
-      g.moff = (int)Mall.size();
-      Mall.insert(Mall.end(), M.begin(), M.end());
-    }
-    const int stride = toff;
-    ctx->pstride = poff;
-    std::vector<double> base(stride, 0.0);
-    std::vector<int> cmap(stride, -1);
-    for (int s = 0; s < ns; ++s) {
-      const Spline3 &sp = pot.spline(s);
-      const int o = geom[s].toff, n = sp.nknots;
-      for (int k = 0; k < n; ++k) base[o + k] = sp.y[k];
-      for (int e = 0; e < 2; ++e) base[o + 2 * n + e] = sp.grad[e];
-      if (sp.quintic)
-        for (int e = 0; e < 2; ++e) base[o + 3 * n + 2 + e] = sp.grad2[e];
-    }
-    // coefficient i -> table entry, in Potential::coeff's order
-    int ci = 0;
-    for (auto &cs : pot.coeff_slots()) {
-      const int o = geom[cs.first].toff, n = geom[cs.first].n, slot = cs.second;
-      const int at = slot < n ? o + slot : slot < n + 2 ? o + 2 * n + (slot - n) : o + 3 * n + 2 + (slot - n - 2);
-      cmap[at] = ci++;
-    }
-    ctx->P = ci;
+    const PotImage im = pot_image(pot);
+    const std::vector<SplineGeom> &geom = im.geom;
+    const std::vector<int> &nat = im.nat, &cmap = im.cmap;
+    const std::vector<double> &base = im.base, &Mall = im.M;
+    const int stride = im.stride;
+    ctx->pstride = im.pstride;
+    ctx->P = im.P;
     ctx->q5 = ns > 0 && pot.spline(0).quintic;
     if (ctx->q5 && (style_meam(pot.style) && pot.style != MZ_STYLE_MEAM_SPLINE))
       throw Failure{MZ_ERR_UNSUPPORTED, "spline5eq is implemented for eam/spline, meam/spline and pair/spline"};
@@ -781,8 +820,7 @@ mz_status mz_create(const mz_db *dbh, const mz_pot *poth, const mz_settings *set
     }
     for (int64_t s = 0; s < Np; ++s) {
       inslot32[s] = (int)db.in_slot[s];
-      knot32[s] = (db.pair_knot[nf * s] + 1) | ((db.pair_knot[nf * s + 1] + 1) << 8) |
-                  ((db.pair_knot[nf * s + 2] + 1) << 16) | (nf > 3 ? (db.pair_knot[nf * s + 3] + 1) << 24 : 0);
+      knot32[s] = packed_knots(db, s);
       if (nf > 4) knotp2[s] = db.pair_knot[nf * s + 4];
     }
     d.pair_knot_p2 = nf > 4 ? dupload(ctx, knotp2.data(), knotp2.size()) : nullptr;
@@ -889,6 +927,8 @@ mz_status mz_create(const mz_db *dbh, const mz_pot *poth, const mz_settings *set
       d.adj_blk0 = ctx->d_adjblk[0];
       d.adj_desc = ctx->d_adjdesc[0];
       d.adj_amax = ctx->adjamax[0];
+      // FP64 adjoint groups: at most about 1024 partials per candidate
+      d.adj_group = std::max(1, ctx->nadjblk[0] / 1024);
     }
 
     // ---- shared memory of the kernels
@@ -971,6 +1011,10 @@ mz_status mz_create(const mz_db *dbh, const mz_pot *poth, const mz_settings *set
       const char *env = std::getenv("MZ_GRAPH");
       ctx->use_graphs = !(env && env[0] == '0');
     }
+    {
+      const char *env = std::getenv("MZ_ADJ_CTAS");
+      ctx->adj_ctas_force = env ? std::max(0, std::atoi(env)) : 0;
+    }
     // tensor-core forward (mixed precision, MEAM with TC_NB B-spline coefficients per g spline)
     {
       const char *env = std::getenv("MZ_TC");  // opt-in: "1"
@@ -990,7 +1034,7 @@ mz_status mz_create(const mz_db *dbh, const mz_pot *poth, const mz_settings *set
     const size_t per_cand =
         sizeof(double) * ((size_t)(3 + (meam ? dp.aux_rows : 0)) * Np + (size_t)(AO_COUNT + 3 + 3) * N +
                           (size_t)ctx->esize + (size_t)(8 + 1 + CS_COUNT) * db.ncells + 2 * (size_t)stride + ctx->pstride +
-                          (size_t)ctx->adj_ctas_max * stride * (1 + ADJ_WARPS) +
+                          (size_t)ctx->adj_ctas_max * stride * (1 + ADJ_WARPS) + (size_t)2048 * stride +
                           2 * (size_t)ctx->P + 1);
     const size_t budget = (size_t)(0.6 * (double)freeb);
     const int cap = (int)std::max<size_t>(1, budget / std::max<size_t>(per_cand, 1));
@@ -1010,7 +1054,8 @@ mz_status mz_create(const mz_db *dbh, const mz_pot *poth, const mz_settings *set
     ctx->d_aux = meam ? dalloc<double>(ctx, C * dp.aux_rows * Np) : nullptr;
     ctx->d_lam = dalloc<double>(ctx, C * 3 * N);
     ctx->d_seeds = dalloc<double>(ctx, C * CS_COUNT * db.ncells);
-    ctx->d_partial = dalloc<double>(ctx, C * (size_t)ctx->adj_ctas_max * stride);
+    const size_t nparts = std::max<size_t>(ctx->adj_ctas_max, (ctx->nadjblk[0] + d.adj_group - 1) / d.adj_group);
+    ctx->d_partial = dalloc<double>(ctx, C * nparts * stride);
     ctx->d_wglob = dalloc<double>(ctx, C * (size_t)ctx->adj_ctas_max * ADJ_WARPS * stride);
     ctx->d_grad = dalloc<double>(ctx, C * ctx->P);
     ctx->d_ptabf = dalloc<float>(ctx, C * ctx->pstride);
@@ -1214,10 +1259,27 @@ struct Carve {
 
 }  // namespace
 
+// Makes `device` current for its lifetime and then restores the caller's
+// current device, on every exit path.
+struct DeviceGuard {
+  int prev = -1;
+  explicit DeviceGuard(int device) {
+    ck(cudaGetDevice(&prev), "cudaGetDevice");
+    ck(cudaSetDevice(device), "cudaSetDevice");
+  }
+  ~DeviceGuard() {
+    if (prev >= 0) cudaSetDevice(prev);
+  }
+};
+
 extern "C" mz_status mz_objective_noalloc(const mz_db *dbh, const mz_pot *poth, const mz_settings *set,
                                           const double *params, double *obj, double *forces) {
   return guarded([&] {
     if (!dbh || !poth || !set || !params || !obj) throw Failure{MZ_ERR_ARG, "null argument"};
+    int ndev = 0;
+    ck(cudaGetDeviceCount(&ndev), "cudaGetDeviceCount");
+    if (set->device < 0 || set->device >= ndev || set->device >= 64)
+      throw Failure{MZ_ERR_ARG, "device ordinal out of range"};
     const Db &db = dbh->db;
     const Pot &pot = poth->pot;
     const bool meam = pot.style == MZ_STYLE_MEAM_SPLINE;
@@ -1233,45 +1295,12 @@ extern "C" mz_status mz_objective_noalloc(const mz_db *dbh, const mz_pot *poth, 
     const int N = db.natoms, NC = db.ncells, ns = pot.nsplines();
     const int64_t Np = db.npairs;
 
-    // ---- host images of the potential structure (as mz_create builds them)
-    std::vector<SplineGeom> geom(ns);
-    std::vector<int> nat(2 * ns);
-    int toff = 0, poff = 0;
-    for (int s = 0; s < ns; ++s) {
-      const Spline3 &sp = pot.spline(s);
-      SplineGeom &g = geom[s];
-      g.x0 = sp.x[0];
-      g.xN = sp.x[sp.nknots - 1];
-      g.step = sp.step;
-      g.invstep = sp.invstep;
-      g.cut = sp.x.back() * (1. + 1.e-8);
-      g.cutf = (float)g.cut;
-      g.n = sp.nknots;
-      g.toff = toff;
-      g.moff = 0;
-      g.poff = poff;
-      toff += 2 * sp.nknots + 2;
-      poff += 4 * (sp.nknots - 1);
-      nat[2 * s] = sp.nat[0];
-      nat[2 * s + 1] = sp.nat[1];
-    }
-    const int stride = toff, pstride = poff;
-    std::vector<double> base(stride, 0.0);
-    std::vector<int> cmap(stride, -1);
-    int ci = 0;
-    for (int s = 0; s < ns; ++s) {
-      const Spline3 &sp = pot.spline(s);
-      const int o = geom[s].toff, n = sp.nknots;
-      for (int k = 0; k < n; ++k) {
-        base[o + k] = sp.y[k];
-        if (!sp.y_fixed[k]) cmap[o + k] = ci++;
-      }
-      for (int e = 0; e < 2; ++e) {
-        base[o + 2 * n + e] = sp.grad[e];
-        if (!sp.grad_fixed[e] && !sp.nat[e]) cmap[o + 2 * n + e] = ci++;
-      }
-    }
-    const int P = ci;
+    // ---- host images of the potential structure (the same as mz_create's)
+    const PotImage im = pot_image(pot);
+    const std::vector<SplineGeom> &geom = im.geom;
+    const std::vector<int> &nat = im.nat, &cmap = im.cmap;
+    const std::vector<double> &base = im.base;
+    const int stride = im.stride, pstride = im.pstride, P = im.P;
     DevPot dp{};
     dp.style = pot.style;
     dp.ntypes = pot.ntypes;
@@ -1300,8 +1329,7 @@ extern "C" mz_status mz_objective_noalloc(const mz_db *dbh, const mz_pot *poth, 
     std::vector<double> ux(Np), uy(Np), uz(Np), sh(3 * Np);
     for (int64_t q = 0; q < Np; ++q) {
       inslot32[q] = (int)db.in_slot[q];
-      knot32[q] = (db.pair_knot[db.nfun * q] + 1) | ((db.pair_knot[db.nfun * q + 1] + 1) << 8) |
-                  ((db.pair_knot[db.nfun * q + 2] + 1) << 16);
+      knot32[q] = packed_knots(db, q);
       ux[q] = db.pair_u[3 * q];
       uy[q] = db.pair_u[3 * q + 1];
       uz[q] = db.pair_u[3 * q + 2];
@@ -1346,19 +1374,14 @@ extern "C" mz_status mz_objective_noalloc(const mz_db *dbh, const mz_pot *poth, 
                                       std::to_string((size_t)MZ_NOALLOC_SCRATCH_BYTES)};
 
     // ---- per-device set-up: the array's device address, with that device current
-    ck(cudaSetDevice(set->device), "cudaSetDevice");
-    if (set->device < 0 || set->device >= 64) throw Failure{MZ_ERR_ARG, "device ordinal out of range"};
+    // (the caller's current device is restored on return)
+    DeviceGuard dev(set->device);
     unsigned char *base_ptr = nullptr;
     {
       std::lock_guard<std::mutex> lk(g_noalloc_mutex);
       if (!g_noalloc_addr[set->device]) {
         void *p = nullptr;
         ck(cudaGetSymbolAddress(&p, g_noalloc_scratch), "cudaGetSymbolAddress");
-        const size_t sa = atoms_smem_bytes<double>(ns, pstride);
-        ck(cudaFuncSetAttribute(k_atoms<true, double, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sa),
-           "smem attribute");
-        ck(cudaFuncSetAttribute(k_atoms<false, double, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sa),
-           "smem attribute");
         g_noalloc_addr[set->device] = p;
       }
       base_ptr = static_cast<unsigned char *>(g_noalloc_addr[set->device]);

@@ -65,6 +65,10 @@ struct DevDb {
   // (0, slot count, na | type << 8, 0) for a = na; adj_amax = max na + 1
   const int4 *adj_desc;
   int adj_amax;
+  // FP64 adjoint: runs of adj_group consecutive blocks (of the 256-slot
+  // partition) form one group, whose table gradients are summed on their own
+  // and stored as one partial; the partials are summed in group order
+  int adj_group;
 };
 
 struct DevPot {

@@ -67,6 +67,9 @@ def _lib():
         L = C.CDLL(LIBORACLE)
         L.mzo_objective.restype = C.c_double
         L.mzo_objective.argtypes = [C.POINTER(_Db), C.POINTER(_Pot), C.c_void_p] + [C.c_void_p] * 5
+        L.mzo_objective_tangent.restype = C.c_double
+        L.mzo_objective_tangent.argtypes = [C.POINTER(_Db), C.POINTER(_Pot), C.c_void_p, C.c_void_p,
+                                            C.POINTER(C.c_double)]
         L.mzo_esize.restype = C.c_int
         L.mzo_esize.argtypes = [C.POINTER(_Db), C.POINTER(_Pot)]
         _liboracle = L
@@ -143,6 +146,28 @@ class CRestatement:
         obj = _lib().mzo_objective(C.byref(self.db), C.byref(self.pot), x.ctypes.data, ev.ctypes.data,
                                    fo.ctypes.data, en.ctypes.data, st.ctypes.data, de.ctypes.data)
         return dict(obj=obj, errvec=ev, forces=fo, energy=en, stress=st, dens=de)
+
+
+    def tangent(self, coeffs, direction):
+        """(objective, exact derivative along `direction`): the tangent-linear
+        restatement, forward-mode differentiation of the objective."""
+        x = np.ascontiguousarray(coeffs, dtype=np.float64)
+        d = np.ascontiguousarray(direction, dtype=np.float64)
+        out = C.c_double(0.0)
+        obj = _lib().mzo_objective_tangent(C.byref(self.db), C.byref(self.pot), x.ctypes.data, d.ctypes.data,
+                                           C.byref(out))
+        return obj, out.value
+
+    def gradient(self, coeffs):
+        """Exact gradient: one tangent evaluation per coefficient direction."""
+        x = np.ascontiguousarray(coeffs, dtype=np.float64)
+        g = np.zeros(x.size)
+        e = np.zeros(x.size)
+        for i in range(x.size):
+            e[:] = 0.0
+            e[i] = 1.0
+            g[i] = self.tangent(x, e)[1]
+        return g
 
 
 def run_reference(param_path: str, coeffs=None, fd_h: float = 0.0, reps: int = 0, fast: bool = False,

@@ -554,3 +554,387 @@ double mzo_objective(const mzo_db *db, const mzo_pot *pot, const double *coeffs,
   free(sp);
   return sum;
 }
+
+/* ------------------------------------------------------------------------
+ * Tangent-linear restatement: the objective and its exact derivative along
+ * one direction of the coefficient vector (forward-mode differentiation of
+ * mzo_objective, statement by statement).  Every spline's knot table is
+ * linear in its coefficients (Spline3Eq::refresh_basis spline3eq.cpp:192-225
+ * and Spline5Eq::refresh_basis spline5eq.cpp:209-293 solve linear systems
+ * whose right-hand sides are linear in y and the end derivatives), so the
+ * derivative of a spline value at a fixed knot and shift is the value of the
+ * "tangent spline" whose coefficients are the direction; at a variable point
+ * x(t) the chain rule adds S'(x) x'. */
+
+/* S''(x) of Spline3Eq / Spline5Eq::splint_comb(double, double*)
+ * (spline3eq.h:204-236, spline5eq.h:226-255): zero (cubic) or the end y''
+ * (quintic) on the extrapolated ranges. */
+static double sp_second_x(const sp_t *s, double r) {
+  int n = s->n, k;
+  double dr, b, a;
+  if (r < s->x[0]) return s->quintic ? s->grad2[0] : 0.0;
+  if (r > s->x[n - 1]) return s->quintic ? s->grad2[1] : 0.0;
+  dr = r - s->x[0];
+  if (dr < 0) k = 0;
+  else {
+    k = (int)(dr * s->invstep);
+    if (k >= n - 1) k = n - 2;
+  }
+  b = (dr - k * s->step) * s->invstep;
+  a = 1.0 - b;
+  if (!s->quintic) return a * s->ypp[k] + b * s->ypp[k + 1];
+  /* d^2/dx^2 of the quintic piece of sp_comb_k5 */
+  return a * s->ypp[k] + b * s->ypp[k + 1] +
+         ((a * a * a - a) * s->yp4[k] + (b * b * b - b) * s->yp4[k + 1]) * (s->step * s->step) / 6.0;
+}
+
+/* The tangent spline of `in` along `dir`: zero knots and end values, the
+ * direction's entries at the coefficient positions, refreshed. */
+static void sp_setup_tangent(sp_t *t, const mzo_spline *in, const double *dir, int *ci, int ncoeff) {
+  mzo_spline z = *in;
+  double *zy = (double *)calloc(in->nknots, sizeof(double));
+  z.y = zy;
+  z.grad[0] = z.grad[1] = 0.0;
+  z.grad2[0] = z.grad2[1] = 0.0;
+  sp_setup(t, &z, dir, ci, ncoeff);
+  free(zy);
+}
+
+/* value and derivative of a spline at a fixed knot and shift, and their tangents */
+static double tcomb_k(const sp_t *s, const sp_t *ts, int knot, double shift, double *grad, double *tval,
+                      double *tgrad) {
+  *tval = sp_comb_k(ts, knot, shift, tgrad);
+  return sp_comb_k(s, knot, shift, grad);
+}
+
+double mzo_objective_tangent(const mzo_db *db, const mzo_pot *pot, const double *coeffs, const double *dir,
+                             double *dobj) {
+  const int meam = pot->style == 1 || pot->style == 2 || pot->style == 4 || pot->style == 5;
+  const int gmeam = pot->style == 2, pairpot = pot->style == 3;
+  const int nj = pot->style == 4 ? 1 : pot->style == 5 ? 2 : 0;
+  const int nf = db->nfun;
+  const int nt = pot->ntypes, npair = nt * (nt + 1) / 2;
+  const int N = db->natoms, NC = db->ncells;
+  int s, ci = 0, cj = 0, i, m, d;
+  sp_t *sp = (sp_t *)malloc(sizeof(sp_t) * pot->nsplines);
+  sp_t *tsp = (sp_t *)malloc(sizeof(sp_t) * pot->nsplines);
+  const int P = mzo_ncoeff(pot);
+  for (s = 0; s < pot->nsplines; ++s) {
+    sp_setup(&sp[s], &pot->splines[s], coeffs, &ci, P);
+    sp_setup_tangent(&tsp[s], &pot->splines[s], dir, &cj, P);
+  }
+#define SPL(base, idx) (&sp[(base) + (idx)])
+#define TSPL(base, idx) (&tsp[(base) + (idx)])
+  const int o_phi = 0, o_rho = npair, o_U = npair + nt, o_f = npair + 2 * nt, o_g = 2 * npair + 2 * nt;
+  int o_p[2] = {0, 0}, o_q[2] = {0, 0};
+  for (m = 0; m < nj; ++m) {
+    o_p[m] = 2 * npair + 3 * nt + m * (npair + nt);
+    o_q[m] = o_p[m] + npair;
+  }
+
+  double *energy = (double *)calloc(NC, sizeof(double)), *tenergy = (double *)calloc(NC, sizeof(double));
+  double *stress = (double *)calloc(6 * (size_t)NC, sizeof(double));
+  double *tstress = (double *)calloc(6 * (size_t)NC, sizeof(double));
+  double *force = (double *)calloc(3 * (size_t)N, sizeof(double));
+  double *tforce = (double *)calloc(3 * (size_t)N, sizeof(double));
+  double *constraint = (double *)calloc(NC, sizeof(double)), *tconstraint = (double *)calloc(NC, sizeof(double));
+  int maxrow = 0;
+  for (i = 0; i < N; ++i) {
+    int n = (int)(db->pair_off[i + 1] - db->pair_off[i]);
+    if (n > maxrow) maxrow = n;
+  }
+  const size_t R1 = (size_t)maxrow + 1;
+  double *drho = (double *)calloc(R1, sizeof(double)), *tdrho = (double *)calloc(R1, sizeof(double));
+  double *fv = (double *)calloc(R1, sizeof(double)), *tfv = (double *)calloc(R1, sizeof(double));
+  double *dfv = (double *)calloc(R1, sizeof(double)), *tdfv = (double *)calloc(R1, sizeof(double));
+  double *pv = (double *)calloc(2 * R1, sizeof(double)), *tpv = (double *)calloc(2 * R1, sizeof(double));
+  double *dpv = (double *)calloc(2 * R1, sizeof(double)), *tdpv = (double *)calloc(2 * R1, sizeof(double));
+  size_t maxtrip = (size_t)maxrow * (maxrow > 0 ? maxrow - 1 : 0) / 2 + 1;
+  double *tq = (double *)malloc(sizeof(double) * 2 * maxtrip), *tdq = (double *)malloc(sizeof(double) * 2 * maxtrip);
+  double *ttq = (double *)malloc(sizeof(double) * 2 * maxtrip), *ttdq = (double *)malloc(sizeof(double) * 2 * maxtrip);
+  int *tj_ = (int *)malloc(sizeof(int) * maxtrip), *tk_ = (int *)malloc(sizeof(int) * maxtrip);
+  double *tg = (double *)malloc(sizeof(double) * maxtrip), *tdg = (double *)malloc(sizeof(double) * maxtrip);
+  double *ttg = (double *)malloc(sizeof(double) * maxtrip), *ttdg = (double *)malloc(sizeof(double) * maxtrip);
+  double *tcos = (double *)malloc(sizeof(double) * maxtrip);
+
+  for (i = 0; i < N; ++i) {
+    const int cell = db->atom_cell[i], ti = db->atom_type[i];
+    const int64_t p0 = db->pair_off[i];
+    const int n = (int)(db->pair_off[i + 1] - p0);
+    double *Fi = force + 3 * (size_t)i, *S = stress + 6 * (size_t)cell;
+    double *tFi = tforce + 3 * (size_t)i, *tS = tstress + 6 * (size_t)cell;
+    double rho_val = 0.0, trho = 0.0, dF = 0.0, tdF = 0.0;
+    int p, ntrip = 0, t;
+    for (p = 0; p < n; ++p) {
+      const int64_t q = p0 + p;
+      const int j = db->pair_nbr[q], tj = db->atom_type[j];
+      const double *u = db->pair_u + 3 * q, r = db->pair_r[q];
+      const int kphi = db->pair_knot[nf * q], krho = db->pair_knot[nf * q + 1], kf = db->pair_knot[nf * q + 2];
+      double *Fj = force + 3 * (size_t)j, *tFj = tforce + 3 * (size_t)j;
+      if (kphi != -1) {
+        const int pij = pair_ij(nt, ti, tj);
+        double phigrad, tphigrad, tphival, phival, tmp[3], ttmp[3];
+        phival = tcomb_k(SPL(o_phi, pij), TSPL(o_phi, pij), kphi, db->pair_shift[nf * q], &phigrad, &tphival,
+                         &tphigrad);
+        if (!pairpot || j == i) {
+          phival *= 0.5; phigrad *= 0.5; tphival *= 0.5; tphigrad *= 0.5;
+        }
+        energy[cell] += phival;
+        tenergy[cell] += tphival;
+        for (d = 0; d < 3; ++d) {
+          tmp[d] = u[d] * phigrad;
+          ttmp[d] = u[d] * tphigrad;
+          Fi[d] += tmp[d]; Fj[d] -= tmp[d];
+          tFi[d] += ttmp[d]; tFj[d] -= ttmp[d];
+        }
+        S[0] -= u[0] * (tmp[0] * r); S[1] -= u[1] * (tmp[1] * r); S[2] -= u[2] * (tmp[2] * r);
+        S[3] -= u[0] * (tmp[1] * r); S[4] -= u[1] * (tmp[2] * r); S[5] -= u[2] * (tmp[0] * r);
+        tS[0] -= u[0] * (ttmp[0] * r); tS[1] -= u[1] * (ttmp[1] * r); tS[2] -= u[2] * (ttmp[2] * r);
+        tS[3] -= u[0] * (ttmp[1] * r); tS[4] -= u[1] * (ttmp[2] * r); tS[5] -= u[2] * (ttmp[0] * r);
+      }
+      if (!pairpot && krho != -1) {
+        double tv;
+        rho_val += tcomb_k(SPL(o_rho, tj), TSPL(o_rho, tj), krho, db->pair_shift[nf * q + 1], &drho[p], &tv,
+                           &tdrho[p]);
+        trho += tv;
+      } else {
+        drho[p] = tdrho[p] = 0.0;
+      }
+      if (meam) {
+        const int pij = pair_ij(nt, ti, tj);
+        if (kf != -1)
+          fv[p] = tcomb_k(SPL(o_f, pij), TSPL(o_f, pij), kf, db->pair_shift[nf * q + 2], &dfv[p], &tfv[p], &tdfv[p]);
+        else
+          fv[p] = dfv[p] = tfv[p] = tdfv[p] = 0.0;
+      }
+      for (m = 0; m < nj; ++m) {
+        const int kp = db->pair_knot[nf * q + 3 + m], pij = pair_ij(nt, ti, tj);
+        if (kp != -1)
+          pv[2 * p + m] = tcomb_k(SPL(o_p[m], pij), TSPL(o_p[m], pij), kp, db->pair_shift[nf * q + 3 + m],
+                                  &dpv[2 * p + m], &tpv[2 * p + m], &tdpv[2 * p + m]);
+        else
+          pv[2 * p + m] = dpv[2 * p + m] = tpv[2 * p + m] = tdpv[2 * p + m] = 0.0;
+      }
+    }
+    if (meam) {
+      int j, k;
+      for (j = 0; j < n - 1; ++j)
+        for (k = j + 1; k < n; ++k) {
+          const int gi = gmeam ? ti * npair + pair_ij(nt, db->atom_type[db->pair_nbr[p0 + j]],
+                                                      db->atom_type[db->pair_nbr[p0 + k]])
+                               : ti;
+          const sp_t *g = SPL(o_g, gi), *tgs = TSPL(o_g, gi);
+          const double *uj = db->pair_u + 3 * (p0 + j), *uk = db->pair_u + 3 * (p0 + k);
+          double c = uj[0] * uk[0] + uj[1] * uk[1] + uj[2] * uk[2];
+          double gsh, qs[2];
+          int gk = sp_knotshift(g, c, &gsh), qk[2] = {-1, -1}, anyq = 0;
+          for (m = 0; m < nj; ++m) {
+            qk[m] = sp_knotshift(SPL(o_q[m], ti), c, &qs[m]);
+            anyq |= qk[m] != -1;
+          }
+          if (gk == -1 && !anyq) continue;
+          tj_[ntrip] = j;
+          tk_[ntrip] = k;
+          tcos[ntrip] = c;
+          if (gk != -1) tg[ntrip] = tcomb_k(g, tgs, gk, gsh, &tdg[ntrip], &ttg[ntrip], &ttdg[ntrip]);
+          else tg[ntrip] = tdg[ntrip] = ttg[ntrip] = ttdg[ntrip] = 0.0;
+          for (m = 0; m < nj; ++m) {
+            const size_t e = 2 * (size_t)ntrip + m;
+            if (qk[m] != -1)
+              tq[e] = tcomb_k(SPL(o_q[m], ti), TSPL(o_q[m], ti), qk[m], qs[m], &tdq[e], &ttq[e], &ttdq[e]);
+            else tq[e] = tdq[e] = ttq[e] = ttdq[e] = 0.0;
+          }
+          rho_val += fv[j] * fv[k] * tg[ntrip];
+          trho += tfv[j] * fv[k] * tg[ntrip] + fv[j] * tfv[k] * tg[ntrip] + fv[j] * fv[k] * ttg[ntrip];
+          for (m = 0; m < nj; ++m) {
+            const size_t e = 2 * (size_t)ntrip + m;
+            energy[cell] += pv[2 * j + m] * pv[2 * k + m] * tq[e];
+            tenergy[cell] += tpv[2 * j + m] * pv[2 * k + m] * tq[e] + pv[2 * j + m] * tpv[2 * k + m] * tq[e] +
+                             pv[2 * j + m] * pv[2 * k + m] * ttq[e];
+          }
+          ++ntrip;
+        }
+    }
+    if (pairpot) continue;
+    {
+      const sp_t *Ui = SPL(o_U, ti), *tUi = TSPL(o_U, ti);
+      const double w = db->cell_weight[cell];
+      double tUv, tUg;
+      if (rho_val < Ui->x[0]) {
+        double rho_i = Ui->x[0];
+        constraint[cell] += w * DUMMY_WEIGHT * 10. * (rho_i - rho_val) * (rho_i - rho_val);
+        tconstraint[cell] += w * DUMMY_WEIGHT * 10. * 2.0 * (rho_i - rho_val) * (-trho);
+        if (!pot->embed_extrap) { rho_val = rho_i; trho = 0.0; }
+      } else if (rho_val > Ui->x[Ui->n - 1]) {
+        double rho_f = Ui->x[Ui->n - 1];
+        constraint[cell] += w * DUMMY_WEIGHT * 10. * (rho_val - rho_f) * (rho_val - rho_f);
+        tconstraint[cell] += w * DUMMY_WEIGHT * 10. * 2.0 * (rho_val - rho_f) * trho;
+        if (!pot->embed_extrap) { rho_val = rho_f; trho = 0.0; }
+      }
+      energy[cell] += sp_comb_x(Ui, rho_val, &dF);
+      tUv = sp_comb_x(tUi, rho_val, &tUg);
+      tenergy[cell] += tUv + dF * trho;
+      tdF = tUg + sp_second_x(Ui, rho_val) * trho;
+    }
+    for (p = 0; p < n; ++p) {
+      const int64_t q = p0 + p;
+      const int j = db->pair_nbr[q];
+      const double *u = db->pair_u + 3 * q, r = db->pair_r[q];
+      double *Fj = force + 3 * (size_t)j, *tFj = tforce + 3 * (size_t)j, tmp[3], ttmp[3];
+      for (d = 0; d < 3; ++d) {
+        tmp[d] = u[d] * drho[p] * dF;
+        ttmp[d] = u[d] * (tdrho[p] * dF + drho[p] * tdF);
+        Fi[d] += tmp[d]; Fj[d] -= tmp[d];
+        tFi[d] += ttmp[d]; tFj[d] -= ttmp[d];
+      }
+      S[0] -= u[0] * (tmp[0] * r); S[1] -= u[1] * (tmp[1] * r); S[2] -= u[2] * (tmp[2] * r);
+      S[3] -= u[0] * (tmp[1] * r); S[4] -= u[1] * (tmp[2] * r); S[5] -= u[2] * (tmp[0] * r);
+      tS[0] -= u[0] * (ttmp[0] * r); tS[1] -= u[1] * (ttmp[1] * r); tS[2] -= u[2] * (ttmp[2] * r);
+      tS[3] -= u[0] * (ttmp[1] * r); tS[4] -= u[1] * (ttmp[2] * r); tS[5] -= u[2] * (ttmp[0] * r);
+    }
+    for (t = 0; t < ntrip; ++t) {
+      const int j = tj_[t], k = tk_[t];
+      const int64_t qj = p0 + j, qk = p0 + k;
+      const double *uj = db->pair_u + 3 * qj, *uk = db->pair_u + 3 * qk;
+      const double rj = db->pair_r[qj], rk = db->pair_r[qk];
+      const double invrj = 1.0 / rj, invrk = 1.0 / rk;
+      double *Fj = force + 3 * (size_t)db->pair_nbr[qj], *Fk = force + 3 * (size_t)db->pair_nbr[qk];
+      double *tFj = tforce + 3 * (size_t)db->pair_nbr[qj], *tFk = tforce + 3 * (size_t)db->pair_nbr[qk];
+      double dV3j = tg[t] * dfv[j] * fv[k] * dF;
+      double dV3k = tg[t] * fv[j] * dfv[k] * dF;
+      double V3 = tdg[t] * fv[j] * fv[k] * dF;
+      double tdV3j = ttg[t] * dfv[j] * fv[k] * dF + tg[t] * tdfv[j] * fv[k] * dF + tg[t] * dfv[j] * tfv[k] * dF +
+                     tg[t] * dfv[j] * fv[k] * tdF;
+      double tdV3k = ttg[t] * fv[j] * dfv[k] * dF + tg[t] * tfv[j] * dfv[k] * dF + tg[t] * fv[j] * tdfv[k] * dF +
+                     tg[t] * fv[j] * dfv[k] * tdF;
+      double tV3 = ttdg[t] * fv[j] * fv[k] * dF + tdg[t] * tfv[j] * fv[k] * dF + tdg[t] * fv[j] * tfv[k] * dF +
+                   tdg[t] * fv[j] * fv[k] * tdF;
+      for (m = 0; m < nj; ++m) {
+        const size_t e = 2 * (size_t)t + m;
+        const double pj = pv[2 * j + m], pk = pv[2 * k + m], dpj = dpv[2 * j + m], dpk = dpv[2 * k + m];
+        const double tpj = tpv[2 * j + m], tpk = tpv[2 * k + m], tdpj = tdpv[2 * j + m], tdpk = tdpv[2 * k + m];
+        dV3j += tq[e] * dpj * pk;
+        dV3k += tq[e] * pj * dpk;
+        V3 += tdq[e] * pj * pk;
+        tdV3j += ttq[e] * dpj * pk + tq[e] * tdpj * pk + tq[e] * dpj * tpk;
+        tdV3k += ttq[e] * pj * dpk + tq[e] * tpj * dpk + tq[e] * pj * tdpk;
+        tV3 += ttdq[e] * pj * pk + tdq[e] * tpj * pk + tdq[e] * pj * tpk;
+      }
+      const double vlj = V3 * invrj, vlk = V3 * invrk, tvlj = tV3 * invrj, tvlk = tV3 * invrk;
+      const double vv3j = dV3j - vlj * tcos[t], vv3k = dV3k - vlk * tcos[t];
+      const double tvv3j = tdV3j - tvlj * tcos[t], tvv3k = tdV3k - tvlk * tcos[t];
+      double dfj[3], dfk[3], tdfj[3], tdfk[3];
+      for (d = 0; d < 3; ++d) {
+        dfj[d] = uj[d] * vv3j + uk[d] * vlj;
+        dfk[d] = uk[d] * vv3k + uj[d] * vlk;
+        tdfj[d] = uj[d] * tvv3j + uk[d] * tvlj;
+        tdfk[d] = uk[d] * tvv3k + uj[d] * tvlk;
+        Fi[d] += dfj[d] + dfk[d];
+        Fj[d] -= dfj[d];
+        Fk[d] -= dfk[d];
+        tFi[d] += tdfj[d] + tdfk[d];
+        tFj[d] -= tdfj[d];
+        tFk[d] -= tdfk[d];
+      }
+      for (d = 0; d < 3; ++d) {
+        dfj[d] *= rj; dfk[d] *= rk; tdfj[d] *= rj; tdfk[d] *= rk;
+      }
+      S[0] -= uj[0] * dfj[0]; S[1] -= uj[1] * dfj[1]; S[2] -= uj[2] * dfj[2];
+      S[3] -= uj[0] * dfj[1]; S[4] -= uj[1] * dfj[2]; S[5] -= uj[2] * dfj[0];
+      S[0] -= uk[0] * dfk[0]; S[1] -= uk[1] * dfk[1]; S[2] -= uk[2] * dfk[2];
+      S[3] -= uk[0] * dfk[1]; S[4] -= uk[1] * dfk[2]; S[5] -= uk[2] * dfk[0];
+      tS[0] -= uj[0] * tdfj[0]; tS[1] -= uj[1] * tdfj[1]; tS[2] -= uj[2] * tdfj[2];
+      tS[3] -= uj[0] * tdfj[1]; tS[4] -= uj[1] * tdfj[2]; tS[5] -= uj[2] * tdfj[0];
+      tS[0] -= uk[0] * tdfk[0]; tS[1] -= uk[1] * tdfk[1]; tS[2] -= uk[2] * tdfk[2];
+      tS[3] -= uk[0] * tdfk[1]; tS[4] -= uk[1] * tdfk[2]; tS[5] -= uk[2] * tdfk[0];
+    }
+  }
+
+  /* accumulate_error (potential.cpp:415-491) and its tangent: F = sum e^2, dF = 2 sum e de */
+  double sum = 0.0, tsum = 0.0;
+  int c;
+  for (c = 0; c < NC; ++c) {
+    const int a0 = db->cell_atom0[c], na = db->cell_atom0[c + 1] - a0;
+    const double w = db->cell_weight[c];
+    const double ew = w * db->cell_eweight[c] * pot->energy_weight * na;
+    const double sw = w * db->cell_sweight[c] * pot->stress_weight;
+    int q, a;
+    double e = ew * (energy[c] / na - db->cell_energy0[c]), te = ew * (tenergy[c] / na);
+    sum += e * e;
+    tsum += 2.0 * e * te;
+    for (q = 0; q < 6; ++q) {
+      e = sw * (stress[6 * c + q] / db->cell_vol[c] - db->cell_stress0[6 * c + q]);
+      te = sw * (tstress[6 * c + q] / db->cell_vol[c]);
+      sum += e * e;
+      tsum += 2.0 * e * te;
+    }
+    for (a = a0; a < a0 + na; ++a)
+      for (d = 0; d < 3; ++d) {
+        e = w * (force[3 * a + d] - db->atom_force0[3 * a + d]);
+        te = w * tforce[3 * a + d];
+        sum += e * e;
+        tsum += 2.0 * e * te;
+      }
+  }
+  for (c = 0; c < NC && !pairpot; ++c) {
+    sum += constraint[c] * constraint[c];
+    tsum += 2.0 * constraint[c] * tconstraint[c];
+  }
+  if (pairpot) {
+    /* no punishments */
+  } else if (meam) {
+    /* signed largest-|y| knot (Spline::get_max_y_mag spline.cpp:58-67 over the
+     * group, PotFns::get_max_y_mag pot_fns.cpp:223-234; GMEAM per f spline):
+     * fe = 2500 (1 - |m|)^2, dfe = -5000 (1 - |m|) sign(m) dm */
+    int grp, ngrp = gmeam ? npair : 1 + nj;
+    for (grp = 0; grp < ngrp; ++grp) {
+      const int base = gmeam ? o_f + grp : (grp == 0 ? o_f : o_p[grp - 1]);
+      const int nspl = gmeam ? 1 : npair;
+      double my = 0.0, tmy = 0.0;
+      int f, k;
+      for (f = 0; f < nspl; ++f) {
+        double mm = 0.0, tmm = 0.0;
+        for (k = 0; k < sp[base + f].n; ++k)
+          if (fabs(mm) < fabs(sp[base + f].y[k])) {
+            mm = sp[base + f].y[k];
+            tmm = tsp[base + f].y[k];
+          }
+        if (fabs(my) < fabs(mm)) {
+          my = mm;
+          tmy = tmm;
+        }
+      }
+      const double mag = fabs(my);
+      const double fe = DUMMY_WEIGHT * 25. * (1.0 - mag) * (1.0 - mag);
+      const double sg = my > 0 ? 1.0 : (my < 0 ? -1.0 : 0.0);
+      const double tfe = DUMMY_WEIGHT * 25. * 2.0 * (1.0 - mag) * (-sg * tmy);
+      sum += fe * fe;
+      tsum += 2.0 * fe * tfe;
+    }
+  } else {
+    int t;
+    for (t = 0; t < nt; ++t) {
+      double g, tgv, mid = 0.5 * (sp[o_U + t].x[0] + sp[o_U + t].x[sp[o_U + t].n - 1]);
+      sp_comb_x(&sp[o_U + t], mid, &g);
+      sp_comb_x(&tsp[o_U + t], mid, &tgv);
+      const double e = DUMMY_WEIGHT * g, te = DUMMY_WEIGHT * tgv;
+      sum += e * e;
+      tsum += 2.0 * e * te;
+    }
+  }
+#undef SPL
+#undef TSPL
+  if (dobj) *dobj = tsum;
+  free(tj_); free(tk_); free(tg); free(tdg); free(ttg); free(ttdg); free(tcos);
+  free(drho); free(tdrho); free(fv); free(tfv); free(dfv); free(tdfv);
+  free(pv); free(tpv); free(dpv); free(tdpv); free(tq); free(tdq); free(ttq); free(ttdq);
+  free(energy); free(tenergy); free(stress); free(tstress); free(force); free(tforce);
+  free(constraint); free(tconstraint);
+  for (s = 0; s < pot->nsplines; ++s) {
+    sp_free(&sp[s]);
+    sp_free(&tsp[s]);
+  }
+  free(sp);
+  free(tsp);
+  return sum;
+}

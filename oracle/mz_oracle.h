@@ -77,6 +77,13 @@ typedef struct {
 double mzo_objective(const mzo_db *db, const mzo_pot *pot, const double *coeffs, double *errvec,
                      double *forces, double *energy, double *stress, double *dens);
 
+/* The objective of `coeffs` and, in *dobj, its exact derivative along the
+ * direction `dir` [ncoeff] (tangent-linear restatement of mzo_objective:
+ * forward-mode differentiation statement by statement, no finite
+ * differences).  Returns the objective. */
+double mzo_objective_tangent(const mzo_db *db, const mzo_pot *pot, const double *coeffs, const double *dir,
+                             double *dobj);
+
 /* Length of the residual vector. */
 int mzo_esize(const mzo_db *db, const mzo_pot *pot);
 

@@ -57,3 +57,44 @@ def test_oracle_against_live_reference(tmp_path):
     assert rel(r["obj"], ref["obj"]) <= 1e-12
     assert np.max(np.abs(r["forces"].ravel() - ref["force"])) <= 1e-10
     assert np.array_equal(np.sort(r["dens"]), np.sort(ref["dens"])) or np.allclose(r["dens"], ref["dens"], rtol=1e-14)
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_tangent_oracle_matches_central_differences(name):
+    """The tangent-linear restatement (exact directional derivatives) against
+    central differences: the reference's own (h = 1e-6, golden `fdgrad`) where
+    the case has them, and the oracle's otherwise.  Central differences carry
+    O(h^2) truncation and rounding error, about 1e-9 of the largest
+    component here, so the bar is 1e-8 of max|g|.  The objective the tangent
+    pass returns is the plain restatement's, bit for bit."""
+    case = load_case(name)
+    g = case["gold"]
+    orc = oracle_for(case)
+    x = g["coeff"]
+    grad = orc.gradient(x)
+    obj, _ = orc.tangent(x, np.zeros_like(x))
+    assert obj == orc.objective(x)
+    if "fdgrad" in g:
+        fd = g["fdgrad"]
+    else:
+        fd = np.zeros_like(x)
+        for i in range(x.size):
+            h = 1e-6 * max(1.0, abs(x[i]))
+            e = np.zeros_like(x)
+            e[i] = h
+            fd[i] = (orc.objective(x + e) - orc.objective(x - e)) / (2 * h)
+    scale = np.max(np.abs(grad))
+    assert np.max(np.abs(grad - fd)) <= 1e-8 * scale, (name, np.max(np.abs(grad - fd)) / scale)
+
+
+def test_tangent_oracle_is_linear_in_the_direction():
+    """d/dt F(x + t (a u + b v)) = a dF.u + b dF.v (forward mode is linear in
+    the direction), on a two-species MEAM case."""
+    case = load_case("meam_sparse")
+    orc = oracle_for(case)
+    x = case["gold"]["coeff"]
+    rng = np.random.default_rng(3)
+    u, v = rng.standard_normal(x.size), rng.standard_normal(x.size)
+    du, dv = orc.tangent(x, u)[1], orc.tangent(x, v)[1]
+    dw = orc.tangent(x, 2.0 * u - 0.5 * v)[1]
+    assert abs(dw - (2.0 * du - 0.5 * dv)) <= 1e-12 * (abs(2.0 * du) + abs(0.5 * dv))

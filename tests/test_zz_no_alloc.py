@@ -49,6 +49,36 @@ def test_noalloc_matches_objective_two_calls(name):
         assert np.max(np.abs(forces - ref["forces"][0])) <= FP64_FORCE
 
 
+def test_noalloc_allocates_no_device_memory():
+    """After a first call (which loads the kernels and looks up the array's
+    address), further calls leave the device's free memory unchanged."""
+    import torch
+    case = load_case("meam_mix6")
+    g = case["gold"]
+    _noalloc(case, g["coeff"])
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info(0)[0]
+    for x in (g["coeff"], g["coeff2"], g["coeff"]):
+        _noalloc(case, x)
+    torch.cuda.synchronize()
+    assert torch.cuda.mem_get_info(0)[0] == free0
+
+
+def test_noalloc_rejects_bad_device_ordinal():
+    from meamzilla_b200 import _lib
+    from meamzilla_b200._lib import MzError, lib, ptr
+    case = load_case("eam_bcc3")
+    w = case["weights"]
+    for dev in (-1, 1 << 20):
+        s = _lib.Settings(w["energy_weight"], w["stress_weight"], w["embed_extrap"], dev, 1, 0)
+        x = np.ascontiguousarray(case["gold"]["coeff"])
+        obj = np.zeros(1)
+        with pytest.raises(MzError) as e:
+            _lib.check(lib().mz_objective_noalloc(case["db"].handle, case["pot"].handle, C.byref(s), ptr(x),
+                                                  ptr(obj), None))
+        assert "MZ_ERR_ARG" in str(e.value) and "ordinal" in str(e.value)
+
+
 def test_noalloc_rejects_database_beyond_its_array():
     from meamzilla_b200 import synth
     from meamzilla_b200._lib import MzError
