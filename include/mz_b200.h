@@ -321,6 +321,13 @@ enum {
   MZ_K_FINAL,       /* sum of squares + punishments                         */
   MZ_K_ADJ,         /* adjoint pass over the neighbour rows                 */
   MZ_K_GRAD_FINAL,  /* table gradient -> coefficient gradient               */
+  /* mixed-precision meam/spline over triplet moments (the "FM" path):       */
+  MZ_K_FM_COEF,     /* candidates' B-spline coefficients and their products */
+  MZ_K_FM_FWD,      /* contraction of the moments: G, Y1, Y2 per slot       */
+  MZ_K_FM_EPI,      /* densities, embedding, reaction vectors               */
+  MZ_K_FM_PRE,      /* adjoint weights, pair-function and U gradients       */
+  MZ_K_FM_ADJ,      /* transposed contraction: moment-space gradient        */
+  MZ_K_FM_GRAD,     /* moment-space and B-spline gradients -> knot table    */
   MZ_NKERNELS
 };
 const char *mz_kernel_name(int kernel);
@@ -330,6 +337,13 @@ const char *mz_kernel_name(int kernel);
  * and their count to launches[kernel] (arrays of MZ_NKERNELS, zeroed by the
  * caller), and forgets them. */
 mz_status mz_profile(mz_ctx *ctx, int on);
+/* 1 when the tuned launches of (precision, grad) use the triplet-moment
+ * path for mixed-precision meam/spline (the candidates' triplet sums as
+ * contractions of per-slot moments built once per database: MZ_K_FM_*), 0
+ * when they use the row kernels.  MZ_FM=0 in the environment at mz_create
+ * keeps the row kernels, MZ_FM=2 always takes the moment path where it
+ * applies, the default lets the tuner time both.  No reference counterpart. */
+mz_status mz_moment_path(const mz_ctx *ctx, int precision, int grad, int *on);
 mz_status mz_kernel_times(mz_ctx *ctx, double *ms, int64_t *launches);
 
 /* Objective of one coefficient vector without allocating any device memory.

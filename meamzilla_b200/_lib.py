@@ -122,6 +122,7 @@ _SIGS = {
     "mz_launch_count": (C.c_int, [C.c_void_p, C.POINTER(C.c_int64)]),
     "mz_tensor_core_forward": (C.c_int, [C.c_void_p, C.POINTER(C.c_int)]),
     "mz_kernel_name": (C.c_char_p, [C.c_int]),
+    "mz_moment_path": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_int)]),
     "mz_profile": (C.c_int, [C.c_void_p, C.c_int]),
     "mz_tuning": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_void_p]),
     "mz_kernel_times": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
@@ -130,7 +131,7 @@ _SIGS = {
                                        C.c_void_p]),
 }
 
-MZ_NKERNELS = 7
+MZ_NKERNELS = 13
 
 
 def lib() -> C.CDLL:

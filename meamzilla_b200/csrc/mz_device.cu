@@ -47,6 +47,7 @@
 #include "mz_fwd2.cuh"
 #include "mz_adj2.cuh"
 #include "mz_tc_fwd.cuh"
+#include "mz_fm.cuh"
 
 // ================================================================= context
 
@@ -102,6 +103,7 @@ struct mz_ctx {
   int adj_ctas_max = 1, adj_per_sm = 1;
   struct Tune {
     bool done = false;
+    bool fm = false;  // mixed meam/spline: the triplet-moment path
     int fwd = 0, adj = 0, ctas = 0;
     int nc = 1;      // candidates per CTA of the forward (2: k_atoms2, mixed meam/spline)
     int adj_nc = 1;  // candidates per CTA of the adjoint (2: k_adj2)
@@ -115,6 +117,18 @@ struct mz_ctx {
   int autotune = 1;  // MZ_TUNE: 1 time the variants, 0 the first variant, 2 the first with two candidates per CTA
   int adj_ctas_force = 0;  // MZ_ADJ_CTAS: persistent CTAs of the adjoint, fixed (0: the tuner's)
   bool profiling = false;
+  // Mixed-precision meam/spline over triplet moments (mz_fm.cuh): eligible
+  // from the potential's shape; the moments are built at the first mixed
+  // launch that uses the path; MZ_FM=0 never uses it, 2 always, 1 (default)
+  // lets the tuner time it against the row kernels.
+  struct Fm {
+    bool eligible = false, ready = false, failed = false;
+    FmPlan plan{};
+    int CGmax = 8, ngroups_max = 1;
+    size_t smem_pre = 0;
+  } fm;
+  int fm_mode = 1;
+  bool fm_on = false;  // the moment path in force for mixed launches
   struct Mark {
     int kernel;
     cudaEvent_t start, stop;
@@ -282,6 +296,189 @@ void launch_adj(mz_ctx *ctx, int n, size_t smem) {
                                                             ctx->d_partial, ctx->d_wglob);
 }
 
+template <class K>
+void smem_attr(K kernel, size_t bytes) {
+  ck(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes), "smem attribute");
+}
+
+// ------------------------------------------------------- triplet moments
+
+// Candidates per group of the moment path's layouts for a launch of n.
+int fm_cg(int n) {
+  int cg = 8;
+  while (cg < n && cg < 64) cg *= 2;
+  return cg;
+}
+
+template <int NW>
+void fm_fwd_launch(mz_ctx *ctx, const FmPlan &fp, int G) {
+  k_fm_gemm_fwd<NW><<<dim3(fp.ntiles, G), NW * 32, fm_fwd_smem<NW>(fp.Dpad), ctx->stream>>>(fp);
+}
+
+// The moments, the slots' frames and the path's buffers, at the first
+// launch that uses the path.  Buffers of the row kernels are reused where
+// they are large enough for the path's layouts.  False (and the path stays
+// off for the context) when the device memory is not there.
+bool fm_prepare(mz_ctx *ctx) {
+  auto &fm = ctx->fm;
+  if (fm.ready) return true;
+  if (fm.failed || !fm.eligible) return false;
+  FmPlan &fp = fm.plan;
+  const size_t C = ctx->cand_cap;
+  fm.CGmax = fm_cg((int)std::min<size_t>(C, 64));
+  fm.ngroups_max = (int)((C + fm.CGmax - 1) / fm.CGmax);
+  const size_t G = fm.ngroups_max, CG = fm.CGmax, Cp = G * CG;
+  const size_t Q = fp.Q, N = ctx->natoms, NC = ctx->ncells, Np = ctx->npairs, ns = ctx->nsplines;
+  const size_t stride = ctx->stride;
+  fp.nctas_pre = std::max(1, std::min(fp.nblk, ctx->nsm));
+  fp.nctas_adj = std::max(1, std::min(fp.ntiles, ctx->nsm));
+  const size_t aux_rows = (size_t)ctx->pot.aux_rows;
+  struct Need {
+    void *have;
+    size_t have_bytes, need_bytes;
+  };
+  Need need[] = {
+      {ctx->d_aux, sizeof(double) * C * aux_rows * Np, sizeof(float) * G * Q * 3 * CG},        // Y
+      {ctx->d_V, sizeof(double) * C * 3 * Np, sizeof(double) * Cp * Np * 3},                   // V
+      {ctx->d_aout, sizeof(double) * C * AO_COUNT * N, sizeof(double) * Cp * AO_COUNT * N},    // aoutF
+      {ctx->d_lam, sizeof(double) * C * 3 * N, sizeof(float) * Cp * 3 * N},                    // lamf
+      {ctx->d_seeds, sizeof(double) * C * CS_COUNT * NC, sizeof(double) * Cp * CS_COUNT * NC}, // seedF
+  };
+  size_t extra = sizeof(float) * (3 * (size_t)fp.Dpad * Q + 8 * Q) + sizeof(float) * G * fp.nt * fp.Dpad * CG +
+                 sizeof(double) * C * ns * FM_MAXB + sizeof(float) * G * ns * FM_MAXB * CG +
+                 sizeof(double) * G * CG *
+                     ((size_t)fp.nctas_adj * fp.nt * fp.Dpad + (size_t)fp.nctas_pre * (ns * FM_MAXB + stride));
+  for (auto &x : need)
+    if (x.need_bytes > x.have_bytes) extra += x.need_bytes;
+  size_t freeb = 0, totalb = 0;
+  ck(cudaMemGetInfo(&freeb, &totalb), "cudaMemGetInfo");
+  if (extra > (size_t)(0.85 * (double)freeb)) {
+    fm.failed = true;
+    return false;
+  }
+  auto pick = [&](Need &x) -> void * {
+    return x.need_bytes <= x.have_bytes ? x.have : (void *)dalloc<unsigned char>(ctx, x.need_bytes);
+  };
+  fp.Y = static_cast<float *>(pick(need[0]));
+  fp.V = static_cast<double *>(pick(need[1]));
+  fp.aoutF = static_cast<double *>(pick(need[2]));
+  fp.lamf = static_cast<float *>(pick(need[3]));
+  fp.seedF = static_cast<double *>(pick(need[4]));
+  float *X = dalloc<float>(ctx, 3 * (size_t)fp.Dpad * Q);
+  float *E = dalloc<float>(ctx, 8 * Q);
+  fp.X = X;
+  fp.E = E;
+  fp.Kf = dalloc<float>(ctx, G * fp.nt * fp.Dpad * CG);
+  double *coef64 = dalloc<double>(ctx, C * ns * FM_MAXB);
+  float *coef32 = dalloc<float>(ctx, G * ns * FM_MAXB * CG);
+  fp.coef64 = coef64;
+  fp.coef32 = coef32;
+  fp.Kbar = dalloc<double>(ctx, G * fp.nctas_adj * fp.nt * fp.Dpad * CG);
+  fp.Pbar = dalloc<double>(ctx, G * fp.nctas_pre * ns * FM_MAXB * CG);
+  fp.Tbar = dalloc<double>(ctx, G * fp.nctas_pre * CG * stride);
+  ck(cudaMemsetAsync(X, 0, sizeof(float) * 3 * (size_t)fp.Dpad * Q, ctx->stream), "memset");
+  ck(cudaMemsetAsync(E, 0, sizeof(float) * 8 * Q, ctx->stream), "memset");
+  ck(cudaMemsetAsync(coef64, 0, sizeof(double) * C * ns * FM_MAXB, ctx->stream), "memset");
+  ck(cudaMemsetAsync(coef32, 0, sizeof(float) * G * ns * FM_MAXB * CG, ctx->stream), "memset");
+  fp.CG = fm.CGmax;
+  k_fm_features<<<ctx->natoms, 256, 0, ctx->stream>>>(ctx->db, ctx->pot, ctx->d_geom, fp, X, E);
+  ck(cudaGetLastError(), "k_fm_features launch");
+  ck(cudaStreamSynchronize(ctx->stream), "moments");
+  smem_attr(k_fm_gemm_fwd<1>, fm_fwd_smem<1>(fp.Dpad));
+  smem_attr(k_fm_gemm_fwd<2>, fm_fwd_smem<2>(fp.Dpad));
+  smem_attr(k_fm_gemm_fwd<4>, fm_fwd_smem<4>(fp.Dpad));
+  smem_attr(k_fm_gemm_fwd<8>, fm_fwd_smem<8>(fp.Dpad));
+  fm.smem_pre = fm_pre_smem(ctx->nsplines);
+  smem_attr(k_fm_adj_pre, fm.smem_pre);
+  smem_attr(k_fm_gemm_adj, fm_adj_smem(fp.Dpad, 64));
+  fm.ready = true;
+  return true;
+}
+
+// The moment path's launch sequence (after k_prep): objective, and with
+// d_grad the gradient.
+void enqueue_fm(mz_ctx *ctx, int n, double *d_obj, double *d_errvec, double *d_forces, double *d_energy,
+                double *d_stress, double *d_grad) {
+  cudaStream_t st = ctx->stream;
+  FmPlan fp = ctx->fm.plan;
+  fp.CG = fm_cg(std::min(n, 64));
+  const int G = (n + fp.CG - 1) / fp.CG, CG = fp.CG;
+  const int ns = ctx->nsplines, N = ctx->natoms, NC = ctx->ncells;
+  const bool grad = d_grad != nullptr;
+  {
+    Bracket b(ctx, MZ_K_FM_COEF);
+    k_fm_coef<<<n, std::max(32, ((ns + 31) / 32) * 32), 0, st>>>(n, ctx->d_geom, ns, ctx->stride, ctx->d_tabs, fp,
+                                                                  const_cast<double *>(fp.coef64),
+                                                                  const_cast<float *>(fp.coef32));
+    ck(cudaGetLastError(), "k_fm_coef launch");
+  }
+  {
+    Bracket b(ctx, MZ_K_FM_COEF);
+    const int zs = std::max(1, std::min(64, fp.Dpad * CG / 2048));
+    k_fm_kmat<<<dim3(fp.nt, G, zs), 256, 0, st>>>(n, ctx->pot, fp, fp.coef64, const_cast<float *>(fp.Kf));
+    ck(cudaGetLastError(), "k_fm_kmat launch");
+  }
+  {
+    Bracket b(ctx, MZ_K_FM_FWD);
+    switch (CG / 8) {
+      case 1: fm_fwd_launch<1>(ctx, fp, G); break;
+      case 2: fm_fwd_launch<2>(ctx, fp, G); break;
+      case 4: fm_fwd_launch<4>(ctx, fp, G); break;
+      default: fm_fwd_launch<8>(ctx, fp, G); break;
+    }
+    ck(cudaGetLastError(), "k_fm_gemm_fwd launch");
+  }
+  const unsigned ablocks = (unsigned)(((int64_t)N * CG + 255) / 256);
+  {
+    Bracket b(ctx, MZ_K_FM_EPI);
+    k_fm_epi<<<dim3(ablocks, G), 256, 0, st>>>(ctx->db, ctx->pot, ctx->d_geom, ctx->d_tabs, fp, n);
+    ck(cudaGetLastError(), "k_fm_epi launch");
+  }
+  {
+    Bracket b(ctx, MZ_K_GATHER);
+    k_fm_gather<<<dim3(ablocks, G), 256, 0, st>>>(ctx->db, fp, n, d_forces, d_errvec, ctx->esize, grad ? 1 : 0);
+    ck(cudaGetLastError(), "k_fm_gather launch");
+  }
+  {
+    Bracket b(ctx, MZ_K_CELLS);
+    const unsigned cblocks = (unsigned)(((int64_t)NC * CG + 255) / 256);
+    k_fm_cells<<<dim3(cblocks, G), 256, 0, st>>>(ctx->db, ctx->pot, fp, n, ctx->d_cellobj, d_errvec, ctx->esize,
+                                                 d_energy, d_stress, grad ? 1 : 0);
+    ck(cudaGetLastError(), "k_fm_cells launch");
+  }
+  {
+    Bracket b(ctx, MZ_K_FINAL);
+    k_final<<<n, 256, 0, st>>>(ctx->db, ctx->pot, ctx->d_geom, ctx->d_tabs, ctx->d_cellobj, d_obj, d_errvec,
+                               ctx->esize);
+    ck(cudaGetLastError(), "k_final launch");
+  }
+  if (!grad) return;
+  {
+    Bracket b(ctx, MZ_K_FM_PRE);
+    k_fm_adj_pre<<<dim3(fp.nctas_pre, G), 256, ctx->fm.smem_pre, st>>>(ctx->db, ctx->pot, ctx->d_geom, ctx->d_tabs,
+                                                                       fp, n);
+    ck(cudaGetLastError(), "k_fm_adj_pre launch");
+  }
+  {
+    Bracket b(ctx, MZ_K_FM_ADJ);
+    const int threads = ((fp.Dpad / FM_ROWS) * (CG / 8) + 31) / 32 * 32;
+    k_fm_gemm_adj<<<dim3(fp.nctas_adj, G), std::min(threads, 256), fm_adj_smem(fp.Dpad, CG), st>>>(fp);
+    ck(cudaGetLastError(), "k_fm_gemm_adj launch");
+  }
+  {
+    Bracket b(ctx, MZ_K_FM_GRAD);
+    const size_t sm = sizeof(double) * ((size_t)ns * FM_MAXB + ctx->stride + (size_t)fp.nt * fp.Dpad);
+    k_fm_grad<<<n, 256, sm, st>>>(ctx->pot, ctx->d_geom, fp, fp.coef64, ctx->d_partial);
+    ck(cudaGetLastError(), "k_fm_grad launch");
+  }
+  {
+    Bracket b(ctx, MZ_K_GRAD_FINAL);
+    k_grad_final<<<n, 256, sizeof(double) * ctx->stride, st>>>(ctx->pot, ctx->d_geom, ctx->d_tabs, ctx->d_partial,
+                                                                1, ctx->d_M, ctx->d_cmap, ctx->P, d_grad);
+    ck(cudaGetLastError(), "k_grad_final launch");
+  }
+}
+
 // Enqueue the objective (and, with d_grad, its gradient) of n candidates
 // whose coefficient vectors are already on the device.
 void enqueue(mz_ctx *ctx, int n, const double *d_params, int precision, double *d_obj, double *d_errvec,
@@ -297,6 +494,10 @@ void enqueue(mz_ctx *ctx, int n, const double *d_params, int precision, double *
         ctx->d_tabs, ctx->pstride, ctx->d_ptabs, ctx->d_ptabf, ctx->tc_ok ? ctx->d_wtab : nullptr, ctx->pot.s_g,
         ctx->pot.ntypes, TC_NB, ctx->d_M);
     ck(cudaGetLastError(), "k_prep launch");
+  }
+  if (mixed && meam && ctx->fm_on && ctx->fm.ready) {
+    enqueue_fm(ctx, n, d_obj, d_errvec, d_forces, d_energy, d_stress, d_grad);
+    return;
   }
   {
     Bracket b(ctx, MZ_K_ATOMS);
@@ -376,10 +577,6 @@ __global__ void k_fma_peak(T *out, int iters, T a, T b) {
   if (s == (T)-1.2345) out[0] = s;  // keeps the chain alive
 }
 
-template <class K>
-void smem_attr(K kernel, size_t bytes) {
-  ck(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes), "smem attribute");
-}
 
 // d(ypp)/d(y, slope_left, slope_right) of one spline: the refresh is linear,
 // so its columns are the refresh of unit inputs.
@@ -501,6 +698,7 @@ std::mutex g_tune_mu;
 std::map<std::vector<int64_t>, mz_ctx::Tune> g_tune_cache;
 
 void apply_variant(mz_ctx *ctx, const mz_ctx::Tune &t) {
+  ctx->fm_on = t.fm;
   ctx->fwd_nc = t.nc;
   ctx->adj_nc = t.adj_nc;
   ctx->db.nblocks = ctx->nblk[t.fwd];
@@ -517,7 +715,8 @@ int adj_ctas_for(const mz_ctx *ctx, int v, int per_sm) {
 }
 
 // One objective (+ gradient) with events around every kernel: the device
-// time of `kernel` in ms.  The caller's profiling marks are kept aside.
+// time of `kernel` in ms (of all of them for kernel < 0).  The caller's
+// profiling marks are kept aside.
 double trial(mz_ctx *ctx, int n, const double *d_params, int precision, bool grad, int kernel) {
   std::vector<mz_ctx::Mark> keep;
   keep.swap(ctx->marks);
@@ -539,7 +738,7 @@ double trial(mz_ctx *ctx, int n, const double *d_params, int precision, bool gra
     for (auto &m : ctx->marks) {
       float t = 0.f;
       ck(cudaEventElapsedTime(&t, m.start, m.stop), "cudaEventElapsedTime");
-      if (m.kernel == kernel) ms += t;
+      if (m.kernel == kernel || kernel < 0) ms += t;
     }
   } catch (...) {
     restore();
@@ -557,7 +756,7 @@ void tune_variant(mz_ctx *ctx, int n, const double *d_params, int precision, boo
   if (!t.done) {
     const std::vector<int64_t> key = {ctx->device,     ctx->natoms,    ctx->npairs, ctx->ncells, ctx->pot.style,
                                       ctx->pot.ntypes, ctx->P,         precision,   grad,        ctx->q5,
-                                      ctx->autotune,   ctx->nblk[0],   ctx->nadjblk[0]};
+                                      ctx->autotune,   ctx->nblk[0],   ctx->nadjblk[0], ctx->fm_mode};
     bool cached = false;
     {
       std::lock_guard<std::mutex> lk(g_tune_mu);
@@ -567,6 +766,7 @@ void tune_variant(mz_ctx *ctx, int n, const double *d_params, int precision, boo
         cached = true;
       }
     }
+    if (cached && t.fm && !fm_prepare(ctx)) t.fm = false;
     if (!cached) {
       mz_ctx::Tune best;
       best.ctas = adj_ctas_for(ctx, 0, ctx->adj_per_sm);
@@ -619,6 +819,26 @@ void tune_variant(mz_ctx *ctx, int n, const double *d_params, int precision, boo
           }
         }
         ctx->launches = l0;  // trials are not the caller's launches
+      }
+      // mixed meam/spline: the triplet-moment path, against the row kernels'
+      // best (whole call), or always with MZ_FM=2
+      if (precision == MZ_MIXED && ctx->fm.eligible && ctx->fm_mode > 0 &&
+          (ctx->fm_mode == 2 || ctx->autotune == 1) && fm_prepare(ctx)) {
+        if (ctx->fm_mode == 2) {
+          best.fm = true;
+        } else {
+          const int64_t l0 = ctx->launches;
+          mz_ctx::Tune c = best;
+          apply_variant(ctx, c);
+          trial(ctx, n, d_params, precision, grad, -1);
+          const double t_rows = trial(ctx, n, d_params, precision, grad, -1);
+          c.fm = true;
+          apply_variant(ctx, c);
+          trial(ctx, n, d_params, precision, grad, -1);
+          const double t_fm = trial(ctx, n, d_params, precision, grad, -1);
+          best.fm = t_fm < t_rows;
+          ctx->launches = l0;
+        }
       }
       best.done = true;
       t = best;
@@ -929,6 +1149,46 @@ mz_status mz_create(const mz_db *dbh, const mz_pot *poth, const mz_settings *set
       d.adj_amax = ctx->adjamax[0];
       // FP64 adjoint groups: at most about 1024 partials per candidate
       d.adj_group = std::max(1, ctx->nadjblk[0] / 1024);
+
+      // ---- triplet-moment path (mixed meam/spline): shape, feature slots
+      // (the type-sorted rows, each type's run padded to FM_TILE)
+      if (pot.style == MZ_STYLE_MEAM_SPLINE && !(ns > 0 && pot.spline(0).quintic) && pot.ntypes <= FM_MAXT) {
+        int NA = 0, NN = 0, PB = 0;
+        for (int t = 0; t < dp.npair; ++t) NA = std::max(NA, pot.spline(dp.s_f + t).nknots + 2);
+        for (int t = 0; t < pot.ntypes; ++t) NN = std::max(NN, pot.spline(dp.s_g + t).nknots + 2);
+        for (int s = 0; s < ns; ++s)
+          if (s < dp.s_U || s >= dp.s_f) PB = std::max(PB, pot.spline(s).nknots + 2);
+        if (pot.ntypes * NA <= 32 && NN <= FM_MAXN && PB <= 23 && db.max_row <= BLOCK_SLOTS) {
+          FmPlan &fp = ctx->fm.plan;
+          fp.nt = pot.ntypes;
+          fp.NA = NA;
+          fp.NN = NN;
+          fp.D = pot.ntypes * NA * NN;
+          fp.Dpad = (fp.D + FM_DC - 1) / FM_DC * FM_DC;
+          fp.nch = fp.Dpad / FM_DC;
+          std::vector<int> row0(N, 0);
+          int64_t q = 0;
+          int tix = 0;
+          for (int t = 0; t < pot.ntypes; ++t) {
+            fp.tile0[t] = (int)(q / FM_TILE);
+            for (; tix < N && db.atom_type[order[tix]] == t; ++tix) {
+              const int i = order[tix];
+              row0[i] = (int)q;
+              q += db.pair_off[i + 1] - db.pair_off[i];
+            }
+            q = (q + FM_TILE - 1) / FM_TILE * FM_TILE;
+          }
+          fp.Q = q;
+          fp.ntiles = (int)(q / FM_TILE);
+          for (int t = pot.ntypes; t <= FM_MAXT; ++t) fp.tile0[t] = fp.ntiles;
+          if (q < (int64_t(1) << 31) && tix == N) {
+            fp.row0 = dupload(ctx, row0.data(), row0.size());
+            fp.nblk = ctx->nadjblk[0];
+            fp.blk0 = ctx->d_adjblk[0];
+            ctx->fm.eligible = true;
+          }
+        }
+      }
     }
 
     // ---- shared memory of the kernels
@@ -1014,6 +1274,10 @@ mz_status mz_create(const mz_db *dbh, const mz_pot *poth, const mz_settings *set
     {
       const char *env = std::getenv("MZ_ADJ_CTAS");
       ctx->adj_ctas_force = env ? std::max(0, std::atoi(env)) : 0;
+    }
+    {
+      const char *env = std::getenv("MZ_FM");
+      ctx->fm_mode = (env && env[0] == '0') ? 0 : (env && env[0] == '2') ? 2 : 1;
     }
     // tensor-core forward (mixed precision, MEAM with TC_NB B-spline coefficients per g spline)
     {
@@ -1145,8 +1409,9 @@ mz_status mz_sync(mz_ctx *ctx) {
 void *mz_stream(mz_ctx *ctx) { return ctx ? (void *)ctx->stream : nullptr; }
 
 const char *mz_kernel_name(int k) {
-  static const char *names[MZ_NKERNELS] = {"k_prep", "k_atoms", "k_gather", "k_cells",
-                                           "k_final", "k_adj", "k_grad_final"};
+  static const char *names[MZ_NKERNELS] = {"k_prep",   "k_atoms",      "k_gather",  "k_cells",  "k_final",
+                                           "k_adj",    "k_grad_final", "k_fm_coef", "k_fm_fwd", "k_fm_epi",
+                                           "k_fm_pre", "k_fm_adj",     "k_fm_grad"};
   return (k >= 0 && k < MZ_NKERNELS) ? names[k] : "?";
 }
 
@@ -1159,6 +1424,14 @@ mz_status mz_tuning(mz_ctx *ctx, int precision, int grad, int *choice) {
     choice[2] = t.done ? t.ctas : 0;
     choice[3] = t.done ? t.nc : 0;
     choice[4] = t.done ? t.adj_nc : 0;
+  });
+}
+
+mz_status mz_moment_path(const mz_ctx *ctx, int precision, int grad, int *on) {
+  return guarded([&] {
+    if (!ctx || !on || (precision != MZ_FP64 && precision != MZ_MIXED)) throw Failure{MZ_ERR_ARG, "bad argument"};
+    const mz_ctx::Tune &t = ctx->tune[precision][grad ? 1 : 0];
+    *on = (t.done && t.fm && ctx->fm.ready) ? 1 : 0;
   });
 }
 

@@ -340,8 +340,18 @@ class Evaluator:
         adjoint candidates per CTA (zeros before the first such call)."""
         c = np.zeros(5, dtype=np.int32)
         check(lib().mz_tuning(self._h, int(precision), 1 if grad else 0, ptr(c)))
+        on = C.c_int()
+        check(lib().mz_moment_path(self._h, int(precision), 1 if grad else 0, C.byref(on)))
         return dict(forward_block_slots=int(c[0]), adjoint_block_slots=int(c[1]), adjoint_ctas=int(c[2]),
-                    forward_candidates_per_cta=int(c[3]), adjoint_candidates_per_cta=int(c[4]))
+                    forward_candidates_per_cta=int(c[3]), adjoint_candidates_per_cta=int(c[4]),
+                    triplet_moments=bool(on.value))
+
+    def moment_path(self, precision=MZ_MIXED, grad=True) -> bool:
+        """True when the tuned (precision, gradient) launches run the
+        triplet-moment path (mixed-precision meam/spline)."""
+        on = C.c_int()
+        check(lib().mz_moment_path(self._h, int(precision), 1 if grad else 0, C.byref(on)))
+        return bool(on.value)
 
     def launches(self) -> int:
         n = C.c_int64()
