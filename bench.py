@@ -150,12 +150,86 @@ def build_workload(args, device):
 
 
 def algorithmic(stats, ncand, P):
-    """Fixed algorithmic bytes and flops of one batched objective+gradient step
-    (per-pair / per-triplet / per-atom / per-cell figures of the design notes)."""
+    """Fixed algorithmic work of one batched objective+gradient step, counted
+    from the reference's expressions (splint_comb, spline3eq.h:110-122;
+    fast_compute, pot_meam_spline.cpp:152-269): bytes
+    B32 = 20 Np + 4 Nt + 48 N + 112 ncells + ncand (8 + 16 P) (FP32 pair and
+    cosine streams, per-atom forces, per-cell targets and outputs, the
+    candidates' coefficients and gradients) and forward flops
+    145 Np + 111 Nt + 40 N per candidate (pairs: three cubic pieces with
+    slopes and the force terms; triplets: the cosine, one g piece and the
+    density and force terms; atoms: the embedding); the gradient costs two
+    forward passes more."""
     Np, Nt, N, nc = stats["npairs"], stats["ntriplets"], stats["natoms"], stats["ncells"]
     b32 = 20 * Np + 4 * Nt + 48 * N + 112 * nc + ncand * (8 + 8 * P + 8 * P)
     fwd = 145 * Np + 111 * Nt + 40 * N
     return b32, fwd
+
+
+def kernel_algorithmic_flops(name, stats, ncand):
+    """The share of the step's algorithmic flops a kernel carries: the row
+    kernels' forward (k_atoms) and adjoint (k_adj); on the triplet-moment path
+    the contractions carry the triplet terms (forward 111 Nt, adjoint twice
+    that) and the epilogues the pair and atom terms."""
+    Np, Nt, N = stats["npairs"], stats["ntriplets"], stats["natoms"]
+    fwd = 145 * Np + 111 * Nt + 40 * N
+    table = {"k_atoms": fwd, "k_adj": 2 * fwd, "k_fm_fwd": 111 * Nt, "k_fm_adj": 2 * 111 * Nt,
+             "k_fm_epi": 145 * Np + 40 * N, "k_fm_pre": 2 * (145 * Np + 40 * N)}
+    return table.get(name, 0) * ncand
+
+
+def executed_flops(name, stats, ncand, fm_dpad):
+    """Flops a moment contraction executes (one FMA = 2): 2 x 3 Dpad x slots x
+    candidates; None for the other kernels."""
+    if name in ("k_fm_fwd", "k_fm_adj") and fm_dpad:
+        return 2 * 3 * fm_dpad * stats["npairs"] * ncand
+    return None
+
+
+def cpu_model():
+    try:
+        with open("/proc/cpuinfo") as fh:
+            for line in fh:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def row_counts(cell, rcut):
+    """Neighbours of every atom of a periodic cell within rcut over its
+    images (the reference's full list, config.cpp:186-228), counted with a
+    k-d tree -- the reference arm's own count, independent of the evaluator
+    library."""
+    from scipy.spatial import cKDTree
+    L = np.asarray(cell.lattice, dtype=float)
+    pos = np.asarray(cell.pos, dtype=float)
+    vol = abs(np.linalg.det(L))
+    m = [int(math.ceil(rcut / (vol / np.linalg.norm(np.cross(L[(k + 1) % 3], L[(k + 2) % 3]))))) for k in range(3)]
+    shifts = np.array([[i, j, k] for i in range(-m[0], m[0] + 1) for j in range(-m[1], m[1] + 1)
+                       for k in range(-m[2], m[2] + 1)], dtype=float) @ L
+    images = (pos[None, :, :] + shifts[:, None, :]).reshape(-1, 3)
+    return cKDTree(images).query_ball_point(pos, rcut, return_length=True) - 1
+
+
+# Features per kind of the triplet-moment path on this workload: 2 partner
+# types x 12 B-spline coefficients of f (10 knots) x 10 of g (8 knots) = 240.
+FM_DPAD_MEAM2K = 240
+
+# Algorithmic bytes of one launch per kernel (None where not stated): the
+# moment contractions stream the FP32 moments once (4 B x 3 x 240 per slot)
+# plus their candidate-side operand (4 B x 3 per slot-candidate, in and out).
+KERNEL_BYTES = {
+    "k_fm_fwd": lambda st, nc: 4 * 3 * FM_DPAD_MEAM2K * st["npairs"] + 4 * 3 * st["npairs"] * nc,
+    "k_fm_adj": lambda st, nc: 4 * 3 * FM_DPAD_MEAM2K * st["npairs"] + 4 * 3 * st["npairs"] * nc,
+}
+# DRAM bytes per launch measured by ncu (dram__bytes_read.sum + dram__bytes_write.sum) on a smaller
+# case of this workload, scaled by the units a full launch processes (profiles/ holds the captures).
+KERNEL_TRAFFIC = {
+    "k_adj": lambda st, nc: 2480.3e6 / 15.8433e6 * st["npairs"] * nc,
+    "k_atoms": lambda st, nc: 496.0e6 / 3.9608e6 * st["npairs"] * nc,
+}
 
 
 # --------------------------------------------------------- CPU reference arm
@@ -208,13 +282,13 @@ def cpu_reference(spec, cells, stats, P, reps, target_triplets=1.0e7, max_procs=
         sample_trip += t
     subprocess.run(["rm", "-rf", tmp])
     obj_evals = rate / stats["ntriplets"]
-    desc = ("%d concurrent single-thread processes of the reference (-Ofast -march=x86-64-v3), each on a disjoint "
-            "run of cells (%d cells, %.3g triplets in all), %d timed compute() calls each after one warm-up; "
-            "objective evals/s of the full database extrapolated by triplet count; objective+gradient = "
-            "objective + %d forward differences" % (len(procs), samples[-1][1] - samples[0][0], sample_trip,
-                                                     reps, P))
+    desc = ("%d concurrent single-thread processes of the reference (-Ofast -march=x86-64-v3) on %s, each on a "
+            "disjoint run of cells (%d cells, %.3g triplets in all), %d timed compute() calls each after one "
+            "warm-up; objective evals/s of the full database extrapolated by triplet count; objective+gradient = "
+            "objective + %d forward differences" % (len(procs), cpu_model(), samples[-1][1] - samples[0][0],
+                                                     sample_trip, reps, P))
     return {"obj_evals_per_s": obj_evals, "objgrad_evals_per_s": obj_evals / (P + 1), "cores": len(procs),
-            "sample": desc}, None
+            "sample": desc, "cpu": cpu_model()}, None
 
 
 # ------------------------------------------------------------------- arms
@@ -222,15 +296,14 @@ def cpu_reference(spec, cells, stats, P, reps, target_triplets=1.0e7, max_procs=
 def run_reference_arm(args, world, rank):
     if rank != 0:
         return
-    from meamzilla_b200 import synth
-    from meamzilla_b200.potential import Database, PotentialFile
+    from meamzilla_b200 import synth  # the generator only: numpy, no evaluator library
     spec, cells = synth.make_workload("meam2k", seed=args.seed, ncells=args.ncells)
-    pot = PotentialFile.from_spec(spec)
-    db = Database.from_cells(cells, pot)
-    stats = db.stats()
-    v = db.view()
-    stats["rows_per_cell"] = _rows_per_cell(v)
-    P = pot.ncoeff
+    rcut = synth.WORKLOADS["meam2k"][2]
+    rows = [row_counts(c, rcut) for c in cells]
+    stats = {"ncells": len(cells), "natoms": int(sum(c.natoms for c in cells)),
+             "npairs": int(sum(int(r.sum()) for r in rows)),
+             "ntriplets": int(sum(int((r * (r - 1) // 2).sum()) for r in rows)), "rows_per_cell": rows}
+    P = spec_ncoeff(spec)
     t0 = time.time()
     res, err = cpu_reference(spec, cells, stats, P, reps=max(1, args.steps))
     wall = time.time() - t0
@@ -252,6 +325,17 @@ def run_reference_arm(args, world, rank):
         "wall_s": wall,
     }
     print(json.dumps(line))
+
+
+def spec_ncoeff(spec):
+    """Adjustable coefficients of a generated potential: free knots and free
+    end slopes (Potential::get_ncoeff)."""
+    n = 0
+    for grp in spec.groups:
+        for s in grp:
+            fixed = s.fixed if s.fixed is not None else np.zeros(s.nknots, dtype=int)
+            n += int(np.sum(np.asarray(fixed) == 0)) + sum(1 for e in s.bc if e == 0)
+    return n
 
 
 def _rows_per_cell(v):
@@ -288,16 +372,27 @@ def run_mine(args, world, rank, local):
     ev.objective_grad_device(Xd, obj, grad, MZ_MIXED)
     ev.sync()
 
-    # accuracy of the mixed path against FP64 on these candidates
+    # accuracy of the mixed path against FP64: objectives of all candidates,
+    # forces and gradients of ACC_SAMPLE of them (every 64 / ACC_SAMPLE-th)
+    ACC_SAMPLE = 8
     o64 = ev.objective(X, MZ_FP64)
     o32 = ev.objective(X, MZ_MIXED)
-    f64 = ev.objective(X[:1], MZ_FP64, forces=True)["forces"][0]
-    f32 = ev.objective(X[:1], MZ_MIXED, forces=True)["forces"][0]
-    _, g64 = ev.objective_grad(X[:2], MZ_FP64)
-    _, g32 = ev.objective_grad(X[:2], MZ_MIXED)
+    pick = np.arange(0, args.ncand, max(1, args.ncand // ACC_SAMPLE))[:ACC_SAMPLE]
+    ferr, gerr = [], []
+    for c in pick:
+        f64 = ev.objective(X[c:c + 1], MZ_FP64, forces=True)["forces"][0]
+        f32 = ev.objective(X[c:c + 1], MZ_MIXED, forces=True)["forces"][0]
+        ferr.append(float(np.max(np.abs(f32 - f64))))
+    _, g64 = ev.objective_grad(X[pick], MZ_FP64)
+    _, g32 = ev.objective_grad(X[pick], MZ_MIXED)
+    for k in range(len(pick)):
+        gerr.append(float(np.max(np.abs(g32[k] - g64[k])) / np.max(np.abs(g64[k]))))
     accuracy = {"obj_rel_err_max": float(np.max(np.abs(o32 - o64) / np.abs(o64))),
-                "force_err_max_eV_per_A": float(np.max(np.abs(f32 - f64))),
-                "grad_err_max_rel_to_max": float(np.max(np.abs(g32 - g64)) / np.max(np.abs(g64)))}
+                "obj_candidates": int(args.ncand),
+                "force_err_max_eV_per_A": float(max(ferr)),
+                "grad_err_max_rel_to_max": float(max(gerr)),
+                "force_grad_candidates": [int(c) for c in pick],
+                "reference": "the GPU's own FP64 path, itself pinned to the reference at 1e-12"}
 
     def barrier():
         if world > 1:
@@ -396,28 +491,39 @@ def run_mine(args, world, rank, local):
         if world > 1:
             torch.distributed.destroy_process_group()
         return
+    tuned = ev.tuning(MZ_MIXED, True)
 
-    # ---- roofline of the dominant kernel
+    # ---- roofline of the dominant kernel: the binding bound is the FP32
+    # CUDA-core pipe (algorithmic flops of the kernel's share of the step);
+    # HBM beside it with the kernel's own bytes
     hbm, hbm_src = measured_peaks()
     fp32_peak = alu_peak(local, MZ_MIXED)
     fp64_peak = alu_peak(local, MZ_FP64)
     b32, fwd = algorithmic(stats, args.ncand, P)
     dom = max(kt, key=lambda k: kt[k][0])
     dom_ms = kt[dom][0] / kt[dom][1]
-    # flops of the dominant kernel: the forward pass is 1x, the adjoint 2x of the forward count
-    kflops = {"k_atoms": fwd * args.ncand, "k_adj": 2 * fwd * args.ncand}.get(dom, 3 * fwd * args.ncand)
-    # DRAM traffic per launch from ncu (dram__bytes_read.sum + dram__bytes_write.sum) on the 200-cell
-    # case of this workload, 8 candidates, scaled by pair slots x candidates (the full launch is too
-    # large to capture): k_adj 2480.3 MB / 15.84 M slot-candidates; k_atoms 496.0 MB / 3.96 M.
-    per_slot_cand = {"k_adj": 2480.3e6 / 15.8433e6, "k_atoms": 496.0e6 / 3.9608e6}.get(dom)
-    traffic = per_slot_cand * stats["npairs"] * args.ncand if per_slot_cand else None
-    roof = {"bound": "hbm", "kernel": dom, "achieved": b32 / (dom_ms * 1e-3) / 1e9, "peak": hbm, "unit": "GB/s",
-            "frac": b32 / (dom_ms * 1e-3) / 1e9 / hbm, "traffic": traffic, "algorithmic_bytes": b32,
-            "traffic_source": "ncu, 200-cell case scaled by pair slots x candidates",
-            "peak_source": hbm_src}
-    roof_alu = {"bound": "fp32", "kernel": dom, "achieved": kflops / (dom_ms * 1e-3) / 1e12, "peak": fp32_peak,
-                "unit": "TFLOP/s", "frac": kflops / (dom_ms * 1e-3) / 1e12 / fp32_peak, "algorithmic_flops": kflops,
-                "peak_source": "measured FMA stream, FP32 (FP64: %.1f TFLOP/s)" % fp64_peak}
+    kflops = kernel_algorithmic_flops(dom, stats, args.ncand)
+    fm_dpad = FM_DPAD_MEAM2K if tuned.get("triplet_moments") else None
+    xflops = executed_flops(dom, stats, args.ncand, fm_dpad)
+    kbytes = KERNEL_BYTES.get(dom, lambda st, nc: None)(stats, args.ncand)
+    roof = {"bound": "fp32", "kernel": dom, "achieved": kflops / (dom_ms * 1e-3) / 1e12, "peak": fp32_peak,
+            "unit": "TFLOP/s", "frac": kflops / (dom_ms * 1e-3) / 1e12 / fp32_peak, "algorithmic_flops": kflops,
+            "traffic": KERNEL_TRAFFIC.get(dom, lambda st, nc: None)(stats, args.ncand),
+            "peak_source": "measured FMA stream on this GPU, FP32 (FP64: %.1f TFLOP/s)" % fp64_peak,
+            "ms_per_launch": dom_ms}
+    if xflops:
+        roof["executed_flops"] = xflops
+        roof["executed_frac"] = xflops / (dom_ms * 1e-3) / 1e12 / fp32_peak
+    roof_hbm = {"bound": "hbm", "kernel": dom, "algorithmic_bytes": kbytes,
+                "achieved": kbytes / (dom_ms * 1e-3) / 1e9 if kbytes else None, "peak": hbm, "unit": "GB/s",
+                "frac": kbytes / (dom_ms * 1e-3) / 1e9 / hbm if kbytes else None, "peak_source": hbm_src}
+    step_flops = 3 * fwd * args.ncand
+    roof_step = {"algorithmic_flops": step_flops, "achieved_tflops": step_flops / (ms / args.steps * 1e-3) / 1e12,
+                 "frac_fp32": step_flops / (ms / args.steps * 1e-3) / 1e12 / fp32_peak,
+                 "algorithmic_bytes": b32}
+    roof_fp64 = {"bound": "fp64", "achieved": fwd / (ms64 / k64 * 1e-3) / 1e12, "peak": fp64_peak,
+                 "unit": "TFLOP/s", "frac": fwd / (ms64 / k64 * 1e-3) / 1e12 / fp64_peak,
+                 "algorithmic_flops": fwd}
 
     line = {
         "metric": METRIC, "value": value, "unit": "evals/s", "n_gpus": world, "steps": args.steps,
@@ -427,7 +533,7 @@ def run_mine(args, world, rank, local):
                    "npairs": stats["npairs"], "ntriplets": stats["ntriplets"], "ncoeff": P,
                    "candidates_per_step_per_gpu": args.ncand, "precision": "mixed (FP32 splines, FP64 sums)",
                    "l2": "inputs larger than L2: pair streams %.2f GB" % (stats["npairs"] * 36 / 1e9),
-                   "autotuned": ev.tuning(MZ_MIXED, True)},
+                   "autotuned": tuned},
         "fp64_plain": {"value": fp64_rate, "unit": "objective evals/s", "ms_per_eval": ms64 / k64,
                        "candidates_per_launch": 1},
         "ratio_vs_fp64_plain": value / fp64_rate,
@@ -435,7 +541,9 @@ def run_mine(args, world, rank, local):
         "accuracy_vs_fp64": accuracy,
         "kernels_ms_per_step": {k: kt[k][0] / args.steps for k in kt},
         "roofline": roof,
-        "roofline_alu": roof_alu,
+        "roofline_hbm": roof_hbm,
+        "roofline_step": roof_step,
+        "roofline_fp64_plain": roof_fp64,
         "e2e": {"value": e2e, "unit": "evals/s", "h2d_bytes_per_step": args.ncand * P * 8,
                 "d2h_bytes_per_step": args.ncand * (P + 1) * 8},
         "gpu_launches": launches,
@@ -446,8 +554,14 @@ def run_mine(args, world, rank, local):
         res, err = cpu_reference(spec, cells, stats, P, reps=3)
         if res is not None:
             line["cpu_baseline"] = {"value": res["objgrad_evals_per_s"], "unit": "evals/s", "cores": res["cores"],
-                                    "kind": "reference", "sample": res["sample"],
+                                    "kind": "reference", "sample": res["sample"], "cpu": res["cpu"],
                                     "objective_evals_per_s": res["obj_evals_per_s"]}
+            # measured against measured: objective evaluations, FP64 GPU (one candidate per launch)
+            # and mixed batched, over the reference's objective on the host cores
+            line["vs_reference_objective"] = {
+                "fp64_plain_over_cpu": fp64_rate / res["obj_evals_per_s"],
+                "mixed_batched_over_cpu": batched["mixed_evals_per_s"] / res["obj_evals_per_s"],
+                "objgrad_over_modelled_cpu_objgrad": value / res["objgrad_evals_per_s"]}
         else:
             line["cpu_baseline"] = {"value": None, "unavailable": err}
     print(json.dumps(line))
