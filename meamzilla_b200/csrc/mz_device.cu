@@ -338,13 +338,13 @@ bool fm_prepare(mz_ctx *ctx) {
     size_t have_bytes, need_bytes;
   };
   Need need[] = {
-      {ctx->d_aux, sizeof(double) * C * aux_rows * Np, sizeof(float) * G * Q * 3 * CG},        // Y
+      {ctx->d_aux, sizeof(double) * C * aux_rows * Np, (sizeof(double) + sizeof(float)) * G * Q * 3 * CG},  // Y, Yb
       {ctx->d_V, sizeof(double) * C * 3 * Np, sizeof(double) * Cp * Np * 3},                   // V
       {ctx->d_aout, sizeof(double) * C * AO_COUNT * N, sizeof(double) * Cp * AO_COUNT * N},    // aoutF
       {ctx->d_lam, sizeof(double) * C * 3 * N, sizeof(float) * Cp * 3 * N},                    // lamf
       {ctx->d_seeds, sizeof(double) * C * CS_COUNT * NC, sizeof(double) * Cp * CS_COUNT * NC}, // seedF
   };
-  size_t extra = sizeof(float) * (3 * (size_t)fp.Dpad * Q + 8 * Q) + sizeof(float) * G * fp.nt * fp.Dpad * CG +
+  size_t extra = sizeof(float) * 3 * (size_t)fp.Dpad * Q + sizeof(double) * 8 * Q + sizeof(float) * G * fp.nt * fp.Dpad * CG +
                  sizeof(double) * C * ns * FM_MAXB + sizeof(float) * G * ns * FM_MAXB * CG +
                  sizeof(double) * G * CG *
                      ((size_t)fp.nctas_adj * fp.nt * fp.Dpad + (size_t)fp.nctas_pre * (ns * FM_MAXB + stride));
@@ -359,13 +359,14 @@ bool fm_prepare(mz_ctx *ctx) {
   auto pick = [&](Need &x) -> void * {
     return x.need_bytes <= x.have_bytes ? x.have : (void *)dalloc<unsigned char>(ctx, x.need_bytes);
   };
-  fp.Y = static_cast<float *>(pick(need[0]));
+  fp.Y = static_cast<double *>(pick(need[0]));
+  fp.Yb = reinterpret_cast<float *>(fp.Y + G * Q * 3 * CG);
   fp.V = static_cast<double *>(pick(need[1]));
   fp.aoutF = static_cast<double *>(pick(need[2]));
   fp.lamf = static_cast<float *>(pick(need[3]));
   fp.seedF = static_cast<double *>(pick(need[4]));
   float *X = dalloc<float>(ctx, 3 * (size_t)fp.Dpad * Q);
-  float *E = dalloc<float>(ctx, 8 * Q);
+  double *E = dalloc<double>(ctx, 8 * Q);
   fp.X = X;
   fp.E = E;
   fp.Kf = dalloc<float>(ctx, G * fp.nt * fp.Dpad * CG);
@@ -377,7 +378,7 @@ bool fm_prepare(mz_ctx *ctx) {
   fp.Pbar = dalloc<double>(ctx, G * fp.nctas_pre * ns * FM_MAXB * CG);
   fp.Tbar = dalloc<double>(ctx, G * fp.nctas_pre * CG * stride);
   ck(cudaMemsetAsync(X, 0, sizeof(float) * 3 * (size_t)fp.Dpad * Q, ctx->stream), "memset");
-  ck(cudaMemsetAsync(E, 0, sizeof(float) * 8 * Q, ctx->stream), "memset");
+  ck(cudaMemsetAsync(E, 0, sizeof(double) * 8 * Q, ctx->stream), "memset");
   ck(cudaMemsetAsync(coef64, 0, sizeof(double) * C * ns * FM_MAXB, ctx->stream), "memset");
   ck(cudaMemsetAsync(coef32, 0, sizeof(float) * G * ns * FM_MAXB * CG, ctx->stream), "memset");
   fp.CG = fm.CGmax;
@@ -388,8 +389,9 @@ bool fm_prepare(mz_ctx *ctx) {
   smem_attr(k_fm_gemm_fwd<2>, fm_fwd_smem<2>(fp.Dpad));
   smem_attr(k_fm_gemm_fwd<4>, fm_fwd_smem<4>(fp.Dpad));
   smem_attr(k_fm_gemm_fwd<8>, fm_fwd_smem<8>(fp.Dpad));
-  fm.smem_pre = fm_pre_smem(ctx->nsplines);
+  fm.smem_pre = fm_pre_smem(ctx->nsplines, 64, fp.nt, fp.NB, 256);
   smem_attr(k_fm_adj_pre, fm.smem_pre);
+  smem_attr(k_fm_epi, fm_epi_smem(ctx->nsplines, fp.nt, fp.NB, 64));
   smem_attr(k_fm_gemm_adj, fm_adj_smem(fp.Dpad, 64));
   fm.ready = true;
   return true;
@@ -431,7 +433,9 @@ void enqueue_fm(mz_ctx *ctx, int n, double *d_obj, double *d_errvec, double *d_f
   const unsigned ablocks = (unsigned)(((int64_t)N * CG + 255) / 256);
   {
     Bracket b(ctx, MZ_K_FM_EPI);
-    k_fm_epi<<<dim3(ablocks, G), 256, 0, st>>>(ctx->db, ctx->pot, ctx->d_geom, ctx->d_tabs, fp, n);
+    const int eb = std::max(1, std::min(fp.nblk, 4 * ctx->nsm));
+    k_fm_epi<<<dim3(eb, G), 256, fm_epi_smem(ns, fp.nt, fp.NB, CG), st>>>(ctx->db, ctx->pot, ctx->d_geom,
+                                                                         ctx->d_tabs, fp, n);
     ck(cudaGetLastError(), "k_fm_epi launch");
   }
   {
@@ -455,8 +459,8 @@ void enqueue_fm(mz_ctx *ctx, int n, double *d_obj, double *d_errvec, double *d_f
   if (!grad) return;
   {
     Bracket b(ctx, MZ_K_FM_PRE);
-    k_fm_adj_pre<<<dim3(fp.nctas_pre, G), 256, ctx->fm.smem_pre, st>>>(ctx->db, ctx->pot, ctx->d_geom, ctx->d_tabs,
-                                                                       fp, n);
+    k_fm_adj_pre<<<dim3(fp.nctas_pre, G), 256, fm_pre_smem(ns, CG, fp.nt, fp.NB, 256), st>>>(
+        ctx->db, ctx->pot, ctx->d_geom, ctx->d_tabs, fp, n);
     ck(cudaGetLastError(), "k_fm_adj_pre launch");
   }
   {
@@ -1153,16 +1157,19 @@ mz_status mz_create(const mz_db *dbh, const mz_pot *poth, const mz_settings *set
       // ---- triplet-moment path (mixed meam/spline): shape, feature slots
       // (the type-sorted rows, each type's run padded to FM_TILE)
       if (pot.style == MZ_STYLE_MEAM_SPLINE && !(ns > 0 && pot.spline(0).quintic) && pot.ntypes <= FM_MAXT) {
-        int NA = 0, NN = 0, PB = 0;
+        int NA = 0, NN = 0, PB = 0, NBp = 0;
         for (int t = 0; t < dp.npair; ++t) NA = std::max(NA, pot.spline(dp.s_f + t).nknots + 2);
         for (int t = 0; t < pot.ntypes; ++t) NN = std::max(NN, pot.spline(dp.s_g + t).nknots + 2);
         for (int s = 0; s < ns; ++s)
           if (s < dp.s_U || s >= dp.s_f) PB = std::max(PB, pot.spline(s).nknots + 2);
+        for (int s = 0; s < dp.s_g; ++s)
+          if (s < dp.s_U || s >= dp.s_f) NBp = std::max(NBp, pot.spline(s).nknots + 2);
         if (pot.ntypes * NA <= 32 && NN <= FM_MAXN && PB <= 23 && db.max_row <= BLOCK_SLOTS) {
           FmPlan &fp = ctx->fm.plan;
           fp.nt = pot.ntypes;
           fp.NA = NA;
           fp.NN = NN;
+          fp.NB = NBp;
           fp.D = pot.ntypes * NA * NN;
           fp.Dpad = (fp.D + FM_DC - 1) / FM_DC * FM_DC;
           fp.nch = fp.Dpad / FM_DC;

@@ -28,9 +28,9 @@
 // Layouts (feature slots q: the atoms in type-sorted order, each row
 // contiguous, each type's run padded to a multiple of FM_TILE):
 //   X     [nch][3][FM_DC][Q]         moments, FM_DC features per chunk
-//   E     [Q][8]                     e1, e2 of the slot (FP32)
-//   Y     [ngroups][Q][3][CG]        G, Y1, Y2; the adjoint overwrites them with
-//                                    dL/dG, dL/dY1, dL/dY2
+//   E     [Q][8]                     e1, e2 of the slot (FP64)
+//   Y     [ngroups][Q][3][CG]        G, Y1, Y2 (FP64)
+//   Yb    [ngroups][Q][3][CG]        dL/dG, dL/dY1, dL/dY2 (FP32)
 //   V     [ngroups][Np][CG][3]       reaction vectors (FP64), global slot order
 //   aoutF [ngroups][N][AO_COUNT][CG] per-atom outputs (FP64)
 // with candidates in groups of CG (the launch's candidates rounded up to a
@@ -41,7 +41,7 @@
 
 namespace mzb {
 
-constexpr int FM_TILE = 128;   // feature slots per contraction tile
+constexpr int FM_TILE = 64;    // feature slots per contraction tile
 constexpr int FM_DC = 24;      // features per chunk of the forward contraction
 constexpr int FM_MAXT = 2;     // atom types
 constexpr int FM_MAXN = 16;    // B-spline coefficients of a g spline (knots + 2)
@@ -59,12 +59,14 @@ struct FmPlan {
   int64_t Q;       // feature slots
   int ntiles;      // Q / FM_TILE
   int tile0[FM_MAXT + 1];  // first tile of each type
+  int NB;          // B-spline coefficients of the phi, rho and f splines (the largest)
   int nblk;        // atom blocks of the adjoint epilogue (type-pure, <= 256 slots, <= 64 atoms)
   const int *blk0;         // [nblk + 1] into adj_atoms
   const int *row0;         // [N] feature slot of each atom's first pair
   const float *X;
-  const float *E;
-  float *Y;
+  const double *E;         // [Q][8] e1, e2 of each slot (FP64)
+  double *Y;               // [ngroups][Q][3][CG] G, Y1, Y2 (FP64 sums of the contraction)
+  float *Yb;               // [ngroups][Q][3][CG] dL/dG, dL/dY1, dL/dY2 (FP32, the adjoint's operand)
   const float *Kf;         // [ngroups][nt][Dpad][CG]
   const double *coef64;    // [ncand][nsplines][FM_MAXB]
   const float *coef32;     // [ngroups][nsplines][FM_MAXB][CG]
@@ -142,7 +144,7 @@ __device__ __forceinline__ int fm_tile_type(const FmPlan &fp, int tile) {
 // kernels take them: every other slot of the row whose cosine is below g's
 // cut (triplet_meam_spline.cpp:65-70), the g interval by g_knot.
 __global__ void __launch_bounds__(256) k_fm_features(DevDb db, DevPot pot, const SplineGeom *__restrict__ geom,
-                                                     FmPlan fp, float *__restrict__ X, float *__restrict__ E) {
+                                                     FmPlan fp, float *__restrict__ X, double *__restrict__ E) {
   __shared__ double su[3][BLOCK_SLOTS], sbf[BLOCK_SLOTS];
   __shared__ int so[BLOCK_SLOTS], skf[BLOCK_SLOTS];
   const int i = db.adj_atoms[blockIdx.x];
@@ -220,10 +222,10 @@ __global__ void __launch_bounds__(256) k_fm_features(DevDb db, DevPot pot, const
           }
     }
     if (lane == 0) {
-      float *e = E + (size_t)q * 8;
-      e[0] = (float)e1[0]; e[1] = (float)e1[1]; e[2] = (float)e1[2];
-      e[3] = (float)e2[0]; e[4] = (float)e2[1]; e[5] = (float)e2[2];
-      e[6] = 0.f; e[7] = 0.f;
+      double *e = E + (size_t)q * 8;
+      e[0] = e1[0]; e[1] = e1[1]; e[2] = e1[2];
+      e[3] = e2[0]; e[4] = e2[1]; e[5] = e2[2];
+      e[6] = 0.0; e[7] = 0.0;
     }
   }
 }
@@ -281,10 +283,11 @@ __global__ void k_fm_kmat(int ncand, DevPot pot, FmPlan fp, const double *__rest
 
 // Y[q][t][c] = sum_d X[t][d][q] K_s[d][c] over one tile of FM_TILE feature
 // slots (one atom type s) and one group of CG = 8 NW candidates.  Thread
-// (lane, warp): slots 4 lane .. 4 lane + 3, candidates 8 warp .. 8 warp + 7,
-// all three kinds -- 96 FP32 sums as packed pairs of slots.  The moments are
-// streamed in chunks of FM_DC features through a double buffer filled by
-// cp.async; K_s stays in shared memory for the whole tile.
+// (lane, warp): slots 2 lane and 2 lane + 1, candidates 8 warp .. 8 warp + 7,
+// all three kinds.  Each chunk of FM_DC features is summed in FP32 (packed
+// pairs of slots) and added to FP64 totals, which are stored in FP64, so a
+// sum carries the rounding of FM_DC terms, not of all Dpad.  The moments stream through a double buffer
+// filled by cp.async; K_s stays in shared memory for the whole tile.
 template <int NW>
 __host__ __device__ constexpr size_t fm_fwd_smem(int Dpad) {
   return sizeof(float) * ((size_t)Dpad * NW * 8 + 2 * 3 * FM_DC * FM_TILE);
@@ -312,13 +315,13 @@ __global__ void __launch_bounds__(NW * 32, 1) k_fm_gemm_fwd(FmPlan fp) {
     cp_async_commit();
   };
   load_chunk(0, 0);
-  float2 acc[3][2][8];  // [kind][slot pair][candidate]: (slot 2 sp, slot 2 sp + 1)
+  double tot[3][2][8];  // [kind][slot][candidate]
 #pragma unroll
   for (int t = 0; t < 3; ++t)
 #pragma unroll
-    for (int sp = 0; sp < 2; ++sp)
+    for (int h = 0; h < 2; ++h)
 #pragma unroll
-      for (int c = 0; c < 8; ++c) acc[t][sp][c] = make_float2(0.f, 0.f);
+      for (int c = 0; c < 8; ++c) tot[t][h][c] = 0.0;
   for (int ch = 0; ch < fp.nch; ++ch) {
     if (ch + 1 < fp.nch) {
       load_chunk(ch + 1, (ch + 1) & 1);
@@ -327,195 +330,276 @@ __global__ void __launch_bounds__(NW * 32, 1) k_fm_gemm_fwd(FmPlan fp) {
       cp_async_wait<0>();
     }
     __syncthreads();
-    const float *xb = Xs + (size_t)(ch & 1) * 3 * FM_DC * FM_TILE + 4 * lane;
+    const float *xb = Xs + (size_t)(ch & 1) * 3 * FM_DC * FM_TILE + 2 * lane;
     const float *kb = Ks + (size_t)ch * FM_DC * CG + warp * 8;
-#pragma unroll 2
+    float2 acc[3][8];  // this chunk, (slot 2 lane, slot 2 lane + 1)
+#pragma unroll
+    for (int t = 0; t < 3; ++t)
+#pragma unroll
+      for (int c = 0; c < 8; ++c) acc[t][c] = make_float2(0.f, 0.f);
+#pragma unroll 4
     for (int din = 0; din < FM_DC; ++din) {
       const float4 k0 = *reinterpret_cast<const float4 *>(kb + din * CG);
       const float4 k1 = *reinterpret_cast<const float4 *>(kb + din * CG + 4);
       const float kk[8] = {k0.x, k0.y, k0.z, k0.w, k1.x, k1.y, k1.z, k1.w};
 #pragma unroll
       for (int t = 0; t < 3; ++t) {
-        const float4 xv = *reinterpret_cast<const float4 *>(xb + (t * FM_DC + din) * FM_TILE);
-        const float2 x01 = make_float2(xv.x, xv.y), x23 = make_float2(xv.z, xv.w);
+        const float2 xv = *reinterpret_cast<const float2 *>(xb + (t * FM_DC + din) * FM_TILE);
 #pragma unroll
-        for (int c = 0; c < 8; ++c) {
-          const float2 kc = bcast2(kk[c]);
-          acc[t][0][c] = fma2(x01, kc, acc[t][0][c]);
-          acc[t][1][c] = fma2(x23, kc, acc[t][1][c]);
-        }
+        for (int c = 0; c < 8; ++c) acc[t][c] = fma2(xv, bcast2(kk[c]), acc[t][c]);
       }
     }
+#pragma unroll
+    for (int t = 0; t < 3; ++t)
+#pragma unroll
+      for (int c = 0; c < 8; ++c) {
+        tot[t][0][c] += (double)acc[t][c].x;
+        tot[t][1][c] += (double)acc[t][c].y;
+      }
     __syncthreads();
   }
-  float *Yb = fp.Y + ((size_t)gy * fp.Q + qb + 4 * lane) * 3 * CG + warp * 8;
+  double *Yo = fp.Y + ((size_t)gy * fp.Q + qb + 2 * lane) * 3 * CG + warp * 8;
 #pragma unroll
-  for (int sl = 0; sl < 4; ++sl)
+  for (int h = 0; h < 2; ++h)
 #pragma unroll
     for (int t = 0; t < 3; ++t) {
-      float v[8];
+      double *dst = Yo + ((size_t)h * 3 + t) * CG;
 #pragma unroll
-      for (int c = 0; c < 8; ++c) v[c] = (sl & 1) ? acc[t][sl >> 1][c].y : acc[t][sl >> 1][c].x;
-      float *dst = Yb + ((size_t)sl * 3 + t) * CG;
-      *reinterpret_cast<float4 *>(dst) = make_float4(v[0], v[1], v[2], v[3]);
-      *reinterpret_cast<float4 *>(dst + 4) = make_float4(v[4], v[5], v[6], v[7]);
+      for (int c = 0; c < 8; c += 2)
+        *reinterpret_cast<double2 *>(dst + c) = make_double2(tot[t][h][c], tot[t][h][c + 1]);
     }
 }
 
-// ------------------------------------------------------ per-slot helpers
+// ------------------------------------------------------ block staging
 
-// One pair function (FP32) of a slot from the candidate's B-spline
-// coefficients: value and d/dr.
-__device__ __forceinline__ float fm_pair_val(const float *coef, int CG, int k, float b, float inv, float &d) {
-  float N[4], Nd[4];
-  bsp_basis<float>(b, N);
-  bsp_dbasis<float>(b, Nd);
-  const float c0 = coef[(size_t)k * CG], c1 = coef[(size_t)(k + 1) * CG], c2 = coef[(size_t)(k + 2) * CG],
-              c3 = coef[(size_t)(k + 3) * CG];
-  d = (Nd[0] * c0 + Nd[1] * c1 + Nd[2] * c2 + Nd[3] * c3) * inv;
-  return N[0] * c0 + N[1] * c1 + N[2] * c2 + N[3] * c3;
-}
+// The epilogues walk the type-pure atom blocks (at most BLOCK_SLOTS slots
+// and FM_ABLK atoms).  Everything of a block that does not depend on the
+// candidate is staged once in shared memory: per slot its global index,
+// neighbour, neighbour type, knots, the FP32 unit vector and 1/r, the FP64
+// frame (e1, e2), and the B-spline basis values (and d/dr) of phi, rho and f
+// at its shifts; and the pair splines' B-spline coefficients of the block's
+// atom type for the group's candidates.
+constexpr int FM_ABLK = 64;  // atoms per block of the epilogues
 
-struct FmSlot {
-  int64_t gs;
-  int j, tj, pij;
-  float ux, uy, uz, r, invr;
-  int kphi, krho, kf;
-  float bphi, brho, bf;
+struct FmStage {
+  int *satom, *arow;  // [FM_ABLK], [FM_ABLK + 1]
+  int *gs, *nbr, *tj, *kn;  // [BLOCK_SLOTS]
+  float4 *uf;         // [BLOCK_SLOTS] (ux, uy, uz, 1/r)
+  double *e;          // [BLOCK_SLOTS][6] e1, e2
+  float *bas;         // [BLOCK_SLOTS][3][8] basis N0..N3 and d/dr N0'..N3' of phi, rho, f
+  float *coef;        // [3][nt][NB][CG]
 };
 
-__device__ __forceinline__ FmSlot fm_slot(const DevDb &db, const DevPot &pot, int64_t gs, int ti) {
-  FmSlot s;
-  s.gs = gs;
-  const int64_t Np = db.npairs;
-  s.j = db.pair_nbr[gs];
-  s.tj = db.atom_type[s.j];
-  s.pij = pair_ij_index(ti, s.tj, pot.ntypes);
-  s.ux = db.pair_uxf[gs];
-  s.uy = db.pair_uyf[gs];
-  s.uz = db.pair_uzf[gs];
-  s.r = db.pair_rf[gs];
-  s.invr = 1.f / s.r;
-  const int kn = db.pair_knot[gs];
-  s.kphi = (kn & 0xff) - 1;
-  s.krho = ((kn >> 8) & 0xff) - 1;
-  s.kf = ((kn >> 16) & 0xff) - 1;
-  s.bphi = db.pair_shiftf[gs];
-  s.brho = db.pair_shiftf[Np + gs];
-  s.bf = db.pair_shiftf[2 * Np + gs];
-  return s;
+__host__ __device__ inline size_t fm_stage_bytes(int nt, int NB, int CG) {
+  return sizeof(int) * (2 * FM_ABLK + 1 + 4 * BLOCK_SLOTS) + 16 + sizeof(float4) * BLOCK_SLOTS +
+         sizeof(double) * 6 * BLOCK_SLOTS + sizeof(float) * 24 * BLOCK_SLOTS + sizeof(float) * 3 * nt * NB * CG;
 }
 
-// phi, rho, f (values and slopes) of a slot for candidate cl of the group
+// carves the staging arrays out of shared memory at `base` (16-byte aligned)
+__device__ __forceinline__ FmStage fm_stage_carve(unsigned char *base, const FmPlan &fp) {
+  FmStage st;
+  double *e = reinterpret_cast<double *>(base);
+  st.e = e;
+  float4 *uf = reinterpret_cast<float4 *>(e + 6 * BLOCK_SLOTS);
+  st.uf = uf;
+  float *bas = reinterpret_cast<float *>(uf + BLOCK_SLOTS);
+  st.bas = bas;
+  float *coef = bas + 24 * BLOCK_SLOTS;
+  st.coef = coef;
+  int *ip = reinterpret_cast<int *>(coef + 3 * fp.nt * fp.NB * fp.CG);
+  st.satom = ip;
+  st.arow = ip + FM_ABLK;
+  st.gs = st.arow + FM_ABLK + 1;
+  st.nbr = st.gs + BLOCK_SLOTS;
+  st.tj = st.nbr + BLOCK_SLOTS;
+  st.kn = st.tj + BLOCK_SLOTS;
+  return st;
+}
+
+// The spline of pair function F (0 phi, 1 rho, 2 f) for a centre of type ti
+// and a neighbour of type tj.
+__device__ __forceinline__ int fm_pair_spline(const DevPot &pot, int F, int ti, int tj) {
+  return F == 1 ? pot.s_rho + tj : (F == 0 ? pot.s_phi : pot.s_f) + pair_ij_index(ti, tj, pot.ntypes);
+}
+
+// Stages block blk; returns its slot count (all threads; barriers inside).
+__device__ int fm_stage_block(const DevDb &db, const DevPot &pot, const SplineGeom *sg, const FmPlan &fp,
+                              const FmStage &st, int blk, int gy, int &na_out, int &ti_out) {
+  const int tid = threadIdx.x, T = blockDim.x, CG = fp.CG;
+  const int a0 = fp.blk0[blk], na = fp.blk0[blk + 1] - a0;
+  __syncthreads();  // the previous block is done with the staging
+  if (tid < na) st.satom[tid] = db.adj_atoms[a0 + tid];
+  __syncthreads();
+  if (tid == 0) {
+    int lo = 0;
+    for (int a = 0; a < na; ++a) {
+      st.arow[a] = lo;
+      lo += db.pair_off[st.satom[a] + 1] - db.pair_off[st.satom[a]];
+    }
+    st.arow[na] = lo;
+  }
+  __syncthreads();
+  const int nslot = st.arow[na];
+  const int ti = db.atom_type[st.satom[0]];
+  const int64_t Np = db.npairs;
+  for (int ql = tid; ql < nslot; ql += T) {
+    const int a = slot_owner(st.arow, na, ql);
+    const int i = st.satom[a], p = ql - st.arow[a];
+    const int64_t gs = db.pair_off[i] + p;
+    const int j = db.pair_nbr[gs];
+    st.gs[ql] = (int)gs;
+    st.nbr[ql] = j;
+    const int tj = db.atom_type[j];
+    st.tj[ql] = tj;
+    const int kn = db.pair_knot[gs];
+    st.kn[ql] = kn;
+    st.uf[ql] = make_float4(db.pair_uxf[gs], db.pair_uyf[gs], db.pair_uzf[gs], 1.f / db.pair_rf[gs]);
+    const double *e = fp.E + (size_t)(fp.row0[i] + p) * 8;
+#pragma unroll
+    for (int k = 0; k < 6; ++k) st.e[ql * 6 + k] = e[k];
+#pragma unroll
+    for (int F = 0; F < 3; ++F) {
+      const int k = ((kn >> (8 * F)) & 0xff) - 1;
+      float *bs = st.bas + (ql * 3 + F) * 8;
+      if (k >= 0) {
+        const float b = db.pair_shiftf[(int64_t)F * Np + gs];
+        bsp_basis<float>(b, bs);
+        bsp_dbasis<float>(b, bs + 4);
+        const float inv = (float)sg[fm_pair_spline(pot, F, ti, tj)].invstep;
+#pragma unroll
+        for (int q = 4; q < 8; ++q) bs[q] *= inv;
+      } else {
+#pragma unroll
+        for (int q = 0; q < 8; ++q) bs[q] = 0.f;
+      }
+    }
+  }
+  const int ncf = 3 * fp.nt * fp.NB * CG;
+  for (int idx = tid; idx < ncf; idx += T) {
+    const int cl = idx % CG, a = (idx / CG) % fp.NB, o = (idx / (CG * fp.NB)) % fp.nt, F = idx / (CG * fp.NB * fp.nt);
+    st.coef[idx] = fp.coef32[(((size_t)gy * pot.nsplines + fm_pair_spline(pot, F, ti, o)) * FM_MAXB + a) * CG + cl];
+  }
+  __syncthreads();
+  na_out = na;
+  ti_out = ti;
+  return nslot;
+}
+
+// phi, rho, f (values and d/dr) of staged slot ql for candidate cl
 struct FmPairVals {
   float phi, dphi, rho, drho, f, df;
 };
-__device__ __forceinline__ FmPairVals fm_pair_vals(const DevPot &pot, const SplineGeom *sg, const float *coefg,
-                                                   int CG, const FmSlot &s) {
-  FmPairVals v{0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-  if (s.kphi >= 0) {
-    const int sp = pot.s_phi + s.pij;
-    v.phi = fm_pair_val(coefg + (size_t)sp * FM_MAXB * CG, CG, s.kphi, s.bphi, (float)sg[sp].invstep, v.dphi);
+__device__ __forceinline__ FmPairVals fm_pair_vals(const FmStage &st, const FmPlan &fp, int ql, int cl) {
+  float v[3], d[3];
+  const int kn = st.kn[ql], tj = st.tj[ql], CG = fp.CG;
+#pragma unroll
+  for (int F = 0; F < 3; ++F) {
+    const int k = ((kn >> (8 * F)) & 0xff) - 1;
+    const float *bs = st.bas + (ql * 3 + F) * 8;
+    const float *cf = st.coef + ((size_t)(F * fp.nt + tj) * fp.NB + (k < 0 ? 0 : k)) * CG + cl;
+    const float c0 = cf[0], c1 = cf[CG], c2 = cf[2 * CG], c3 = cf[3 * CG];
+    v[F] = bs[0] * c0 + bs[1] * c1 + bs[2] * c2 + bs[3] * c3;  // zero basis where k < 0
+    d[F] = bs[4] * c0 + bs[5] * c1 + bs[6] * c2 + bs[7] * c3;
   }
-  if (s.krho >= 0) {
-    const int sp = pot.s_rho + s.tj;
-    v.rho = fm_pair_val(coefg + (size_t)sp * FM_MAXB * CG, CG, s.krho, s.brho, (float)sg[sp].invstep, v.drho);
-  }
-  if (s.kf >= 0) {
-    const int sp = pot.s_f + s.pij;
-    v.f = fm_pair_val(coefg + (size_t)sp * FM_MAXB * CG, CG, s.kf, s.bf, (float)sg[sp].invstep, v.df);
-  }
-  return v;
+  return FmPairVals{v[0], d[0], v[1], d[1], v[2], d[2]};
 }
 
 // ---------------------------------------------------------------- k_fm_epi
 
-// Forward epilogue, thread = (atom in type order, candidate of group
-// blockIdx.y): the density rho_i = sum_p rho_p + 1/2 f_p G_p and the pair
-// energy in FP64 over the atom's row, the embedding (clamp and punishment,
-// pot_meam_spline.cpp:208-223), then per slot the reaction vector
+// Forward epilogue, persistent CTAs over the atom blocks, one task per
+// (atom, candidate of group blockIdx.y): the density
+// rho_i = sum_p rho_p + 1/2 f_p G_p and the pair energy in FP64 over the
+// atom's row, the embedding (clamp and punishment,
+// pot_meam_spline.cpp:208-223), then per slot the reaction vector, in FP64,
 //   V_p = u_p (phi'_p / 2 + U' (rho'_p + f'_p G_p)) + U' f_p / r_p (e1 Y1 + e2 Y2)
 // (the force atom i's terms put on it along slot p; the neighbour receives
 // -V_p), with the atom's own force and virial sums.
+__host__ __device__ inline size_t fm_epi_smem(int nsplines, int nt, int NB, int CG) {
+  return ((fm_stage_bytes(nt, NB, CG) + 15) & ~size_t(15)) + sizeof(SplineGeom) * (size_t)nsplines;
+}
+
 __global__ void __launch_bounds__(256) k_fm_epi(DevDb db, DevPot pot, const SplineGeom *__restrict__ geom,
                                                const double *__restrict__ tabs, FmPlan fp, int ncand) {
-  __shared__ SplineGeom sg[MAX_SPLINES];
-  const int gy = blockIdx.y, CG = fp.CG;
-  for (int s = threadIdx.x; s < pot.nsplines; s += blockDim.x) sg[s] = geom[s];
-  __syncthreads();
-  const int N = db.natoms;
-  const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (idx >= (int64_t)N * CG) return;
-  const int qa = (int)(idx / CG), cl = (int)(idx % CG);
+  extern __shared__ __align__(16) unsigned char fm_raw[];
+  const FmStage st = fm_stage_carve(fm_raw, fp);
+  SplineGeom *sg = reinterpret_cast<SplineGeom *>(
+      fm_raw + ((fm_stage_bytes(fp.nt, fp.NB, fp.CG) + 15) & ~size_t(15)));
+  const int gy = blockIdx.y, CG = fp.CG, N = db.natoms;
+  const int tid = threadIdx.x, T = blockDim.x;
+  for (int s = tid; s < pot.nsplines; s += T) sg[s] = geom[s];
+  const int cl = tid % CG;
   const int c = gy * CG + cl;
-  if (c >= ncand) return;
-  const float *coefg = fp.coef32 + (size_t)gy * pot.nsplines * FM_MAXB * CG + cl;
-  const double *tc = tabs + (size_t)c * pot.tab_stride;
-  const int i = db.adj_atoms[qa];
-  const int ti = db.atom_type[i];
-  const int64_t p0 = db.pair_off[i];
-  const int n = db.pair_off[i + 1] - (int)p0;
-  const int64_t q0 = fp.row0[i];
-  const float *Yq = fp.Y + ((size_t)gy * fp.Q + q0) * 3 * CG + cl;
-  double rho = 0.0, epair = 0.0;
-  for (int p = 0; p < n; ++p) {
-    const FmSlot s = fm_slot(db, pot, p0 + p, ti);
-    const FmPairVals v = fm_pair_vals(pot, sg, coefg, CG, s);
-    const float G = Yq[(size_t)p * 3 * CG];
-    rho += (double)v.rho + 0.5 * (double)v.f * (double)G;
-    epair += 0.5 * (double)v.phi;
-  }
-  // embedding
-  const SplineGeom &gU = sg[pot.s_U + ti];
-  const double w = db.cell_w[db.atom_cell[i]];
-  double pen = 0.0, rt = rho;
-  if (rho < gU.x0) {
-    pen = w * 100.0 * 10. * (gU.x0 - rho) * (gU.x0 - rho);
-    if (!pot.embed_extrap) rt = gU.x0;
-  } else if (rho > gU.xN) {
-    pen = w * 100.0 * 10. * (rho - gU.xN) * (rho - gU.xN);
-    if (!pot.embed_extrap) rt = gU.xN;
-  }
-  const PointEval U = spl_point(tc, gU, rt);
-  const float dF = (float)U.grad;
-  double F[3] = {0, 0, 0}, S[6] = {0, 0, 0, 0, 0, 0};
-  double *Vg = fp.V + (size_t)gy * db.npairs * CG * 3;
-  for (int p = 0; p < n; ++p) {
-    const FmSlot s = fm_slot(db, pot, p0 + p, ti);
-    const FmPairVals v = fm_pair_vals(pot, sg, coefg, CG, s);
-    const float *yp = Yq + (size_t)p * 3 * CG;
-    const float G = yp[0], Y1 = yp[CG], Y2 = yp[2 * CG];
-    const float4 e = *reinterpret_cast<const float4 *>(fp.E + (size_t)(q0 + p) * 8);
-    const float2 e2 = *reinterpret_cast<const float2 *>(fp.E + (size_t)(q0 + p) * 8 + 4);
-    const float A = 0.5f * v.dphi + dF * (v.drho + v.df * G);
-    const float B = dF * v.f * s.invr;
-    const double Vx = (double)(s.ux * A + B * (e.x * Y1 + e.w * Y2));
-    const double Vy = (double)(s.uy * A + B * (e.y * Y1 + e2.x * Y2));
-    const double Vz = (double)(s.uz * A + B * (e.z * Y1 + e2.y * Y2));
-    double *Vd = Vg + ((size_t)s.gs * CG + cl) * 3;
-    Vd[0] = Vx;
-    Vd[1] = Vy;
-    Vd[2] = Vz;
-    const double rr = db.pair_r[s.gs], dx = db.pair_ux[s.gs], dy = db.pair_uy[s.gs], dz = db.pair_uz[s.gs];
-    F[0] += Vx;
-    F[1] += Vy;
-    F[2] += Vz;
-    S[0] -= dx * (Vx * rr);
-    S[1] -= dy * (Vy * rr);
-    S[2] -= dz * (Vz * rr);
-    S[3] -= dx * (Vy * rr);
-    S[4] -= dy * (Vz * rr);
-    S[5] -= dz * (Vx * rr);
-  }
-  double *ao = fp.aoutF + ((size_t)gy * N + i) * AO_COUNT * CG + cl;
-  ao[AO_AX * CG] = F[0];
-  ao[AO_AY * CG] = F[1];
-  ao[AO_AZ * CG] = F[2];
-  ao[AO_E * CG] = epair + U.val;
+  const bool live = c < ncand;
+  const double *tc = tabs + (size_t)(live ? c : 0) * pot.tab_stride;
+  double *__restrict__ Vg = fp.V + (size_t)gy * db.npairs * CG * 3 + cl * 3;
+  for (int blk = blockIdx.x; blk < fp.nblk; blk += gridDim.x) {
+    int na, ti;
+    const int nslot = fm_stage_block(db, pot, sg, fp, st, blk, gy, na, ti);
+    (void)nslot;
+    if (!live) continue;
+    const SplineGeom &gU = sg[pot.s_U + ti];
+    for (int task = tid; task < na * CG; task += T) {
+      const int a = task / CG;
+      const int i = st.satom[a], lo = st.arow[a], n = st.arow[a + 1] - lo;
+      const double *Yq = fp.Y + ((size_t)gy * fp.Q + fp.row0[i]) * 3 * CG + cl;
+      double rho = 0.0, epair = 0.0;
+#pragma unroll 4
+      for (int p = 0; p < n; ++p) {
+        const FmPairVals v = fm_pair_vals(st, fp, lo + p, cl);
+        rho += (double)v.rho + 0.5 * (double)v.f * Yq[(size_t)p * 3 * CG];
+        epair += 0.5 * (double)v.phi;
+      }
+      const double w = db.cell_w[db.atom_cell[i]];
+      double pen = 0.0, rt = rho;
+      if (rho < gU.x0) {
+        pen = w * 100.0 * 10. * (gU.x0 - rho) * (gU.x0 - rho);
+        if (!pot.embed_extrap) rt = gU.x0;
+      } else if (rho > gU.xN) {
+        pen = w * 100.0 * 10. * (rho - gU.xN) * (rho - gU.xN);
+        if (!pot.embed_extrap) rt = gU.xN;
+      }
+      const PointEval U = spl_point(tc, gU, rt);
+      const double dF = U.grad;
+      double F[3] = {0, 0, 0}, S[6] = {0, 0, 0, 0, 0, 0};
+#pragma unroll 2
+      for (int p = 0; p < n; ++p) {
+        const int ql = lo + p;
+        const FmPairVals v = fm_pair_vals(st, fp, ql, cl);
+        const double *yp = Yq + (size_t)p * 3 * CG;
+        const double G = yp[0], Y1 = yp[CG], Y2 = yp[2 * CG];
+        const double *e = st.e + ql * 6;
+        const int64_t gs = st.gs[ql];
+        const double rr = db.pair_r[gs], dx = db.pair_ux[gs], dy = db.pair_uy[gs], dz = db.pair_uz[gs];
+        const double A = 0.5 * (double)v.dphi + dF * ((double)v.drho + (double)v.df * G);
+        const double B = dF * (double)v.f / rr;
+        const double Vx = dx * A + B * (e[0] * Y1 + e[3] * Y2);
+        const double Vy = dy * A + B * (e[1] * Y1 + e[4] * Y2);
+        const double Vz = dz * A + B * (e[2] * Y1 + e[5] * Y2);
+        double *Vd = Vg + (size_t)gs * CG * 3;
+        Vd[0] = Vx;
+        Vd[1] = Vy;
+        Vd[2] = Vz;
+        F[0] += Vx;
+        F[1] += Vy;
+        F[2] += Vz;
+        S[0] -= dx * (Vx * rr);
+        S[1] -= dy * (Vy * rr);
+        S[2] -= dz * (Vz * rr);
+        S[3] -= dx * (Vy * rr);
+        S[4] -= dy * (Vz * rr);
+        S[5] -= dz * (Vx * rr);
+      }
+      double *ao = fp.aoutF + ((size_t)gy * N + i) * AO_COUNT * CG + cl;
+      ao[AO_AX * CG] = F[0];
+      ao[AO_AY * CG] = F[1];
+      ao[AO_AZ * CG] = F[2];
+      ao[AO_E * CG] = epair + U.val;
 #pragma unroll
-  for (int q = 0; q < 6; ++q) ao[(AO_S0 + q) * CG] = S[q];
-  ao[AO_PEN * CG] = pen;
-  ao[AO_RHO * CG] = rho;
+      for (int q = 0; q < 6; ++q) ao[(AO_S0 + q) * CG] = S[q];
+      ao[AO_PEN * CG] = pen;
+      ao[AO_RHO * CG] = rho;
+    }
+  }
 }
 
 // ------------------------------------------------------------- k_fm_gather
@@ -629,137 +713,115 @@ __global__ void k_fm_cells(DevDb db, DevPot pot, FmPlan fp, int ncand, double *_
 
 // ------------------------------------------------------------ k_fm_adj_pre
 
-// Adjoint epilogue, persistent CTAs over the atom blocks (type-pure, at most
-// 256 slots and 64 atoms), candidate group blockIdx.y.  With the residual
-// sensitivities frozen (lambda, eps, mu, kappa),
-// L = sum_i [eps E_i + kappa pen_i] + sum_p Lambda_p . V_p and, per slot,
-// Lambda_p = lambda_i - lambda_j - r_p M_cell u_p, a_p = Lambda_p . u_p:
+// Adjoint epilogue, persistent CTAs over the atom blocks, candidate group
+// blockIdx.y.  With the residual sensitivities frozen (lambda, eps, mu,
+// kappa), L = sum_i [eps E_i + kappa pen_i] + sum_p Lambda_p . V_p and, per
+// slot, Lambda_p = lambda_i - lambda_j - r_p M_cell u_p, a_p = Lambda_p . u_p:
 //   k_p   = a_p (rho'_p + f'_p G_p) + f_p / r_p (Lambda.e1 Y1 + Lambda.e2 Y2)
 //   K_i   = sum_p k_p,  chi_i = dL/drho_i = (eps U' + U'' K_i) [unclamped] + kappa dpen/drho
 //   dL/dG_p = 1/2 f_p chi_i + a_p U' f'_p,  dL/dY1|2 = U' f_p / r_p Lambda.e1|2
-// (written over Y for k_fm_gemm_adj), and the pair functions' (value, slope)
-// weights
+// (into Yb for k_fm_gemm_adj), and the pair functions' (value, slope) weights
 //   phi: (eps / 2, a_p / 2), rho: (chi, U' a_p),
 //   f:   (chi G_p / 2 + U' (Lambda.e1 Y1 + Lambda.e2 Y2) / r_p, U' a_p G_p)
-// (f's role as the partner k goes through the contraction).  The weights of
-// FM_PCHUNK slots at a time are staged in shared memory and added into
-// per-(function, candidate) FP32 B-spline coefficient sums by whole warps
-// (the slot, hence the interval, is warp-uniform, so a switch picks the four
-// coefficients), flushed to this CTA's FP64 partial at a change of atom type
-// and every FM_PFLUSH blocks; the embedding table gradient (value weight
-// eps, slope weight K_i) is added per atom, in atom order, by the thread of
-// each candidate, in FP64.  Fixed order throughout.
-constexpr int FM_ABLK = 64;   // atoms per block of the adjoint epilogue
+// (f's role as the partner k goes through the contraction).  Phase 1: one
+// task per (atom, candidate) gives K_i and chi_i; phase 2: one task per
+// (slot, candidate) writes dL/dY and adds the pair-function weights times the
+// slot's four B-spline basis values into the thread's own FP32 coefficient
+// sums in shared memory (so no two threads add to the same word).  The
+// threads' sums are combined, in thread order, into this CTA's FP64 partials
+// at a change of atom type and every FM_PFLUSH blocks; the embedding table
+// gradient (value weight eps, slope weight K_i) is added per atom, in atom
+// order, by the thread of each candidate, in FP64.  Fixed order throughout.
 constexpr int FM_PFLUSH = 4;  // blocks between flushes of the pair-function sums
-struct FmAdjSmem {
-  double chi[FM_ABLK][64];
-  double dF[FM_ABLK][64];
-  double K[FM_ABLK][64];
-  float w[FM_PCHUNK][6][64];
-  int sk[FM_PCHUNK][3];    // knots of phi, rho, f
-  float sb[FM_PCHUNK][3];  // shifts
-  int stj[FM_PCHUNK];      // neighbour type
-  int satom[FM_ABLK];
-  int arow[FM_ABLK + 1];   // block-local first slot of each atom
-};
 
-__device__ __forceinline__ void fm_lambda(const DevDb &db, const FmPlan &fp, int gy, int cl, int i, int cell,
-                                          const FmSlot &s, float &lx, float &ly, float &lz) {
-  const int CG = fp.CG, N = db.natoms;
+__host__ __device__ inline size_t fm_pre_smem(int nsplines, int CG, int nt, int NB, int threads) {
+  size_t b = (fm_stage_bytes(nt, NB, CG) + 15) & ~size_t(15);
+  b += sizeof(float) * 3 * (size_t)FM_ABLK * CG;
+  b = (b + 15) & ~size_t(15);
+  b += sizeof(SplineGeom) * (size_t)nsplines;
+  b = (b + 15) & ~size_t(15);
+  b += sizeof(float) * (size_t)3 * nt * NB * threads;
+  return b;
+}
+
+__device__ __forceinline__ void fm_lambda(const FmPlan &fp, int N, int NC, int gy, int cl, int i, int j, int cell,
+                                          float ux, float uy, float uz, float r, float &lx, float &ly, float &lz) {
+  const int CG = fp.CG;
   const float *Li = fp.lamf + ((size_t)gy * N + i) * 3 * CG + cl;
-  const float *Lj = fp.lamf + ((size_t)gy * N + s.j) * 3 * CG + cl;
-  const double *sd = fp.seedF + ((size_t)gy * db.ncells + cell) * CS_COUNT * CG + cl;
+  const float *Lj = fp.lamf + ((size_t)gy * N + j) * 3 * CG + cl;
+  const double *sd = fp.seedF + ((size_t)gy * NC + cell) * CS_COUNT * CG + cl;
   const float mxx = (float)sd[(CS_MU0 + 0) * CG], myy = (float)sd[(CS_MU0 + 1) * CG],
               mzz = (float)sd[(CS_MU0 + 2) * CG], mxy = (float)sd[(CS_MU0 + 3) * CG],
               myz = (float)sd[(CS_MU0 + 4) * CG], mzx = (float)sd[(CS_MU0 + 5) * CG];
-  lx = Li[0] - Lj[0] - s.r * (mxx * s.ux + mzx * s.uz);
-  ly = Li[CG] - Lj[CG] - s.r * (myy * s.uy + mxy * s.ux);
-  lz = Li[2 * CG] - Lj[2 * CG] - s.r * (mzz * s.uz + myz * s.uy);
+  lx = Li[0] - Lj[0] - r * (mxx * ux + mzx * uz);
+  ly = Li[CG] - Lj[CG] - r * (myy * uy + mxy * ux);
+  lz = Li[2 * CG] - Lj[2 * CG] - r * (mzz * uz + myz * uy);
 }
 
-// The spline of pair function F (0 phi, 1 rho, 2 f) for a centre of type ti
-// and a neighbour of type tj.
-__device__ __forceinline__ int fm_pair_spline(const DevPot &pot, int F, int ti, int tj) {
-  return F == 1 ? pot.s_rho + tj : (F == 0 ? pot.s_phi : pot.s_f) + pair_ij_index(ti, tj, pot.ntypes);
-}
-
-__host__ __device__ inline size_t fm_pre_smem(int nsplines) {
-  return sizeof(FmAdjSmem) + sizeof(SplineGeom) * (size_t)nsplines;
-}
-
-__global__ void __launch_bounds__(256, 1) k_fm_adj_pre(DevDb db, DevPot pot, const SplineGeom *__restrict__ geom,
-                                                      const double *__restrict__ tabs, FmPlan fp, int ncand) {
+__global__ void __launch_bounds__(256) k_fm_adj_pre(DevDb db, DevPot pot, const SplineGeom *__restrict__ geom,
+                                                   const double *__restrict__ tabs, FmPlan fp, int ncand) {
   extern __shared__ __align__(16) unsigned char fm_raw[];
-  FmAdjSmem &sm = *reinterpret_cast<FmAdjSmem *>(fm_raw);
-  SplineGeom *sg = reinterpret_cast<SplineGeom *>(fm_raw + sizeof(FmAdjSmem));
   const int gy = blockIdx.y, CG = fp.CG, N = db.natoms, NC = db.ncells;
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  for (int s = tid; s < pot.nsplines; s += blockDim.x) sg[s] = geom[s];
-  const int cl = tid % CG, set = tid / CG, nsets = blockDim.x / CG;
+  const int tid = threadIdx.x, T = blockDim.x;
+  const FmStage st = fm_stage_carve(fm_raw, fp);
+  size_t off = (fm_stage_bytes(fp.nt, fp.NB, CG) + 15) & ~size_t(15);
+  float *chi = reinterpret_cast<float *>(fm_raw + off);
+  float *dFs = chi + FM_ABLK * CG;
+  float *Ks = dFs + FM_ABLK * CG;
+  off += sizeof(float) * 3 * (size_t)FM_ABLK * CG;
+  off = (off + 15) & ~size_t(15);
+  SplineGeom *sg = reinterpret_cast<SplineGeom *>(fm_raw + off);
+  off += sizeof(SplineGeom) * (size_t)pot.nsplines;
+  off = (off + 15) & ~size_t(15);
+  float *pacc = reinterpret_cast<float *>(fm_raw + off);  // entry e of thread t at e T + t
+  const int npe = 3 * fp.nt * fp.NB;
+  for (int sidx = tid; sidx < pot.nsplines; sidx += T) sg[sidx] = geom[sidx];
+  for (int e = 0; e < npe; ++e) pacc[(size_t)e * T + tid] = 0.f;
+  const int cl = tid % CG, set = tid / CG, nsets = T / CG;
   const int c = gy * CG + cl;
   const bool live = c < ncand;
-  const float *coefg = fp.coef32 + (size_t)gy * pot.nsplines * FM_MAXB * CG + cl;
   const double *tc = tabs + (size_t)(live ? c : 0) * pot.tab_stride;
-  // pair-function lanes: function pF = warp / wpf, candidate pc
-  const int wpf = (CG + 31) / 32;
-  const int pF = warp / wpf, pc = (warp % wpf) * 32 + lane;
-  const bool pworker = pF < 3 && pc < CG && gy * CG + pc < ncand;
-  float pacc[FM_MAXT][FM_MAXB];
-#pragma unroll
-  for (int o = 0; o < FM_MAXT; ++o)
-#pragma unroll
-    for (int a = 0; a < FM_MAXB; ++a) pacc[o][a] = 0.f;
   double *Pb = fp.Pbar + ((size_t)gy * gridDim.x + blockIdx.x) * pot.nsplines * FM_MAXB * CG;
   double *Tb = fp.Tbar + ((size_t)gy * gridDim.x + blockIdx.x) * CG * pot.tab_stride;
-  for (int i = tid; i < pot.nsplines * FM_MAXB * CG; i += blockDim.x) Pb[i] = 0.0;
-  for (int i = tid; i < CG * pot.tab_stride; i += blockDim.x) Tb[i] = 0.0;
+  for (int i = tid; i < pot.nsplines * FM_MAXB * CG; i += T) Pb[i] = 0.0;
+  for (int i = tid; i < CG * pot.tab_stride; i += T) Tb[i] = 0.0;
+  // the threads' sums of atom type tf into the FP64 partial, threads in order
   auto flush_pairs = [&](int tf) {
-    if (!pworker) return;
-#pragma unroll
-    for (int ot = 0; ot < FM_MAXT; ++ot)
-      if (ot < pot.ntypes) {
-        double *pb = Pb + (size_t)fm_pair_spline(pot, pF, tf, ot) * FM_MAXB * CG + pc;
-#pragma unroll
-        for (int a = 0; a < FM_MAXB; ++a) {
-          pb[(size_t)a * CG] += (double)pacc[ot][a];
-          pacc[ot][a] = 0.f;
-        }
+    __syncthreads();
+    for (int idx = tid; idx < npe * CG; idx += T) {
+      const int e = idx / CG, c2 = idx % CG;
+      const int F = e / (fp.nt * fp.NB), o = (e / fp.NB) % fp.nt, a = e % fp.NB;
+      float *pe = pacc + (size_t)e * T + c2;
+      double v = 0.0;
+      for (int k = 0; k < nsets; ++k) {
+        v += (double)pe[k * CG];
+        pe[k * CG] = 0.f;
       }
+      Pb[((size_t)fm_pair_spline(pot, F, tf, o) * FM_MAXB + a) * CG + c2] += v;
+    }
+    __syncthreads();
   };
   __syncthreads();
 
   int pacc_t = -1, since = 0;
   for (int blk = blockIdx.x; blk < fp.nblk; blk += gridDim.x) {
-    const int a0 = fp.blk0[blk], na = fp.blk0[blk + 1] - a0;
-    __syncthreads();
-    if (tid < na) sm.satom[tid] = db.adj_atoms[a0 + tid];
-    __syncthreads();
-    if (tid == 0) {
-      int lo = 0;
-      for (int a = 0; a < na; ++a) {
-        sm.arow[a] = lo;
-        lo += db.pair_off[sm.satom[a] + 1] - db.pair_off[sm.satom[a]];
-      }
-      sm.arow[na] = lo;
-    }
-    __syncthreads();
-    const int nslot = sm.arow[na];
-    const int ti = db.atom_type[sm.satom[0]];
-    if (pacc_t >= 0 && (ti != pacc_t || since == FM_PFLUSH)) {
+    // the block's type decides the pair splines of the sums: flush before staging
+    const int ti_next = db.atom_type[db.adj_atoms[fp.blk0[blk]]];
+    if (pacc_t >= 0 && (ti_next != pacc_t || since == FM_PFLUSH)) {
       flush_pairs(pacc_t);
       since = 0;
     }
+    int na, ti;
+    const int nslot = fm_stage_block(db, pot, sg, fp, st, blk, gy, na, ti);
     pacc_t = ti;
     ++since;
     const SplineGeom &gU = sg[pot.s_U + ti];
-    // ---- per (atom, candidate): K_i, chi_i
-    for (int a = set; a < na && live; a += nsets) {
-      const int i = sm.satom[a];
-      const int64_t p0 = db.pair_off[i];
-      const int n = db.pair_off[i + 1] - (int)p0;
+    // ---- phase 1: K_i and chi_i, one task per (atom, candidate)
+    for (int task = tid; task < na * CG && live; task += T) {
+      const int a = task / CG;
+      const int i = st.satom[a], lo = st.arow[a], n = st.arow[a + 1] - lo;
       const int cell = db.atom_cell[i];
-      const int64_t q0 = fp.row0[i];
-      const float *Yq = fp.Y + ((size_t)gy * fp.Q + q0) * 3 * CG + cl;
+      const double *Yq = fp.Y + ((size_t)gy * fp.Q + fp.row0[i]) * 3 * CG + cl;
       const double rho = fp.aoutF[((size_t)gy * N + i) * AO_COUNT * CG + AO_RHO * CG + cl];
       const double w = db.cell_w[cell];
       double rt = rho, dpen = 0.0, drt = 1.0;
@@ -772,121 +834,81 @@ __global__ void __launch_bounds__(256, 1) k_fm_adj_pre(DevDb db, DevPot pot, con
       }
       const PointEval U = spl_point(tc, gU, rt);
       double K = 0.0;
+#pragma unroll 2
       for (int p = 0; p < n; ++p) {
-        const FmSlot s = fm_slot(db, pot, p0 + p, ti);
-        const FmPairVals v = fm_pair_vals(pot, sg, coefg, CG, s);
-        const float *yp = Yq + (size_t)p * 3 * CG;
-        const float4 e = *reinterpret_cast<const float4 *>(fp.E + (size_t)(q0 + p) * 8);
-        const float2 e2 = *reinterpret_cast<const float2 *>(fp.E + (size_t)(q0 + p) * 8 + 4);
+        const int ql = lo + p;
+        const FmPairVals v = fm_pair_vals(st, fp, ql, cl);
+        const double *yp = Yq + (size_t)p * 3 * CG;
+        const float4 u = st.uf[ql];
+        const double *e = st.e + ql * 6;
         float lx, ly, lz;
-        fm_lambda(db, fp, gy, cl, i, cell, s, lx, ly, lz);
-        const float ap = lx * s.ux + ly * s.uy + lz * s.uz;
-        const float l1 = lx * e.x + ly * e.y + lz * e.z, l2 = lx * e.w + ly * e2.x + lz * e2.y;
-        K += (double)(ap * (v.drho + v.df * yp[0]) + v.f * s.invr * (l1 * yp[CG] + l2 * yp[2 * CG]));
+        fm_lambda(fp, N, NC, gy, cl, i, st.nbr[ql], cell, u.x, u.y, u.z, 1.f / u.w, lx, ly, lz);
+        const double ap = lx * u.x + ly * u.y + lz * u.z;
+        const double l1 = lx * e[0] + ly * e[1] + lz * e[2], l2 = lx * e[3] + ly * e[4] + lz * e[5];
+        K += ap * ((double)v.drho + (double)v.df * yp[0]) + (double)v.f * (double)u.w * (l1 * yp[CG] + l2 * yp[2 * CG]);
       }
       const double *sd = fp.seedF + ((size_t)gy * NC + cell) * CS_COUNT * CG + cl;
       const double eps = sd[CS_EPS * CG], kap = sd[CS_KAPPA * CG];
-      sm.chi[a][cl] = (eps * U.grad + U.grad2 * K) * drt + kap * dpen;
-      sm.dF[a][cl] = U.grad;
-      sm.K[a][cl] = K;
+      chi[a * CG + cl] = (float)((eps * U.grad + U.grad2 * K) * drt + kap * dpen);
+      dFs[a * CG + cl] = (float)U.grad;
+      Ks[a * CG + cl] = (float)K;
     }
     __syncthreads();
-    // ---- embedding table gradients: one thread per candidate, atoms in order
+    // ---- embedding table gradients: the thread of each candidate, atoms in order
     if (set == 0 && live) {
       double *tb = Tb + (size_t)cl * pot.tab_stride + gU.toff;
       for (int a = 0; a < na; ++a) {
-        const int i = sm.satom[a];
+        const int i = st.satom[a];
         const double rho = fp.aoutF[((size_t)gy * N + i) * AO_COUNT * CG + AO_RHO * CG + cl];
         const double rt = pot.embed_extrap ? rho : (rho < gU.x0 ? gU.x0 : (rho > gU.xN ? gU.xN : rho));
         const PointEval U = spl_point(tc, gU, rt);
         const double eps = fp.seedF[((size_t)gy * NC + db.atom_cell[i]) * CS_COUNT * CG + CS_EPS * CG + cl];
-        spl_point_adjoint(gU, U, rt, eps, sm.K[a][cl], [&](int ix, double x) { tb[ix] += x; });
+        spl_point_adjoint(gU, U, rt, eps, (double)Ks[a * CG + cl], [&](int ix, double x) { tb[ix] += x; });
       }
     }
-    // ---- dL/dY over Y and the pair-function weights, chunk by chunk
-    for (int c0 = 0; c0 < nslot; c0 += FM_PCHUNK) {
-      const int qn = min(FM_PCHUNK, nslot - c0);
-      __syncthreads();  // the previous chunk's weights are consumed
-      for (int qq = set; qq < qn; qq += nsets) {
-        const int ql = c0 + qq;
-        int a = 0;
-        while (a + 1 < na && sm.arow[a + 1] <= ql) ++a;
-        const int i = sm.satom[a];
-        const int p = ql - sm.arow[a];
-        const FmSlot s = fm_slot(db, pot, db.pair_off[i] + p, ti);
-        if (cl == 0) {
-          sm.sk[qq][0] = s.kphi;
-          sm.sk[qq][1] = s.krho;
-          sm.sk[qq][2] = s.kf;
-          sm.sb[qq][0] = s.bphi;
-          sm.sb[qq][1] = s.brho;
-          sm.sb[qq][2] = s.bf;
-          sm.stj[qq] = s.tj;
-        }
-        if (!live) continue;
+    // ---- phase 2: dL/dY into Yb and the pair-function gradients, one task per (slot, candidate)
+    if (live) {
+      int a = 0;
+      for (int ql = set; ql < nslot; ql += nsets) {
+        while (a + 1 < na && st.arow[a + 1] <= ql) ++a;
+        const int i = st.satom[a];
+        const int p = ql - st.arow[a];
         const int cell = db.atom_cell[i];
-        const FmPairVals v = fm_pair_vals(pot, sg, coefg, CG, s);
+        const FmPairVals v = fm_pair_vals(st, fp, ql, cl);
         const int64_t q = fp.row0[i] + p;
-        float *yp = fp.Y + ((size_t)gy * fp.Q + q) * 3 * CG + cl;
-        const float G = yp[0], Y1 = yp[CG], Y2 = yp[2 * CG];
-        const float4 e = *reinterpret_cast<const float4 *>(fp.E + (size_t)q * 8);
-        const float2 e2 = *reinterpret_cast<const float2 *>(fp.E + (size_t)q * 8 + 4);
+        const double *yp = fp.Y + ((size_t)gy * fp.Q + q) * 3 * CG + cl;
+        const float G = (float)yp[0], Y1 = (float)yp[CG], Y2 = (float)yp[2 * CG];
+        const float4 u = st.uf[ql];
+        const double *e = st.e + ql * 6;
         float lx, ly, lz;
-        fm_lambda(db, fp, gy, cl, i, cell, s, lx, ly, lz);
-        const float ap = lx * s.ux + ly * s.uy + lz * s.uz;
-        const float l1 = lx * e.x + ly * e.y + lz * e.z, l2 = lx * e.w + ly * e2.x + lz * e2.y;
-        const float chi = (float)sm.chi[a][cl], dF = (float)sm.dF[a][cl];
+        fm_lambda(fp, N, NC, gy, cl, i, st.nbr[ql], cell, u.x, u.y, u.z, 1.f / u.w, lx, ly, lz);
+        const float ap = lx * u.x + ly * u.y + lz * u.z;
+        const float l1 = (float)(lx * e[0] + ly * e[1] + lz * e[2]), l2 = (float)(lx * e[3] + ly * e[4] + lz * e[5]);
+        const float ch = chi[a * CG + cl], dF = dFs[a * CG + cl];
         const float eps = (float)fp.seedF[((size_t)gy * NC + cell) * CS_COUNT * CG + CS_EPS * CG + cl];
-        const float B = dF * v.f * s.invr;
-        yp[0] = 0.5f * v.f * chi + ap * dF * v.df;
-        yp[CG] = B * l1;
-        yp[2 * CG] = B * l2;
-        sm.w[qq][0][cl] = 0.5f * eps;
-        sm.w[qq][1][cl] = 0.5f * ap;
-        sm.w[qq][2][cl] = chi;
-        sm.w[qq][3][cl] = dF * ap;
-        sm.w[qq][4][cl] = 0.5f * chi * G + dF * (l1 * Y1 + l2 * Y2) * s.invr;
-        sm.w[qq][5][cl] = dF * ap * G;
-      }
-      __syncthreads();
-      if (pworker) {
-        for (int qq = 0; qq < qn; ++qq) {
-          const int k = sm.sk[qq][pF];
-          if (k < 0) continue;  // warp-uniform
-          const int ot = sm.stj[qq];
-          const float b = sm.sb[qq][pF];
-          float Nv[4], Nd[4];
-          bsp_basis<float>(b, Nv);
-          bsp_dbasis<float>(b, Nd);
-          const float inv = (float)sg[fm_pair_spline(pot, pF, ti, ot)].invstep;
-          const float wv = sm.w[qq][2 * pF][pc], wd = sm.w[qq][2 * pF + 1][pc] * inv;
-          const float c0v = wv * Nv[0] + wd * Nd[0], c1v = wv * Nv[1] + wd * Nd[1], c2v = wv * Nv[2] + wd * Nd[2],
-                      c3v = wv * Nv[3] + wd * Nd[3];
-          switch (ot * FM_MAXB + k) {
-#define FM_CASE(OT, K)      \
-  case OT * FM_MAXB + K:    \
-    pacc[OT][K] += c0v;     \
-    pacc[OT][K + 1] += c1v; \
-    pacc[OT][K + 2] += c2v; \
-    pacc[OT][K + 3] += c3v; \
-    break;
-#define FM_CASES(OT)                                                                                       \
-  FM_CASE(OT, 0) FM_CASE(OT, 1) FM_CASE(OT, 2) FM_CASE(OT, 3) FM_CASE(OT, 4) FM_CASE(OT, 5) FM_CASE(OT, 6) \
-  FM_CASE(OT, 7) FM_CASE(OT, 8) FM_CASE(OT, 9) FM_CASE(OT, 10) FM_CASE(OT, 11) FM_CASE(OT, 12)             \
-  FM_CASE(OT, 13) FM_CASE(OT, 14) FM_CASE(OT, 15) FM_CASE(OT, 16) FM_CASE(OT, 17) FM_CASE(OT, 18)          \
-  FM_CASE(OT, 19) FM_CASE(OT, 20)
-            FM_CASES(0)
-            FM_CASES(1)
-#undef FM_CASES
-#undef FM_CASE
-            default:
-              break;
-          }
+        const float B = dF * v.f * u.w;
+        float *yb = fp.Yb + ((size_t)gy * fp.Q + q) * 3 * CG + cl;
+        yb[0] = 0.5f * v.f * ch + ap * dF * v.df;
+        yb[CG] = B * l1;
+        yb[2 * CG] = B * l2;
+        // (value, slope) weights of phi, rho, f times the basis values
+        const float wv[3] = {0.5f * eps, ch, 0.5f * ch * G + dF * (l1 * Y1 + l2 * Y2) * u.w};
+        const float wd[3] = {0.5f * ap, dF * ap, dF * ap * G};
+        const int kn = st.kn[ql], tj = st.tj[ql];
+#pragma unroll
+        for (int F = 0; F < 3; ++F) {
+          const int k = ((kn >> (8 * F)) & 0xff) - 1;
+          if (k < 0) continue;
+          const float *bs = st.bas + (ql * 3 + F) * 8;
+          float *pe = pacc + ((size_t)(F * fp.nt + tj) * fp.NB + k) * T + tid;
+          pe[0] += wv[F] * bs[0] + wd[F] * bs[4];
+          pe[T] += wv[F] * bs[1] + wd[F] * bs[5];
+          pe[2 * T] += wv[F] * bs[2] + wd[F] * bs[6];
+          pe[3 * T] += wv[F] * bs[3] + wd[F] * bs[7];
         }
       }
     }
   }
-  __syncthreads();
   if (pacc_t >= 0) flush_pairs(pacc_t);
 }
 
@@ -894,82 +916,95 @@ __global__ void __launch_bounds__(256, 1) k_fm_adj_pre(DevDb db, DevPot pot, con
 
 // Kbar_s[d][c] += sum_{q,t} X[t][d][q] Ybar[q][t][c] over this CTA's run of
 // tiles, sub-tile by sub-tile of FM_SUB slots (all Dpad features of the three
-// kinds in shared memory).  Thread: FM_ROWS consecutive features x 8
-// candidates, FP32 sums flushed into this CTA's FP64 partial of the tile's
-// atom type after every tile.
+// kinds in shared memory, two sub-tiles in flight: cp.async fills one while
+// the other is consumed).  Thread: FM_ROWS consecutive features x 8
+// candidates as packed pairs of candidates; the FP32 sums of a tile are
+// added to this CTA's FP64 partial of the tile's atom type.
 __host__ __device__ inline size_t fm_adj_smem(int Dpad, int CG) {
-  return sizeof(float) * ((size_t)3 * Dpad * FM_SUB + (size_t)FM_SUB * 3 * CG);
+  return 2 * sizeof(float) * ((size_t)3 * Dpad * FM_SUB + (size_t)FM_SUB * 3 * CG);
 }
 
 __global__ void __launch_bounds__(256, 1) k_fm_gemm_adj(FmPlan fp) {
   extern __shared__ __align__(16) float asm_[];
   const int CG = fp.CG, gy = blockIdx.y;
-  float *Xs = asm_;                               // [3 Dpad rows: (kind, feature)][FM_SUB]
-  float *Ys = Xs + (size_t)3 * fp.Dpad * FM_SUB;  // [FM_SUB][3][CG]
+  const size_t xsz = (size_t)3 * fp.Dpad * FM_SUB, ysz = (size_t)FM_SUB * 3 * CG;
   const int tid = threadIdx.x;
   const int ncs = CG / 8, nds = fp.Dpad / FM_ROWS;
   const int cs = tid % ncs, ds = tid / ncs;
   const bool worker = ds < nds;
   const int per = (fp.ntiles + gridDim.x - 1) / gridDim.x;
   const int tb = blockIdx.x * per, te = min(fp.ntiles, tb + per);
+  constexpr int NSUB = FM_TILE / FM_SUB;
+  const int total = te > tb ? (te - tb) * NSUB : 0;
   double *Kb = fp.Kbar + ((size_t)gy * gridDim.x + blockIdx.x) * fp.nt * fp.Dpad * CG;
   for (int i = tid; i < fp.nt * fp.Dpad * CG; i += blockDim.x) Kb[i] = 0.0;
-  float acc[FM_ROWS][8];
+  auto load = [&](int k, float *bx) {
+    const int64_t qb = (int64_t)(tb + k / NSUB) * FM_TILE + (k % NSUB) * FM_SUB;
+    const int nrow = 3 * fp.Dpad;
+    for (int i = tid; i < nrow * (FM_SUB / 4); i += blockDim.x) {
+      const int row = i / (FM_SUB / 4), col = (i % (FM_SUB / 4)) * 4;
+      const int t = row / fp.Dpad, d = row % fp.Dpad;
+      const size_t grow = (size_t)((d / FM_DC) * 3 + t) * FM_DC + d % FM_DC;
+      cp_async16(bx + (size_t)row * FM_SUB + col, fp.X + grow * fp.Q + qb + col);
+    }
+    const float *ysrc = fp.Yb + ((size_t)gy * fp.Q + qb) * 3 * CG;
+    float *by = bx + xsz;
+    for (int i = tid * 4; i < (int)ysz; i += blockDim.x * 4) cp_async16(by + i, ysrc + i);
+    cp_async_commit();
+  };
+  float2 acc[FM_ROWS][4];
 #pragma unroll
   for (int r = 0; r < FM_ROWS; ++r)
 #pragma unroll
-    for (int c = 0; c < 8; ++c) acc[r][c] = 0.f;
-  for (int tile = tb; tile < te; ++tile) {
-    const int s = fm_tile_type(fp, tile);
-    for (int sub = 0; sub < FM_TILE; sub += FM_SUB) {
-      const int64_t qb = (int64_t)tile * FM_TILE + sub;
-      __syncthreads();
-      const int nrow = 3 * fp.Dpad;
-      for (int i = tid; i < nrow * (FM_SUB / 4); i += blockDim.x) {
-        const int row = i / (FM_SUB / 4), col = (i % (FM_SUB / 4)) * 4;
-        const int t = row / fp.Dpad, d = row % fp.Dpad;
-        const size_t grow = (size_t)((d / FM_DC) * 3 + t) * FM_DC + d % FM_DC;
-        cp_async16(Xs + (size_t)row * FM_SUB + col, fp.X + grow * fp.Q + qb + col);
-      }
-      const float *ysrc = fp.Y + ((size_t)gy * fp.Q + qb) * 3 * CG;
-      for (int i = tid * 4; i < FM_SUB * 3 * CG; i += blockDim.x * 4) cp_async16(Ys + i, ysrc + i);
-      cp_async_commit();
+    for (int c = 0; c < 4; ++c) acc[r][c] = make_float2(0.f, 0.f);
+  if (total > 0) load(0, asm_);
+  for (int k = 0; k < total; ++k) {
+    if (k + 1 < total) {
+      load(k + 1, asm_ + ((k + 1) & 1) * (xsz + ysz));
+      cp_async_wait<1>();
+    } else {
       cp_async_wait<0>();
-      __syncthreads();
-      if (worker) {
+    }
+    __syncthreads();
+    const float *Xs = asm_ + (k & 1) * (xsz + ysz), *Ys = Xs + xsz;
+    if (worker) {
 #pragma unroll
-        for (int t = 0; t < 3; ++t)
+      for (int t = 0; t < 3; ++t)
 #pragma unroll
-          for (int qg = 0; qg < FM_SUB; qg += 4) {
-            float4 xv[FM_ROWS];
+        for (int qg = 0; qg < FM_SUB; qg += 4) {
+          float4 xv[FM_ROWS];
 #pragma unroll
-            for (int r = 0; r < FM_ROWS; ++r)
-              xv[r] = *reinterpret_cast<const float4 *>(Xs + ((size_t)t * fp.Dpad + ds * FM_ROWS + r) * FM_SUB + qg);
+          for (int r = 0; r < FM_ROWS; ++r)
+            xv[r] = *reinterpret_cast<const float4 *>(Xs + ((size_t)t * fp.Dpad + ds * FM_ROWS + r) * FM_SUB + qg);
 #pragma unroll
-            for (int qq = 0; qq < 4; ++qq) {
-              const float *yq = Ys + ((size_t)(qg + qq) * 3 + t) * CG + cs * 8;
-              const float4 y0 = *reinterpret_cast<const float4 *>(yq), y1 = *reinterpret_cast<const float4 *>(yq + 4);
-              const float yv[8] = {y0.x, y0.y, y0.z, y0.w, y1.x, y1.y, y1.z, y1.w};
+          for (int qq = 0; qq < 4; ++qq) {
+            const float *yq = Ys + ((size_t)(qg + qq) * 3 + t) * CG + cs * 8;
+            const float4 y0 = *reinterpret_cast<const float4 *>(yq), y1 = *reinterpret_cast<const float4 *>(yq + 4);
+            const float2 yv[4] = {make_float2(y0.x, y0.y), make_float2(y0.z, y0.w), make_float2(y1.x, y1.y),
+                                  make_float2(y1.z, y1.w)};
 #pragma unroll
-              for (int r = 0; r < FM_ROWS; ++r) {
-                const float x = qq == 0 ? xv[r].x : qq == 1 ? xv[r].y : qq == 2 ? xv[r].z : xv[r].w;
+            for (int r = 0; r < FM_ROWS; ++r) {
+              const float x = qq == 0 ? xv[r].x : qq == 1 ? xv[r].y : qq == 2 ? xv[r].z : xv[r].w;
+              const float2 xx = bcast2(x);
 #pragma unroll
-                for (int c = 0; c < 8; ++c) acc[r][c] = fmaf(x, yv[c], acc[r][c]);
-              }
+              for (int c = 0; c < 4; ++c) acc[r][c] = fma2(xx, yv[c], acc[r][c]);
             }
           }
-      }
+        }
     }
-    if (worker) {
+    if ((k + 1) % NSUB == 0 && worker) {  // end of a tile: into the FP64 partial of its type
+      const int s = fm_tile_type(fp, tb + k / NSUB);
       double *kb = Kb + ((size_t)s * fp.Dpad + ds * FM_ROWS) * CG + cs * 8;
 #pragma unroll
       for (int r = 0; r < FM_ROWS; ++r)
 #pragma unroll
-        for (int c = 0; c < 8; ++c) {
-          kb[(size_t)r * CG + c] += (double)acc[r][c];
-          acc[r][c] = 0.f;
+        for (int c = 0; c < 4; ++c) {
+          kb[(size_t)r * CG + 2 * c] += (double)acc[r][c].x;
+          kb[(size_t)r * CG + 2 * c + 1] += (double)acc[r][c].y;
+          acc[r][c] = make_float2(0.f, 0.f);
         }
     }
+    __syncthreads();
   }
 }
 
