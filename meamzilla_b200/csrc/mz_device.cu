@@ -1183,6 +1183,7 @@ mz_status mz_create(const mz_db *dbh, const mz_pot *poth, const mz_settings *set
               row0[i] = (int)q;
               q += db.pair_off[i + 1] - db.pair_off[i];
             }
+            fp.qend[t] = q;
             q = (q + FM_TILE - 1) / FM_TILE * FM_TILE;
           }
           fp.Q = q;

@@ -59,6 +59,7 @@ struct FmPlan {
   int64_t Q;       // feature slots
   int ntiles;      // Q / FM_TILE
   int tile0[FM_MAXT + 1];  // first tile of each type
+  int64_t qend[FM_MAXT];   // end of each type's real slots (the rest of its last tile is padding)
   int NB;          // B-spline coefficients of the phi, rho and f splines (the largest)
   int nblk;        // atom blocks of the adjoint epilogue (type-pure, <= 256 slots, <= 64 atoms)
   const int *blk0;         // [nblk + 1] into adj_atoms
@@ -381,30 +382,33 @@ __global__ void __launch_bounds__(NW * 32, 1) k_fm_gemm_fwd(FmPlan fp) {
 // atom type for the group's candidates.
 constexpr int FM_ABLK = 64;  // atoms per block of the epilogues
 
+template <typename R>
 struct FmStage {
   int *satom, *arow;  // [FM_ABLK], [FM_ABLK + 1]
   int *gs, *nbr, *tj, *kn;  // [BLOCK_SLOTS]
   float4 *uf;         // [BLOCK_SLOTS] (ux, uy, uz, 1/r)
   double *e;          // [BLOCK_SLOTS][6] e1, e2
-  float *bas;         // [BLOCK_SLOTS][3][8] basis N0..N3 and d/dr N0'..N3' of phi, rho, f
-  float *coef;        // [3][nt][NB][CG]
+  R *bas;             // [BLOCK_SLOTS][3][8] basis N0..N3 and d/dr N0'..N3' of phi, rho, f
+  R *coef;            // [3][nt][NB][CG]
 };
 
+template <typename R>
 __host__ __device__ inline size_t fm_stage_bytes(int nt, int NB, int CG) {
   return sizeof(int) * (2 * FM_ABLK + 1 + 4 * BLOCK_SLOTS) + 16 + sizeof(float4) * BLOCK_SLOTS +
-         sizeof(double) * 6 * BLOCK_SLOTS + sizeof(float) * 24 * BLOCK_SLOTS + sizeof(float) * 3 * nt * NB * CG;
+         sizeof(double) * 6 * BLOCK_SLOTS + sizeof(R) * 24 * BLOCK_SLOTS + sizeof(R) * 3 * nt * NB * CG;
 }
 
 // carves the staging arrays out of shared memory at `base` (16-byte aligned)
-__device__ __forceinline__ FmStage fm_stage_carve(unsigned char *base, const FmPlan &fp) {
-  FmStage st;
+template <typename R>
+__device__ __forceinline__ FmStage<R> fm_stage_carve(unsigned char *base, const FmPlan &fp) {
+  FmStage<R> st;
   double *e = reinterpret_cast<double *>(base);
   st.e = e;
   float4 *uf = reinterpret_cast<float4 *>(e + 6 * BLOCK_SLOTS);
   st.uf = uf;
-  float *bas = reinterpret_cast<float *>(uf + BLOCK_SLOTS);
+  R *bas = reinterpret_cast<R *>(uf + BLOCK_SLOTS);
   st.bas = bas;
-  float *coef = bas + 24 * BLOCK_SLOTS;
+  R *coef = bas + 24 * BLOCK_SLOTS;
   st.coef = coef;
   int *ip = reinterpret_cast<int *>(coef + 3 * fp.nt * fp.NB * fp.CG);
   st.satom = ip;
@@ -423,8 +427,11 @@ __device__ __forceinline__ int fm_pair_spline(const DevPot &pot, int F, int ti, 
 }
 
 // Stages block blk; returns its slot count (all threads; barriers inside).
+// FP32 coefficients come from the group's FP32 table, FP64 ones from the
+// candidates' FP64 coefficients.
+template <typename R>
 __device__ int fm_stage_block(const DevDb &db, const DevPot &pot, const SplineGeom *sg, const FmPlan &fp,
-                              const FmStage &st, int blk, int gy, int &na_out, int &ti_out) {
+                              const FmStage<R> &st, int blk, int gy, int ncand, int &na_out, int &ti_out) {
   const int tid = threadIdx.x, T = blockDim.x, CG = fp.CG;
   const int a0 = fp.blk0[blk], na = fp.blk0[blk + 1] - a0;
   __syncthreads();  // the previous block is done with the staging
@@ -460,24 +467,30 @@ __device__ int fm_stage_block(const DevDb &db, const DevPot &pot, const SplineGe
 #pragma unroll
     for (int F = 0; F < 3; ++F) {
       const int k = ((kn >> (8 * F)) & 0xff) - 1;
-      float *bs = st.bas + (ql * 3 + F) * 8;
+      R *bs = st.bas + (ql * 3 + F) * 8;
       if (k >= 0) {
-        const float b = db.pair_shiftf[(int64_t)F * Np + gs];
-        bsp_basis<float>(b, bs);
-        bsp_dbasis<float>(b, bs + 4);
-        const float inv = (float)sg[fm_pair_spline(pot, F, ti, tj)].invstep;
+        const R b = sizeof(R) == 8 ? (R)db.pair_shift[(int64_t)F * Np + gs] : (R)db.pair_shiftf[(int64_t)F * Np + gs];
+        bsp_basis<R>(b, bs);
+        bsp_dbasis<R>(b, bs + 4);
+        const R inv = (R)sg[fm_pair_spline(pot, F, ti, tj)].invstep;
 #pragma unroll
         for (int q = 4; q < 8; ++q) bs[q] *= inv;
       } else {
 #pragma unroll
-        for (int q = 0; q < 8; ++q) bs[q] = 0.f;
+        for (int q = 0; q < 8; ++q) bs[q] = R(0);
       }
     }
   }
   const int ncf = 3 * fp.nt * fp.NB * CG;
   for (int idx = tid; idx < ncf; idx += T) {
     const int cl = idx % CG, a = (idx / CG) % fp.NB, o = (idx / (CG * fp.NB)) % fp.nt, F = idx / (CG * fp.NB * fp.nt);
-    st.coef[idx] = fp.coef32[(((size_t)gy * pot.nsplines + fm_pair_spline(pot, F, ti, o)) * FM_MAXB + a) * CG + cl];
+    const int sp = fm_pair_spline(pot, F, ti, o);
+    if (sizeof(R) == 8) {
+      const int c = gy * CG + cl;
+      st.coef[idx] = c < ncand ? (R)fp.coef64[((size_t)c * pot.nsplines + sp) * FM_MAXB + a] : R(0);
+    } else {
+      st.coef[idx] = (R)fp.coef32[(((size_t)gy * pot.nsplines + sp) * FM_MAXB + a) * CG + cl];
+    }
   }
   __syncthreads();
   na_out = na;
@@ -486,22 +499,24 @@ __device__ int fm_stage_block(const DevDb &db, const DevPot &pot, const SplineGe
 }
 
 // phi, rho, f (values and d/dr) of staged slot ql for candidate cl
+template <typename R>
 struct FmPairVals {
-  float phi, dphi, rho, drho, f, df;
+  R phi, dphi, rho, drho, f, df;
 };
-__device__ __forceinline__ FmPairVals fm_pair_vals(const FmStage &st, const FmPlan &fp, int ql, int cl) {
-  float v[3], d[3];
+template <typename R>
+__device__ __forceinline__ FmPairVals<R> fm_pair_vals(const FmStage<R> &st, const FmPlan &fp, int ql, int cl) {
+  R v[3], d[3];
   const int kn = st.kn[ql], tj = st.tj[ql], CG = fp.CG;
 #pragma unroll
   for (int F = 0; F < 3; ++F) {
     const int k = ((kn >> (8 * F)) & 0xff) - 1;
-    const float *bs = st.bas + (ql * 3 + F) * 8;
-    const float *cf = st.coef + ((size_t)(F * fp.nt + tj) * fp.NB + (k < 0 ? 0 : k)) * CG + cl;
-    const float c0 = cf[0], c1 = cf[CG], c2 = cf[2 * CG], c3 = cf[3 * CG];
+    const R *bs = st.bas + (ql * 3 + F) * 8;
+    const R *cf = st.coef + ((size_t)(F * fp.nt + tj) * fp.NB + (k < 0 ? 0 : k)) * CG + cl;
+    const R c0 = cf[0], c1 = cf[CG], c2 = cf[2 * CG], c3 = cf[3 * CG];
     v[F] = bs[0] * c0 + bs[1] * c1 + bs[2] * c2 + bs[3] * c3;  // zero basis where k < 0
     d[F] = bs[4] * c0 + bs[5] * c1 + bs[6] * c2 + bs[7] * c3;
   }
-  return FmPairVals{v[0], d[0], v[1], d[1], v[2], d[2]};
+  return FmPairVals<R>{v[0], d[0], v[1], d[1], v[2], d[2]};
 }
 
 // ---------------------------------------------------------------- k_fm_epi
@@ -513,17 +528,19 @@ __device__ __forceinline__ FmPairVals fm_pair_vals(const FmStage &st, const FmPl
 // pot_meam_spline.cpp:208-223), then per slot the reaction vector, in FP64,
 //   V_p = u_p (phi'_p / 2 + U' (rho'_p + f'_p G_p)) + U' f_p / r_p (e1 Y1 + e2 Y2)
 // (the force atom i's terms put on it along slot p; the neighbour receives
-// -V_p), with the atom's own force and virial sums.
+// -V_p), with the atom's own force and virial sums.  The pair functions are
+// evaluated in FP64 here (from the candidates' FP64 B-spline coefficients):
+// the forces are sums of reaction vectors much larger than they are.
 __host__ __device__ inline size_t fm_epi_smem(int nsplines, int nt, int NB, int CG) {
-  return ((fm_stage_bytes(nt, NB, CG) + 15) & ~size_t(15)) + sizeof(SplineGeom) * (size_t)nsplines;
+  return ((fm_stage_bytes<double>(nt, NB, CG) + 15) & ~size_t(15)) + sizeof(SplineGeom) * (size_t)nsplines;
 }
 
 __global__ void __launch_bounds__(256) k_fm_epi(DevDb db, DevPot pot, const SplineGeom *__restrict__ geom,
                                                const double *__restrict__ tabs, FmPlan fp, int ncand) {
   extern __shared__ __align__(16) unsigned char fm_raw[];
-  const FmStage st = fm_stage_carve(fm_raw, fp);
+  const FmStage<double> st = fm_stage_carve<double>(fm_raw, fp);
   SplineGeom *sg = reinterpret_cast<SplineGeom *>(
-      fm_raw + ((fm_stage_bytes(fp.nt, fp.NB, fp.CG) + 15) & ~size_t(15)));
+      fm_raw + ((fm_stage_bytes<double>(fp.nt, fp.NB, fp.CG) + 15) & ~size_t(15)));
   const int gy = blockIdx.y, CG = fp.CG, N = db.natoms;
   const int tid = threadIdx.x, T = blockDim.x;
   for (int s = tid; s < pot.nsplines; s += T) sg[s] = geom[s];
@@ -534,7 +551,7 @@ __global__ void __launch_bounds__(256) k_fm_epi(DevDb db, DevPot pot, const Spli
   double *__restrict__ Vg = fp.V + (size_t)gy * db.npairs * CG * 3 + cl * 3;
   for (int blk = blockIdx.x; blk < fp.nblk; blk += gridDim.x) {
     int na, ti;
-    const int nslot = fm_stage_block(db, pot, sg, fp, st, blk, gy, na, ti);
+    const int nslot = fm_stage_block<double>(db, pot, sg, fp, st, blk, gy, ncand, na, ti);
     (void)nslot;
     if (!live) continue;
     const SplineGeom &gU = sg[pot.s_U + ti];
@@ -545,9 +562,9 @@ __global__ void __launch_bounds__(256) k_fm_epi(DevDb db, DevPot pot, const Spli
       double rho = 0.0, epair = 0.0;
 #pragma unroll 4
       for (int p = 0; p < n; ++p) {
-        const FmPairVals v = fm_pair_vals(st, fp, lo + p, cl);
-        rho += (double)v.rho + 0.5 * (double)v.f * Yq[(size_t)p * 3 * CG];
-        epair += 0.5 * (double)v.phi;
+        const FmPairVals<double> v = fm_pair_vals<double>(st, fp, lo + p, cl);
+        rho += v.rho + 0.5 * v.f * Yq[(size_t)p * 3 * CG];
+        epair += 0.5 * v.phi;
       }
       const double w = db.cell_w[db.atom_cell[i]];
       double pen = 0.0, rt = rho;
@@ -564,14 +581,14 @@ __global__ void __launch_bounds__(256) k_fm_epi(DevDb db, DevPot pot, const Spli
 #pragma unroll 2
       for (int p = 0; p < n; ++p) {
         const int ql = lo + p;
-        const FmPairVals v = fm_pair_vals(st, fp, ql, cl);
+        const FmPairVals<double> v = fm_pair_vals<double>(st, fp, ql, cl);
         const double *yp = Yq + (size_t)p * 3 * CG;
         const double G = yp[0], Y1 = yp[CG], Y2 = yp[2 * CG];
         const double *e = st.e + ql * 6;
         const int64_t gs = st.gs[ql];
         const double rr = db.pair_r[gs], dx = db.pair_ux[gs], dy = db.pair_uy[gs], dz = db.pair_uz[gs];
-        const double A = 0.5 * (double)v.dphi + dF * ((double)v.drho + (double)v.df * G);
-        const double B = dF * (double)v.f / rr;
+        const double A = 0.5 * v.dphi + dF * (v.drho + v.df * G);
+        const double B = dF * v.f / rr;
         const double Vx = dx * A + B * (e[0] * Y1 + e[3] * Y2);
         const double Vy = dy * A + B * (e[1] * Y1 + e[4] * Y2);
         const double Vz = dz * A + B * (e[2] * Y1 + e[5] * Y2);
@@ -735,7 +752,7 @@ __global__ void k_fm_cells(DevDb db, DevPot pot, FmPlan fp, int ncand, double *_
 constexpr int FM_PFLUSH = 4;  // blocks between flushes of the pair-function sums
 
 __host__ __device__ inline size_t fm_pre_smem(int nsplines, int CG, int nt, int NB, int threads) {
-  size_t b = (fm_stage_bytes(nt, NB, CG) + 15) & ~size_t(15);
+  size_t b = (fm_stage_bytes<float>(nt, NB, CG) + 15) & ~size_t(15);
   b += sizeof(float) * 3 * (size_t)FM_ABLK * CG;
   b = (b + 15) & ~size_t(15);
   b += sizeof(SplineGeom) * (size_t)nsplines;
@@ -763,8 +780,8 @@ __global__ void __launch_bounds__(256) k_fm_adj_pre(DevDb db, DevPot pot, const 
   extern __shared__ __align__(16) unsigned char fm_raw[];
   const int gy = blockIdx.y, CG = fp.CG, N = db.natoms, NC = db.ncells;
   const int tid = threadIdx.x, T = blockDim.x;
-  const FmStage st = fm_stage_carve(fm_raw, fp);
-  size_t off = (fm_stage_bytes(fp.nt, fp.NB, CG) + 15) & ~size_t(15);
+  const FmStage<float> st = fm_stage_carve<float>(fm_raw, fp);
+  size_t off = (fm_stage_bytes<float>(fp.nt, fp.NB, CG) + 15) & ~size_t(15);
   float *chi = reinterpret_cast<float *>(fm_raw + off);
   float *dFs = chi + FM_ABLK * CG;
   float *Ks = dFs + FM_ABLK * CG;
@@ -812,7 +829,7 @@ __global__ void __launch_bounds__(256) k_fm_adj_pre(DevDb db, DevPot pot, const 
       since = 0;
     }
     int na, ti;
-    const int nslot = fm_stage_block(db, pot, sg, fp, st, blk, gy, na, ti);
+    const int nslot = fm_stage_block<float>(db, pot, sg, fp, st, blk, gy, ncand, na, ti);
     pacc_t = ti;
     ++since;
     const SplineGeom &gU = sg[pot.s_U + ti];
@@ -837,7 +854,7 @@ __global__ void __launch_bounds__(256) k_fm_adj_pre(DevDb db, DevPot pot, const 
 #pragma unroll 2
       for (int p = 0; p < n; ++p) {
         const int ql = lo + p;
-        const FmPairVals v = fm_pair_vals(st, fp, ql, cl);
+        const FmPairVals<float> v = fm_pair_vals<float>(st, fp, ql, cl);
         const double *yp = Yq + (size_t)p * 3 * CG;
         const float4 u = st.uf[ql];
         const double *e = st.e + ql * 6;
@@ -874,7 +891,7 @@ __global__ void __launch_bounds__(256) k_fm_adj_pre(DevDb db, DevPot pot, const 
         const int i = st.satom[a];
         const int p = ql - st.arow[a];
         const int cell = db.atom_cell[i];
-        const FmPairVals v = fm_pair_vals(st, fp, ql, cl);
+        const FmPairVals<float> v = fm_pair_vals<float>(st, fp, ql, cl);
         const int64_t q = fp.row0[i] + p;
         const double *yp = fp.Y + ((size_t)gy * fp.Q + q) * 3 * CG + cl;
         const float G = (float)yp[0], Y1 = (float)yp[CG], Y2 = (float)yp[2 * CG];
@@ -917,9 +934,11 @@ __global__ void __launch_bounds__(256) k_fm_adj_pre(DevDb db, DevPot pot, const 
 // Kbar_s[d][c] += sum_{q,t} X[t][d][q] Ybar[q][t][c] over this CTA's run of
 // tiles, sub-tile by sub-tile of FM_SUB slots (all Dpad features of the three
 // kinds in shared memory, two sub-tiles in flight: cp.async fills one while
-// the other is consumed).  Thread: FM_ROWS consecutive features x 8
-// candidates as packed pairs of candidates; the FP32 sums of a tile are
-// added to this CTA's FP64 partial of the tile's atom type.
+// the other is consumed).  Thread: FM_ROWS features (every nds-th, so that
+// the threads of a warp read neighbouring rows) x 8 candidates as packed
+// pairs of candidates; the FP32 sums of a tile are added to this CTA's FP64
+// partial of the tile's atom type.  The operand of padding slots (past a
+// type's last real slot) is taken as zero.
 __host__ __device__ inline size_t fm_adj_smem(int Dpad, int CG) {
   return 2 * sizeof(float) * ((size_t)3 * Dpad * FM_SUB + (size_t)FM_SUB * 3 * CG);
 }
@@ -949,7 +968,11 @@ __global__ void __launch_bounds__(256, 1) k_fm_gemm_adj(FmPlan fp) {
     }
     const float *ysrc = fp.Yb + ((size_t)gy * fp.Q + qb) * 3 * CG;
     float *by = bx + xsz;
-    for (int i = tid * 4; i < (int)ysz; i += blockDim.x * 4) cp_async16(by + i, ysrc + i);
+    const int64_t qe = fp.qend[fm_tile_type(fp, (int)(qb / FM_TILE))];
+    for (int i = tid * 4; i < (int)ysz; i += blockDim.x * 4) {
+      if (qb + i / (3 * CG) < qe) cp_async16(by + i, ysrc + i);
+      else *reinterpret_cast<float4 *>(by + i) = make_float4(0.f, 0.f, 0.f, 0.f);
+    }
     cp_async_commit();
   };
   float2 acc[FM_ROWS][4];
@@ -975,7 +998,7 @@ __global__ void __launch_bounds__(256, 1) k_fm_gemm_adj(FmPlan fp) {
           float4 xv[FM_ROWS];
 #pragma unroll
           for (int r = 0; r < FM_ROWS; ++r)
-            xv[r] = *reinterpret_cast<const float4 *>(Xs + ((size_t)t * fp.Dpad + ds * FM_ROWS + r) * FM_SUB + qg);
+            xv[r] = *reinterpret_cast<const float4 *>(Xs + ((size_t)t * fp.Dpad + r * nds + ds) * FM_SUB + qg);
 #pragma unroll
           for (int qq = 0; qq < 4; ++qq) {
             const float *yq = Ys + ((size_t)(qg + qq) * 3 + t) * CG + cs * 8;
@@ -994,13 +1017,13 @@ __global__ void __launch_bounds__(256, 1) k_fm_gemm_adj(FmPlan fp) {
     }
     if ((k + 1) % NSUB == 0 && worker) {  // end of a tile: into the FP64 partial of its type
       const int s = fm_tile_type(fp, tb + k / NSUB);
-      double *kb = Kb + ((size_t)s * fp.Dpad + ds * FM_ROWS) * CG + cs * 8;
+      double *kb = Kb + ((size_t)s * fp.Dpad + ds) * CG + cs * 8;
 #pragma unroll
       for (int r = 0; r < FM_ROWS; ++r)
 #pragma unroll
         for (int c = 0; c < 4; ++c) {
-          kb[(size_t)r * CG + 2 * c] += (double)acc[r][c].x;
-          kb[(size_t)r * CG + 2 * c + 1] += (double)acc[r][c].y;
+          kb[(size_t)r * nds * CG + 2 * c] += (double)acc[r][c].x;
+          kb[(size_t)r * nds * CG + 2 * c + 1] += (double)acc[r][c].y;
           acc[r][c] = make_float2(0.f, 0.f);
         }
     }
