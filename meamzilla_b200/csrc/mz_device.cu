@@ -330,7 +330,7 @@ bool fm_prepare(mz_ctx *ctx) {
   const size_t G = fm.ngroups_max, CG = fm.CGmax, Cp = G * CG;
   const size_t Q = fp.Q, N = ctx->natoms, NC = ctx->ncells, Np = ctx->npairs, ns = ctx->nsplines;
   const size_t stride = ctx->stride;
-  fp.nctas_pre = std::max(1, std::min(fp.nblk, ctx->nsm));
+  fp.nctas_pre = std::max(1, std::min(fp.nblk, 2 * ctx->nsm));
   fp.nctas_adj = std::max(1, std::min(fp.ntiles, ctx->nsm));
   const size_t aux_rows = (size_t)ctx->pot.aux_rows;
   struct Need {
@@ -389,7 +389,7 @@ bool fm_prepare(mz_ctx *ctx) {
   smem_attr(k_fm_gemm_fwd<2>, fm_fwd_smem<2>(fp.Dpad));
   smem_attr(k_fm_gemm_fwd<4>, fm_fwd_smem<4>(fp.Dpad));
   smem_attr(k_fm_gemm_fwd<8>, fm_fwd_smem<8>(fp.Dpad));
-  fm.smem_pre = fm_pre_smem(ctx->nsplines, 64, fp.nt, fp.NB, 256);
+  fm.smem_pre = fm_pre_smem(ctx->nsplines, 64, fp.nt, fp.NB, fp.ustride);
   smem_attr(k_fm_adj_pre, fm.smem_pre);
   smem_attr(k_fm_epi, fm_epi_smem(ctx->nsplines, fp.nt, fp.NB, 64));
   smem_attr(k_fm_gemm_adj, fm_adj_smem(fp.Dpad, 64));
@@ -459,7 +459,7 @@ void enqueue_fm(mz_ctx *ctx, int n, double *d_obj, double *d_errvec, double *d_f
   if (!grad) return;
   {
     Bracket b(ctx, MZ_K_FM_PRE);
-    k_fm_adj_pre<<<dim3(fp.nctas_pre, G), 256, fm_pre_smem(ns, CG, fp.nt, fp.NB, 256), st>>>(
+    k_fm_adj_pre<<<dim3(fp.nctas_pre, G), 256, fm_pre_smem(ns, CG, fp.nt, fp.NB, fp.ustride), st>>>(
         ctx->db, ctx->pot, ctx->d_geom, ctx->d_tabs, fp, n);
     ck(cudaGetLastError(), "k_fm_adj_pre launch");
   }
@@ -1170,6 +1170,9 @@ mz_status mz_create(const mz_db *dbh, const mz_pot *poth, const mz_settings *set
           fp.NA = NA;
           fp.NN = NN;
           fp.NB = NBp;
+          // the U splines are consecutive in the knot table
+          fp.utoff = im.geom[dp.s_U].toff;
+          fp.ustride = im.geom[dp.s_U + pot.ntypes - 1].toff + 2 * im.geom[dp.s_U + pot.ntypes - 1].n + 2 - fp.utoff;
           fp.D = pot.ntypes * NA * NN;
           fp.Dpad = (fp.D + FM_DC - 1) / FM_DC * FM_DC;
           fp.nch = fp.Dpad / FM_DC;

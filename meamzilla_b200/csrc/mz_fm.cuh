@@ -61,6 +61,7 @@ struct FmPlan {
   int tile0[FM_MAXT + 1];  // first tile of each type
   int64_t qend[FM_MAXT];   // end of each type's real slots (the rest of its last tile is padding)
   int NB;          // B-spline coefficients of the phi, rho and f splines (the largest)
+  int utoff, ustride;  // the U splines' part of a knot table: its offset and length
   int nblk;        // atom blocks of the adjoint epilogue (type-pure, <= 256 slots, <= 64 atoms)
   const int *blk0;         // [nblk + 1] into adj_atoms
   const int *row0;         // [N] feature slot of each atom's first pair
@@ -740,81 +741,56 @@ __global__ void k_fm_cells(DevDb db, DevPot pot, FmPlan fp, int ncand, double *_
 // (into Yb for k_fm_gemm_adj), and the pair functions' (value, slope) weights
 //   phi: (eps / 2, a_p / 2), rho: (chi, U' a_p),
 //   f:   (chi G_p / 2 + U' (Lambda.e1 Y1 + Lambda.e2 Y2) / r_p, U' a_p G_p)
-// (f's role as the partner k goes through the contraction).  Phase 1: one
-// task per (atom, candidate) gives K_i and chi_i; phase 2: one task per
-// (slot, candidate) writes dL/dY and adds the pair-function weights times the
-// slot's four B-spline basis values into the thread's own FP32 coefficient
-// sums in shared memory (so no two threads add to the same word).  The
-// threads' sums are combined, in thread order, into this CTA's FP64 partials
-// at a change of atom type and every FM_PFLUSH blocks; the embedding table
-// gradient (value weight eps, slope weight K_i) is added per atom, in atom
-// order, by the thread of each candidate, in FP64.  Fixed order throughout.
+// (f's role as the partner k goes through the contraction).  One task per
+// (atom, candidate) walks the atom's row twice: K_i and chi_i, then dL/dY and
+// the pair-function weights times the slot's four B-spline basis values,
+// added into the CTA's FP32 coefficient sums in shared memory; the embedding
+// table gradient (value weight eps, slope weight K_i) goes into the CTA's
+// FP64 table sums.  Both use shared-memory atomics (the lanes of a warp add
+// to different candidates' words; the order of additions from different
+// warps is not fixed, so this gradient is reproducible to FP32 rounding, not
+// bit for bit).  The sums go to this CTA's FP64 partials at a change of atom
+// type, every FM_PFLUSH blocks and at the end.
 constexpr int FM_PFLUSH = 4;  // blocks between flushes of the pair-function sums
 
-__host__ __device__ inline size_t fm_pre_smem(int nsplines, int CG, int nt, int NB, int threads) {
+__host__ __device__ inline size_t fm_pre_smem(int nsplines, int CG, int nt, int NB, int ustride) {
   size_t b = (fm_stage_bytes<float>(nt, NB, CG) + 15) & ~size_t(15);
-  b += sizeof(float) * 3 * (size_t)FM_ABLK * CG;
-  b = (b + 15) & ~size_t(15);
   b += sizeof(SplineGeom) * (size_t)nsplines;
   b = (b + 15) & ~size_t(15);
-  b += sizeof(float) * (size_t)3 * nt * NB * threads;
+  b += sizeof(double) * (size_t)ustride * CG;
+  b += sizeof(float) * (size_t)3 * nt * NB * CG;
   return b;
 }
 
-__device__ __forceinline__ void fm_lambda(const FmPlan &fp, int N, int NC, int gy, int cl, int i, int j, int cell,
-                                          float ux, float uy, float uz, float r, float &lx, float &ly, float &lz) {
-  const int CG = fp.CG;
-  const float *Li = fp.lamf + ((size_t)gy * N + i) * 3 * CG + cl;
-  const float *Lj = fp.lamf + ((size_t)gy * N + j) * 3 * CG + cl;
-  const double *sd = fp.seedF + ((size_t)gy * NC + cell) * CS_COUNT * CG + cl;
-  const float mxx = (float)sd[(CS_MU0 + 0) * CG], myy = (float)sd[(CS_MU0 + 1) * CG],
-              mzz = (float)sd[(CS_MU0 + 2) * CG], mxy = (float)sd[(CS_MU0 + 3) * CG],
-              myz = (float)sd[(CS_MU0 + 4) * CG], mzx = (float)sd[(CS_MU0 + 5) * CG];
-  lx = Li[0] - Lj[0] - r * (mxx * ux + mzx * uz);
-  ly = Li[CG] - Lj[CG] - r * (myy * uy + mxy * ux);
-  lz = Li[2 * CG] - Lj[2 * CG] - r * (mzz * uz + myz * uy);
-}
-
-__global__ void __launch_bounds__(256) k_fm_adj_pre(DevDb db, DevPot pot, const SplineGeom *__restrict__ geom,
-                                                   const double *__restrict__ tabs, FmPlan fp, int ncand) {
+__global__ void __launch_bounds__(256, 2) k_fm_adj_pre(DevDb db, DevPot pot, const SplineGeom *__restrict__ geom,
+                                                      const double *__restrict__ tabs, FmPlan fp, int ncand) {
   extern __shared__ __align__(16) unsigned char fm_raw[];
   const int gy = blockIdx.y, CG = fp.CG, N = db.natoms, NC = db.ncells;
   const int tid = threadIdx.x, T = blockDim.x;
   const FmStage<float> st = fm_stage_carve<float>(fm_raw, fp);
   size_t off = (fm_stage_bytes<float>(fp.nt, fp.NB, CG) + 15) & ~size_t(15);
-  float *chi = reinterpret_cast<float *>(fm_raw + off);
-  float *dFs = chi + FM_ABLK * CG;
-  float *Ks = dFs + FM_ABLK * CG;
-  off += sizeof(float) * 3 * (size_t)FM_ABLK * CG;
-  off = (off + 15) & ~size_t(15);
   SplineGeom *sg = reinterpret_cast<SplineGeom *>(fm_raw + off);
   off += sizeof(SplineGeom) * (size_t)pot.nsplines;
   off = (off + 15) & ~size_t(15);
-  float *pacc = reinterpret_cast<float *>(fm_raw + off);  // entry e of thread t at e T + t
+  // embedding tables of the candidates: the U splines' slices, [CG][ustride]
+  double *utab = reinterpret_cast<double *>(fm_raw + off);
+  float *pacc = reinterpret_cast<float *>(utab + (size_t)fp.ustride * CG);  // [3][nt][NB][CG]
   const int npe = 3 * fp.nt * fp.NB;
   for (int sidx = tid; sidx < pot.nsplines; sidx += T) sg[sidx] = geom[sidx];
-  for (int e = 0; e < npe; ++e) pacc[(size_t)e * T + tid] = 0.f;
-  const int cl = tid % CG, set = tid / CG, nsets = T / CG;
-  const int c = gy * CG + cl;
-  const bool live = c < ncand;
-  const double *tc = tabs + (size_t)(live ? c : 0) * pot.tab_stride;
+  for (int e = tid; e < npe * CG; e += T) pacc[e] = 0.f;
+  for (int e = tid; e < fp.ustride * CG; e += T) utab[e] = 0.0;
   double *Pb = fp.Pbar + ((size_t)gy * gridDim.x + blockIdx.x) * pot.nsplines * FM_MAXB * CG;
   double *Tb = fp.Tbar + ((size_t)gy * gridDim.x + blockIdx.x) * CG * pot.tab_stride;
   for (int i = tid; i < pot.nsplines * FM_MAXB * CG; i += T) Pb[i] = 0.0;
   for (int i = tid; i < CG * pot.tab_stride; i += T) Tb[i] = 0.0;
-  // the threads' sums of atom type tf into the FP64 partial, threads in order
+  // the CTA's sums of atom type tf into its FP64 partials
   auto flush_pairs = [&](int tf) {
     __syncthreads();
     for (int idx = tid; idx < npe * CG; idx += T) {
       const int e = idx / CG, c2 = idx % CG;
       const int F = e / (fp.nt * fp.NB), o = (e / fp.NB) % fp.nt, a = e % fp.NB;
-      float *pe = pacc + (size_t)e * T + c2;
-      double v = 0.0;
-      for (int k = 0; k < nsets; ++k) {
-        v += (double)pe[k * CG];
-        pe[k * CG] = 0.f;
-      }
-      Pb[((size_t)fm_pair_spline(pot, F, tf, o) * FM_MAXB + a) * CG + c2] += v;
+      Pb[((size_t)fm_pair_spline(pot, F, tf, o) * FM_MAXB + a) * CG + c2] += (double)pacc[idx];
+      pacc[idx] = 0.f;
     }
     __syncthreads();
   };
@@ -829,16 +805,28 @@ __global__ void __launch_bounds__(256) k_fm_adj_pre(DevDb db, DevPot pot, const 
       since = 0;
     }
     int na, ti;
-    const int nslot = fm_stage_block<float>(db, pot, sg, fp, st, blk, gy, ncand, na, ti);
+    fm_stage_block<float>(db, pot, sg, fp, st, blk, gy, ncand, na, ti);
     pacc_t = ti;
     ++since;
     const SplineGeom &gU = sg[pot.s_U + ti];
-    // ---- phase 1: K_i and chi_i, one task per (atom, candidate)
-    for (int task = tid; task < na * CG && live; task += T) {
-      const int a = task / CG;
+    for (int task = tid; task < na * CG; task += T) {
+      const int a = task / CG, cl = task % CG;
+      const int c = gy * CG + cl;
+      if (c >= ncand) continue;
+      const double *tc = tabs + (size_t)c * pot.tab_stride;
       const int i = st.satom[a], lo = st.arow[a], n = st.arow[a + 1] - lo;
       const int cell = db.atom_cell[i];
-      const double *Yq = fp.Y + ((size_t)gy * fp.Q + fp.row0[i]) * 3 * CG + cl;
+      const int64_t q0 = fp.row0[i];
+      const double *Yq = fp.Y + ((size_t)gy * fp.Q + q0) * 3 * CG + cl;
+      float *Ybq = fp.Yb + ((size_t)gy * fp.Q + q0) * 3 * CG + cl;
+      // the atom's and its cell's candidate data
+      const float *Li = fp.lamf + ((size_t)gy * N + i) * 3 * CG + cl;
+      const float lix = Li[0], liy = Li[CG], liz = Li[2 * CG];
+      const double *sd = fp.seedF + ((size_t)gy * NC + cell) * CS_COUNT * CG + cl;
+      const float mxx = (float)sd[(CS_MU0 + 0) * CG], myy = (float)sd[(CS_MU0 + 1) * CG],
+                  mzz = (float)sd[(CS_MU0 + 2) * CG], mxy = (float)sd[(CS_MU0 + 3) * CG],
+                  myz = (float)sd[(CS_MU0 + 4) * CG], mzx = (float)sd[(CS_MU0 + 5) * CG];
+      const double eps = sd[CS_EPS * CG], kap = sd[CS_KAPPA * CG];
       const double rho = fp.aoutF[((size_t)gy * N + i) * AO_COUNT * CG + AO_RHO * CG + cl];
       const double w = db.cell_w[cell];
       double rt = rho, dpen = 0.0, drt = 1.0;
@@ -850,6 +838,14 @@ __global__ void __launch_bounds__(256) k_fm_adj_pre(DevDb db, DevPot pot, const 
         if (!pot.embed_extrap) { rt = gU.xN; drt = 0.0; }
       }
       const PointEval U = spl_point(tc, gU, rt);
+      auto lam = [&](int ql, const float4 &u, float &lx, float &ly, float &lz) {
+        const float *Lj = fp.lamf + ((size_t)gy * N + st.nbr[ql]) * 3 * CG + cl;
+        const float r = 1.f / u.w;
+        lx = lix - Lj[0] - r * (mxx * u.x + mzx * u.z);
+        ly = liy - Lj[CG] - r * (myy * u.y + mxy * u.x);
+        lz = liz - Lj[2 * CG] - r * (mzz * u.z + myz * u.y);
+      };
+      // ---- pass 1: K_i
       double K = 0.0;
 #pragma unroll 2
       for (int p = 0; p < n; ++p) {
@@ -859,57 +855,35 @@ __global__ void __launch_bounds__(256) k_fm_adj_pre(DevDb db, DevPot pot, const 
         const float4 u = st.uf[ql];
         const double *e = st.e + ql * 6;
         float lx, ly, lz;
-        fm_lambda(fp, N, NC, gy, cl, i, st.nbr[ql], cell, u.x, u.y, u.z, 1.f / u.w, lx, ly, lz);
+        lam(ql, u, lx, ly, lz);
         const double ap = lx * u.x + ly * u.y + lz * u.z;
         const double l1 = lx * e[0] + ly * e[1] + lz * e[2], l2 = lx * e[3] + ly * e[4] + lz * e[5];
         K += ap * ((double)v.drho + (double)v.df * yp[0]) + (double)v.f * (double)u.w * (l1 * yp[CG] + l2 * yp[2 * CG]);
       }
-      const double *sd = fp.seedF + ((size_t)gy * NC + cell) * CS_COUNT * CG + cl;
-      const double eps = sd[CS_EPS * CG], kap = sd[CS_KAPPA * CG];
-      chi[a * CG + cl] = (float)((eps * U.grad + U.grad2 * K) * drt + kap * dpen);
-      dFs[a * CG + cl] = (float)U.grad;
-      Ks[a * CG + cl] = (float)K;
-    }
-    __syncthreads();
-    // ---- embedding table gradients: the thread of each candidate, atoms in order
-    if (set == 0 && live) {
-      double *tb = Tb + (size_t)cl * pot.tab_stride + gU.toff;
-      for (int a = 0; a < na; ++a) {
-        const int i = st.satom[a];
-        const double rho = fp.aoutF[((size_t)gy * N + i) * AO_COUNT * CG + AO_RHO * CG + cl];
-        const double rt = pot.embed_extrap ? rho : (rho < gU.x0 ? gU.x0 : (rho > gU.xN ? gU.xN : rho));
-        const PointEval U = spl_point(tc, gU, rt);
-        const double eps = fp.seedF[((size_t)gy * NC + db.atom_cell[i]) * CS_COUNT * CG + CS_EPS * CG + cl];
-        spl_point_adjoint(gU, U, rt, eps, (double)Ks[a * CG + cl], [&](int ix, double x) { tb[ix] += x; });
-      }
-    }
-    // ---- phase 2: dL/dY into Yb and the pair-function gradients, one task per (slot, candidate)
-    if (live) {
-      int a = 0;
-      for (int ql = set; ql < nslot; ql += nsets) {
-        while (a + 1 < na && st.arow[a + 1] <= ql) ++a;
-        const int i = st.satom[a];
-        const int p = ql - st.arow[a];
-        const int cell = db.atom_cell[i];
+      const float ch = (float)((eps * U.grad + U.grad2 * K) * drt + kap * dpen);
+      const float dF = (float)U.grad;
+      spl_point_adjoint(gU, U, rt, eps, K,
+                        [&](int ix, double x) { atomicAdd(utab + (size_t)cl * fp.ustride + (gU.toff - fp.utoff) + ix, x); });
+      // ---- pass 2: dL/dY and the pair-function gradients
+      const float epsf = (float)eps;
+#pragma unroll 2
+      for (int p = 0; p < n; ++p) {
+        const int ql = lo + p;
         const FmPairVals<float> v = fm_pair_vals<float>(st, fp, ql, cl);
-        const int64_t q = fp.row0[i] + p;
-        const double *yp = fp.Y + ((size_t)gy * fp.Q + q) * 3 * CG + cl;
+        const double *yp = Yq + (size_t)p * 3 * CG;
         const float G = (float)yp[0], Y1 = (float)yp[CG], Y2 = (float)yp[2 * CG];
         const float4 u = st.uf[ql];
         const double *e = st.e + ql * 6;
         float lx, ly, lz;
-        fm_lambda(fp, N, NC, gy, cl, i, st.nbr[ql], cell, u.x, u.y, u.z, 1.f / u.w, lx, ly, lz);
+        lam(ql, u, lx, ly, lz);
         const float ap = lx * u.x + ly * u.y + lz * u.z;
         const float l1 = (float)(lx * e[0] + ly * e[1] + lz * e[2]), l2 = (float)(lx * e[3] + ly * e[4] + lz * e[5]);
-        const float ch = chi[a * CG + cl], dF = dFs[a * CG + cl];
-        const float eps = (float)fp.seedF[((size_t)gy * NC + cell) * CS_COUNT * CG + CS_EPS * CG + cl];
         const float B = dF * v.f * u.w;
-        float *yb = fp.Yb + ((size_t)gy * fp.Q + q) * 3 * CG + cl;
+        float *yb = Ybq + (size_t)p * 3 * CG;
         yb[0] = 0.5f * v.f * ch + ap * dF * v.df;
         yb[CG] = B * l1;
         yb[2 * CG] = B * l2;
-        // (value, slope) weights of phi, rho, f times the basis values
-        const float wv[3] = {0.5f * eps, ch, 0.5f * ch * G + dF * (l1 * Y1 + l2 * Y2) * u.w};
+        const float wv[3] = {0.5f * epsf, ch, 0.5f * ch * G + dF * (l1 * Y1 + l2 * Y2) * u.w};
         const float wd[3] = {0.5f * ap, dF * ap, dF * ap * G};
         const int kn = st.kn[ql], tj = st.tj[ql];
 #pragma unroll
@@ -917,16 +891,21 @@ __global__ void __launch_bounds__(256) k_fm_adj_pre(DevDb db, DevPot pot, const 
           const int k = ((kn >> (8 * F)) & 0xff) - 1;
           if (k < 0) continue;
           const float *bs = st.bas + (ql * 3 + F) * 8;
-          float *pe = pacc + ((size_t)(F * fp.nt + tj) * fp.NB + k) * T + tid;
-          pe[0] += wv[F] * bs[0] + wd[F] * bs[4];
-          pe[T] += wv[F] * bs[1] + wd[F] * bs[5];
-          pe[2 * T] += wv[F] * bs[2] + wd[F] * bs[6];
-          pe[3 * T] += wv[F] * bs[3] + wd[F] * bs[7];
+          float *pe = pacc + ((size_t)(F * fp.nt + tj) * fp.NB + k) * CG + cl;
+          atomicAdd(pe, wv[F] * bs[0] + wd[F] * bs[4]);
+          atomicAdd(pe + CG, wv[F] * bs[1] + wd[F] * bs[5]);
+          atomicAdd(pe + 2 * CG, wv[F] * bs[2] + wd[F] * bs[6]);
+          atomicAdd(pe + 3 * CG, wv[F] * bs[3] + wd[F] * bs[7]);
         }
       }
     }
   }
   if (pacc_t >= 0) flush_pairs(pacc_t);
+  // the embedding table sums into this CTA's partial
+  for (int idx = tid; idx < fp.ustride * CG; idx += T) {
+    const int c2 = idx / fp.ustride, e = idx % fp.ustride;
+    Tb[(size_t)c2 * pot.tab_stride + fp.utoff + e] = utab[idx];
+  }
 }
 
 // ---------------------------------------------------------- k_fm_gemm_adj
