@@ -330,7 +330,7 @@ bool fm_prepare(mz_ctx *ctx) {
   const size_t G = fm.ngroups_max, CG = fm.CGmax, Cp = G * CG;
   const size_t Q = fp.Q, N = ctx->natoms, NC = ctx->ncells, Np = ctx->npairs, ns = ctx->nsplines;
   const size_t stride = ctx->stride;
-  fp.nctas_pre = std::max(1, std::min(fp.nblk, 2 * ctx->nsm));
+  fp.nctas_pre = std::max(1, std::min(fp.nblk, 3 * ctx->nsm));
   fp.nctas_adj = std::max(1, std::min(fp.ntiles, ctx->nsm));
   const size_t aux_rows = (size_t)ctx->pot.aux_rows;
   struct Need {
@@ -433,7 +433,7 @@ void enqueue_fm(mz_ctx *ctx, int n, double *d_obj, double *d_errvec, double *d_f
   const unsigned ablocks = (unsigned)(((int64_t)N * CG + 255) / 256);
   {
     Bracket b(ctx, MZ_K_FM_EPI);
-    const int eb = std::max(1, std::min(fp.nblk, 4 * ctx->nsm));
+    const int eb = std::max(1, std::min(fp.nblk, 8 * ctx->nsm));
     k_fm_epi<<<dim3(eb, G), 256, fm_epi_smem(ns, fp.nt, fp.NB, CG), st>>>(ctx->db, ctx->pot, ctx->d_geom,
                                                                          ctx->d_tabs, fp, n);
     ck(cudaGetLastError(), "k_fm_epi launch");
@@ -1194,8 +1194,25 @@ mz_status mz_create(const mz_db *dbh, const mz_pot *poth, const mz_settings *set
           for (int t = pot.ntypes; t <= FM_MAXT; ++t) fp.tile0[t] = fp.ntiles;
           if (q < (int64_t(1) << 31) && tix == N) {
             fp.row0 = dupload(ctx, row0.data(), row0.size());
-            fp.nblk = ctx->nadjblk[0];
-            fp.blk0 = ctx->d_adjblk[0];
+            // the epilogues' atom blocks: type-pure runs of the type-sorted
+            // order, <= BLOCK_SLOTS slots and <= FM_ABLK atoms
+            std::vector<int> b0(1, 0);
+            int slots = 0, atoms = 0, ty = -1;
+            for (int qa = 0; qa < N; ++qa) {
+              const int i = order[qa];
+              const int nr = (int)(db.pair_off[i + 1] - db.pair_off[i]);
+              if (atoms > 0 && (db.atom_type[i] != ty || slots + nr > BLOCK_SLOTS || atoms + 1 > FM_ABLK)) {
+                b0.push_back(qa);
+                slots = 0;
+                atoms = 0;
+              }
+              ty = db.atom_type[i];
+              slots += nr;
+              atoms += 1;
+            }
+            b0.push_back(N);
+            fp.nblk = (int)b0.size() - 1;
+            fp.blk0 = dupload(ctx, b0.data(), b0.size());
             ctx->fm.eligible = true;
           }
         }

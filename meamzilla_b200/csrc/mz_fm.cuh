@@ -62,7 +62,7 @@ struct FmPlan {
   int64_t qend[FM_MAXT];   // end of each type's real slots (the rest of its last tile is padding)
   int NB;          // B-spline coefficients of the phi, rho and f splines (the largest)
   int utoff, ustride;  // the U splines' part of a knot table: its offset and length
-  int nblk;        // atom blocks of the adjoint epilogue (type-pure, <= 256 slots, <= 64 atoms)
+  int nblk;        // atom blocks of the epilogues (type-pure, <= BLOCK_SLOTS slots, <= FM_ABLK atoms)
   const int *blk0;         // [nblk + 1] into adj_atoms
   const int *row0;         // [N] feature slot of each atom's first pair
   const float *X;
@@ -287,8 +287,10 @@ __global__ void k_fm_kmat(int ncand, DevPot pot, FmPlan fp, const double *__rest
 // slots (one atom type s) and one group of CG = 8 NW candidates.  Thread
 // (lane, warp): slots 2 lane and 2 lane + 1, candidates 8 warp .. 8 warp + 7,
 // all three kinds.  Each chunk of FM_DC features is summed in FP32 (packed
-// pairs of slots) and added to FP64 totals, which are stored in FP64, so a
-// sum carries the rounding of FM_DC terms, not of all Dpad.  The moments stream through a double buffer
+// pairs of slots) and added to a compensated FP32 total (TwoSum: the total
+// and the exact rounding error of each addition, packed pairs), stored as
+// their FP64 sum, so a sum carries the rounding of FM_DC terms, not of all
+// Dpad.  The moments stream through a double buffer
 // filled by cp.async; K_s stays in shared memory for the whole tile.
 template <int NW>
 __host__ __device__ constexpr size_t fm_fwd_smem(int Dpad) {
@@ -317,13 +319,14 @@ __global__ void __launch_bounds__(NW * 32, 1) k_fm_gemm_fwd(FmPlan fp) {
     cp_async_commit();
   };
   load_chunk(0, 0);
-  double tot[3][2][8];  // [kind][slot][candidate]
+  float2 tot[3][8], cmp[3][8];  // [kind][candidate]: (slot 2 lane, slot 2 lane + 1), total and its error
 #pragma unroll
   for (int t = 0; t < 3; ++t)
 #pragma unroll
-    for (int h = 0; h < 2; ++h)
-#pragma unroll
-      for (int c = 0; c < 8; ++c) tot[t][h][c] = 0.0;
+    for (int c = 0; c < 8; ++c) {
+      tot[t][c] = make_float2(0.f, 0.f);
+      cmp[t][c] = make_float2(0.f, 0.f);
+    }
   for (int ch = 0; ch < fp.nch; ++ch) {
     if (ch + 1 < fp.nch) {
       load_chunk(ch + 1, (ch + 1) & 1);
@@ -351,12 +354,17 @@ __global__ void __launch_bounds__(NW * 32, 1) k_fm_gemm_fwd(FmPlan fp) {
         for (int c = 0; c < 8; ++c) acc[t][c] = fma2(xv, bcast2(kk[c]), acc[t][c]);
       }
     }
+    // TwoSum (Knuth): s = a + b exactly as s + err
 #pragma unroll
     for (int t = 0; t < 3; ++t)
 #pragma unroll
       for (int c = 0; c < 8; ++c) {
-        tot[t][0][c] += (double)acc[t][c].x;
-        tot[t][1][c] += (double)acc[t][c].y;
+        const float2 a = tot[t][c], b = acc[t][c];
+        const float2 sum = add2(a, b);
+        const float2 bb = add2(sum, make_float2(-a.x, -a.y));
+        const float2 err = add2(add2(a, make_float2(-(sum.x - bb.x), -(sum.y - bb.y))), add2(b, make_float2(-bb.x, -bb.y)));
+        tot[t][c] = sum;
+        cmp[t][c] = add2(cmp[t][c], err);
       }
     __syncthreads();
   }
@@ -367,8 +375,12 @@ __global__ void __launch_bounds__(NW * 32, 1) k_fm_gemm_fwd(FmPlan fp) {
     for (int t = 0; t < 3; ++t) {
       double *dst = Yo + ((size_t)h * 3 + t) * CG;
 #pragma unroll
-      for (int c = 0; c < 8; c += 2)
-        *reinterpret_cast<double2 *>(dst + c) = make_double2(tot[t][h][c], tot[t][h][c + 1]);
+      for (int c = 0; c < 8; c += 2) {
+        const double v0 = h ? (double)tot[t][c].y + (double)cmp[t][c].y : (double)tot[t][c].x + (double)cmp[t][c].x;
+        const double v1 =
+            h ? (double)tot[t][c + 1].y + (double)cmp[t][c + 1].y : (double)tot[t][c + 1].x + (double)cmp[t][c + 1].x;
+        *reinterpret_cast<double2 *>(dst + c) = make_double2(v0, v1);
+      }
     }
 }
 
@@ -381,33 +393,39 @@ __global__ void __launch_bounds__(NW * 32, 1) k_fm_gemm_fwd(FmPlan fp) {
 // frame (e1, e2), and the B-spline basis values (and d/dr) of phi, rho and f
 // at its shifts; and the pair splines' B-spline coefficients of the block's
 // atom type for the group's candidates.
-constexpr int FM_ABLK = 64;  // atoms per block of the epilogues
+constexpr int FM_ABLK = 4;   // atoms per block of the epilogues: 4 x 64 candidates fill 256 threads
 
 template <typename R>
 struct FmStage {
   int *satom, *arow;  // [FM_ABLK], [FM_ABLK + 1]
   int *gs, *nbr, *tj, *kn;  // [BLOCK_SLOTS]
+  int *ctype;         // type whose coefficients are staged (-1: none yet)
   float4 *uf;         // [BLOCK_SLOTS] (ux, uy, uz, 1/r)
   double *e;          // [BLOCK_SLOTS][6] e1, e2
+  double4 *ur;        // [BLOCK_SLOTS] (ux, uy, uz, r) in FP64
   R *bas;             // [BLOCK_SLOTS][3][8] basis N0..N3 and d/dr N0'..N3' of phi, rho, f
   R *coef;            // [3][nt][NB][CG]
 };
 
 template <typename R>
 __host__ __device__ inline size_t fm_stage_bytes(int nt, int NB, int CG) {
-  return sizeof(int) * (2 * FM_ABLK + 1 + 4 * BLOCK_SLOTS) + 16 + sizeof(float4) * BLOCK_SLOTS +
-         sizeof(double) * 6 * BLOCK_SLOTS + sizeof(R) * 24 * BLOCK_SLOTS + sizeof(R) * 3 * nt * NB * CG;
+  return sizeof(int) * (2 * FM_ABLK + 2 + 4 * BLOCK_SLOTS) + 16 + (sizeof(R) == 4 ? sizeof(float4) * BLOCK_SLOTS : 0) +
+         sizeof(double4) * BLOCK_SLOTS + sizeof(double) * 6 * BLOCK_SLOTS + sizeof(R) * 24 * BLOCK_SLOTS +
+         sizeof(R) * 3 * nt * NB * CG;
 }
 
 // carves the staging arrays out of shared memory at `base` (16-byte aligned)
 template <typename R>
 __device__ __forceinline__ FmStage<R> fm_stage_carve(unsigned char *base, const FmPlan &fp) {
   FmStage<R> st;
-  double *e = reinterpret_cast<double *>(base);
+  double4 *ur = reinterpret_cast<double4 *>(base);
+  st.ur = ur;
+  double *e = reinterpret_cast<double *>(ur + BLOCK_SLOTS);
   st.e = e;
+  // the FP32 unit vectors only where the FP32 epilogue reads them
   float4 *uf = reinterpret_cast<float4 *>(e + 6 * BLOCK_SLOTS);
   st.uf = uf;
-  R *bas = reinterpret_cast<R *>(uf + BLOCK_SLOTS);
+  R *bas = reinterpret_cast<R *>(uf + (sizeof(R) == 4 ? BLOCK_SLOTS : 0));
   st.bas = bas;
   R *coef = bas + 24 * BLOCK_SLOTS;
   st.coef = coef;
@@ -418,6 +436,7 @@ __device__ __forceinline__ FmStage<R> fm_stage_carve(unsigned char *base, const 
   st.nbr = st.gs + BLOCK_SLOTS;
   st.tj = st.nbr + BLOCK_SLOTS;
   st.kn = st.tj + BLOCK_SLOTS;
+  st.ctype = st.kn + BLOCK_SLOTS;
   return st;
 }
 
@@ -461,7 +480,8 @@ __device__ int fm_stage_block(const DevDb &db, const DevPot &pot, const SplineGe
     st.tj[ql] = tj;
     const int kn = db.pair_knot[gs];
     st.kn[ql] = kn;
-    st.uf[ql] = make_float4(db.pair_uxf[gs], db.pair_uyf[gs], db.pair_uzf[gs], 1.f / db.pair_rf[gs]);
+    if (sizeof(R) == 4) st.uf[ql] = make_float4(db.pair_uxf[gs], db.pair_uyf[gs], db.pair_uzf[gs], 1.f / db.pair_rf[gs]);
+    st.ur[ql] = make_double4(db.pair_ux[gs], db.pair_uy[gs], db.pair_uz[gs], db.pair_r[gs]);
     const double *e = fp.E + (size_t)(fp.row0[i] + p) * 8;
 #pragma unroll
     for (int k = 0; k < 6; ++k) st.e[ql * 6 + k] = e[k];
@@ -482,7 +502,12 @@ __device__ int fm_stage_block(const DevDb &db, const DevPot &pot, const SplineGe
       }
     }
   }
-  const int ncf = 3 * fp.nt * fp.NB * CG;
+  // the pair coefficients of the block's type (consecutive blocks of a CTA
+  // are mostly of one type: restaged only at a change)
+  const bool restage = *st.ctype != ti;
+  __syncthreads();
+  const int ncf = restage ? 3 * fp.nt * fp.NB * CG : 0;
+  if (restage && tid == 0) *st.ctype = ti;
   for (int idx = tid; idx < ncf; idx += T) {
     const int cl = idx % CG, a = (idx / CG) % fp.NB, o = (idx / (CG * fp.NB)) % fp.nt, F = idx / (CG * fp.NB * fp.nt);
     const int sp = fm_pair_spline(pot, F, ti, o);
@@ -545,6 +570,7 @@ __global__ void __launch_bounds__(256) k_fm_epi(DevDb db, DevPot pot, const Spli
   const int gy = blockIdx.y, CG = fp.CG, N = db.natoms;
   const int tid = threadIdx.x, T = blockDim.x;
   for (int s = tid; s < pot.nsplines; s += T) sg[s] = geom[s];
+  if (tid == 0) *st.ctype = -1;
   const int cl = tid % CG;
   const int c = gy * CG + cl;
   const bool live = c < ncand;
@@ -587,7 +613,8 @@ __global__ void __launch_bounds__(256) k_fm_epi(DevDb db, DevPot pot, const Spli
         const double G = yp[0], Y1 = yp[CG], Y2 = yp[2 * CG];
         const double *e = st.e + ql * 6;
         const int64_t gs = st.gs[ql];
-        const double rr = db.pair_r[gs], dx = db.pair_ux[gs], dy = db.pair_uy[gs], dz = db.pair_uz[gs];
+        const double4 ur = st.ur[ql];
+        const double rr = ur.w, dx = ur.x, dy = ur.y, dz = ur.z;
         const double A = 0.5 * v.dphi + dF * (v.drho + v.df * G);
         const double B = dF * v.f / rr;
         const double Vx = dx * A + B * (e[0] * Y1 + e[3] * Y2);
@@ -777,6 +804,7 @@ __global__ void __launch_bounds__(256, 2) k_fm_adj_pre(DevDb db, DevPot pot, con
   float *pacc = reinterpret_cast<float *>(utab + (size_t)fp.ustride * CG);  // [3][nt][NB][CG]
   const int npe = 3 * fp.nt * fp.NB;
   for (int sidx = tid; sidx < pot.nsplines; sidx += T) sg[sidx] = geom[sidx];
+  if (tid == 0) *st.ctype = -1;
   for (int e = tid; e < npe * CG; e += T) pacc[e] = 0.f;
   for (int e = tid; e < fp.ustride * CG; e += T) utab[e] = 0.0;
   double *Pb = fp.Pbar + ((size_t)gy * gridDim.x + blockIdx.x) * pot.nsplines * FM_MAXB * CG;
@@ -912,20 +940,22 @@ __global__ void __launch_bounds__(256, 2) k_fm_adj_pre(DevDb db, DevPot pot, con
 
 // Kbar_s[d][c] += sum_{q,t} X[t][d][q] Ybar[q][t][c] over this CTA's run of
 // tiles, sub-tile by sub-tile of FM_SUB slots (all Dpad features of the three
-// kinds in shared memory, two sub-tiles in flight: cp.async fills one while
-// the other is consumed).  Thread: FM_ROWS features (every nds-th, so that
-// the threads of a warp read neighbouring rows) x 8 candidates as packed
-// pairs of candidates; the FP32 sums of a tile are added to this CTA's FP64
+// kinds in shared memory at an 80-byte row stride, two sub-tiles in flight:
+// cp.async fills one while the other is consumed).  Thread: FM_ROWS features
+// (every nds-th, so that the threads of a warp read neighbouring rows) x 8
+// candidates (four from each half of the group, so that the threads of a
+// warp read one contiguous 128-byte run) as packed pairs of candidates; the FP32 sums of a tile are added to this CTA's FP64
 // partial of the tile's atom type.  The operand of padding slots (past a
 // type's last real slot) is taken as zero.
+constexpr int FM_XS = FM_SUB + 4;  // shared-memory row stride of the moments (80 B: no bank aliasing)
 __host__ __device__ inline size_t fm_adj_smem(int Dpad, int CG) {
-  return 2 * sizeof(float) * ((size_t)3 * Dpad * FM_SUB + (size_t)FM_SUB * 3 * CG);
+  return 2 * sizeof(float) * ((size_t)3 * Dpad * FM_XS + (size_t)FM_SUB * 3 * CG);
 }
 
 __global__ void __launch_bounds__(256, 1) k_fm_gemm_adj(FmPlan fp) {
   extern __shared__ __align__(16) float asm_[];
   const int CG = fp.CG, gy = blockIdx.y;
-  const size_t xsz = (size_t)3 * fp.Dpad * FM_SUB, ysz = (size_t)FM_SUB * 3 * CG;
+  const size_t xsz = (size_t)3 * fp.Dpad * FM_XS, ysz = (size_t)FM_SUB * 3 * CG;
   const int tid = threadIdx.x;
   const int ncs = CG / 8, nds = fp.Dpad / FM_ROWS;
   const int cs = tid % ncs, ds = tid / ncs;
@@ -943,7 +973,7 @@ __global__ void __launch_bounds__(256, 1) k_fm_gemm_adj(FmPlan fp) {
       const int row = i / (FM_SUB / 4), col = (i % (FM_SUB / 4)) * 4;
       const int t = row / fp.Dpad, d = row % fp.Dpad;
       const size_t grow = (size_t)((d / FM_DC) * 3 + t) * FM_DC + d % FM_DC;
-      cp_async16(bx + (size_t)row * FM_SUB + col, fp.X + grow * fp.Q + qb + col);
+      cp_async16(bx + (size_t)row * FM_XS + col, fp.X + grow * fp.Q + qb + col);
     }
     const float *ysrc = fp.Yb + ((size_t)gy * fp.Q + qb) * 3 * CG;
     float *by = bx + xsz;
@@ -977,11 +1007,13 @@ __global__ void __launch_bounds__(256, 1) k_fm_gemm_adj(FmPlan fp) {
           float4 xv[FM_ROWS];
 #pragma unroll
           for (int r = 0; r < FM_ROWS; ++r)
-            xv[r] = *reinterpret_cast<const float4 *>(Xs + ((size_t)t * fp.Dpad + r * nds + ds) * FM_SUB + qg);
+            xv[r] = *reinterpret_cast<const float4 *>(Xs + ((size_t)t * fp.Dpad + r * nds + ds) * FM_XS + qg);
 #pragma unroll
           for (int qq = 0; qq < 4; ++qq) {
-            const float *yq = Ys + ((size_t)(qg + qq) * 3 + t) * CG + cs * 8;
-            const float4 y0 = *reinterpret_cast<const float4 *>(yq), y1 = *reinterpret_cast<const float4 *>(yq + 4);
+            // candidates 4 cs .. 4 cs + 3 and CG/2 + 4 cs .. CG/2 + 4 cs + 3
+            const float *yq = Ys + ((size_t)(qg + qq) * 3 + t) * CG + cs * 4;
+            const float4 y0 = *reinterpret_cast<const float4 *>(yq),
+                         y1 = *reinterpret_cast<const float4 *>(yq + CG / 2);
             const float2 yv[4] = {make_float2(y0.x, y0.y), make_float2(y0.z, y0.w), make_float2(y1.x, y1.y),
                                   make_float2(y1.z, y1.w)};
 #pragma unroll
@@ -996,13 +1028,14 @@ __global__ void __launch_bounds__(256, 1) k_fm_gemm_adj(FmPlan fp) {
     }
     if ((k + 1) % NSUB == 0 && worker) {  // end of a tile: into the FP64 partial of its type
       const int s = fm_tile_type(fp, tb + k / NSUB);
-      double *kb = Kb + ((size_t)s * fp.Dpad + ds) * CG + cs * 8;
+      double *kb = Kb + ((size_t)s * fp.Dpad + ds) * CG + cs * 4;
 #pragma unroll
       for (int r = 0; r < FM_ROWS; ++r)
 #pragma unroll
         for (int c = 0; c < 4; ++c) {
-          kb[(size_t)r * nds * CG + 2 * c] += (double)acc[r][c].x;
-          kb[(size_t)r * nds * CG + 2 * c + 1] += (double)acc[r][c].y;
+          const int cc = (c < 2 ? 0 : CG / 2) + 2 * (c & 1);
+          kb[(size_t)r * nds * CG + cc] += (double)acc[r][c].x;
+          kb[(size_t)r * nds * CG + cc + 1] += (double)acc[r][c].y;
           acc[r][c] = make_float2(0.f, 0.f);
         }
     }
