@@ -58,10 +58,14 @@ class ShardedObjective:
     The result is the sum over ranks, identical on every rank."""
 
     def __init__(self, local: Callable, group=None, device=None):
+        import torch
         import torch.distributed as dist
         self.dist = dist
         self.local = local
         self.group = group
+        if device is None and dist.get_backend(group) == "nccl":
+            # NCCL reduces device buffers: this rank's current CUDA device
+            device = torch.device("cuda", torch.cuda.current_device())
         self.device = device
 
     def __call__(self, x, grad: bool = False):
@@ -82,14 +86,16 @@ class ShardedObjective:
 
 
 def gpu_shard(cells, spec, rank: int, world: int, rcut: float, energy_weight=1.0, stress_weight=1.0,
-              embed_extrap=0, max_candidates=1, device=None):
-    """This rank's evaluator for its run of cells (GPU)."""
+              embed_extrap=0, max_candidates=1, device=None, make_evaluator=None):
+    """This rank's evaluator for its run of cells: the GPU Evaluator, or
+    whatever `make_evaluator` (same arguments as Evaluator) builds."""
     from .potential import Database, Evaluator, PotentialFile
     lo, hi = shard_cells(row_lengths_of_cells(cells, rcut), world)[rank]
     pot = PotentialFile.from_spec(spec)
     db = Database.from_cells(cells[lo:hi], pot)
-    ev = Evaluator(db, pot, energy_weight, stress_weight, embed_extrap, device=rank if device is None else device,
-                   max_candidates=max_candidates, omit_punishments=(rank != 0))
+    factory = Evaluator if make_evaluator is None else make_evaluator
+    ev = factory(db, pot, energy_weight, stress_weight, embed_extrap, device=rank if device is None else device,
+                 max_candidates=max_candidates, omit_punishments=(rank != 0))
 
     def local(x, grad):
         if grad:

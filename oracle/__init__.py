@@ -41,7 +41,8 @@ class _Spline(C.Structure):
 
 class _Pot(C.Structure):
     _fields_ = [("style", C.c_int), ("ntypes", C.c_int), ("nsplines", C.c_int), ("splines", C.POINTER(_Spline)),
-                ("embed_extrap", C.c_int), ("energy_weight", C.c_double), ("stress_weight", C.c_double)]
+                ("embed_extrap", C.c_int), ("energy_weight", C.c_double), ("stress_weight", C.c_double),
+                ("omit_punishments", C.c_int)]
 
 
 class _Db(C.Structure):
@@ -87,7 +88,7 @@ class CRestatement:
     PotentialFile.spline(s) dicts."""
 
     def __init__(self, view: dict, splines: list, style: int, ntypes: int, energy_weight=0.0, stress_weight=0.0,
-                 embed_extrap=0):
+                 embed_extrap=0, omit_punishments=0):
         self._keep = []
         arr = []
         for s in splines:
@@ -108,7 +109,7 @@ class CRestatement:
             arr.append(sp)
         self._splines = (_Spline * len(arr))(*arr)
         self.pot = _Pot(style, ntypes, len(arr), C.cast(self._splines, C.POINTER(_Spline)), embed_extrap,
-                        energy_weight, stress_weight)
+                        energy_weight, stress_weight, int(omit_punishments))
         v = {k: (np.ascontiguousarray(x) if isinstance(x, np.ndarray) else x) for k, x in view.items()}
         self._v = v
         d = _Db()

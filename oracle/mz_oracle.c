@@ -498,6 +498,10 @@ double mzo_objective(const mzo_db *db, const mzo_pot *pot, const double *coeffs,
   }
   if (pairpot) {
     /* no punishments */
+  } else if (pot->omit_punishments) {
+    /* a shard past the first: its punishment entries are zero */
+    int q, npen = gmeam ? npair : meam ? 1 + nj : nt;
+    for (q = 0; q < npen; ++q) ev[idx++] = 0.0;
   } else if (gmeam) {
     /* pot_gmeam_spline.cpp:173-178: one punishment per f spline */
     int f, k;
@@ -880,7 +884,7 @@ double mzo_objective_tangent(const mzo_db *db, const mzo_pot *pot, const double 
     sum += constraint[c] * constraint[c];
     tsum += 2.0 * constraint[c] * tconstraint[c];
   }
-  if (pairpot) {
+  if (pairpot || pot->omit_punishments) {
     /* no punishments */
   } else if (meam) {
     /* signed largest-|y| knot (Spline::get_max_y_mag spline.cpp:58-67 over the

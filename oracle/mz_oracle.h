@@ -53,6 +53,7 @@ typedef struct {
   const mzo_spline *splines;
   int embed_extrap;
   double energy_weight, stress_weight;
+  int omit_punishments; /* leave the style punishments out (a database shard past the first) */
 } mzo_pot;
 
 typedef struct {
