@@ -283,6 +283,22 @@ mz_status mz_sync(mz_ctx *ctx);
  * work against it. */
 void *mz_stream(mz_ctx *ctx);
 
+/* Products of two row sets over a long shared axis, FP64, on the device:
+ *   out[i][j] = sum over k < n of A[i][k] * B[j][k]   (i < na, j < nb)
+ * with row i of A at d_a + i * lda and row j of B at d_b + j * ldb (device
+ * pointers, lda and ldb >= n), out[na][nb] on the device.  Enqueued on the
+ * context's stream like mz_objective_device.  With the residual vectors'
+ * derivatives as the rows of A this gives Powell's linear system
+ * gamma^T gamma (A == B) and its right-hand side gamma^T e (B = the ErrorVec,
+ * nb = 1) (OptPowell::lineqsys_init / lineqsys_update,
+ * opt_powell.cpp:438-493, which sum k in one sequential host loop).  Sums
+ * run in a fixed order: bit-reproducible on a device for given shapes; when
+ * d_a == d_b with the same stride and count, out is exactly symmetric.  The
+ * first call of a larger shape grows a context-owned workspace.  No
+ * reference counterpart as an entry point. */
+mz_status mz_gram_device(mz_ctx *ctx, int na, const double *d_a, int64_t lda, int nb, const double *d_b,
+                         int64_t ldb, int64_t n, double *d_out);
+
 /* Counters since mz_create: kernel launches issued by this context. */
 mz_status mz_launch_count(const mz_ctx *ctx, int64_t *launches);
 

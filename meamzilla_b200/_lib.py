@@ -119,6 +119,8 @@ _SIGS = {
     "mz_objective_grad_device": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]),
     "mz_sync": (C.c_int, [C.c_void_p]),
     "mz_stream": (C.c_void_p, [C.c_void_p]),
+    "mz_gram_device": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_int64, C.c_int, C.c_void_p, C.c_int64,
+                                 C.c_int64, C.c_void_p]),
     "mz_launch_count": (C.c_int, [C.c_void_p, C.POINTER(C.c_int64)]),
     "mz_tensor_core_forward": (C.c_int, [C.c_void_p, C.POINTER(C.c_int)]),
     "mz_kernel_name": (C.c_char_p, [C.c_int]),

@@ -48,6 +48,7 @@
 #include "mz_adj2.cuh"
 #include "mz_tc_fwd.cuh"
 #include "mz_fm.cuh"
+#include "mz_gram.cuh"
 
 // ================================================================= context
 
@@ -129,6 +130,8 @@ struct mz_ctx {
   } fm;
   int fm_mode = 1;
   bool fm_on = false;  // the moment path in force for mixed launches
+  double *d_gram = nullptr;  // partial sums of mz_gram_device, grown on demand
+  size_t gram_cap = 0;       // doubles
   struct Mark {
     int kernel;
     cudaEvent_t start, stop;
@@ -195,6 +198,9 @@ void release(mz_ctx *ctx) {
   ctx->graphs.clear();
   for (void *p : ctx->allocs) cudaFree(p);
   ctx->allocs.clear();
+  if (ctx->d_gram) cudaFree(ctx->d_gram);
+  ctx->d_gram = nullptr;
+  ctx->gram_cap = 0;
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
   ctx->stream = nullptr;
 }
@@ -1435,6 +1441,61 @@ mz_status mz_sync(mz_ctx *ctx) {
 }
 
 void *mz_stream(mz_ctx *ctx) { return ctx ? (void *)ctx->stream : nullptr; }
+
+mz_status mz_gram_device(mz_ctx *ctx, int na, const double *d_a, int64_t lda, int nb, const double *d_b,
+                         int64_t ldb, int64_t n, double *d_out) {
+  return guarded([&] {
+    if (!ctx || !d_a || !d_b || !d_out || na <= 0 || nb <= 0 || n <= 0 || lda < n || ldb < n)
+      throw Failure{MZ_ERR_ARG, "bad argument"};
+    if ((int64_t)na * nb > (int64_t)1 << 26) throw Failure{MZ_ERR_RANGE, "na * nb too large"};
+    ck(cudaSetDevice(ctx->device), "cudaSetDevice");
+    GramArgs g{};
+    g.A = d_a;
+    g.B = d_b;
+    g.lda = lda;
+    g.ldb = ldb;
+    g.n = n;
+    g.na = na;
+    g.nb = nb;
+    g.sym = (d_a == d_b && lda == ldb && na == nb) ? 1 : 0;
+    g.out = d_out;
+    const bool vec = nb <= GRAM_VEC;
+    const int64_t unit = vec ? GRAM_VK : GRAM_BK;
+    const int64_t units = (n + unit - 1) / unit;
+    const int Ti = (na + GRAM_T - 1) / GRAM_T, Tj = (nb + GRAM_T - 1) / GRAM_T;
+    const int ntiles = vec ? 1 : (g.sym ? Tj * (Tj + 1) / 2 : Ti * Tj);
+    // about four CTAs per SM over all tiles and k ranges
+    const int64_t want = std::max<int64_t>(1, (4 * (int64_t)ctx->nsm + ntiles - 1) / ntiles);
+    int64_t S = std::min(units, want);
+    const int64_t per = (units + S - 1) / S;
+    S = (units + per - 1) / per;  // no empty range
+    g.S = (int)S;
+    g.kper = per * unit;
+    const size_t need = (size_t)S * na * nb;
+    if (need > ctx->gram_cap) {
+      ck(cudaStreamSynchronize(ctx->stream), "gram workspace");
+      if (ctx->d_gram) cudaFree(ctx->d_gram);
+      ctx->d_gram = nullptr;
+      ctx->gram_cap = 0;
+      void *p = nullptr;
+      cudaError_t e = cudaMalloc(&p, need * sizeof(double));
+      if (e != cudaSuccess)
+        throw Failure{MZ_ERR_NOMEM, std::string("gram workspace: ") + cudaGetErrorString(e)};
+      ctx->d_gram = static_cast<double *>(p);
+      ctx->gram_cap = need;
+    }
+    g.partial = ctx->d_gram;
+    if (vec)
+      k_gram_vec<<<(unsigned)S, 256, 0, ctx->stream>>>(g);
+    else
+      k_gram_tile<<<dim3((unsigned)ntiles, (unsigned)S), 256, 0, ctx->stream>>>(g);
+    ck(cudaGetLastError(), "k_gram");
+    const int outs = na * nb;
+    k_gram_sum<<<(outs + 255) / 256, 256, 0, ctx->stream>>>(g);
+    ck(cudaGetLastError(), "k_gram_sum");
+    ctx->launches += 2;
+  });
+}
 
 const char *mz_kernel_name(int k) {
   static const char *names[MZ_NKERNELS] = {"k_prep",   "k_atoms",      "k_gather",  "k_cells",  "k_final",

@@ -163,17 +163,58 @@ class _DeviceResiduals:
         return obj, E
 
 
+def _gram(ev, A, B):
+    """A @ B.T in FP64 (A: na x n, B: nb x n).  Device residuals go through
+    the evaluator's hand-written kernel (mz_gram_device); host tensors, which
+    only a host evaluator's residuals produce, are multiplied on the host."""
+    import torch
+    if not A.is_cuda:
+        return A @ B.T
+    out = torch.empty((A.shape[0], B.shape[0]), dtype=torch.float64, device=A.device)
+    ev.gram_device(A, B, out)
+    ev.sync()
+    return out
+
+
+def device_rescaler(precision=MZ_FP64):
+    """Rescale hook of powell_fit on the GPU: Potential::rescale(flag) from
+    the evaluator's densities; (evaluator, coefficients, residuals) of the
+    rescaled potential, or None when nothing changed."""
+    def rescaler(ev, x, flag):
+        from .potential import Potential
+        pt = Potential(ev, x, precision)
+        if not pt.rescale(flag):
+            return None
+        return pt.ev, np.array(pt.x, dtype=np.float64), _DeviceResiduals(pt.ev, precision)
+    return rescaler
+
+
 def powell_fit(ev: Evaluator, x0, max_steps: int = 1000, d_eps: float = 0.0, precision=MZ_FP64,
                log: Optional[Callable[[str], None]] = None, max_evals: Optional[int] = None,
-               residuals: Optional[Callable] = None):
+               residuals: Optional[Callable] = None, rescale: int = 0, rescaler: Optional[Callable] = None):
     """Powell least-squares fit of the coefficient vector x0.
 
     `residuals(X) -> (obj[n], errvec[n, esize])` as torch tensors evaluates
     many candidates at once; by default the evaluator's device residuals.
-    Returns (x, F, info) with info = {outer, evals, seconds, history}."""
+    `rescale` is the parameter file's value (PotList::get_rescale): non-zero
+    turns on the optimizer's two rescale hooks -- Potential::rescale(1) when F
+    does not depend on a coefficient, then one more try
+    (opt_powell.cpp:138-146), and a trial Potential::rescale(0) every 4th
+    outer step, kept when it does not raise F (opt_powell.cpp:262-292).
+    `rescaler(ev, x, flag)` does the rescale: None when nothing changed, else
+    (evaluator, coefficients, residuals) of the rescaled potential -- a new
+    evaluator, since a rescale may move U's knots; device_rescaler() by
+    default.  Returns (x, F, info) with info = {outer, evals, seconds,
+    history, outer_history, rescales, evaluator}: history holds (seconds, F)
+    after each inner step, outer_history (F, x) after each outer step, and
+    evaluator is the evaluator of x."""
     import torch
     t0 = time.time()
     res = _DeviceResiduals(ev, precision) if residuals is None else residuals
+    if rescaler is None:
+        rescaler = device_rescaler(precision)
+    rescales = []
+    outer_history = []
     P = ev.ncoeff
     x = np.array(x0, dtype=np.float64)
     evals = [0]
@@ -194,31 +235,48 @@ def powell_fit(ev: Evaluator, x0, max_steps: int = 1000, d_eps: float = 0.0, pre
     e = E[0].clone()
     history.append((time.time() - t0, F))
     if F < NOTHING or max_steps == 0:
-        return x, F, dict(outer=0, evals=evals[0], seconds=time.time() - t0, history=history)
+        return x, F, dict(outer=0, evals=evals[0], seconds=time.time() - t0, history=history,
+                          outer_history=outer_history, rescales=rescales,
+                          evaluator=ev)
 
     def gamma_init(x, e):
-        """P forward differences in one launch; normalised columns."""
+        """P forward differences in one launch; normalised columns
+        (OptPowell::gamma_init, opt_powell.cpp:348-389).  Column j of the
+        reference's gamma is row j here (P x esize, as the residual vectors
+        come out of the evaluator)."""
         X = np.repeat(x[None, :], P, axis=0) + EPS * np.eye(P)
         _, Ep = resid(X)
-        gam = ((Ep - e[None, :]) / EPS).T.contiguous()      # esize x P
-        mag = torch.sqrt((gam * gam).sum(dim=0))
+        gam = (Ep - e[None, :]) / EPS
+        mag = torch.sqrt((gam * gam).sum(dim=1))
         bad = torch.nonzero(mag < NOTHING)
         if bad.numel():
             return int(bad[0, 0]) + 1, None, None
-        gam /= mag[None, :]
+        gam /= mag[:, None]
         d = np.diag(1.0 / mag.cpu().numpy())
         return 0, gam, d
 
     n_out = 0
     while True:
-        F_older = F
         code, gam, d = gamma_init(x, e)
+        if code and rescale:
+            if log:
+                log("F does not depend on coefficient %d, trying to rescale if it is an option!" % (code - 1))
+            r = rescaler(ev, x, 1)
+            if r is not None:
+                ev, x, res = r
+                rescales.append((n_out, "flag 1"))
+            o, E = resid(x)
+            F = float(o[0])
+            e = E[0].clone()
+            code, gam, d = gamma_init(x, e)
         if code:
             if log:
                 log("F does not depend on coefficient %d, fit impossible!" % (code - 1))
             break
-        lin = (gam.T @ gam).cpu().numpy()                    # gamma^T gamma (device GEMM)
-        p = -(gam.T @ e).cpu().numpy()
+        F_older = F
+        # lineqsys_init (opt_powell.cpp:438-472): gamma^T gamma, -gamma^T e
+        lin = _gram(ev, gam, gam).cpu().numpy()
+        p = -_gram(ev, gam, e[None, :])[:, 0].cpu().numpy()
         m = 0
         while True:
             F_old = F
@@ -252,12 +310,14 @@ def powell_fit(ev: Evaluator, x0, max_steps: int = 1000, d_eps: float = 0.0, pre
                 if log:
                     log("Matrix gamma singular after step %d, restarting inner loop" % m)
                 break
-            gam[:, max_col] = col / mag
+            gam[max_col] = col / mag
             delta = delta / mag
             d[:, max_col] = delta
-            # lineqsys_update (opt_powell.cpp:476-493)
-            p = -(gam.T @ e).cpu().numpy()
-            row = (gam.T @ gam[:, max_col]).cpu().numpy()
+            # lineqsys_update (opt_powell.cpp:476-493): -gamma^T e and
+            # gamma^T gamma[:, max_col] in one pass over gamma
+            pr = _gram(ev, gam, torch.stack((e, gam[max_col]))).cpu().numpy()
+            p = -pr[:, 0]
+            row = pr[:, 1]
             lin[max_col, :] = row
             lin[:, max_col] = row
             dF = F_old - F
@@ -267,14 +327,30 @@ def powell_fit(ev: Evaluator, x0, max_steps: int = 1000, d_eps: float = 0.0, pre
                 break
             if not ((m < P or (m <= INNERLOOPS and dF > PRECISION)) and dF < TOOBIG and delta_mag < TOOBIG):
                 break
-        n_out += 1
         if log:
-            log("powell outer %d: F = %.10e (%d evaluations)" % (n_out, F, evals[0]))
+            log("powell outer %d: F = %.10e (%d evaluations)" % (n_out + 1, F, evals[0]))
+        # every 4th outer step, a trial rescale kept when F does not rise
+        if (n_out + 1) % 4 == 0 and rescale:
+            r = rescaler(ev, x, 0)
+            if r is not None:
+                F2 = float(r[0].objective(r[1][None, :], precision)[0])
+                evals[0] += 1
+                if log:
+                    log("F before rescale = %f, after = %f" % (F, F2))
+                if F2 <= F:
+                    ev, x, res = r
+                    o, E = resid(x)
+                    F = float(o[0])
+                    e = E[0].clone()
+                    rescales.append((n_out, "flag 0"))
+        n_out += 1
+        outer_history.append((F, x.copy()))
         if max_evals and evals[0] >= max_evals:
             break
         if not (((F_older - F > PRECISION / 10.0) or (F_older - F < 0)) and (F_older - F > d_eps) and n_out < max_steps):
             break
-    return x, F, dict(outer=n_out, evals=evals[0], seconds=time.time() - t0, history=history)
+    return x, F, dict(outer=n_out, evals=evals[0], seconds=time.time() - t0, history=history,
+                      outer_history=outer_history, rescales=rescales, evaluator=ev)
 
 
 # -------------------------------------------------------------------- L-BFGS

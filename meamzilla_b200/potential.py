@@ -388,6 +388,22 @@ class Evaluator:
         check(lib().mz_objective_grad_device(self._h, n, C.c_void_p(params.data_ptr()), int(precision),
                                              C.c_void_p(obj.data_ptr()), C.c_void_p(grad.data_ptr())))
 
+    def gram_device(self, A, B, out) -> None:
+        """out[i, j] = sum_k A[i, k] * B[j, k] in FP64 on this evaluator's
+        stream (mz_gram_device): A (na, n), B (nb, n), out (na, nb) float64
+        CUDA tensors with unit stride along k.  Call sync() before reading
+        out."""
+        for t in (A, B, out):
+            if not t.is_cuda or t.dtype.itemsize != 8 or not t.dtype.is_floating_point:
+                raise TypeError("gram_device takes float64 CUDA tensors")
+        if A.dim() != 2 or B.dim() != 2 or A.stride(1) != 1 or B.stride(1) != 1 or not out.is_contiguous():
+            raise ValueError("rows with unit stride and a contiguous output are required")
+        if A.shape[1] != B.shape[1] or tuple(out.shape) != (A.shape[0], B.shape[0]):
+            raise ValueError("shapes do not match")
+        self._after_torch(A)
+        check(lib().mz_gram_device(self._h, A.shape[0], C.c_void_p(A.data_ptr()), A.stride(0), B.shape[0],
+                                   C.c_void_p(B.data_ptr()), B.stride(0), A.shape[1], C.c_void_p(out.data_ptr())))
+
     def sync(self) -> None:
         check(lib().mz_sync(self._h))
 

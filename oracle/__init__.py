@@ -172,7 +172,7 @@ class CRestatement:
 
 
 def run_reference(param_path: str, coeffs=None, fd_h: float = 0.0, reps: int = 0, fast: bool = False,
-                  timeout: float = 600.0, cwd=None, rescale=None, write_prefix=None) -> dict:
+                  timeout: float = 600.0, cwd=None, rescale=None, write_prefix=None, powell_steps: int = 0) -> dict:
     """Run the compiled reference on a parameter file; returns its outputs."""
     exe = MZREF_FAST if fast else MZREF
     if not os.path.exists(exe):
@@ -192,11 +192,13 @@ def run_reference(param_path: str, coeffs=None, fd_h: float = 0.0, reps: int = 0
             cmd += ["-rescale", str(int(rescale))]
         if write_prefix is not None:
             cmd += ["-write", os.path.abspath(write_prefix)]
+        if powell_steps > 0:
+            cmd += ["-powell", str(int(powell_steps))]
         res = subprocess.run(cmd, capture_output=True, text=True, timeout=timeout, cwd=cwd)
         if res.returncode != 0:
             raise RuntimeError("mzref failed (%d): %s %s" % (res.returncode, res.stdout[-2000:], res.stderr[-2000:]))
         out = {}
-        for k in ("obj", "errvec", "energy", "stress", "force", "dens", "coeff", "fdgrad", "rescale"):
+        for k in ("obj", "errvec", "energy", "stress", "force", "dens", "coeff", "fdgrad", "rescale", "powell"):
             f = "%s.%s.bin" % (prefix, k)
             if os.path.exists(f):
                 out[k] = np.fromfile(f, dtype=np.float64)

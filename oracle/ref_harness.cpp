@@ -25,6 +25,11 @@
 //            after -x, then dump every spline -> <prefix>.rescale.bin:
 //            [returned value, nsplines, per spline: n, x[n], y[n], grad[2],
 //            natural[2], step] (function groups in file order)
+//     -powell K  the reference's own Powell optimizer (OptPowell::compute_pot,
+//            src/opt_powell.cpp:96-315) from the -x start, for k = 1..K
+//            outer steps each from that same start -> <prefix>.powell.bin:
+//            per k the objective of the returned potential and its
+//            get_ncoeff() coefficients
 #define protected public
 #include "meamzilla.h"
 #include "universe.h"
@@ -36,6 +41,7 @@
 #include "pots/pot_eam/pot_eam.h"
 #include "pot_fns.h"
 #include "spline3eq.h"
+#include "opt_powell.h"
 #undef protected
 
 #include <chrono>
@@ -59,7 +65,7 @@ static void dump(const std::string &path, const std::vector<double> &v) {
 
 int main(int argc, char **argv) {
   std::string param, xfile, prefix, write_prefix;
-  int reps = 0, quiet = 0, rescale_flag = 0;
+  int reps = 0, quiet = 0, rescale_flag = 0, powell_steps = 0;
   bool do_rescale = false;
   double fd_h = 0.0;
   for (int i = 1; i < argc; ++i) {
@@ -72,6 +78,7 @@ int main(int argc, char **argv) {
     else if (a == "-write" && i + 1 < argc) write_prefix = argv[++i];
     else if (a == "-rescale" && i + 1 < argc) rescale_flag = std::atoi(argv[++i]), do_rescale = true;
     else if (a == "-q") quiet = 1;
+    else if (a == "-powell" && i + 1 < argc) powell_steps = std::atoi(argv[++i]);
     else { std::fprintf(stderr, "mzref: bad argument %s\n", a.c_str()); return 2; }
   }
   if (param.empty()) { std::fprintf(stderr, "mzref: -p <param> required\n"); return 2; }
@@ -133,6 +140,18 @@ int main(int argc, char **argv) {
   }
 
   if (!write_prefix.empty()) pot->write_data(comm, write_prefix, -1);
+
+  if (powell_steps > 0) {
+    OptPowell opt(mmz, nullptr);
+    std::vector<double> out;
+    for (int k = 1; k <= powell_steps; ++k) {
+      Potential *p = opt.compute_pot(pot, k);
+      out.push_back(p->compute(comm));
+      for (int i = 0; i < ncoeff; ++i) out.push_back(p->coeff(i));
+      delete p;
+    }
+    if (!prefix.empty()) dump(prefix + ".powell.bin", out);
+  }
 
   ErrorVec evec;
   double obj = pot->compute(comm, &evec);

@@ -10,7 +10,8 @@ through Potential::compute for two coefficient vectors:
     fdgrad (central differences of the objective, h = 1e-6; small cases)
 
 Run here (needs the reference sources to build mzref):
-    make -C oracle && python tests/golden/make_golden.py [--gmeam | --grad10 | --pair | --jmeam | --quintic]
+    make -C oracle && python tests/golden/make_golden.py [--gmeam | --grad10 | --pair | --jmeam | --quintic
+                                                          | --powell]
 """
 from __future__ import annotations
 
@@ -234,6 +235,58 @@ def grad10_goldens():
     np.savez_compressed(os.path.join(d, "grad10.npz"), **out)
 
 
+POWELL = dict(workload="eam54", seed=5, ncells=6, start_seed=9, start_sigma=0.01, steps=4)
+
+
+def powell_case():
+    """The Powell parity case: eam54 cells (seed 5, 6 cells), the in-range
+    teacher; phi and rho free except knots 0-2, U fixed, both end slopes of
+    every spline fixed -- 14 coefficients, a well-determined least-squares
+    problem (with U free the exact-target problem is ill-conditioned and
+    Powell's path is too sensitive to rounding to compare)."""
+    pot, cells = synth.make_workload(POWELL["workload"], seed=POWELL["seed"], ncells=POWELL["ncells"])
+    pot = synth.in_range_variant(pot)
+    for gi, grp in enumerate(pot.groups):
+        for sp in grp:
+            fixed = np.zeros(sp.nknots, dtype=int)
+            fixed[:3 if gi < 2 else sp.nknots] = 1
+            sp.fixed = fixed
+            sp.bc = (1, 1)
+    return pot, cells
+
+
+def powell_goldens():
+    """eam_powell4/powell.npz: the reference's OptPowell::compute_pot
+    (opt_powell.cpp:96-315) run for 1..4 outer steps by the harness
+    (oracle/ref_harness.cpp -powell) from a seeded start, with targets = the
+    reference's own teacher outputs.  F[k] and X[k] after outer step k+1."""
+    name = "eam_powell4"
+    d = os.path.join(HERE, name)
+    os.makedirs(d, exist_ok=True)
+    pot, cells = powell_case()
+    synth.write_pot(os.path.join(d, "start.pot"), pot)
+    synth.write_config(os.path.join(d, "db.conf"), cells)
+    with open(os.path.join(d, "param"), "w") as fh:
+        fh.write("config db.conf\nstartpot start.pot\ntempfile tempfile\nendpot endpot\n"
+                 "energy_weight 1.0\nstress_weight 1.0\nrescale 0\n")
+    t = oracle.run_reference("param", cwd=d)
+    a0 = np.cumsum([0] + [c.natoms for c in cells])
+    force = np.asarray(t["force"]).reshape(-1, 3)
+    for i, c in enumerate(cells):
+        c.energy0 = float(t["energy"][i])
+        c.stress0 = np.asarray(t["stress"]).reshape(-1, 6)[i].copy()
+        c.force0 = force[a0[i]:a0[i + 1]].copy()
+    synth.write_config(os.path.join(d, "db.conf"), cells)
+    x_teacher = t["coeff"]
+    x0 = x_teacher + np.random.default_rng(POWELL["start_seed"]).normal(0.0, POWELL["start_sigma"], x_teacher.size)
+    K = POWELL["steps"]
+    r = oracle.run_reference("param", cwd=d, coeffs=x0, powell_steps=K)
+    pw = np.asarray(r["powell"]).reshape(K, x0.size + 1)
+    np.savez_compressed(os.path.join(d, "powell.npz"), x0=x0, obj0=r["obj"], F=pw[:, 0], X=pw[:, 1:],
+                        x_teacher=x_teacher)
+    print(name, "P", x0.size, "F0", r["obj"], "F", pw[:, 0])
+
+
 def main():
     # 1. EAM, 3 bcc cells (the eam54 rules)
     pot, cells = synth.make_workload("eam54", seed=3, ncells=3)
@@ -284,6 +337,9 @@ def main():
 
 if __name__ == "__main__":
     import sys
+    if "--powell" in sys.argv:
+        powell_goldens()
+        sys.exit(0)
     if "--grad10" in sys.argv:
         grad10_goldens()
         sys.exit(0)

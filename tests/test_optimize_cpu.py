@@ -81,3 +81,71 @@ def test_powell_reports_a_coefficient_the_objective_ignores():
     x, F, info = powell_fit(ev, x0, max_steps=3, residuals=residuals, log=msgs.append)
     assert info["outer"] == 0 and np.array_equal(x, x0)
     assert any("coefficient %d" % dead in m and "impossible" in m for m in msgs)
+
+
+def test_powell_rescales_when_a_coefficient_is_ignored():
+    """With rescale on, a coefficient that F ignores triggers
+    Potential::rescale(1), F is recomputed and gamma_init retried
+    (opt_powell.cpp:138-146); here the rescaled potential depends on every
+    coefficient again, so the fit goes on."""
+    from meamzilla_b200.optimize import powell_fit
+    pot, ev = exact_target_eam()
+    dead = 3
+    calls = []
+
+    def residuals(X):
+        X = np.array(np.atleast_2d(X))
+        X[:, dead] = pot.coeffs()[dead]
+        return ev.residuals(X)
+
+    def rescaler(e, x, flag):
+        calls.append(flag)
+        return (ev, x.copy(), ev.residuals) if flag == 1 else None
+
+    msgs = []
+    x0 = pot.coeffs() + 0.01
+    x, F, info = powell_fit(ev, x0, max_steps=2, residuals=residuals, rescale=1, rescaler=rescaler, log=msgs.append)
+    assert calls[0] == 1 and info["rescales"][0] == (0, "flag 1")
+    assert any("trying to rescale" in m for m in msgs)
+    assert info["outer"] == 2 and F < float(ev.objective(x0)[0])
+
+    # a rescale that changes nothing leaves the fit impossible
+    calls.clear()
+    x, F, info = powell_fit(ev, x0, max_steps=2, residuals=residuals, rescale=1,
+                            rescaler=lambda e, x, flag: calls.append(flag))
+    assert calls == [1] and info["outer"] == 0
+
+
+def test_powell_trial_rescale_every_fourth_step():
+    """Every 4th outer step a trial Potential::rescale(0) is kept when F does
+    not rise and dropped otherwise (opt_powell.cpp:262-292)."""
+    from meamzilla_b200.optimize import powell_fit
+    pot, ev = exact_target_eam()
+    x0 = pot.coeffs() + np.random.default_rng(9).normal(0.0, 0.01, pot.ncoeff)
+
+    class Other(OracleEvaluator):
+        pass
+
+    other = Other(ev.orc, ev.ncoeff)
+    seen = []
+
+    def keep(e, x, flag):  # the same potential under another evaluator: F2 == F
+        seen.append((flag, e))
+        return other, x.copy(), other.residuals
+
+    x, F, info = powell_fit(ev, x0, max_steps=5, residuals=ev.residuals, rescale=1, rescaler=keep)
+    assert [f for f, _ in seen] == [0] and seen[0][1] is ev
+    assert info["rescales"] == [(3, "flag 0")] and info["evaluator"] is other
+
+    def worse(e, x, flag):
+        return other, x + 0.05, other.residuals
+
+    x, F, info = powell_fit(ev, x0, max_steps=5, residuals=ev.residuals, rescale=1, rescaler=worse)
+    assert info["rescales"] == [] and info["evaluator"] is ev
+    hist = [h[0] for h in info["outer_history"]]
+    assert all(b <= a for a, b in zip(hist, hist[1:]))
+
+    # rescale 0: no trial
+    seen.clear()
+    powell_fit(ev, x0, max_steps=5, residuals=ev.residuals, rescale=0, rescaler=keep)
+    assert seen == []
