@@ -83,7 +83,7 @@ constexpr int FT_FLUSH_BLOCKS = 8;
 //   R4 gacc[gtabs][ng-1][BLOCK_SLOTS]       per-thread g-table gradients, power basis: one table
 //                                           (the block's type) for MEAM; one per partner type for
 //                                           GMEAM, flushed every block
-//   R2 gacc5[ng-1][BLOCK_SLOTS]             spline5eq: the fifth and sixth power coefficients
+//   R2 gacc5[gtabs][ng-1][BLOCK_SLOTS]      spline5eq angular splines: the b^4, b^5 coefficients
 //   double red[BLOCK_SLOTS], a_chi[BLOCK_ATOMS], a_dF[BLOCK_ATOMS]
 //   SplineGeom sg[nsplines]; int a_lo[BLOCK_ATOMS+2], a_idx[BLOCK_ATOMS+2], a_cell[BLOCK_ATOMS+2],
 //                            a_na (atom count | type << 8)
@@ -94,10 +94,10 @@ constexpr int FT_FLUSH_BLOCKS = 8;
 //   int stype[BLOCK_SLOTS+8] neighbour type of every slot (GMEAM)
 template <typename R>
 __host__ __device__ inline size_t adj_smem_bytes(int nsplines, int stride, int pstride, bool meam, int gtabs,
-                                                 int ng, bool q5 = false) {
+                                                 int ng, bool gq5 = false) {
   size_t b = (sizeof(R) == 8 ? sizeof(double) : sizeof(float)) * (size_t)ADJ_WARPS * stride;
   b = (b + 31) & ~size_t(31);
-  if (meam) b += (q5 ? 6 : 4) * sizeof(R) * (size_t)gtabs * (ng - 1) * BLOCK_SLOTS;
+  if (meam) b += (gq5 ? 6 : 4) * sizeof(R) * (size_t)gtabs * (ng - 1) * BLOCK_SLOTS;
   b += sizeof(double) * (BLOCK_SLOTS + 2 * BLOCK_ATOMS);
   b += sizeof(SplineGeom) * nsplines;
   b += sizeof(int) * (3 * BLOCK_ATOMS + 8);
@@ -144,7 +144,8 @@ __global__ void __launch_bounds__(BLOCK_SLOTS, JM || sizeof(R) == 8 ? 2 : (GM ||
   R4 *gacc = reinterpret_cast<R4 *>(smem_raw + off);
   if (MEAM) off += 4 * sizeof(R) * (size_t)gtabs * nint * BLOCK_SLOTS;
   R2 *gacc5 = reinterpret_cast<R2 *>(smem_raw + off);
-  if (MEAM && Q5) off += 2 * sizeof(R) * (size_t)nint * BLOCK_SLOTS;
+  const bool gq5 = Q5 && pot.g_q5;  // quintic accumulators of the angular splines
+  if (MEAM && gq5) off += 2 * sizeof(R) * (size_t)gtabs * nint * BLOCK_SLOTS;
   double *red = reinterpret_cast<double *>(smem_raw + off);
   double *a_chi = red + BLOCK_SLOTS;
   double *a_dF = a_chi + BLOCK_ATOMS;
@@ -196,15 +197,15 @@ __global__ void __launch_bounds__(BLOCK_SLOTS, JM || sizeof(R) == 8 ? 2 : (GM ||
   }
   if (MEAM)
     for (int i = tid; i < gtabs * nint * BLOCK_SLOTS; i += blockDim.x) gacc[i] = R4{};
-  if (MEAM && Q5)
-    for (int i = tid; i < nint * BLOCK_SLOTS; i += blockDim.x) gacc5[i] = R2{};
+  if (MEAM && gq5)
+    for (int i = tid; i < gtabs * nint * BLOCK_SLOTS; i += blockDim.x) gacc5[i] = R2{};
   for (int i = tid; i < pot.nsplines; i += blockDim.x) sg[i] = geom[i];
   FT *ft = ftab + (size_t)warp * stride;
   double *wt = DET ? reinterpret_cast<double *>(ft) : wtab + (size_t)warp * stride;
   // Table contributions of this thread's slot.  Mixed: FP32 shared atomics.
-  // FP64: kept per thread (at most 24: phi, rho, f and JMEAM's p, p2 with four
-  // entries each, or three quintic pieces with six) and added by det_flush.
-  constexpr int NCONTRIB = DET ? 24 : 1;
+  // FP64: kept per thread (phi, rho, f and JMEAM's p, p2: four entries each,
+  // six for a quintic piece, at most 30) and added by det_flush.
+  constexpr int NCONTRIB = DET ? (JM && Q5 ? 30 : 24) : 1;
   int c_idx[NCONTRIB];
   double c_val[NCONTRIB];
   int c_n = 0;
@@ -248,7 +249,7 @@ __global__ void __launch_bounds__(BLOCK_SLOTS, JM || sizeof(R) == 8 ? 2 : (GM ||
     for (int m = 0; m < gg.n - 1; ++m) {
       const R4 v = gacc[m * BLOCK_SLOTS + tid];
       double d[6] = {(double)v.x, (double)v.y, (double)v.z, (double)v.w, 0.0, 0.0};
-      if (Q5) {
+      if (gq5) {
         const R2 v5 = gacc5[m * BLOCK_SLOTS + tid];
         d[4] = (double)v5.x;
         d[5] = (double)v5.y;
@@ -257,12 +258,12 @@ __global__ void __launch_bounds__(BLOCK_SLOTS, JM || sizeof(R) == 8 ? 2 : (GM ||
       for (int q = 0; q < (Q5 ? 6 : 4); ++q)
         for (int o = 16; o > 0; o >>= 1) d[q] += __shfl_down_sync(0xffffffffu, d[q], o);
       if (lane == 0) {
-        if (Q5) power_to_table5(gg, m, d, [&](int idx, double x) { wt[gg.toff + idx] += x; });
+        if (quintic_of<Q5>(gg)) power_to_table5(gg, m, d, [&](int idx, double x) { wt[gg.toff + idx] += x; });
         else power_to_table(gg, m, d[0], d[1], d[2], d[3], [&](int idx, double x) { wt[gg.toff + idx] += x; });
       }
     }
     for (int m = 0; m < nint; ++m) gacc[m * BLOCK_SLOTS + tid] = R4{};
-    if (Q5)
+    if (gq5)
       for (int m = 0; m < nint; ++m) gacc5[m * BLOCK_SLOTS + tid] = R2{};
   };
   auto flush_gacc = [&](int t) { flush_gacc_spline(pot.s_g + t); };
@@ -274,17 +275,25 @@ __global__ void __launch_bounds__(BLOCK_SLOTS, JM || sizeof(R) == 8 ? 2 : (GM ||
         const SplineGeom &g2 = sg[gmeam_g_index(pot, t, v, tk)];
         for (int m = 0; m < g2.n - 1; ++m) {
           R4 val = R4{};
-          if (have_t && tj_mine == v) val = gacc[(tk * nint + m) * BLOCK_SLOTS + tid];
-          double d[4] = {(double)val.x, (double)val.y, (double)val.z, (double)val.w};
+          R2 val5 = R2{};
+          if (have_t && tj_mine == v) {
+            val = gacc[(tk * nint + m) * BLOCK_SLOTS + tid];
+            if (gq5) val5 = gacc5[(tk * nint + m) * BLOCK_SLOTS + tid];
+          }
+          double d[6] = {(double)val.x, (double)val.y, (double)val.z, (double)val.w, (double)val5.x,
+                         (double)val5.y};
 #pragma unroll
-          for (int q = 0; q < 4; ++q)
+          for (int q = 0; q < (Q5 ? 6 : 4); ++q)
             for (int o = 16; o > 0; o >>= 1) d[q] += __shfl_down_sync(0xffffffffu, d[q], o);
-          if (lane == 0)
-            power_to_table(g2, m, d[0], d[1], d[2], d[3],
-                           [&](int idx, double x) { wt[g2.toff + idx] += x; });
+          if (lane == 0) {
+            if (quintic_of<Q5>(g2)) power_to_table5(g2, m, d, [&](int idx, double x) { wt[g2.toff + idx] += x; });
+            else power_to_table(g2, m, d[0], d[1], d[2], d[3], [&](int idx, double x) { wt[g2.toff + idx] += x; });
+          }
         }
       }
     for (int i = 0; i < gtabs * nint; ++i) gacc[i * BLOCK_SLOTS + tid] = R4{};
+    if (gq5)
+      for (int i = 0; i < gtabs * nint; ++i) gacc5[i * BLOCK_SLOTS + tid] = R2{};
   };
 
   // the warp's FP32 sums into its FP64 table (global memory): a lane's loads
@@ -444,7 +453,7 @@ __global__ void __launch_bounds__(BLOCK_SLOTS, JM || sizeof(R) == 8 ? 2 : (GM ||
         // into the warp's FP32 table (lane 0 alone writes it in this phase), so
         // that no global read-modify-write stands before the barrier
         FT *ftU = ft + gU.toff;
-        if (Q5) spl_point_adjoint5(gU, U, rt, eps, K, [&](int idx, double v) { ftU[idx] += (FT)v; });
+        if (quintic_of<Q5>(gU)) spl_point_adjoint5(gU, U, rt, eps, K, [&](int idx, double v) { ftU[idx] += (FT)v; });
         else spl_point_adjoint(gU, U, rt, eps, K, [&](int idx, double v) { ftU[idx] += (FT)v; });
       }
     }
@@ -476,7 +485,7 @@ __global__ void __launch_bounds__(BLOCK_SLOTS, JM || sizeof(R) == 8 ? 2 : (GM ||
             R b;
             const int m = g_knot<R>(cs, (R)g2.x0, ginv, g2.n, b);
             R dg;
-            const R gv = cubic_val_grad<R>(ptab + g2.poff, m, b, ginv, dg);
+            const R gv = piece_val_grad<Q5, R>(ptab + g2.poff, m, b, ginv, dg, g2.q5);
             const R qu = q.z * pe.ux + q.w * pe.uy + sqz[k] * pe.uz;
             dk8 += wk * (q.x * gv - q.y * dg * cs + dg * qu);
             const R bpk = lx * o.x + ly * o.y + lz * o.z;
@@ -491,6 +500,14 @@ __global__ void __launch_bounds__(BLOCK_SLOTS, JM || sizeof(R) == 8 ? 2 : (GM ||
             d.z += cg * b2 + R(2) * cs1 * b;
             d.w += cg * b2 * b + R(3) * cs1 * b2;
             *ga = d;
+            if (quintic_of<Q5>(g2)) {  // quintic pieces: the b^4 and b^5 coefficients
+              R2 *g5 = gacc5 + (size_t)(tk * nint + m) * BLOCK_SLOTS + tid;
+              R2 e = *g5;
+              const R b3 = b2 * b;
+              e.x += cg * b3 * b + R(4) * cs1 * b3;
+              e.y += cg * b3 * b2 + R(5) * cs1 * b3 * b;
+              *g5 = e;
+            }
           }
           dKdf += (double)dk8;
         }
@@ -588,7 +605,7 @@ __global__ void __launch_bounds__(BLOCK_SLOTS, JM || sizeof(R) == 8 ? 2 : (GM ||
             R b;
             const int m = g_knot<R>(cs, gx0, ginv, ngt, b);
             R dg;
-            const R gv = piece_val_grad<Q5, R>(gpc, m, b, ginv, dg);
+            const R gv = piece_val_grad<Q5, R>(gpc, m, b, ginv, dg, gg.q5);
             // d K / d f_p from the triplet terms of slot k
             const R qu = q.z * pe.ux + q.w * pe.uy + sqz[k] * pe.uz;
             dk8 += wk * (q.x * gv - q.y * dg * cs + dg * qu);
@@ -604,7 +621,7 @@ __global__ void __launch_bounds__(BLOCK_SLOTS, JM || sizeof(R) == 8 ? 2 : (GM ||
             d.z += cg * b2 + R(2) * cs1 * b;
             d.w += cg * b2 * b + R(3) * cs1 * b2;
             ga[m * BLOCK_SLOTS] = d;
-            if (Q5) {  // quintic pieces: the b^4 and b^5 coefficients
+            if (quintic_of<Q5>(gg)) {  // quintic pieces: the b^4 and b^5 coefficients
               R2 e = gacc5[m * BLOCK_SLOTS + tid];
               const R b3 = b2 * b;
               e.x += cg * b3 * b + R(4) * cs1 * b3;
@@ -619,7 +636,7 @@ __global__ void __launch_bounds__(BLOCK_SLOTS, JM || sizeof(R) == 8 ? 2 : (GM ||
       // ---- pair-function tables: phi (energy + force), rho (density + force), f
       auto pair_adj = [&](int s, int k, R b, double cv, double cd) {
         const SplineGeom &g = sg[s];
-        if (Q5) {
+        if (quintic_of<Q5>(g)) {
           const SplW5<double> w = spl_weights5<double>((double)b, g.step, g.invstep);
           add_f(g.toff + k, cv * w.wa + cd * w.da);
           add_f(g.toff + k + 1, cv * w.wb + cd * w.db);
@@ -646,7 +663,7 @@ __global__ void __launch_bounds__(BLOCK_SLOTS, JM || sizeof(R) == 8 ? 2 : (GM ||
       // gradients; flush them, then one pass per term with the rows of p
       flush_gacc(tab_t);
       since_flush = 0;
-      if (have) eval_pair_p<MEAM, R>(db, pot, sg, ptab, gs, pe);
+      if (have) eval_pair_p<MEAM, R, Q5>(db, pot, sg, ptab, gs, pe);
       const double eps = sd[CS_EPS * NC + cell];
       for (int ch = 0; ch < pot.nj; ++ch) {
         const double *axm = ax + (size_t)AUX_COUNT * (1 + ch) * Np;
@@ -692,7 +709,7 @@ __global__ void __launch_bounds__(BLOCK_SLOTS, JM || sizeof(R) == 8 ? 2 : (GM ||
               R b;
               const int m = g_knot<R>(cs, qx0, qinv, qg.n, b);
               R dq;
-              const R qv = cubic_val_grad<R>(qpc, m, b, qinv, dq);
+              const R qv = piece_val_grad<Q5, R>(qpc, m, b, qinv, dq, qg.q5);
               const R qu = q.z * pe.ux + q.w * pe.uy + sqz[k] * pe.uz;
               dk8 += wk * (q.x * qv - q.y * dq * cs + dq * qu);
               const R bpk = lx * o.x + ly * o.y + lz * o.z;
@@ -706,18 +723,36 @@ __global__ void __launch_bounds__(BLOCK_SLOTS, JM || sizeof(R) == 8 ? 2 : (GM ||
               d.z += cg * b2 + R(2) * cs1 * b;
               d.w += cg * b2 * b + R(3) * cs1 * b2;
               ga[m * BLOCK_SLOTS] = d;
+              if (quintic_of<Q5>(qg)) {  // quintic pieces: the b^4 and b^5 coefficients
+                R2 e = gacc5[m * BLOCK_SLOTS + tid];
+                const R b3 = b2 * b;
+                e.x += cg * b3 * b + R(4) * cs1 * b3;
+                e.y += cg * b3 * b2 + R(5) * cs1 * b3 * b;
+                gacc5[m * BLOCK_SLOTS + tid] = e;
+              }
             }
             dKdp += (double)dk8;
           }
           dKdp += ip * (J2 - a_p * H2);
           if (pe.kp[ch] >= 0) {
             const SplineGeom &g = sg[pot.s_p[ch] + pe.pij];
-            const SplW<double> w = spl_weights<double>((double)pe.bp[ch], g.step, g.invstep);
             const double cv = eps * G2 + dKdp, cd = a_p * G2;
-            add_f(g.toff + pe.kp[ch], cv * w.wa + cd * w.da);
-            add_f(g.toff + pe.kp[ch] + 1, cv * w.wb + cd * w.db);
-            add_f(g.toff + g.n + pe.kp[ch], cv * w.wA + cd * w.dA);
-            add_f(g.toff + g.n + pe.kp[ch] + 1, cv * w.wB + cd * w.dB);
+            const int kp = pe.kp[ch];
+            if (quintic_of<Q5>(g)) {
+              const SplW5<double> w = spl_weights5<double>((double)pe.bp[ch], g.step, g.invstep);
+              add_f(g.toff + kp, cv * w.wa + cd * w.da);
+              add_f(g.toff + kp + 1, cv * w.wb + cd * w.db);
+              add_f(g.toff + g.n + kp, cv * w.wA + cd * w.dA);
+              add_f(g.toff + g.n + kp + 1, cv * w.wB + cd * w.dB);
+              add_f(g.toff + 2 * g.n + 2 + kp, cv * w.w4a + cd * w.d4a);
+              add_f(g.toff + 2 * g.n + 3 + kp, cv * w.w4b + cd * w.d4b);
+            } else {
+              const SplW<double> w = spl_weights<double>((double)pe.bp[ch], g.step, g.invstep);
+              add_f(g.toff + kp, cv * w.wa + cd * w.da);
+              add_f(g.toff + kp + 1, cv * w.wb + cd * w.db);
+              add_f(g.toff + g.n + kp, cv * w.wA + cd * w.dA);
+              add_f(g.toff + g.n + kp + 1, cv * w.wB + cd * w.dB);
+            }
           }
         }
         flush_gacc_spline(pot.s_q[ch] + ti);

@@ -89,6 +89,7 @@ struct mz_ctx {
   std::map<uint64_t, Graph> graphs;
   size_t smem_atoms[2] = {0, 0};  // [FP64, MIXED]
   size_t smem_adj[2] = {0, 0};
+  bool adj_fits[2] = {true, true};  // the adjoint's shared-memory tables fit [FP64, MIXED]
   // Launch variants the autotuner picks from, per (precision, gradient):
   // atoms per block of the forward and of the adjoint (partitions capped at
   // TUNE_CAPS[i] pair slots and a quarter as many atoms) and the adjoint's
@@ -215,6 +216,15 @@ void check_device_flag(mz_ctx *ctx) {
   }
 }
 
+// The gradient needs the adjoint's shared-memory tables, sized by the
+// potential (per-thread angular tables, per-warp tables of every spline).
+void check_adjoint(const mz_ctx *ctx, int precision) {
+  if (!ctx->adj_fits[precision == MZ_FP64 ? 0 : 1])
+    throw Failure{MZ_ERR_RANGE, std::string("potential too large for the adjoint's shared-memory tables in ") +
+                                    (precision == MZ_FP64 ? "FP64" : "mixed precision") +
+                                    " (the objective is available)"};
+}
+
 // Brackets one kernel launch with events when the context is profiling.
 struct Bracket {
   mz_ctx *ctx;
@@ -245,9 +255,16 @@ void launch_atoms(mz_ctx *ctx, int n, size_t smem) {
       return;
     }
   }
-  if (ctx->q5) {  // spline5eq pieces
-    k_atoms<MEAM, R, AUX, false, false, true><<<ga, BLOCK_SLOTS, smem, ctx->stream>>>(
-        ctx->db, ctx->pot, ctx->d_geom, ctx->d_tabs, ctx->d_ptabs, ctx->d_V, ctx->d_aout, ctx->d_aux);
+  if (ctx->q5) {  // spline5eq pieces where a spline's basis is spline5eq
+    if (MEAM && ctx->pot.nj > 0)
+      k_atoms<MEAM, R, AUX, false, true, true><<<ga, BLOCK_SLOTS, smem, ctx->stream>>>(
+          ctx->db, ctx->pot, ctx->d_geom, ctx->d_tabs, ctx->d_ptabs, ctx->d_V, ctx->d_aout, ctx->d_aux);
+    else if (MEAM && ctx->pot.gmeam)
+      k_atoms<MEAM, R, AUX, true, false, true><<<ga, BLOCK_SLOTS, smem, ctx->stream>>>(
+          ctx->db, ctx->pot, ctx->d_geom, ctx->d_tabs, ctx->d_ptabs, ctx->d_V, ctx->d_aout, ctx->d_aux);
+    else
+      k_atoms<MEAM, R, AUX, false, false, true><<<ga, BLOCK_SLOTS, smem, ctx->stream>>>(
+          ctx->db, ctx->pot, ctx->d_geom, ctx->d_tabs, ctx->d_ptabs, ctx->d_V, ctx->d_aout, ctx->d_aux);
     return;
   }
   if constexpr (MEAM) {
@@ -269,10 +286,19 @@ void launch_atoms(mz_ctx *ctx, int n, size_t smem) {
 template <bool MEAM, typename R>
 void launch_adj(mz_ctx *ctx, int n, size_t smem) {
   dim3 ga(ctx->adj_ctas, n);
-  if (ctx->q5) {  // spline5eq pieces
-    k_adj<MEAM, R, false, false, true><<<ga, BLOCK_SLOTS, smem, ctx->stream>>>(
-        ctx->db, ctx->pot, ctx->d_geom, ctx->d_tabs, ctx->d_ptabs, ctx->d_aout, ctx->d_aux, ctx->d_lam,
-        ctx->d_seeds, ctx->d_partial, ctx->d_wglob);
+  if (ctx->q5) {  // spline5eq pieces where a spline's basis is spline5eq
+    if (MEAM && ctx->pot.nj > 0)
+      k_adj<MEAM, R, false, true, true><<<ga, BLOCK_SLOTS, smem, ctx->stream>>>(
+          ctx->db, ctx->pot, ctx->d_geom, ctx->d_tabs, ctx->d_ptabs, ctx->d_aout, ctx->d_aux, ctx->d_lam,
+          ctx->d_seeds, ctx->d_partial, ctx->d_wglob);
+    else if (MEAM && ctx->pot.gmeam)
+      k_adj<MEAM, R, true, false, true><<<ga, BLOCK_SLOTS, smem, ctx->stream>>>(
+          ctx->db, ctx->pot, ctx->d_geom, ctx->d_tabs, ctx->d_ptabs, ctx->d_aout, ctx->d_aux, ctx->d_lam,
+          ctx->d_seeds, ctx->d_partial, ctx->d_wglob);
+    else
+      k_adj<MEAM, R, false, false, true><<<ga, BLOCK_SLOTS, smem, ctx->stream>>>(
+          ctx->db, ctx->pot, ctx->d_geom, ctx->d_tabs, ctx->d_ptabs, ctx->d_aout, ctx->d_aux, ctx->d_lam,
+          ctx->d_seeds, ctx->d_partial, ctx->d_wglob);
     return;
   }
   if constexpr (MEAM && sizeof(R) == 4) {
@@ -909,6 +935,7 @@ void run_host(mz_ctx *ctx, int ncand, const double *params, int precision, doubl
               double *forces, double *energy, double *stress, double *grad) {
   if (!ctx || !params || !obj || ncand <= 0) throw Failure{MZ_ERR_ARG, "bad argument"};
   if (precision != MZ_FP64 && precision != MZ_MIXED) throw Failure{MZ_ERR_ARG, "unknown precision"};
+  if (grad) check_adjoint(ctx, precision);
   ck(cudaSetDevice(ctx->device), "cudaSetDevice");
   const int P = ctx->P, E = ctx->esize, N = ctx->natoms, NC = ctx->ncells;
   for (int c0 = 0; c0 < ncand; c0 += ctx->cand_cap) {
@@ -987,9 +1014,8 @@ mz_status mz_create(const mz_db *dbh, const mz_pot *poth, const mz_settings *set
     const int stride = im.stride;
     ctx->pstride = im.pstride;
     ctx->P = im.P;
-    ctx->q5 = ns > 0 && pot.spline(0).quintic;
-    if (ctx->q5 && (style_meam(pot.style) && pot.style != MZ_STYLE_MEAM_SPLINE))
-      throw Failure{MZ_ERR_UNSUPPORTED, "spline5eq is implemented for eam/spline, meam/spline and pair/spline"};
+    ctx->q5 = false;  // any spline5eq spline: the kernels built for per-spline bases
+    for (int s = 0; s < ns; ++s) ctx->q5 = ctx->q5 || pot.spline(s).quintic;
     ctx->nsplines = ns;
     ctx->stride = stride;
     ctx->d_geom = dupload(ctx, geom.data(), ns);
@@ -1162,7 +1188,7 @@ mz_status mz_create(const mz_db *dbh, const mz_pot *poth, const mz_settings *set
 
       // ---- triplet-moment path (mixed meam/spline): shape, feature slots
       // (the type-sorted rows, each type's run padded to FM_TILE)
-      if (pot.style == MZ_STYLE_MEAM_SPLINE && !(ns > 0 && pot.spline(0).quintic) && pot.ntypes <= FM_MAXT) {
+      if (pot.style == MZ_STYLE_MEAM_SPLINE && !ctx->q5 && pot.ntypes <= FM_MAXT) {
         int NA = 0, NN = 0, PB = 0, NBp = 0;
         for (int t = 0; t < dp.npair; ++t) NA = std::max(NA, pot.spline(dp.s_f + t).nknots + 2);
         for (int t = 0; t < pot.ntypes; ++t) NN = std::max(NN, pot.spline(dp.s_g + t).nknots + 2);
@@ -1229,40 +1255,48 @@ mz_status mz_create(const mz_db *dbh, const mz_pot *poth, const mz_settings *set
     ctx->smem_atoms[0] = atoms_smem_bytes<double>(ns, ctx->pstride, dp.nj);
     ctx->smem_atoms[1] = atoms_smem_bytes<float>(ns, ctx->pstride, dp.nj);
     int ng = 2;  // the adjoint's per-thread tables hold the largest angular spline (g, q, q2)
+    bool gq5 = false;
     if (meam)
       for (int gi : {(int)G_G, (int)G_Q1, (int)G_Q2})
         if (gi < (int)pot.groups.size())
-          for (auto &g : pot.groups[gi]) ng = std::max(ng, g.nknots);
+          for (auto &g : pot.groups[gi]) {
+            ng = std::max(ng, g.nknots);
+            gq5 = gq5 || g.quintic;
+          }
     dp.g_nmax = ng;
+    dp.g_q5 = gq5 ? 1 : 0;
     const int gtabs = dp.gmeam ? pot.ntypes : 1;
-    ctx->smem_adj[0] = adj_smem_bytes<double>(ns, stride, ctx->pstride, meam, gtabs, ng, ctx->q5);
-    ctx->smem_adj[1] = adj_smem_bytes<float>(ns, stride, ctx->pstride, meam, gtabs, ng, ctx->q5);
+    ctx->smem_adj[0] = adj_smem_bytes<double>(ns, stride, ctx->pstride, meam, gtabs, ng, gq5);
+    ctx->smem_adj[1] = adj_smem_bytes<float>(ns, stride, ctx->pstride, meam, gtabs, ng, gq5);
     int smem_max = 0;
     ck(cudaDeviceGetAttribute(&smem_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx->device), "attribute");
-    if (ctx->smem_adj[0] > (size_t)smem_max || ctx->smem_atoms[0] > (size_t)smem_max)
+    if (ctx->smem_atoms[0] > (size_t)smem_max)
       throw Failure{MZ_ERR_RANGE, "potential too large for the kernels' shared-memory tables"};
+    // the gradient of a precision whose adjoint tables do not fit is refused at the call
+    ctx->adj_fits[0] = ctx->smem_adj[0] <= (size_t)smem_max;
+    ctx->adj_fits[1] = ctx->smem_adj[1] <= (size_t)smem_max;
     smem_attr(k_atoms<true, double, false>, ctx->smem_atoms[0]);
     smem_attr(k_atoms<true, double, true>, ctx->smem_atoms[0]);
     smem_attr(k_atoms<false, double, false>, ctx->smem_atoms[0]);
     smem_attr(k_atoms<true, float, false>, ctx->smem_atoms[1]);
     smem_attr(k_atoms<true, float, true>, ctx->smem_atoms[1]);
     smem_attr(k_atoms<false, float, false>, ctx->smem_atoms[1]);
-    smem_attr(k_adj<true, double>, ctx->smem_adj[0]);
-    smem_attr(k_adj<false, double>, ctx->smem_adj[0]);
-    smem_attr(k_adj<true, float>, ctx->smem_adj[1]);
-    smem_attr(k_adj<false, float>, ctx->smem_adj[1]);
+    if (ctx->adj_fits[0]) smem_attr(k_adj<true, double>, ctx->smem_adj[0]);
+    if (ctx->adj_fits[0]) smem_attr(k_adj<false, double>, ctx->smem_adj[0]);
+    if (ctx->adj_fits[1]) smem_attr(k_adj<true, float>, ctx->smem_adj[1]);
+    if (ctx->adj_fits[1]) smem_attr(k_adj<false, float>, ctx->smem_adj[1]);
     smem_attr(k_atoms<true, double, false, true>, ctx->smem_atoms[0]);
     smem_attr(k_atoms<true, double, true, true>, ctx->smem_atoms[0]);
     smem_attr(k_atoms<true, float, false, true>, ctx->smem_atoms[1]);
     smem_attr(k_atoms<true, float, true, true>, ctx->smem_atoms[1]);
-    smem_attr(k_adj<true, double, true>, ctx->smem_adj[0]);
-    smem_attr(k_adj<true, float, true>, ctx->smem_adj[1]);
+    if (ctx->adj_fits[0]) smem_attr(k_adj<true, double, true>, ctx->smem_adj[0]);
+    if (ctx->adj_fits[1]) smem_attr(k_adj<true, float, true>, ctx->smem_adj[1]);
     smem_attr(k_atoms<true, double, false, false, true>, ctx->smem_atoms[0]);
     smem_attr(k_atoms<true, double, true, false, true>, ctx->smem_atoms[0]);
     smem_attr(k_atoms<true, float, false, false, true>, ctx->smem_atoms[1]);
     smem_attr(k_atoms<true, float, true, false, true>, ctx->smem_atoms[1]);
-    smem_attr(k_adj<true, double, false, true>, ctx->smem_adj[0]);
-    smem_attr(k_adj<true, float, false, true>, ctx->smem_adj[1]);
+    if (ctx->adj_fits[0]) smem_attr(k_adj<true, double, false, true>, ctx->smem_adj[0]);
+    if (ctx->adj_fits[1]) smem_attr(k_adj<true, float, false, true>, ctx->smem_adj[1]);
     ctx->smem_atoms2 = atoms2_smem_bytes(ns, ctx->pstride);
     ctx->smem_adj2 = adj2_smem_bytes(ns, stride, ctx->pstride, ng);
     ctx->nc2_ok = pot.style == MZ_STYLE_MEAM_SPLINE && !ctx->q5 && ctx->smem_atoms2 <= (size_t)smem_max &&
@@ -1274,18 +1308,32 @@ mz_status mz_create(const mz_db *dbh, const mz_pot *poth, const mz_settings *set
     }
     smem_attr(k_atoms<true, double, true, false, false, true>, ctx->smem_atoms[0]);
     smem_attr(k_atoms<true, float, true, false, false, true>, ctx->smem_atoms[1]);
-    smem_attr(k_adj<true, double, false, false, true>, ctx->smem_adj[0]);
-    smem_attr(k_adj<false, double, false, false, true>, ctx->smem_adj[0]);
-    smem_attr(k_adj<true, float, false, false, true>, ctx->smem_adj[1]);
-    smem_attr(k_adj<false, float, false, false, true>, ctx->smem_adj[1]);
+    if (ctx->adj_fits[0]) smem_attr(k_adj<true, double, false, false, true>, ctx->smem_adj[0]);
+    if (ctx->adj_fits[0]) smem_attr(k_adj<false, double, false, false, true>, ctx->smem_adj[0]);
+    if (ctx->adj_fits[1]) smem_attr(k_adj<true, float, false, false, true>, ctx->smem_adj[1]);
+    if (ctx->adj_fits[1]) smem_attr(k_adj<false, float, false, false, true>, ctx->smem_adj[1]);
     smem_attr(k_atoms<true, double, false, false, false, true>, ctx->smem_atoms[0]);
     smem_attr(k_atoms<false, double, false, false, false, true>, ctx->smem_atoms[0]);
     smem_attr(k_atoms<true, float, false, false, false, true>, ctx->smem_atoms[1]);
     smem_attr(k_atoms<false, float, false, false, false, true>, ctx->smem_atoms[1]);
+    // spline5eq in gmeam/spline and jmeam[2]/spline potentials
+    smem_attr(k_atoms<true, double, false, true, false, true>, ctx->smem_atoms[0]);
+    smem_attr(k_atoms<true, double, true, true, false, true>, ctx->smem_atoms[0]);
+    smem_attr(k_atoms<true, float, false, true, false, true>, ctx->smem_atoms[1]);
+    smem_attr(k_atoms<true, float, true, true, false, true>, ctx->smem_atoms[1]);
+    smem_attr(k_atoms<true, double, false, false, true, true>, ctx->smem_atoms[0]);
+    smem_attr(k_atoms<true, double, true, false, true, true>, ctx->smem_atoms[0]);
+    smem_attr(k_atoms<true, float, false, false, true, true>, ctx->smem_atoms[1]);
+    smem_attr(k_atoms<true, float, true, false, true, true>, ctx->smem_atoms[1]);
+    if (ctx->adj_fits[0]) smem_attr(k_adj<true, double, true, false, true>, ctx->smem_adj[0]);
+    if (ctx->adj_fits[1]) smem_attr(k_adj<true, float, true, false, true>, ctx->smem_adj[1]);
+    if (ctx->adj_fits[0]) smem_attr(k_adj<true, double, false, true, true>, ctx->smem_adj[0]);
+    if (ctx->adj_fits[1]) smem_attr(k_adj<true, float, false, true, true>, ctx->smem_adj[1]);
     int nsm = 0, per_sm = 0;
     ck(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, ctx->device), "attribute");
-    ck(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_adj<true, float>, BLOCK_SLOTS, ctx->smem_adj[1]),
-       "occupancy");
+    if (ctx->adj_fits[1])
+      ck(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_adj<true, float>, BLOCK_SLOTS, ctx->smem_adj[1]),
+         "occupancy");
     ctx->adj_per_sm = std::max(1, per_sm);
     if (ctx->nc2_ok) {
       int p2 = 0;
@@ -1409,6 +1457,7 @@ mz_status mz_objective_grad_device(mz_ctx *ctx, int ncand, const double *d_param
       throw Failure{MZ_ERR_RANGE,
                     "ncand exceeds the candidates one launch can hold (" + std::to_string(ctx->cand_cap) + ")"};
     if (precision != MZ_FP64 && precision != MZ_MIXED) throw Failure{MZ_ERR_ARG, "unknown precision"};
+    check_adjoint(ctx, precision);
     ck(cudaSetDevice(ctx->device), "cudaSetDevice");
     tune_variant(ctx, ncand, d_params, precision, true);
     enqueue(ctx, ncand, d_params, precision, d_obj, nullptr, nullptr, nullptr, nullptr, d_grad);
@@ -1645,7 +1694,9 @@ extern "C" mz_status mz_objective_noalloc(const mz_db *dbh, const mz_pot *poth, 
     const Db &db = dbh->db;
     const Pot &pot = poth->pot;
     const bool meam = pot.style == MZ_STYLE_MEAM_SPLINE;
-    if (pot.style == MZ_STYLE_GMEAM_SPLINE || style_nj(pot.style) > 0 || (pot.nsplines() && pot.spline(0).quintic))
+    bool any_quintic = false;
+    for (int s = 0; s < pot.nsplines(); ++s) any_quintic = any_quintic || pot.spline(s).quintic;
+    if (pot.style == MZ_STYLE_GMEAM_SPLINE || style_nj(pot.style) > 0 || any_quintic)
       throw Failure{MZ_ERR_UNSUPPORTED,
                     "the no-allocation objective supports eam/spline, meam/spline and pair/spline with spline3eq"};
     if (style_pair(db.style) != style_pair(pot.style) || (meam && !style_meam(db.style)))

@@ -80,6 +80,7 @@ struct DevPot {
   int s_phi, s_rho, s_U, s_f, s_g;  // first spline of each group
   int embed_extrap;
   int g_nmax;         // largest g-spline knot count (MEAM)
+  int g_q5;           // an angular spline (g, q, q2) is spline5eq: the adjoint's quintic accumulators
   int omit_pen;       // leave out the style punishments (sharded databases)
   int gmeam;          // g indexed by (i; j, k) types and one f punishment per f spline
   int npair;          // ntypes (ntypes + 1) / 2

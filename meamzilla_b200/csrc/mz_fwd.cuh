@@ -199,23 +199,23 @@ __device__ __forceinline__ PairEval<MEAM, R> eval_pair(const DevDb &db, const De
   if (p.kphi >= 0) {
     const SplineGeom &g = sg[pot.s_phi + p.pij];
     p.bphi = sizeof(R) == 8 ? (R)db.pair_shift[gs] : (R)db.pair_shiftf[gs];
-    p.phi = piece_val_grad<Q5, R>(ptab + g.poff, p.kphi, p.bphi, (R)g.invstep, p.dphi);
+    p.phi = piece_val_grad<Q5, R>(ptab + g.poff, p.kphi, p.bphi, (R)g.invstep, p.dphi, g.q5);
   }
   if (p.krho >= 0) {
     const SplineGeom &g = sg[pot.s_rho + p.tj];
     p.brho = sizeof(R) == 8 ? (R)db.pair_shift[Np + gs] : (R)db.pair_shiftf[Np + gs];
-    p.rho = piece_val_grad<Q5, R>(ptab + g.poff, p.krho, p.brho, (R)g.invstep, p.drho);
+    p.rho = piece_val_grad<Q5, R>(ptab + g.poff, p.krho, p.brho, (R)g.invstep, p.drho, g.q5);
   }
   if (MEAM && p.kf >= 0) {
     const SplineGeom &g = sg[pot.s_f + p.pij];
     p.bf = sizeof(R) == 8 ? (R)db.pair_shift[2 * Np + gs] : (R)db.pair_shiftf[2 * Np + gs];
-    p.f = piece_val_grad<Q5, R>(ptab + g.poff, p.kf, p.bf, (R)g.invstep, p.df);
+    p.f = piece_val_grad<Q5, R>(ptab + g.poff, p.kf, p.bf, (R)g.invstep, p.df, g.q5);
   }
   return p;
 }
 
 // The JMEAM radial functions p (p2) of one slot.
-template <bool MEAM, typename R>
+template <bool MEAM, typename R, bool Q5 = false>
 __device__ __forceinline__ void eval_pair_p(const DevDb &db, const DevPot &pot, const SplineGeom *sg, const R *ptab,
                                             int64_t gs, PairEval<MEAM, R> &p) {
   const int64_t Np = db.npairs;
@@ -227,7 +227,7 @@ __device__ __forceinline__ void eval_pair_p(const DevDb &db, const DevPot &pot, 
     if (m < pot.nj && p.kp[m] >= 0) {
       const SplineGeom &g = sg[pot.s_p[m] + p.pij];
       p.bp[m] = sizeof(R) == 8 ? (R)db.pair_shift[(3 + m) * Np + gs] : (R)db.pair_shiftf[(3 + m) * Np + gs];
-      p.p[m] = cubic_val_grad<R>(ptab + g.poff, p.kp[m], p.bp[m], (R)g.invstep, p.dp[m]);
+      p.p[m] = piece_val_grad<Q5, R>(ptab + g.poff, p.kp[m], p.bp[m], (R)g.invstep, p.dp[m], g.q5);
     }
   }
 }
@@ -288,7 +288,7 @@ __device__ __forceinline__ float cos_dot(float ax, float ay, float az, float bx,
 //   S = sum_k s(cos) w_k,  T = sum_k s'(cos) w_k cos,  v = sum_k s'(cos) w_k u_k
 // over the row's other slots whose cosine has a knot of s.  FP32 chunks of 8
 // terms are added to FP64 totals (as the g loop of k_atoms).
-template <typename R, typename R4, class W, bool Q5 = false>
+template <bool Q5, typename R, typename R4, class W>
 __device__ __forceinline__ void channel_row_sums(const R4 *srow, W weight, int row_lo, int row_hi, int tid, R ux,
                                                  R uy, R uz, const SplineGeom &gs, const R *spc, double &S, double &T,
                                                  double &vx, double &vy, double &vz) {
@@ -306,7 +306,7 @@ __device__ __forceinline__ void channel_row_sums(const R4 *srow, W weight, int r
       R b;
       const int kk = g_knot<R>(cs, x0, inv, gs.n, b);
       R ds;
-      const R sv = piece_val_grad<Q5, R>(spc, kk, b, inv, ds);
+      const R sv = piece_val_grad<Q5, R>(spc, kk, b, inv, ds, gs.q5);
       const R dsw = ds * wk;
       s8 += sv * wk;
       t8 += dsw * cs;
@@ -402,7 +402,7 @@ __global__ void __launch_bounds__(BLOCK_SLOTS, JM ? 2 : sizeof(R) == 4 ? 4 : 3)
       if (tid < 8) stype[BLOCK_SLOTS + tid] = 0;
     }
     if (JM) {
-      if (have) eval_pair_p<MEAM, R>(db, pot, sg, ptab, gs, pe);
+      if (have) eval_pair_p<MEAM, R, Q5>(db, pot, sg, ptab, gs, pe);
       for (int m = 0; m < pot.nj; ++m) {
         spv[m * (BLOCK_SLOTS + 8) + tid] = have ? pe.p[m] : R(0);
         if (tid < 8) spv[m * (BLOCK_SLOTS + 8) + BLOCK_SLOTS + tid] = R(0);
@@ -430,7 +430,7 @@ __global__ void __launch_bounds__(BLOCK_SLOTS, JM ? 2 : sizeof(R) == 4 ? 4 : 3)
         R b;
         const int kk = g_knot<R>(cs, (R)g2.x0, ginv, g2.n, b);
         R dg;
-        const R gv = piece_val_grad<Q5, R>(ptab + g2.poff, kk, b, ginv, dg);
+        const R gv = piece_val_grad<Q5, R>(ptab + g2.poff, kk, b, ginv, dg, g2.q5);
         const R dgfk = dg * fk;
         g8 += gv * fk;
         h8 += dgfk * cs;
@@ -473,7 +473,7 @@ __global__ void __launch_bounds__(BLOCK_SLOTS, JM ? 2 : sizeof(R) == 4 ? 4 : 3)
         R b;
         const int kk = g_knot<R>(cs, gx0, ginv, gg.n, b);
         R dg;
-        const R gv = piece_val_grad<Q5, R>(gpc, kk, b, ginv, dg);
+        const R gv = piece_val_grad<Q5, R>(gpc, kk, b, ginv, dg, gg.q5);
         const R dgfk = dg * fk;
         g8 += gv * fk;
         h8 += dgfk * cs;
@@ -503,7 +503,7 @@ __global__ void __launch_bounds__(BLOCK_SLOTS, JM ? 2 : sizeof(R) == 4 ? 4 : 3)
       if (!AUX && pe.p[m] == R(0) && pe.dp[m] == R(0)) continue;
       const SplineGeom qg = sg[pot.s_q[m] + ti];
       const R *wm = spv + m * (BLOCK_SLOTS + 8);
-      channel_row_sums<R>(srow, [&](int k) { return wm[k]; }, a_lo[me], a_lo[me + 1], tid, pe.ux, pe.uy, pe.uz,
+      channel_row_sums<Q5, R>(srow, [&](int k) { return wm[k]; }, a_lo[me], a_lo[me + 1], tid, pe.ux, pe.uy, pe.uz,
                           qg, ptab + qg.poff, G2[m], H2[m], v2x[m], v2y[m], v2z[m]);
       if (AUX) {
         double *ax = aux + ((size_t)cand * pot.aux_rows + AUX_COUNT * (1 + m)) * Np;

@@ -502,7 +502,7 @@ void parse_pot(const std::string &text, Pot &pot) {
   pot.ngroups = (int)nalloy.size();
   if (ln >= L.size() || L[ln++].substr(0, 2) != "#P") fail(MZ_ERR_FORMAT, "potential line (#P ...) missing");
   pot.groups.assign(pot.ngroups, {});
-  bool quintic = false, first_quintic = false;
+  bool quintic = false;
   for (int g = 0; g < pot.ngroups; ++g) {
     for (int a = 0; a < nalloy[g]; ++a) {
       // PotFns::read_pot_fns (pot_fns.cpp:439-465) + Spline3Eq::read_basis
@@ -514,10 +514,7 @@ void parse_pot(const std::string &text, Pot &pot) {
         if (is.fail()) fail(MZ_ERR_FORMAT, "incorrect basis definition, use format (#B <basis type>)");
         if (basis != "spline3eq" && basis != "spline5eq")
           fail(MZ_ERR_UNSUPPORTED, "basis \"" + basis + "\" is not implemented (spline3eq, spline5eq)");
-        quintic = basis == "spline5eq";
-        if (g == 0 && a == 0) first_quintic = quintic;
-        else if (quintic != first_quintic)
-          fail(MZ_ERR_UNSUPPORTED, "potentials mixing spline3eq and spline5eq bases are not implemented");
+        quintic = basis == "spline5eq";  // per function (pot_fns.cpp:439-465): bases may be mixed
       }
       Spline3 s;
       s.quintic = quintic ? 1 : 0;

@@ -67,11 +67,23 @@ __device__ __forceinline__ R quintic_val_grad(const R *ptab, int k, R b, R invst
   grad = (c[1] + b * (R(2) * c[2] + b * (R(3) * c[3] + b * (R(4) * c[4] + R(5) * b * c[5])))) * invstep;
   return c[0] + b * (c[1] + b * (c[2] + b * (c[3] + b * (c[4] + b * c[5]))));
 }
-// The piece of the potential's basis: cubic, or quintic when Q5.
+// The piece of a spline: cubic, or -- in kernels built with Q5, for
+// potentials with spline5eq splines -- quintic where the spline's own basis
+// is spline5eq (`q5`, its SplineGeom flag; the reference picks the basis per
+// function, pot_fns.cpp:439-465, with the virtual Spline path for mixed
+// potentials, pot_meam_spline.cpp:56-73).
 template <bool Q5, typename R>
-__device__ __forceinline__ R piece_val_grad(const R *ptab, int k, R b, R invstep, R &grad) {
-  if constexpr (Q5) return quintic_val_grad<R>(ptab, k, b, invstep, grad);
-  else return cubic_val_grad<R>(ptab, k, b, invstep, grad);
+__device__ __forceinline__ R piece_val_grad(const R *ptab, int k, R b, R invstep, R &grad, int q5) {
+  if constexpr (Q5) {
+    if (q5) return quintic_val_grad<R>(ptab, k, b, invstep, grad);
+  }
+  return cubic_val_grad<R>(ptab, k, b, invstep, grad);
+}
+// The spline's basis is quintic (only in kernels built with Q5).
+template <bool Q5>
+__device__ __forceinline__ bool quintic_of(const SplineGeom &g) {
+  if constexpr (Q5) return g.q5 != 0;
+  else return false;
 }
 
 // Weights of the value (w*) and of the slope (d*) on the table entries
@@ -169,11 +181,13 @@ __device__ __forceinline__ PointEval spl_point(const double *tab, const SplineGe
   return e;
 }
 
-// The basis chosen at compile time (the hot kernels) or from the spline.
+// The basis from the spline (kernels built with Q5) or cubic.
 template <bool Q5>
 __device__ __forceinline__ PointEval spl_point_t(const double *tab, const SplineGeom &g, double r) {
-  if constexpr (Q5) return spl_point5(tab, g, r);
-  else return spl_point(tab, g, r);
+  if constexpr (Q5) {
+    if (g.q5) return spl_point5(tab, g, r);
+  }
+  return spl_point(tab, g, r);
 }
 __device__ __noinline__ PointEval spl_point_any(const double *tab, const SplineGeom &g, double r) {
   return g.q5 ? spl_point5(tab, g, r) : spl_point(tab, g, r);

@@ -331,12 +331,16 @@ def grad10_workload(variant: str):
     return (in_range_variant(pot) if variant == "inrange" else pot), cells
 
 
-def quintic_variant(pot: PotSpec, seed: int = 0) -> PotSpec:
+def quintic_variant(pot: PotSpec, seed: int = 0, groups=None) -> PotSpec:
     """The same knots as spline5eq splines (Spline5Eq, spline5eq.cpp), with
-    end second derivatives from the knots' second differences."""
+    end second derivatives from the knots' second differences.  `groups`
+    (function group indices, default all) picks the groups made quintic; the
+    others keep spline3eq (a mixed-basis potential)."""
     p = pot.copy()
     rng = np.random.default_rng(seed)
-    for group in p.groups:
+    for gi, group in enumerate(p.groups):
+        if groups is not None and gi not in groups:
+            continue
         for s in group:
             h = (s.right - s.left) / (s.nknots - 1)
             d2 = np.diff(s.y, 2) / (h * h)

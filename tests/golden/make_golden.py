@@ -11,7 +11,7 @@ through Potential::compute for two coefficient vectors:
 
 Run here (needs the reference sources to build mzref):
     make -C oracle && python tests/golden/make_golden.py [--gmeam | --grad10 | --pair | --jmeam | --quintic
-                                                          | --powell]
+                                                          | --powell | --quintic-styles]
 """
 from __future__ import annotations
 
@@ -172,6 +172,52 @@ def quintic_goldens():
     _write(Q5_CASES[2], pot, cells)
 
 
+Q5B_CASES = ["gmeam_q5", "gmeam_q5mix2", "jmeam_q5", "jmeam2_q5mix2", "meam_mixb2", "eam_mixb"]
+
+
+def quintic_styles_goldens():
+    """spline5eq in gmeam/spline and jmeam[2]/spline potentials, and
+    potentials mixing spline3eq and spline5eq functions (the reference reads
+    the basis per function, pot_fns.cpp:439-465, and evaluates a mixed
+    potential through the virtual Spline path, pot_meam_spline.cpp:56-73)."""
+    # 16. gmeam, one species in range, every function quintic, per-cell weights
+    _, cells = synth.make_workload("meam200", seed=31, ncells=3)
+    _targets(cells, 16)
+    for i, c in enumerate(cells):
+        c.weight = 1.0 + 0.25 * i
+    pot = synth.quintic_variant(in_range_meam(synth.teacher_potential("gmeam/spline", 1, 4.5, seed=32)), seed=4)
+    _write(Q5B_CASES[0], pot, cells, fd=True, energy_weight=1.3, stress_weight=0.7)
+    # 17. gmeam, two species: phi and f quintic, the rest cubic
+    _, cells = synth.make_workload("meam2k", seed=33, ncells=4)
+    cells = [c for c in cells if c.natoms <= 300][:3] or cells[:1]
+    _targets(cells, 17)
+    pot = synth.quintic_variant(synth.teacher_potential("gmeam/spline", 2, 5.5, seed=34), seed=5, groups=(0, 3))
+    _write(Q5B_CASES[1], pot, cells, fd=True)
+    # 18. jmeam, one species in range, every function quintic
+    _, cells = synth.make_workload("meam200", seed=35, ncells=3)
+    _targets(cells, 18)
+    pot = synth.quintic_variant(in_range_meam(synth.teacher_potential("jmeam/spline", 1, 4.5, seed=36)), seed=6)
+    _write(Q5B_CASES[2], pot, cells, fd=True)
+    # 19. jmeam2, two species: phi, g and q quintic, the rest cubic
+    _, cells = synth.make_workload("meam2k", seed=37, ncells=4)
+    cells = [c for c in cells if c.natoms <= 300][:3] or cells[:1]
+    _targets(cells, 19)
+    pot = synth.quintic_variant(synth.teacher_potential("jmeam2/spline", 2, 5.5, seed=38), seed=7, groups=(0, 4, 6))
+    _write(Q5B_CASES[3], pot, cells, fd=True)
+    # 20. meam, two species: U and g quintic, the rest cubic; in range
+    _, cells = synth.make_workload("meam2k", seed=39, ncells=4)
+    cells = [c for c in cells if c.natoms <= 300][:3] or cells[:1]
+    _targets(cells, 20)
+    pot = synth.quintic_variant(in_range_meam(synth.teacher_potential("meam/spline", 2, 5.5, seed=40)), seed=8,
+                                groups=(2, 4))
+    _write(Q5B_CASES[4], pot, cells, fd=True)
+    # 21. eam: phi quintic, rho and U cubic
+    _, cells = synth.make_workload("eam54", seed=41, ncells=3)
+    _targets(cells, 21)
+    pot = synth.quintic_variant(synth.teacher_potential("eam/spline", 1, 5.0, seed=42), seed=9, groups=(0,))
+    _write(Q5B_CASES[5], pot, cells, fd=True)
+
+
 def data_goldens(names=None):
     """ref.{rho,energy,stress,force,error,punish}: the text files the
     reference's Potential::write_data writes for the start potential."""
@@ -235,7 +281,7 @@ def grad10_goldens():
     np.savez_compressed(os.path.join(d, "grad10.npz"), **out)
 
 
-POWELL = dict(workload="eam54", seed=5, ncells=6, start_seed=9, start_sigma=0.01, steps=4)
+POWELL = dict(workload="eam54", seed=5, ncells=6, start_seed=9, start_sigma=0.01, steps=8)
 
 
 def powell_case():
@@ -282,6 +328,9 @@ def powell_goldens():
     K = POWELL["steps"]
     r = oracle.run_reference("param", cwd=d, coeffs=x0, powell_steps=K)
     pw = np.asarray(r["powell"]).reshape(K, x0.size + 1)
+    for f in os.listdir(d):  # the optimizer's temporary potentials
+        if f.startswith("tempfile"):
+            os.remove(os.path.join(d, f))
     np.savez_compressed(os.path.join(d, "powell.npz"), x0=x0, obj0=r["obj"], F=pw[:, 0], X=pw[:, 1:],
                         x_teacher=x_teacher)
     print(name, "P", x0.size, "F0", r["obj"], "F", pw[:, 0])
@@ -339,6 +388,11 @@ if __name__ == "__main__":
     import sys
     if "--powell" in sys.argv:
         powell_goldens()
+        sys.exit(0)
+    if "--quintic-styles" in sys.argv:
+        quintic_styles_goldens()
+        rescale_goldens(Q5B_CASES)
+        data_goldens(Q5B_CASES)
         sys.exit(0)
     if "--grad10" in sys.argv:
         grad10_goldens()

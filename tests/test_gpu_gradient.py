@@ -53,7 +53,8 @@ def test_fp64_gradient_vs_finite_differences(name):
 
 
 @pytest.mark.parametrize("name", ["meam_mix6", "meam2_edge", "eam_bcc3", "pair_mix2", "jmeam_inrange1",
-                                  "jmeam2_mix2", "meam_q5_inrange", "eam_q5"])
+                                  "jmeam2_mix2", "meam_q5_inrange", "eam_q5", "gmeam_q5", "jmeam_q5",
+                                  "jmeam2_q5mix2", "meam_mixb2", "eam_mixb"])
 def test_mixed_gradient_vs_fp64(name):
     from meamzilla_b200.potential import MZ_FP64, MZ_MIXED, Evaluator
     case = load_case(name)

@@ -55,7 +55,8 @@ def _evaluator_with(env, case):
                 os.environ[k] = v
 
 
-@pytest.mark.parametrize("name", ["meam_mix6", "gmeam_mix2", "jmeam2_mix2", "meam_q5_inrange", "eam_bcc3"])
+@pytest.mark.parametrize("name", ["meam_mix6", "gmeam_mix2", "jmeam2_mix2", "meam_q5_inrange", "eam_bcc3",
+                                  "gmeam_q5mix2", "jmeam2_q5mix2"])
 def test_fp64_gradient_is_bitwise_reproducible(name):
     """Three calls give the same bits, and so do evaluators whose launch
     variants differ: the first variant (MZ_TUNE=0), the tuner's choice, and

@@ -15,6 +15,10 @@ pytestmark = pytest.mark.gpu
 
 FP64_OBJ = 1e-12
 FP64_FORCE = 1e-10
+# ErrorVec entries relative to max(|entry|, 1): an entry is a difference of
+# sums over up to ~1e5 terms (cell energies and stresses of 1000-atom cells,
+# forces that cancel across a neighbour row), summed in another order here
+FP64_ERRVEC = 1e-10
 MIX_OBJ = 1e-6
 MIX_FORCE = 1e-5
 
@@ -68,7 +72,8 @@ def test_meam2k_fp64_and_mixed_vs_oracle(meam2k):
         assert rel(out["obj"][c], r["obj"]) <= FP64_OBJ, (out["obj"][c], r["obj"])
         assert np.max(np.abs(out["forces"][c] - r["forces"])) <= FP64_FORCE
         scale = np.maximum(np.abs(r["errvec"]), 1.0)
-        assert np.max(np.abs(out["errvec"][c] - r["errvec"]) / scale) <= 1e-11
+        d = np.abs(out["errvec"][c] - r["errvec"]) / scale
+        assert np.max(d) <= FP64_ERRVEC, (int(np.argmax(d)), float(np.max(d)))
         for mix in (mix_rows, mix_fm):
             assert rel(mix["obj"][c], r["obj"]) <= MIX_OBJ
             assert np.max(np.abs(mix["forces"][c] - r["forces"])) <= MIX_FORCE

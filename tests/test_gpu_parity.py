@@ -157,7 +157,7 @@ def test_tensor_core_forward_opt_in(name, monkeypatch):
 
 
 @pytest.mark.parametrize("name", ["meam_mix6", "eam_bcc3", "pair_bcc1", "jmeam_inrange1", "eam_q5",
-                                  "meam_q5_inrange"])
+                                  "meam_q5_inrange", "gmeam_q5", "jmeam_q5", "meam_mixb2", "eam_mixb"])
 def test_rescale_then_objective_matches_reference(name):
     """Potential.rescale on the GPU densities, then the objective of the
     rescaled potential, against the reference's rescale + compute."""
@@ -181,7 +181,8 @@ def _same_layout(ours: str, ref: str):
         assert re.sub(r"[0-9]", "0", x) == re.sub(r"[0-9]", "0", y), (x, y)
 
 
-@pytest.mark.parametrize("name", ["meam_mix6", "eam_bcc3", "meam2_edge", "pair_mix2", "jmeam2_mix2", "eam_q5"])
+@pytest.mark.parametrize("name", ["meam_mix6", "eam_bcc3", "meam2_edge", "pair_mix2", "jmeam2_mix2", "eam_q5",
+                                  "gmeam_q5mix2", "jmeam2_q5mix2"])
 def test_write_data_from_gpu_matches_reference_files(name, tmp_path):
     """Potential.write_data evaluates on the GPU (FP64) and writes the
     reference's data files: the same layout as the reference's files, and the

@@ -104,8 +104,9 @@ def test_missing_files_are_io_errors(tmp_path):
     ("comment\n#T eam/spline 1\n#B spline3eq\n", 3, "#P"),
     ("comment\n#T meam 1\n#P\n", 5, "not implemented"),
     ("comment\n#T eam/spline 1\n#P\n#B spline7eq\n1 2 3\n", 5, "spline7eq"),
-    ("comment\n#T eam/spline 1\n#P\n#B spline3eq\n1.8 5.0 3\n0 0\n1 1\n0 1\n0 1\n0 1\n#B spline5eq\n1 2 3\n", 5,
-     "mixing"),
+    # bases may mix (one per function): a truncated spline5eq block after a spline3eq one
+    ("comment\n#T eam/spline 1\n#P\n#B spline3eq\n1.8 5.0 3\n0 0\n1 1\n0 1\n0 1\n0 1\n#B spline5eq\n1 2 3\n", 3,
+     "unexpected end"),
     ("comment\n#T eam/spline 1\n#P\n#B spline3eq\n1.8 5.0 10\n0 7\n1 1\n0 1\n", 3, "constraint"),
     ("comment\n#T eam/spline 1\n#P\n#B spline3eq\n1.8 5.0 4\n0 0\n1 1\n0 1\n0 x\n", 3, "knot line"),
 ])
