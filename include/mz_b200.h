@@ -355,10 +355,14 @@ const char *mz_kernel_name(int kernel);
 mz_status mz_profile(mz_ctx *ctx, int on);
 /* 1 when the tuned launches of (precision, grad) use the triplet-moment
  * path for mixed-precision meam/spline (the candidates' triplet sums as
- * contractions of per-slot moments built once per database: MZ_K_FM_*), 0
- * when they use the row kernels.  MZ_FM=0 in the environment at mz_create
- * keeps the row kernels, MZ_FM=2 always takes the moment path where it
- * applies, the default lets the tuner time both.  No reference counterpart. */
+ * contractions of per-slot moments built once per database: MZ_K_FM_*), 2
+ * when they do and its forward contraction runs on the tensor cores in
+ * integers (tcgen05 kind::i8 over four 8-bit digits of each operand, exact
+ * 32-bit sums), 0 when they use the row kernels.  MZ_FM=0 in the
+ * environment at mz_create keeps the row kernels, MZ_FM=2 always takes the
+ * moment path where it applies, the default lets the tuner time both;
+ * MZ_FM8=0 keeps the moment path's forward on the CUDA cores.  No reference
+ * counterpart. */
 mz_status mz_moment_path(const mz_ctx *ctx, int precision, int grad, int *on);
 mz_status mz_kernel_times(mz_ctx *ctx, double *ms, int64_t *launches);
 

@@ -48,6 +48,7 @@
 #include "mz_adj2.cuh"
 #include "mz_tc_fwd.cuh"
 #include "mz_fm.cuh"
+#include "mz_fm8.cuh"
 #include "mz_gram.cuh"
 
 // ================================================================= context
@@ -125,11 +126,14 @@ struct mz_ctx {
   // lets the tuner time it against the row kernels.
   struct Fm {
     bool eligible = false, ready = false, failed = false;
+    bool tc8 = false;  // the forward contraction on the tensor cores (mz_fm8.cuh)
     FmPlan plan{};
     int CGmax = 8, ngroups_max = 1;
     size_t smem_pre = 0;
   } fm;
   int fm_mode = 1;
+  int fm8_mode = 0;  // MZ_FM8=1: the forward contraction on the tensor cores
+  int smem_optin = 0;  // largest dynamic shared memory a block may opt into
   bool fm_on = false;  // the moment path in force for mixed launches
   double *d_gram = nullptr;  // partial sums of mz_gram_device, grown on demand
   size_t gram_cap = 0;       // doubles
@@ -388,6 +392,12 @@ bool fm_prepare(mz_ctx *ctx) {
     fm.failed = true;
     return false;
   }
+  // the integer contraction's digits, when they fit beside the rest
+  const size_t ntile8 = Q / FM8_TM;
+  const size_t bytes8 = ntile8 * 3 * 2 * FM8_STAGE + 4 * Q + G * fp.nt * FM8_BTYPE + sizeof(int) * G * fp.nt * FM8_NC;
+  fm.tc8 = ctx->fm8_mode != 0 && fp.D <= FM8_D && Q % FM8_TM == 0 &&
+           extra + bytes8 <= (size_t)(0.85 * (double)freeb) &&
+           fm8_smem(fp.nt) <= (size_t)ctx->smem_optin;
   auto pick = [&](Need &x) -> void * {
     return x.need_bytes <= x.have_bytes ? x.have : (void *)dalloc<unsigned char>(ctx, x.need_bytes);
   };
@@ -413,8 +423,20 @@ bool fm_prepare(mz_ctx *ctx) {
   ck(cudaMemsetAsync(E, 0, sizeof(double) * 8 * Q, ctx->stream), "memset");
   ck(cudaMemsetAsync(coef64, 0, sizeof(double) * C * ns * FM_MAXB, ctx->stream), "memset");
   ck(cudaMemsetAsync(coef32, 0, sizeof(float) * G * ns * FM_MAXB * CG, ctx->stream), "memset");
+  signed char *X8 = nullptr, *xe = nullptr;
+  if (fm.tc8) {
+    X8 = dalloc<signed char>(ctx, ntile8 * 3 * 2 * FM8_STAGE);
+    xe = dalloc<signed char>(ctx, 4 * Q);
+    fp.K8 = dalloc<signed char>(ctx, G * fp.nt * FM8_BTYPE);
+    fp.ke = dalloc<int>(ctx, G * fp.nt * FM8_NC);
+    ck(cudaMemsetAsync(X8, 0, ntile8 * 3 * 2 * FM8_STAGE, ctx->stream), "memset");
+    ck(cudaMemsetAsync(xe, 0, 4 * Q, ctx->stream), "memset");
+    fp.X8 = X8;
+    fp.xe = xe;
+    smem_attr(k_fm_gemm_fwd8, fm8_smem(fp.nt));
+  }
   fp.CG = fm.CGmax;
-  k_fm_features<<<ctx->natoms, 256, 0, ctx->stream>>>(ctx->db, ctx->pot, ctx->d_geom, fp, X, E);
+  k_fm_features<<<ctx->natoms, 256, 0, ctx->stream>>>(ctx->db, ctx->pot, ctx->d_geom, fp, X, E, X8, xe);
   ck(cudaGetLastError(), "k_fm_features launch");
   ck(cudaStreamSynchronize(ctx->stream), "moments");
   smem_attr(k_fm_gemm_fwd<1>, fm_fwd_smem<1>(fp.Dpad));
@@ -446,13 +468,23 @@ void enqueue_fm(mz_ctx *ctx, int n, double *d_obj, double *d_errvec, double *d_f
                                                                   const_cast<float *>(fp.coef32));
     ck(cudaGetLastError(), "k_fm_coef launch");
   }
-  {
-    Bracket b(ctx, MZ_K_FM_COEF);
-    const int zs = std::max(1, std::min(64, fp.Dpad * CG / 2048));
-    k_fm_kmat<<<dim3(fp.nt, G, zs), 256, 0, st>>>(n, ctx->pot, fp, fp.coef64, const_cast<float *>(fp.Kf));
-    ck(cudaGetLastError(), "k_fm_kmat launch");
-  }
-  {
+  if (ctx->fm.tc8) {  // the forward contraction in integers on the tensor cores
+    {
+      Bracket b(ctx, MZ_K_FM_COEF);
+      k_fm_kmat8<<<dim3(fp.nt, G), 256, 0, st>>>(n, ctx->pot, fp, fp.coef64, fp.K8, fp.ke);
+      ck(cudaGetLastError(), "k_fm_kmat8 launch");
+    }
+    Bracket b(ctx, MZ_K_FM_FWD);
+    const int ntile8 = (int)(fp.Q / FM8_TM);
+    k_fm_gemm_fwd8<<<dim3(std::min(ntile8, ctx->nsm), G), FM8_THREADS, fm8_smem(fp.nt), st>>>(fp, ctx->d_err);
+    ck(cudaGetLastError(), "k_fm_gemm_fwd8 launch");
+  } else {
+    {
+      Bracket b(ctx, MZ_K_FM_COEF);
+      const int zs = std::max(1, std::min(64, fp.Dpad * CG / 2048));
+      k_fm_kmat<<<dim3(fp.nt, G, zs), 256, 0, st>>>(n, ctx->pot, fp, fp.coef64, const_cast<float *>(fp.Kf));
+      ck(cudaGetLastError(), "k_fm_kmat launch");
+    }
     Bracket b(ctx, MZ_K_FM_FWD);
     switch (CG / 8) {
       case 1: fm_fwd_launch<1>(ctx, fp, G); break;
@@ -685,6 +717,10 @@ PotImage pot_image(const Pot &pot) {
     g.q5 = sp.quintic;
     g.toff = toff;
     toff += (sp.quintic ? 3 : 2) * sp.nknots + (sp.quintic ? 4 : 2);
+    // every spline's pieces start on 4 entries (16 bytes in FP32): cubic
+    // pieces are loaded as float4 / double2 pairs, quintic ones as pairs, and
+    // a mixed-basis potential puts cubic splines after quintic ones
+    poff = (poff + 3) & ~3;
     g.poff = poff;
     poff += (sp.quintic ? 6 : 4) * (sp.nknots - 1);
     im.nat[2 * s] = sp.nat[0];
@@ -696,7 +732,7 @@ PotImage pot_image(const Pot &pot) {
     im.M.insert(im.M.end(), M.begin(), M.end());
   }
   im.stride = toff;
-  im.pstride = poff;
+  im.pstride = (poff + 3) & ~3;  // candidates' tables start on 16 bytes too
   im.base.assign(toff, 0.0);
   im.cmap.assign(toff, -1);
   for (int s = 0; s < ns; ++s) {
@@ -1219,7 +1255,7 @@ mz_status mz_create(const mz_db *dbh, const mz_pot *poth, const mz_settings *set
               q += db.pair_off[i + 1] - db.pair_off[i];
             }
             fp.qend[t] = q;
-            q = (q + FM_TILE - 1) / FM_TILE * FM_TILE;
+            q = (q + FM8_TM - 1) / FM8_TM * FM8_TM;  // type runs on 128-slot tiles (mz_fm8.cuh)
           }
           fp.Q = q;
           fp.ntiles = (int)(q / FM_TILE);
@@ -1270,6 +1306,7 @@ mz_status mz_create(const mz_db *dbh, const mz_pot *poth, const mz_settings *set
     ctx->smem_adj[1] = adj_smem_bytes<float>(ns, stride, ctx->pstride, meam, gtabs, ng, gq5);
     int smem_max = 0;
     ck(cudaDeviceGetAttribute(&smem_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx->device), "attribute");
+    ctx->smem_optin = smem_max;
     if (ctx->smem_atoms[0] > (size_t)smem_max)
       throw Failure{MZ_ERR_RANGE, "potential too large for the kernels' shared-memory tables"};
     // the gradient of a precision whose adjoint tables do not fit is refused at the call
@@ -1360,6 +1397,10 @@ mz_status mz_create(const mz_db *dbh, const mz_pot *poth, const mz_settings *set
     {
       const char *env = std::getenv("MZ_FM");
       ctx->fm_mode = (env && env[0] == '0') ? 0 : (env && env[0] == '2') ? 2 : 1;
+    }
+    {
+      const char *env = std::getenv("MZ_FM8");
+      ctx->fm8_mode = (env && env[0] == '1') ? 1 : 0;
     }
     // tensor-core forward (mixed precision, MEAM with TC_NB B-spline coefficients per g spline)
     {
@@ -1569,7 +1610,7 @@ mz_status mz_moment_path(const mz_ctx *ctx, int precision, int grad, int *on) {
   return guarded([&] {
     if (!ctx || !on || (precision != MZ_FP64 && precision != MZ_MIXED)) throw Failure{MZ_ERR_ARG, "bad argument"};
     const mz_ctx::Tune &t = ctx->tune[precision][grad ? 1 : 0];
-    *on = (t.done && t.fm && ctx->fm.ready) ? 1 : 0;
+    *on = (t.done && t.fm && ctx->fm.ready) ? (ctx->fm.tc8 ? 2 : 1) : 0;
   });
 }
 

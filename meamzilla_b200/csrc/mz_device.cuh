@@ -22,7 +22,8 @@ struct SplineGeom {
   int toff;     // offset of this spline in a candidate's table
   int moff;     // offset of its refresh matrix d(ypp)/d(y, grad) [n][n+2]
                 // (spline5eq: d(ypp, y'''')/d(y, grad, y''_end) [2n][n+4])
-  int poff;     // offset of its per-interval polynomial coefficients [n-1][4] (spline5eq [n-1][6])
+  int poff;     // offset of its per-interval polynomial coefficients [n-1][4] (spline5eq [n-1][6]),
+                // a multiple of 4
   int q5;       // spline5eq (quintic pieces)
 };
 

@@ -80,7 +80,62 @@ struct FmPlan {
   double *Pbar;            // [ngroups][nctas_pre][nsplines][FM_MAXB][CG]  pair-function B-spline gradients
   double *Tbar;            // [ngroups][nctas_pre][CG][stride]  embedding table gradients
   int nctas_adj, nctas_pre;
+  // the integer contraction (mz_fm8.cuh), when built
+  const signed char *X8;   // [Q / 128][3][2][3][16 KB]
+  const signed char *xe;   // [Q][4]
+  signed char *K8;         // [ngroups][nt][2][3][8 KB]
+  int *ke;                 // [ngroups][nt][64]
 };
+
+// ------------------------------------------- digits of the integer contraction
+// (the tensor-core forward of mz_fm8.cuh; constants and layouts described there)
+constexpr int FM8_TM = 128;                      // slots per tile (MMA M)
+constexpr int FM8_D = 256;                       // features per kind, padded (MMA K in bytes)
+constexpr int FM8_NC = 64;                       // candidates per MMA (N), the group padded
+constexpr int FM8_DIG = 4;                       // base-256 digits per number
+constexpr int FM8_CLS = 4;                       // weight classes kept (i + j <= 3)
+constexpr int FM8_XBLK = FM8_TM * 128;           // one (digit, kblock) block of a tile: 16 KB
+constexpr int FM8_KBLK = FM8_NC * 128;           // one (digit, kblock) block of K8: 8 KB
+constexpr int FM8_STAGE = FM8_DIG * FM8_XBLK;    // one (tile, kind, kblock): 64 KB
+constexpr int FM8_BTYPE = 2 * FM8_DIG * FM8_KBLK;  // K8 of one type: 64 KB
+constexpr int FM8_SHIFT = 30;                    // |X_int|, |K_int| <= 2^30
+constexpr int FM8_NST = 2;                       // stages in the ring
+constexpr int FM8_THREADS = 192;
+constexpr uint32_t FM8_WAIT = 1u << 26;          // polls before a wait gives up
+
+// byte of (row r, byte k) in a SW128 K-major block
+__host__ __device__ inline uint32_t sw128_byte(int r, int k) {
+  return (uint32_t)((r >> 3) * 1024 + (r & 7) * 128 + ((((k >> 4) ^ r) & 7) << 4) + (k & 15));
+}
+// first byte of X8 block (tile T, kind t, kblock kb, digit l)
+__host__ __device__ inline size_t x8_block(int64_t T, int t, int kb, int l) {
+  return ((((size_t)T * 3 + t) * 2 + kb) * FM8_DIG + l) * FM8_XBLK;
+}
+// first byte of K8 block (group gy, type s, kblock kb, digit l)
+__host__ __device__ inline size_t k8_block(int gy, int s, int nt, int kb, int l) {
+  return ((((size_t)gy * nt + s) * 2 + kb) * FM8_DIG + l) * FM8_KBLK;
+}
+
+// Balanced base-256 digits of an integer |v| <= 2^30:
+// v = d0 2^24 + d1 2^16 + d2 2^8 + d3, d1..d3 in [-128, 127], d0 in [-64, 64].
+__host__ __device__ inline void digits256(long long v, signed char *d) {
+#pragma unroll
+  for (int l = FM8_DIG - 1; l > 0; --l) {
+    const long long lo = ((v + 128) & 255) - 128;
+    d[l] = (signed char)lo;
+    v = (v - lo) / 256;
+  }
+  d[0] = (signed char)v;
+}
+
+// The binary exponent e with |v| < 2^e for the largest |v| of a row (0 for a
+// zero row), kept in [-100, 100] (smaller rows quantise to zero).
+__host__ __device__ inline int fm8_exponent(double amax) {
+  if (!(amax > 0.0)) return 0;
+  int e;
+  frexp(amax, &e);
+  return e < -100 ? -100 : (e > 100 ? 100 : e);
+}
 
 // ------------------------------------------------------------- helpers
 
@@ -146,7 +201,8 @@ __device__ __forceinline__ int fm_tile_type(const FmPlan &fp, int tile) {
 // kernels take them: every other slot of the row whose cosine is below g's
 // cut (triplet_meam_spline.cpp:65-70), the g interval by g_knot.
 __global__ void __launch_bounds__(256) k_fm_features(DevDb db, DevPot pot, const SplineGeom *__restrict__ geom,
-                                                     FmPlan fp, float *__restrict__ X, double *__restrict__ E) {
+                                                     FmPlan fp, float *__restrict__ X, double *__restrict__ E,
+                                                     signed char *__restrict__ X8, signed char *__restrict__ xe) {
   __shared__ double su[3][BLOCK_SLOTS], sbf[BLOCK_SLOTS];
   __shared__ int so[BLOCK_SLOTS], skf[BLOCK_SLOTS];
   const int i = db.adj_atoms[blockIdx.x];
@@ -222,6 +278,33 @@ __global__ void __launch_bounds__(256) k_fm_features(DevDb db, DevPot pot, const
             const int d = lane * fp.NN + nn, ch = d / FM_DC, din = d % FM_DC;
             X[((size_t)(ch * 3 + t) * FM_DC + din) * fp.Q + q] = (float)acc[t][nn];
           }
+    }
+    if (X8) {  // the same moments as digits for the integer contraction (mz_fm8.cuh)
+#pragma unroll
+      for (int t = 0; t < 3; ++t) {
+        double m = 0.0;
+#pragma unroll
+        for (int nn = 0; nn < FM_MAXN; ++nn)
+          if (active && nn < fp.NN) m = fmax(m, fabs(acc[t][nn]));
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+        const int e = fm8_exponent(m);
+        if (lane == 0) xe[q * 4 + t] = (signed char)e;
+        if (active) {
+          const int64_t T = q / FM8_TM;
+          const int r = (int)(q % FM8_TM);
+#pragma unroll
+          for (int nn = 0; nn < FM_MAXN; ++nn)
+            if (nn < fp.NN) {
+              const int d = lane * fp.NN + nn;
+              signed char dg[FM8_DIG];
+              digits256(llrint(ldexp(acc[t][nn], FM8_SHIFT - e)), dg);
+              const uint32_t o = sw128_byte(r, d & 127);
+#pragma unroll
+              for (int l = 0; l < FM8_DIG; ++l) X8[x8_block(T, t, d >> 7, l) + o] = dg[l];
+            }
+        }
+      }
     }
     if (lane == 0) {
       double *e = E + (size_t)q * 8;

@@ -1,0 +1,293 @@
+// The forward moment contraction on the tensor cores, exactly in integers
+// (tcgen05.mma.kind::i8, S32 accumulators in tensor memory).
+//
+//   Y[q][t][c] = sum_d X[t][d][q] K_s[d][c]            (k_fm_gemm_fwd's sum)
+//
+// Both operands are written as 31-bit fixed-point numbers with a power-of-two
+// scale: the moments per (slot q, kind t) over the row's features,
+// X = 2^(e_q - 30) X_int, and the candidates' products per (type s,
+// candidate c) over the features, K = 2^(e_c - 30) K_int, with |X_int|,
+// |K_int| <= 2^30 (e: the binary exponent of the row's or column's largest
+// magnitude).  Each integer is four balanced base-256 digits
+//   X_int = a0 2^24 + a1 2^16 + a2 2^8 + a3,  a_i in [-128, 127] (a0 in [-64, 64]),
+// so X_int K_int = sum_{i,j} a_i b_j 2^(48 - 8 (i + j)).  The digit products
+// of the weight classes m = i + j = 0..3 (ten pairs; the classes 4..6 weigh
+// at most 2^-38 of the scale and are left out) are summed over the
+// features by the MMA exactly in 32 bits (at most 4 x 256 x 128^2 < 2^31),
+// and the epilogue forms, exactly in FP64 up to one final rounding,
+//   Y = 2^(e_q + e_c - 60) (acc_0 2^48 + acc_1 2^40 + acc_2 2^32 + acc_3 2^24).
+// The moments' digits are built once per database from their FP64 values
+// (k_fm_features); so the roundings are the two 31-bit quantisations,
+// relative to the row's and the column's largest entries, and there is no
+// accumulation error (the FP32 contraction rounds every addition).
+//
+// Layouts (each block a 128-byte-swizzled K-major tile, the image the MMA
+// reads from shared memory; rows of 128 bytes, 8-row groups 1 KiB apart,
+// 16-byte chunk j of row r at chunk j ^ (r % 8)):
+//   X8 [ntile8][3 kinds][2 kblocks][4 digits][128 slots x 128 B]   16 KB blocks
+//   xe [Q][4]                               e_q of kinds 0..2 (int8)
+//   K8 [ngroups][nt][2 kblocks][4 digits][64 candidates x 128 B]   8 KB blocks
+//   ke [ngroups][nt][64]                    e_c (int32)
+// Feature d of a row sits in kblock d / 128 at byte d % 128; features past
+// the potential's D are zero.  One (tile, kind, kblock) is 64 KB contiguous:
+// one bulk copy.
+//
+// k_fm_gemm_fwd8: persistent, one CTA per SM over a contiguous run of 128-slot
+// tiles (type-pure: each type's slots are padded to 128).  Warp 0 streams the
+// tiles' digit blocks into a two-stage ring (cp.async.bulk, completion on an
+// mbarrier), warp 1 issues the MMAs (M = 128 slots, N = 64 candidates, K = 32
+// bytes; ten digit pairs per K step into four class accumulators of 64
+// columns) and commits them to mbarriers, warps 2-5 read the accumulators of
+// the previous (tile, kind) out of tensor memory (two sets of 256 columns, so
+// the MMAs of the next kind overlap the epilogue) and store Y.  The
+// candidates' digit blocks of the current atom type sit in shared memory and
+// are reloaded where a CTA's run of tiles crosses into the next type.  Every
+// wait is bounded: a wait that gives up sets the context's error flag and its
+// role stops; the producer then waits for its copies in flight and the MMA
+// thread for its MMAs before tensor memory is freed.
+#pragma once
+
+#include "mz_fm.cuh"
+#include "mz_tc.cuh"
+
+namespace mzb {
+
+// ---------------------------------------------------------- k_fm_kmat8
+
+// K8 and ke of one (type s, group gy): K_s[d][c] = c^{f(s,o)}_a w^{g(s)}_n in
+// FP64 (as k_fm_kmat), the column exponent over d, the digits.  Candidates
+// past ncand and features past D are zero.
+__global__ void __launch_bounds__(256) k_fm_kmat8(int ncand, DevPot pot, FmPlan fp,
+                                                  const double *__restrict__ coef64, signed char *__restrict__ K8,
+                                                  int *__restrict__ ke) {
+  __shared__ int se[FM8_NC];
+  const int s = blockIdx.x, gy = blockIdx.y;
+  const int nt = fp.nt;
+  auto kval = [&](int d, int cl) -> double {
+    const int c = gy * fp.CG + cl;
+    if (cl >= fp.CG || c >= ncand || d >= fp.D) return 0.0;
+    const int o = d / (fp.NA * fp.NN), a = (d / fp.NN) % fp.NA, nn = d % fp.NN;
+    const int fs = pot.s_f + pair_ij_index(s, o, pot.ntypes), gs = pot.s_g + s;
+    return coef64[((size_t)c * pot.nsplines + fs) * FM_MAXB + a] *
+           coef64[((size_t)c * pot.nsplines + gs) * FM_MAXB + nn];
+  };
+  // column maxima: one warp per candidate, lanes over the features
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int cl = warp; cl < FM8_NC; cl += blockDim.x >> 5) {
+    double m = 0.0;
+    for (int d = lane; d < FM8_D; d += 32) m = fmax(m, fabs(kval(d, cl)));
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if (lane == 0) se[cl] = fm8_exponent(m);
+  }
+  __syncthreads();
+  if (threadIdx.x < FM8_NC) ke[((size_t)gy * nt + s) * FM8_NC + threadIdx.x] = se[threadIdx.x];
+  for (int idx = threadIdx.x; idx < FM8_NC * FM8_D; idx += blockDim.x) {
+    const int cl = idx % FM8_NC, d = idx / FM8_NC;
+    const long long v = llrint(ldexp(kval(d, cl), FM8_SHIFT - se[cl]));
+    signed char dg[FM8_DIG];
+    digits256(v, dg);
+    const int kb = d >> 7;
+    const uint32_t o = sw128_byte(cl, d & 127);
+#pragma unroll
+    for (int l = 0; l < FM8_DIG; ++l) K8[k8_block(gy, s, nt, kb, l) + o] = dg[l];
+  }
+}
+
+// ---------------------------------------------------------- k_fm_gemm_fwd8
+
+__host__ __device__ constexpr size_t fm8_smem(int nt) {
+  return 1024 + (size_t)FM8_NST * FM8_STAGE + (size_t)FM8_BTYPE + sizeof(double) * FM_MAXT * FM8_NC +
+         sizeof(uint64_t) * (2 * FM8_NST + 8) + 16;
+}
+
+__global__ void __launch_bounds__(FM8_THREADS, 1) k_fm_gemm_fwd8(FmPlan fp, int *__restrict__ err) {
+  extern __shared__ __align__(16) unsigned char sm8raw[];
+  const uint32_t raw = tc::smem_u32(sm8raw);
+  unsigned char *sA = sm8raw + (((raw + 1023u) & ~1023u) - raw);  // 1 KiB aligned
+  unsigned char *sB = sA + FM8_NST * FM8_STAGE;                    // K8 of the current type
+  double *ssc = reinterpret_cast<double *>(sB + FM8_BTYPE);        // [nt][64] 2^(e_c - 60)
+  uint64_t *full = reinterpret_cast<uint64_t *>(ssc + FM_MAXT * FM8_NC);
+  uint64_t *empty = full + FM8_NST;
+  uint64_t *accf = empty + FM8_NST;  // [2] accumulators of a (tile, kind) complete
+  uint64_t *acce = accf + 2;         // [2] accumulators read out
+  uint64_t *bload = acce + 2;        // K8 of a type landed
+  uint64_t *bfree = bload + 1;       // the MMAs reading the previous type's K8 are done
+  uint64_t *mdone = bfree + 1;       // every MMA of the CTA is done
+  uint32_t *tslot = reinterpret_cast<uint32_t *>(mdone + 1);
+
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int gy = blockIdx.y, CG = fp.CG, nt = fp.nt;
+  const int64_t ntile8 = fp.Q / FM8_TM;
+  const int64_t per = (ntile8 + gridDim.x - 1) / gridDim.x;
+  const int64_t tb = (int64_t)blockIdx.x * per, te = min(ntile8, tb + per);
+
+  if (tid == 0) {
+    for (int i = 0; i < FM8_NST; ++i) {
+      tc::mbar_init(full + i, 1);
+      tc::mbar_init(empty + i, 1);
+    }
+    for (int b = 0; b < 2; ++b) {
+      tc::mbar_init(accf + b, 1);
+      tc::mbar_init(acce + b, 4);
+    }
+    tc::mbar_init(bload, 1);
+    tc::mbar_init(bfree, 1);
+    tc::mbar_init(mdone, 1);
+  }
+  for (int i = tid; i < nt * FM8_NC; i += blockDim.x)
+    ssc[i] = ldexp(1.0, fp.ke[(size_t)gy * nt * FM8_NC + i] - FM8_SHIFT);
+  if (warp == 1) tc::tmem_alloc(tslot, 512);
+  tc::fence_before_sync();
+  __syncthreads();
+  tc::fence_after_sync();
+  const uint32_t tm = *tslot;
+
+  if (warp == 0) {
+    // ---------------- producer: K8 of each type as the tiles reach it, the tiles' digit blocks
+    if (lane == 0 && tb < te) {
+      int cur = fm_tile_type(fp, (int)(2 * tb)), nb = 0;
+      tc::mbar_expect_tx(bload, FM8_BTYPE);
+      tc::bulk_g2s(sB, fp.K8 + k8_block(gy, cur, nt, 0, 0), FM8_BTYPE, bload);
+      ++nb;
+      int64_t it = 0;
+      bool ok = true;
+      for (int64_t T = tb; T < te && ok; ++T) {
+        const int s = fm_tile_type(fp, (int)(2 * T));
+        if (s != cur) {  // the next type's K8, once the MMAs have left the current one
+          if (!tc::mbar_wait(bfree, (uint32_t)((nb - 1) & 1), FM8_WAIT)) {
+            atomicExch(err, 2);
+            ok = false;
+            break;
+          }
+          tc::mbar_expect_tx(bload, FM8_BTYPE);
+          tc::bulk_g2s(sB, fp.K8 + k8_block(gy, s, nt, 0, 0), FM8_BTYPE, bload);
+          ++nb;
+          cur = s;
+        }
+        for (int t = 0; t < 3 && ok; ++t)
+          for (int kb = 0; kb < 2; ++kb, ++it) {
+            const int st = (int)(it % FM8_NST);
+            if (it >= FM8_NST && !tc::mbar_wait(empty + st, (uint32_t)(((it / FM8_NST) & 1) ^ 1), FM8_WAIT)) {
+              atomicExch(err, 2);
+              ok = false;
+              break;
+            }
+            tc::mbar_expect_tx(full + st, FM8_STAGE);
+            tc::bulk_g2s(sA + st * FM8_STAGE, fp.X8 + x8_block(T, t, kb, 0), FM8_STAGE, full + st);
+          }
+      }
+      // copies in flight land before the CTA can exit
+      for (int64_t j = it > FM8_NST ? it - FM8_NST : 0; j < it; ++j)
+        if (!tc::mbar_wait(full + (int)(j % FM8_NST), (uint32_t)((j / FM8_NST) & 1), FM8_WAIT)) atomicExch(err, 2);
+      if (!tc::mbar_wait(bload, (uint32_t)((nb - 1) & 1), FM8_WAIT)) atomicExch(err, 2);
+    }
+  } else if (warp == 1) {
+    // ---------------- MMA issue
+    if (lane == 0) {
+      constexpr uint32_t idesc = tc::idesc_s8(FM8_TM, FM8_NC);
+      // digit pairs (i, j) of classes i + j <= 3; the first of each class starts its sum
+      constexpr int NP = 10;
+      const int pi[NP] = {0, 0, 1, 0, 1, 2, 0, 1, 2, 3}, pj[NP] = {0, 1, 0, 2, 1, 0, 3, 2, 1, 0};
+      const int pm[NP] = {0, 1, 1, 2, 2, 2, 3, 3, 3, 3};
+      const bool first[NP] = {true, true, false, true, false, false, true, false, false, false};
+      bool ok = true;
+      int64_t it = 0, seq = 0;
+      int cur = -1, nb = 0;
+      const uint32_t b0 = tc::smem_u32(sB);
+      for (int64_t T = tb; T < te && ok; ++T) {
+        const int s = fm_tile_type(fp, (int)(2 * T));
+        if (s != cur) {
+          if (cur >= 0) tc::commit(bfree);  // after the last MMAs on the previous type's K8
+          if (!tc::mbar_wait(bload, (uint32_t)(nb & 1), FM8_WAIT)) {
+            atomicExch(err, 3);
+            ok = false;
+            break;
+          }
+          ++nb;
+          cur = s;
+        }
+        for (int t = 0; t < 3 && ok; ++t, ++seq) {
+          const int buf = (int)(seq & 1);
+          if (seq >= 2 && !tc::mbar_wait(acce + buf, (uint32_t)(((seq >> 1) & 1) ^ 1), FM8_WAIT)) {
+            atomicExch(err, 3);
+            ok = false;
+            break;
+          }
+          tc::fence_after_sync();
+          for (int kb = 0; kb < 2; ++kb, ++it) {
+            const int st = (int)(it % FM8_NST);
+            if (!tc::mbar_wait(full + st, (uint32_t)((it / FM8_NST) & 1), FM8_WAIT)) {
+              atomicExch(err, 3);
+              ok = false;
+              break;
+            }
+            tc::fence_after_sync();
+            const uint32_t a0 = tc::smem_u32(sA + st * FM8_STAGE);
+#pragma unroll
+            for (int kk = 0; kk < 4; ++kk)
+#pragma unroll
+              for (int p = 0; p < NP; ++p) {
+                const uint64_t ad = tc::desc_sw128(a0 + pi[p] * FM8_XBLK + 32 * kk, 16, 1024);
+                const uint64_t bd = tc::desc_sw128(b0 + (kb * FM8_DIG + pj[p]) * FM8_KBLK + 32 * kk, 16, 1024);
+                const uint32_t d = tm + (uint32_t)(buf * 256 + pm[p] * FM8_NC);
+                tc::mma_s8(d, ad, bd, idesc, (kb == 0 && kk == 0 && first[p]) ? 0u : 1u);
+              }
+            tc::commit(empty + st);  // the stage is free once these MMAs are done
+          }
+          if (ok) tc::commit(accf + buf);
+        }
+      }
+      tc::commit(mdone);
+      if (!tc::mbar_wait(mdone, 0, FM8_WAIT)) atomicExch(err, 3);
+    }
+  } else {
+    // ---------------- epilogue: warps 2..5, TMEM lane quarter warp % 4
+    const int quarter = warp & 3, r = 32 * quarter + lane;
+    int64_t seq = 0;
+    bool ok = true;
+    for (int64_t T = tb; T < te && ok; ++T) {
+      const int s = fm_tile_type(fp, (int)(2 * T));
+      const int64_t q = T * FM8_TM + r;
+      for (int t = 0; t < 3; ++t, ++seq) {
+        const int buf = (int)(seq & 1);
+        if (!tc::mbar_wait(accf + buf, (uint32_t)((seq >> 1) & 1), FM8_WAIT)) {
+          atomicExch(err, 4);
+          ok = false;
+          break;
+        }
+        tc::fence_after_sync();
+        const double sq = ldexp(1.0, (int)fp.xe[q * 4 + t] - FM8_SHIFT);
+        double *yo = fp.Y + (((size_t)gy * fp.Q + q) * 3 + t) * CG;
+        const uint32_t ta = tm + ((uint32_t)(32 * quarter) << 16) + (uint32_t)(buf * 256);
+        for (int cb = 0; cb < FM8_NC / 16 && cb * 16 < CG; ++cb) {
+          int v[FM8_CLS][16];
+#pragma unroll
+          for (int m = 0; m < FM8_CLS; ++m) tc::tmem_ld16i(ta + m * FM8_NC + cb * 16, v[m]);
+          tc::tmem_wait_ld();
+#pragma unroll
+          for (int u = 0; u < 16; u += 2) {
+            double y2[2];
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+              // X_int K_int = sum_m acc_m 2^(48 - 8 m), scaled by 2^(e_q - 30) 2^(e_c - 30)
+              const double a = ((double)v[0][u + h] * 281474976710656.0 + (double)v[1][u + h] * 1099511627776.0) +
+                               ((double)v[2][u + h] * 4294967296.0 + (double)v[3][u + h] * 16777216.0);
+              y2[h] = a * sq * ssc[s * FM8_NC + cb * 16 + u + h];
+            }
+            if (cb * 16 + u + 1 < CG) *reinterpret_cast<double2 *>(yo + cb * 16 + u) = make_double2(y2[0], y2[1]);
+          }
+        }
+        tc::fence_before_sync();
+        __syncwarp();
+        if (lane == 0) tc::mbar_arrive(acce + buf);
+      }
+    }
+  }
+  tc::fence_before_sync();
+  __syncthreads();
+  tc::fence_after_sync();
+  if (warp == 1) tc::tmem_dealloc(tm, 512);
+}
+
+}  // namespace mzb

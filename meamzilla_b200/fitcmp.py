@@ -9,7 +9,9 @@ objective as its target, and prints one JSON line: final objectives, wall
 seconds, objective evaluations.  With --rescale F the start potential is first
 rescaled as Meamzilla does at start-up (meamzilla.cpp:135-143: parameter
 `rescale` 2 -> flag 0, rescale when the densities leave U's range; 3 -> flag 1)
-and both fits start from the rescaled coefficients.
+and both fits start from the rescaled coefficients; Powell then runs with the
+reference's rescale hooks on (its `rescale` parameter is F + 2, non-zero:
+opt_powell.cpp:138-146, 262-292).
 """
 from __future__ import annotations
 
@@ -67,14 +69,18 @@ def main():
         ev, x0 = start.ev, start.x
         pot = ev.pot
     F0 = float(ev.objective(x0[None, :])[0])
-    xp, Fp, ip = powell_fit(ev, x0, max_steps=args.powell_steps)
+    hooks = args.rescale + 2 if args.rescale is not None else 0
+    # (a rescale inside Powell gives its potential a new evaluator, ip["evaluator"];
+    # L-BFGS starts from the same start potential)
+    xp, Fp, ip = powell_fit(ev, x0, max_steps=args.powell_steps, rescale=hooks)
     xl, Fl, il = lbfgs_fit(ev, x0, MZ_FP64, maxiter=20000, target=Fp)
     xm, Fm, im = lbfgs_fit(ev, x0, MZ_MIXED, maxiter=20000, target=Fp)
     st = db.stats()
     print(json.dumps({
         "workload": args.workload + (" (in-range variant)" if args.in_range else ""), "natoms": st["natoms"], "ntriplets": st["ntriplets"], "ncoeff": P,
         "start_objective": F0, "rescale": rescaled,
-        "powell": {"objective": Fp, "seconds": ip["seconds"], "evals": ip["evals"], "outer": ip["outer"]},
+        "powell": {"objective": Fp, "seconds": ip["seconds"], "evals": ip["evals"], "outer": ip["outer"],
+                   "rescales": ip["rescales"]},
         "lbfgs_fp64": {"objective": Fl, "seconds": il["seconds"], "evals": il["evals"],
                        "reached_powell": bool(Fl <= Fp)},
         "lbfgs_mixed": {"objective": Fm, "seconds": im["seconds"], "evals": im["evals"],

@@ -346,12 +346,13 @@ class Evaluator:
                     forward_candidates_per_cta=int(c[3]), adjoint_candidates_per_cta=int(c[4]),
                     triplet_moments=bool(on.value))
 
-    def moment_path(self, precision=MZ_MIXED, grad=True) -> bool:
-        """True when the tuned (precision, gradient) launches run the
-        triplet-moment path (mixed-precision meam/spline)."""
+    def moment_path(self, precision=MZ_MIXED, grad=True) -> int:
+        """Non-zero when the tuned (precision, gradient) launches run the
+        triplet-moment path (mixed-precision meam/spline): 1 with the forward
+        contraction on the CUDA cores, 2 with it on the tensor cores."""
         on = C.c_int()
         check(lib().mz_moment_path(self._h, int(precision), 1 if grad else 0, C.byref(on)))
-        return bool(on.value)
+        return int(on.value)
 
     def launches(self) -> int:
         n = C.c_int64()

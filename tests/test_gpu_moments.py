@@ -105,3 +105,51 @@ def test_moment_path_matches_row_kernels_mixed():
     fa = a.objective(x[:2], MZ_MIXED, forces=True)["forces"]
     f64 = b.objective(x[:2], MZ_FP64, forces=True)["forces"]
     assert np.max(np.abs(fa - f64)) <= FORCE
+
+
+def _evaluator8(case, ncand, fm8):
+    old = os.environ.get("MZ_FM8")
+    os.environ["MZ_FM8"] = fm8
+    try:
+        return _evaluator(case, ncand, "2")
+    finally:
+        if old is None:
+            del os.environ["MZ_FM8"]
+        else:
+            os.environ["MZ_FM8"] = old
+
+
+@pytest.mark.parametrize("ncand", [64, 24, 8])
+def test_integer_tensor_core_forward(ncand):
+    """The forward contraction on the tensor cores (four 8-bit digits per
+    operand, exact integer sums) against the CUDA-core FP32 contraction and
+    FP64: objective, forces and gradient at the mixed bars, the integer path
+    no less accurate than the FP32 one (twice its error at most, plus 1e-12),
+    for full and partial candidate groups on a 60-cell two-species
+    workload of the benchmark's rules."""
+    from meamzilla_b200 import synth
+    from meamzilla_b200.potential import MZ_FP64, MZ_MIXED, Database, PotentialFile
+    spec, cells = synth.make_workload("meam2k", seed=3, ncells=60)
+    pot = PotentialFile.from_spec(spec)
+    db = Database.from_cells(cells, pot)
+    case = dict(db=db, pot=pot, weights=dict(energy_weight=1.0, stress_weight=1.0, embed_extrap=0))
+    x = synth.perturbed(pot.coeffs(), ncand, 0.05, seed=21)
+    a = _evaluator8(case, ncand, "1")
+    b = _evaluator8(case, ncand, "0")
+    oa, ga = a.objective_grad(x, MZ_MIXED)
+    ob, gb = b.objective_grad(x, MZ_MIXED)
+    assert a.moment_path(MZ_MIXED, True) == 2 and b.moment_path(MZ_MIXED, True) == 1
+    o64, g64 = b.objective_grad(x, MZ_FP64)
+    ea, eb = np.abs(oa - o64) / np.abs(o64), np.abs(ob - o64) / np.abs(o64)
+    assert np.all(ea <= OBJ), ea.max()
+    assert ea.max() <= 2 * eb.max() + 1e-12, (ea.max(), eb.max())
+    for c in range(0, ncand, max(1, ncand // 8)):
+        assert _err(ga[c], g64[c]) <= GRAD
+    fa = a.objective(x[:2], MZ_MIXED, forces=True)["forces"]
+    fb = b.objective(x[:2], MZ_MIXED, forces=True)["forces"]
+    f64 = b.objective(x[:2], MZ_FP64, forces=True)["forces"]
+    assert np.max(np.abs(fa - f64)) <= FORCE
+    assert np.max(np.abs(fa - f64)) <= 2 * np.max(np.abs(fb - f64)) + 1e-12
+    # repeatable: integer sums in a fixed order
+    oa2, _ = a.objective_grad(x, MZ_MIXED)
+    assert np.array_equal(oa, oa2)
