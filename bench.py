@@ -220,9 +220,18 @@ FM_DPAD_MEAM2K = 240
 # Algorithmic bytes of one launch per kernel (None where not stated): the
 # moment contractions stream the FP32 moments once (4 B x 3 x 240 per slot)
 # plus their candidate-side operand (4 B x 3 per slot-candidate, in and out).
+# Algorithmic bytes per launch of the moment contractions: the moments read
+# once (FP32, or four 8-bit digits of 256 padded features per kind when the
+# forward runs on the tensor cores) and the per-slot sums written (FP64 Y) or
+# read (FP32 dL/dY).
+FM8_BYTES_PER_SLOT = 3 * 256 * 4
 KERNEL_BYTES = {
-    "k_fm_fwd": lambda st, nc: 4 * 3 * FM_DPAD_MEAM2K * st["npairs"] + 4 * 3 * st["npairs"] * nc,
+    "k_fm_fwd": lambda st, nc: 4 * 3 * FM_DPAD_MEAM2K * st["npairs"] + 8 * 3 * st["npairs"] * nc,
     "k_fm_adj": lambda st, nc: 4 * 3 * FM_DPAD_MEAM2K * st["npairs"] + 4 * 3 * st["npairs"] * nc,
+}
+KERNEL_BYTES_TC = {
+    "k_fm_fwd": lambda st, nc: FM8_BYTES_PER_SLOT * st["npairs"] + 8 * 3 * st["npairs"] * nc,
+    "k_fm_adj": lambda st, nc: FM8_BYTES_PER_SLOT * st["npairs"] + 4 * 3 * st["npairs"] * nc,
 }
 # DRAM bytes per launch measured by ncu (dram__bytes_read.sum + dram__bytes_write.sum) on a smaller
 # case of this workload, scaled by the units a full launch processes (profiles/ holds the captures).
@@ -505,7 +514,8 @@ def run_mine(args, world, rank, local):
     kflops = kernel_algorithmic_flops(dom, stats, args.ncand)
     fm_dpad = FM_DPAD_MEAM2K if tuned.get("triplet_moments") else None
     xflops = executed_flops(dom, stats, args.ncand, fm_dpad)
-    kbytes = KERNEL_BYTES.get(dom, lambda st, nc: None)(stats, args.ncand)
+    tc8 = bool(tuned.get("moment_forward_tensor_cores"))
+    kbytes = (KERNEL_BYTES_TC if tc8 else KERNEL_BYTES).get(dom, lambda st, nc: None)(stats, args.ncand)
     # A moment contraction executes a different count from the row
     # formulation's triplet flops (the moments are built once per database):
     # its roofline is on the flops it executes, the row-equivalent rate beside.

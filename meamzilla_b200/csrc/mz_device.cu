@@ -392,12 +392,14 @@ bool fm_prepare(mz_ctx *ctx) {
     fm.failed = true;
     return false;
   }
-  // the integer contraction's digits, when they fit beside the rest
+  // the integer contraction's digits, in place of the FP32 moments, when they fit
   const size_t ntile8 = Q / FM8_TM;
   const size_t bytes8 = ntile8 * 3 * 2 * FM8_STAGE + 4 * Q + G * fp.nt * FM8_BTYPE + sizeof(int) * G * fp.nt * FM8_NC;
+  const size_t bytesX = sizeof(float) * 3 * (size_t)fp.Dpad * Q;
   fm.tc8 = ctx->fm8_mode != 0 && fp.D <= FM8_D && Q % FM8_TM == 0 &&
-           extra + bytes8 <= (size_t)(0.85 * (double)freeb) &&
-           fm8_smem(fp.nt) <= (size_t)ctx->smem_optin;
+           extra - bytesX + bytes8 <= (size_t)(0.85 * (double)freeb) &&
+           fm8_smem(fp.nt) <= (size_t)ctx->smem_optin &&
+           fm_adj_smem(fp.Dpad, 64, true) <= (size_t)ctx->smem_optin;
   auto pick = [&](Need &x) -> void * {
     return x.need_bytes <= x.have_bytes ? x.have : (void *)dalloc<unsigned char>(ctx, x.need_bytes);
   };
@@ -407,7 +409,7 @@ bool fm_prepare(mz_ctx *ctx) {
   fp.aoutF = static_cast<double *>(pick(need[2]));
   fp.lamf = static_cast<float *>(pick(need[3]));
   fp.seedF = static_cast<double *>(pick(need[4]));
-  float *X = dalloc<float>(ctx, 3 * (size_t)fp.Dpad * Q);
+  float *X = fm.tc8 ? nullptr : dalloc<float>(ctx, 3 * (size_t)fp.Dpad * Q);
   double *E = dalloc<double>(ctx, 8 * Q);
   fp.X = X;
   fp.E = E;
@@ -419,7 +421,7 @@ bool fm_prepare(mz_ctx *ctx) {
   fp.Kbar = dalloc<double>(ctx, G * fp.nctas_adj * fp.nt * fp.Dpad * CG);
   fp.Pbar = dalloc<double>(ctx, G * fp.nctas_pre * ns * FM_MAXB * CG);
   fp.Tbar = dalloc<double>(ctx, G * fp.nctas_pre * CG * stride);
-  ck(cudaMemsetAsync(X, 0, sizeof(float) * 3 * (size_t)fp.Dpad * Q, ctx->stream), "memset");
+  if (X) ck(cudaMemsetAsync(X, 0, sizeof(float) * 3 * (size_t)fp.Dpad * Q, ctx->stream), "memset");
   ck(cudaMemsetAsync(E, 0, sizeof(double) * 8 * Q, ctx->stream), "memset");
   ck(cudaMemsetAsync(coef64, 0, sizeof(double) * C * ns * FM_MAXB, ctx->stream), "memset");
   ck(cudaMemsetAsync(coef32, 0, sizeof(float) * G * ns * FM_MAXB * CG, ctx->stream), "memset");
@@ -446,7 +448,8 @@ bool fm_prepare(mz_ctx *ctx) {
   fm.smem_pre = fm_pre_smem(ctx->nsplines, 64, fp.nt, fp.NB, fp.ustride);
   smem_attr(k_fm_adj_pre, fm.smem_pre);
   smem_attr(k_fm_epi, fm_epi_smem(ctx->nsplines, fp.nt, fp.NB, 64));
-  smem_attr(k_fm_gemm_adj, fm_adj_smem(fp.Dpad, 64));
+  smem_attr(k_fm_gemm_adj<false>, fm_adj_smem(fp.Dpad, 64));
+  if (fm.tc8) smem_attr(k_fm_gemm_adj<true>, fm_adj_smem(fp.Dpad, 64, true));
   fm.ready = true;
   return true;
 }
@@ -530,7 +533,10 @@ void enqueue_fm(mz_ctx *ctx, int n, double *d_obj, double *d_errvec, double *d_f
   {
     Bracket b(ctx, MZ_K_FM_ADJ);
     const int threads = ((fp.Dpad / FM_ROWS) * (CG / 8) + 31) / 32 * 32;
-    k_fm_gemm_adj<<<dim3(fp.nctas_adj, G), std::min(threads, 256), fm_adj_smem(fp.Dpad, CG), st>>>(fp);
+    if (ctx->fm.tc8)
+      k_fm_gemm_adj<true><<<dim3(fp.nctas_adj, G), std::min(threads, 256), fm_adj_smem(fp.Dpad, CG, true), st>>>(fp);
+    else
+      k_fm_gemm_adj<false><<<dim3(fp.nctas_adj, G), std::min(threads, 256), fm_adj_smem(fp.Dpad, CG), st>>>(fp);
     ck(cudaGetLastError(), "k_fm_gemm_adj launch");
   }
   {

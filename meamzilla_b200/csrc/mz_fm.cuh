@@ -269,7 +269,7 @@ __global__ void __launch_bounds__(256) k_fm_features(DevDb db, DevPot pot, const
       }
     }
     const int64_t q = q0 + p;
-    if (active) {
+    if (X && active) {
 #pragma unroll
       for (int t = 0; t < 3; ++t)
 #pragma unroll
@@ -1030,15 +1030,27 @@ __global__ void __launch_bounds__(256, 2) k_fm_adj_pre(DevDb db, DevPot pot, con
 // warp read one contiguous 128-byte run) as packed pairs of candidates; the FP32 sums of a tile are added to this CTA's FP64
 // partial of the tile's atom type.  The operand of padding slots (past a
 // type's last real slot) is taken as zero.
+//
+// With DIG8 the moments come from the integer forward's digits (X8, xe; no
+// FP32 copy is kept): each sub-tile's digit rows (16 rows of every (kind,
+// kblock, digit) block, 2 KB contiguous each, 48 KB in all) are copied raw
+// into one staging buffer and turned into the FP32 operand, X_int 2^(e - 30)
+// rounded once, before the sub-tile is consumed; the copy of the next
+// sub-tile's digits overlaps the arithmetic.
 constexpr int FM_XS = FM_SUB + 4;  // shared-memory row stride of the moments (80 B: no bank aliasing)
-__host__ __device__ inline size_t fm_adj_smem(int Dpad, int CG) {
-  return 2 * sizeof(float) * ((size_t)3 * Dpad * FM_XS + (size_t)FM_SUB * 3 * CG);
+constexpr int FM8_SUBRAW = 3 * 2 * FM8_DIG * FM_SUB * 128;  // digit rows of one sub-tile: 48 KB
+__host__ __device__ inline size_t fm_adj_smem(int Dpad, int CG, bool dig8 = false) {
+  return 2 * sizeof(float) * ((size_t)3 * Dpad * FM_XS + (size_t)FM_SUB * 3 * CG) +
+         (dig8 ? (size_t)FM8_SUBRAW + sizeof(double) * 3 * FM_SUB : 0);
 }
 
+template <bool DIG8>
 __global__ void __launch_bounds__(256, 1) k_fm_gemm_adj(FmPlan fp) {
   extern __shared__ __align__(16) float asm_[];
   const int CG = fp.CG, gy = blockIdx.y;
   const size_t xsz = (size_t)3 * fp.Dpad * FM_XS, ysz = (size_t)FM_SUB * 3 * CG;
+  unsigned char *raw = reinterpret_cast<unsigned char *>(asm_ + 2 * (xsz + ysz));  // DIG8: digit rows
+  double *rsc = reinterpret_cast<double *>(raw + FM8_SUBRAW);                      // DIG8: [3][FM_SUB] scales
   const int tid = threadIdx.x;
   const int ncs = CG / 8, nds = fp.Dpad / FM_ROWS;
   const int cs = tid % ncs, ds = tid / ncs;
@@ -1051,12 +1063,23 @@ __global__ void __launch_bounds__(256, 1) k_fm_gemm_adj(FmPlan fp) {
   for (int i = tid; i < fp.nt * fp.Dpad * CG; i += blockDim.x) Kb[i] = 0.0;
   auto load = [&](int k, float *bx) {
     const int64_t qb = (int64_t)(tb + k / NSUB) * FM_TILE + (k % NSUB) * FM_SUB;
-    const int nrow = 3 * fp.Dpad;
-    for (int i = tid; i < nrow * (FM_SUB / 4); i += blockDim.x) {
-      const int row = i / (FM_SUB / 4), col = (i % (FM_SUB / 4)) * 4;
-      const int t = row / fp.Dpad, d = row % fp.Dpad;
-      const size_t grow = (size_t)((d / FM_DC) * 3 + t) * FM_DC + d % FM_DC;
-      cp_async16(bx + (size_t)row * FM_XS + col, fp.X + grow * fp.Q + qb + col);
+    if constexpr (DIG8) {
+      // the 16 digit rows of every (kind, kblock, digit) block: 2 KB each
+      const int64_t T = qb / FM8_TM;
+      const int r0 = (int)(qb % FM8_TM);
+      for (int i = tid; i < 3 * 2 * FM8_DIG * 128; i += blockDim.x) {
+        const int blk = i >> 7, ch = i & 127;  // blk = (t * 2 + kb) * FM8_DIG + l
+        const size_t src = (size_t)T * 3 * 2 * FM8_STAGE + (size_t)blk * FM8_XBLK + (size_t)(r0 >> 3) * 1024 + ch * 16;
+        cp_async16(raw + (size_t)blk * 2048 + ch * 16, fp.X8 + src);
+      }
+    } else {
+      const int nrow = 3 * fp.Dpad;
+      for (int i = tid; i < nrow * (FM_SUB / 4); i += blockDim.x) {
+        const int row = i / (FM_SUB / 4), col = (i % (FM_SUB / 4)) * 4;
+        const int t = row / fp.Dpad, d = row % fp.Dpad;
+        const size_t grow = (size_t)((d / FM_DC) * 3 + t) * FM_DC + d % FM_DC;
+        cp_async16(bx + (size_t)row * FM_XS + col, fp.X + grow * fp.Q + qb + col);
+      }
     }
     const float *ysrc = fp.Yb + ((size_t)gy * fp.Q + qb) * 3 * CG;
     float *by = bx + xsz;
@@ -1072,15 +1095,56 @@ __global__ void __launch_bounds__(256, 1) k_fm_gemm_adj(FmPlan fp) {
   for (int r = 0; r < FM_ROWS; ++r)
 #pragma unroll
     for (int c = 0; c < 4; ++c) acc[r][c] = make_float2(0.f, 0.f);
-  if (total > 0) load(0, asm_);
-  for (int k = 0; k < total; ++k) {
-    if (k + 1 < total) {
-      load(k + 1, asm_ + ((k + 1) & 1) * (xsz + ysz));
-      cp_async_wait<1>();
-    } else {
-      cp_async_wait<0>();
+  // DIG8: the staged digits of sub-tile k -> its FP32 operand
+  auto dequant = [&](int k, float *bx) {
+    const int64_t qb = (int64_t)(tb + k / NSUB) * FM_TILE + (k % NSUB) * FM_SUB;
+    if (tid < 3 * FM_SUB) {
+      const int t = tid / FM_SUB, j = tid % FM_SUB;
+      rsc[tid] = ldexp(1.0, (int)fp.xe[(qb + j) * 4 + t] - FM8_SHIFT);
     }
     __syncthreads();
+    const int nd4 = fp.Dpad / 4;
+    for (int i = tid; i < 3 * nd4 * FM_SUB; i += blockDim.x) {
+      const int j = i % FM_SUB, d4 = (i / FM_SUB) % nd4, t = i / (FM_SUB * nd4);
+      const int d = 4 * d4, kb = d >> 7;
+      const uint32_t o = sw128_byte(j, d & 127);
+      uint32_t w[FM8_DIG];
+#pragma unroll
+      for (int l = 0; l < FM8_DIG; ++l)
+        w[l] = *reinterpret_cast<const uint32_t *>(raw + (size_t)((t * 2 + kb) * FM8_DIG + l) * 2048 + o);
+      const double sc = rsc[t * FM_SUB + j];
+#pragma unroll
+      for (int b = 0; b < 4; ++b) {
+        int v = 0;
+#pragma unroll
+        for (int l = 0; l < FM8_DIG; ++l) v = v * 256 + (int)(signed char)(w[l] >> (8 * b));
+        bx[((size_t)t * fp.Dpad + d + b) * FM_XS + j] = (float)((double)v * sc);
+      }
+    }
+  };
+  if constexpr (DIG8) {
+    if (total > 0) {
+      load(0, asm_);
+      cp_async_wait<0>();
+      __syncthreads();
+      dequant(0, asm_);
+    }
+  } else if (total > 0) {
+    load(0, asm_);
+  }
+  for (int k = 0; k < total; ++k) {
+    if constexpr (DIG8) {
+      __syncthreads();  // the digits of sub-tile k are in its operand; the staging buffer is free
+      if (k + 1 < total) load(k + 1, asm_ + ((k + 1) & 1) * (xsz + ysz));
+    } else {
+      if (k + 1 < total) {
+        load(k + 1, asm_ + ((k + 1) & 1) * (xsz + ysz));
+        cp_async_wait<1>();
+      } else {
+        cp_async_wait<0>();
+      }
+      __syncthreads();
+    }
     const float *Xs = asm_ + (k & 1) * (xsz + ysz), *Ys = Xs + xsz;
     if (worker) {
 #pragma unroll
@@ -1121,6 +1185,13 @@ __global__ void __launch_bounds__(256, 1) k_fm_gemm_adj(FmPlan fp) {
           kb[(size_t)r * nds * CG + cc + 1] += (double)acc[r][c].y;
           acc[r][c] = make_float2(0.f, 0.f);
         }
+    }
+    if constexpr (DIG8) {
+      if (k + 1 < total) {  // the next sub-tile's digits have landed: its operand
+        cp_async_wait<0>();
+        __syncthreads();
+        dequant(k + 1, asm_ + ((k + 1) & 1) * (xsz + ysz));
+      }
     }
     __syncthreads();
   }

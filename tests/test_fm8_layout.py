@@ -1,0 +1,144 @@
+"""The integer forward contraction's host-side arithmetic, restated on the
+CPU (mz_fm.cuh / mz_fm8.cuh): balanced base-256 digits of 31-bit integers,
+the 128-byte-swizzled K-major block layout of the moments' and the
+candidates' digits, the ten digit-pair MMAs summed per weight class (what
+tcgen05.mma.kind::i8 adds exactly in 32 bits), the FP64 epilogue, and the
+adjoint's dequantised operand read back from 16-slot sub-tiles.  The device
+result against FP64 is tests/test_gpu_moments.py's."""
+import math
+
+import numpy as np
+
+TM, D8, NC, DIG = 128, 256, 64, 4
+XBLK, KBLK = TM * 128, NC * 128
+STAGE = DIG * XBLK
+SHIFT = 30
+PAIRS = [(0, 0), (0, 1), (1, 0), (0, 2), (1, 1), (2, 0), (0, 3), (1, 2), (2, 1), (3, 0)]
+
+
+def sw128(r, k):
+    return (r >> 3) * 1024 + (r & 7) * 128 + ((((k >> 4) ^ r) & 7) << 4) + (k & 15)
+
+
+def x8_block(T, t, kb, l):
+    return (((T * 3 + t) * 2 + kb) * DIG + l) * XBLK
+
+
+def k8_block(gy, s, nt, kb, l):
+    return (((gy * nt + s) * 2 + kb) * DIG + l) * KBLK
+
+
+def digits(v):
+    d = [0] * DIG
+    for l in range(DIG - 1, 0, -1):
+        lo = ((v + 128) & 255) - 128
+        d[l] = lo
+        v = (v - lo) // 256
+    d[0] = v
+    return d
+
+
+def exponent(m):
+    if not m > 0:
+        return 0
+    return max(-100, min(100, math.frexp(m)[1]))
+
+
+def test_digits_round_trip_and_ranges():
+    rng = np.random.default_rng(0)
+    for v in list(rng.integers(-2 ** 30, 2 ** 30, 2000)) + [2 ** 30, -2 ** 30, 0, 1, -1, 127, -128, 255]:
+        d = digits(int(v))
+        assert -64 <= d[0] <= 64 and all(-128 <= x <= 127 for x in d[1:])
+        assert sum(d[l] * 256 ** (DIG - 1 - l) for l in range(DIG)) == v
+
+
+def test_swizzle_is_a_permutation_of_each_block():
+    offs = {sw128(r, k) for r in range(TM) for k in range(128)}
+    assert offs == set(range(XBLK))
+    # 4-byte groups of a feature quad stay contiguous (the adjoint reads them as words)
+    for r in range(16):
+        for d in range(0, 128, 4):
+            assert [sw128(r, d + b) for b in range(4)] == [sw128(r, d) + b for b in range(4)]
+
+
+def _build(rng, nt, D, Q, CG):
+    X = rng.normal(size=(3, Q, D)) * np.exp(rng.normal(size=(3, Q, 1)) * 3)
+    X[:, Q - 20:, :] = 0.0
+    K = rng.normal(size=(nt, CG, D)) * np.exp(rng.normal(size=(nt, CG, 1)))
+    ntile8 = Q // TM
+    X8 = np.zeros(ntile8 * 3 * 2 * STAGE, np.int8)
+    xe = np.zeros(4 * Q, np.int8)
+    for t in range(3):
+        for q in range(Q):
+            e = exponent(np.max(np.abs(X[t, q])))
+            xe[q * 4 + t] = e
+            T, r = divmod(q, TM)
+            for d in range(D):
+                dg = digits(int(np.rint(math.ldexp(X[t, q, d], SHIFT - e))))
+                for l in range(DIG):
+                    X8[x8_block(T, t, d >> 7, l) + sw128(r, d & 127)] = dg[l]
+    K8 = np.zeros(nt * 2 * DIG * KBLK, np.int8)
+    ke = np.zeros((nt, NC), int)
+    for s in range(nt):
+        for c in range(NC):
+            e = exponent(np.max(np.abs(K[s, c]))) if c < CG else 0
+            ke[s, c] = e
+            for d in range(D8):
+                kv = K[s, c, d] if (c < CG and d < D) else 0.0
+                dg = digits(int(np.rint(math.ldexp(kv, SHIFT - e))))
+                for l in range(DIG):
+                    K8[k8_block(0, s, nt, d >> 7, l) + sw128(c, d & 127)] = dg[l]
+    return X, K, X8, xe, K8, ke
+
+
+def test_class_sums_and_epilogue_match_fp64():
+    rng = np.random.default_rng(1)
+    nt, D, Q, CG = 2, 240, 256, 64
+    X, K, X8, xe, K8, ke = _build(rng, nt, D, Q, CG)
+    idxA = np.array([[sw128(r, k) for k in range(128)] for r in range(TM)])
+    idxB = np.array([[sw128(c, k) for k in range(128)] for c in range(NC)])
+    worst = 0.0
+    for T, s in ((0, 0), (1, 1)):
+        for t in range(3):
+            acc = np.zeros((4, TM, NC), np.int64)
+            for kb in range(2):
+                for i, j in PAIRS:
+                    A = X8[x8_block(T, t, kb, i) + idxA].astype(np.int64)
+                    B = K8[k8_block(0, s, nt, kb, j) + idxB].astype(np.int64)
+                    acc[i + j] += A @ B.T
+            assert np.max(np.abs(acc)) < 2 ** 31
+            for r in range(TM):
+                q = T * TM + r
+                a = (acc[0, r] * 2.0 ** 48 + acc[1, r] * 2.0 ** 40) + (acc[2, r] * 2.0 ** 32 + acc[3, r] * 2.0 ** 24)
+                y = a * 2.0 ** (int(xe[q * 4 + t]) - SHIFT) * 2.0 ** (ke[s].astype(float) - SHIFT)
+                scale = np.max(np.abs(X[t, q])) * np.max(np.abs(K[s]), axis=1) + 1e-300
+                worst = max(worst, float(np.max(np.abs(y[:CG] - X[t, q] @ K[s].T) / scale)))
+    assert worst <= 2e-7, worst
+
+
+def test_adjoint_sub_tile_dequantisation():
+    rng = np.random.default_rng(2)
+    nt, D, Q, CG, SUB, Dpad = 1, 240, 128, 8, 16, 240
+    X, K, X8, xe, K8, ke = _build(rng, nt, D, Q, CG)
+    worst = 0.0
+    for qb in range(0, Q, SUB):
+        T, r0 = divmod(qb, TM)
+        raw = np.zeros(3 * 2 * DIG * 2048, np.int8)
+        for blk in range(3 * 2 * DIG):
+            src = T * 3 * 2 * STAGE + blk * XBLK + (r0 >> 3) * 1024
+            raw[blk * 2048:(blk + 1) * 2048] = X8[src:src + 2048]
+        for t in range(3):
+            for j in range(SUB):
+                sc = 2.0 ** (int(xe[(qb + j) * 4 + t]) - SHIFT)
+                m = np.max(np.abs(X[t, qb + j]))
+                for d in range(0, Dpad, 4):
+                    o = sw128(j, d & 127)
+                    for b in range(4):
+                        v = 0
+                        for l in range(DIG):
+                            v = v * 256 + int(raw[((t * 2 + (d >> 7)) * DIG + l) * 2048 + o + b])
+                        x = float(np.float32(v * sc))
+                        ref = X[t, qb + j, d + b] if d + b < D else 0.0
+                        if m > 0:
+                            worst = max(worst, abs(x - ref) / m)
+    assert worst <= 1.2e-7, worst
