@@ -55,6 +55,9 @@ def parse_args():
     ap.add_argument("--ncells", type=int, default=2000)
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-configs", action="store_true",
+                    help="time the compiled reference's objective on the smaller workloads (one JSON line each) "
+                         "and exit")
     return ap.parse_args()
 
 
@@ -217,9 +220,6 @@ def row_counts(cell, rcut):
 # types x 12 B-spline coefficients of f (10 knots) x 10 of g (8 knots) = 240.
 FM_DPAD_MEAM2K = 240
 
-# Algorithmic bytes of one launch per kernel (None where not stated): the
-# moment contractions stream the FP32 moments once (4 B x 3 x 240 per slot)
-# plus their candidate-side operand (4 B x 3 per slot-candidate, in and out).
 # Algorithmic bytes per launch of the moment contractions: the moments read
 # once (FP32, or four 8-bit digits of 256 padded features per kind when the
 # forward runs on the tensor cores) and the per-slot sums written (FP64 Y) or
@@ -298,6 +298,50 @@ def cpu_reference(spec, cells, stats, P, reps, target_triplets=1.0e7, max_procs=
                                                      sample_trip, reps, P))
     return {"obj_evals_per_s": obj_evals, "objgrad_evals_per_s": obj_evals / (P + 1), "cores": len(procs),
             "sample": desc, "cpu": cpu_model()}, None
+
+
+def cpu_configs(reps=3):
+    """The reference's objective on the three smaller workloads, on the host
+    cores: the EAM database of 20 bcc cells (54 atoms), the single-species
+    MEAM database of 200 cells (its 10 gradient points and the L-BFGS /
+    Powell comparison use the same database) and the 500-cell MEAM
+    population database.  One single-threaded process on the whole database,
+    and the whole-core decomposition of cpu_reference.  Rows counted without
+    the evaluator library."""
+    from meamzilla_b200 import synth
+    out = []
+    for name in ("eam54", "meam200", "meam500"):
+        spec, cells = synth.make_workload(name, seed=0)
+        rcut = synth.WORKLOADS[name][2]
+        rows = [row_counts(c, rcut) for c in cells]
+        ntrip = int(sum(int((r * (r - 1) // 2).sum()) for r in rows)) if spec.style != "eam/spline" else 0
+        stats = {"ntriplets": max(ntrip, 1), "rows_per_cell": rows, "natoms": sum(c.natoms for c in cells),
+                 "npairs": int(sum(int(r.sum()) for r in rows))}
+        # one process, the whole database (-np 1)
+        import oracle
+        tmp = tempfile.mkdtemp(prefix="mzcfg_")
+        par = synth.write_case(os.path.join(tmp, name), spec, cells)
+        t0 = time.perf_counter()
+        r1 = subprocess.run([oracle.MZREF_FAST, "-p", par, "-reps", str(reps), "-q"], capture_output=True,
+                            text=True, timeout=1800)
+        sec1 = None
+        for line in r1.stdout.splitlines():
+            if line.startswith("seconds_per_eval"):
+                sec1 = float(line.split()[1])
+        subprocess.run(["rm", "-rf", tmp])
+        line = {"workload": name, "ncells": len(cells), "natoms": stats["natoms"], "npairs": stats["npairs"],
+                "ntriplets": ntrip, "ncoeff": spec_ncoeff(spec), "cpu": cpu_model(),
+                "one_process": {"objective_evals_per_s": (1.0 / sec1) if sec1 else None, "cores": 1,
+                                "reps": reps},
+                "wall_s": time.perf_counter() - t0}
+        if spec.style != "eam/spline":
+            stats["rows_per_cell"] = rows
+            res, err = cpu_reference(spec, cells, stats, spec_ncoeff(spec), reps, target_triplets=2.0e6)
+            line["all_cores"] = ({"objective_evals_per_s": res["obj_evals_per_s"], "cores": res["cores"],
+                                  "sample": res["sample"]} if res else {"unavailable": err})
+        out.append(line)
+        print(json.dumps(line), flush=True)
+    return out
 
 
 # ------------------------------------------------------------------- arms
@@ -586,6 +630,10 @@ def run_mine(args, world, rank, local):
 def main():
     args = parse_args()
     world, rank, local = dist_setup(args)
+    if args.cpu_configs:
+        if rank == 0:
+            cpu_configs()
+        return
     if args.impl == "reference":
         run_reference_arm(args, world, rank)
     else:

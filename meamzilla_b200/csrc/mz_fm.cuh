@@ -970,6 +970,11 @@ __global__ void __launch_bounds__(256, 2) k_fm_adj_pre(DevDb db, DevPot pot, con
         const double ap = lx * u.x + ly * u.y + lz * u.z;
         const double l1 = lx * e[0] + ly * e[1] + lz * e[2], l2 = lx * e[3] + ly * e[4] + lz * e[5];
         K += ap * ((double)v.drho + (double)v.df * yp[0]) + (double)v.f * (double)u.w * (l1 * yp[CG] + l2 * yp[2 * CG]);
+        // kept for pass 2 in this slot's dL/dY words, which pass 2 then overwrites
+        float *yb = Ybq + (size_t)p * 3 * CG;
+        yb[0] = (float)ap;
+        yb[CG] = (float)l1;
+        yb[2 * CG] = (float)l2;
       }
       const float ch = (float)((eps * U.grad + U.grad2 * K) * drt + kap * dpen);
       const float dF = (float)U.grad;
@@ -984,13 +989,9 @@ __global__ void __launch_bounds__(256, 2) k_fm_adj_pre(DevDb db, DevPot pot, con
         const double *yp = Yq + (size_t)p * 3 * CG;
         const float G = (float)yp[0], Y1 = (float)yp[CG], Y2 = (float)yp[2 * CG];
         const float4 u = st.uf[ql];
-        const double *e = st.e + ql * 6;
-        float lx, ly, lz;
-        lam(ql, u, lx, ly, lz);
-        const float ap = lx * u.x + ly * u.y + lz * u.z;
-        const float l1 = (float)(lx * e[0] + ly * e[1] + lz * e[2]), l2 = (float)(lx * e[3] + ly * e[4] + lz * e[5]);
-        const float B = dF * v.f * u.w;
         float *yb = Ybq + (size_t)p * 3 * CG;
+        const float ap = yb[0], l1 = yb[CG], l2 = yb[2 * CG];  // from pass 1
+        const float B = dF * v.f * u.w;
         yb[0] = 0.5f * v.f * ch + ap * dF * v.df;
         yb[CG] = B * l1;
         yb[2 * CG] = B * l2;
