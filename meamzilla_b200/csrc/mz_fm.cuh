@@ -1099,9 +1099,9 @@ __global__ void __launch_bounds__(256, 1) k_fm_gemm_adj(FmPlan fp) {
   // DIG8: the staged digits of sub-tile k -> its FP32 operand
   auto dequant = [&](int k, float *bx) {
     const int64_t qb = (int64_t)(tb + k / NSUB) * FM_TILE + (k % NSUB) * FM_SUB;
-    if (tid < 3 * FM_SUB) {
-      const int t = tid / FM_SUB, j = tid % FM_SUB;
-      rsc[tid] = ldexp(1.0, (int)fp.xe[(qb + j) * 4 + t] - FM8_SHIFT);
+    for (int i = tid; i < 3 * FM_SUB; i += blockDim.x) {  // the block can be a single warp
+      const int t = i / FM_SUB, j = i % FM_SUB;
+      rsc[i] = ldexp(1.0, (int)fp.xe[(qb + j) * 4 + t] - FM8_SHIFT);
     }
     __syncthreads();
     const int nd4 = fp.Dpad / 4;
