@@ -336,7 +336,9 @@ def cpu_configs(reps=3):
                 "wall_s": time.perf_counter() - t0}
         if spec.style != "eam/spline":
             stats["rows_per_cell"] = rows
-            res, err = cpu_reference(spec, cells, stats, spec_ncoeff(spec), reps, target_triplets=2.0e6)
+            # one disjoint run of cells per host core
+            target = max(1.0e5, ntrip / float(os.cpu_count() or 1))
+            res, err = cpu_reference(spec, cells, stats, spec_ncoeff(spec), reps, target_triplets=target)
             line["all_cores"] = ({"objective_evals_per_s": res["obj_evals_per_s"], "cores": res["cores"],
                                   "sample": res["sample"]} if res else {"unavailable": err})
         out.append(line)

@@ -361,8 +361,9 @@ mz_status mz_profile(mz_ctx *ctx, int on);
  * 32-bit sums), 0 when they use the row kernels.  MZ_FM=0 in the
  * environment at mz_create keeps the row kernels, MZ_FM=2 always takes the
  * moment path where it applies, the default lets the tuner time both;
- * MZ_FM8=0 keeps the moment path's forward on the CUDA cores.  No reference
- * counterpart. */
+ * MZ_FM8=0 keeps the moment path's forward on the CUDA cores (the default
+ * uses the tensor cores where the digits fit in device memory).  No
+ * reference counterpart. */
 mz_status mz_moment_path(const mz_ctx *ctx, int precision, int grad, int *on);
 mz_status mz_kernel_times(mz_ctx *ctx, double *ms, int64_t *launches);
 

@@ -132,7 +132,7 @@ struct mz_ctx {
     size_t smem_pre = 0;
   } fm;
   int fm_mode = 1;
-  int fm8_mode = 0;  // MZ_FM8=1: the forward contraction on the tensor cores
+  int fm8_mode = 1;  // MZ_FM8=0 keeps the forward contraction on the CUDA cores
   int smem_optin = 0;  // largest dynamic shared memory a block may opt into
   bool fm_on = false;  // the moment path in force for mixed launches
   double *d_gram = nullptr;  // partial sums of mz_gram_device, grown on demand
@@ -1406,7 +1406,7 @@ mz_status mz_create(const mz_db *dbh, const mz_pot *poth, const mz_settings *set
     }
     {
       const char *env = std::getenv("MZ_FM8");
-      ctx->fm8_mode = (env && env[0] == '1') ? 1 : 0;
+      ctx->fm8_mode = (env && env[0] == '0') ? 0 : 1;
     }
     // tensor-core forward (mixed precision, MEAM with TC_NB B-spline coefficients per g spline)
     {
