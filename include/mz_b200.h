@@ -358,7 +358,8 @@ mz_status mz_profile(mz_ctx *ctx, int on);
  * contractions of per-slot moments built once per database: MZ_K_FM_*), 2
  * when they do and its forward contraction runs on the tensor cores in
  * integers (tcgen05 kind::i8 over four 8-bit digits of each operand, exact
- * 32-bit sums), 0 when they use the row kernels.  MZ_FM=0 in the
+ * 32-bit sums), 3 when its adjoint contraction does too (MZ_FM8ADJ=0 keeps
+ * that one on the CUDA cores), 0 when they use the row kernels.  MZ_FM=0 in the
  * environment at mz_create keeps the row kernels, MZ_FM=2 always takes the
  * moment path where it applies, the default lets the tuner time both;
  * MZ_FM8=0 keeps the moment path's forward on the CUDA cores (the default

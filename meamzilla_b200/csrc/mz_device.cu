@@ -126,13 +126,17 @@ struct mz_ctx {
   // lets the tuner time it against the row kernels.
   struct Fm {
     bool eligible = false, ready = false, failed = false;
-    bool tc8 = false;  // the forward contraction on the tensor cores (mz_fm8.cuh)
+    bool tc8 = false;   // the forward contraction on the tensor cores (mz_fm8.cuh)
+    bool tc8a = false;  // and the adjoint contraction
+    signed char *Z8 = nullptr;
+    int *ze = nullptr;
     FmPlan plan{};
     int CGmax = 8, ngroups_max = 1;
     size_t smem_pre = 0;
   } fm;
   int fm_mode = 1;
   int fm8_mode = 1;  // MZ_FM8=0 keeps the forward contraction on the CUDA cores
+  int fm8a_mode = 1;  // MZ_FM8ADJ=0 keeps the adjoint contraction on the CUDA cores
   int smem_optin = 0;  // largest dynamic shared memory a block may opt into
   bool fm_on = false;  // the moment path in force for mixed launches
   double *d_gram = nullptr;  // partial sums of mz_gram_device, grown on demand
@@ -400,6 +404,11 @@ bool fm_prepare(mz_ctx *ctx) {
            extra - bytesX + bytes8 <= (size_t)(0.85 * (double)freeb) &&
            fm8_smem(fp.nt) <= (size_t)ctx->smem_optin &&
            fm_adj_smem(fp.Dpad, 64, true) <= (size_t)ctx->smem_optin;
+  // the adjoint on the tensor cores as well: Z's digits per candidate group
+  const size_t bytesZ = G * ntile8 * 3 * FM8_ZSTAGE + sizeof(int) * G * ntile8 * FM8_NC;
+  fm.tc8a = fm.tc8 && ctx->fm8a_mode != 0 && extra - bytesX + bytes8 + bytesZ <= (size_t)(0.85 * (double)freeb) &&
+            fm8_adj_smem() <= (size_t)ctx->smem_optin &&
+            (size_t)3 * FM8_ZSTAGE + 256 <= (size_t)ctx->smem_optin;
   auto pick = [&](Need &x) -> void * {
     return x.need_bytes <= x.have_bytes ? x.have : (void *)dalloc<unsigned char>(ctx, x.need_bytes);
   };
@@ -436,6 +445,12 @@ bool fm_prepare(mz_ctx *ctx) {
     fp.X8 = X8;
     fp.xe = xe;
     smem_attr(k_fm_gemm_fwd8, fm8_smem(fp.nt));
+    if (fm.tc8a) {
+      fm.Z8 = dalloc<signed char>(ctx, G * ntile8 * 3 * FM8_ZSTAGE);
+      fm.ze = dalloc<int>(ctx, G * ntile8 * FM8_NC);
+      smem_attr(k_fm_gemm_adj8, fm8_adj_smem());
+      smem_attr(k_fm_zdig, (size_t)3 * FM8_ZSTAGE);
+    }
   }
   fp.CG = fm.CGmax;
   k_fm_features<<<ctx->natoms, 256, 0, ctx->stream>>>(ctx->db, ctx->pot, ctx->d_geom, fp, X, E, X8, xe);
@@ -533,7 +548,13 @@ void enqueue_fm(mz_ctx *ctx, int n, double *d_obj, double *d_errvec, double *d_f
   {
     Bracket b(ctx, MZ_K_FM_ADJ);
     const int threads = ((fp.Dpad / FM_ROWS) * (CG / 8) + 31) / 32 * 32;
-    if (ctx->fm.tc8)
+    if (ctx->fm.tc8a) {
+      const int ntile8 = (int)(fp.Q / FM8_TM);
+      k_fm_zdig<<<dim3(ntile8, G), 256, (size_t)3 * FM8_ZSTAGE, st>>>(fp, ctx->fm.Z8, ctx->fm.ze);
+      ck(cudaGetLastError(), "k_fm_zdig launch");
+      k_fm_gemm_adj8<<<dim3(fp.nctas_adj, G), FM8_ATHREADS, fm8_adj_smem(), st>>>(fp, ctx->fm.Z8, ctx->fm.ze,
+                                                                                   ctx->d_err);
+    } else if (ctx->fm.tc8)
       k_fm_gemm_adj<true><<<dim3(fp.nctas_adj, G), std::min(threads, 256), fm_adj_smem(fp.Dpad, CG, true), st>>>(fp);
     else
       k_fm_gemm_adj<false><<<dim3(fp.nctas_adj, G), std::min(threads, 256), fm_adj_smem(fp.Dpad, CG), st>>>(fp);
@@ -1408,6 +1429,10 @@ mz_status mz_create(const mz_db *dbh, const mz_pot *poth, const mz_settings *set
       const char *env = std::getenv("MZ_FM8");
       ctx->fm8_mode = (env && env[0] == '0') ? 0 : 1;
     }
+    {
+      const char *env = std::getenv("MZ_FM8ADJ");
+      ctx->fm8a_mode = (env && env[0] == '0') ? 0 : 1;
+    }
     // tensor-core forward (mixed precision, MEAM with TC_NB B-spline coefficients per g spline)
     {
       const char *env = std::getenv("MZ_TC");  // opt-in: "1"
@@ -1616,7 +1641,7 @@ mz_status mz_moment_path(const mz_ctx *ctx, int precision, int grad, int *on) {
   return guarded([&] {
     if (!ctx || !on || (precision != MZ_FP64 && precision != MZ_MIXED)) throw Failure{MZ_ERR_ARG, "bad argument"};
     const mz_ctx::Tune &t = ctx->tune[precision][grad ? 1 : 0];
-    *on = (t.done && t.fm && ctx->fm.ready) ? (ctx->fm.tc8 ? 2 : 1) : 0;
+    *on = (t.done && t.fm && ctx->fm.ready) ? (ctx->fm.tc8a ? 3 : ctx->fm.tc8 ? 2 : 1) : 0;
   });
 }
 

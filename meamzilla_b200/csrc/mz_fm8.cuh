@@ -291,3 +291,278 @@ __global__ void __launch_bounds__(FM8_THREADS, 1) k_fm_gemm_fwd8(FmPlan fp, int 
 }
 
 }  // namespace mzb
+
+namespace mzb {
+
+// ------------------------------------------------------- integer adjoint
+//
+//   Kbar_s[d][c] = sum_{t,q} X[t][q][d] Ybar[q][t][c]                 (k_fm_gemm_adj's sum)
+//
+// With X = 2^(e_q - 30) X_int the row scale folds into the other operand,
+// Z[t][q][c] = 2^(e_q - 30) Ybar[q][t][c], so Kbar = sum X_int Z.  k_fm_zdig
+// writes Z of every 128-slot tile as four balanced base-256 digits of a
+// 31-bit integer with one power-of-two scale per (tile, candidate) over the
+// tile's three kinds (Z = 2^(e_Tc - 30) Z_int); padding slots are zero.  The
+// MMA reads the moments' digit blocks as they are stored for the forward --
+// 128 slot rows of 128 feature bytes -- as an MN-major operand (M = 128
+// features, K = slots: 8-row groups 1 KiB apart), and Z's as a K-major one
+// (N = 64 candidates, K = slots), so one tile's three kinds are 3 x 4 K steps
+// of 32 slots per 128-feature half, ten digit pairs each, into the four class
+// accumulators of each half (all 512 TMEM columns; at most 4 x 384 x 128^2
+// < 2^31 per tile).  At the end of a tile the sixteen epilogue warps (lane
+// quarter x feature half x candidate half) read them out and add
+//   2^(e_Tc - 30) (acc_0 2^48 + acc_1 2^40 + acc_2 2^32 + acc_3 2^24)
+// to FP64 sums held per thread (32 candidates of one feature), written to the
+// CTA's partial of the type when the CTA's run of tiles changes type and at
+// its end.
+//   Z8 [ngroups][ntile8][3 kinds][4 digits][64 candidates x 128 B]   8 KB blocks
+//   ze [ngroups][ntile8][64]                e_Tc (int32)
+
+constexpr int FM8_ZBLK = FM8_NC * 128;         // one (tile, kind, digit) block of Z8: 8 KB
+constexpr int FM8_ZSTAGE = FM8_DIG * FM8_ZBLK;  // one (tile, kind): 32 KB
+constexpr int FM8_ATHREADS = 576;              // producer, MMA, sixteen epilogue warps
+
+__host__ __device__ inline size_t z8_block(int gy, int64_t T, int64_t ntile8, int t, int l) {
+  return ((((size_t)gy * ntile8 + T) * 3 + t) * FM8_DIG + l) * FM8_ZBLK;
+}
+
+// Z's digits of one tile (blockIdx.x) of group blockIdx.y: the candidates'
+// exponents over the tile, the digits into a shared image of the tile's
+// 96 KB of blocks, written out in 16-byte pieces.
+__global__ void __launch_bounds__(256) k_fm_zdig(FmPlan fp, signed char *__restrict__ Z8, int *__restrict__ ze) {
+  extern __shared__ __align__(16) unsigned char zsm[];  // [3][4][8 KB]
+  __shared__ int se[FM8_NC];
+  const int64_t T = blockIdx.x, ntile8 = fp.Q / FM8_TM;
+  const int gy = blockIdx.y, CG = fp.CG, tid = threadIdx.x;
+  const int s = fm_tile_type(fp, (int)(2 * T));
+  const int64_t qend = fp.qend[s];
+  if (tid < FM8_NC) se[tid] = -1000;
+  for (int i = tid; i < 3 * FM8_ZSTAGE / 16; i += blockDim.x) reinterpret_cast<int4 *>(zsm)[i] = make_int4(0, 0, 0, 0);
+  __syncthreads();
+  auto zval = [&](int idx, int &t, int &c, int &r) -> double {
+    r = idx / (3 * CG);
+    const int rem = idx % (3 * CG);
+    t = rem / CG;
+    c = rem % CG;
+    const int64_t q = T * FM8_TM + r;
+    if (q >= qend) return 0.0;
+    return ldexp((double)fp.Yb[(((size_t)gy * fp.Q + q) * 3 + t) * CG + c], (int)fp.xe[q * 4 + t] - FM8_SHIFT);
+  };
+  for (int idx = tid; idx < FM8_TM * 3 * CG; idx += blockDim.x) {
+    int t, c, r;
+    const double z = zval(idx, t, c, r);
+    if (z != 0.0) atomicMax(se + c, fm8_exponent(fabs(z)));
+  }
+  __syncthreads();
+  for (int idx = tid; idx < FM8_TM * 3 * CG; idx += blockDim.x) {
+    int t, c, r;
+    const double z = zval(idx, t, c, r);
+    const int e = se[c] == -1000 ? 0 : se[c];
+    signed char dg[FM8_DIG];
+    digits256(llrint(ldexp(z, FM8_SHIFT - e)), dg);
+    const uint32_t o = sw128_byte(c, r);
+#pragma unroll
+    for (int l = 0; l < FM8_DIG; ++l) zsm[(size_t)(t * FM8_DIG + l) * FM8_ZBLK + o] = dg[l];
+  }
+  __syncthreads();
+  int4 *dst = reinterpret_cast<int4 *>(Z8 + z8_block(gy, T, ntile8, 0, 0));
+  for (int i = tid; i < 3 * FM8_ZSTAGE / 16; i += blockDim.x) dst[i] = reinterpret_cast<const int4 *>(zsm)[i];
+  if (tid < FM8_NC) ze[((size_t)gy * ntile8 + T) * FM8_NC + tid] = se[tid] == -1000 ? 0 : se[tid];
+}
+
+__host__ __device__ constexpr size_t fm8_adj_smem() {
+  return 1024 + 2 * (size_t)FM8_STAGE + 2 * (size_t)FM8_ZSTAGE + sizeof(uint64_t) * 12 + 16;
+}
+
+__global__ void __maxnreg__(112) k_fm_gemm_adj8(FmPlan fp, const signed char *__restrict__ Z8,
+                                                                 const int *__restrict__ ze, int *__restrict__ err) {
+  extern __shared__ __align__(16) unsigned char sm8raw[];
+  const uint32_t raw = tc::smem_u32(sm8raw);
+  unsigned char *sA = sm8raw + (((raw + 1023u) & ~1023u) - raw);  // [2][64 KB] moments' digits (tile, kind, half)
+  unsigned char *sB = sA + 2 * FM8_STAGE;                          // [2][32 KB] Z digits (tile, kind)
+  uint64_t *afull = reinterpret_cast<uint64_t *>(sB + 2 * FM8_ZSTAGE);
+  uint64_t *aempty = afull + 2, *bfull = aempty + 2, *bempty = bfull + 2;
+  uint64_t *accf = bempty + 2, *acce = accf + 1, *mdone = acce + 1;
+  uint32_t *tslot = reinterpret_cast<uint32_t *>(mdone + 1);
+
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int gy = blockIdx.y, CG = fp.CG, nt = fp.nt;
+  const int64_t ntile8 = fp.Q / FM8_TM;
+  const int64_t per = (ntile8 + gridDim.x - 1) / gridDim.x;
+  const int64_t tb = (int64_t)blockIdx.x * per, te = min(ntile8, tb + per);
+  double *Kb = fp.Kbar + ((size_t)gy * gridDim.x + blockIdx.x) * nt * fp.Dpad * CG;
+  for (int i = tid; i < nt * fp.Dpad * CG; i += blockDim.x) Kb[i] = 0.0;
+
+  if (tid == 0) {
+    for (int i = 0; i < 2; ++i) {
+      tc::mbar_init(afull + i, 1);
+      tc::mbar_init(aempty + i, 1);
+      tc::mbar_init(bfull + i, 1);
+      tc::mbar_init(bempty + i, 1);
+    }
+    tc::mbar_init(accf, 1);
+    tc::mbar_init(acce, 16);
+    tc::mbar_init(mdone, 1);
+  }
+  if (warp == 1) tc::tmem_alloc(tslot, 512);
+  tc::fence_before_sync();
+  __syncthreads();
+  tc::fence_after_sync();
+  const uint32_t tm = *tslot;
+
+  if (warp == 0) {
+    // ---------------- producer: per (tile, kind) Z's 32 KB, then the moments' two 64 KB halves
+    if (lane == 0) {
+      int64_t ia = 0, ib = 0;
+      bool ok = true;
+      for (int64_t T = tb; T < te && ok; ++T)
+        for (int t = 0; t < 3 && ok; ++t) {
+          const int bst = (int)(ib & 1);
+          if (ib >= 2 && !tc::mbar_wait(bempty + bst, (uint32_t)(((ib >> 1) & 1) ^ 1), FM8_WAIT)) {
+            atomicExch(err, 5);
+            ok = false;
+            break;
+          }
+          tc::mbar_expect_tx(bfull + bst, FM8_ZSTAGE);
+          tc::bulk_g2s(sB + bst * FM8_ZSTAGE, Z8 + z8_block(gy, T, ntile8, t, 0), FM8_ZSTAGE, bfull + bst);
+          ++ib;
+          for (int kb = 0; kb < 2; ++kb) {
+            const int ast = (int)(ia & 1);
+            if (ia >= 2 && !tc::mbar_wait(aempty + ast, (uint32_t)(((ia >> 1) & 1) ^ 1), FM8_WAIT)) {
+              atomicExch(err, 5);
+              ok = false;
+              break;
+            }
+            tc::mbar_expect_tx(afull + ast, FM8_STAGE);
+            tc::bulk_g2s(sA + ast * FM8_STAGE, fp.X8 + x8_block(T, t, kb, 0), FM8_STAGE, afull + ast);
+            ++ia;
+          }
+        }
+      // copies in flight land before the CTA can exit
+      for (int64_t j = ia > 2 ? ia - 2 : 0; j < ia; ++j)
+        if (!tc::mbar_wait(afull + (int)(j & 1), (uint32_t)((j >> 1) & 1), FM8_WAIT)) atomicExch(err, 5);
+      for (int64_t j = ib > 2 ? ib - 2 : 0; j < ib; ++j)
+        if (!tc::mbar_wait(bfull + (int)(j & 1), (uint32_t)((j >> 1) & 1), FM8_WAIT)) atomicExch(err, 5);
+    }
+  } else if (warp == 1) {
+    // ---------------- MMA issue: A = moments (MN-major), B = Z (K-major)
+    if (lane == 0) {
+      constexpr uint32_t idesc = tc::idesc_s8(FM8_TM, FM8_NC, 1, 0);
+      // the ten digit pairs (i, j), their class i + j and the first of each
+      // class, four bits per pair
+      constexpr int NP = 10;
+      constexpr uint64_t PI = 0x3210210100ull, PJ = 0x0123012010ull, PM = 0x3333222110ull, PF = 0x0001001011ull;
+      bool ok = true;
+      int64_t ia = 0, ib = 0, tile = 0;
+      for (int64_t T = tb; T < te && ok; ++T, ++tile) {
+        if (tile >= 1 && !tc::mbar_wait(acce, (uint32_t)((tile - 1) & 1), FM8_WAIT)) {
+          atomicExch(err, 6);
+          ok = false;
+          break;
+        }
+        tc::fence_after_sync();
+        for (int t = 0; t < 3 && ok; ++t) {
+          const int bst = (int)(ib & 1);
+          if (!tc::mbar_wait(bfull + bst, (uint32_t)((ib >> 1) & 1), FM8_WAIT)) {
+            atomicExch(err, 6);
+            ok = false;
+            break;
+          }
+          tc::fence_after_sync();
+          const uint32_t b0 = tc::smem_u32(sB + bst * FM8_ZSTAGE);
+          for (int kb = 0; kb < 2; ++kb) {
+            const int ast = (int)(ia & 1);
+            if (!tc::mbar_wait(afull + ast, (uint32_t)((ia >> 1) & 1), FM8_WAIT)) {
+              atomicExch(err, 6);
+              ok = false;
+              break;
+            }
+            tc::fence_after_sync();
+            const uint32_t a0 = tc::smem_u32(sA + ast * FM8_STAGE);
+#pragma unroll 1
+            for (int kk = 0; kk < 4; ++kk)
+#pragma unroll 1
+              for (int p = 0; p < NP; ++p) {
+                const int i = (int)((PI >> (4 * p)) & 15), j = (int)((PJ >> (4 * p)) & 15);
+                const int m = (int)((PM >> (4 * p)) & 15), f = (int)((PF >> (4 * p)) & 15);
+                // 32 slot rows per K step: 4 groups of 8 rows, 1 KiB apart
+                const uint64_t ad = tc::desc_sw128(a0 + i * FM8_XBLK + 4096 * kk, FM8_STAGE, 1024);
+                const uint64_t bd = tc::desc_sw128(b0 + j * FM8_ZBLK + 32 * kk, 16, 1024);
+                const uint32_t d = tm + (uint32_t)(kb * 256 + m * FM8_NC);
+                tc::mma_s8(d, ad, bd, idesc, (t == 0 && kk == 0 && f) ? 0u : 1u);
+              }
+            tc::commit(aempty + ast);
+            ++ia;
+          }
+          if (!ok) break;
+          tc::commit(bempty + bst);
+          ++ib;
+        }
+        if (ok) tc::commit(accf);
+      }
+      tc::commit(mdone);
+      if (!tc::mbar_wait(mdone, 0, FM8_WAIT)) atomicExch(err, 6);
+    }
+  } else {
+    // ---------------- epilogue: warps 2..17, lane quarter warp % 4, feature half and
+    // candidate half from (warp - 2) / 4
+    constexpr int NCH = FM8_NC / 2;
+    const int grp = (warp - 2) >> 2, quarter = warp & 3, half = grp & 1, c0 = (grp >> 1) * NCH;
+    const int d = half * FM8_TM + 32 * quarter + lane;
+    double acc[NCH];
+#pragma unroll
+    for (int c = 0; c < NCH; ++c) acc[c] = 0.0;
+    auto flush = [&](int s) {
+      if (d < fp.Dpad) {
+        double *kb = Kb + ((size_t)s * fp.Dpad + d) * CG + c0;
+#pragma unroll
+        for (int c = 0; c < NCH; ++c)
+          if (c0 + c < CG) kb[c] += acc[c];
+      }
+#pragma unroll
+      for (int c = 0; c < NCH; ++c) acc[c] = 0.0;
+    };
+    int cur = -1;
+    int64_t tile = 0;
+    bool ok = true;
+    for (int64_t T = tb; T < te && ok; ++T, ++tile) {
+      const int s = fm_tile_type(fp, (int)(2 * T));
+      if (s != cur && cur >= 0) flush(cur);
+      cur = s;
+      const int *zt = ze + ((size_t)gy * ntile8 + T) * FM8_NC;
+      if (!tc::mbar_wait(accf, (uint32_t)(tile & 1), FM8_WAIT)) {
+        atomicExch(err, 7);
+        ok = false;
+        break;
+      }
+      tc::fence_after_sync();
+      const uint32_t ta = tm + ((uint32_t)(32 * quarter) << 16) + (uint32_t)(half * 256 + c0);
+#pragma unroll
+      for (int cb = 0; cb < NCH / 4; ++cb) {
+        int v[FM8_CLS][4];
+#pragma unroll
+        for (int m = 0; m < FM8_CLS; ++m) tc::tmem_ld4i(ta + m * FM8_NC + cb * 4, v[m]);
+        const int4 ez = *reinterpret_cast<const int4 *>(zt + c0 + cb * 4);
+        tc::tmem_wait_ld();
+        const int e4[4] = {ez.x, ez.y, ez.z, ez.w};
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          const double a = ((double)v[0][u] * 281474976710656.0 + (double)v[1][u] * 1099511627776.0) +
+                           ((double)v[2][u] * 4294967296.0 + (double)v[3][u] * 16777216.0);
+          // 2^(e - 30), e in [-100, 100]: a normal double built from its exponent field
+          acc[cb * 4 + u] += a * __longlong_as_double((long long)(e4[u] - FM8_SHIFT + 1023) << 52);
+        }
+      }
+      tc::fence_before_sync();
+      __syncwarp();
+      if (lane == 0) tc::mbar_arrive(acce);
+    }
+    if (cur >= 0) flush(cur);
+  }
+  tc::fence_before_sync();
+  __syncthreads();
+  tc::fence_after_sync();
+  if (warp == 1) tc::tmem_dealloc(tm, 512);
+}
+
+}  // namespace mzb

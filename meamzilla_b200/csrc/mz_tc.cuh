@@ -43,10 +43,12 @@ __host__ __device__ constexpr uint32_t idesc_tf32(int M, int N, int a_mn, int b_
          ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
 }
 
-// Instruction descriptor of kind::i8: D S32, A and B signed 8-bit, both
-// K-major, N >> 3 and M >> 4.
-__host__ __device__ constexpr uint32_t idesc_s8(int M, int N) {
-  return (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+// Instruction descriptor of kind::i8: D S32, A and B signed 8-bit, the
+// majors (0 = K-major, 1 = MN-major: allowed for 8-bit integers), N >> 3 and
+// M >> 4.
+__host__ __device__ constexpr uint32_t idesc_s8(int M, int N, int a_mn = 0, int b_mn = 0) {
+  return (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)a_mn << 15) | ((uint32_t)b_mn << 16) |
+         ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
 }
 
 // D[tmem] (+)= A * B^T over signed 8-bit operands, S32 accumulator, one thread.
@@ -154,6 +156,18 @@ __device__ __forceinline__ void tmem_ld16i(uint32_t taddr, int *v) {
       : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
         "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
       : "r"(taddr));
+}
+// 4 consecutive 32-bit columns of this thread's lane.
+__device__ __forceinline__ void tmem_ld4i(uint32_t taddr, int *v) {
+  asm volatile("tcgen05.ld.sync.aligned.32x32b.x4.b32 {%0,%1,%2,%3}, [%4];"
+               : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3])
+               : "r"(taddr));
+}
+// 8 consecutive 32-bit columns of this thread's lane.
+__device__ __forceinline__ void tmem_ld8i(uint32_t taddr, int *v) {
+  asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+               : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7])
+               : "r"(taddr));
 }
 __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 

@@ -344,12 +344,14 @@ class Evaluator:
         check(lib().mz_moment_path(self._h, int(precision), 1 if grad else 0, C.byref(on)))
         return dict(forward_block_slots=int(c[0]), adjoint_block_slots=int(c[1]), adjoint_ctas=int(c[2]),
                     forward_candidates_per_cta=int(c[3]), adjoint_candidates_per_cta=int(c[4]),
-                    triplet_moments=bool(on.value), moment_forward_tensor_cores=on.value == 2)
+                    triplet_moments=bool(on.value), moment_forward_tensor_cores=on.value >= 2,
+                    moment_adjoint_tensor_cores=on.value == 3)
 
     def moment_path(self, precision=MZ_MIXED, grad=True) -> int:
         """Non-zero when the tuned (precision, gradient) launches run the
-        triplet-moment path (mixed-precision meam/spline): 1 with the forward
-        contraction on the CUDA cores, 2 with it on the tensor cores."""
+        triplet-moment path (mixed-precision meam/spline): 1 with the
+        contractions on the CUDA cores, 2 with the forward one on the tensor
+        cores, 3 with both."""
         on = C.c_int()
         check(lib().mz_moment_path(self._h, int(precision), 1 if grad else 0, C.byref(on)))
         return int(on.value)

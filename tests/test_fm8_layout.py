@@ -142,3 +142,56 @@ def test_adjoint_sub_tile_dequantisation():
                         if m > 0:
                             worst = max(worst, abs(x - ref) / m)
     assert worst <= 1.2e-7, worst
+
+
+ZBLK = NC * 128
+
+
+def z8_block(T, t, l):
+    return ((T * 3 + t) * DIG + l) * ZBLK
+
+
+def test_adjoint_class_sums_read_moments_mn_major():
+    """The adjoint's MMAs read the moments' digit blocks as an MN-major
+    operand (features along M, slots along K) and Z = 2^(e_q - 30) Ybar as
+    K-major digit blocks with one exponent per (tile, candidate); the class
+    sums and the epilogue give Kbar = sum_{t,q} X Ybar."""
+    rng = np.random.default_rng(3)
+    nt, D, Q, CG = 1, 240, 256, 64
+    X, K, X8, xe, K8, ke = _build(rng, nt, D, Q, CG)
+    Yb = (rng.normal(size=(Q, 3, CG)) * np.exp(rng.normal(size=(Q, 1, 1)) * 2)).astype(np.float32)
+    ntile8 = Q // TM
+    Z8 = np.zeros(ntile8 * 3 * DIG * ZBLK, np.int8)
+    ze = np.zeros((ntile8, NC), int)
+    for T in range(ntile8):
+        Z = np.zeros((3, TM, NC))
+        for t in range(3):
+            for r in range(TM):
+                q = T * TM + r
+                Z[t, r, :CG] = Yb[q, t].astype(np.float64) * 2.0 ** (int(xe[q * 4 + t]) - SHIFT)
+        for c in range(NC):
+            ze[T, c] = exponent(np.max(np.abs(Z[:, :, c])))
+        for t in range(3):
+            for r in range(TM):
+                for c in range(NC):
+                    dg = digits(int(np.rint(math.ldexp(Z[t, r, c], SHIFT - int(ze[T, c])))))
+                    for l in range(DIG):
+                        Z8[z8_block(T, t, l) + sw128(c, r)] = dg[l]
+    # A[d][q]: the moments' block read MN-major, element (d, q) at sw128(q, d)
+    idxA = np.array([[sw128(q, d) for q in range(TM)] for d in range(128)])
+    idxB = np.array([[sw128(c, q) for q in range(TM)] for c in range(NC)])
+    Kbar = np.zeros((256, NC))
+    for T in range(ntile8):
+        for kb in range(2):
+            acc = np.zeros((4, 128, NC), np.int64)
+            for t in range(3):
+                for i, j in PAIRS:
+                    A = X8[x8_block(T, t, kb, i) + idxA].astype(np.int64)
+                    B = Z8[z8_block(T, t, j) + idxB].astype(np.int64)
+                    acc[i + j] += A @ B.T
+            assert np.max(np.abs(acc)) < 2 ** 31
+            a = (acc[0] * 2.0 ** 48 + acc[1] * 2.0 ** 40) + (acc[2] * 2.0 ** 32 + acc[3] * 2.0 ** 24)
+            Kbar[kb * 128:(kb + 1) * 128] += a * 2.0 ** (ze[T].astype(float) - SHIFT)
+    ref = np.einsum("tqd,qtc->dc", X, Yb.astype(np.float64))
+    scale = np.einsum("tqd,qtc->dc", np.abs(X), np.abs(Yb.astype(np.float64)))
+    assert np.max(np.abs(Kbar[:D, :CG] - ref) / scale) <= 1e-7

@@ -138,7 +138,7 @@ def test_integer_tensor_core_forward(ncand):
     b = _evaluator8(case, ncand, "0")
     oa, ga = a.objective_grad(x, MZ_MIXED)
     ob, gb = b.objective_grad(x, MZ_MIXED)
-    assert a.moment_path(MZ_MIXED, True) == 2 and b.moment_path(MZ_MIXED, True) == 1
+    assert a.moment_path(MZ_MIXED, True) == 3 and b.moment_path(MZ_MIXED, True) == 1
     o64, g64 = b.objective_grad(x, MZ_FP64)
     ea, eb = np.abs(oa - o64) / np.abs(o64), np.abs(ob - o64) / np.abs(o64)
     assert np.all(ea <= OBJ), ea.max()
@@ -153,3 +153,36 @@ def test_integer_tensor_core_forward(ncand):
     # repeatable: integer sums in a fixed order
     oa2, _ = a.objective_grad(x, MZ_MIXED)
     assert np.array_equal(oa, oa2)
+
+
+def test_integer_adjoint_against_cuda_core_adjoint():
+    """The adjoint contraction on the tensor cores (MN-major moment digits,
+    Z digits per tile and candidate) against the CUDA-core one reading the
+    same moment digits: gradients agree to the mixed path's rounding and both
+    meet the bar against FP64."""
+    from meamzilla_b200 import synth
+    from meamzilla_b200.potential import MZ_FP64, MZ_MIXED, Database, PotentialFile
+    spec, cells = synth.make_workload("meam2k", seed=4, ncells=40)
+    pot = PotentialFile.from_spec(spec)
+    db = Database.from_cells(cells, pot)
+    case = dict(db=db, pot=pot, weights=dict(energy_weight=1.0, stress_weight=1.0, embed_extrap=0))
+    x = synth.perturbed(pot.coeffs(), 32, 0.05, seed=23)
+    old = os.environ.get("MZ_FM8ADJ")
+    os.environ["MZ_FM8ADJ"] = "0"
+    try:
+        b = _evaluator8(case, 32, "1")
+    finally:
+        if old is None:
+            del os.environ["MZ_FM8ADJ"]
+        else:
+            os.environ["MZ_FM8ADJ"] = old
+    a = _evaluator8(case, 32, "1")
+    oa, ga = a.objective_grad(x, MZ_MIXED)
+    ob, gb = b.objective_grad(x, MZ_MIXED)
+    assert a.moment_path(MZ_MIXED, True) == 3 and b.moment_path(MZ_MIXED, True) == 2
+    np.testing.assert_array_equal(oa, ob)  # the same forward
+    o64, g64 = b.objective_grad(x, MZ_FP64)
+    for c in range(32):
+        assert _err(ga[c], g64[c]) <= GRAD
+        assert _err(gb[c], g64[c]) <= GRAD
+        assert _err(ga[c], gb[c]) <= GRAD
