@@ -229,6 +229,22 @@ KERNEL_BYTES = {
     "k_fm_fwd": lambda st, nc: 4 * 3 * FM_DPAD_MEAM2K * st["npairs"] + 8 * 3 * st["npairs"] * nc,
     "k_fm_adj": lambda st, nc: 4 * 3 * FM_DPAD_MEAM2K * st["npairs"] + 4 * 3 * st["npairs"] * nc,
 }
+# The epilogues' per-slot, per-candidate streams: k_fm_epi reads Y (FP64 x 3)
+# and writes V (FP64 x 3); k_fm_pre reads Y, the neighbours' lambda (FP32 x 3)
+# and writes dL/dY (FP32 x 3).
+KERNEL_BYTES["k_fm_epi"] = lambda st, nc: (24 + 24) * st["npairs"] * nc
+KERNEL_BYTES["k_fm_pre"] = lambda st, nc: (24 + 12 + 12) * st["npairs"] * nc
+
+
+def int8_mma_ops(stats, ncand):
+    """Integer operations one moment contraction on the tensor cores
+    executes: ten digit-pair MMAs over 3 kinds x 256 features per slot and
+    64 candidates (2 ops per multiply-add), slots padded to 128-slot tiles."""
+    slots = stats["npairs"]
+    groups = (ncand + 63) // 64
+    return 2 * 10 * 3 * 256 * slots * 64 * groups
+
+
 KERNEL_BYTES_TC = {
     "k_fm_fwd": lambda st, nc: FM8_BYTES_PER_SLOT * st["npairs"] + 8 * 3 * st["npairs"] * nc,
     "k_fm_adj": lambda st, nc: FM8_BYTES_PER_SLOT * st["npairs"] + 4 * 3 * st["npairs"] * nc,
@@ -548,9 +564,13 @@ def run_mine(args, world, rank, local):
         return
     tuned = ev.tuning(MZ_MIXED, True)
 
-    # ---- roofline of the dominant kernel: the binding bound is the FP32
-    # CUDA-core pipe (algorithmic flops of the kernel's share of the step);
-    # HBM beside it with the kernel's own bytes
+    # ---- roofline of the dominant kernel, on the bound that binds it: the
+    # FP32 pipe for a CUDA-core contraction (the flops it executes; the row
+    # formulation's algorithmic flops beside); HBM for the integer
+    # tensor-core contractions (their digits and operands are read once;
+    # the int8 MMA rate beside, against the nominal dense int8 peak) and for
+    # the epilogues (their per-slot, per-candidate streams).  HBM is always
+    # reported beside (roofline_hbm).
     hbm, hbm_src = measured_peaks()
     fp32_peak = alu_peak(local, MZ_MIXED)
     fp64_peak = alu_peak(local, MZ_FP64)
@@ -559,24 +579,36 @@ def run_mine(args, world, rank, local):
     dom_ms = kt[dom][0] / kt[dom][1]
     kflops = kernel_algorithmic_flops(dom, stats, args.ncand)
     fm_dpad = FM_DPAD_MEAM2K if tuned.get("triplet_moments") else None
-    xflops = executed_flops(dom, stats, args.ncand, fm_dpad)
-    tc8 = bool(tuned.get("moment_forward_tensor_cores"))
-    kbytes = (KERNEL_BYTES_TC if tc8 else KERNEL_BYTES).get(dom, lambda st, nc: None)(stats, args.ncand)
-    # A moment contraction executes a different count from the row
-    # formulation's triplet flops (the moments are built once per database):
-    # its roofline is on the flops it executes, the row-equivalent rate beside.
-    rflops = xflops if xflops else kflops
-    roof = {"bound": "fp32", "kernel": dom, "achieved": rflops / (dom_ms * 1e-3) / 1e12, "peak": fp32_peak,
-            "unit": "TFLOP/s", "frac": rflops / (dom_ms * 1e-3) / 1e12 / fp32_peak,
-            "flops_per_launch": rflops, "flops_counted": "executed" if xflops else "algorithmic",
-            "algorithmic_flops": kflops,
-            "algorithmic_tflops": kflops / (dom_ms * 1e-3) / 1e12,
-            "traffic": KERNEL_TRAFFIC.get(dom, lambda st, nc: None)(stats, args.ncand),
-            "peak_source": "measured FMA stream on this GPU, FP32 (FP64: %.1f TFLOP/s)" % fp64_peak,
-            "ms_per_launch": dom_ms}
+    tc_fwd = bool(tuned.get("moment_forward_tensor_cores"))
+    tc_adj = bool(tuned.get("moment_adjoint_tensor_cores"))
+    on_tc = (dom == "k_fm_fwd" and tc_fwd) or (dom == "k_fm_adj" and tc_adj)
+    table = dict(KERNEL_BYTES)
+    if tc_fwd:
+        table["k_fm_fwd"] = KERNEL_BYTES_TC["k_fm_fwd"]
+        table["k_fm_adj"] = KERNEL_BYTES_TC["k_fm_adj"]
+    kbytes = table.get(dom, lambda st, nc: None)(stats, args.ncand)
     roof_hbm = {"bound": "hbm", "kernel": dom, "algorithmic_bytes": kbytes,
                 "achieved": kbytes / (dom_ms * 1e-3) / 1e9 if kbytes else None, "peak": hbm, "unit": "GB/s",
-                "frac": kbytes / (dom_ms * 1e-3) / 1e9 / hbm if kbytes else None, "peak_source": hbm_src}
+                "frac": kbytes / (dom_ms * 1e-3) / 1e9 / hbm if kbytes else None, "peak_source": hbm_src,
+                "ms_per_launch": dom_ms}
+    xflops = None if on_tc else executed_flops(dom, stats, args.ncand, fm_dpad)
+    if on_tc or dom in ("k_fm_epi", "k_fm_pre"):
+        roof = dict(roof_hbm, traffic=KERNEL_TRAFFIC.get(dom, lambda st, nc: None)(stats, args.ncand))
+        if on_tc:
+            ops = int8_mma_ops(stats, args.ncand)
+            roof["int8_mma_ops"] = ops
+            roof["int8_tops"] = ops / (dom_ms * 1e-3) / 1e12
+            roof["int8_frac_of_nominal_4500"] = ops / (dom_ms * 1e-3) / 1e12 / 4500.0
+    else:
+        rflops = xflops if xflops else kflops
+        roof = {"bound": "fp32", "kernel": dom, "achieved": rflops / (dom_ms * 1e-3) / 1e12, "peak": fp32_peak,
+                "unit": "TFLOP/s", "frac": rflops / (dom_ms * 1e-3) / 1e12 / fp32_peak,
+                "flops_per_launch": rflops, "flops_counted": "executed" if xflops else "algorithmic",
+                "algorithmic_flops": kflops,
+                "algorithmic_tflops": kflops / (dom_ms * 1e-3) / 1e12,
+                "traffic": KERNEL_TRAFFIC.get(dom, lambda st, nc: None)(stats, args.ncand),
+                "peak_source": "measured FMA stream on this GPU, FP32 (FP64: %.1f TFLOP/s)" % fp64_peak,
+                "ms_per_launch": dom_ms}
     step_flops = 3 * fwd * args.ncand
     roof_step = {"algorithmic_flops": step_flops, "achieved_tflops": step_flops / (ms / args.steps * 1e-3) / 1e12,
                  "frac_fp32": step_flops / (ms / args.steps * 1e-3) / 1e12 / fp32_peak,

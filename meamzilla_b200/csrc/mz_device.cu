@@ -404,9 +404,20 @@ bool fm_prepare(mz_ctx *ctx) {
            extra - bytesX + bytes8 <= (size_t)(0.85 * (double)freeb) &&
            fm8_smem(fp.nt) <= (size_t)ctx->smem_optin &&
            fm_adj_smem(fp.Dpad, 64, true) <= (size_t)ctx->smem_optin;
+  // the kernels' own limits (registers x threads) allow their block sizes
+  {
+    cudaFuncAttributes fa{};
+    if (fm.tc8 && (cudaFuncGetAttributes(&fa, k_fm_gemm_fwd8) != cudaSuccess || fa.maxThreadsPerBlock < FM8_THREADS))
+      fm.tc8 = false;
+  }
+  bool adj8_ok = false;
+  {
+    cudaFuncAttributes fa{};
+    adj8_ok = cudaFuncGetAttributes(&fa, k_fm_gemm_adj8) == cudaSuccess && fa.maxThreadsPerBlock >= FM8_ATHREADS;
+  }
   // the adjoint on the tensor cores as well: Z's digits per candidate group
   const size_t bytesZ = G * ntile8 * 3 * FM8_ZSTAGE + sizeof(int) * G * ntile8 * FM8_NC;
-  fm.tc8a = fm.tc8 && ctx->fm8a_mode != 0 && extra - bytesX + bytes8 + bytesZ <= (size_t)(0.85 * (double)freeb) &&
+  fm.tc8a = fm.tc8 && adj8_ok && ctx->fm8a_mode != 0 && extra - bytesX + bytes8 + bytesZ <= (size_t)(0.85 * (double)freeb) &&
             fm8_adj_smem() <= (size_t)ctx->smem_optin &&
             (size_t)3 * FM8_ZSTAGE + 256 <= (size_t)ctx->smem_optin;
   auto pick = [&](Need &x) -> void * {

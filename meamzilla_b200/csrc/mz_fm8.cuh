@@ -249,6 +249,7 @@ __global__ void __launch_bounds__(FM8_THREADS, 1) k_fm_gemm_fwd8(FmPlan fp, int 
     for (int64_t T = tb; T < te && ok; ++T) {
       const int s = fm_tile_type(fp, (int)(2 * T));
       const int64_t q = T * FM8_TM + r;
+      const char4 eq = *reinterpret_cast<const char4 *>(fp.xe + q * 4);  // the slot's three exponents, early
       for (int t = 0; t < 3; ++t, ++seq) {
         const int buf = (int)(seq & 1);
         if (!tc::mbar_wait(accf + buf, (uint32_t)((seq >> 1) & 1), FM8_WAIT)) {
@@ -257,7 +258,8 @@ __global__ void __launch_bounds__(FM8_THREADS, 1) k_fm_gemm_fwd8(FmPlan fp, int 
           break;
         }
         tc::fence_after_sync();
-        const double sq = ldexp(1.0, (int)fp.xe[q * 4 + t] - FM8_SHIFT);
+        const int e = t == 0 ? eq.x : (t == 1 ? eq.y : eq.z);
+        const double sq = __longlong_as_double((long long)(e - FM8_SHIFT + 1023) << 52);  // 2^(e - 30)
         double *yo = fp.Y + (((size_t)gy * fp.Q + q) * 3 + t) * CG;
         const uint32_t ta = tm + ((uint32_t)(32 * quarter) << 16) + (uint32_t)(buf * 256);
         for (int cb = 0; cb < FM8_NC / 16 && cb * 16 < CG; ++cb) {
@@ -374,7 +376,7 @@ __host__ __device__ constexpr size_t fm8_adj_smem() {
   return 1024 + 2 * (size_t)FM8_STAGE + 2 * (size_t)FM8_ZSTAGE + sizeof(uint64_t) * 12 + 16;
 }
 
-__global__ void __maxnreg__(112) k_fm_gemm_adj8(FmPlan fp, const signed char *__restrict__ Z8,
+__global__ void __maxnreg__(96) k_fm_gemm_adj8(FmPlan fp, const signed char *__restrict__ Z8,
                                                                  const int *__restrict__ ze, int *__restrict__ err) {
   extern __shared__ __align__(16) unsigned char sm8raw[];
   const uint32_t raw = tc::smem_u32(sm8raw);
