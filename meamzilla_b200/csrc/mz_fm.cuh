@@ -958,7 +958,7 @@ __global__ void __launch_bounds__(256, 2) k_fm_adj_pre(DevDb db, DevPot pot, con
       };
       // ---- pass 1: K_i
       double K = 0.0;
-#pragma unroll 2
+#pragma unroll 4
       for (int p = 0; p < n; ++p) {
         const int ql = lo + p;
         const FmPairVals<float> v = fm_pair_vals<float>(st, fp, ql, cl);
@@ -982,7 +982,7 @@ __global__ void __launch_bounds__(256, 2) k_fm_adj_pre(DevDb db, DevPot pot, con
                         [&](int ix, double x) { atomicAdd(utab + (size_t)cl * fp.ustride + (gU.toff - fp.utoff) + ix, x); });
       // ---- pass 2: dL/dY and the pair-function gradients
       const float epsf = (float)eps;
-#pragma unroll 2
+#pragma unroll 4
       for (int p = 0; p < n; ++p) {
         const int ql = lo + p;
         const FmPairVals<float> v = fm_pair_vals<float>(st, fp, ql, cl);

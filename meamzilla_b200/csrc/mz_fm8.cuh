@@ -328,48 +328,68 @@ __host__ __device__ inline size_t z8_block(int gy, int64_t T, int64_t ntile8, in
   return ((((size_t)gy * ntile8 + T) * 3 + t) * FM8_DIG + l) * FM8_ZBLK;
 }
 
-// Z's digits of one tile (blockIdx.x) of group blockIdx.y: the candidates'
-// exponents over the tile, the digits into a shared image of the tile's
-// 96 KB of blocks, written out in 16-byte pieces.
+// Z's digits of one tile (blockIdx.x) of group blockIdx.y.  Thread = one
+// candidate (c = thread % 64) and a quarter of the tile's 96 (kind, 4-slot
+// group) items.  Pass 1: the exponent bound of every Z = 2^(e_q - 30) Ybar
+// from the FP32 exponent field (|v| < 2^(field - 126)), the candidate's
+// maximum through a shared atomicMax.  Pass 2: the digits of four slots at a
+// time, packed into one word per digit of the swizzled K-major image.  The
+// tile's 96 KB image is then written out in 16-byte pieces.
 __global__ void __launch_bounds__(256) k_fm_zdig(FmPlan fp, signed char *__restrict__ Z8, int *__restrict__ ze) {
   extern __shared__ __align__(16) unsigned char zsm[];  // [3][4][8 KB]
   __shared__ int se[FM8_NC];
   const int64_t T = blockIdx.x, ntile8 = fp.Q / FM8_TM;
   const int gy = blockIdx.y, CG = fp.CG, tid = threadIdx.x;
+  const int c = tid & (FM8_NC - 1), g = tid >> 6;  // 4 item groups (blockDim.x == 256)
   const int s = fm_tile_type(fp, (int)(2 * T));
-  const int64_t qend = fp.qend[s];
+  const int64_t q0t = T * FM8_TM, qend = fp.qend[s];
   if (tid < FM8_NC) se[tid] = -1000;
   for (int i = tid; i < 3 * FM8_ZSTAGE / 16; i += blockDim.x) reinterpret_cast<int4 *>(zsm)[i] = make_int4(0, 0, 0, 0);
   __syncthreads();
-  auto zval = [&](int idx, int &t, int &c, int &r) -> double {
-    r = idx / (3 * CG);
-    const int rem = idx % (3 * CG);
-    t = rem / CG;
-    c = rem % CG;
-    const int64_t q = T * FM8_TM + r;
-    if (q >= qend) return 0.0;
-    return ldexp((double)fp.Yb[(((size_t)gy * fp.Q + q) * 3 + t) * CG + c], (int)fp.xe[q * 4 + t] - FM8_SHIFT);
-  };
-  for (int idx = tid; idx < FM8_TM * 3 * CG; idx += blockDim.x) {
-    int t, c, r;
-    const double z = zval(idx, t, c, r);
-    if (z != 0.0) atomicMax(se + c, fm8_exponent(fabs(z)));
-  }
-  __syncthreads();
-  for (int idx = tid; idx < FM8_TM * 3 * CG; idx += blockDim.x) {
-    int t, c, r;
-    const double z = zval(idx, t, c, r);
-    const int e = se[c] == -1000 ? 0 : se[c];
-    signed char dg[FM8_DIG];
-    digits256(llrint(ldexp(z, FM8_SHIFT - e)), dg);
-    const uint32_t o = sw128_byte(c, r);
+  const bool live = c < CG;
+  const float *Yg = fp.Yb + ((size_t)gy * fp.Q + q0t) * 3 * CG + c;
+  // items it = g + 4 k: kind t = it % 3, slots 4 (it / 3) .. + 3
+  int emax = -1000;
+  if (live)
+    for (int it = g; it < 3 * (FM8_TM / 4); it += 4) {
+      const int t = it % 3, r0 = 4 * (it / 3);
 #pragma unroll
-    for (int l = 0; l < FM8_DIG; ++l) zsm[(size_t)(t * FM8_DIG + l) * FM8_ZBLK + o] = dg[l];
-  }
+      for (int k = 0; k < 4; ++k) {
+        const int r = r0 + k;
+        if (q0t + r >= qend) continue;
+        const float v = Yg[(size_t)(r * 3 + t) * CG];
+        if (v != 0.f) {
+          const int ef = (int)((__float_as_uint(v) >> 23) & 255) - 126;
+          emax = max(emax, ef + (int)fp.xe[(q0t + r) * 4 + t] - FM8_SHIFT);
+        }
+      }
+    }
+  if (live && emax > -1000) atomicMax(se + c, emax);
+  __syncthreads();
+  const int e = (live && se[c] > -1000) ? max(-100, se[c]) : 0;  // a bound: |Z| < 2^e
+  if (live)
+    for (int it = g; it < 3 * (FM8_TM / 4); it += 4) {
+      const int t = it % 3, r0 = 4 * (it / 3);
+      uint32_t w[FM8_DIG] = {0u, 0u, 0u, 0u};
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        const int r = r0 + k;
+        if (q0t + r >= qend) continue;
+        const double z = ldexp((double)Yg[(size_t)(r * 3 + t) * CG], (int)fp.xe[(q0t + r) * 4 + t] - e);
+        signed char dg[FM8_DIG];
+        digits256(llrint(z), dg);
+#pragma unroll
+        for (int l = 0; l < FM8_DIG; ++l) w[l] |= (uint32_t)(unsigned char)dg[l] << (8 * k);
+      }
+      const uint32_t o = sw128_byte(c, r0);  // 4 slots: 4 bytes of one 16-byte chunk
+#pragma unroll
+      for (int l = 0; l < FM8_DIG; ++l)
+        *reinterpret_cast<uint32_t *>(zsm + (size_t)(t * FM8_DIG + l) * FM8_ZBLK + o) = w[l];
+    }
   __syncthreads();
   int4 *dst = reinterpret_cast<int4 *>(Z8 + z8_block(gy, T, ntile8, 0, 0));
   for (int i = tid; i < 3 * FM8_ZSTAGE / 16; i += blockDim.x) dst[i] = reinterpret_cast<const int4 *>(zsm)[i];
-  if (tid < FM8_NC) ze[((size_t)gy * ntile8 + T) * FM8_NC + tid] = se[tid] == -1000 ? 0 : se[tid];
+  if (tid < FM8_NC) ze[((size_t)gy * ntile8 + T) * FM8_NC + tid] = (tid < CG && se[tid] > -1000) ? max(-100, se[tid]) : 0;
 }
 
 __host__ __device__ constexpr size_t fm8_adj_smem() {
