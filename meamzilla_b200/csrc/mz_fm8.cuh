@@ -375,11 +375,18 @@ __global__ void __launch_bounds__(256) k_fm_zdig(FmPlan fp, signed char *__restr
       for (int k = 0; k < 4; ++k) {
         const int r = r0 + k;
         if (q0t + r >= qend) continue;
-        const double z = ldexp((double)Yg[(size_t)(r * 3 + t) * CG], (int)fp.xe[(q0t + r) * 4 + t] - e);
-        signed char dg[FM8_DIG];
-        digits256(llrint(z), dg);
+        // Z_int = Ybar 2^(e_q - e) (|Z_int| < 2^30): a power-of-two scaling, one rounding to int32
+        const int sh = (int)fp.xe[(q0t + r) * 4 + t] - e;
+        int zi = __double2int_rn((double)Yg[(size_t)(r * 3 + t) * CG] *
+                                 __longlong_as_double((long long)(sh + 1023) << 52));
+        // balanced base-256 digits, least significant first, in 32-bit arithmetic
 #pragma unroll
-        for (int l = 0; l < FM8_DIG; ++l) w[l] |= (uint32_t)(unsigned char)dg[l] << (8 * k);
+        for (int l = FM8_DIG - 1; l > 0; --l) {
+          const int lo = ((zi + 128) & 255) - 128;
+          w[l] |= (uint32_t)(lo & 255) << (8 * k);
+          zi = (zi - lo) >> 8;
+        }
+        w[0] |= (uint32_t)(zi & 255) << (8 * k);
       }
       const uint32_t o = sw128_byte(c, r0);  // 4 slots: 4 bytes of one 16-byte chunk
 #pragma unroll
@@ -406,6 +413,7 @@ __global__ void __maxnreg__(96) k_fm_gemm_adj8(FmPlan fp, const signed char *__r
   uint64_t *aempty = afull + 2, *bfull = aempty + 2, *bempty = bfull + 2;
   uint64_t *accf = bempty + 2, *acce = accf + 1, *mdone = acce + 1;
   uint32_t *tslot = reinterpret_cast<uint32_t *>(mdone + 1);
+  __shared__ __align__(16) int zes[2 * FM8_NC];  // candidate exponents of a tile, double-buffered
 
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int gy = blockIdx.y, CG = fp.CG, nt = fp.nt;
@@ -551,7 +559,15 @@ __global__ void __maxnreg__(96) k_fm_gemm_adj8(FmPlan fp, const signed char *__r
       const int s = fm_tile_type(fp, (int)(2 * T));
       if (s != cur && cur >= 0) flush(cur);
       cur = s;
-      const int *zt = ze + ((size_t)gy * ntile8 + T) * FM8_NC;
+      // the tile's candidate exponents into shared memory while its MMAs run
+      // (double-buffered: every epilogue warp has left tile - 1 at the barrier)
+      int *zs = zes + (tile & 1) * FM8_NC;
+      if (warp == 2) {
+        const int *zt = ze + ((size_t)gy * ntile8 + T) * FM8_NC;
+        zs[lane] = zt[lane];
+        zs[lane + 32] = zt[lane + 32];
+      }
+      asm volatile("bar.sync 1, 512;" ::: "memory");  // the sixteen epilogue warps
       if (!tc::mbar_wait(accf, (uint32_t)(tile & 1), FM8_WAIT)) {
         atomicExch(err, 7);
         ok = false;
@@ -564,7 +580,7 @@ __global__ void __maxnreg__(96) k_fm_gemm_adj8(FmPlan fp, const signed char *__r
         int v[FM8_CLS][4];
 #pragma unroll
         for (int m = 0; m < FM8_CLS; ++m) tc::tmem_ld4i(ta + m * FM8_NC + cb * 4, v[m]);
-        const int4 ez = *reinterpret_cast<const int4 *>(zt + c0 + cb * 4);
+        const int4 ez = *reinterpret_cast<const int4 *>(zs + c0 + cb * 4);
         tc::tmem_wait_ld();
         const int e4[4] = {ez.x, ez.y, ez.z, ez.w};
 #pragma unroll
