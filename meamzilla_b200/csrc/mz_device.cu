@@ -416,7 +416,7 @@ bool fm_prepare(mz_ctx *ctx) {
     adj8_ok = cudaFuncGetAttributes(&fa, k_fm_gemm_adj8) == cudaSuccess && fa.maxThreadsPerBlock >= FM8_ATHREADS;
   }
   // the adjoint on the tensor cores as well: Z's digits per candidate group
-  const size_t bytesZ = G * ntile8 * 3 * FM8_ZSTAGE + sizeof(int) * G * ntile8 * FM8_NC;
+  const size_t bytesZ = G * ntile8 * 3 * FM8_ZSTAGE + 2 * sizeof(int) * G * ntile8 * FM8_NC;
   fm.tc8a = fm.tc8 && adj8_ok && ctx->fm8a_mode != 0 && extra - bytesX + bytes8 + bytesZ <= (size_t)(0.85 * (double)freeb) &&
             fm8_adj_smem() <= (size_t)ctx->smem_optin &&
             (size_t)3 * FM8_ZSTAGE + 256 <= (size_t)ctx->smem_optin;
@@ -459,6 +459,7 @@ bool fm_prepare(mz_ctx *ctx) {
     if (fm.tc8a) {
       fm.Z8 = dalloc<signed char>(ctx, G * ntile8 * 3 * FM8_ZSTAGE);
       fm.ze = dalloc<int>(ctx, G * ntile8 * FM8_NC);
+      fp.zmax = dalloc<int>(ctx, G * ntile8 * FM8_NC);
       smem_attr(k_fm_gemm_adj8, fm8_adj_smem());
       smem_attr(k_fm_zdig, (size_t)3 * FM8_ZSTAGE);
     }
@@ -550,6 +551,8 @@ void enqueue_fm(mz_ctx *ctx, int n, double *d_obj, double *d_errvec, double *d_f
     ck(cudaGetLastError(), "k_final launch");
   }
   if (!grad) return;
+  if (fp.zmax)  // the pre pass's per-tile exponent bounds start below every bound
+    ck(cudaMemsetAsync(fp.zmax, 0x80, sizeof(int) * (size_t)G * (fp.Q / FM8_TM) * FM8_NC, st), "memset");
   {
     Bracket b(ctx, MZ_K_FM_PRE);
     k_fm_adj_pre<<<dim3(fp.nctas_pre, G), 256, fm_pre_smem(ns, CG, fp.nt, fp.NB, fp.ustride), st>>>(

@@ -85,6 +85,7 @@ struct FmPlan {
   const signed char *xe;   // [Q][4]
   signed char *K8;         // [ngroups][nt][2][3][8 KB]
   int *ke;                 // [ngroups][nt][64]
+  int *zmax;               // [ngroups][Q / 128][64] exponent bounds of the adjoint operand per tile (or null)
 };
 
 // ------------------------------------------- digits of the integer contraction
@@ -484,7 +485,7 @@ struct FmStage {
   int *gs, *nbr, *tj, *kn;  // [BLOCK_SLOTS]
   int *ctype;         // type whose coefficients are staged (-1: none yet)
   float4 *uf;         // [BLOCK_SLOTS] (ux, uy, uz, 1/r)
-  double *e;          // [BLOCK_SLOTS][6] e1, e2
+  double *e;          // [BLOCK_SLOTS][6] e1, e2 (FP32 stages keep them as floats in the same space)
   double4 *ur;        // [BLOCK_SLOTS] (ux, uy, uz, r) in FP64
   R *bas;             // [BLOCK_SLOTS][3][8] basis N0..N3 and d/dr N0'..N3' of phi, rho, f
   R *coef;            // [3][nt][NB][CG]
@@ -567,7 +568,10 @@ __device__ int fm_stage_block(const DevDb &db, const DevPot &pot, const SplineGe
     st.ur[ql] = make_double4(db.pair_ux[gs], db.pair_uy[gs], db.pair_uz[gs], db.pair_r[gs]);
     const double *e = fp.E + (size_t)(fp.row0[i] + p) * 8;
 #pragma unroll
-    for (int k = 0; k < 6; ++k) st.e[ql * 6 + k] = e[k];
+    for (int k = 0; k < 6; ++k) {
+      if (sizeof(R) == 4) reinterpret_cast<float *>(st.e)[ql * 6 + k] = (float)e[k];
+      else st.e[ql * 6 + k] = e[k];
+    }
 #pragma unroll
     for (int F = 0; F < 3; ++F) {
       const int k = ((kn >> (8 * F)) & 0xff) - 1;
@@ -964,12 +968,13 @@ __global__ void __launch_bounds__(256, 2) k_fm_adj_pre(DevDb db, DevPot pot, con
         const FmPairVals<float> v = fm_pair_vals<float>(st, fp, ql, cl);
         const double *yp = Yq + (size_t)p * 3 * CG;
         const float4 u = st.uf[ql];
-        const double *e = st.e + ql * 6;
+        const float *e = reinterpret_cast<const float *>(st.e) + ql * 6;
         float lx, ly, lz;
         lam(ql, u, lx, ly, lz);
-        const double ap = lx * u.x + ly * u.y + lz * u.z;
-        const double l1 = lx * e[0] + ly * e[1] + lz * e[2], l2 = lx * e[3] + ly * e[4] + lz * e[5];
-        K += ap * ((double)v.drho + (double)v.df * yp[0]) + (double)v.f * (double)u.w * (l1 * yp[CG] + l2 * yp[2 * CG]);
+        const float ap = lx * u.x + ly * u.y + lz * u.z;
+        const float l1 = lx * e[0] + ly * e[1] + lz * e[2], l2 = lx * e[3] + ly * e[4] + lz * e[5];
+        // the slot's term in FP32, the atom's sum in FP64
+        K += (double)(ap * (v.drho + v.df * (float)yp[0]) + v.f * u.w * (l1 * (float)yp[CG] + l2 * (float)yp[2 * CG]));
         // kept for pass 2 in this slot's dL/dY words, which pass 2 then overwrites
         float *yb = Ybq + (size_t)p * 3 * CG;
         yb[0] = (float)ap;
@@ -982,6 +987,8 @@ __global__ void __launch_bounds__(256, 2) k_fm_adj_pre(DevDb db, DevPot pot, con
                         [&](int ix, double x) { atomicAdd(utab + (size_t)cl * fp.ustride + (gU.toff - fp.utoff) + ix, x); });
       // ---- pass 2: dL/dY and the pair-function gradients
       const float epsf = (float)eps;
+      int64_t ztile = -1;
+      int zexp = -1000;
 #pragma unroll 4
       for (int p = 0; p < n; ++p) {
         const int ql = lo + p;
@@ -992,9 +999,27 @@ __global__ void __launch_bounds__(256, 2) k_fm_adj_pre(DevDb db, DevPot pot, con
         float *yb = Ybq + (size_t)p * 3 * CG;
         const float ap = yb[0], l1 = yb[CG], l2 = yb[2 * CG];  // from pass 1
         const float B = dF * v.f * u.w;
-        yb[0] = 0.5f * v.f * ch + ap * dF * v.df;
-        yb[CG] = B * l1;
-        yb[2 * CG] = B * l2;
+        const float y0 = 0.5f * v.f * ch + ap * dF * v.df, y1 = B * l1, y2 = B * l2;
+        yb[0] = y0;
+        yb[CG] = y1;
+        yb[2 * CG] = y2;
+        if (fp.zmax) {
+          // the integer adjoint's operand Z = 2^(e_q - 30) dL/dY: its exponent
+          // bound per (128-slot tile, candidate), |v| < 2^(field - 126)
+          const int64_t q = q0 + p, Tq = q >> 7;
+          if (Tq != ztile) {
+            if (ztile >= 0 && zexp > -1000) atomicMax(fp.zmax + ((size_t)gy * (fp.Q >> 7) + ztile) * 64 + cl, zexp);
+            ztile = Tq;
+            zexp = -1000;
+          }
+          const char4 eq = *reinterpret_cast<const char4 *>(fp.xe + q * 4);
+          const float yy[3] = {y0, y1, y2};
+          const int ee[3] = {eq.x, eq.y, eq.z};
+#pragma unroll
+          for (int t = 0; t < 3; ++t)
+            if (yy[t] != 0.f)
+              zexp = max(zexp, (int)((__float_as_uint(yy[t]) >> 23) & 255) - 126 + ee[t] - FM8_SHIFT);
+        }
         const float wv[3] = {0.5f * epsf, ch, 0.5f * ch * G + dF * (l1 * Y1 + l2 * Y2) * u.w};
         const float wd[3] = {0.5f * ap, dF * ap, dF * ap * G};
         const int kn = st.kn[ql], tj = st.tj[ql];
@@ -1010,6 +1035,8 @@ __global__ void __launch_bounds__(256, 2) k_fm_adj_pre(DevDb db, DevPot pot, con
           atomicAdd(pe + 3 * CG, wv[F] * bs[3] + wd[F] * bs[7]);
         }
       }
+      if (fp.zmax && ztile >= 0 && zexp > -1000)
+        atomicMax(fp.zmax + ((size_t)gy * (fp.Q >> 7) + ztile) * 64 + cl, zexp);
     }
   }
   if (pacc_t >= 0) flush_pairs(pacc_t);

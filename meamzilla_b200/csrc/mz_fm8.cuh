@@ -328,46 +328,32 @@ __host__ __device__ inline size_t z8_block(int gy, int64_t T, int64_t ntile8, in
   return ((((size_t)gy * ntile8 + T) * 3 + t) * FM8_DIG + l) * FM8_ZBLK;
 }
 
-// Z's digits of one tile (blockIdx.x) of group blockIdx.y.  Thread = one
-// candidate (c = thread % 64) and a quarter of the tile's 96 (kind, 4-slot
-// group) items.  Pass 1: the exponent bound of every Z = 2^(e_q - 30) Ybar
-// from the FP32 exponent field (|v| < 2^(field - 126)), the candidate's
-// maximum through a shared atomicMax.  Pass 2: the digits of four slots at a
-// time, packed into one word per digit of the swizzled K-major image.  The
-// tile's 96 KB image is then written out in 16-byte pieces.
+// Z's digits of one tile (blockIdx.x) of group blockIdx.y, one pass: the
+// exponent bound of every candidate over the tile comes from the pre pass
+// (fp.zmax, maximum of the FP32 exponent fields plus e_q - 30).  Thread =
+// one candidate (c = thread % 64) and a quarter of the tile's 96 (kind,
+// 4-slot group) items; the digits of four slots are packed into one word per
+// digit of the swizzled K-major image, which is then written out in 16-byte
+// pieces.
 __global__ void __launch_bounds__(256) k_fm_zdig(FmPlan fp, signed char *__restrict__ Z8, int *__restrict__ ze) {
   extern __shared__ __align__(16) unsigned char zsm[];  // [3][4][8 KB]
-  __shared__ int se[FM8_NC];
+  __shared__ char4 sxe[FM8_TM];
   const int64_t T = blockIdx.x, ntile8 = fp.Q / FM8_TM;
   const int gy = blockIdx.y, CG = fp.CG, tid = threadIdx.x;
   const int c = tid & (FM8_NC - 1), g = tid >> 6;  // 4 item groups (blockDim.x == 256)
   const int s = fm_tile_type(fp, (int)(2 * T));
   const int64_t q0t = T * FM8_TM, qend = fp.qend[s];
-  if (tid < FM8_NC) se[tid] = -1000;
-  for (int i = tid; i < 3 * FM8_ZSTAGE / 16; i += blockDim.x) reinterpret_cast<int4 *>(zsm)[i] = make_int4(0, 0, 0, 0);
+  if (CG < FM8_NC)  // rows of absent candidates stay zero
+    for (int i = tid; i < 3 * FM8_ZSTAGE / 16; i += blockDim.x)
+      reinterpret_cast<int4 *>(zsm)[i] = make_int4(0, 0, 0, 0);
+  if (tid < FM8_TM) sxe[tid] = *reinterpret_cast<const char4 *>(fp.xe + (q0t + tid) * 4);
   __syncthreads();
   const bool live = c < CG;
+  const int zm = live ? fp.zmax[((size_t)gy * ntile8 + T) * FM8_NC + c] : -2000;
+  const int e = zm > -1000 ? max(-100, zm) : 0;  // a bound: |Z| < 2^e
   const float *Yg = fp.Yb + ((size_t)gy * fp.Q + q0t) * 3 * CG + c;
-  // items it = g + 4 k: kind t = it % 3, slots 4 (it / 3) .. + 3
-  int emax = -1000;
-  if (live)
-    for (int it = g; it < 3 * (FM8_TM / 4); it += 4) {
-      const int t = it % 3, r0 = 4 * (it / 3);
-#pragma unroll
-      for (int k = 0; k < 4; ++k) {
-        const int r = r0 + k;
-        if (q0t + r >= qend) continue;
-        const float v = Yg[(size_t)(r * 3 + t) * CG];
-        if (v != 0.f) {
-          const int ef = (int)((__float_as_uint(v) >> 23) & 255) - 126;
-          emax = max(emax, ef + (int)fp.xe[(q0t + r) * 4 + t] - FM8_SHIFT);
-        }
-      }
-    }
-  if (live && emax > -1000) atomicMax(se + c, emax);
-  __syncthreads();
-  const int e = (live && se[c] > -1000) ? max(-100, se[c]) : 0;  // a bound: |Z| < 2^e
-  if (live)
+  if (live) {
+#pragma unroll 2
     for (int it = g; it < 3 * (FM8_TM / 4); it += 4) {
       const int t = it % 3, r0 = 4 * (it / 3);
       uint32_t w[FM8_DIG] = {0u, 0u, 0u, 0u};
@@ -375,8 +361,9 @@ __global__ void __launch_bounds__(256) k_fm_zdig(FmPlan fp, signed char *__restr
       for (int k = 0; k < 4; ++k) {
         const int r = r0 + k;
         if (q0t + r >= qend) continue;
-        // Z_int = Ybar 2^(e_q - e) (|Z_int| < 2^30): a power-of-two scaling, one rounding to int32
-        const int sh = (int)fp.xe[(q0t + r) * 4 + t] - e;
+        const char4 x4 = sxe[r];
+        const int sh = (t == 0 ? x4.x : (t == 1 ? x4.y : x4.z)) - e;
+        // Z_int = Ybar 2^(e_q - e): a power-of-two scaling, one rounding to int32
         int zi = __double2int_rn((double)Yg[(size_t)(r * 3 + t) * CG] *
                                  __longlong_as_double((long long)(sh + 1023) << 52));
         // balanced base-256 digits, least significant first, in 32-bit arithmetic
@@ -393,10 +380,11 @@ __global__ void __launch_bounds__(256) k_fm_zdig(FmPlan fp, signed char *__restr
       for (int l = 0; l < FM8_DIG; ++l)
         *reinterpret_cast<uint32_t *>(zsm + (size_t)(t * FM8_DIG + l) * FM8_ZBLK + o) = w[l];
     }
+  }
   __syncthreads();
   int4 *dst = reinterpret_cast<int4 *>(Z8 + z8_block(gy, T, ntile8, 0, 0));
   for (int i = tid; i < 3 * FM8_ZSTAGE / 16; i += blockDim.x) dst[i] = reinterpret_cast<const int4 *>(zsm)[i];
-  if (tid < FM8_NC) ze[((size_t)gy * ntile8 + T) * FM8_NC + tid] = (tid < CG && se[tid] > -1000) ? max(-100, se[tid]) : 0;
+  if (tid < FM8_NC) ze[((size_t)gy * ntile8 + T) * FM8_NC + tid] = e;
 }
 
 __host__ __device__ constexpr size_t fm8_adj_smem() {
