@@ -128,8 +128,6 @@ struct mz_ctx {
     bool eligible = false, ready = false, failed = false;
     bool tc8 = false;   // the forward contraction on the tensor cores (mz_fm8.cuh)
     bool tc8a = false;  // and the adjoint contraction
-    signed char *Z8 = nullptr;
-    int *ze = nullptr;
     FmPlan plan{};
     int CGmax = 8, ngroups_max = 1;
     size_t smem_pre = 0;
@@ -415,11 +413,10 @@ bool fm_prepare(mz_ctx *ctx) {
     cudaFuncAttributes fa{};
     adj8_ok = cudaFuncGetAttributes(&fa, k_fm_gemm_adj8) == cudaSuccess && fa.maxThreadsPerBlock >= FM8_ATHREADS;
   }
-  // the adjoint on the tensor cores as well: Z's digits per candidate group
-  const size_t bytesZ = G * ntile8 * 3 * FM8_ZSTAGE + 2 * sizeof(int) * G * ntile8 * FM8_NC;
+  // the adjoint on the tensor cores as well: its operand's exponent bounds per (span, candidate)
+  const size_t bytesZ = sizeof(int) * G * (size_t)fm8_nspan((int64_t)Q) * FM8_NC;
   fm.tc8a = fm.tc8 && adj8_ok && ctx->fm8a_mode != 0 && extra - bytesX + bytes8 + bytesZ <= (size_t)(0.85 * (double)freeb) &&
-            fm8_adj_smem() <= (size_t)ctx->smem_optin &&
-            (size_t)3 * FM8_ZSTAGE + 256 <= (size_t)ctx->smem_optin;
+            fm8_adj_smem() <= (size_t)ctx->smem_optin;
   auto pick = [&](Need &x) -> void * {
     return x.need_bytes <= x.have_bytes ? x.have : (void *)dalloc<unsigned char>(ctx, x.need_bytes);
   };
@@ -457,11 +454,8 @@ bool fm_prepare(mz_ctx *ctx) {
     fp.xe = xe;
     smem_attr(k_fm_gemm_fwd8, fm8_smem(fp.nt));
     if (fm.tc8a) {
-      fm.Z8 = dalloc<signed char>(ctx, G * ntile8 * 3 * FM8_ZSTAGE);
-      fm.ze = dalloc<int>(ctx, G * ntile8 * FM8_NC);
-      fp.zmax = dalloc<int>(ctx, G * ntile8 * FM8_NC);
+      fp.zmax = dalloc<int>(ctx, G * (size_t)fm8_nspan((int64_t)Q) * FM8_NC);
       smem_attr(k_fm_gemm_adj8, fm8_adj_smem());
-      smem_attr(k_fm_zdig, (size_t)3 * FM8_ZSTAGE);
     }
   }
   fp.CG = fm.CGmax;
@@ -551,8 +545,8 @@ void enqueue_fm(mz_ctx *ctx, int n, double *d_obj, double *d_errvec, double *d_f
     ck(cudaGetLastError(), "k_final launch");
   }
   if (!grad) return;
-  if (fp.zmax)  // the pre pass's per-tile exponent bounds start below every bound
-    ck(cudaMemsetAsync(fp.zmax, 0x80, sizeof(int) * (size_t)G * (fp.Q / FM8_TM) * FM8_NC, st), "memset");
+  if (fp.zmax)  // the pre pass's per-span exponent bounds start below every bound
+    ck(cudaMemsetAsync(fp.zmax, 0x80, sizeof(int) * (size_t)G * fm8_nspan(fp.Q) * FM8_NC, st), "memset");
   {
     Bracket b(ctx, MZ_K_FM_PRE);
     k_fm_adj_pre<<<dim3(fp.nctas_pre, G), 256, fm_pre_smem(ns, CG, fp.nt, fp.NB, fp.ustride), st>>>(
@@ -563,11 +557,7 @@ void enqueue_fm(mz_ctx *ctx, int n, double *d_obj, double *d_errvec, double *d_f
     Bracket b(ctx, MZ_K_FM_ADJ);
     const int threads = ((fp.Dpad / FM_ROWS) * (CG / 8) + 31) / 32 * 32;
     if (ctx->fm.tc8a) {
-      const int ntile8 = (int)(fp.Q / FM8_TM);
-      k_fm_zdig<<<dim3(ntile8, G), 256, (size_t)3 * FM8_ZSTAGE, st>>>(fp, ctx->fm.Z8, ctx->fm.ze);
-      ck(cudaGetLastError(), "k_fm_zdig launch");
-      k_fm_gemm_adj8<<<dim3(fp.nctas_adj, G), FM8_ATHREADS, fm8_adj_smem(), st>>>(fp, ctx->fm.Z8, ctx->fm.ze,
-                                                                                   ctx->d_err);
+      k_fm_gemm_adj8<<<dim3(fp.nctas_adj, G), FM8_ATHREADS, fm8_adj_smem(), st>>>(fp, n, ctx->d_err);
     } else if (ctx->fm.tc8)
       k_fm_gemm_adj<true><<<dim3(fp.nctas_adj, G), std::min(threads, 256), fm_adj_smem(fp.Dpad, CG, true), st>>>(fp);
     else

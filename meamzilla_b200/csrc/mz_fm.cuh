@@ -49,6 +49,7 @@ constexpr int FM_MAXB = 24;    // B-spline coefficients of any spline the path r
 constexpr int FM_SUB = 16;     // feature slots per sub-tile of the adjoint contraction
 constexpr int FM_ROWS = 8;     // features per thread in the adjoint contraction
 constexpr int FM_PCHUNK = 32;  // slots per chunk of the pair-function gradient
+constexpr int FM_PB = 4;       // slots per batch of loads in the epilogues' row walks
 
 struct FmPlan {
   int nt;          // atom types
@@ -103,6 +104,8 @@ constexpr int FM8_SHIFT = 30;                    // |X_int|, |K_int| <= 2^30
 constexpr int FM8_NST = 2;                       // stages in the ring
 constexpr int FM8_THREADS = 192;
 constexpr uint32_t FM8_WAIT = 1u << 26;          // polls before a wait gives up
+constexpr int FM8_SPAN_LOG = 3;
+constexpr int FM8_SPAN = 1 << FM8_SPAN_LOG;      // tiles per exponent span of the integer adjoint's operand
 
 // byte of (row r, byte k) in a SW128 K-major block
 __host__ __device__ inline uint32_t sw128_byte(int r, int k) {
@@ -616,19 +619,63 @@ template <typename R>
 struct FmPairVals {
   R phi, dphi, rho, drho, f, df;
 };
+// the staged basis of slot ql for pair function F: N0..N3, then their d/dr
+// (16-byte shared loads, the same address in every lane)
+__device__ __forceinline__ void fm_bas(const FmStage<float> &st, int ql, int F, float *b) {
+  const float4 *p = reinterpret_cast<const float4 *>(st.bas + (ql * 3 + F) * 8);
+  const float4 x = p[0], y = p[1];
+  b[0] = x.x; b[1] = x.y; b[2] = x.z; b[3] = x.w;
+  b[4] = y.x; b[5] = y.y; b[6] = y.z; b[7] = y.w;
+}
+__device__ __forceinline__ void fm_bas(const FmStage<double> &st, int ql, int F, double *b) {
+  const double2 *p = reinterpret_cast<const double2 *>(st.bas + (ql * 3 + F) * 8);
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const double2 x = p[i];
+    b[2 * i] = x.x;
+    b[2 * i + 1] = x.y;
+  }
+}
+
+// value and d/dr of pair function F at staged slot ql for candidate cl
+template <typename R>
+__device__ __forceinline__ void fm_pair_val(const FmStage<R> &st, const FmPlan &fp, int ql, int cl, int F, int kn,
+                                            int tj, R &v, R &d) {
+  const int k = ((kn >> (8 * F)) & 0xff) - 1;
+  R bs[8];
+  fm_bas(st, ql, F, bs);
+  const int CG = fp.CG;
+  const R *cf = st.coef + ((size_t)(F * fp.nt + tj) * fp.NB + (k < 0 ? 0 : k)) * CG + cl;
+  const R c0 = cf[0], c1 = cf[CG], c2 = cf[2 * CG], c3 = cf[3 * CG];
+  v = bs[0] * c0 + bs[1] * c1 + bs[2] * c2 + bs[3] * c3;  // zero basis where k < 0
+  d = bs[4] * c0 + bs[5] * c1 + bs[6] * c2 + bs[7] * c3;
+}
+
+// only the value (d = 0) or only d/dr (d = 1) of pair function F
+template <typename R>
+__device__ __forceinline__ R fm_pair_one(const FmStage<R> &st, const FmPlan &fp, int ql, int cl, int F, int kn, int tj,
+                                         int d) {
+  const int k = ((kn >> (8 * F)) & 0xff) - 1;
+  const R *bs = st.bas + (ql * 3 + F) * 8 + 4 * d;
+  R b[4];
+  if (sizeof(R) == 4) {
+    const float4 x = *reinterpret_cast<const float4 *>(bs);
+    b[0] = x.x; b[1] = x.y; b[2] = x.z; b[3] = x.w;
+  } else {
+    const double2 x = reinterpret_cast<const double2 *>(bs)[0], y = reinterpret_cast<const double2 *>(bs)[1];
+    b[0] = x.x; b[1] = x.y; b[2] = y.x; b[3] = y.y;
+  }
+  const int CG = fp.CG;
+  const R *cf = st.coef + ((size_t)(F * fp.nt + tj) * fp.NB + (k < 0 ? 0 : k)) * CG + cl;
+  return b[0] * cf[0] + b[1] * cf[CG] + b[2] * cf[2 * CG] + b[3] * cf[3 * CG];  // zero basis where k < 0
+}
+
 template <typename R>
 __device__ __forceinline__ FmPairVals<R> fm_pair_vals(const FmStage<R> &st, const FmPlan &fp, int ql, int cl) {
   R v[3], d[3];
-  const int kn = st.kn[ql], tj = st.tj[ql], CG = fp.CG;
+  const int kn = st.kn[ql], tj = st.tj[ql];
 #pragma unroll
-  for (int F = 0; F < 3; ++F) {
-    const int k = ((kn >> (8 * F)) & 0xff) - 1;
-    const R *bs = st.bas + (ql * 3 + F) * 8;
-    const R *cf = st.coef + ((size_t)(F * fp.nt + tj) * fp.NB + (k < 0 ? 0 : k)) * CG + cl;
-    const R c0 = cf[0], c1 = cf[CG], c2 = cf[2 * CG], c3 = cf[3 * CG];
-    v[F] = bs[0] * c0 + bs[1] * c1 + bs[2] * c2 + bs[3] * c3;  // zero basis where k < 0
-    d[F] = bs[4] * c0 + bs[5] * c1 + bs[6] * c2 + bs[7] * c3;
-  }
+  for (int F = 0; F < 3; ++F) fm_pair_val(st, fp, ql, cl, F, kn, tj, v[F], d[F]);
   return FmPairVals<R>{v[0], d[0], v[1], d[1], v[2], d[2]};
 }
 
@@ -676,9 +723,12 @@ __global__ void __launch_bounds__(256) k_fm_epi(DevDb db, DevPot pot, const Spli
       double rho = 0.0, epair = 0.0;
 #pragma unroll 4
       for (int p = 0; p < n; ++p) {
-        const FmPairVals<double> v = fm_pair_vals<double>(st, fp, lo + p, cl);
-        rho += v.rho + 0.5 * v.f * Yq[(size_t)p * 3 * CG];
-        epair += 0.5 * v.phi;
+        const int ql = lo + p, kn = st.kn[ql], tj = st.tj[ql];
+        const double phi = fm_pair_one<double>(st, fp, ql, cl, 0, kn, tj, 0);
+        const double rv = fm_pair_one<double>(st, fp, ql, cl, 1, kn, tj, 0);
+        const double fv = fm_pair_one<double>(st, fp, ql, cl, 2, kn, tj, 0);
+        rho += rv + 0.5 * fv * Yq[(size_t)p * 3 * CG];
+        epair += 0.5 * phi;
       }
       const double w = db.cell_w[db.atom_cell[i]];
       double pen = 0.0, rt = rho;
@@ -692,12 +742,29 @@ __global__ void __launch_bounds__(256) k_fm_epi(DevDb db, DevPot pot, const Spli
       const PointEval U = spl_point(tc, gU, rt);
       const double dF = U.grad;
       double F[3] = {0, 0, 0}, S[6] = {0, 0, 0, 0, 0, 0};
-#pragma unroll 2
-      for (int p = 0; p < n; ++p) {
+      // slots in batches of FM_PB, every load of a batch before its stores
+      for (int p0 = 0; p0 < n; p0 += FM_PB) {
+        double yv[FM_PB][3];
+#pragma unroll
+        for (int j = 0; j < FM_PB; ++j) {
+          const double *yp = Yq + (size_t)min(p0 + j, n - 1) * 3 * CG;
+          yv[j][0] = yp[0];
+          yv[j][1] = yp[CG];
+          yv[j][2] = yp[2 * CG];
+        }
+#pragma unroll
+      for (int j = 0; j < FM_PB; ++j) {
+        const int p = p0 + j;
+        if (p >= n) break;
         const int ql = lo + p;
-        const FmPairVals<double> v = fm_pair_vals<double>(st, fp, ql, cl);
-        const double *yp = Yq + (size_t)p * 3 * CG;
-        const double G = yp[0], Y1 = yp[CG], Y2 = yp[2 * CG];
+        FmPairVals<double> v;
+        {
+          const int kn = st.kn[ql], tj = st.tj[ql];
+          v.dphi = fm_pair_one<double>(st, fp, ql, cl, 0, kn, tj, 1);
+          v.drho = fm_pair_one<double>(st, fp, ql, cl, 1, kn, tj, 1);
+          fm_pair_val<double>(st, fp, ql, cl, 2, kn, tj, v.f, v.df);
+        }
+        const double G = yv[j][0], Y1 = yv[j][1], Y2 = yv[j][2];
         const double *e = st.e + ql * 6;
         const int64_t gs = st.gs[ql];
         const double4 ur = st.ur[ql];
@@ -720,6 +787,7 @@ __global__ void __launch_bounds__(256) k_fm_epi(DevDb db, DevPot pot, const Spli
         S[3] -= dx * (Vy * rr);
         S[4] -= dy * (Vz * rr);
         S[5] -= dz * (Vx * rr);
+      }
       }
       double *ao = fp.aoutF + ((size_t)gy * N + i) * AO_COUNT * CG + cl;
       ao[AO_AX * CG] = F[0];
@@ -890,6 +958,7 @@ __global__ void __launch_bounds__(256, 2) k_fm_adj_pre(DevDb db, DevPot pot, con
   double *utab = reinterpret_cast<double *>(fm_raw + off);
   float *pacc = reinterpret_cast<float *>(utab + (size_t)fp.ustride * CG);  // [3][nt][NB][CG]
   const int npe = 3 * fp.nt * fp.NB;
+  const int64_t nspan8 = ((fp.Q >> 7) + FM8_SPAN - 1) >> FM8_SPAN_LOG;  // spans of the integer adjoint's exponents
   for (int sidx = tid; sidx < pot.nsplines; sidx += T) sg[sidx] = geom[sidx];
   if (tid == 0) *st.ctype = -1;
   for (int e = tid; e < npe * CG; e += T) pacc[e] = 0.f;
@@ -953,90 +1022,134 @@ __global__ void __launch_bounds__(256, 2) k_fm_adj_pre(DevDb db, DevPot pot, con
         if (!pot.embed_extrap) { rt = gU.xN; drt = 0.0; }
       }
       const PointEval U = spl_point(tc, gU, rt);
-      auto lam = [&](int ql, const float4 &u, float &lx, float &ly, float &lz) {
-        const float *Lj = fp.lamf + ((size_t)gy * N + st.nbr[ql]) * 3 * CG + cl;
+      auto lam = [&](const float *Lj, const float4 &u, float &lx, float &ly, float &lz) {
         const float r = 1.f / u.w;
         lx = lix - Lj[0] - r * (mxx * u.x + mzx * u.z);
-        ly = liy - Lj[CG] - r * (myy * u.y + mxy * u.x);
-        lz = liz - Lj[2 * CG] - r * (mzz * u.z + myz * u.y);
+        ly = liy - Lj[1] - r * (myy * u.y + mxy * u.x);
+        lz = liz - Lj[2] - r * (mzz * u.z + myz * u.y);
       };
-      // ---- pass 1: K_i
+      // the integer adjoint's operand Z = 2^(e_q - 30) dL/dY: its exponent
+      // bound per (span of FM8_SPAN 128-slot tiles, candidate),
+      // |v| < 2^(field - 126), kept as the running maximum of the span
+      int64_t zspan = -1;
+      int zexp = -1000;
+      auto zbound = [&](int64_t q, float v, int eq) {
+        const int64_t sp = q >> (7 + FM8_SPAN_LOG);
+        if (sp != zspan) {
+          if (zspan >= 0 && zexp > -1000) atomicMax(fp.zmax + ((size_t)gy * nspan8 + zspan) * 64 + cl, zexp);
+          zspan = sp;
+          zexp = -1000;
+        }
+        if (v != 0.f) zexp = max(zexp, (int)((__float_as_uint(v) >> 23) & 255) - 126 + eq - FM8_SHIFT);
+      };
+      auto zflush = [&]() {
+        if (zspan >= 0 && zexp > -1000) atomicMax(fp.zmax + ((size_t)gy * nspan8 + zspan) * 64 + cl, zexp);
+        zspan = -1;
+        zexp = -1000;
+      };
+      const float dF = (float)U.grad;
+      // ---- pass 1: K_i, dL/dY1 and dL/dY2 (they do not depend on chi_i), and
+      // per slot (a_p, G_p, U' (Lambda.e1 Y1 + Lambda.e2 Y2) / r_p) for pass 2,
+      // kept as FP32 in the slot's own Y words (Y is not read again)
       double K = 0.0;
-#pragma unroll 4
-      for (int p = 0; p < n; ++p) {
-        const int ql = lo + p;
-        const FmPairVals<float> v = fm_pair_vals<float>(st, fp, ql, cl);
-        const double *yp = Yq + (size_t)p * 3 * CG;
-        const float4 u = st.uf[ql];
-        const float *e = reinterpret_cast<const float *>(st.e) + ql * 6;
-        float lx, ly, lz;
-        lam(ql, u, lx, ly, lz);
-        const float ap = lx * u.x + ly * u.y + lz * u.z;
-        const float l1 = lx * e[0] + ly * e[1] + lz * e[2], l2 = lx * e[3] + ly * e[4] + lz * e[5];
-        // the slot's term in FP32, the atom's sum in FP64
-        K += (double)(ap * (v.drho + v.df * (float)yp[0]) + v.f * u.w * (l1 * (float)yp[CG] + l2 * (float)yp[2 * CG]));
-        // kept for pass 2 in this slot's dL/dY words, which pass 2 then overwrites
-        float *yb = Ybq + (size_t)p * 3 * CG;
-        yb[0] = (float)ap;
-        yb[CG] = (float)l1;
-        yb[2 * CG] = (float)l2;
+      // slots in batches of FM_PB: every load of a batch is issued before its
+      // stores (the stores go to the same arrays, so the compiler would
+      // otherwise keep each slot's loads behind the previous slot's stores)
+      for (int p0 = 0; p0 < n; p0 += FM_PB) {
+        double yv[FM_PB][3];
+        float lj[FM_PB][3];
+#pragma unroll
+        for (int j = 0; j < FM_PB; ++j) {
+          const int p = min(p0 + j, n - 1);  // past the row: the last slot again, not used
+          const double *yp = Yq + (size_t)p * 3 * CG;
+          yv[j][0] = yp[0];
+          yv[j][1] = yp[CG];
+          yv[j][2] = yp[2 * CG];
+          const float *Lj = fp.lamf + ((size_t)gy * N + st.nbr[lo + p]) * 3 * CG + cl;
+          lj[j][0] = __ldg(Lj);
+          lj[j][1] = __ldg(Lj + CG);
+          lj[j][2] = __ldg(Lj + 2 * CG);
+        }
+#pragma unroll
+        for (int j = 0; j < FM_PB; ++j) {
+          const int p = p0 + j;
+          if (p >= n) break;
+          const int ql = lo + p;
+          const FmPairVals<float> v = fm_pair_vals<float>(st, fp, ql, cl);
+          double *yp = const_cast<double *>(Yq) + (size_t)p * 3 * CG;
+          const float G = (float)yv[j][0], Y1 = (float)yv[j][1], Y2 = (float)yv[j][2];
+          const float4 u = st.uf[ql];
+          const float *e = reinterpret_cast<const float *>(st.e) + ql * 6;
+          float lx, ly, lz;
+          lam(lj[j], u, lx, ly, lz);
+          const float ap = lx * u.x + ly * u.y + lz * u.z;
+          const float l1 = lx * e[0] + ly * e[1] + lz * e[2], l2 = lx * e[3] + ly * e[4] + lz * e[5];
+          const float t12 = (l1 * Y1 + l2 * Y2) * u.w;
+          // the slot's term in FP32, the atom's sum in FP64
+          K += (double)(ap * (v.drho + v.df * G) + v.f * t12);
+          const float B = dF * v.f * u.w, y1 = B * l1, y2 = B * l2;
+          float *yb = Ybq + (size_t)p * 3 * CG;
+          yb[CG] = y1;
+          yb[2 * CG] = y2;
+          *reinterpret_cast<float2 *>(yp) = make_float2(ap, G);
+          *reinterpret_cast<float *>(yp + CG) = dF * t12;
+          if (fp.zmax) {
+            const char4 eq = *reinterpret_cast<const char4 *>(fp.xe + (q0 + p) * 4);
+            zbound(q0 + p, y1, eq.y);
+            zbound(q0 + p, y2, eq.z);
+          }
+        }
       }
       const float ch = (float)((eps * U.grad + U.grad2 * K) * drt + kap * dpen);
-      const float dF = (float)U.grad;
       spl_point_adjoint(gU, U, rt, eps, K,
                         [&](int ix, double x) { atomicAdd(utab + (size_t)cl * fp.ustride + (gU.toff - fp.utoff) + ix, x); });
-      // ---- pass 2: dL/dY and the pair-function gradients
+      // ---- pass 2: dL/dG and the pair-function gradients
       const float epsf = (float)eps;
-      int64_t ztile = -1;
-      int zexp = -1000;
-#pragma unroll 4
-      for (int p = 0; p < n; ++p) {
-        const int ql = lo + p;
-        const FmPairVals<float> v = fm_pair_vals<float>(st, fp, ql, cl);
-        const double *yp = Yq + (size_t)p * 3 * CG;
-        const float G = (float)yp[0], Y1 = (float)yp[CG], Y2 = (float)yp[2 * CG];
-        const float4 u = st.uf[ql];
-        float *yb = Ybq + (size_t)p * 3 * CG;
-        const float ap = yb[0], l1 = yb[CG], l2 = yb[2 * CG];  // from pass 1
-        const float B = dF * v.f * u.w;
-        const float y0 = 0.5f * v.f * ch + ap * dF * v.df, y1 = B * l1, y2 = B * l2;
-        yb[0] = y0;
-        yb[CG] = y1;
-        yb[2 * CG] = y2;
-        if (fp.zmax) {
-          // the integer adjoint's operand Z = 2^(e_q - 30) dL/dY: its exponent
-          // bound per (128-slot tile, candidate), |v| < 2^(field - 126)
-          const int64_t q = q0 + p, Tq = q >> 7;
-          if (Tq != ztile) {
-            if (ztile >= 0 && zexp > -1000) atomicMax(fp.zmax + ((size_t)gy * (fp.Q >> 7) + ztile) * 64 + cl, zexp);
-            ztile = Tq;
-            zexp = -1000;
-          }
-          const char4 eq = *reinterpret_cast<const char4 *>(fp.xe + q * 4);
-          const float yy[3] = {y0, y1, y2};
-          const int ee[3] = {eq.x, eq.y, eq.z};
+      for (int p0 = 0; p0 < n; p0 += FM_PB) {
+        float2 aGv[FM_PB];
+        float svv[FM_PB];
 #pragma unroll
-          for (int t = 0; t < 3; ++t)
-            if (yy[t] != 0.f)
-              zexp = max(zexp, (int)((__float_as_uint(yy[t]) >> 23) & 255) - 126 + ee[t] - FM8_SHIFT);
+        for (int j = 0; j < FM_PB; ++j) {
+          const double *yp = Yq + (size_t)min(p0 + j, n - 1) * 3 * CG;
+          aGv[j] = *reinterpret_cast<const float2 *>(yp);
+          svv[j] = *reinterpret_cast<const float *>(yp + CG);
         }
-        const float wv[3] = {0.5f * epsf, ch, 0.5f * ch * G + dF * (l1 * Y1 + l2 * Y2) * u.w};
-        const float wd[3] = {0.5f * ap, dF * ap, dF * ap * G};
+#pragma unroll
+      for (int j = 0; j < FM_PB; ++j) {
+        const int p = p0 + j;
+        if (p >= n) break;
+        const int ql = lo + p;
+        const float ap = aGv[j].x, G = aGv[j].y, sv = svv[j];
         const int kn = st.kn[ql], tj = st.tj[ql];
+        float bs[3][8];
+#pragma unroll
+        for (int F = 0; F < 3; ++F) fm_bas(st, ql, F, bs[F]);
+        float f, df;
+        {
+          const int k = ((kn >> 16) & 0xff) - 1;
+          const float *cf = st.coef + ((size_t)(2 * fp.nt + tj) * fp.NB + (k < 0 ? 0 : k)) * CG + cl;
+          const float c0 = cf[0], c1 = cf[CG], c2 = cf[2 * CG], c3 = cf[3 * CG];
+          f = bs[2][0] * c0 + bs[2][1] * c1 + bs[2][2] * c2 + bs[2][3] * c3;  // zero basis where k < 0
+          df = bs[2][4] * c0 + bs[2][5] * c1 + bs[2][6] * c2 + bs[2][7] * c3;
+        }
+        const float y0 = 0.5f * f * ch + ap * dF * df;
+        Ybq[(size_t)p * 3 * CG] = y0;
+        if (fp.zmax) zbound(q0 + p, y0, (int)fp.xe[(q0 + p) * 4]);
+        const float wv[3] = {0.5f * epsf, ch, 0.5f * ch * G + sv};
+        const float wd[3] = {0.5f * ap, dF * ap, dF * ap * G};
 #pragma unroll
         for (int F = 0; F < 3; ++F) {
           const int k = ((kn >> (8 * F)) & 0xff) - 1;
           if (k < 0) continue;
-          const float *bs = st.bas + (ql * 3 + F) * 8;
           float *pe = pacc + ((size_t)(F * fp.nt + tj) * fp.NB + k) * CG + cl;
-          atomicAdd(pe, wv[F] * bs[0] + wd[F] * bs[4]);
-          atomicAdd(pe + CG, wv[F] * bs[1] + wd[F] * bs[5]);
-          atomicAdd(pe + 2 * CG, wv[F] * bs[2] + wd[F] * bs[6]);
-          atomicAdd(pe + 3 * CG, wv[F] * bs[3] + wd[F] * bs[7]);
+          atomicAdd(pe, wv[F] * bs[F][0] + wd[F] * bs[F][4]);
+          atomicAdd(pe + CG, wv[F] * bs[F][1] + wd[F] * bs[F][5]);
+          atomicAdd(pe + 2 * CG, wv[F] * bs[F][2] + wd[F] * bs[F][6]);
+          atomicAdd(pe + 3 * CG, wv[F] * bs[F][3] + wd[F] * bs[F][7]);
         }
       }
-      if (fp.zmax && ztile >= 0 && zexp > -1000)
-        atomicMax(fp.zmax + ((size_t)gy * (fp.Q >> 7) + ztile) * 64 + cl, zexp);
+      }
+      if (fp.zmax) zflush();
     }
   }
   if (pacc_t >= 0) flush_pairs(pacc_t);

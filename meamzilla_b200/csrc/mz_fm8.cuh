@@ -301,98 +301,46 @@ namespace mzb {
 //   Kbar_s[d][c] = sum_{t,q} X[t][q][d] Ybar[q][t][c]                 (k_fm_gemm_adj's sum)
 //
 // With X = 2^(e_q - 30) X_int the row scale folds into the other operand,
-// Z[t][q][c] = 2^(e_q - 30) Ybar[q][t][c], so Kbar = sum X_int Z.  k_fm_zdig
-// writes Z of every 128-slot tile as four balanced base-256 digits of a
-// 31-bit integer with one power-of-two scale per (tile, candidate) over the
-// tile's three kinds (Z = 2^(e_Tc - 30) Z_int); padding slots are zero.  The
-// MMA reads the moments' digit blocks as they are stored for the forward --
-// 128 slot rows of 128 feature bytes -- as an MN-major operand (M = 128
-// features, K = slots: 8-row groups 1 KiB apart), and Z's as a K-major one
-// (N = 64 candidates, K = slots), so one tile's three kinds are 3 x 4 K steps
-// of 32 slots per 128-feature half, ten digit pairs each, into the four class
-// accumulators of each half (all 512 TMEM columns; at most 4 x 384 x 128^2
-// < 2^31 per tile).  At the end of a tile the sixteen epilogue warps (lane
-// quarter x feature half x candidate half) read them out and add
-//   2^(e_Tc - 30) (acc_0 2^48 + acc_1 2^40 + acc_2 2^32 + acc_3 2^24)
-// to FP64 sums held per thread (32 candidates of one feature), written to the
-// CTA's partial of the type when the CTA's run of tiles changes type and at
-// its end.
-//   Z8 [ngroups][ntile8][3 kinds][4 digits][64 candidates x 128 B]   8 KB blocks
-//   ze [ngroups][ntile8][64]                e_Tc (int32)
+// Z[t][q][c] = 2^(e_q - 30) Ybar[q][t][c], so Kbar = sum X_int Z.  Z is
+// written as four balanced base-256 digits of a 31-bit integer with one
+// power-of-two scale per (span of FM8_SPAN tiles, candidate),
+// Z = 2^(e_Sc - 30) Z_int; the adjoint pre pass leaves the bound e_Sc
+// (|Z| < 2^e_Sc over the span) in fp.zmax.  The digits never reach global
+// memory: sixteen converter warps read Ybar (FP32) of each (tile, kind) and
+// write Z's digits straight into the shared-memory stage the MMA reads, a
+// K-major operand (N = 64 candidates, K = slots, rows of 128 slot bytes).
+// The MMA reads the moments' digit blocks as they are stored for the
+// forward -- 128 slot rows of 128 feature bytes -- as an MN-major operand
+// (M = 128 features, K = slots: 8-row groups 1 KiB apart).  One tile's three
+// kinds are 3 x 4 K steps of 32 slots per 128-feature half, ten digit pairs
+// each, into the four class accumulators of each half (all 512 TMEM
+// columns).  The accumulators carry the sums of a whole segment -- the tiles
+// of one span and one atom type in this CTA's run -- exactly (at most
+// 4 x 384 x FM8_SPAN x 128^2 < 2^31), and at its end the same sixteen warps
+// (lane quarter x feature half x candidate half) read them out and add
+//   2^(e_Sc - 30) (acc_0 2^48 + acc_1 2^40 + acc_2 2^32 + acc_3 2^24)
+// to the CTA's FP64 partial of the type (each (feature, candidate) word has
+// one owner thread).  Padding slots (past a type's last real slot) and
+// absent candidates give zero digits.
 
-constexpr int FM8_ZBLK = FM8_NC * 128;         // one (tile, kind, digit) block of Z8: 8 KB
+constexpr int FM8_ZBLK = FM8_NC * 128;          // one (tile, kind, digit) block of Z: 8 KB
 constexpr int FM8_ZSTAGE = FM8_DIG * FM8_ZBLK;  // one (tile, kind): 32 KB
-constexpr int FM8_ATHREADS = 576;              // producer, MMA, sixteen epilogue warps
+constexpr int FM8_ATHREADS = 576;               // producer, MMA, sixteen converter / epilogue warps
 
-__host__ __device__ inline size_t z8_block(int gy, int64_t T, int64_t ntile8, int t, int l) {
-  return ((((size_t)gy * ntile8 + T) * 3 + t) * FM8_DIG + l) * FM8_ZBLK;
-}
+static_assert(4LL * 3 * FM8_TM * FM8_SPAN * 128 * 128 < (1LL << 31), "segment class sums must stay exact in S32");
 
-// Z's digits of one tile (blockIdx.x) of group blockIdx.y, one pass: the
-// exponent bound of every candidate over the tile comes from the pre pass
-// (fp.zmax, maximum of the FP32 exponent fields plus e_q - 30).  Thread =
-// one candidate (c = thread % 64) and a quarter of the tile's 96 (kind,
-// 4-slot group) items; the digits of four slots are packed into one word per
-// digit of the swizzled K-major image, which is then written out in 16-byte
-// pieces.
-__global__ void __launch_bounds__(256) k_fm_zdig(FmPlan fp, signed char *__restrict__ Z8, int *__restrict__ ze) {
-  extern __shared__ __align__(16) unsigned char zsm[];  // [3][4][8 KB]
-  __shared__ char4 sxe[FM8_TM];
-  const int64_t T = blockIdx.x, ntile8 = fp.Q / FM8_TM;
-  const int gy = blockIdx.y, CG = fp.CG, tid = threadIdx.x;
-  const int c = tid & (FM8_NC - 1), g = tid >> 6;  // 4 item groups (blockDim.x == 256)
-  const int s = fm_tile_type(fp, (int)(2 * T));
-  const int64_t q0t = T * FM8_TM, qend = fp.qend[s];
-  if (CG < FM8_NC)  // rows of absent candidates stay zero
-    for (int i = tid; i < 3 * FM8_ZSTAGE / 16; i += blockDim.x)
-      reinterpret_cast<int4 *>(zsm)[i] = make_int4(0, 0, 0, 0);
-  if (tid < FM8_TM) sxe[tid] = *reinterpret_cast<const char4 *>(fp.xe + (q0t + tid) * 4);
-  __syncthreads();
-  const bool live = c < CG;
-  const int zm = live ? fp.zmax[((size_t)gy * ntile8 + T) * FM8_NC + c] : -2000;
-  const int e = zm > -1000 ? max(-100, zm) : 0;  // a bound: |Z| < 2^e
-  const float *Yg = fp.Yb + ((size_t)gy * fp.Q + q0t) * 3 * CG + c;
-  if (live) {
-#pragma unroll 2
-    for (int it = g; it < 3 * (FM8_TM / 4); it += 4) {
-      const int t = it % 3, r0 = 4 * (it / 3);
-      uint32_t w[FM8_DIG] = {0u, 0u, 0u, 0u};
-#pragma unroll
-      for (int k = 0; k < 4; ++k) {
-        const int r = r0 + k;
-        if (q0t + r >= qend) continue;
-        const char4 x4 = sxe[r];
-        const int sh = (t == 0 ? x4.x : (t == 1 ? x4.y : x4.z)) - e;
-        // Z_int = Ybar 2^(e_q - e): a power-of-two scaling, one rounding to int32
-        int zi = __double2int_rn((double)Yg[(size_t)(r * 3 + t) * CG] *
-                                 __longlong_as_double((long long)(sh + 1023) << 52));
-        // balanced base-256 digits, least significant first, in 32-bit arithmetic
-#pragma unroll
-        for (int l = FM8_DIG - 1; l > 0; --l) {
-          const int lo = ((zi + 128) & 255) - 128;
-          w[l] |= (uint32_t)(lo & 255) << (8 * k);
-          zi = (zi - lo) >> 8;
-        }
-        w[0] |= (uint32_t)(zi & 255) << (8 * k);
-      }
-      const uint32_t o = sw128_byte(c, r0);  // 4 slots: 4 bytes of one 16-byte chunk
-#pragma unroll
-      for (int l = 0; l < FM8_DIG; ++l)
-        *reinterpret_cast<uint32_t *>(zsm + (size_t)(t * FM8_DIG + l) * FM8_ZBLK + o) = w[l];
-    }
-  }
-  __syncthreads();
-  int4 *dst = reinterpret_cast<int4 *>(Z8 + z8_block(gy, T, ntile8, 0, 0));
-  for (int i = tid; i < 3 * FM8_ZSTAGE / 16; i += blockDim.x) dst[i] = reinterpret_cast<const int4 *>(zsm)[i];
-  if (tid < FM8_NC) ze[((size_t)gy * ntile8 + T) * FM8_NC + tid] = e;
-}
+// spans of the adjoint operand's exponents
+__host__ __device__ inline int64_t fm8_nspan(int64_t Q) { return (Q / FM8_TM + FM8_SPAN - 1) >> FM8_SPAN_LOG; }
+
+// The span exponent of a bound from the pre pass (|Z| < 2^zm; below -1000:
+// no non-zero value), kept in [-100, ...).
+__device__ __forceinline__ int fm8_span_exp(int zm) { return zm > -1000 ? max(-100, zm) : 0; }
 
 __host__ __device__ constexpr size_t fm8_adj_smem() {
   return 1024 + 2 * (size_t)FM8_STAGE + 2 * (size_t)FM8_ZSTAGE + sizeof(uint64_t) * 12 + 16;
 }
 
-__global__ void __maxnreg__(96) k_fm_gemm_adj8(FmPlan fp, const signed char *__restrict__ Z8,
-                                                                 const int *__restrict__ ze, int *__restrict__ err) {
+__global__ void __maxnreg__(96) k_fm_gemm_adj8(FmPlan fp, int ncand, int *__restrict__ err) {
   extern __shared__ __align__(16) unsigned char sm8raw[];
   const uint32_t raw = tc::smem_u32(sm8raw);
   unsigned char *sA = sm8raw + (((raw + 1023u) & ~1023u) - raw);  // [2][64 KB] moments' digits (tile, kind, half)
@@ -401,21 +349,26 @@ __global__ void __maxnreg__(96) k_fm_gemm_adj8(FmPlan fp, const signed char *__r
   uint64_t *aempty = afull + 2, *bfull = aempty + 2, *bempty = bfull + 2;
   uint64_t *accf = bempty + 2, *acce = accf + 1, *mdone = acce + 1;
   uint32_t *tslot = reinterpret_cast<uint32_t *>(mdone + 1);
-  __shared__ __align__(16) int zes[2 * FM8_NC];  // candidate exponents of a tile, double-buffered
 
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int gy = blockIdx.y, CG = fp.CG, nt = fp.nt;
-  const int64_t ntile8 = fp.Q / FM8_TM;
+  const int64_t ntile8 = fp.Q / FM8_TM, nspan = fm8_nspan(fp.Q);
   const int64_t per = (ntile8 + gridDim.x - 1) / gridDim.x;
   const int64_t tb = (int64_t)blockIdx.x * per, te = min(ntile8, tb + per);
   double *Kb = fp.Kbar + ((size_t)gy * gridDim.x + blockIdx.x) * nt * fp.Dpad * CG;
   for (int i = tid; i < nt * fp.Dpad * CG; i += blockDim.x) Kb[i] = 0.0;
+  // a segment ends at the last tile of a span, before a change of atom type
+  // and at the end of the CTA's run
+  auto seg_end = [&](int64_t T) {
+    return T + 1 >= te || ((T + 1) & (FM8_SPAN - 1)) == 0 ||
+           fm_tile_type(fp, (int)(2 * (T + 1))) != fm_tile_type(fp, (int)(2 * T));
+  };
 
   if (tid == 0) {
     for (int i = 0; i < 2; ++i) {
       tc::mbar_init(afull + i, 1);
       tc::mbar_init(aempty + i, 1);
-      tc::mbar_init(bfull + i, 1);
+      tc::mbar_init(bfull + i, 16);
       tc::mbar_init(bempty + i, 1);
     }
     tc::mbar_init(accf, 1);
@@ -429,21 +382,12 @@ __global__ void __maxnreg__(96) k_fm_gemm_adj8(FmPlan fp, const signed char *__r
   const uint32_t tm = *tslot;
 
   if (warp == 0) {
-    // ---------------- producer: per (tile, kind) Z's 32 KB, then the moments' two 64 KB halves
+    // ---------------- producer: per (tile, kind) the moments' two 64 KB halves
     if (lane == 0) {
-      int64_t ia = 0, ib = 0;
+      int64_t ia = 0;
       bool ok = true;
       for (int64_t T = tb; T < te && ok; ++T)
-        for (int t = 0; t < 3 && ok; ++t) {
-          const int bst = (int)(ib & 1);
-          if (ib >= 2 && !tc::mbar_wait(bempty + bst, (uint32_t)(((ib >> 1) & 1) ^ 1), FM8_WAIT)) {
-            atomicExch(err, 5);
-            ok = false;
-            break;
-          }
-          tc::mbar_expect_tx(bfull + bst, FM8_ZSTAGE);
-          tc::bulk_g2s(sB + bst * FM8_ZSTAGE, Z8 + z8_block(gy, T, ntile8, t, 0), FM8_ZSTAGE, bfull + bst);
-          ++ib;
+        for (int t = 0; t < 3 && ok; ++t)
           for (int kb = 0; kb < 2; ++kb) {
             const int ast = (int)(ia & 1);
             if (ia >= 2 && !tc::mbar_wait(aempty + ast, (uint32_t)(((ia >> 1) & 1) ^ 1), FM8_WAIT)) {
@@ -455,12 +399,9 @@ __global__ void __maxnreg__(96) k_fm_gemm_adj8(FmPlan fp, const signed char *__r
             tc::bulk_g2s(sA + ast * FM8_STAGE, fp.X8 + x8_block(T, t, kb, 0), FM8_STAGE, afull + ast);
             ++ia;
           }
-        }
       // copies in flight land before the CTA can exit
       for (int64_t j = ia > 2 ? ia - 2 : 0; j < ia; ++j)
         if (!tc::mbar_wait(afull + (int)(j & 1), (uint32_t)((j >> 1) & 1), FM8_WAIT)) atomicExch(err, 5);
-      for (int64_t j = ib > 2 ? ib - 2 : 0; j < ib; ++j)
-        if (!tc::mbar_wait(bfull + (int)(j & 1), (uint32_t)((j >> 1) & 1), FM8_WAIT)) atomicExch(err, 5);
     }
   } else if (warp == 1) {
     // ---------------- MMA issue: A = moments (MN-major), B = Z (K-major)
@@ -470,10 +411,10 @@ __global__ void __maxnreg__(96) k_fm_gemm_adj8(FmPlan fp, const signed char *__r
       // class, four bits per pair
       constexpr int NP = 10;
       constexpr uint64_t PI = 0x3210210100ull, PJ = 0x0123012010ull, PM = 0x3333222110ull, PF = 0x0001001011ull;
-      bool ok = true;
-      int64_t ia = 0, ib = 0, tile = 0;
-      for (int64_t T = tb; T < te && ok; ++T, ++tile) {
-        if (tile >= 1 && !tc::mbar_wait(acce, (uint32_t)((tile - 1) & 1), FM8_WAIT)) {
+      bool ok = true, fresh = true;  // fresh: the next tile starts a segment
+      int64_t ia = 0, ib = 0, seg = 0;
+      for (int64_t T = tb; T < te && ok; ++T) {
+        if (fresh && seg >= 1 && !tc::mbar_wait(acce, (uint32_t)((seg - 1) & 1), FM8_WAIT)) {
           atomicExch(err, 6);
           ok = false;
           break;
@@ -507,7 +448,7 @@ __global__ void __maxnreg__(96) k_fm_gemm_adj8(FmPlan fp, const signed char *__r
                 const uint64_t ad = tc::desc_sw128(a0 + i * FM8_XBLK + 4096 * kk, FM8_STAGE, 1024);
                 const uint64_t bd = tc::desc_sw128(b0 + j * FM8_ZBLK + 32 * kk, 16, 1024);
                 const uint32_t d = tm + (uint32_t)(kb * 256 + m * FM8_NC);
-                tc::mma_s8(d, ad, bd, idesc, (t == 0 && kk == 0 && f) ? 0u : 1u);
+                tc::mma_s8(d, ad, bd, idesc, (fresh && t == 0 && kk == 0 && f) ? 0u : 1u);
               }
             tc::commit(aempty + ast);
             ++ia;
@@ -516,74 +457,150 @@ __global__ void __maxnreg__(96) k_fm_gemm_adj8(FmPlan fp, const signed char *__r
           tc::commit(bempty + bst);
           ++ib;
         }
-        if (ok) tc::commit(accf);
+        if (!ok) break;
+        fresh = seg_end(T);
+        if (fresh) {
+          tc::commit(accf);
+          ++seg;
+        }
       }
       tc::commit(mdone);
       if (!tc::mbar_wait(mdone, 0, FM8_WAIT)) atomicExch(err, 6);
     }
   } else {
-    // ---------------- epilogue: warps 2..17, lane quarter warp % 4, feature half and
-    // candidate half from (warp - 2) / 4
+    // ---------------- converters / epilogue: warps 2..17
+    // conversion: candidate cc, slots 16 g .. 16 g + 15 of each (tile, kind)
+    const int ct = tid - 64, cc = ct & (FM8_NC - 1), g = ct >> 6;
+    const bool live = cc < CG && gy * CG + cc < ncand;
+    const float *Ybase = fp.Yb + (size_t)gy * fp.Q * 3 * CG + cc;
+    // read-out: TMEM lane quarter warp % 4, feature half and candidate half from (warp - 2) / 4
     constexpr int NCH = FM8_NC / 2;
     const int grp = (warp - 2) >> 2, quarter = warp & 3, half = grp & 1, c0 = (grp >> 1) * NCH;
     const int d = half * FM8_TM + 32 * quarter + lane;
-    double acc[NCH];
-#pragma unroll
-    for (int c = 0; c < NCH; ++c) acc[c] = 0.0;
-    auto flush = [&](int s) {
-      if (d < fp.Dpad) {
-        double *kb = Kb + ((size_t)s * fp.Dpad + d) * CG + c0;
-#pragma unroll
-        for (int c = 0; c < NCH; ++c)
-          if (c0 + c < CG) kb[c] += acc[c];
-      }
-#pragma unroll
-      for (int c = 0; c < NCH; ++c) acc[c] = 0.0;
-    };
-    int cur = -1;
-    int64_t tile = 0;
+    int64_t ib = 0, seg = 0, pend = -1, cspan = -1;
+    int e = 0;
     bool ok = true;
-    for (int64_t T = tb; T < te && ok; ++T, ++tile) {
-      const int s = fm_tile_type(fp, (int)(2 * T));
-      if (s != cur && cur >= 0) flush(cur);
-      cur = s;
-      // the tile's candidate exponents into shared memory while its MMAs run
-      // (double-buffered: every epilogue warp has left tile - 1 at the barrier)
-      int *zs = zes + (tile & 1) * FM8_NC;
-      if (warp == 2) {
-        const int *zt = ze + ((size_t)gy * ntile8 + T) * FM8_NC;
-        zs[lane] = zt[lane];
-        zs[lane + 32] = zt[lane + 32];
-      }
-      asm volatile("bar.sync 1, 512;" ::: "memory");  // the sixteen epilogue warps
-      if (!tc::mbar_wait(accf, (uint32_t)(tile & 1), FM8_WAIT)) {
+    auto drain = [&](int64_t Tend) {
+      if (!tc::mbar_wait(accf, (uint32_t)(seg & 1), FM8_WAIT)) {
         atomicExch(err, 7);
         ok = false;
-        break;
+        return;
       }
       tc::fence_after_sync();
+      const int s = fm_tile_type(fp, (int)(2 * Tend));
+      const int *zm = fp.zmax + ((size_t)gy * nspan + (Tend >> FM8_SPAN_LOG)) * FM8_NC + c0;
+      double *kbp = Kb + ((size_t)s * fp.Dpad + d) * CG + c0;
       const uint32_t ta = tm + ((uint32_t)(32 * quarter) << 16) + (uint32_t)(half * 256 + c0);
+#pragma unroll 1
+      for (int cb = 0; cb < NCH / 8; ++cb) {
+        int v[FM8_CLS][8];
 #pragma unroll
-      for (int cb = 0; cb < NCH / 4; ++cb) {
-        int v[FM8_CLS][4];
-#pragma unroll
-        for (int m = 0; m < FM8_CLS; ++m) tc::tmem_ld4i(ta + m * FM8_NC + cb * 4, v[m]);
-        const int4 ez = *reinterpret_cast<const int4 *>(zs + c0 + cb * 4);
+        for (int m = 0; m < FM8_CLS; ++m) tc::tmem_ld8i(ta + m * FM8_NC + cb * 8, v[m]);
+        const int4 z0 = *reinterpret_cast<const int4 *>(zm + cb * 8), z1 = *reinterpret_cast<const int4 *>(zm + cb * 8 + 4);
         tc::tmem_wait_ld();
-        const int e4[4] = {ez.x, ez.y, ez.z, ez.w};
+        const int e8[8] = {z0.x, z0.y, z0.z, z0.w, z1.x, z1.y, z1.z, z1.w};
 #pragma unroll
-        for (int u = 0; u < 4; ++u) {
-          const double a = ((double)v[0][u] * 281474976710656.0 + (double)v[1][u] * 1099511627776.0) +
-                           ((double)v[2][u] * 4294967296.0 + (double)v[3][u] * 16777216.0);
-          // 2^(e - 30), e in [-100, 100]: a normal double built from its exponent field
-          acc[cb * 4 + u] += a * __longlong_as_double((long long)(e4[u] - FM8_SHIFT + 1023) << 52);
+        for (int u = 0; u < 8; ++u) {
+          const int c = c0 + cb * 8 + u;
+          if (d < fp.Dpad && c < CG) {
+            const double a = ((double)v[0][u] * 281474976710656.0 + (double)v[1][u] * 1099511627776.0) +
+                             ((double)v[2][u] * 4294967296.0 + (double)v[3][u] * 16777216.0);
+            // 2^(e - 30), e in [-100, 100]: a normal double built from its exponent field
+            kbp[cb * 8 + u] += a * __longlong_as_double((long long)(fm8_span_exp(e8[u]) - FM8_SHIFT + 1023) << 52);
+          }
         }
       }
       tc::fence_before_sync();
       __syncwarp();
       if (lane == 0) tc::mbar_arrive(acce);
+      ++seg;
+    };
+    float yn[16];  // the next (tile, kind)'s operand, loaded ahead
+    if (tb < te) {
+      const int64_t q0 = tb * FM8_TM + 16 * g, qend = fp.qend[fm_tile_type(fp, (int)(2 * tb))];
+#pragma unroll
+      for (int k = 0; k < 16; ++k) yn[k] = (live && q0 + k < qend) ? Ybase[(size_t)(q0 + k) * 3 * CG] : 0.f;
     }
-    if (cur >= 0) flush(cur);
+    for (int64_t T = tb; T < te && ok; ++T) {
+      const int64_t sp = T >> FM8_SPAN_LOG;
+      if (sp != cspan) {
+        cspan = sp;
+        e = live ? fm8_span_exp(fp.zmax[((size_t)gy * nspan + sp) * FM8_NC + cc]) : 0;
+      }
+      const int s = fm_tile_type(fp, (int)(2 * T));
+      const int64_t q0 = T * FM8_TM + 16 * g, qend = fp.qend[s];
+      for (int t = 0; t < 3 && ok; ++t) {
+        const int bst = (int)(ib & 1);
+        float y[16];
+#pragma unroll
+        for (int k = 0; k < 16; ++k) y[k] = yn[k];
+        {  // the next item's loads in flight while this one is converted
+          const int tn = t == 2 ? 0 : t + 1;
+          const int64_t qn = t == 2 ? q0 + FM8_TM : q0;
+          const bool more = t < 2 || T + 1 < te;
+          const int64_t qendn = t == 2 && more ? fp.qend[fm_tile_type(fp, (int)(2 * (T + 1)))] : qend;
+#pragma unroll
+          for (int k = 0; k < 16; ++k)
+            yn[k] = (more && live && qn + k < qendn) ? Ybase[((size_t)(qn + k) * 3 + tn) * CG] : 0.f;
+        }
+        // the 16 slots' row exponents (kinds 0..2 in bytes 0..2 of each word)
+        int xw[16];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+          const int4 x4 = *reinterpret_cast<const int4 *>(fp.xe + q0 * 4 + 16 * k);
+          xw[4 * k] = x4.x;
+          xw[4 * k + 1] = x4.y;
+          xw[4 * k + 2] = x4.z;
+          xw[4 * k + 3] = x4.w;
+        }
+        if (ib >= 2 && !tc::mbar_wait(bempty + bst, (uint32_t)(((ib >> 1) & 1) ^ 1), FM8_WAIT)) {
+          atomicExch(err, 7);
+          ok = false;
+          break;
+        }
+        // Z_int = Ybar 2^(e_q - e): a power-of-two scaling in two exact FP32
+        // steps (each factor a normal float for |e_q - e| <= 252, below which
+        // every value rounds to zero; the product
+        // neither overflows, |Z_int| <= 2^30, nor underflows where it rounds
+        // to a non-zero integer), one rounding to int32; balanced base-256
+        // digits, least significant first, four slots per 32-bit word of
+        // each digit's 16-byte chunk
+        uint32_t w[FM8_DIG][4];
+#pragma unroll
+        for (int l = 0; l < FM8_DIG; ++l)
+#pragma unroll
+          for (int k4 = 0; k4 < 4; ++k4) w[l][k4] = 0u;
+#pragma unroll
+        for (int k = 0; k < 16; ++k) {
+          const int sh = max(-252, (int)(signed char)((xw[k] >> (8 * t)) & 255) - e), h1 = sh >> 1;
+          const float s1 = __int_as_float((h1 + 127) << 23), s2 = __int_as_float((sh - h1 + 127) << 23);
+          int zi = __float2int_rn((y[k] * s1) * s2);
+#pragma unroll
+          for (int l = FM8_DIG - 1; l > 0; --l) {
+            const int lo = ((zi + 128) & 255) - 128;
+            w[l][k >> 2] |= (uint32_t)(lo & 255) << (8 * (k & 3));
+            zi = (zi - lo) >> 8;
+          }
+          w[0][k >> 2] |= (uint32_t)(zi & 255) << (8 * (k & 3));
+        }
+        unsigned char *zb = sB + bst * FM8_ZSTAGE + sw128_byte(cc, 16 * g);
+#pragma unroll
+        for (int l = 0; l < FM8_DIG; ++l)
+          *reinterpret_cast<uint4 *>(zb + l * FM8_ZBLK) = make_uint4(w[l][0], w[l][1], w[l][2], w[l][3]);
+        tc::fence_async_smem();
+        __syncwarp();
+        if (lane == 0) tc::mbar_arrive(bfull + bst);
+        ++ib;
+        // the previous segment's read-out once the next tile's first kind is
+        // staged (the MMAs wait for both)
+        if (t == 0 && pend >= 0) {
+          drain(pend);
+          pend = -1;
+        }
+      }
+      if (ok && seg_end(T)) pend = T;
+    }
+    if (ok && pend >= 0) drain(pend);
   }
   tc::fence_before_sync();
   __syncthreads();
