@@ -368,7 +368,16 @@ bool fm_prepare(mz_ctx *ctx) {
   const size_t G = fm.ngroups_max, CG = fm.CGmax, Cp = G * CG;
   const size_t Q = fp.Q, N = ctx->natoms, NC = ctx->ncells, Np = ctx->npairs, ns = ctx->nsplines;
   const size_t stride = ctx->stride;
-  fp.nctas_pre = std::max(1, std::min(fp.nblk, 3 * ctx->nsm));
+  // the pre pass's persistent grid: as many CTAs as are resident at once (a
+  // second wave would run a fixed share of the blocks on a half-empty GPU);
+  // launches of fewer candidates stage less and stay resident as well
+  fm.smem_pre = fm_pre_smem(ctx->nsplines, 64, fp.nt, fp.NB, fp.ustride);
+  smem_attr(k_fm_adj_pre, fm.smem_pre);
+  {
+    int occ = 0;
+    ck(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_fm_adj_pre, 256, fm.smem_pre), "occupancy");
+    fp.nctas_pre = std::max(1, std::min(fp.nblk, std::max(1, occ) * ctx->nsm));
+  }
   fp.nctas_adj = std::max(1, std::min(fp.ntiles, ctx->nsm));
   const size_t aux_rows = (size_t)ctx->pot.aux_rows;
   struct Need {
@@ -466,8 +475,6 @@ bool fm_prepare(mz_ctx *ctx) {
   smem_attr(k_fm_gemm_fwd<2>, fm_fwd_smem<2>(fp.Dpad));
   smem_attr(k_fm_gemm_fwd<4>, fm_fwd_smem<4>(fp.Dpad));
   smem_attr(k_fm_gemm_fwd<8>, fm_fwd_smem<8>(fp.Dpad));
-  fm.smem_pre = fm_pre_smem(ctx->nsplines, 64, fp.nt, fp.NB, fp.ustride);
-  smem_attr(k_fm_adj_pre, fm.smem_pre);
   smem_attr(k_fm_epi, fm_epi_smem(ctx->nsplines, fp.nt, fp.NB, 64));
   smem_attr(k_fm_gemm_adj<false>, fm_adj_smem(fp.Dpad, 64));
   if (fm.tc8) smem_attr(k_fm_gemm_adj<true>, fm_adj_smem(fp.Dpad, 64, true));
@@ -521,8 +528,12 @@ void enqueue_fm(mz_ctx *ctx, int n, double *d_obj, double *d_errvec, double *d_f
   const unsigned ablocks = (unsigned)(((int64_t)N * CG + 255) / 256);
   {
     Bracket b(ctx, MZ_K_FM_EPI);
-    const int eb = std::max(1, std::min(fp.nblk, 8 * ctx->nsm));
-    k_fm_epi<<<dim3(eb, G), 256, fm_epi_smem(ns, fp.nt, fp.NB, CG), st>>>(ctx->db, ctx->pot, ctx->d_geom,
+    // persistent CTAs, as many as are resident at once
+    const size_t esm = fm_epi_smem(ns, fp.nt, fp.NB, CG);
+    int occ = 0;
+    ck(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_fm_epi, 256, esm), "occupancy");
+    const int eb = std::max(1, std::min(fp.nblk, std::max(1, occ) * ctx->nsm));
+    k_fm_epi<<<dim3(eb, G), 256, esm, st>>>(ctx->db, ctx->pot, ctx->d_geom,
                                                                          ctx->d_tabs, fp, n);
     ck(cudaGetLastError(), "k_fm_epi launch");
   }

@@ -101,7 +101,7 @@ constexpr int FM8_KBLK = FM8_NC * 128;           // one (digit, kblock) block of
 constexpr int FM8_STAGE = FM8_DIG * FM8_XBLK;    // one (tile, kind, kblock): 64 KB
 constexpr int FM8_BTYPE = 2 * FM8_DIG * FM8_KBLK;  // K8 of one type: 64 KB
 constexpr int FM8_SHIFT = 30;                    // |X_int|, |K_int| <= 2^30
-constexpr int FM8_NST = 2;                       // stages in the ring
+constexpr int FM8_NST = 8;                       // stages in the ring, one (tile, kind, kblock, digit) block each
 constexpr int FM8_THREADS = 192;
 constexpr uint32_t FM8_WAIT = 1u << 26;          // polls before a wait gives up
 constexpr int FM8_SPAN_LOG = 3;
@@ -1105,17 +1105,17 @@ __global__ void __launch_bounds__(256, 2) k_fm_adj_pre(DevDb db, DevPot pot, con
                         [&](int ix, double x) { atomicAdd(utab + (size_t)cl * fp.ustride + (gU.toff - fp.utoff) + ix, x); });
       // ---- pass 2: dL/dG and the pair-function gradients
       const float epsf = (float)eps;
-      for (int p0 = 0; p0 < n; p0 += FM_PB) {
-        float2 aGv[FM_PB];
-        float svv[FM_PB];
+      for (int p0 = 0; p0 < n; p0 += 2 * FM_PB) {
+        float2 aGv[2 * FM_PB];
+        float svv[2 * FM_PB];
 #pragma unroll
-        for (int j = 0; j < FM_PB; ++j) {
+        for (int j = 0; j < 2 * FM_PB; ++j) {
           const double *yp = Yq + (size_t)min(p0 + j, n - 1) * 3 * CG;
           aGv[j] = *reinterpret_cast<const float2 *>(yp);
           svv[j] = *reinterpret_cast<const float *>(yp + CG);
         }
 #pragma unroll
-      for (int j = 0; j < FM_PB; ++j) {
+      for (int j = 0; j < 2 * FM_PB; ++j) {
         const int p = p0 + j;
         if (p >= n) break;
         const int ql = lo + p;

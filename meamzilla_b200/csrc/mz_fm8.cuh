@@ -97,7 +97,7 @@ __global__ void __launch_bounds__(256) k_fm_kmat8(int ncand, DevPot pot, FmPlan 
 // ---------------------------------------------------------- k_fm_gemm_fwd8
 
 __host__ __device__ constexpr size_t fm8_smem(int nt) {
-  return 1024 + (size_t)FM8_NST * FM8_STAGE + (size_t)FM8_BTYPE + sizeof(double) * FM_MAXT * FM8_NC +
+  return 1024 + (size_t)FM8_NST * FM8_XBLK + (size_t)FM8_BTYPE + sizeof(double) * FM_MAXT * FM8_NC +
          sizeof(uint64_t) * (2 * FM8_NST + 8) + 16;
 }
 
@@ -105,7 +105,7 @@ __global__ void __launch_bounds__(FM8_THREADS, 1) k_fm_gemm_fwd8(FmPlan fp, int 
   extern __shared__ __align__(16) unsigned char sm8raw[];
   const uint32_t raw = tc::smem_u32(sm8raw);
   unsigned char *sA = sm8raw + (((raw + 1023u) & ~1023u) - raw);  // 1 KiB aligned
-  unsigned char *sB = sA + FM8_NST * FM8_STAGE;                    // K8 of the current type
+  unsigned char *sB = sA + FM8_NST * FM8_XBLK;                     // K8 of the current type
   double *ssc = reinterpret_cast<double *>(sB + FM8_BTYPE);        // [nt][64] 2^(e_c - 60)
   uint64_t *full = reinterpret_cast<uint64_t *>(ssc + FM_MAXT * FM8_NC);
   uint64_t *empty = full + FM8_NST;
@@ -166,16 +166,17 @@ __global__ void __launch_bounds__(FM8_THREADS, 1) k_fm_gemm_fwd8(FmPlan fp, int 
           cur = s;
         }
         for (int t = 0; t < 3 && ok; ++t)
-          for (int kb = 0; kb < 2; ++kb, ++it) {
-            const int st = (int)(it % FM8_NST);
-            if (it >= FM8_NST && !tc::mbar_wait(empty + st, (uint32_t)(((it / FM8_NST) & 1) ^ 1), FM8_WAIT)) {
-              atomicExch(err, 2);
-              ok = false;
-              break;
+          for (int kb = 0; kb < 2 && ok; ++kb)
+            for (int l = 0; l < FM8_DIG; ++l, ++it) {
+              const int st = (int)(it % FM8_NST);
+              if (it >= FM8_NST && !tc::mbar_wait(empty + st, (uint32_t)(((it / FM8_NST) & 1) ^ 1), FM8_WAIT)) {
+                atomicExch(err, 2);
+                ok = false;
+                break;
+              }
+              tc::mbar_expect_tx(full + st, FM8_XBLK);
+              tc::bulk_g2s(sA + st * FM8_XBLK, fp.X8 + x8_block(T, t, kb, l), FM8_XBLK, full + st);
             }
-            tc::mbar_expect_tx(full + st, FM8_STAGE);
-            tc::bulk_g2s(sA + st * FM8_STAGE, fp.X8 + x8_block(T, t, kb, 0), FM8_STAGE, full + st);
-          }
       }
       // copies in flight land before the CTA can exit
       for (int64_t j = it > FM8_NST ? it - FM8_NST : 0; j < it; ++j)
@@ -186,11 +187,6 @@ __global__ void __launch_bounds__(FM8_THREADS, 1) k_fm_gemm_fwd8(FmPlan fp, int 
     // ---------------- MMA issue
     if (lane == 0) {
       constexpr uint32_t idesc = tc::idesc_s8(FM8_TM, FM8_NC);
-      // digit pairs (i, j) of classes i + j <= 3; the first of each class starts its sum
-      constexpr int NP = 10;
-      const int pi[NP] = {0, 0, 1, 0, 1, 2, 0, 1, 2, 3}, pj[NP] = {0, 1, 0, 2, 1, 0, 3, 2, 1, 0};
-      const int pm[NP] = {0, 1, 1, 2, 2, 2, 3, 3, 3, 3};
-      const bool first[NP] = {true, true, false, true, false, false, true, false, false, false};
       bool ok = true;
       int64_t it = 0, seq = 0;
       int cur = -1, nb = 0;
@@ -215,26 +211,30 @@ __global__ void __launch_bounds__(FM8_THREADS, 1) k_fm_gemm_fwd8(FmPlan fp, int 
             break;
           }
           tc::fence_after_sync();
-          for (int kb = 0; kb < 2; ++kb, ++it) {
-            const int st = (int)(it % FM8_NST);
-            if (!tc::mbar_wait(full + st, (uint32_t)((it / FM8_NST) & 1), FM8_WAIT)) {
-              atomicExch(err, 3);
-              ok = false;
-              break;
-            }
-            tc::fence_after_sync();
-            const uint32_t a0 = tc::smem_u32(sA + st * FM8_STAGE);
-#pragma unroll
-            for (int kk = 0; kk < 4; ++kk)
-#pragma unroll
-              for (int p = 0; p < NP; ++p) {
-                const uint64_t ad = tc::desc_sw128(a0 + pi[p] * FM8_XBLK + 32 * kk, 16, 1024);
-                const uint64_t bd = tc::desc_sw128(b0 + (kb * FM8_DIG + pj[p]) * FM8_KBLK + 32 * kk, 16, 1024);
-                const uint32_t d = tm + (uint32_t)(buf * 256 + pm[p] * FM8_NC);
-                tc::mma_s8(d, ad, bd, idesc, (kb == 0 && kk == 0 && first[p]) ? 0u : 1u);
+          // one stage per digit i of the moments: the pairs (i, j), j <= 3 - i,
+          // of the classes i + j; each class starts with its pair (0, j)
+          for (int kb = 0; kb < 2 && ok; ++kb)
+            for (int i = 0; i < FM8_DIG; ++i, ++it) {
+              const int st = (int)(it % FM8_NST);
+              if (!tc::mbar_wait(full + st, (uint32_t)((it / FM8_NST) & 1), FM8_WAIT)) {
+                atomicExch(err, 3);
+                ok = false;
+                break;
               }
-            tc::commit(empty + st);  // the stage is free once these MMAs are done
-          }
+              tc::fence_after_sync();
+              const uint32_t a0 = tc::smem_u32(sA + st * FM8_XBLK);
+#pragma unroll
+              for (int kk = 0; kk < 4; ++kk)
+#pragma unroll
+                for (int j = 0; j < FM8_DIG; ++j)
+                  if (j < FM8_DIG - i) {
+                    const uint64_t ad = tc::desc_sw128(a0 + 32 * kk, 16, 1024);
+                    const uint64_t bd = tc::desc_sw128(b0 + (kb * FM8_DIG + j) * FM8_KBLK + 32 * kk, 16, 1024);
+                    const uint32_t d = tm + (uint32_t)(buf * 256 + (i + j) * FM8_NC);
+                    tc::mma_s8(d, ad, bd, idesc, (kb == 0 && kk == 0 && i == 0) ? 0u : 1u);
+                  }
+              tc::commit(empty + st);  // the stage is free once these MMAs are done
+            }
           if (ok) tc::commit(accf + buf);
         }
       }
@@ -337,16 +337,16 @@ __host__ __device__ inline int64_t fm8_nspan(int64_t Q) { return (Q / FM8_TM + F
 __device__ __forceinline__ int fm8_span_exp(int zm) { return zm > -1000 ? max(-100, zm) : 0; }
 
 __host__ __device__ constexpr size_t fm8_adj_smem() {
-  return 1024 + 2 * (size_t)FM8_STAGE + 2 * (size_t)FM8_ZSTAGE + sizeof(uint64_t) * 12 + 16;
+  return 1024 + (size_t)FM8_NST * FM8_XBLK + 2 * (size_t)FM8_ZSTAGE + sizeof(uint64_t) * (2 * FM8_NST + 8) + 16;
 }
 
 __global__ void __maxnreg__(96) k_fm_gemm_adj8(FmPlan fp, int ncand, int *__restrict__ err) {
   extern __shared__ __align__(16) unsigned char sm8raw[];
   const uint32_t raw = tc::smem_u32(sm8raw);
-  unsigned char *sA = sm8raw + (((raw + 1023u) & ~1023u) - raw);  // [2][64 KB] moments' digits (tile, kind, half)
-  unsigned char *sB = sA + 2 * FM8_STAGE;                          // [2][32 KB] Z digits (tile, kind)
+  unsigned char *sA = sm8raw + (((raw + 1023u) & ~1023u) - raw);  // [NST][16 KB] moments' digits (tile, kind, half, digit)
+  unsigned char *sB = sA + FM8_NST * FM8_XBLK;                     // [2][32 KB] Z digits (tile, kind)
   uint64_t *afull = reinterpret_cast<uint64_t *>(sB + 2 * FM8_ZSTAGE);
-  uint64_t *aempty = afull + 2, *bfull = aempty + 2, *bempty = bfull + 2;
+  uint64_t *aempty = afull + FM8_NST, *bfull = aempty + FM8_NST, *bempty = bfull + 2;
   uint64_t *accf = bempty + 2, *acce = accf + 1, *mdone = acce + 1;
   uint32_t *tslot = reinterpret_cast<uint32_t *>(mdone + 1);
 
@@ -365,9 +365,11 @@ __global__ void __maxnreg__(96) k_fm_gemm_adj8(FmPlan fp, int ncand, int *__rest
   };
 
   if (tid == 0) {
-    for (int i = 0; i < 2; ++i) {
+    for (int i = 0; i < FM8_NST; ++i) {
       tc::mbar_init(afull + i, 1);
       tc::mbar_init(aempty + i, 1);
+    }
+    for (int i = 0; i < 2; ++i) {
       tc::mbar_init(bfull + i, 16);
       tc::mbar_init(bempty + i, 1);
     }
@@ -382,35 +384,32 @@ __global__ void __maxnreg__(96) k_fm_gemm_adj8(FmPlan fp, int ncand, int *__rest
   const uint32_t tm = *tslot;
 
   if (warp == 0) {
-    // ---------------- producer: per (tile, kind) the moments' two 64 KB halves
+    // ---------------- producer: per (tile, kind, half) the moments' four 16 KB digit blocks
     if (lane == 0) {
       int64_t ia = 0;
       bool ok = true;
       for (int64_t T = tb; T < te && ok; ++T)
         for (int t = 0; t < 3 && ok; ++t)
-          for (int kb = 0; kb < 2; ++kb) {
-            const int ast = (int)(ia & 1);
-            if (ia >= 2 && !tc::mbar_wait(aempty + ast, (uint32_t)(((ia >> 1) & 1) ^ 1), FM8_WAIT)) {
-              atomicExch(err, 5);
-              ok = false;
-              break;
+          for (int kb = 0; kb < 2 && ok; ++kb)
+            for (int l = 0; l < FM8_DIG; ++l) {
+              const int ast = (int)(ia % FM8_NST);
+              if (ia >= FM8_NST && !tc::mbar_wait(aempty + ast, (uint32_t)(((ia / FM8_NST) & 1) ^ 1), FM8_WAIT)) {
+                atomicExch(err, 5);
+                ok = false;
+                break;
+              }
+              tc::mbar_expect_tx(afull + ast, FM8_XBLK);
+              tc::bulk_g2s(sA + ast * FM8_XBLK, fp.X8 + x8_block(T, t, kb, l), FM8_XBLK, afull + ast);
+              ++ia;
             }
-            tc::mbar_expect_tx(afull + ast, FM8_STAGE);
-            tc::bulk_g2s(sA + ast * FM8_STAGE, fp.X8 + x8_block(T, t, kb, 0), FM8_STAGE, afull + ast);
-            ++ia;
-          }
       // copies in flight land before the CTA can exit
-      for (int64_t j = ia > 2 ? ia - 2 : 0; j < ia; ++j)
-        if (!tc::mbar_wait(afull + (int)(j & 1), (uint32_t)((j >> 1) & 1), FM8_WAIT)) atomicExch(err, 5);
+      for (int64_t j = ia > FM8_NST ? ia - FM8_NST : 0; j < ia; ++j)
+        if (!tc::mbar_wait(afull + (int)(j % FM8_NST), (uint32_t)((j / FM8_NST) & 1), FM8_WAIT)) atomicExch(err, 5);
     }
   } else if (warp == 1) {
     // ---------------- MMA issue: A = moments (MN-major), B = Z (K-major)
     if (lane == 0) {
       constexpr uint32_t idesc = tc::idesc_s8(FM8_TM, FM8_NC, 1, 0);
-      // the ten digit pairs (i, j), their class i + j and the first of each
-      // class, four bits per pair
-      constexpr int NP = 10;
-      constexpr uint64_t PI = 0x3210210100ull, PJ = 0x0123012010ull, PM = 0x3333222110ull, PF = 0x0001001011ull;
       bool ok = true, fresh = true;  // fresh: the next tile starts a segment
       int64_t ia = 0, ib = 0, seg = 0;
       for (int64_t T = tb; T < te && ok; ++T) {
@@ -429,30 +428,31 @@ __global__ void __maxnreg__(96) k_fm_gemm_adj8(FmPlan fp, int ncand, int *__rest
           }
           tc::fence_after_sync();
           const uint32_t b0 = tc::smem_u32(sB + bst * FM8_ZSTAGE);
-          for (int kb = 0; kb < 2; ++kb) {
-            const int ast = (int)(ia & 1);
-            if (!tc::mbar_wait(afull + ast, (uint32_t)((ia >> 1) & 1), FM8_WAIT)) {
-              atomicExch(err, 6);
-              ok = false;
-              break;
-            }
-            tc::fence_after_sync();
-            const uint32_t a0 = tc::smem_u32(sA + ast * FM8_STAGE);
-#pragma unroll 1
-            for (int kk = 0; kk < 4; ++kk)
-#pragma unroll 1
-              for (int p = 0; p < NP; ++p) {
-                const int i = (int)((PI >> (4 * p)) & 15), j = (int)((PJ >> (4 * p)) & 15);
-                const int m = (int)((PM >> (4 * p)) & 15), f = (int)((PF >> (4 * p)) & 15);
-                // 32 slot rows per K step: 4 groups of 8 rows, 1 KiB apart
-                const uint64_t ad = tc::desc_sw128(a0 + i * FM8_XBLK + 4096 * kk, FM8_STAGE, 1024);
-                const uint64_t bd = tc::desc_sw128(b0 + j * FM8_ZBLK + 32 * kk, 16, 1024);
-                const uint32_t d = tm + (uint32_t)(kb * 256 + m * FM8_NC);
-                tc::mma_s8(d, ad, bd, idesc, (fresh && t == 0 && kk == 0 && f) ? 0u : 1u);
+          // one stage per digit i of the moments: the pairs (i, j), j <= 3 - i,
+          // of the classes i + j; each class starts with its pair (0, j)
+          for (int kb = 0; kb < 2 && ok; ++kb)
+            for (int i = 0; i < FM8_DIG; ++i) {
+              const int ast = (int)(ia % FM8_NST);
+              if (!tc::mbar_wait(afull + ast, (uint32_t)((ia / FM8_NST) & 1), FM8_WAIT)) {
+                atomicExch(err, 6);
+                ok = false;
+                break;
               }
-            tc::commit(aempty + ast);
-            ++ia;
-          }
+              tc::fence_after_sync();
+              const uint32_t a0 = tc::smem_u32(sA + ast * FM8_XBLK);
+#pragma unroll 1
+              for (int kk = 0; kk < 4; ++kk)
+#pragma unroll 1
+                for (int j = 0; j < FM8_DIG - i; ++j) {
+                  // 32 slot rows per K step: 4 groups of 8 rows, 1 KiB apart
+                  const uint64_t ad = tc::desc_sw128(a0 + 4096 * kk, FM8_STAGE, 1024);
+                  const uint64_t bd = tc::desc_sw128(b0 + j * FM8_ZBLK + 32 * kk, 16, 1024);
+                  const uint32_t d = tm + (uint32_t)(kb * 256 + (i + j) * FM8_NC);
+                  tc::mma_s8(d, ad, bd, idesc, (fresh && t == 0 && kk == 0 && i == 0) ? 0u : 1u);
+                }
+              tc::commit(aempty + ast);
+              ++ia;
+            }
           if (!ok) break;
           tc::commit(bempty + bst);
           ++ib;
