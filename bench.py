@@ -55,6 +55,9 @@ def parse_args():
     ap.add_argument("--ncells", type=int, default=2000)
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--only-step", action="store_true",
+                    help="run only the metric's step (warm-up + steps, no FP64, accuracy, end-to-end or CPU legs) "
+                         "and print its time: the launch sequence the profiles capture")
     ap.add_argument("--cpu-configs", action="store_true",
                     help="time the compiled reference's objective on the smaller workloads (one JSON line each) "
                          "and exit")
@@ -254,7 +257,11 @@ KERNEL_BYTES_TC = {
 KERNEL_TRAFFIC = {
     "k_adj": lambda st, nc: 2480.3e6 / 15.8433e6 * st["npairs"] * nc,
     "k_atoms": lambda st, nc: 496.0e6 / 3.9608e6 * st["npairs"] * nc,
+    # 200-cell case, 1,980,412 pair slots x 64 candidates (profiles/k_fm_epilogues_small.md)
+    "k_fm_adj_pre": lambda st, nc: 7583.3e6 / 126.746e6 * st["npairs"] * nc,
+    "k_fm_epi": lambda st, nc: 7020.8e6 / 126.746e6 * st["npairs"] * nc,
 }
+KERNEL_TRAFFIC["k_fm_pre"] = KERNEL_TRAFFIC["k_fm_adj_pre"]
 
 
 # --------------------------------------------------------- CPU reference arm
@@ -442,6 +449,14 @@ def run_mine(args, world, rank, local):
     # the metric's own call (64 candidates, mixed, with gradient) comes first
     ev.objective_grad_device(Xd, obj, grad, MZ_MIXED)
     ev.sync()
+    if args.only_step:
+        for _ in range(args.warmup + args.steps):
+            ev.objective_grad_device(Xd, obj, grad, MZ_MIXED)
+        ev.sync()
+        if rank == 0:
+            print(json.dumps({"only_step": True, "steps": args.warmup + args.steps, "ncand": args.ncand,
+                              "ncells": args.ncells, "moment_path": ev.moment_path(MZ_MIXED, True)}))
+        return
 
     # accuracy of the mixed path against FP64: objectives of all candidates,
     # forces and gradients of ACC_SAMPLE of them (every 64 / ACC_SAMPLE-th)

@@ -34,8 +34,8 @@
 //
 // k_fm_gemm_fwd8: persistent, one CTA per SM over a contiguous run of 128-slot
 // tiles (type-pure: each type's slots are padded to 128).  Warp 0 streams the
-// tiles' digit blocks into a two-stage ring (cp.async.bulk, completion on an
-// mbarrier), warp 1 issues the MMAs (M = 128 slots, N = 64 candidates, K = 32
+// tiles' 16 KB digit blocks into an eight-stage ring (cp.async.bulk, completion
+// on an mbarrier), warp 1 issues the MMAs (M = 128 slots, N = 64 candidates, K = 32
 // bytes; ten digit pairs per K step into four class accumulators of 64
 // columns) and commits them to mbarriers, warps 2-5 read the accumulators of
 // the previous (tile, kind) out of tensor memory (two sets of 256 columns, so
@@ -560,28 +560,30 @@ __global__ void __maxnreg__(96) k_fm_gemm_adj8(FmPlan fp, int ncand, int *__rest
         }
         // Z_int = Ybar 2^(e_q - e): a power-of-two scaling in two exact FP32
         // steps (each factor a normal float for |e_q - e| <= 252, below which
-        // every value rounds to zero; the product
-        // neither overflows, |Z_int| <= 2^30, nor underflows where it rounds
-        // to a non-zero integer), one rounding to int32; balanced base-256
-        // digits, least significant first, four slots per 32-bit word of
-        // each digit's 16-byte chunk
+        // every value rounds to zero; the product neither overflows,
+        // |Z_int| <= 2^30, nor underflows where it rounds to a non-zero
+        // integer), one rounding to int32.  Its balanced base-256 digits are
+        // the bytes of (Z_int + 0x808080) ^ 0x808080 (the offset makes the
+        // three lower digits + 128 the bytes, without carries; the top byte is
+        // the top digit); a 4 x 4 byte transpose then gathers one digit of four
+        // slots per 32-bit word of that digit's 16-byte chunk
         uint32_t w[FM8_DIG][4];
 #pragma unroll
-        for (int l = 0; l < FM8_DIG; ++l)
+        for (int k4 = 0; k4 < 4; ++k4) {
+          uint32_t v[4];
 #pragma unroll
-          for (int k4 = 0; k4 < 4; ++k4) w[l][k4] = 0u;
-#pragma unroll
-        for (int k = 0; k < 16; ++k) {
-          const int sh = max(-252, (int)(signed char)((xw[k] >> (8 * t)) & 255) - e), h1 = sh >> 1;
-          const float s1 = __int_as_float((h1 + 127) << 23), s2 = __int_as_float((sh - h1 + 127) << 23);
-          int zi = __float2int_rn((y[k] * s1) * s2);
-#pragma unroll
-          for (int l = FM8_DIG - 1; l > 0; --l) {
-            const int lo = ((zi + 128) & 255) - 128;
-            w[l][k >> 2] |= (uint32_t)(lo & 255) << (8 * (k & 3));
-            zi = (zi - lo) >> 8;
+          for (int u = 0; u < 4; ++u) {
+            const int k = 4 * k4 + u;
+            const int sh = max(-252, (int)(signed char)((xw[k] >> (8 * t)) & 255) - e), h1 = sh >> 1;
+            const float s1 = __int_as_float((h1 + 127) << 23), s2 = __int_as_float((sh - h1 + 127) << 23);
+            v[u] = ((uint32_t)__float2int_rn((y[k] * s1) * s2) + 0x808080u) ^ 0x808080u;
           }
-          w[0][k >> 2] |= (uint32_t)(zi & 255) << (8 * (k & 3));
+          const uint32_t ablo = __byte_perm(v[0], v[1], 0x5140), abhi = __byte_perm(v[0], v[1], 0x7362);
+          const uint32_t cdlo = __byte_perm(v[2], v[3], 0x5140), cdhi = __byte_perm(v[2], v[3], 0x7362);
+          w[3][k4] = __byte_perm(ablo, cdlo, 0x5410);  // least significant digit
+          w[2][k4] = __byte_perm(ablo, cdlo, 0x7632);
+          w[1][k4] = __byte_perm(abhi, cdhi, 0x5410);
+          w[0][k4] = __byte_perm(abhi, cdhi, 0x7632);  // most significant digit
         }
         unsigned char *zb = sB + bst * FM8_ZSTAGE + sw128_byte(cc, 16 * g);
 #pragma unroll

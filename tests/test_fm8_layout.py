@@ -236,3 +236,29 @@ def test_adjoint_class_sums_read_moments_mn_major():
     # against the magnitudes: spans of widely varying rows (this data spans a
     # factor 1e4 within a span) lose bits on their small rows, never on the largest
     assert np.max(err / scale) <= 2e-5
+
+
+def _byte_perm(x, y, sel):
+    b = [(x >> (8 * i)) & 255 for i in range(4)] + [(y >> (8 * i)) & 255 for i in range(4)]
+    return sum(b[(sel >> (4 * i)) & 7] << (8 * i) for i in range(4))
+
+
+def test_converter_digit_bytes_and_transpose():
+    """The adjoint's converters take the balanced base-256 digits of
+    |Z_int| <= 2^30 as the bytes of (Z_int + 0x808080) ^ 0x808080 and gather
+    one digit of four slots per word with a 4 x 4 byte transpose
+    (__byte_perm selectors 0x5140 / 0x7362, then 0x5410 / 0x7632)."""
+    rng = np.random.default_rng(5)
+    edge = [2 ** 30, -(2 ** 30), 0, 1, -1, 127, -128, 128, -129, 255, -256, 32767, -32769]
+    vals = [int(v) for v in rng.integers(-(2 ** 30), 2 ** 30 + 1, 4000)] + edge * 4
+    for i in range(0, len(vals) - 3, 4):
+        z = vals[i:i + 4]
+        v = [((x + 0x808080) ^ 0x808080) & 0xFFFFFFFF for x in z]
+        ablo, abhi = _byte_perm(v[0], v[1], 0x5140), _byte_perm(v[0], v[1], 0x7362)
+        cdlo, cdhi = _byte_perm(v[2], v[3], 0x5140), _byte_perm(v[2], v[3], 0x7362)
+        w = {3: _byte_perm(ablo, cdlo, 0x5410), 2: _byte_perm(ablo, cdlo, 0x7632),
+             1: _byte_perm(abhi, cdhi, 0x5410), 0: _byte_perm(abhi, cdhi, 0x7632)}
+        for u, x in enumerate(z):
+            d = digits(x)
+            for l in range(DIG):
+                assert (w[l] >> (8 * u)) & 255 == d[l] & 255, (x, l)
