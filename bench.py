@@ -258,8 +258,8 @@ KERNEL_TRAFFIC = {
     "k_adj": lambda st, nc: 2480.3e6 / 15.8433e6 * st["npairs"] * nc,
     "k_atoms": lambda st, nc: 496.0e6 / 3.9608e6 * st["npairs"] * nc,
     # 200-cell case, 1,980,412 pair slots x 64 candidates (profiles/k_fm_epilogues_small.md)
-    "k_fm_adj_pre": lambda st, nc: 7583.3e6 / 126.746e6 * st["npairs"] * nc,
-    "k_fm_epi": lambda st, nc: 7020.8e6 / 126.746e6 * st["npairs"] * nc,
+    "k_fm_adj_pre": lambda st, nc: 7605.1e6 / 126.746e6 * st["npairs"] * nc,
+    "k_fm_epi": lambda st, nc: 7058.5e6 / 126.746e6 * st["npairs"] * nc,
 }
 KERNEL_TRAFFIC["k_fm_pre"] = KERNEL_TRAFFIC["k_fm_adj_pre"]
 

@@ -488,7 +488,7 @@ struct FmStage {
   int *gs, *nbr, *tj, *kn;  // [BLOCK_SLOTS]
   int *ctype;         // type whose coefficients are staged (-1: none yet)
   float4 *uf;         // [BLOCK_SLOTS] (ux, uy, uz, 1/r)
-  double *e;          // [BLOCK_SLOTS][6] e1, e2 (FP32 stages keep them as floats in the same space)
+  double *e;          // [BLOCK_SLOTS][6] e1 / r, e2 / r (FP32 stages keep e1, e2 as floats in the same space)
   double4 *ur;        // [BLOCK_SLOTS] (ux, uy, uz, r) in FP64
   R *bas;             // [BLOCK_SLOTS][3][8] basis N0..N3 and d/dr N0'..N3' of phi, rho, f
   R *coef;            // [3][nt][NB][CG]
@@ -570,10 +570,11 @@ __device__ int fm_stage_block(const DevDb &db, const DevPot &pot, const SplineGe
     if (sizeof(R) == 4) st.uf[ql] = make_float4(db.pair_uxf[gs], db.pair_uyf[gs], db.pair_uzf[gs], 1.f / db.pair_rf[gs]);
     st.ur[ql] = make_double4(db.pair_ux[gs], db.pair_uy[gs], db.pair_uz[gs], db.pair_r[gs]);
     const double *e = fp.E + (size_t)(fp.row0[i] + p) * 8;
+    const double ir = 1.0 / db.pair_r[gs];  // the FP64 stage keeps e1 / r, e2 / r (its only use)
 #pragma unroll
     for (int k = 0; k < 6; ++k) {
       if (sizeof(R) == 4) reinterpret_cast<float *>(st.e)[ql * 6 + k] = (float)e[k];
-      else st.e[ql * 6 + k] = e[k];
+      else st.e[ql * 6 + k] = e[k] * ir;
     }
 #pragma unroll
     for (int F = 0; F < 3; ++F) {
@@ -770,7 +771,7 @@ __global__ void __launch_bounds__(256) k_fm_epi(DevDb db, DevPot pot, const Spli
         const double4 ur = st.ur[ql];
         const double rr = ur.w, dx = ur.x, dy = ur.y, dz = ur.z;
         const double A = 0.5 * v.dphi + dF * (v.drho + v.df * G);
-        const double B = dF * v.f / rr;
+        const double B = dF * v.f;  // the staged frames carry the 1 / r
         const double Vx = dx * A + B * (e[0] * Y1 + e[3] * Y2);
         const double Vy = dy * A + B * (e[1] * Y1 + e[4] * Y2);
         const double Vz = dz * A + B * (e[2] * Y1 + e[5] * Y2);
@@ -1023,7 +1024,7 @@ __global__ void __launch_bounds__(256, 2) k_fm_adj_pre(DevDb db, DevPot pot, con
       }
       const PointEval U = spl_point(tc, gU, rt);
       auto lam = [&](const float *Lj, const float4 &u, float &lx, float &ly, float &lz) {
-        const float r = 1.f / u.w;
+        const float r = __frcp_rn(u.w);
         lx = lix - Lj[0] - r * (mxx * u.x + mzx * u.z);
         ly = liy - Lj[1] - r * (myy * u.y + mxy * u.x);
         lz = liz - Lj[2] - r * (mzz * u.z + myz * u.y);
@@ -1033,14 +1034,17 @@ __global__ void __launch_bounds__(256, 2) k_fm_adj_pre(DevDb db, DevPot pot, con
       // |v| < 2^(field - 126), kept as the running maximum of the span
       int64_t zspan = -1;
       int zexp = -1000;
-      auto zbound = [&](int64_t q, float v, int eq) {
+      // FP32 exponent field of v plus e_q (a value's bound before the
+      // constant -126 - 30), far below every bound for v = 0
+      auto zfield = [](float v, int eq) { return v != 0.f ? (int)((__float_as_uint(v) >> 23) & 255) + eq : -100000; };
+      auto zbound = [&](int64_t q, int fe) {
         const int64_t sp = q >> (7 + FM8_SPAN_LOG);
         if (sp != zspan) {
           if (zspan >= 0 && zexp > -1000) atomicMax(fp.zmax + ((size_t)gy * nspan8 + zspan) * 64 + cl, zexp);
           zspan = sp;
           zexp = -1000;
         }
-        if (v != 0.f) zexp = max(zexp, (int)((__float_as_uint(v) >> 23) & 255) - 126 + eq - FM8_SHIFT);
+        zexp = max(zexp, fe - 126 - FM8_SHIFT);
       };
       auto zflush = [&]() {
         if (zspan >= 0 && zexp > -1000) atomicMax(fp.zmax + ((size_t)gy * nspan8 + zspan) * 64 + cl, zexp);
@@ -1092,11 +1096,10 @@ __global__ void __launch_bounds__(256, 2) k_fm_adj_pre(DevDb db, DevPot pot, con
           yb[CG] = y1;
           yb[2 * CG] = y2;
           *reinterpret_cast<float2 *>(yp) = make_float2(ap, G);
-          *reinterpret_cast<float *>(yp + CG) = dF * t12;
+          *reinterpret_cast<float2 *>(yp + CG) = make_float2(dF * t12, 0.f);  // whole words: no partial sectors
           if (fp.zmax) {
             const char4 eq = *reinterpret_cast<const char4 *>(fp.xe + (q0 + p) * 4);
-            zbound(q0 + p, y1, eq.y);
-            zbound(q0 + p, y2, eq.z);
+            zbound(q0 + p, max(zfield(y1, eq.y), zfield(y2, eq.z)));
           }
         }
       }
@@ -1134,7 +1137,7 @@ __global__ void __launch_bounds__(256, 2) k_fm_adj_pre(DevDb db, DevPot pot, con
         }
         const float y0 = 0.5f * f * ch + ap * dF * df;
         Ybq[(size_t)p * 3 * CG] = y0;
-        if (fp.zmax) zbound(q0 + p, y0, (int)fp.xe[(q0 + p) * 4]);
+        if (fp.zmax) zbound(q0 + p, zfield(y0, (int)fp.xe[(q0 + p) * 4]));
         const float wv[3] = {0.5f * epsf, ch, 0.5f * ch * G + sv};
         const float wd[3] = {0.5f * ap, dF * ap, dF * ap * G};
 #pragma unroll
