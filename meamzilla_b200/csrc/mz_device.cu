@@ -385,7 +385,7 @@ bool fm_prepare(mz_ctx *ctx) {
     size_t have_bytes, need_bytes;
   };
   Need need[] = {
-      {ctx->d_aux, sizeof(double) * C * aux_rows * Np, (sizeof(double) + sizeof(float)) * G * Q * 3 * CG},  // Y, Yb
+      {ctx->d_aux, sizeof(double) * C * aux_rows * Np, 2 * sizeof(float) * G * Q * 3 * CG},  // Y, Yb
       {ctx->d_V, sizeof(double) * C * 3 * Np, sizeof(double) * Cp * Np * 3},                   // V
       {ctx->d_aout, sizeof(double) * C * AO_COUNT * N, sizeof(double) * Cp * AO_COUNT * N},    // aoutF
       {ctx->d_lam, sizeof(double) * C * 3 * N, sizeof(float) * Cp * 3 * N},                    // lamf
@@ -429,8 +429,8 @@ bool fm_prepare(mz_ctx *ctx) {
   auto pick = [&](Need &x) -> void * {
     return x.need_bytes <= x.have_bytes ? x.have : (void *)dalloc<unsigned char>(ctx, x.need_bytes);
   };
-  fp.Y = static_cast<double *>(pick(need[0]));
-  fp.Yb = reinterpret_cast<float *>(fp.Y + G * Q * 3 * CG);
+  fp.Y = static_cast<float *>(pick(need[0]));
+  fp.Yb = fp.Y + G * Q * 3 * CG;
   fp.V = static_cast<double *>(pick(need[1]));
   fp.aoutF = static_cast<double *>(pick(need[2]));
   fp.lamf = static_cast<float *>(pick(need[3]));

@@ -29,7 +29,7 @@
 // contiguous, each type's run padded to a multiple of FM_TILE):
 //   X     [nch][3][FM_DC][Q]         moments, FM_DC features per chunk
 //   E     [Q][8]                     e1, e2 of the slot (FP64)
-//   Y     [ngroups][Q][3][CG]        G, Y1, Y2 (FP64)
+//   Y     [ngroups][Q][3][CG]        G, Y1, Y2 (FP32)
 //   Yb    [ngroups][Q][3][CG]        dL/dG, dL/dY1, dL/dY2 (FP32)
 //   V     [ngroups][Np][CG][3]       reaction vectors (FP64), global slot order
 //   aoutF [ngroups][N][AO_COUNT][CG] per-atom outputs (FP64)
@@ -68,7 +68,7 @@ struct FmPlan {
   const int *row0;         // [N] feature slot of each atom's first pair
   const float *X;
   const double *E;         // [Q][8] e1, e2 of each slot (FP64)
-  double *Y;               // [ngroups][Q][3][CG] G, Y1, Y2 (FP64 sums of the contraction)
+  float *Y;                // [ngroups][Q][3][CG] G, Y1, Y2 (the contraction's sums, rounded once to FP32)
   float *Yb;               // [ngroups][Q][3][CG] dL/dG, dL/dY1, dL/dY2 (FP32, the adjoint's operand)
   const float *Kf;         // [ngroups][nt][Dpad][CG]
   const double *coef64;    // [ncand][nsplines][FM_MAXB]
@@ -455,18 +455,18 @@ __global__ void __launch_bounds__(NW * 32, 1) k_fm_gemm_fwd(FmPlan fp) {
       }
     __syncthreads();
   }
-  double *Yo = fp.Y + ((size_t)gy * fp.Q + qb + 2 * lane) * 3 * CG + warp * 8;
+  float *Yo = fp.Y + ((size_t)gy * fp.Q + qb + 2 * lane) * 3 * CG + warp * 8;
 #pragma unroll
   for (int h = 0; h < 2; ++h)
 #pragma unroll
     for (int t = 0; t < 3; ++t) {
-      double *dst = Yo + ((size_t)h * 3 + t) * CG;
+      float *dst = Yo + ((size_t)h * 3 + t) * CG;
 #pragma unroll
       for (int c = 0; c < 8; c += 2) {
         const double v0 = h ? (double)tot[t][c].y + (double)cmp[t][c].y : (double)tot[t][c].x + (double)cmp[t][c].x;
         const double v1 =
             h ? (double)tot[t][c + 1].y + (double)cmp[t][c + 1].y : (double)tot[t][c + 1].x + (double)cmp[t][c + 1].x;
-        *reinterpret_cast<double2 *>(dst + c) = make_double2(v0, v1);
+        *reinterpret_cast<float2 *>(dst + c) = make_float2((float)v0, (float)v1);
       }
     }
 }
@@ -720,7 +720,7 @@ __global__ void __launch_bounds__(256) k_fm_epi(DevDb db, DevPot pot, const Spli
     for (int task = tid; task < na * CG; task += T) {
       const int a = task / CG;
       const int i = st.satom[a], lo = st.arow[a], n = st.arow[a + 1] - lo;
-      const double *Yq = fp.Y + ((size_t)gy * fp.Q + fp.row0[i]) * 3 * CG + cl;
+      const float *Yq = fp.Y + ((size_t)gy * fp.Q + fp.row0[i]) * 3 * CG + cl;
       double rho = 0.0, epair = 0.0;
 #pragma unroll 4
       for (int p = 0; p < n; ++p) {
@@ -728,7 +728,7 @@ __global__ void __launch_bounds__(256) k_fm_epi(DevDb db, DevPot pot, const Spli
         const double phi = fm_pair_one<double>(st, fp, ql, cl, 0, kn, tj, 0);
         const double rv = fm_pair_one<double>(st, fp, ql, cl, 1, kn, tj, 0);
         const double fv = fm_pair_one<double>(st, fp, ql, cl, 2, kn, tj, 0);
-        rho += rv + 0.5 * fv * Yq[(size_t)p * 3 * CG];
+        rho += rv + 0.5 * fv * (double)Yq[(size_t)p * 3 * CG];
         epair += 0.5 * phi;
       }
       const double w = db.cell_w[db.atom_cell[i]];
@@ -745,10 +745,10 @@ __global__ void __launch_bounds__(256) k_fm_epi(DevDb db, DevPot pot, const Spli
       double F[3] = {0, 0, 0}, S[6] = {0, 0, 0, 0, 0, 0};
       // slots in batches of FM_PB, every load of a batch before its stores
       for (int p0 = 0; p0 < n; p0 += FM_PB) {
-        double yv[FM_PB][3];
+        float yv[FM_PB][3];
 #pragma unroll
         for (int j = 0; j < FM_PB; ++j) {
-          const double *yp = Yq + (size_t)min(p0 + j, n - 1) * 3 * CG;
+          const float *yp = Yq + (size_t)min(p0 + j, n - 1) * 3 * CG;
           yv[j][0] = yp[0];
           yv[j][1] = yp[CG];
           yv[j][2] = yp[2 * CG];
@@ -765,7 +765,7 @@ __global__ void __launch_bounds__(256) k_fm_epi(DevDb db, DevPot pot, const Spli
           v.drho = fm_pair_one<double>(st, fp, ql, cl, 1, kn, tj, 1);
           fm_pair_val<double>(st, fp, ql, cl, 2, kn, tj, v.f, v.df);
         }
-        const double G = yv[j][0], Y1 = yv[j][1], Y2 = yv[j][2];
+        const double G = yv[j][0], Y1 = yv[j][1], Y2 = yv[j][2];  // FP32 sums, FP64 arithmetic
         const double *e = st.e + ql * 6;
         const int64_t gs = st.gs[ql];
         const double4 ur = st.ur[ql];
@@ -1002,7 +1002,7 @@ __global__ void __launch_bounds__(256, 2) k_fm_adj_pre(DevDb db, DevPot pot, con
       const int i = st.satom[a], lo = st.arow[a], n = st.arow[a + 1] - lo;
       const int cell = db.atom_cell[i];
       const int64_t q0 = fp.row0[i];
-      const double *Yq = fp.Y + ((size_t)gy * fp.Q + q0) * 3 * CG + cl;
+      float *Yq = fp.Y + ((size_t)gy * fp.Q + q0) * 3 * CG + cl;
       float *Ybq = fp.Yb + ((size_t)gy * fp.Q + q0) * 3 * CG + cl;
       // the atom's and its cell's candidate data
       const float *Li = fp.lamf + ((size_t)gy * N + i) * 3 * CG + cl;
@@ -1060,12 +1060,12 @@ __global__ void __launch_bounds__(256, 2) k_fm_adj_pre(DevDb db, DevPot pot, con
       // stores (the stores go to the same arrays, so the compiler would
       // otherwise keep each slot's loads behind the previous slot's stores)
       for (int p0 = 0; p0 < n; p0 += FM_PB) {
-        double yv[FM_PB][3];
+        float yv[FM_PB][3];
         float lj[FM_PB][3];
 #pragma unroll
         for (int j = 0; j < FM_PB; ++j) {
           const int p = min(p0 + j, n - 1);  // past the row: the last slot again, not used
-          const double *yp = Yq + (size_t)p * 3 * CG;
+          const float *yp = Yq + (size_t)p * 3 * CG;
           yv[j][0] = yp[0];
           yv[j][1] = yp[CG];
           yv[j][2] = yp[2 * CG];
@@ -1080,8 +1080,8 @@ __global__ void __launch_bounds__(256, 2) k_fm_adj_pre(DevDb db, DevPot pot, con
           if (p >= n) break;
           const int ql = lo + p;
           const FmPairVals<float> v = fm_pair_vals<float>(st, fp, ql, cl);
-          double *yp = const_cast<double *>(Yq) + (size_t)p * 3 * CG;
-          const float G = (float)yv[j][0], Y1 = (float)yv[j][1], Y2 = (float)yv[j][2];
+          float *yp = Yq + (size_t)p * 3 * CG;
+          const float G = yv[j][0], Y1 = yv[j][1], Y2 = yv[j][2];
           const float4 u = st.uf[ql];
           const float *e = reinterpret_cast<const float *>(st.e) + ql * 6;
           float lx, ly, lz;
@@ -1095,8 +1095,9 @@ __global__ void __launch_bounds__(256, 2) k_fm_adj_pre(DevDb db, DevPot pot, con
           float *yb = Ybq + (size_t)p * 3 * CG;
           yb[CG] = y1;
           yb[2 * CG] = y2;
-          *reinterpret_cast<float2 *>(yp) = make_float2(ap, G);
-          *reinterpret_cast<float2 *>(yp + CG) = make_float2(dF * t12, 0.f);  // whole words: no partial sectors
+          yp[0] = ap;
+          yp[CG] = G;
+          yp[2 * CG] = dF * t12;
           if (fp.zmax) {
             const char4 eq = *reinterpret_cast<const char4 *>(fp.xe + (q0 + p) * 4);
             zbound(q0 + p, max(zfield(y1, eq.y), zfield(y2, eq.z)));
@@ -1113,9 +1114,9 @@ __global__ void __launch_bounds__(256, 2) k_fm_adj_pre(DevDb db, DevPot pot, con
         float svv[2 * FM_PB];
 #pragma unroll
         for (int j = 0; j < 2 * FM_PB; ++j) {
-          const double *yp = Yq + (size_t)min(p0 + j, n - 1) * 3 * CG;
-          aGv[j] = *reinterpret_cast<const float2 *>(yp);
-          svv[j] = *reinterpret_cast<const float *>(yp + CG);
+          const float *yp = Yq + (size_t)min(p0 + j, n - 1) * 3 * CG;
+          aGv[j] = make_float2(yp[0], yp[CG]);
+          svv[j] = yp[2 * CG];
         }
 #pragma unroll
       for (int j = 0; j < 2 * FM_PB; ++j) {

@@ -260,7 +260,7 @@ __global__ void __launch_bounds__(FM8_THREADS, 1) k_fm_gemm_fwd8(FmPlan fp, int 
         tc::fence_after_sync();
         const int e = t == 0 ? eq.x : (t == 1 ? eq.y : eq.z);
         const double sq = __longlong_as_double((long long)(e - FM8_SHIFT + 1023) << 52);  // 2^(e - 30)
-        double *yo = fp.Y + (((size_t)gy * fp.Q + q) * 3 + t) * CG;
+        float *yo = fp.Y + (((size_t)gy * fp.Q + q) * 3 + t) * CG;
         const uint32_t ta = tm + ((uint32_t)(32 * quarter) << 16) + (uint32_t)(buf * 256);
         for (int cb = 0; cb < FM8_NC / 16 && cb * 16 < CG; ++cb) {
           int v[FM8_CLS][16];
@@ -277,7 +277,7 @@ __global__ void __launch_bounds__(FM8_THREADS, 1) k_fm_gemm_fwd8(FmPlan fp, int 
                                ((double)v[2][u + h] * 4294967296.0 + (double)v[3][u + h] * 16777216.0);
               y2[h] = a * sq * ssc[s * FM8_NC + cb * 16 + u + h];
             }
-            if (cb * 16 + u + 1 < CG) *reinterpret_cast<double2 *>(yo + cb * 16 + u) = make_double2(y2[0], y2[1]);
+            if (cb * 16 + u + 1 < CG) *reinterpret_cast<float2 *>(yo + cb * 16 + u) = make_float2((float)y2[0], (float)y2[1]);
           }
         }
         tc::fence_before_sync();
