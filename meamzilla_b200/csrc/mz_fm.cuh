@@ -102,7 +102,7 @@ constexpr int FM8_STAGE = FM8_DIG * FM8_XBLK;    // one (tile, kind, kblock): 64
 constexpr int FM8_BTYPE = 2 * FM8_DIG * FM8_KBLK;  // K8 of one type: 64 KB
 constexpr int FM8_SHIFT = 30;                    // |X_int|, |K_int| <= 2^30
 constexpr int FM8_NST = 8;                       // stages in the ring, one (tile, kind, kblock, digit) block each
-constexpr int FM8_THREADS = 192;
+constexpr int FM8_THREADS = 320;                 // producer, MMA, eight epilogue warps
 constexpr uint32_t FM8_WAIT = 1u << 26;          // polls before a wait gives up
 constexpr int FM8_SPAN_LOG = 3;
 constexpr int FM8_SPAN = 1 << FM8_SPAN_LOG;      // tiles per exponent span of the integer adjoint's operand

@@ -37,7 +37,7 @@
 // tiles' 16 KB digit blocks into an eight-stage ring (cp.async.bulk, completion
 // on an mbarrier), warp 1 issues the MMAs (M = 128 slots, N = 64 candidates, K = 32
 // bytes; ten digit pairs per K step into four class accumulators of 64
-// columns) and commits them to mbarriers, warps 2-5 read the accumulators of
+// columns) and commits them to mbarriers, warps 2-9 read the accumulators of
 // the previous (tile, kind) out of tensor memory (two sets of 256 columns, so
 // the MMAs of the next kind overlap the epilogue) and store Y.  The
 // candidates' digit blocks of the current atom type sit in shared memory and
@@ -129,7 +129,7 @@ __global__ void __launch_bounds__(FM8_THREADS, 1) k_fm_gemm_fwd8(FmPlan fp, int 
     }
     for (int b = 0; b < 2; ++b) {
       tc::mbar_init(accf + b, 1);
-      tc::mbar_init(acce + b, 4);
+      tc::mbar_init(acce + b, 8);
     }
     tc::mbar_init(bload, 1);
     tc::mbar_init(bfree, 1);
@@ -186,7 +186,6 @@ __global__ void __launch_bounds__(FM8_THREADS, 1) k_fm_gemm_fwd8(FmPlan fp, int 
   } else if (warp == 1) {
     // ---------------- MMA issue
     if (lane == 0) {
-      constexpr uint32_t idesc = tc::idesc_s8(FM8_TM, FM8_NC);
       bool ok = true;
       int64_t it = 0, seq = 0;
       int cur = -1, nb = 0;
@@ -211,8 +210,11 @@ __global__ void __launch_bounds__(FM8_THREADS, 1) k_fm_gemm_fwd8(FmPlan fp, int 
             break;
           }
           tc::fence_after_sync();
-          // one stage per digit i of the moments: the pairs (i, j), j <= 3 - i,
-          // of the classes i + j; each class starts with its pair (0, j)
+          // one stage per digit i of the moments.  The candidates' digit blocks
+          // j = 0..3 lie one after another (64 rows each), so one MMA of
+          // N = (4 - i) 64 takes the pairs (i, j), j <= 3 - i, at once; written
+          // from column 64 i, its column block j lands in class i + j.  The
+          // MMA of digit 0 starts every class's sum.
           for (int kb = 0; kb < 2 && ok; ++kb)
             for (int i = 0; i < FM8_DIG; ++i, ++it) {
               const int st = (int)(it % FM8_NST);
@@ -223,16 +225,14 @@ __global__ void __launch_bounds__(FM8_THREADS, 1) k_fm_gemm_fwd8(FmPlan fp, int 
               }
               tc::fence_after_sync();
               const uint32_t a0 = tc::smem_u32(sA + st * FM8_XBLK);
+              const uint32_t idesc_i = tc::idesc_s8(FM8_TM, (FM8_DIG - i) * FM8_NC);
+              const uint32_t d = tm + (uint32_t)(buf * 256 + i * FM8_NC);
 #pragma unroll
-              for (int kk = 0; kk < 4; ++kk)
-#pragma unroll
-                for (int j = 0; j < FM8_DIG; ++j)
-                  if (j < FM8_DIG - i) {
-                    const uint64_t ad = tc::desc_sw128(a0 + 32 * kk, 16, 1024);
-                    const uint64_t bd = tc::desc_sw128(b0 + (kb * FM8_DIG + j) * FM8_KBLK + 32 * kk, 16, 1024);
-                    const uint32_t d = tm + (uint32_t)(buf * 256 + (i + j) * FM8_NC);
-                    tc::mma_s8(d, ad, bd, idesc, (kb == 0 && kk == 0 && i == 0) ? 0u : 1u);
-                  }
+              for (int kk = 0; kk < 4; ++kk) {
+                const uint64_t ad = tc::desc_sw128(a0 + 32 * kk, 16, 1024);
+                const uint64_t bd = tc::desc_sw128(b0 + kb * FM8_DIG * FM8_KBLK + 32 * kk, 16, 1024);
+                tc::mma_s8(d, ad, bd, idesc_i, (kb == 0 && kk == 0 && i == 0) ? 0u : 1u);
+              }
               tc::commit(empty + st);  // the stage is free once these MMAs are done
             }
           if (ok) tc::commit(accf + buf);
@@ -242,8 +242,9 @@ __global__ void __launch_bounds__(FM8_THREADS, 1) k_fm_gemm_fwd8(FmPlan fp, int 
       if (!tc::mbar_wait(mdone, 0, FM8_WAIT)) atomicExch(err, 3);
     }
   } else {
-    // ---------------- epilogue: warps 2..5, TMEM lane quarter warp % 4
-    const int quarter = warp & 3, r = 32 * quarter + lane;
+    // ---------------- epilogue: warps 2..9, TMEM lane quarter warp % 4, candidate
+    // half (warp - 2) / 4
+    const int quarter = warp & 3, r = 32 * quarter + lane, ch = (warp - 2) >> 2;
     int64_t seq = 0;
     bool ok = true;
     for (int64_t T = tb; T < te && ok; ++T) {
@@ -262,7 +263,7 @@ __global__ void __launch_bounds__(FM8_THREADS, 1) k_fm_gemm_fwd8(FmPlan fp, int 
         const double sq = __longlong_as_double((long long)(e - FM8_SHIFT + 1023) << 52);  // 2^(e - 30)
         float *yo = fp.Y + (((size_t)gy * fp.Q + q) * 3 + t) * CG;
         const uint32_t ta = tm + ((uint32_t)(32 * quarter) << 16) + (uint32_t)(buf * 256);
-        for (int cb = 0; cb < FM8_NC / 16 && cb * 16 < CG; ++cb) {
+        for (int cb = 2 * ch; cb < 2 * ch + 2 && cb * 16 < CG; ++cb) {
           int v[FM8_CLS][16];
 #pragma unroll
           for (int m = 0; m < FM8_CLS; ++m) tc::tmem_ld16i(ta + m * FM8_NC + cb * 16, v[m]);
@@ -409,7 +410,6 @@ __global__ void __maxnreg__(96) k_fm_gemm_adj8(FmPlan fp, int ncand, int *__rest
   } else if (warp == 1) {
     // ---------------- MMA issue: A = moments (MN-major), B = Z (K-major)
     if (lane == 0) {
-      constexpr uint32_t idesc = tc::idesc_s8(FM8_TM, FM8_NC, 1, 0);
       bool ok = true, fresh = true;  // fresh: the next tile starts a segment
       int64_t ia = 0, ib = 0, seg = 0;
       for (int64_t T = tb; T < te && ok; ++T) {
@@ -428,8 +428,10 @@ __global__ void __maxnreg__(96) k_fm_gemm_adj8(FmPlan fp, int ncand, int *__rest
           }
           tc::fence_after_sync();
           const uint32_t b0 = tc::smem_u32(sB + bst * FM8_ZSTAGE);
-          // one stage per digit i of the moments: the pairs (i, j), j <= 3 - i,
-          // of the classes i + j; each class starts with its pair (0, j)
+          // one stage per digit i of the moments; Z's digit blocks j = 0..3 lie
+          // one after another (64 rows each), so one MMA of N = (4 - i) 64
+          // takes the pairs (i, j), j <= 3 - i, with its column block j in
+          // class i + j (written from column 64 i); digit 0 starts the sums
           for (int kb = 0; kb < 2 && ok; ++kb)
             for (int i = 0; i < FM8_DIG; ++i) {
               const int ast = (int)(ia % FM8_NST);
@@ -440,16 +442,15 @@ __global__ void __maxnreg__(96) k_fm_gemm_adj8(FmPlan fp, int ncand, int *__rest
               }
               tc::fence_after_sync();
               const uint32_t a0 = tc::smem_u32(sA + ast * FM8_XBLK);
-#pragma unroll 1
-              for (int kk = 0; kk < 4; ++kk)
-#pragma unroll 1
-                for (int j = 0; j < FM8_DIG - i; ++j) {
-                  // 32 slot rows per K step: 4 groups of 8 rows, 1 KiB apart
-                  const uint64_t ad = tc::desc_sw128(a0 + 4096 * kk, FM8_STAGE, 1024);
-                  const uint64_t bd = tc::desc_sw128(b0 + j * FM8_ZBLK + 32 * kk, 16, 1024);
-                  const uint32_t d = tm + (uint32_t)(kb * 256 + (i + j) * FM8_NC);
-                  tc::mma_s8(d, ad, bd, idesc, (fresh && t == 0 && kk == 0 && i == 0) ? 0u : 1u);
-                }
+              const uint32_t idesc_i = tc::idesc_s8(FM8_TM, (FM8_DIG - i) * FM8_NC, 1, 0);
+              const uint32_t d = tm + (uint32_t)(kb * 256 + i * FM8_NC);
+#pragma unroll
+              for (int kk = 0; kk < 4; ++kk) {
+                // 32 slot rows per K step: 4 groups of 8 rows, 1 KiB apart
+                const uint64_t ad = tc::desc_sw128(a0 + 4096 * kk, FM8_STAGE, 1024);
+                const uint64_t bd = tc::desc_sw128(b0 + 32 * kk, 16, 1024);
+                tc::mma_s8(d, ad, bd, idesc_i, (fresh && t == 0 && kk == 0 && i == 0) ? 0u : 1u);
+              }
               tc::commit(aempty + ast);
               ++ia;
             }
