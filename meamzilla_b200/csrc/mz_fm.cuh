@@ -49,7 +49,8 @@ constexpr int FM_MAXB = 24;    // B-spline coefficients of any spline the path r
 constexpr int FM_SUB = 16;     // feature slots per sub-tile of the adjoint contraction
 constexpr int FM_ROWS = 8;     // features per thread in the adjoint contraction
 constexpr int FM_PCHUNK = 32;  // slots per chunk of the pair-function gradient
-constexpr int FM_PB = 4;       // slots per batch of loads in the epilogues' row walks
+constexpr int FM_PB = 4;       // slots per batch of loads in the row walks (the pre pass's second: 2 FM_PB)
+constexpr int FM_PBW = 2 * FM_PB;
 
 struct FmPlan {
   int nt;          // atom types
@@ -1109,17 +1110,17 @@ __global__ void __launch_bounds__(256, 2) k_fm_adj_pre(DevDb db, DevPot pot, con
                         [&](int ix, double x) { atomicAdd(utab + (size_t)cl * fp.ustride + (gU.toff - fp.utoff) + ix, x); });
       // ---- pass 2: dL/dG and the pair-function gradients
       const float epsf = (float)eps;
-      for (int p0 = 0; p0 < n; p0 += 2 * FM_PB) {
-        float2 aGv[2 * FM_PB];
-        float svv[2 * FM_PB];
+      for (int p0 = 0; p0 < n; p0 += FM_PBW) {
+        float2 aGv[FM_PBW];
+        float svv[FM_PBW];
 #pragma unroll
-        for (int j = 0; j < 2 * FM_PB; ++j) {
+        for (int j = 0; j < FM_PBW; ++j) {
           const float *yp = Yq + (size_t)min(p0 + j, n - 1) * 3 * CG;
           aGv[j] = make_float2(yp[0], yp[CG]);
           svv[j] = yp[2 * CG];
         }
 #pragma unroll
-      for (int j = 0; j < 2 * FM_PB; ++j) {
+      for (int j = 0; j < FM_PBW; ++j) {
         const int p = p0 + j;
         if (p >= n) break;
         const int ql = lo + p;
