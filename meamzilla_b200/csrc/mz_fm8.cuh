@@ -35,8 +35,10 @@
 // k_fm_gemm_fwd8: persistent, one CTA per SM over a contiguous run of 128-slot
 // tiles (type-pure: each type's slots are padded to 128).  Warp 0 streams the
 // tiles' 16 KB digit blocks into an eight-stage ring (cp.async.bulk, completion
-// on an mbarrier), warp 1 issues the MMAs (M = 128 slots, N = 64 candidates, K = 32
-// bytes; ten digit pairs per K step into four class accumulators of 64
+// on an mbarrier), warp 1 issues the MMAs (M = 128 slots, K = 32 bytes; per K
+// step one MMA per digit i of the moments, N = (4 - i) x 64 over the
+// candidates' stacked digit blocks, written from column 64 i so that its
+// column block j lands in the class accumulator i + j; four classes of 64
 // columns) and commits them to mbarriers, warps 2-9 read the accumulators of
 // the previous (tile, kind) out of tensor memory (two sets of 256 columns, so
 // the MMAs of the next kind overlap the epilogue) and store Y.  The
@@ -309,13 +311,15 @@ namespace mzb {
 // (|Z| < 2^e_Sc over the span) in fp.zmax.  The digits never reach global
 // memory: sixteen converter warps read Ybar (FP32) of each (tile, kind) and
 // write Z's digits straight into the shared-memory stage the MMA reads, a
-// K-major operand (N = 64 candidates, K = slots, rows of 128 slot bytes).
+// K-major operand (64 candidates per digit block, the four blocks stacked
+// along N; K = slots, rows of 128 slot bytes).
 // The MMA reads the moments' digit blocks as they are stored for the
 // forward -- 128 slot rows of 128 feature bytes -- as an MN-major operand
 // (M = 128 features, K = slots: 8-row groups 1 KiB apart).  One tile's three
-// kinds are 3 x 4 K steps of 32 slots per 128-feature half, ten digit pairs
-// each, into the four class accumulators of each half (all 512 TMEM
-// columns).  The accumulators carry the sums of a whole segment -- the tiles
+// kinds are 3 x 4 K steps of 32 slots per 128-feature half, with one MMA per
+// digit i of the moments (N = (4 - i) x 64 over Z's stacked digit blocks, as
+// in the forward), into the four class accumulators of each half (all 512
+// TMEM columns).  The accumulators carry the sums of a whole segment -- the tiles
 // of one span and one atom type in this CTA's run -- exactly (at most
 // 4 x 384 x FM8_SPAN x 128^2 < 2^31), and at its end the same sixteen warps
 // (lane quarter x feature half x candidate half) read them out and add
