@@ -627,7 +627,11 @@ def run_mine(args, world, rank, local):
     step_flops = 3 * fwd * args.ncand
     roof_step = {"algorithmic_flops": step_flops, "achieved_tflops": step_flops / (ms / args.steps * 1e-3) / 1e12,
                  "frac_fp32": step_flops / (ms / args.steps * 1e-3) / 1e12 / fp32_peak,
-                 "algorithmic_bytes": b32}
+                 "algorithmic_bytes": b32,
+                 "note": "flops of the per-triplet formulation (forward + 2x adjoint); the triplet-moment path "
+                         "runs the triplet sums as integer tensor-core contractions instead, so this rate can "
+                         "exceed the FP32 FMA peak" if tuned.get("triplet_moments") else
+                         "flops of the per-triplet formulation (forward + 2x adjoint)"}
     roof_fp64 = {"bound": "fp64", "achieved": fwd / (ms64 / k64 * 1e-3) / 1e12, "peak": fp64_peak,
                  "unit": "TFLOP/s", "frac": fwd / (ms64 / k64 * 1e-3) / 1e12 / fp64_peak,
                  "algorithmic_flops": fwd}
